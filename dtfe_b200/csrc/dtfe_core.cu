@@ -1,0 +1,832 @@
+// DTFE interpolation path on B200 (sm_100a): kernels and the C ABI of
+// include/dtfe_gpu.h.
+//
+// Pipeline per call (all on the handle's stream):
+//   k_volume_scatter   one thread per tetrahedron: signed volume in FP64,
+//                      scattered to its four vertices (FP64 reduction),
+//                      hull-face marks, lowest incident tetrahedron per vertex
+//   k_vertex_density   rho_v = w (D+1)/(rho_bar sum V), 0 on the hull
+//                      (vertexDensity, triangulation.cpp:200-279)
+//   k_seed_bins        lowest vertex id per grid cell of each tile: the walk
+//                      seed of a sample is an incident tetrahedron of a vertex
+//                      lying in the sample's own cell
+//   k_interpolate      one thread per grid cell: walk to the cell centre,
+//                      evaluate (or average over n points, each walked from
+//                      the centre's tetrahedron as in
+//                      averaged_interpolation_2.cc:123,145), derive
+//                      divergence/shear/vorticity in the epilogue, write every
+//                      requested field once.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/dtfe_gpu.h"
+#include "dtfe_device.cuh"
+#include "philox.h"
+
+using namespace dtfe;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int set_error(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define DTFE_CUDA_TRY(expr)                                                          \
+  do {                                                                               \
+    cudaError_t _e = (expr);                                                         \
+    if (_e != cudaSuccess)                                                           \
+      return set_error(DTFE_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+constexpr int kEmptyBin = 0x7F7F7F7F;  // memset(0x7F) value; above any vertex id
+enum { CNT_LOCATED, CNT_OUTSIDE, CNT_FAIL, CNT_STEPS, CNT_EXACT, CNT_TIES, CNT_N };
+
+// ---------------------------------------------------------------------------
+__global__ void k_pack_xyz(int64_t n, const float* __restrict__ xyz, float4* __restrict__ out, float wval) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], wval);
+}
+
+__global__ void k_volume_scatter(int64_t T, const int4* __restrict__ tet_v, const int4* __restrict__ tet_n,
+                                 const float4* __restrict__ posd, double* __restrict__ volsum,
+                                 int* __restrict__ hull, int* __restrict__ vtx_tet) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= T) return;
+  int4 v = __ldg(&tet_v[t]);
+  int4 n = __ldg(&tet_n[t]);
+  double X[4][3];
+  load_pos(posd, v.x, X[0]);
+  load_pos(posd, v.y, X[1]);
+  load_pos(posd, v.z, X[2]);
+  load_pos(posd, v.w, X[3]);
+  double vt = orient_det(X[0], X[1], X[2], X[3]) / 6.0;
+  atomicAdd(&volsum[v.x], vt);
+  atomicAdd(&volsum[v.y], vt);
+  atomicAdd(&volsum[v.z], vt);
+  atomicAdd(&volsum[v.w], vt);
+  int ti = (int)t;
+  atomicMin(&vtx_tet[v.x], ti);
+  atomicMin(&vtx_tet[v.y], ti);
+  atomicMin(&vtx_tet[v.z], ti);
+  atomicMin(&vtx_tet[v.w], ti);
+  if (n.x < 0) { hull[v.y] = 1; hull[v.z] = 1; hull[v.w] = 1; }
+  if (n.y < 0) { hull[v.x] = 1; hull[v.z] = 1; hull[v.w] = 1; }
+  if (n.z < 0) { hull[v.x] = 1; hull[v.y] = 1; hull[v.w] = 1; }
+  if (n.w < 0) { hull[v.x] = 1; hull[v.y] = 1; hull[v.z] = 1; }
+}
+
+__global__ void k_vertex_density(int64_t V, const float* __restrict__ w, const double* __restrict__ volsum,
+                                 const int* __restrict__ hull, float factor, float4* __restrict__ posd) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= V) return;
+  double vol = volsum[i];
+  float d = (hull[i] || vol == 0.0) ? 0.f : (float)((double)(w[i] * factor) / vol);
+  posd[i].w = d;
+}
+
+__device__ __forceinline__ int find_box(const int64_t* __restrict__ prefix, int K, int64_t s) {
+  int lo = 0, hi = K;  // prefix[lo] <= s < prefix[hi]
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (__ldg(&prefix[mid]) <= s) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void k_seed_bins(int64_t V, const float4* __restrict__ posd, const int* __restrict__ vtx_tet,
+                            const dtfe_subbox* __restrict__ boxes, const int64_t* __restrict__ vprefix,
+                            const int64_t* __restrict__ bin_offset, int K, int* __restrict__ bins) {
+  int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (v >= V) return;
+  int t = vtx_tet[v];
+  if (t < 0 || t >= kEmptyBin) return;  // not a vertex of any tetrahedron
+  int b = find_box(vprefix, K, v);
+  const dtfe_subbox& B = boxes[b];
+  float4 q = posd[v];
+  float c[3] = {q.x, q.y, q.z};
+  int idx[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float f = floorf((c[a] - B.lo[a]) / B.dx[a]);
+    if (!(f >= 0.f && f < (float)B.tile_dims[a])) return;
+    idx[a] = (int)f;
+  }
+  int64_t local = ((int64_t)idx[0] * B.tile_dims[1] + idx[1]) * B.tile_dims[2] + idx[2];
+  atomicMin(&bins[bin_offset[b] + local], (int)v);
+}
+
+struct InterpParams {
+  const int4* tet_v;
+  const int4* tet_n;
+  const float4* posd;
+  const float4* vel4;
+  const float* scal;
+  const int* vtx_tet;
+  const int* bins;
+  const dtfe_subbox* boxes;
+  const int64_t* tile_prefix;
+  const int64_t* bin_offset;
+  const float* eq_off;  // K * NN * 3 equidistant offsets (method 3)
+  const float* xs;
+  const float* ys;
+  const float* zs;
+  int K;
+  int64_t G1, G2;
+  int64_t n_total;
+  int NN;
+  uint64_t seed;
+  uint32_t fields;
+  int fix;
+  int max_steps;
+  float* out[DTFE_NUM_FIELDS];
+  unsigned long long* counters;
+};
+
+__device__ __forceinline__ bool has_field(uint32_t f, int slot) { return (f >> slot) & 1u; }
+
+template <int METHOD, int S>
+__global__ void __launch_bounds__(256) k_interpolate(InterpParams P) {
+  const uint32_t F = P.fields;
+  const bool want_grad = has_field(F, DTFE_VELOCITY_GRADIENT) || has_field(F, DTFE_VELOCITY_DIVERGENCE) ||
+                         has_field(F, DTFE_VELOCITY_SHEAR) || has_field(F, DTFE_VELOCITY_VORTICITY);
+  const bool want_vel = has_field(F, DTFE_VELOCITY) || want_grad || has_field(F, DTFE_VELOCITY_STD);
+  const bool want_dens = has_field(F, DTFE_DENSITY);
+  const bool want_sc = S > 0 && (has_field(F, DTFE_SCALAR) || has_field(F, DTFE_SCALAR_GRADIENT));
+  const bool want_std = METHOD == DTFE_METHOD_MONTE_CARLO && has_field(F, DTFE_VELOCITY_STD);
+  const bool fix = P.fix != 0;
+  WalkStats st{0, 0, 0};
+  unsigned n_loc = 0, n_out = 0, n_fail = 0;
+
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.n_total; s += stride) {
+    const int b = find_box(P.tile_prefix, P.K, s);
+    const dtfe_subbox& B = P.boxes[b];
+    const int64_t local = s - __ldg(&P.tile_prefix[b]);
+    const int nz = B.tile_dims[2], ny = B.tile_dims[1];
+    const int k = (int)(local % nz);
+    const int j = (int)((local / nz) % ny);
+    const int i = (int)(local / ((int64_t)nz * ny));
+    const float x = __ldg(&P.xs[B.coord_offset[0] + i]);
+    const float y = __ldg(&P.ys[B.coord_offset[1] + j]);
+    const float z = __ldg(&P.zs[B.coord_offset[2] + k]);
+    const int64_t cell = ((int64_t)(B.tile_origin[0] + i) * P.G1 + (B.tile_origin[1] + j)) * P.G2 +
+                         (B.tile_origin[2] + k);
+    // seed: a vertex in this cell, else in a neighbouring cell along z/y/x
+    const int* bins = P.bins + __ldg(&P.bin_offset[b]);
+    int sv = __ldg(&bins[local]);
+    if (sv >= kEmptyBin) {
+      const int64_t cand[6] = {k > 0 ? local - 1 : -1, k + 1 < nz ? local + 1 : -1,
+                               j > 0 ? local - nz : -1, j + 1 < ny ? local + nz : -1,
+                               i > 0 ? local - (int64_t)nz * ny : -1,
+                               i + 1 < B.tile_dims[0] ? local + (int64_t)nz * ny : -1};
+#pragma unroll
+      for (int c = 0; c < 6; ++c)
+        if (sv >= kEmptyBin && cand[c] >= 0) sv = __ldg(&bins[cand[c]]);
+    }
+    int t0 = sv < kEmptyBin ? __ldg(&P.vtx_tet[sv]) : (int)B.tet_offset;
+    if (t0 < B.tet_offset || t0 >= B.tet_offset + B.n_tets) t0 = (int)B.tet_offset;
+
+    const double pc[3] = {(double)x, (double)y, (double)z};
+    int v[4];
+    double X[4][3];
+    int tc = walk_locate(P.tet_v, P.tet_n, P.posd, pc, t0, P.max_steps, v, X, st);
+    ++n_loc;
+    if (tc == kWalkFail) { ++n_fail; tc = kOutside; }
+
+    float aD = 0.f, aV[3] = {0.f, 0.f, 0.f}, aG[9], aS[S > 0 ? S : 1], aSG[S > 0 ? 3 * S : 1];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) aG[c] = 0.f;
+#pragma unroll
+    for (int q = 0; q < (S > 0 ? S : 1); ++q) aS[q] = 0.f;
+#pragma unroll
+    for (int q = 0; q < (S > 0 ? 3 * S : 1); ++q) aSG[q] = 0.f;
+    float stdacc[3] = {0.f, 0.f, 0.f};
+
+    if (METHOD == DTFE_METHOD_CENTRE) {
+      if (tc >= 0) {
+        CellOut e;
+        cell_eval<S>(v, X, pc, P.posd, P.vel4, P.scal, want_dens, want_vel, want_sc, fix, e);
+        aD = e.dens;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) aV[c] = e.vel[c];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) aG[c] = e.grad[c];
+#pragma unroll
+        for (int q = 0; q < S; ++q) {
+          aS[q] = e.sc[q];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) aSG[3 * q + c] = e.scg[3 * q + c];
+        }
+      } else {
+        ++n_out;
+      }
+    } else {
+      if (tc < 0) ++n_out;
+      const int NN = P.NN;
+      const uint64_t key = mc_key(P.seed, B.part_no);
+      const int tstart = tc >= 0 ? tc : t0;
+      // velocity standard deviation: two passes over the sample velocities
+      // (standardDeviation, triangulation_miscellaneous.cc:256-271); the
+      // first pass accumulates the mean, the second re-walks the samples.
+      for (int w = 0; w < NN; ++w) {
+        double p[3];
+        if (METHOD == DTFE_METHOD_MONTE_CARLO) {
+          double u[3];
+          mc_offsets(key, (uint64_t)cell, (uint32_t)w, u);
+          p[0] = u[0] * (double)B.dx[0] + pc[0];
+          p[1] = u[1] * (double)B.dx[1] + pc[1];
+          p[2] = u[2] * (double)B.dx[2] + pc[2];
+        } else {
+          const float* eo = P.eq_off + ((int64_t)b * NN + w) * 3;
+          p[0] = (double)(x + __ldg(&eo[0]));
+          p[1] = (double)(y + __ldg(&eo[1]));
+          p[2] = (double)(z + __ldg(&eo[2]));
+        }
+        int vv[4];
+        double XX[4][3];
+        int t = walk_locate(P.tet_v, P.tet_n, P.posd, p, tstart, P.max_steps, vv, XX, st);
+        ++n_loc;
+        if (t == kWalkFail) { ++n_fail; t = kOutside; }
+        if (t < 0) continue;
+        CellOut e;
+        cell_eval<S>(vv, XX, p, P.posd, P.vel4, P.scal, want_dens, want_vel, want_sc, fix, e);
+        aD += e.dens;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) aV[c] += e.vel[c];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) aG[c] += e.grad[c];
+#pragma unroll
+        for (int q = 0; q < S; ++q) {
+          aS[q] += e.sc[q];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) aSG[3 * q + c] += e.scg[3 * q + c];
+        }
+        if (want_std) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) stdacc[c] += e.vel[c];
+        }
+      }
+      const float fn = (float)NN;
+      aD = aD / fn;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) aV[c] = aV[c] / fn;
+#pragma unroll
+      for (int c = 0; c < 9; ++c) aG[c] = aG[c] / fn;
+#pragma unroll
+      for (int q = 0; q < S; ++q) {
+        aS[q] = aS[q] / fn;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) aSG[3 * q + c] = aSG[3 * q + c] / fn;
+      }
+      if (want_std) {
+        float mean[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) mean[c] = stdacc[c] / fn;
+        float r = 0.f;
+        for (int w = 0; w < NN; ++w) {
+          float vel[3] = {0.f, 0.f, 0.f};
+          double u[3], p[3];
+          mc_offsets(key, (uint64_t)cell, (uint32_t)w, u);
+          p[0] = u[0] * (double)B.dx[0] + pc[0];
+          p[1] = u[1] * (double)B.dx[1] + pc[1];
+          p[2] = u[2] * (double)B.dx[2] + pc[2];
+          int vv[4];
+          double XX[4][3];
+          WalkStats st2{0, 0, 0};
+          int t = walk_locate(P.tet_v, P.tet_n, P.posd, p, tstart, P.max_steps, vv, XX, st2);
+          if (t >= 0) {
+            CellOut e;
+            cell_eval<0>(vv, XX, p, P.posd, P.vel4, P.scal, false, true, false, fix, e);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) vel[c] = e.vel[c];
+          }
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            float d = vel[c] - mean[c];
+            r += d * d;
+          }
+        }
+        P.out[DTFE_VELOCITY_STD][cell] = sqrtf(r / fn);
+      }
+    }
+
+    if (has_field(F, DTFE_DENSITY)) P.out[DTFE_DENSITY][cell] = aD;
+    if (has_field(F, DTFE_VELOCITY)) {
+      float* o = P.out[DTFE_VELOCITY] + 3 * cell;
+      o[0] = aV[0]; o[1] = aV[1]; o[2] = aV[2];
+    }
+    if (has_field(F, DTFE_VELOCITY_GRADIENT)) {
+      float* o = P.out[DTFE_VELOCITY_GRADIENT] + 9 * cell;
+#pragma unroll
+      for (int c = 0; c < 9; ++c) o[c] = aG[c];
+    }
+    if (has_field(F, DTFE_VELOCITY_DIVERGENCE) || has_field(F, DTFE_VELOCITY_SHEAR) ||
+        has_field(F, DTFE_VELOCITY_VORTICITY)) {
+      float dv, sh[5], vo[3];
+      derived_fields(aG, dv, sh, vo);
+      if (has_field(F, DTFE_VELOCITY_DIVERGENCE)) P.out[DTFE_VELOCITY_DIVERGENCE][cell] = dv;
+      if (has_field(F, DTFE_VELOCITY_SHEAR)) {
+        float* o = P.out[DTFE_VELOCITY_SHEAR] + 5 * cell;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) o[c] = sh[c];
+      }
+      if (has_field(F, DTFE_VELOCITY_VORTICITY)) {
+        float* o = P.out[DTFE_VELOCITY_VORTICITY] + 3 * cell;
+        o[0] = vo[0]; o[1] = vo[1]; o[2] = vo[2];
+      }
+    }
+    if (S > 0 && has_field(F, DTFE_SCALAR)) {
+      float* o = P.out[DTFE_SCALAR] + (int64_t)S * cell;
+#pragma unroll
+      for (int q = 0; q < S; ++q) o[q] = aS[q];
+    }
+    if (S > 0 && has_field(F, DTFE_SCALAR_GRADIENT)) {
+      float* o = P.out[DTFE_SCALAR_GRADIENT] + (int64_t)3 * S * cell;
+#pragma unroll
+      for (int q = 0; q < 3 * S; ++q) o[q] = aSG[q];
+    }
+  }
+  // fold the per-thread counters into the global ones, one atomic per warp
+  unsigned vals[CNT_N] = {n_loc, n_out, n_fail, (unsigned)st.steps, (unsigned)st.exact, (unsigned)st.tie};
+#pragma unroll
+  for (int c = 0; c < CNT_N; ++c) {
+    unsigned r = __reduce_add_sync(0xffffffffu, vals[c]);
+    if ((threadIdx.x & 31) == 0 && r) atomicAdd(&P.counters[c], (unsigned long long)r);
+  }
+}
+
+// Locate arbitrary points (tests): canonical tetrahedron or -1 / -2.
+__global__ void k_locate_points(int64_t np, const double* __restrict__ pts, const int4* __restrict__ tet_v,
+                                const int4* __restrict__ tet_n, const float4* __restrict__ posd,
+                                int start, int max_steps, int* __restrict__ out) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  double p[3] = {pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
+  int v[4];
+  double X[4][3];
+  WalkStats st{0, 0, 0};
+  out[i] = walk_locate(tet_v, tet_n, posd, p, start, max_steps, v, X, st);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Handle
+struct dtfe_gpu_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int S = 0;
+  int max_steps = 65536;
+  int64_t T = 0, V = 0;
+  int4* tet_v = nullptr;
+  int4* tet_n = nullptr;
+  float4* posd = nullptr;
+  float4* vel4 = nullptr;
+  float* scal = nullptr;
+  float* w = nullptr;
+  double* volsum = nullptr;
+  int* hull = nullptr;
+  int* vtx_tet = nullptr;
+  bool has_vel = false, has_scal = false;
+  bool density_ready = false;
+  // sub-boxes
+  int K = 0;
+  std::vector<dtfe_subbox> boxes_h;
+  dtfe_subbox* boxes = nullptr;
+  int64_t* tile_prefix = nullptr;
+  int64_t* vprefix = nullptr;
+  int64_t* bin_offset = nullptr;
+  int* bins = nullptr;
+  int64_t n_cells = 0;
+  float *xs = nullptr, *ys = nullptr, *zs = nullptr;
+  int32_t grid[3] = {0, 0, 0};
+  bool bins_ready = false;
+  float* eq_off = nullptr;
+  int eq_nn = 0;
+  unsigned long long* counters = nullptr;
+  float* out_buf[DTFE_NUM_FIELDS] = {};
+  size_t out_cap[DTFE_NUM_FIELDS] = {};
+};
+
+namespace {
+
+template <typename Tp>
+int dev_alloc(Tp** p, size_t count) {
+  if (*p) {
+    cudaFree(*p);
+    *p = nullptr;
+  }
+  if (count == 0) return DTFE_OK;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(Tp));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return set_error(DTFE_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  return DTFE_OK;
+}
+
+inline unsigned blocks_for(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+int field_components(int slot, int S) {
+  switch (slot) {
+    case DTFE_DENSITY: return 1;
+    case DTFE_VELOCITY: return 3;
+    case DTFE_VELOCITY_GRADIENT: return 9;
+    case DTFE_VELOCITY_DIVERGENCE: return 1;
+    case DTFE_VELOCITY_SHEAR: return 5;
+    case DTFE_VELOCITY_VORTICITY: return 3;
+    case DTFE_VELOCITY_STD: return 1;
+    case DTFE_SCALAR: return S;
+    case DTFE_SCALAR_GRADIENT: return 3 * S;
+  }
+  return 0;
+}
+
+int prepare_bins(dtfe_handle h) {
+  if (h->bins_ready) return DTFE_OK;
+  if (!h->density_ready) return set_error(DTFE_ERR_STATE, "vertex density not computed");
+  DTFE_CUDA_TRY(cudaMemsetAsync(h->bins, 0x7F, sizeof(int) * h->n_cells, h->stream));
+  k_seed_bins<<<blocks_for(h->V, 256), 256, 0, h->stream>>>(h->V, h->posd, h->vtx_tet, h->boxes, h->vprefix,
+                                                           h->bin_offset, h->K, h->bins);
+  DTFE_CUDA_TRY(cudaGetLastError());
+  h->bins_ready = true;
+  return DTFE_OK;
+}
+
+template <int METHOD>
+void launch_interp_s(const InterpParams& P, int S, cudaStream_t st, unsigned grid, unsigned block) {
+  switch (S) {
+    case 0: k_interpolate<METHOD, 0><<<grid, block, 0, st>>>(P); break;
+    case 1: k_interpolate<METHOD, 1><<<grid, block, 0, st>>>(P); break;
+    case 2: k_interpolate<METHOD, 2><<<grid, block, 0, st>>>(P); break;
+    case 3: k_interpolate<METHOD, 3><<<grid, block, 0, st>>>(P); break;
+    case 4: k_interpolate<METHOD, 4><<<grid, block, 0, st>>>(P); break;
+    default: k_interpolate<METHOD, 8><<<grid, block, 0, st>>>(P); break;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* dtfe_last_error(void) { return g_last_error.c_str(); }
+
+int dtfe_gpu_create(const dtfe_config* cfg, dtfe_handle* out) {
+  if (!out) return set_error(DTFE_ERR_ARG, "null output handle");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_error(DTFE_ERR_NO_DEVICE, "no CUDA device");
+  dtfe_config c = cfg ? *cfg : dtfe_config{0, 0, 0, 0};
+  if (c.device < 0 || c.device >= ndev) return set_error(DTFE_ERR_ARG, "bad device ordinal");
+  if (c.n_scalars < 0 || c.n_scalars > DTFE_MAX_SCALARS || c.n_scalars == 5 || c.n_scalars == 6 ||
+      c.n_scalars == 7)
+    return set_error(DTFE_ERR_ARG, "n_scalars must be 0-4 or 8");
+  DTFE_CUDA_TRY(cudaSetDevice(c.device));
+  dtfe_handle h = new dtfe_gpu_s();
+  h->device = c.device;
+  h->S = c.n_scalars;
+  h->max_steps = c.max_walk_steps > 0 ? c.max_walk_steps : 65536;
+  cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete h;
+    return set_error(DTFE_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+  }
+  int rc = dev_alloc(&h->counters, CNT_N);
+  if (rc) {
+    cudaStreamDestroy(h->stream);
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return DTFE_OK;
+}
+
+int dtfe_gpu_destroy(dtfe_handle h) {
+  if (!h) return DTFE_OK;
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->stream);
+  void* ptrs[] = {h->tet_v, h->tet_n, h->posd, h->vel4, h->scal, h->w, h->volsum, h->hull,
+                  h->vtx_tet, h->boxes, h->tile_prefix, h->vprefix, h->bin_offset, h->bins,
+                  h->xs, h->ys, h->zs, h->eq_off, h->counters};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  for (int i = 0; i < DTFE_NUM_FIELDS; ++i)
+    if (h->out_buf[i]) cudaFree(h->out_buf[i]);
+  cudaStreamDestroy(h->stream);
+  delete h;
+  return DTFE_OK;
+}
+
+void* dtfe_gpu_stream(dtfe_handle h) { return h ? (void*)h->stream : nullptr; }
+
+int dtfe_gpu_synchronize(dtfe_handle h) {
+  if (!h) return set_error(DTFE_ERR_ARG, "null handle");
+  DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return DTFE_OK;
+}
+
+int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n, int64_t n_tets,
+                    const float* xyz, const float* w, const float* vel, const float* scal,
+                    int64_t n_verts) {
+  if (!h || !tet_v || !tet_n || !xyz || !w) return set_error(DTFE_ERR_ARG, "null argument");
+  if (n_tets < 0 || n_verts < 0 || n_tets > 0x7FFFFFFF || n_verts >= 0x7F7F7F7F)
+    return set_error(DTFE_ERR_TOO_LARGE, "tetrahedron or vertex count beyond int32 indexing");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  int rc;
+  h->T = n_tets;
+  h->V = n_verts;
+  if ((rc = dev_alloc(&h->tet_v, n_tets)) || (rc = dev_alloc(&h->tet_n, n_tets)) ||
+      (rc = dev_alloc(&h->posd, n_verts)) || (rc = dev_alloc(&h->vel4, n_verts)) ||
+      (rc = dev_alloc(&h->w, n_verts)) || (rc = dev_alloc(&h->volsum, n_verts)) ||
+      (rc = dev_alloc(&h->hull, n_verts)) || (rc = dev_alloc(&h->vtx_tet, n_verts)) ||
+      (rc = dev_alloc(&h->scal, (size_t)n_verts * h->S)))
+    return rc;
+  cudaStream_t st = h->stream;
+  if (n_tets) {
+    DTFE_CUDA_TRY(cudaMemcpyAsync(h->tet_v, tet_v, 16 * n_tets, cudaMemcpyHostToDevice, st));
+    DTFE_CUDA_TRY(cudaMemcpyAsync(h->tet_n, tet_n, 16 * n_tets, cudaMemcpyHostToDevice, st));
+  }
+  if (n_verts) {
+    // positions and velocities arrive as 3 floats per vertex; pack them into
+    // 16-byte records on the device
+    float* tmp = nullptr;
+    DTFE_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(float) * 3 * n_verts, st));
+    DTFE_CUDA_TRY(cudaMemcpyAsync(tmp, xyz, sizeof(float) * 3 * n_verts, cudaMemcpyHostToDevice, st));
+    k_pack_xyz<<<blocks_for(n_verts, 256), 256, 0, st>>>(n_verts, tmp, h->posd, 0.f);
+    if (vel) {
+      DTFE_CUDA_TRY(cudaMemcpyAsync(tmp, vel, sizeof(float) * 3 * n_verts, cudaMemcpyHostToDevice, st));
+      k_pack_xyz<<<blocks_for(n_verts, 256), 256, 0, st>>>(n_verts, tmp, h->vel4, 0.f);
+    } else {
+      DTFE_CUDA_TRY(cudaMemsetAsync(h->vel4, 0, sizeof(float4) * n_verts, st));
+    }
+    DTFE_CUDA_TRY(cudaFreeAsync(tmp, st));
+    DTFE_CUDA_TRY(cudaMemcpyAsync(h->w, w, sizeof(float) * n_verts, cudaMemcpyHostToDevice, st));
+    if (h->S > 0) {
+      if (scal)
+        DTFE_CUDA_TRY(cudaMemcpyAsync(h->scal, scal, sizeof(float) * h->S * n_verts, cudaMemcpyHostToDevice, st));
+      else
+        DTFE_CUDA_TRY(cudaMemsetAsync(h->scal, 0, sizeof(float) * h->S * n_verts, st));
+    }
+  }
+  DTFE_CUDA_TRY(cudaGetLastError());
+  h->has_vel = vel != nullptr;
+  h->has_scal = scal != nullptr;
+  h->density_ready = false;
+  h->bins_ready = false;
+  return DTFE_OK;
+}
+
+int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* boxes, const float* xs,
+                          int64_t n_xs, const float* ys, int64_t n_ys, const float* zs, int64_t n_zs,
+                          const int32_t grid[3]) {
+  if (!h || n_boxes <= 0 || !boxes || !xs || !ys || !zs || !grid)
+    return set_error(DTFE_ERR_ARG, "null or empty sub-box description");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  std::vector<int64_t> tprefix(n_boxes + 1), vprefix(n_boxes + 1), boff(n_boxes);
+  int64_t cells = 0;
+  for (int b = 0; b < n_boxes; ++b) {
+    const dtfe_subbox& B = boxes[b];
+    for (int a = 0; a < 3; ++a) {
+      int64_t nt = a == 0 ? n_xs : (a == 1 ? n_ys : n_zs);
+      if (B.tile_dims[a] <= 0 || B.tile_origin[a] < 0 || B.tile_origin[a] + B.tile_dims[a] > grid[a] ||
+          B.coord_offset[a] < 0 || B.coord_offset[a] + B.tile_dims[a] > nt || !(B.dx[a] > 0.f))
+        return set_error(DTFE_ERR_ARG, "sub-box tile outside the grid or coordinate tables");
+    }
+    if (B.vert_offset < 0 || B.vert_offset + B.n_verts > h->V || B.tet_offset < 0 ||
+        B.tet_offset + B.n_tets > h->T)
+      return set_error(DTFE_ERR_ARG, "sub-box vertex/tetrahedron range outside the upload");
+    if (b > 0 && B.vert_offset != boxes[b - 1].vert_offset + boxes[b - 1].n_verts)
+      return set_error(DTFE_ERR_ARG, "sub-box vertex ranges must be consecutive");
+    tprefix[b] = cells;
+    boff[b] = cells;
+    vprefix[b] = B.vert_offset;
+    cells += (int64_t)B.tile_dims[0] * B.tile_dims[1] * B.tile_dims[2];
+  }
+  tprefix[n_boxes] = cells;
+  vprefix[n_boxes] = boxes[n_boxes - 1].vert_offset + boxes[n_boxes - 1].n_verts;
+  int rc;
+  if ((rc = dev_alloc(&h->boxes, n_boxes)) || (rc = dev_alloc(&h->tile_prefix, n_boxes + 1)) ||
+      (rc = dev_alloc(&h->vprefix, n_boxes + 1)) || (rc = dev_alloc(&h->bin_offset, n_boxes)) ||
+      (rc = dev_alloc(&h->bins, cells)) || (rc = dev_alloc(&h->xs, n_xs)) ||
+      (rc = dev_alloc(&h->ys, n_ys)) || (rc = dev_alloc(&h->zs, n_zs)))
+    return rc;
+  cudaStream_t st = h->stream;
+  DTFE_CUDA_TRY(cudaMemcpyAsync(h->boxes, boxes, sizeof(dtfe_subbox) * n_boxes, cudaMemcpyHostToDevice, st));
+  DTFE_CUDA_TRY(cudaMemcpyAsync(h->tile_prefix, tprefix.data(), sizeof(int64_t) * (n_boxes + 1),
+                                cudaMemcpyHostToDevice, st));
+  DTFE_CUDA_TRY(cudaMemcpyAsync(h->vprefix, vprefix.data(), sizeof(int64_t) * (n_boxes + 1),
+                                cudaMemcpyHostToDevice, st));
+  DTFE_CUDA_TRY(cudaMemcpyAsync(h->bin_offset, boff.data(), sizeof(int64_t) * n_boxes, cudaMemcpyHostToDevice, st));
+  DTFE_CUDA_TRY(cudaMemcpyAsync(h->xs, xs, sizeof(float) * n_xs, cudaMemcpyHostToDevice, st));
+  DTFE_CUDA_TRY(cudaMemcpyAsync(h->ys, ys, sizeof(float) * n_ys, cudaMemcpyHostToDevice, st));
+  DTFE_CUDA_TRY(cudaMemcpyAsync(h->zs, zs, sizeof(float) * n_zs, cudaMemcpyHostToDevice, st));
+  DTFE_CUDA_TRY(cudaStreamSynchronize(st));  // host vectors go out of scope
+  h->K = n_boxes;
+  h->boxes_h.assign(boxes, boxes + n_boxes);
+  h->n_cells = cells;
+  h->grid[0] = grid[0]; h->grid[1] = grid[1]; h->grid[2] = grid[2];
+  h->bins_ready = false;
+  h->eq_nn = 0;
+  return DTFE_OK;
+}
+
+int dtfe_gpu_vertex_density(dtfe_handle h, double rho_bar) {
+  if (!h) return set_error(DTFE_ERR_ARG, "null handle");
+  if (!(rho_bar > 0.0)) return set_error(DTFE_ERR_ARG, "averageDensity must be positive");
+  if (h->V == 0) return set_error(DTFE_ERR_STATE, "nothing uploaded");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  cudaStream_t st = h->stream;
+  DTFE_CUDA_TRY(cudaMemsetAsync(h->volsum, 0, sizeof(double) * h->V, st));
+  DTFE_CUDA_TRY(cudaMemsetAsync(h->hull, 0, sizeof(int) * h->V, st));
+  DTFE_CUDA_TRY(cudaMemsetAsync(h->vtx_tet, 0x7F, sizeof(int) * h->V, st));
+  if (h->T > 0)
+    k_volume_scatter<<<blocks_for(h->T, 256), 256, 0, st>>>(h->T, h->tet_v, h->tet_n, h->posd, h->volsum,
+                                                           h->hull, h->vtx_tet);
+  // the reference's factor: (NO_DIM+1.)/averageDensity stored as Real
+  float rb = (float)rho_bar;
+  float factor = (float)(4.0 / (double)rb);
+  k_vertex_density<<<blocks_for(h->V, 256), 256, 0, st>>>(h->V, h->w, h->volsum, h->hull, factor, h->posd);
+  DTFE_CUDA_TRY(cudaGetLastError());
+  h->density_ready = true;
+  h->bins_ready = false;
+  return DTFE_OK;
+}
+
+int dtfe_gpu_download_vertex_density(dtfe_handle h, float* dens) {
+  if (!h || !dens) return set_error(DTFE_ERR_ARG, "null argument");
+  if (!h->density_ready) return set_error(DTFE_ERR_STATE, "vertex density not computed");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  // .w of each float4: strided copy
+  DTFE_CUDA_TRY(cudaMemcpy2DAsync(dens, sizeof(float), (const char*)h->posd + 12, sizeof(float4),
+                                  sizeof(float), h->V, cudaMemcpyDeviceToHost, h->stream));
+  DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return DTFE_OK;
+}
+
+static int interpolate_impl(dtfe_handle h, const dtfe_interp_opts* o, float* const out_dev[DTFE_NUM_FIELDS],
+                            dtfe_status* status) {
+  if (!h || !o) return set_error(DTFE_ERR_ARG, "null argument");
+  if (h->K == 0) return set_error(DTFE_ERR_STATE, "sub-boxes not set");
+  if (h->T == 0) return set_error(DTFE_ERR_DEGENERATE, "no tetrahedra");
+  int method = o->method;
+  if (method != DTFE_METHOD_CENTRE && method != DTFE_METHOD_MONTE_CARLO && method != DTFE_METHOD_EQUIDISTANT)
+    return set_error(DTFE_ERR_ARG, "unknown method");
+  int NN = method == DTFE_METHOD_CENTRE ? 1 : o->n_samples;
+  if (NN < 1) return set_error(DTFE_ERR_ARG, "n_samples must be >= 1");
+  uint32_t F = o->fields;
+  if (F >> DTFE_NUM_FIELDS) return set_error(DTFE_ERR_ARG, "unknown field bits");
+  if ((F & DTFE_FIELD_BIT(DTFE_VELOCITY_STD)) && method != DTFE_METHOD_MONTE_CARLO)
+    return set_error(DTFE_ERR_ARG, "velocity_std needs the Monte-Carlo method");
+  if (h->S == 0 && (F & (DTFE_FIELD_BIT(DTFE_SCALAR) | DTFE_FIELD_BIT(DTFE_SCALAR_GRADIENT))))
+    return set_error(DTFE_ERR_ARG, "scalar fields requested but n_scalars == 0");
+  for (int s = 0; s < DTFE_NUM_FIELDS; ++s)
+    if ((F >> s & 1u) && !out_dev[s]) return set_error(DTFE_ERR_ARG, "missing output buffer");
+  int rc = prepare_bins(h);
+  if (rc) return rc;
+  cudaStream_t st = h->stream;
+  if (method == DTFE_METHOD_EQUIDISTANT) {
+    int n = (int)std::lround(std::cbrt((double)NN));
+    if (n * n * n != NN) return set_error(DTFE_ERR_ARG, "equidistant sampling needs a perfect cube");
+    if (h->eq_nn != NN) {
+      // equidistant offsets (averaged_interpolation_2.cc:726-740), per sub-box
+      std::vector<float> eq((size_t)h->K * NN * 3);
+      for (int b = 0; b < h->K; ++b) {
+        const float* dx = h->boxes_h[b].dx;
+        for (int i1 = 0; i1 < n; ++i1)
+          for (int i2 = 0; i2 < n; ++i2)
+            for (int i3 = 0; i3 < n; ++i3) {
+              int idx = i1 * n * n + i2 * n + i3;
+              float* e = &eq[((size_t)b * NN + idx) * 3];
+              e[2] = (float)((i3 + 0.5) * (double)dx[2] / n - (double)dx[2] / 2.);
+              e[0] = (float)((i1 + 0.5) * (double)dx[0] / n - (double)dx[0] / 2.);
+              e[1] = (float)((i2 + 0.5) * (double)dx[1] / n - (double)dx[1] / 2.);
+            }
+      }
+      if ((rc = dev_alloc(&h->eq_off, eq.size()))) return rc;
+      DTFE_CUDA_TRY(cudaMemcpyAsync(h->eq_off, eq.data(), sizeof(float) * eq.size(), cudaMemcpyHostToDevice, st));
+      DTFE_CUDA_TRY(cudaStreamSynchronize(st));
+      h->eq_nn = NN;
+    }
+  }
+  DTFE_CUDA_TRY(cudaMemsetAsync(h->counters, 0, sizeof(unsigned long long) * CNT_N, st));
+  InterpParams P;
+  P.tet_v = h->tet_v;
+  P.tet_n = h->tet_n;
+  P.posd = h->posd;
+  P.vel4 = h->vel4;
+  P.scal = h->scal;
+  P.vtx_tet = h->vtx_tet;
+  P.bins = h->bins;
+  P.boxes = h->boxes;
+  P.tile_prefix = h->tile_prefix;
+  P.bin_offset = h->bin_offset;
+  P.eq_off = h->eq_off;
+  P.xs = h->xs;
+  P.ys = h->ys;
+  P.zs = h->zs;
+  P.K = h->K;
+  P.G1 = h->grid[1];
+  P.G2 = h->grid[2];
+  P.n_total = h->n_cells;
+  P.NN = NN;
+  P.seed = o->seed;
+  P.fields = F;
+  P.fix = (o->flags & DTFE_FLAG_FIX_VALUE_INTERP) ? 1 : 0;
+  P.max_steps = h->max_steps;
+  for (int s = 0; s < DTFE_NUM_FIELDS; ++s) P.out[s] = (F >> s & 1u) ? out_dev[s] : nullptr;
+  P.counters = h->counters;
+  const unsigned block = 256;
+  unsigned grid = blocks_for(h->n_cells, block);
+  if (method == DTFE_METHOD_CENTRE) launch_interp_s<DTFE_METHOD_CENTRE>(P, h->S, st, grid, block);
+  else if (method == DTFE_METHOD_MONTE_CARLO) launch_interp_s<DTFE_METHOD_MONTE_CARLO>(P, h->S, st, grid, block);
+  else launch_interp_s<DTFE_METHOD_EQUIDISTANT>(P, h->S, st, grid, block);
+  DTFE_CUDA_TRY(cudaGetLastError());
+  unsigned long long cnt[CNT_N];
+  DTFE_CUDA_TRY(cudaMemcpyAsync(cnt, h->counters, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+  DTFE_CUDA_TRY(cudaStreamSynchronize(st));
+  if (status) {
+    status->n_samples_located = (int64_t)cnt[CNT_LOCATED];
+    status->n_outside = (int64_t)cnt[CNT_OUTSIDE];
+    status->n_walk_failures = (int64_t)cnt[CNT_FAIL];
+    status->n_walk_steps = (int64_t)cnt[CNT_STEPS];
+    status->n_exact_tests = (int64_t)cnt[CNT_EXACT];
+    status->n_ties = (int64_t)cnt[CNT_TIES];
+  }
+  if (cnt[CNT_FAIL]) return set_error(DTFE_ERR_WALK, "point-location walk hit its step limit");
+  return DTFE_OK;
+}
+
+int dtfe_gpu_interpolate_dev(dtfe_handle h, const dtfe_interp_opts* opts,
+                             float* const out_dev[DTFE_NUM_FIELDS], dtfe_status* st) {
+  if (!h) return set_error(DTFE_ERR_ARG, "null handle");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  return interpolate_impl(h, opts, out_dev, st);
+}
+
+int dtfe_gpu_interpolate(dtfe_handle h, const dtfe_interp_opts* opts, float* const out[DTFE_NUM_FIELDS],
+                         dtfe_status* st) {
+  if (!h || !opts || !out) return set_error(DTFE_ERR_ARG, "null argument");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  int64_t G = (int64_t)h->grid[0] * h->grid[1] * h->grid[2];
+  float* dev[DTFE_NUM_FIELDS] = {};
+  for (int s = 0; s < DTFE_NUM_FIELDS; ++s) {
+    if (!(opts->fields >> s & 1u)) continue;
+    if (!out[s]) return set_error(DTFE_ERR_ARG, "missing output buffer");
+    size_t need = (size_t)G * field_components(s, h->S);
+    if (h->out_cap[s] < need) {
+      int rc = dev_alloc(&h->out_buf[s], need);
+      if (rc) return rc;
+      h->out_cap[s] = need;
+    }
+    dev[s] = h->out_buf[s];
+    // cells outside every tile keep zeros, as the reference's reserved vectors
+    DTFE_CUDA_TRY(cudaMemsetAsync(dev[s], 0, need * sizeof(float), h->stream));
+  }
+  int rc = interpolate_impl(h, opts, dev, st);
+  if (rc) return rc;
+  for (int s = 0; s < DTFE_NUM_FIELDS; ++s) {
+    if (!dev[s]) continue;
+    size_t need = (size_t)G * field_components(s, h->S);
+    DTFE_CUDA_TRY(cudaMemcpyAsync(out[s], dev[s], need * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  }
+  DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return DTFE_OK;
+}
+
+// Canonical location of np points (host doubles) starting from tetrahedron
+// `start`; out receives tetrahedron ids, -1 (outside the hull) or -2 (walk
+// failure).  Test and diagnostic entry point.
+int dtfe_gpu_locate_points(dtfe_handle h, int64_t np, const double* pts, int32_t start, int32_t* out) {
+  if (!h || (np > 0 && (!pts || !out))) return set_error(DTFE_ERR_ARG, "null argument");
+  if (h->T == 0) return set_error(DTFE_ERR_DEGENERATE, "no tetrahedra");
+  if (start < 0 || start >= h->T) return set_error(DTFE_ERR_ARG, "start tetrahedron out of range");
+  if (np == 0) return DTFE_OK;
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  cudaStream_t st = h->stream;
+  double* dp = nullptr;
+  int* dout = nullptr;
+  DTFE_CUDA_TRY(cudaMallocAsync((void**)&dp, sizeof(double) * 3 * np, st));
+  DTFE_CUDA_TRY(cudaMallocAsync((void**)&dout, sizeof(int) * np, st));
+  DTFE_CUDA_TRY(cudaMemcpyAsync(dp, pts, sizeof(double) * 3 * np, cudaMemcpyHostToDevice, st));
+  k_locate_points<<<blocks_for(np, 128), 128, 0, st>>>(np, dp, h->tet_v, h->tet_n, h->posd, start,
+                                                       h->max_steps, dout);
+  DTFE_CUDA_TRY(cudaGetLastError());
+  DTFE_CUDA_TRY(cudaMemcpyAsync(out, dout, sizeof(int) * np, cudaMemcpyDeviceToHost, st));
+  DTFE_CUDA_TRY(cudaFreeAsync(dp, st));
+  DTFE_CUDA_TRY(cudaFreeAsync(dout, st));
+  DTFE_CUDA_TRY(cudaStreamSynchronize(st));
+  return DTFE_OK;
+}
+
+}  // extern "C"

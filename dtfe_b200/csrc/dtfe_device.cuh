@@ -1,0 +1,365 @@
+// Device building blocks of the DTFE interpolation path (sm_100a).
+//
+//  * walk_locate: hinted visibility walk over the flat tetrahedron arrays with
+//    filtered FP64 orientation tests and an exact fallback — the device
+//    counterpart of CGAL's dt.locate(p, lt, li, lj, hint)
+//    (unaveraged_interpolation.cc:289, averaged_interpolation_2.cc:123,145);
+//  * canonical_tie: the documented tie rule (lowest tetrahedron id among the
+//    tetrahedra whose closure holds p), so the located tetrahedron does not
+//    depend on the walk path;
+//  * cell_eval: the per-sample field arithmetic of positionMatrix,
+//    matrixInverse, densityGrad/Value, velocityGrad/Value, velocityGradient,
+//    scalarGrad/Value/Gradient (unaveraged_interpolation.cc:34-173,
+//    triangulation_miscellaneous.cc:25,42-96) in the reference's precision
+//    pattern: double edge matrix and inverse, rounded to float; float
+//    gradients; double products of the float offset.  The translation unit is
+//    compiled with -fmad=false so no product is fused into an FMA.
+#pragma once
+
+#include <cstdint>
+#include "predicates.h"
+
+namespace dtfe {
+
+constexpr int kOutside = -1;
+constexpr int kWalkFail = -2;
+
+struct WalkStats {
+  int steps;
+  int exact;
+  int tie;
+};
+
+__device__ __forceinline__ void load_pos(const float4* __restrict__ posd, int v, double X[3]) {
+  float4 q = __ldg(&posd[v]);
+  X[0] = (double)q.x;
+  X[1] = (double)q.y;
+  X[2] = (double)q.z;
+}
+
+// Signs of the four face orientations of tetrahedron with vertices X[0..3]
+// for point p (o_i = orient with vertex i replaced by p), evaluating only the
+// faces in `need` (bit mask).  Returns the mask of evaluated faces.
+__device__ __forceinline__ void face_signs(const double X[4][3], const double p[3], int need,
+                                          int sgn[4], int& nexact) {
+  double d[4][3];
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) d[k][c] = X[k][c] - p[c];
+  if (need & 3) {
+    // c23 = d2 x d3
+    double m0 = d[2][1] * d[3][2], m1 = d[2][2] * d[3][1];
+    double m2 = d[2][2] * d[3][0], m3 = d[2][0] * d[3][2];
+    double m4 = d[2][0] * d[3][1], m5 = d[2][1] * d[3][0];
+    double cx = m0 - m1, cy = m2 - m3, cz = m4 - m5;
+    double ax = fabs(m0) + fabs(m1), ay = fabs(m2) + fabs(m3), az = fabs(m4) + fabs(m5);
+    if (need & 1) {
+      double det = d[1][0] * cx + d[1][1] * cy + d[1][2] * cz;
+      double perm = fabs(d[1][0]) * ax + fabs(d[1][1]) * ay + fabs(d[1][2]) * az;
+      double b = kOrientErr * perm;
+      if (det > b) sgn[0] = 1;
+      else if (-det > b) sgn[0] = -1;
+      else { sgn[0] = orient_exact(p, X[1], X[2], X[3]); ++nexact; }
+    }
+    if (need & 2) {
+      double det = -(d[0][0] * cx + d[0][1] * cy + d[0][2] * cz);
+      double perm = fabs(d[0][0]) * ax + fabs(d[0][1]) * ay + fabs(d[0][2]) * az;
+      double b = kOrientErr * perm;
+      if (det > b) sgn[1] = 1;
+      else if (-det > b) sgn[1] = -1;
+      else { sgn[1] = orient_exact(X[0], p, X[2], X[3]); ++nexact; }
+    }
+  }
+  if (need & 12) {
+    // c01 = d0 x d1
+    double m0 = d[0][1] * d[1][2], m1 = d[0][2] * d[1][1];
+    double m2 = d[0][2] * d[1][0], m3 = d[0][0] * d[1][2];
+    double m4 = d[0][0] * d[1][1], m5 = d[0][1] * d[1][0];
+    double cx = m0 - m1, cy = m2 - m3, cz = m4 - m5;
+    double ax = fabs(m0) + fabs(m1), ay = fabs(m2) + fabs(m3), az = fabs(m4) + fabs(m5);
+    if (need & 4) {
+      double det = d[3][0] * cx + d[3][1] * cy + d[3][2] * cz;
+      double perm = fabs(d[3][0]) * ax + fabs(d[3][1]) * ay + fabs(d[3][2]) * az;
+      double b = kOrientErr * perm;
+      if (det > b) sgn[2] = 1;
+      else if (-det > b) sgn[2] = -1;
+      else { sgn[2] = orient_exact(X[0], X[1], p, X[3]); ++nexact; }
+    }
+    if (need & 8) {
+      double det = -(d[2][0] * cx + d[2][1] * cy + d[2][2] * cz);
+      double perm = fabs(d[2][0]) * ax + fabs(d[2][1]) * ay + fabs(d[2][2]) * az;
+      double b = kOrientErr * perm;
+      if (det > b) sgn[3] = 1;
+      else if (-det > b) sgn[3] = -1;
+      else { sgn[3] = orient_exact(X[0], X[1], X[2], p); ++nexact; }
+    }
+  }
+}
+
+__device__ __forceinline__ void load_tet(const int4* __restrict__ tet_v, const float4* __restrict__ posd,
+                                        int t, int v[4], double X[4][3]) {
+  int4 q = __ldg(&tet_v[t]);
+  v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) load_pos(posd, v[a], X[a]);
+}
+
+__device__ __forceinline__ int nb_of(const int4& n, int i) {
+  return i == 0 ? n.x : (i == 1 ? n.y : (i == 2 ? n.z : n.w));
+}
+
+// True if the closure of tetrahedron t holds p; zero[] marks faces through p.
+__device__ __noinline__ bool tet_contains(const int4* __restrict__ tet_v, const float4* __restrict__ posd,
+                                          int t, const double p[3], int& zmask, int& nexact) {
+  int v[4];
+  double X[4][3];
+  load_tet(tet_v, posd, t, v, X);
+  int s[4];
+  face_signs(X, p, 15, s, nexact);
+  zmask = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    if (s[i] < 0) return false;
+    if (s[i] == 0) zmask |= 1 << i;
+  }
+  return true;
+}
+
+// Canonical tie rule: the lowest id among the tetrahedra whose closure holds
+// p, found by exploring across faces that pass through p.  Bounded: gives up
+// (keeps the best so far, sets overflow) after kTieMax tetrahedra.
+constexpr int kTieMax = 96;
+__device__ __noinline__ int canonical_tie(const int4* __restrict__ tet_v, const int4* __restrict__ tet_n,
+                                          const float4* __restrict__ posd, int t, int zmask,
+                                          const double p[3], int& nexact) {
+  int seen[kTieMax];
+  int nseen = 1, head = 0;
+  seen[0] = t;
+  int best = t;
+  // seen[] doubles as the BFS queue (entries before head are expanded)
+  int zm = zmask;
+  while (head < nseen) {
+    int u = seen[head];
+    if (head > 0) {
+      int dummy;
+      tet_contains(tet_v, posd, u, p, zm, dummy);
+    }
+    ++head;
+    int4 n = __ldg(&tet_n[u]);
+    for (int i = 0; i < 4; ++i) {
+      if (!(zm & (1 << i))) continue;
+      int nb = nb_of(n, i);
+      if (nb < 0) continue;
+      bool dup = false;
+      for (int q = 0; q < nseen; ++q)
+        if (seen[q] == nb) { dup = true; break; }
+      if (dup) continue;
+      int zn;
+      if (!tet_contains(tet_v, posd, nb, p, zn, nexact)) continue;
+      if (nseen >= kTieMax) return best;
+      seen[nseen++] = nb;
+      if (nb < best) best = nb;
+    }
+  }
+  return best;
+}
+
+// Visibility walk from tetrahedron t toward p.  Returns the canonical
+// containing tetrahedron, kOutside, or kWalkFail.  On success v/X hold the
+// vertices and positions of the returned tetrahedron.
+__device__ __forceinline__ int walk_locate(const int4* __restrict__ tet_v, const int4* __restrict__ tet_n,
+                                           const float4* __restrict__ posd, const double p[3], int t,
+                                           int max_steps, int v[4], double X[4][3], WalkStats& st) {
+  int came = -1;
+  int fv0 = -1, fv1 = -1, fv2 = -1;
+  for (int step = 0; step < max_steps; ++step) {
+    ++st.steps;
+    load_tet(tet_v, posd, t, v, X);
+    if (fv0 >= 0) {
+      came = -1;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (v[j] != fv0 && v[j] != fv1 && v[j] != fv2) came = j;
+    }
+    int need = 15 & ~(came >= 0 ? (1 << came) : 0);
+    int s[4] = {1, 1, 1, 1};
+    face_signs(X, p, need, s, st.exact);
+    int exit_face = -1;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      if (exit_face < 0 && (need & (1 << i)) && s[i] < 0) exit_face = i;
+    if (exit_face < 0) {
+      int zmask = 0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if ((need & (1 << i)) && s[i] == 0) zmask |= 1 << i;
+      if (zmask) {
+        ++st.tie;
+        int b = canonical_tie(tet_v, tet_n, posd, t, zmask, p, st.exact);
+        if (b != t) {
+          t = b;
+          load_tet(tet_v, posd, t, v, X);
+        }
+      }
+      return t;
+    }
+    int4 n = __ldg(&tet_n[t]);
+    int nb = nb_of(n, exit_face);
+    if (nb < 0) return kOutside;
+    // remember the face we cross to skip it in the next tetrahedron
+    int k = 0;
+    int f[3];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (j != exit_face) f[k++] = v[j];
+    fv0 = f[0]; fv1 = f[1]; fv2 = f[2];
+    t = nb;
+  }
+  return kWalkFail;
+}
+
+// ---- per-sample arithmetic (reference precision pattern) -----------------
+
+// minorDeterminant + matrixInverse (triangulation_miscellaneous.cc:42-96).
+__device__ __forceinline__ void matrix_inverse_f(const double A[3][3], float M[3][3]) {
+#define DTFE_MINOR(row, col)                                                        \
+  (A[((col) + 1) % 3][((row) + 1) % 3] * A[((col) + 2) % 3][((row) + 2) % 3] -      \
+   A[((col) + 1) % 3][((row) + 2) % 3] * A[((col) + 2) % 3][((row) + 1) % 3])
+  double det = A[0][0] * DTFE_MINOR(0, 0) + A[0][1] * DTFE_MINOR(1, 0) + A[0][2] * DTFE_MINOR(2, 0);
+  double s = fabs(A[0][0]) + fabs(A[0][1]) + fabs(A[0][2]) + fabs(A[1][0]) + fabs(A[1][1]) +
+             fabs(A[1][2]) + fabs(A[2][0]) + fabs(A[2][1]) + fabs(A[2][2]);
+  bool ok = fabs(det / s) > 1.e-6;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) M[r][c] = ok ? (float)(DTFE_MINOR(r, c) / det) : 0.f;
+#undef DTFE_MINOR
+}
+
+struct CellOut {
+  float dens;
+  float vel[3];
+  float grad[9];
+  float sc[8];
+  float scg[24];
+};
+
+// Evaluates the requested fields of the located tetrahedron at p.
+template <int S>
+__device__ __forceinline__ void cell_eval(const int v[4], const double X[4][3], const double p[3],
+                                          const float4* __restrict__ posd,
+                                          const float4* __restrict__ vel4,
+                                          const float* __restrict__ scal, bool want_dens,
+                                          bool want_vel, bool want_sc, bool fix, CellOut& e) {
+  double A[3][3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) A[r][c] = X[r + 1][c] - X[0][c];
+  float M[3][3];
+  matrix_inverse_f(A, M);
+  float rel[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) rel[c] = (float)(p[c] - X[0][c]);
+  if (want_dens) {
+    float d0 = __ldg(&posd[v[0]]).w;
+    float dd[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) dd[i] = __ldg(&posd[v[i + 1]]).w - d0;
+    float gr[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      float acc = 0.f;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) acc += M[i][j] * dd[j];
+      gr[i] = acc;
+    }
+    double s = (double)rel[0] * gr[0] + (double)rel[1] * gr[1] + (double)rel[2] * gr[2];
+    e.dens = d0 + (float)s;
+  }
+  if (want_vel) {
+    float4 w0 = __ldg(&vel4[v[0]]);
+    float v0[3] = {w0.x, w0.y, w0.z};
+    float dv[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      float4 wk = __ldg(&vel4[v[k + 1]]);
+      dv[k][0] = wk.x - v0[0];
+      dv[k][1] = wk.y - v0[1];
+      dv[k][2] = wk.z - v0[2];
+    }
+    float VG[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        float acc = 0.f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) acc += M[i][k] * dv[k][j];
+        VG[i][j] = acc;
+      }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      float tmp = 0.f;
+      if (fix) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) tmp = (float)((double)tmp + (double)VG[j][i] * (double)rel[j]);
+      } else {
+        tmp = (float)((double)VG[2][i] * (double)rel[2]);
+      }
+      e.vel[i] = tmp + v0[i];
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) e.grad[j * 3 + i] = VG[i][j];
+  }
+  if (S > 0 && want_sc) {
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+      float s0 = __ldg(&scal[(int64_t)S * v[0] + q]);
+      float ds[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) ds[k] = __ldg(&scal[(int64_t)S * v[k + 1] + q]) - s0;
+      float SG[3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        float acc = 0.f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) acc += M[i][k] * ds[k];
+        SG[i] = acc;
+      }
+      float tmp = 0.f;
+      if (fix) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) tmp = (float)((double)tmp + (double)SG[j] * (double)rel[j]);
+      } else {
+        tmp = (float)((double)SG[2] * (double)rel[2]);
+      }
+      e.sc[q] = tmp + s0;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) e.scg[q * 3 + i] = SG[i];
+    }
+  }
+}
+
+// velocityDivergence / velocityShear / velocityVorticity (src/DTFE.cpp:394-433)
+__device__ __forceinline__ void derived_fields(const float g[9], float& div, float sh[5], float vo[3]) {
+  div = g[0] + g[4] + g[8];
+  int idx = 0;
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = i; j < 3; ++j) sh[idx++] = (float)((double)(g[i * 3 + j] + g[j * 3 + i]) / 2.);
+  float trace = (float)((double)(sh[0] + sh[3] + g[8]) / 3.);
+  sh[0] -= trace;
+  sh[3] -= trace;
+  idx = 0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = i + 1; j < 3; ++j) vo[idx++] = (float)((double)(g[i * 3 + j] - g[j * 3 + i]) / 2.);
+}
+
+}  // namespace dtfe

@@ -1,0 +1,319 @@
+// Host-side planning of a DTFE run: the control flow DTFE() executes before
+// the tessellation is built.  Each function restates one reference routine
+// with the same float arithmetic, so sub-box regions, padded particle sets and
+// sample coordinates come out bit-identical.
+//
+//   dtfe_padding_length     User_options::updatePadding   src/user_options.cc:1062-1089
+//   dtfe_average_density    averageDensity                src/subpartition.h:437-449
+//                           (Box::volume() is hard-coded to 35000^3, src/box.h:142-149)
+//   dtfe_select_in_box      findParticlesInBox / insertParticlesInBox
+//                                                         src/subpartition.h:79-154
+//   dtfe_parallel_grid      parallelGrid                  src/subpartition.h:454-555
+//   dtfe_optimal_partition  optimalPartitionSplit + optimalSplit + NGP_particle_count
+//                           src/subpartition.h:163-372, src/NGP_interpolation.cc:140-174
+//   dtfe_axis_coords        the x += dx sample raster     unaveraged_interpolation.cc:252-358
+
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+extern "C" {
+
+// Padding length on each of the 6 box sides (xmin, xmax, ymin, ...).
+// kind: 0 = DTFE or SPH, 1 = TSC or NGP, 2 = CIC.  The reference indexes the
+// box lengths with i%2 rather than i/2 (so side 4 uses the x length); that is
+// kept.  A non-null user padding (already in box units) is returned as is.
+void dtfe_padding_length(int kind, float padding_particles, int64_t n_total,
+                         const float full_box_length[3], const int64_t grid[3], float out[6]) {
+  if (padding_particles <= 0.f) {
+    for (int i = 0; i < 6; ++i) out[i] = 0.f;
+    return;
+  }
+  for (int i = 0; i < 6; ++i) {
+    if (kind == 0)
+      out[i] = padding_particles / (float)(std::pow((double)n_total, 1. / 3)) * full_box_length[i % 2];
+    else if (kind == 1)
+      out[i] = full_box_length[i % 2] / (float)grid[i % 2];
+    else
+      out[i] = 0.f;
+  }
+}
+
+// Sum of weights (double) over the hard-coded box volume, as a float.
+float dtfe_average_density(const float* w, int64_t n) {
+  double total = 0.;
+  for (int64_t i = 0; i < n; ++i) total += w ? (double)w[i] : 1.0;
+  float vol = 1.f;
+  for (int i = 0; i < 3; ++i) vol *= 35000;
+  return (float)(total / vol);
+}
+
+static inline bool in_box(const float* p, const float* b) {
+  return p[0] >= b[0] && p[0] <= b[1] && p[1] >= b[2] && p[1] <= b[3] && p[2] >= b[4] && p[2] <= b[5];
+}
+
+// Particles inside the padded box.  Non-periodic: particles with
+// padded[lo] <= pos <= padded[hi].  Periodic: for each of the 27 box
+// translations (order i1,i2,i3 over {-1,0,1} times the full box length) the
+// translated padded box selects particles, which are emitted shifted back by
+// the translation — the reference's order and float arithmetic.  Returns the
+// number selected; idx/pos_out (may be NULL for a count) receive the source
+// index and the (shifted) position of each.
+int64_t dtfe_select_in_box(const float* pos, int64_t n, const float full_box[6], const float padded[6],
+                           int periodic, int32_t* idx_out, float* pos_out) {
+  struct Off { float o[3]; float box[6]; };
+  std::vector<Off> offs;
+  if (!periodic) {
+    Off o{{0.f, 0.f, 0.f}, {padded[0], padded[1], padded[2], padded[3], padded[4], padded[5]}};
+    offs.push_back(o);
+  } else {
+    float len[3];
+    for (int i = 0; i < 3; ++i) len[i] = full_box[2 * i + 1] - full_box[2 * i];
+    for (int i1 = 0; i1 < 3; ++i1)
+      for (int i2 = 0; i2 < 3; ++i2)
+        for (int i3 = 0; i3 < 3; ++i3) {
+          Off o;
+          o.o[0] = (float)(i1 - 1) * len[0];
+          o.o[1] = (float)(i2 - 1) * len[1];
+          o.o[2] = (float)(i3 - 1) * len[2];
+          for (int k = 0; k < 3; ++k) {
+            o.box[2 * k] = padded[2 * k] + o.o[k];
+            o.box[2 * k + 1] = padded[2 * k + 1] + o.o[k];
+          }
+          offs.push_back(o);
+        }
+  }
+  // parallel two-pass selection preserving the serial order
+  const int64_t chunk = 1 << 16;
+  const int64_t nchunks = (n + chunk - 1) / chunk;
+  const int64_t nblk = (int64_t)offs.size() * nchunks;
+  std::vector<int64_t> count(nblk + 1, 0);
+#pragma omp parallel for schedule(static)
+  for (int64_t b = 0; b < nblk; ++b) {
+    const Off& o = offs[b / nchunks];
+    int64_t lo = (b % nchunks) * chunk, hi = std::min<int64_t>(n, lo + chunk);
+    int64_t c = 0;
+    for (int64_t i = lo; i < hi; ++i) c += in_box(&pos[3 * i], o.box);
+    count[b + 1] = c;
+  }
+  for (int64_t b = 0; b < nblk; ++b) count[b + 1] += count[b];
+  if (idx_out || pos_out) {
+#pragma omp parallel for schedule(static)
+    for (int64_t b = 0; b < nblk; ++b) {
+      const Off& o = offs[b / nchunks];
+      int64_t lo = (b % nchunks) * chunk, hi = std::min<int64_t>(n, lo + chunk);
+      int64_t k = count[b];
+      for (int64_t i = lo; i < hi; ++i) {
+        const float* p = &pos[3 * i];
+        if (!in_box(p, o.box)) continue;
+        if (idx_out) idx_out[k] = (int32_t)i;
+        if (pos_out) {
+          pos_out[3 * k] = p[0] - o.o[0];
+          pos_out[3 * k + 1] = p[1] - o.o[1];
+          pos_out[3 * k + 2] = p[2] - o.o[2];
+        }
+        ++k;
+      }
+    }
+  }
+  return count[nblk];
+}
+
+// parallelGrid: a 2^a 3^b processor grid close to n_threads, balanced over
+// the axes and no finer than the main grid.
+void dtfe_parallel_grid(int64_t n_threads, const int64_t main_grid[3], int64_t grid[3]) {
+  const int D = 3;
+  int64_t n = n_threads;
+  int x2 = 0, x3 = 0;
+  while (n / 2 != 0) { n /= 2; ++x2; }
+  n = n_threads;
+  while (n / 3 != 0) { n /= 3; ++x3; }
+  n = n_threads;
+  int64_t diff = n;
+  int j2 = 0, j3 = 0;
+  int64_t napprox = 1;
+  for (int i2 = 0; i2 <= x2; ++i2) {
+    int64_t temp = napprox;
+    for (int i3 = 0; i3 <= x3; ++i3) {
+      // (n-temp) is unsigned in the reference: only temp <= n qualifies
+      if (temp <= n && (n - temp) < diff) {
+        diff = n - temp;
+        j2 = i2;
+        j3 = i3;
+      }
+      temp *= 3;
+    }
+    napprox *= 2;
+  }
+  x2 = j2;
+  x3 = j3;
+  for (int i = 0; i < D; ++i) grid[i] = 1;
+  while (x3 - D >= 0) {
+    for (int i = 0; i < D; ++i) grid[i] *= 3;
+    x3 -= D;
+  }
+  for (int i = D - 1; i >= (D - x3); --i) grid[i] *= 3;
+  int i1 = x2 > (D - x3) ? (D - x3) : x2;
+  for (int i = 0; i < i1; ++i) grid[i % (D - x3)] *= 2;
+  for (int i = 0; i < x2 - i1; ++i) grid[i % D] *= 2;
+  for (int i = 0; i < D; ++i) {
+    if (main_grid[i] >= grid[i]) continue;
+    int next1 = (i + 1) % D, next2 = (i + 2) % D;
+    while (grid[i] > main_grid[i] && grid[i] % 3 == 0) {
+      grid[i] /= 3;
+      if (3 * grid[next1] <= main_grid[next1]) grid[next1] *= 3;
+      else if (3 * grid[next2] <= main_grid[next2]) grid[next2] *= 3;
+    }
+    while (grid[i] > main_grid[i] && grid[i] % 2 == 0) {
+      grid[i] /= 2;
+      if (2 * grid[next1] <= main_grid[next1]) grid[next1] *= 2;
+      else if (2 * grid[next2] <= main_grid[next2]) grid[next2] *= 2;
+    }
+  }
+}
+
+// optimalSplit: indices splitting `counts` into `parts` runs of similar sums.
+static void optimal_split(const std::vector<size_t>& counts, size_t parts, size_t* idx) {
+  if (parts <= 1 || counts.size() == 1) return;
+  size_t total = 0;
+  for (size_t c : counts) total += c;
+  size_t load = total / parts;
+  size_t remaining = total, temp = 0, pic = 1;
+  idx[0] = 0;
+  idx[parts] = counts.size();
+  for (size_t i = 0; i < counts.size(); ++i) {
+    temp += counts[i];
+    if (temp >= load) {
+      size_t t1 = ((remaining + counts[i]) - temp) / (parts - pic);
+      size_t t2 = (remaining - temp) / (parts - pic);
+      if (i == 0) {
+      } else if (i == counts.size() - 1) {
+        temp -= counts[i];
+        --i;
+      } else if (pic > 1 && (i - idx[pic - 1]) == 1) {
+      } else if (std::abs((int)temp - (int)t1) < std::abs((int)temp - (int)t2)) {
+        temp -= counts[i];
+        --i;
+      }
+      idx[pic] = i;
+      remaining -= temp;
+      load = remaining / (parts - pic);
+      temp = 0;
+      ++pic;
+      if (pic == parts) break;
+    }
+  }
+}
+
+// optimalPartitionSplit over the main grid of `region` (6 floats): splits
+// along x, then y inside each x slab, then z, balancing NGP particle counts.
+// subgrid (6 per partition): [x0,x1,y0,y1,z0,z1) cell ranges; coords (6 per
+// partition): region bounds region[lo] + dx * index (float).  Partition p has
+// index (px*part[1] + py)*part[2] + pz.  Returns 0, or 1 when a partition
+// count exceeds the grid.
+int dtfe_optimal_partition(const float* pos, int64_t n, const int64_t grid_in[3], const float region[6],
+                           const int64_t part_in[3], int64_t* subgrid, float* coords) {
+  const size_t grid[3] = {(size_t)grid_in[0], (size_t)grid_in[1], (size_t)grid_in[2]};
+  const size_t part[3] = {(size_t)part_in[0], (size_t)part_in[1], (size_t)part_in[2]};
+  for (int i = 0; i < 3; ++i)
+    if (part[i] == 0 || part[i] > grid[i]) return 1;
+  float dx[3];
+  for (int i = 0; i < 3; ++i) dx[i] = (region[2 * i + 1] - region[2 * i]) / grid[i];
+  // NGP_particle_count
+  std::vector<int> counts(grid[0] * grid[1] * grid[2], 0);
+  for (int64_t p = 0; p < n; ++p) {
+    int cell[3];
+    bool ok = true;
+    for (int j = 0; j < 3; ++j) {
+      cell[j] = (int)std::floor((pos[3 * p + j] - region[2 * j]) / dx[j]);
+      if (cell[j] < 0 || (size_t)cell[j] >= grid[j]) ok = false;
+    }
+    if (!ok) continue;
+    counts[cell[0] * grid[1] * grid[2] + cell[1] * grid[2] + cell[2]] += 1;
+  }
+  const size_t np = part[0] * part[1] * part[2];
+  std::vector<size_t> xs(part[0] + 1, 0), ys(part[1] + 1, 0), zs(part[2] + 1, 0);
+  if (part[0] > 1) {
+    std::vector<size_t> tc(grid[0], 0);
+    for (size_t i1 = 0; i1 < grid[0]; ++i1)
+      for (size_t i2 = 0; i2 < grid[1]; ++i2)
+        for (size_t i3 = 0; i3 < grid[2]; ++i3) tc[i1] += counts[i1 * grid[1] * grid[2] + i2 * grid[2] + i3];
+    optimal_split(tc, part[0], xs.data());
+  } else {
+    xs[0] = 0;
+    xs[1] = grid[0];
+  }
+  for (size_t i1 = 0; i1 < part[0]; ++i1)
+    for (size_t i2 = 0; i2 < part[1]; ++i2)
+      for (size_t i3 = 0; i3 < part[2]; ++i3) {
+        size_t p = i1 * part[1] * part[2] + i2 * part[2] + i3;
+        subgrid[6 * p + 0] = (int64_t)xs[i1];
+        subgrid[6 * p + 1] = (int64_t)xs[i1 + 1];
+        coords[6 * p + 0] = region[0] + dx[0] * xs[i1];
+        coords[6 * p + 1] = region[0] + dx[0] * xs[i1 + 1];
+      }
+  for (size_t i = 0; i < part[0]; ++i) {
+    if (part[1] > 1) {
+      std::vector<size_t> tc(grid[1], 0);
+      for (size_t i1 = xs[i]; i1 < xs[i + 1]; ++i1)
+        for (size_t i2 = 0; i2 < grid[1]; ++i2)
+          for (size_t i3 = 0; i3 < grid[2]; ++i3) tc[i2] += counts[i1 * grid[1] * grid[2] + i2 * grid[2] + i3];
+      optimal_split(tc, part[1], ys.data());
+    } else {
+      ys[0] = 0;
+      ys[1] = grid[1];
+    }
+    for (size_t i2 = 0; i2 < part[1]; ++i2)
+      for (size_t i3 = 0; i3 < part[2]; ++i3) {
+        size_t p = i * part[1] * part[2] + i2 * part[2] + i3;
+        subgrid[6 * p + 2] = (int64_t)ys[i2];
+        subgrid[6 * p + 3] = (int64_t)ys[i2 + 1];
+        coords[6 * p + 2] = region[2] + dx[1] * ys[i2];
+        coords[6 * p + 3] = region[2] + dx[1] * ys[i2 + 1];
+      }
+  }
+  for (size_t i = 0; i < part[0]; ++i)
+    for (size_t j = 0; j < part[1]; ++j) {
+      // The z balance counts particles over the y range ys[j..j+1] left by the
+      // y loop, i.e. the split of the LAST x slab, for every slab (the
+      // reference reuses ySplitIndices, src/subpartition.h:334-339).
+      size_t y0 = ys[j], y1 = ys[j + 1];
+      if (part[2] > 1) {
+        std::vector<size_t> tc(grid[2], 0);
+        for (size_t i1 = xs[i]; i1 < xs[i + 1]; ++i1)
+          for (size_t i2 = y0; i2 < y1; ++i2)
+            for (size_t i3 = 0; i3 < grid[2]; ++i3) tc[i3] += counts[i1 * grid[1] * grid[2] + i2 * grid[2] + i3];
+        optimal_split(tc, part[2], zs.data());
+      } else {
+        zs[0] = 0;
+        zs[1] = grid[2];
+      }
+      for (size_t i3 = 0; i3 < part[2]; ++i3) {
+        size_t p = i * part[1] * part[2] + j * part[2] + i3;
+        subgrid[6 * p + 4] = (int64_t)zs[i3];
+        subgrid[6 * p + 5] = (int64_t)zs[i3 + 1];
+        coords[6 * p + 4] = region[4] + dx[2] * zs[i3];
+        coords[6 * p + 5] = region[4] + dx[2] * zs[i3 + 1];
+      }
+    }
+  (void)np;
+  return 0;
+}
+
+// Sample coordinates along one axis: x = lo + dx/2 (double, rounded to
+// float), then x += dx in float.
+void dtfe_axis_coords(float lo, float dx, int64_t n, float* out) {
+  float x = (float)((double)lo + (double)dx / 2.);
+  for (int64_t i = 0; i < n; ++i) {
+    out[i] = x;
+    x += dx;
+  }
+}
+
+}  // extern "C"

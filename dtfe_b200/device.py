@@ -1,0 +1,117 @@
+"""Python handle over the C ABI of include/dtfe_gpu.h (libdtfe_gpu.so)."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+
+
+def _mask(fields) -> int:
+    m = 0
+    for f in fields:
+        m |= 1 << N.FIELD_SLOTS[f]
+    return m
+
+
+class DeviceDTFE:
+    """One device handle: uploaded multi-tessellation, sub-boxes, vertex data."""
+
+    def __init__(self, device: int = 0, n_scalars: int = 0, max_walk_steps: int = 0):
+        self.lib = N.gpu()
+        self.h = C.c_void_p()
+        cfg = N.Config(device, n_scalars, max_walk_steps, 0)
+        N.check(self.lib.dtfe_gpu_create(C.byref(cfg), C.byref(self.h)))
+        self.n_scalars = n_scalars
+        self.grid = None
+        self.last_status = None
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.dtfe_gpu_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.dtfe_gpu_stream(self.h) or 0)
+
+    def synchronize(self) -> None:
+        N.check(self.lib.dtfe_gpu_synchronize(self.h))
+
+    def upload(self, plan) -> None:
+        N.check(self.lib.dtfe_gpu_upload(
+            self.h, N.ptr(plan.tet_v), N.ptr(plan.tet_n), plan.n_tets, N.ptr(plan.xyz),
+            N.ptr(plan.weight), N.ptr(plan.velocity), N.ptr(plan.scalar), plan.n_verts))
+
+    def set_subboxes(self, plan) -> None:
+        grid = np.asarray(plan.grid, np.int32)
+        N.check(self.lib.dtfe_gpu_set_subboxes(
+            self.h, plan.n_boxes, C.addressof(plan.boxes), N.ptr(plan.xs), len(plan.xs),
+            N.ptr(plan.ys), len(plan.ys), N.ptr(plan.zs), len(plan.zs), grid.ctypes.data))
+        self.grid = tuple(plan.grid)
+
+    def load(self, plan) -> None:
+        self.upload(plan)
+        self.set_subboxes(plan)
+
+    def vertex_density(self, rho_bar: float) -> None:
+        N.check(self.lib.dtfe_gpu_vertex_density(self.h, float(rho_bar)))
+
+    def download_vertex_density(self, n_verts: int) -> np.ndarray:
+        out = np.empty(n_verts, np.float32)
+        N.check(self.lib.dtfe_gpu_download_vertex_density(self.h, out.ctypes.data))
+        return out
+
+    def _opts(self, fields, method, n_samples, seed, fix):
+        return N.InterpOpts(method, n_samples, seed, _mask(fields), N.FLAG_FIX_VALUE_INTERP if fix else 0)
+
+    def interpolate(self, fields, method: int = 0, n_samples: int = 1, seed: int = 0, fix: bool = False,
+                    out: dict | None = None) -> dict:
+        """Host outputs: dict field -> float32 array (G, ncomp) or (G,)."""
+        G = int(np.prod(self.grid))
+        outs = [None] * N.NUM_FIELDS
+        res = {}
+        for f in fields:
+            s = N.FIELD_SLOTS[f]
+            nc = N.field_components(s, self.n_scalars)
+            a = out[f] if out and f in out else np.empty((G, nc) if nc > 1 else G, np.float32)
+            res[f] = a
+            outs[s] = N.ptr(a)
+        optr = (C.c_void_p * N.NUM_FIELDS)(*outs)
+        st = N.Status()
+        o = self._opts(fields, method, n_samples, seed, fix)
+        N.check(self.lib.dtfe_gpu_interpolate(self.h, C.byref(o), optr, C.byref(st)))
+        self.last_status = st.as_dict()
+        return res
+
+    def interpolate_dev(self, fields, outs_dev: dict, method: int = 0, n_samples: int = 1, seed: int = 0,
+                        fix: bool = False) -> dict:
+        """Device outputs: dict field -> device pointer or tensor."""
+        outs = [None] * N.NUM_FIELDS
+        for f in fields:
+            outs[N.FIELD_SLOTS[f]] = N.ptr(outs_dev[f]) if not isinstance(outs_dev[f], int) else outs_dev[f]
+        optr = (C.c_void_p * N.NUM_FIELDS)(*outs)
+        st = N.Status()
+        o = self._opts(fields, method, n_samples, seed, fix)
+        N.check(self.lib.dtfe_gpu_interpolate_dev(self.h, C.byref(o), optr, C.byref(st)))
+        self.last_status = st.as_dict()
+        return self.last_status
+
+    def locate_points(self, pts: np.ndarray, start: int = 0) -> np.ndarray:
+        pts = np.ascontiguousarray(pts, np.float64)
+        out = np.empty(len(pts), np.int32)
+        N.check(self.lib.dtfe_gpu_locate_points(self.h, len(pts), pts.ctypes.data, int(start), out.ctypes.data))
+        return out

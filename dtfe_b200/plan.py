@@ -1,0 +1,282 @@
+"""Host planning of a DTFE run (the part of DTFE() before the device work).
+
+``make_plan`` follows the reference's control flow
+(src/DTFE.cpp:76-251 and DTFE_parallel, src/DTFE.cpp:287-385):
+
+1. padding length from the particle count (User_options::updatePadding,
+   src/user_options.cc:1062-1089) and the average density
+   (averageDensity, src/subpartition.h:437-449) unless given;
+2. for a periodic box, the particles of the padded box from the 27 periodic
+   images (findParticlesInBox, src/subpartition.h:79-154);
+3. the sub-box split — a 2^a 3^b processor grid (parallelGrid) balanced by NGP
+   particle counts (optimalPartitionSplit) — each sub-box with its own padded
+   particle set;
+4. one Delaunay tessellation per sub-box (host, in parallel);
+5. per-tile sample coordinates with the reference's float raster.
+
+The result is a multi-tessellation in the flat format of include/dtfe_gpu.h:
+vertex and tetrahedron arrays of all sub-boxes concatenated, with global
+indices, plus one dtfe_subbox record per tile.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as N
+
+
+@dataclass
+class Plan:
+    tet_v: np.ndarray          # (T, 4) int32, global vertex ids
+    tet_n: np.ndarray          # (T, 4) int32, global tetrahedron ids or -1
+    xyz: np.ndarray            # (V, 3) float32 vertex positions
+    src: np.ndarray            # (V,) int32 source particle of each vertex
+    weight: np.ndarray         # (V,) float32
+    velocity: np.ndarray | None
+    scalar: np.ndarray | None
+    boxes: C.Array             # dtfe_subbox[K]
+    xs: np.ndarray
+    ys: np.ndarray
+    zs: np.ndarray
+    grid: tuple
+    rho_bar: float
+    padding: np.ndarray        # (6,) float32
+    timings: dict = field(default_factory=dict)
+
+    @property
+    def n_tets(self) -> int:
+        return int(self.tet_v.shape[0])
+
+    @property
+    def n_verts(self) -> int:
+        return int(self.xyz.shape[0])
+
+    @property
+    def n_boxes(self) -> int:
+        return len(self.boxes)
+
+    @property
+    def n_scalars(self) -> int:
+        return 0 if self.scalar is None else int(self.scalar.shape[1])
+
+    def box_list(self) -> list:
+        return [self.boxes[i] for i in range(len(self.boxes))]
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def padding_length(n_total: int, box_length, grid, padding_particles: float = 5.0, kind: int = 0) -> np.ndarray:
+    out = np.zeros(6, np.float32)
+    bl = _f32(box_length)
+    g = np.ascontiguousarray(grid, dtype=np.int64)
+    N.host().dtfe_padding_length(kind, padding_particles, n_total, bl.ctypes.data, g.ctypes.data, out.ctypes.data)
+    return out
+
+
+def average_density(weight: np.ndarray) -> float:
+    w = _f32(weight)
+    return float(N.host().dtfe_average_density(w.ctypes.data, len(w)))
+
+
+def select_in_box(pos: np.ndarray, full_box, padded_box, periodic: bool):
+    pos = _f32(pos)
+    fb = _f32(full_box)
+    pb = _f32(padded_box)
+    lib = N.host()
+    n = lib.dtfe_select_in_box(pos.ctypes.data, len(pos), fb.ctypes.data, pb.ctypes.data, int(periodic), None, None)
+    idx = np.empty(n, np.int32)
+    out = np.empty((n, 3), np.float32)
+    lib.dtfe_select_in_box(pos.ctypes.data, len(pos), fb.ctypes.data, pb.ctypes.data, int(periodic),
+                           idx.ctypes.data, out.ctypes.data)
+    return idx, out
+
+
+def parallel_grid(n_threads: int, grid) -> tuple:
+    g = np.ascontiguousarray(grid, dtype=np.int64)
+    out = np.zeros(3, np.int64)
+    N.host().dtfe_parallel_grid(int(n_threads), g.ctypes.data, out.ctypes.data)
+    return tuple(int(x) for x in out)
+
+
+def optimal_partition(pos: np.ndarray, grid, region, parts):
+    pos = _f32(pos)
+    g = np.ascontiguousarray(grid, dtype=np.int64)
+    r = _f32(region)
+    p = np.ascontiguousarray(parts, dtype=np.int64)
+    n = int(np.prod(p))
+    sub = np.zeros((n, 6), np.int64)
+    coords = np.zeros((n, 6), np.float32)
+    rc = N.host().dtfe_optimal_partition(pos.ctypes.data, len(pos), g.ctypes.data, r.ctypes.data, p.ctypes.data,
+                                         sub.ctypes.data, coords.ctypes.data)
+    if rc:
+        raise ValueError("more partitions than grid cells along an axis")
+    return sub, coords
+
+
+def axis_coords(lo: float, dx: float, n: int) -> np.ndarray:
+    out = np.empty(n, np.float32)
+    N.host().dtfe_axis_coords(float(np.float32(lo)), float(np.float32(dx)), n, out.ctypes.data)
+    return out
+
+
+def tessellate_many(point_sets: list, seed: int = 12345, sort_tets: bool = True):
+    """Delaunay tessellations of several float32 point sets in parallel.
+
+    Returns [(tet_v (T,4) int32, tet_n (T,4) int32, vmap (n,) int32)]."""
+    lib = N.host()
+    k = len(point_sets)
+    xyz64 = [np.ascontiguousarray(p, dtype=np.float64) for p in point_sets]
+    ptrs = (C.c_void_p * k)(*[a.ctypes.data for a in xyz64])
+    ns = (C.c_int64 * k)(*[len(a) for a in xyz64])
+    handles = (C.c_void_p * k)()
+    rcs = (C.c_int * k)()
+    lib.dtfe_tessellate_batch(k, ptrs, ns, seed, int(sort_tets), handles, rcs)
+    out = []
+    for i in range(k):
+        nt, npt, nd = C.c_int64(), C.c_int64(), C.c_int64()
+        lib.dtfe_tess_sizes(handles[i], C.byref(nt), C.byref(npt), C.byref(nd))
+        tv = np.empty((nt.value, 4), np.int32)
+        tn = np.empty((nt.value, 4), np.int32)
+        vm = np.empty(npt.value, np.int32)
+        lib.dtfe_tess_export(handles[i], tv.ctypes.data, tn.ctypes.data, vm.ctypes.data)
+        lib.dtfe_tess_release(handles[i])
+        if rcs[i] not in (0, 1):
+            raise RuntimeError(f"tessellation of point set {i} failed (status {rcs[i]})")
+        out.append((tv, tn, vm))
+    return out
+
+
+def _make_box(voff, nv, toff, nt, origin, dims, coff, dx, lo, part_no):
+    b = N.Subbox()
+    b.vert_offset, b.n_verts, b.tet_offset, b.n_tets = voff, nv, toff, nt
+    for a in range(3):
+        b.tile_origin[a] = int(origin[a])
+        b.tile_dims[a] = int(dims[a])
+        b.coord_offset[a] = int(coff[a])
+        b.dx[a] = float(dx[a])
+        b.lo[a] = float(lo[a])
+    b.part_no = int(part_no)
+    return b
+
+
+def assemble(sets: list, tiles: list, weight, velocity, scalar, grid, rho_bar, padding, timings) -> Plan:
+    """Concatenates per-sub-box (positions, source ids) and their tessellations.
+
+    sets:  [(src_idx int32, pos float32 (n,3))]
+    tiles: [(origin(3), dims(3), region(6) float32, part_no)]"""
+    t0 = time.time()
+    tess = tessellate_many([p for _, p in sets])
+    timings["tessellation_s"] = time.time() - t0
+    tv_all, tn_all, xyz_all, src_all = [], [], [], []
+    xs, ys, zs = [], [], []
+    boxes = (N.Subbox * len(sets))()
+    voff = toff = 0
+    coff = [0, 0, 0]
+    for k, ((src, pos), (tv, tn, _vm), (origin, dims, region, part_no)) in enumerate(zip(sets, tess, tiles)):
+        nv, nt = len(pos), len(tv)
+        tv_all.append(tv + voff)
+        tn_all.append(np.where(tn >= 0, tn + toff, -1).astype(np.int32))
+        xyz_all.append(pos)
+        src_all.append(src)
+        region = np.asarray(region, np.float32)
+        dx = np.empty(3, np.float32)
+        for a in range(3):
+            length = np.float32(region[2 * a + 1] - region[2 * a])
+            dx[a] = np.float32(length / np.float32(dims[a]))
+        xs.append(axis_coords(region[0], dx[0], dims[0]))
+        ys.append(axis_coords(region[2], dx[1], dims[1]))
+        zs.append(axis_coords(region[4], dx[2], dims[2]))
+        boxes[k] = _make_box(voff, nv, toff, nt, origin, dims, coff, dx, region[0::2], part_no)
+        coff = [coff[0] + dims[0], coff[1] + dims[1], coff[2] + dims[2]]
+        voff += nv
+        toff += nt
+    src = np.concatenate(src_all).astype(np.int32)
+    return Plan(
+        tet_v=np.ascontiguousarray(np.concatenate(tv_all)),
+        tet_n=np.ascontiguousarray(np.concatenate(tn_all)),
+        xyz=np.ascontiguousarray(np.concatenate(xyz_all)),
+        src=src,
+        weight=np.ascontiguousarray(weight[src], np.float32),
+        velocity=None if velocity is None else np.ascontiguousarray(velocity[src], np.float32),
+        scalar=None if scalar is None else np.ascontiguousarray(scalar[src], np.float32),
+        boxes=boxes,
+        xs=np.concatenate(xs), ys=np.concatenate(ys), zs=np.concatenate(zs),
+        grid=tuple(int(g) for g in grid), rho_bar=float(rho_bar),
+        padding=np.asarray(padding, np.float32), timings=timings)
+
+
+def make_plan(pos, weight, velocity=None, scalar=None, grid=(64, 64, 64), box=(0, 100, 0, 100, 0, 100),
+              periodic: bool = True, n_threads: int = 1, padding_particles: float = 5.0,
+              padding=None, average_density_value: float | None = None) -> Plan:
+    """Plans a single-box DTFE run split into parallelGrid(n_threads) sub-boxes.
+
+    average_density_value=None reproduces the reference's automatic value
+    (sum of weights / 35000^3); pass sum(w)/L^3 for the physical normalisation."""
+    timings = {}
+    t0 = time.time()
+    pos = _f32(pos)
+    weight = _f32(weight) if weight is not None else np.ones(len(pos), np.float32)
+    box = np.asarray(box, np.float32)
+    blen = np.array([box[1] - box[0], box[3] - box[2], box[5] - box[4]], np.float32)
+    pad = padding_length(len(pos), blen, grid, padding_particles) if padding is None else np.asarray(padding, np.float32)
+    rho_bar = average_density(weight) if average_density_value is None else float(np.float32(average_density_value))
+    padded = np.array([box[0] - pad[0], box[1] + pad[1], box[2] - pad[2], box[3] + pad[3],
+                       box[4] - pad[4], box[5] + pad[5]], np.float32)
+    if periodic:
+        src, ppos = select_in_box(pos, box, padded, True)
+    else:
+        src, ppos = np.arange(len(pos), dtype=np.int32), pos
+    pgrid = parallel_grid(n_threads, grid)
+    sets, tiles = [], []
+    if np.prod(pgrid) == 1:
+        sets.append((src, ppos))
+        tiles.append(((0, 0, 0), tuple(grid), box, -1))
+    else:
+        sub, coords = optimal_partition(ppos, grid, box, pgrid)
+        for k in range(len(sub)):
+            region = coords[k]
+            pb = np.array([region[0] - pad[0], region[1] + pad[1], region[2] - pad[2], region[3] + pad[3],
+                           region[4] - pad[4], region[5] + pad[5]], np.float32)
+            ki, kp = select_in_box(ppos, region, pb, False)
+            sets.append((src[ki], kp))
+            origin = (sub[k, 0], sub[k, 2], sub[k, 4])
+            dims = (sub[k, 1] - sub[k, 0], sub[k, 3] - sub[k, 2], sub[k, 5] - sub[k, 4])
+            tiles.append((origin, dims, region, k))
+    timings["selection_s"] = time.time() - t0
+    return assemble(sets, tiles, weight, velocity, scalar, grid, rho_bar, pad, timings)
+
+
+def make_subbox_plan(subboxes: list, grid=(64, 64, 64), padding_fraction: float = 0.1,
+                     velocity_key: str = "velocity") -> Plan:
+    """Plans independent periodic boxes, each interpolated to its own grid,
+    stacked along x in one main grid of (K*gx, gy, gz) cells."""
+    timings = {}
+    t0 = time.time()
+    sets, tiles = [], []
+    ws, vs, ss = [], [], []
+    base = 0
+    for k, p in enumerate(subboxes):
+        box = np.asarray(p.box, np.float32)
+        side = np.float32(box[1] - box[0])
+        pad = np.full(6, np.float32(padding_fraction) * side, np.float32)
+        padded = np.array([box[0] - pad[0], box[1] + pad[1], box[2] - pad[2], box[3] + pad[3],
+                           box[4] - pad[4], box[5] + pad[5]], np.float32)
+        src, ppos = select_in_box(p.pos, box, padded, True)
+        sets.append((src + base, ppos))
+        tiles.append(((k * grid[0], 0, 0), tuple(grid), box, -1))
+        ws.append(p.weight)
+        vs.append(p.velocity if p.velocity is not None else np.zeros((p.n, 3), np.float32))
+        base += p.n
+    timings["selection_s"] = time.time() - t0
+    weight = np.concatenate(ws)
+    velocity = np.concatenate(vs)
+    side = float(subboxes[0].box[1] - subboxes[0].box[0])
+    rho_bar = float(np.float32(sum(float(p.weight.sum()) for p in subboxes) / (len(subboxes) * side ** 3)))
+    main = (len(subboxes) * grid[0], grid[1], grid[2])
+    return assemble(sets, tiles, weight, velocity, None, main, rho_bar, np.zeros(6, np.float32), timings)

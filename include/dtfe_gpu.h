@@ -1,0 +1,181 @@
+/*
+ * dtfe_gpu.h — C ABI of the B200 DTFE interpolation path.
+ *
+ * The reference exposes one C++ entry point,
+ *     void DTFE(std::vector<Particle_data>*, std::vector<Sample_point>&,
+ *               User_options&, Quantities* u, Quantities* a)
+ * (src/DTFE.h:36-40, body src/DTFE.cpp:76-251), whose hot section is
+ * DTFE_interpolation() after the Delaunay tessellation is built
+ * (src/CGAL_triangulation/triangulation.cpp:98-144) and DTFE_parallel()
+ * for the sub-box split (src/DTFE.cpp:287-385).  This header is the seam at
+ * that point: the host builds the tessellation, flattens it, and drives the
+ * device through these functions.  A C++ shim with the reference's exact
+ * DTFE(...) signature (include/dtfe/DTFE.h) sits on top of it.
+ *
+ * Conventions
+ *  - Every function returns an int status (DTFE_OK = 0); nothing calls exit().
+ *  - Plain pointers and sizes only.  Pointers are HOST memory unless the
+ *    argument name ends in _dev.
+ *  - A handle owns its device buffers and one CUDA stream; use one handle
+ *    from one host thread at a time.  Calls are ordered on that stream.
+ *  - Tetrahedra are positively oriented (CGAL's cell orientation);
+ *    tet_v[4t+i] is vertex i of tetrahedron t and tet_n[4t+i] is the
+ *    tetrahedron across the face opposite vertex i, or -1 on the convex hull
+ *    (the reference's infinite cells).  Indices are global over all sub-boxes.
+ *  - Grids are x-slowest, z-fastest (gridCellIndex,
+ *    src/CGAL_triangulation/triangulation_miscellaneous.cc:219-237); each
+ *    output field is an array of cells, each cell holding the field's
+ *    components contiguously, i.e. the layout of the vectors in struct
+ *    Quantities (src/quantities.h:56-76).
+ */
+#ifndef DTFE_GPU_H
+#define DTFE_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+enum {
+  DTFE_OK = 0,
+  DTFE_ERR_ARG = 1,          /* invalid argument or size */
+  DTFE_ERR_CUDA = 2,         /* CUDA runtime error (message: dtfe_last_error) */
+  DTFE_ERR_ALLOC = 3,        /* device allocation failed */
+  DTFE_ERR_STATE = 4,        /* call out of order (e.g. interpolate before upload) */
+  DTFE_ERR_WALK = 5,         /* a point-location walk hit its step limit */
+  DTFE_ERR_DEGENERATE = 6,   /* fewer than 4 vertices: no tetrahedra */
+  DTFE_ERR_NO_DEVICE = 7,    /* no usable CUDA device / extension */
+  DTFE_ERR_TOO_LARGE = 8     /* request exceeds a documented maximum */
+};
+
+/* ---- output field slots (bit i of a field mask = slot i) --------------- */
+enum {
+  DTFE_DENSITY = 0,              /* 1 component            */
+  DTFE_VELOCITY = 1,             /* 3 components           */
+  DTFE_VELOCITY_GRADIENT = 2,    /* 9: [j*3+i] = d v_j / d x_i */
+  DTFE_VELOCITY_DIVERGENCE = 3,  /* 1                      */
+  DTFE_VELOCITY_SHEAR = 4,       /* 5: xx,xy,xz,yy,yz traceless */
+  DTFE_VELOCITY_VORTICITY = 5,   /* 3: xy,xz,yz            */
+  DTFE_VELOCITY_STD = 6,         /* 1 (Monte-Carlo method only) */
+  DTFE_SCALAR = 7,               /* S components           */
+  DTFE_SCALAR_GRADIENT = 8,      /* 3*S: [s*3+i]           */
+  DTFE_NUM_FIELDS = 9
+};
+#define DTFE_FIELD_BIT(slot) (1u << (slot))
+
+/* ---- interpolation methods (User_options::method, plus plain sampling) -- */
+enum {
+  DTFE_METHOD_CENTRE = 0,       /* field at the cell centre (uQuantities) */
+  DTFE_METHOD_MONTE_CARLO = 2,  /* mean of n random points per cell       */
+  DTFE_METHOD_EQUIDISTANT = 3   /* mean of n = m^3 equidistant points     */
+};
+
+/* ---- behaviour flags ---------------------------------------------------- */
+/* Reference velocityValue()/scalarValue() keep only the z term of the
+ * gradient product (unaveraged_interpolation.cc:116,159).  Default: keep that
+ * behaviour for parity; this flag evaluates the full dot product instead. */
+#define DTFE_FLAG_FIX_VALUE_INTERP 1u
+
+/* ---- limits -------------------------------------------------------------- */
+#define DTFE_MAX_SCALARS 8
+#define DTFE_MAX_STD_SAMPLES 64   /* velocity_std keeps every sample velocity */
+
+typedef struct dtfe_gpu_s* dtfe_handle;
+
+typedef struct {
+  int32_t device;        /* CUDA device ordinal */
+  int32_t n_scalars;     /* S, 0..DTFE_MAX_SCALARS */
+  int32_t max_walk_steps;/* 0 = default (65536) */
+  int32_t reserved;
+} dtfe_config;
+
+/* One sub-box: a padded tessellation of its own and the grid tile it owns.
+ * (DTFE_parallel / --partition chunks, src/DTFE.cpp:169-218,287-385;
+ * copySubgridInformation, src/subpartition.h:376-383.)  A single-box run is
+ * one sub-box covering the whole grid. */
+typedef struct {
+  int64_t vert_offset, n_verts;   /* vertex range of this tessellation */
+  int64_t tet_offset, n_tets;     /* tetrahedron range */
+  int32_t tile_origin[3];         /* first main-grid cell of the tile */
+  int32_t tile_dims[3];           /* tile size in cells */
+  int64_t coord_offset[3];        /* into the per-axis coordinate tables */
+  float   dx[3];                  /* cell size of the tile (float, as the reference) */
+  float   lo[3];                  /* lower corner of the tile region */
+  int32_t part_no;                /* partition number (Monte-Carlo seed offset) */
+  int32_t reserved;
+} dtfe_subbox;
+
+typedef struct {
+  int32_t method;       /* DTFE_METHOD_* */
+  int32_t n_samples;    /* points per cell for methods 2 and 3 */
+  uint64_t seed;        /* Monte-Carlo key (randomSeed) */
+  uint32_t fields;      /* mask of DTFE_FIELD_BIT(slot) */
+  uint32_t flags;       /* DTFE_FLAG_* */
+} dtfe_interp_opts;
+
+typedef struct {
+  int64_t n_samples_located;  /* point locations performed */
+  int64_t n_outside;          /* samples outside the hull (zeros, as infinite cells) */
+  int64_t n_walk_failures;    /* walks that hit the step limit */
+  int64_t n_walk_steps;       /* total walk steps */
+  int64_t n_exact_tests;      /* orientation tests resolved by exact arithmetic */
+  int64_t n_ties;             /* samples on a shared face/edge/vertex */
+} dtfe_status;
+
+/* ---- lifecycle ---------------------------------------------------------- */
+int dtfe_gpu_create(const dtfe_config* cfg, dtfe_handle* out);
+int dtfe_gpu_destroy(dtfe_handle h);
+/* Last error message of this thread (static storage). */
+const char* dtfe_last_error(void);
+
+/* Upload a (multi-)tessellation and its vertex data (host arrays).
+ * xyz: 3V floats (vertex positions, Particle_data::pos), w: V weights,
+ * vel: 3V velocities or NULL, scal: V*S scalars or NULL.
+ * Replaces the CGAL vertex storage filled by vertexData::setData
+ * (src/CGAL_triangulation/vertexData.h:45-56). */
+int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n,
+                    int64_t n_tets, const float* xyz, const float* w,
+                    const float* vel, const float* scal, int64_t n_verts);
+
+/* Describe the sub-boxes and the main grid.  xs/ys/zs hold the sample
+ * coordinates of every tile along each axis (the reference's running
+ * float sums x += dx, unaveraged_interpolation.cc:270-358). */
+int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* boxes,
+                          const float* xs, int64_t n_xs, const float* ys, int64_t n_ys,
+                          const float* zs, int64_t n_zs, const int32_t grid[3]);
+
+/* Vertex densities rho_v = w_v (D+1) / (rho_bar * sum of incident volumes),
+ * 0 on the hull (vertexDensity, triangulation.cpp:200-279). */
+int dtfe_gpu_vertex_density(dtfe_handle h, double rho_bar);
+
+/* Interpolate to the grid.  out[slot] receives field `slot` when its bit is
+ * set in opts->fields (host pointers, sized grid cells x components).
+ * (interpolateGrid, unaveraged_interpolation.cc:209-369;
+ *  interpolateGrid_averaged_2/_3, averaged_interpolation_2.cc:35-233,664-866;
+ *  computeDivergenceShearVorticity, src/DTFE.cpp:394-475.) */
+int dtfe_gpu_interpolate(dtfe_handle h, const dtfe_interp_opts* opts,
+                         float* const out[DTFE_NUM_FIELDS], dtfe_status* st);
+/* Same, writing into device buffers. */
+int dtfe_gpu_interpolate_dev(dtfe_handle h, const dtfe_interp_opts* opts,
+                             float* const out_dev[DTFE_NUM_FIELDS], dtfe_status* st);
+
+/* Copy the vertex densities (V floats) to the host. */
+int dtfe_gpu_download_vertex_density(dtfe_handle h, float* dens);
+
+/* Locate np points (host doubles, 3 per point) with the device walk from
+ * tetrahedron `start`; out[i] = canonical tetrahedron id, -1 outside the
+ * hull, -2 walk failure.  (dt.locate, unaveraged_interpolation.cc:289.) */
+int dtfe_gpu_locate_points(dtfe_handle h, int64_t np, const double* pts, int32_t start,
+                           int32_t* out);
+
+/* Stream the handle's work is ordered on (a cudaStream_t). */
+void* dtfe_gpu_stream(dtfe_handle h);
+/* Block until the handle's stream is idle. */
+int dtfe_gpu_synchronize(dtfe_handle h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DTFE_GPU_H */

@@ -1,0 +1,550 @@
+// CPU oracle for the DTFE interpolation path — TEST INFRASTRUCTURE ONLY.
+//
+// Only tests, the smoke check and bench.py's CPU-baseline leg may load this
+// library, and only as the checker or the timed CPU baseline; the product path
+// never calls it.
+//
+// It restates, function by function, the reference algorithm
+// (lrwesterhoek/DTFE, C++/CGAL/OpenMP) on the flat tessellation format:
+//   vertexDensity            src/CGAL_triangulation/triangulation.cpp:200-279
+//   matrixInverse, minorDeterminant
+//                            src/CGAL_triangulation/triangulation_miscellaneous.cc:25,42-96
+//   positionMatrix .. scalarGradient
+//                            src/CGAL_triangulation/unaveraged_interpolation.cc:34-173
+//   interpolateGrid          unaveraged_interpolation.cc:209-369
+//   interpolateGrid_averaged_2 / _3
+//                            src/CGAL_triangulation/averaged_interpolation_2.cc:35-233,664-866
+//   standardDeviation        triangulation_miscellaneous.cc:256-271
+//   velocityDivergence/Shear/Vorticity
+//                            src/DTFE.cpp:394-433
+// in two arithmetic modes:
+//   mode 0 "ref":  the reference's precision pattern (double edge matrix and
+//                  inverse rounded to float, float gradients and values,
+//                  double products of the float offset) without FMA
+//                  contraction; vertex-volume sums in FP64;
+//   mode 1 "fp64": every quantity in double — the accuracy yardstick.
+// Point location is a visibility walk with exact predicates followed by the
+// canonical tie rule (the lowest-numbered tetrahedron whose closure holds the
+// point), so it is independent of the walk path.
+//
+// Parity status: the reference cannot be built in this environment (CGAL,
+// Boost and GSL are absent) and ships no tests or golden data; the
+// restatement is pinned by the analytic known-answer tests in tests/ and by
+// agreement with an independent tessellator (scipy Qhull).
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "../include/dtfe_gpu.h"
+#include "../dtfe_b200/csrc/philox.h"
+#include "../dtfe_b200/csrc/predicates.h"
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+struct Tess {
+  int64_t T, V;
+  const int32_t* tv;
+  const int32_t* tn;
+  const float* xyz;
+  const float* vel;
+  const float* scal;
+  int S;
+  void P(int32_t v, double out[3]) const {
+    for (int k = 0; k < 3; ++k) out[k] = (double)xyz[3 * (int64_t)v + k];
+  }
+};
+
+// orientation of tetrahedron t with vertex i replaced by p
+int face_orient(const Tess& g, int64_t t, int i, const double* p) {
+  double q[4][3];
+  for (int a = 0; a < 4; ++a) {
+    if (a == i) { q[a][0] = p[0]; q[a][1] = p[1]; q[a][2] = p[2]; }
+    else g.P(g.tv[4 * t + a], q[a]);
+  }
+  return dtfe::orient(q[0], q[1], q[2], q[3]);
+}
+
+bool contains(const Tess& g, int64_t t, const double* p, int zero[4]) {
+  for (int i = 0; i < 4; ++i) {
+    int o = face_orient(g, t, i, p);
+    if (o < 0) return false;
+    zero[i] = (o == 0);
+  }
+  return true;
+}
+
+// Canonical location: walk, then the lowest id among tetrahedra whose closure
+// contains p.  Returns -1 when p is outside the hull (an infinite cell in the
+// reference), -2 when the walk fails.
+int64_t locate(const Tess& g, const double* p, int64_t start, int64_t lo, int64_t hi) {
+  int64_t t = start;
+  if (t < lo || t >= hi) t = lo;
+  int64_t limit = 4 * (hi - lo) + 64;
+  for (int64_t step = 0;; ++step) {
+    if (step > limit) return -2;
+    int moved = -1;
+    for (int i = 0; i < 4; ++i) {
+      if (face_orient(g, t, i, p) < 0) { moved = i; break; }
+    }
+    if (moved < 0) break;
+    int64_t nb = g.tn[4 * t + moved];
+    if (nb < 0) return -1;
+    t = nb;
+  }
+  int zero[4];
+  contains(g, t, p, zero);
+  if (!zero[0] && !zero[1] && !zero[2] && !zero[3]) return t;
+  // tie: explore the tetrahedra around the face/edge/vertex holding p
+  std::vector<int64_t> seen{t}, queue{t};
+  int64_t best = t;
+  while (!queue.empty()) {
+    int64_t u = queue.back();
+    queue.pop_back();
+    int zu[4];
+    contains(g, u, p, zu);
+    for (int i = 0; i < 4; ++i) {
+      if (!zu[i]) continue;
+      int64_t nb = g.tn[4 * u + i];
+      if (nb < 0) continue;
+      if (std::find(seen.begin(), seen.end(), nb) != seen.end()) continue;
+      seen.push_back(nb);
+      int zn[4];
+      if (!contains(g, nb, p, zn)) continue;
+      queue.push_back(nb);
+      best = std::min(best, nb);
+    }
+  }
+  return best;
+}
+
+// ---- the reference's per-cell arithmetic ---------------------------------
+
+// minorDeterminant + matrixInverse (triangulation_miscellaneous.cc:42-96):
+// double cofactors divided by det; zero when |det|/sum|m| <= 1e-6.
+template <typename R>
+void matrix_inverse(const double A[3][3], R out[3][3]) {
+  auto minor = [&](int row, int col) {
+    int i1 = (row + 1) % 3, i2 = (row + 2) % 3, j1 = (col + 1) % 3, j2 = (col + 2) % 3;
+    return A[j1][i1] * A[j2][i2] - A[j1][i2] * A[j2][i1];
+  };
+  double det = A[0][0] * minor(0, 0) + A[0][1] * minor(1, 0) + A[0][2] * minor(2, 0);
+  double tmp[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) tmp[r][c] = minor(r, c) / det;
+  // accumulation order of the reference: left-to-right over the 9 entries
+  double s = std::fabs(A[0][0]) + std::fabs(A[0][1]) + std::fabs(A[0][2]) + std::fabs(A[1][0]) +
+      std::fabs(A[1][1]) + std::fabs(A[1][2]) + std::fabs(A[2][0]) + std::fabs(A[2][1]) +
+      std::fabs(A[2][2]);
+  bool ok = std::fabs(det / s) > 1.e-6;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) out[r][c] = ok ? (R)tmp[r][c] : (R)0;
+}
+
+struct CellEval {
+  // results of one sample
+  double dens, vel[3], grad[9], sc[DTFE_MAX_SCALARS], scg[3 * DTFE_MAX_SCALARS];
+};
+
+// Evaluates the fields of tetrahedron t at point p in the given mode.
+// positionMatrix/relativeSamplePoint (unaveraged_interpolation.cc:34-59),
+// densityGrad/densityValue (:66-87), velocityGrad/velocityValue (:94-120),
+// velocityGradient (:123-130), scalarGrad/scalarValue/scalarGradient (:137-173).
+void eval_cell(const Tess& g, const float* dens32, const double* dens64, int64_t t,
+               const double* p, int mode, bool fix, bool want_vel, bool want_sc,
+               CellEval& e) {
+  const int32_t* v = &g.tv[4 * t];
+  double X[4][3];
+  for (int a = 0; a < 4; ++a) g.P(v[a], X[a]);
+  double A[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) A[r][c] = X[r + 1][c] - X[0][c];
+  if (mode == 0) {
+    float M[3][3];
+    matrix_inverse<float>(A, M);
+    float rel[3];
+    for (int c = 0; c < 3; ++c) rel[c] = (float)(p[c] - X[0][c]);
+    // density
+    float d0 = dens32[v[0]];
+    float dd[3];
+    for (int i = 0; i < 3; ++i) dd[i] = dens32[v[i + 1]] - d0;
+    float gr[3];
+    for (int i = 0; i < 3; ++i) {
+      float acc = 0.f;
+      for (int j = 0; j < 3; ++j) acc += M[i][j] * dd[j];
+      gr[i] = acc;
+    }
+    double s = (double)rel[0] * gr[0] + (double)rel[1] * gr[1] + (double)rel[2] * gr[2];
+    e.dens = (double)(d0 + (float)s);
+    if (want_vel && g.vel) {
+      float dv[3][3], VG[3][3];
+      const float* v0 = &g.vel[3 * (int64_t)v[0]];
+      for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 3; ++j) dv[k][j] = g.vel[3 * (int64_t)v[k + 1] + j] - v0[j];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          float acc = 0.f;
+          for (int k = 0; k < 3; ++k) acc += M[i][k] * dv[k][j];
+          VG[i][j] = acc;
+        }
+      for (int i = 0; i < 3; ++i) {
+        float tmp = 0.f;
+        if (fix) {
+          for (int j = 0; j < 3; ++j) tmp = (float)((double)tmp + (double)VG[j][i] * (double)rel[j]);
+        } else {
+          for (int j = 0; j < 3; ++j) tmp = (float)((double)VG[j][i] * (double)rel[j]);
+        }
+        e.vel[i] = (double)(tmp + v0[i]);
+      }
+      for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) e.grad[j * 3 + i] = (double)VG[i][j];
+    }
+    if (want_sc && g.scal && g.S > 0) {
+      int S = g.S;
+      const float* s0 = &g.scal[(int64_t)S * v[0]];
+      for (int q = 0; q < S; ++q) {
+        float ds[3], SG[3];
+        for (int k = 0; k < 3; ++k) ds[k] = g.scal[(int64_t)S * v[k + 1] + q] - s0[q];
+        for (int i = 0; i < 3; ++i) {
+          float acc = 0.f;
+          for (int k = 0; k < 3; ++k) acc += M[i][k] * ds[k];
+          SG[i] = acc;
+        }
+        float tmp = 0.f;
+        if (fix) {
+          for (int j = 0; j < 3; ++j) tmp = (float)((double)tmp + (double)SG[j] * (double)rel[j]);
+        } else {
+          for (int j = 0; j < 3; ++j) tmp = (float)((double)SG[j] * (double)rel[j]);
+        }
+        e.sc[q] = (double)(tmp + s0[q]);
+        for (int i = 0; i < 3; ++i) e.scg[q * 3 + i] = (double)SG[i];
+      }
+    }
+  } else {
+    double M[3][3];
+    matrix_inverse<double>(A, M);
+    double rel[3];
+    for (int c = 0; c < 3; ++c) rel[c] = p[c] - X[0][c];
+    double d0 = dens64[v[0]];
+    double gr[3];
+    for (int i = 0; i < 3; ++i) {
+      gr[i] = 0;
+      for (int j = 0; j < 3; ++j) gr[i] += M[i][j] * (dens64[v[j + 1]] - d0);
+    }
+    e.dens = d0 + rel[0] * gr[0] + rel[1] * gr[1] + rel[2] * gr[2];
+    if (want_vel && g.vel) {
+      double VG[3][3];
+      const float* v0 = &g.vel[3 * (int64_t)v[0]];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          VG[i][j] = 0;
+          for (int k = 0; k < 3; ++k)
+            VG[i][j] += M[i][k] * ((double)g.vel[3 * (int64_t)v[k + 1] + j] - (double)v0[j]);
+        }
+      for (int i = 0; i < 3; ++i) {
+        double tmp = 0;
+        if (fix) for (int j = 0; j < 3; ++j) tmp += VG[j][i] * rel[j];
+        else tmp = VG[2][i] * rel[2];
+        e.vel[i] = tmp + (double)v0[i];
+      }
+      for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) e.grad[j * 3 + i] = VG[i][j];
+    }
+    if (want_sc && g.scal && g.S > 0) {
+      int S = g.S;
+      const float* s0 = &g.scal[(int64_t)S * v[0]];
+      for (int q = 0; q < S; ++q) {
+        double SG[3];
+        for (int i = 0; i < 3; ++i) {
+          SG[i] = 0;
+          for (int k = 0; k < 3; ++k)
+            SG[i] += M[i][k] * ((double)g.scal[(int64_t)S * v[k + 1] + q] - (double)s0[q]);
+        }
+        double tmp = 0;
+        if (fix) for (int j = 0; j < 3; ++j) tmp += SG[j] * rel[j];
+        else tmp = SG[2] * rel[2];
+        e.sc[q] = tmp + (double)s0[q];
+        for (int i = 0; i < 3; ++i) e.scg[q * 3 + i] = SG[i];
+      }
+    }
+  }
+}
+
+// velocityDivergence / velocityShear / velocityVorticity (src/DTFE.cpp:394-433)
+void derived(const double* g9, int mode, double* div, double* shear, double* vort) {
+  if (mode == 0) {
+    float g[9];
+    for (int i = 0; i < 9; ++i) g[i] = (float)g9[i];
+    *div = (double)(g[0] + g[4] + g[8]);
+    float t[5];
+    int idx = 0;
+    for (int i = 0; i < 2; ++i)
+      for (int j = i; j < 3; ++j) t[idx++] = (float)((double)(g[i * 3 + j] + g[j * 3 + i]) / 2.);
+    float trace = (float)((double)(t[0] + t[3] + g[8]) / 3.);
+    t[0] -= trace;
+    t[3] -= trace;
+    for (int i = 0; i < 5; ++i) shear[i] = t[i];
+    idx = 0;
+    for (int i = 0; i < 3; ++i)
+      for (int j = i + 1; j < 3; ++j)
+        vort[idx++] = (double)(float)((double)(g[i * 3 + j] - g[j * 3 + i]) / 2.);
+  } else {
+    const double* g = g9;
+    *div = g[0] + g[4] + g[8];
+    double t[5];
+    int idx = 0;
+    for (int i = 0; i < 2; ++i)
+      for (int j = i; j < 3; ++j) t[idx++] = (g[i * 3 + j] + g[j * 3 + i]) / 2.;
+    double trace = (t[0] + t[3] + g[8]) / 3.;
+    t[0] -= trace;
+    t[3] -= trace;
+    for (int i = 0; i < 5; ++i) shear[i] = t[i];
+    idx = 0;
+    for (int i = 0; i < 3; ++i)
+      for (int j = i + 1; j < 3; ++j) vort[idx++] = (g[i * 3 + j] - g[j * 3 + i]) / 2.;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+// vertexDensity (triangulation.cpp:200-279): rho_v = w_v*(D+1)/(rho_bar*sum V),
+// 0 when any incident cell is infinite.  Volumes are the double determinant/6
+// (Tetrahedron_3::volume, triangulation_miscellaneous.cc:205-213), summed in
+// double in ascending tetrahedron order.  dens32: mode-0 result, float
+// factor (D+1)/rho_bar (:220) times the weight, divided by the double sum;
+// dens64: all-double result.  Either output may be NULL.
+int oracle_vertex_density(int64_t T, const int32_t* tv, const int32_t* tn, int64_t V,
+                          const float* xyz, const float* w, double rho_bar, float* dens32,
+                          double* dens64, double* volsum_out) {
+  std::vector<double> vol(V, 0.0);
+  std::vector<char> hull(V, 0);
+  for (int64_t t = 0; t < T; ++t) {
+    double X[4][3];
+    for (int a = 0; a < 4; ++a)
+      for (int k = 0; k < 3; ++k) X[a][k] = (double)xyz[3 * (int64_t)tv[4 * t + a] + k];
+    double v6 = dtfe::orient_det(X[0], X[1], X[2], X[3]);
+    double vt = v6 / 6.0;
+    for (int a = 0; a < 4; ++a) vol[tv[4 * t + a]] += vt;
+    for (int i = 0; i < 4; ++i)
+      if (tn[4 * t + i] < 0)
+        for (int a = 0; a < 4; ++a)
+          if (a != i) hull[tv[4 * t + a]] = 1;
+  }
+  float rb = (float)rho_bar;
+  float factor = (float)(4.0 / (double)rb);
+  for (int64_t v = 0; v < V; ++v) {
+    bool zero = hull[v] || vol[v] == 0.0;
+    if (dens32) dens32[v] = zero ? 0.f : (float)((double)(w[v] * factor) / vol[v]);
+    if (dens64) dens64[v] = zero ? 0.0 : (double)w[v] * 4.0 / ((double)rb * vol[v]);
+    if (volsum_out) volsum_out[v] = vol[v];
+  }
+  return 0;
+}
+
+// Canonical location of np points (double xyz) in tetrahedra [lo, hi).
+int oracle_locate(int64_t T, const int32_t* tv, const int32_t* tn, const float* xyz,
+                  int64_t lo, int64_t hi, int64_t np, const double* pts, int64_t* out) {
+  Tess g{T, 0, tv, tn, xyz, nullptr, nullptr, 0};
+  int64_t hint = lo;
+  for (int64_t i = 0; i < np; ++i) {
+    int64_t r = locate(g, &pts[3 * i], hint, lo, hi);
+    out[i] = r;
+    if (r >= 0) hint = r;
+  }
+  return 0;
+}
+
+// Interpolation over the sub-boxes into double outputs (main-grid layout).
+// out[slot] may be NULL for unrequested fields.  loc (optional) receives the
+// canonical tetrahedron of every cell centre (-1 outside the hull).
+// nthreads > 0 parallelises over x-slabs of each tile.
+int oracle_interpolate(int64_t T, const int32_t* tv, const int32_t* tn, int64_t V,
+                       const float* xyz, const float* vel, const float* scal, int S,
+                       const float* dens32, const double* dens64, int K,
+                       const dtfe_subbox* boxes, const float* xs, const float* ys,
+                       const float* zs, const int32_t grid[3], const dtfe_interp_opts* o,
+                       int mode, double* const out[DTFE_NUM_FIELDS], int64_t* loc,
+                       int nthreads, int64_t* n_fail) {
+  Tess g{T, V, tv, tn, xyz, vel, scal, S};
+  const uint32_t f = o->fields;
+  const bool fix = (o->flags & DTFE_FLAG_FIX_VALUE_INTERP) != 0;
+  auto has = [&](int s) { return (f & DTFE_FIELD_BIT(s)) != 0 && out[s] != nullptr; };
+  const bool want_grad = has(DTFE_VELOCITY_GRADIENT) || has(DTFE_VELOCITY_DIVERGENCE) ||
+                         has(DTFE_VELOCITY_SHEAR) || has(DTFE_VELOCITY_VORTICITY);
+  const bool want_vel = has(DTFE_VELOCITY) || want_grad || has(DTFE_VELOCITY_STD);
+  const bool want_sc = has(DTFE_SCALAR) || has(DTFE_SCALAR_GRADIENT);
+  const int method = o->method;
+  const int NN = method == DTFE_METHOD_CENTRE ? 1 : o->n_samples;
+  if (NN < 1) return DTFE_ERR_ARG;
+  if (has(DTFE_VELOCITY_STD) && (method != DTFE_METHOD_MONTE_CARLO || NN > DTFE_MAX_STD_SAMPLES))
+    return DTFE_ERR_ARG;
+  int nroot = 1;
+  if (method == DTFE_METHOD_EQUIDISTANT) {
+    nroot = (int)std::lround(std::cbrt((double)NN));
+    if (nroot * nroot * nroot != NN) return DTFE_ERR_ARG;
+  }
+  int64_t fails = 0;
+  const int64_t G1 = grid[1], G2 = grid[2];
+  for (int b = 0; b < K; ++b) {
+    const dtfe_subbox& B = boxes[b];
+    const int64_t lo = B.tet_offset, hi = B.tet_offset + B.n_tets;
+    const float dx[3] = {B.dx[0], B.dx[1], B.dx[2]};
+    const uint64_t key = dtfe::mc_key(o->seed, B.part_no);
+    // equidistant offsets (averaged_interpolation_2.cc:726-740)
+    std::vector<float> eq(3 * (size_t)NN);
+    if (method == DTFE_METHOD_EQUIDISTANT) {
+      for (int i1 = 0; i1 < nroot; ++i1)
+        for (int i2 = 0; i2 < nroot; ++i2)
+          for (int i3 = 0; i3 < nroot; ++i3) {
+            int idx = i1 * nroot * nroot + i2 * nroot + i3;
+            eq[3 * idx + 2] = (float)((i3 + 0.5) * (double)dx[2] / nroot - (double)dx[2] / 2.);
+            eq[3 * idx + 0] = (float)((i1 + 0.5) * (double)dx[0] / nroot - (double)dx[0] / 2.);
+            eq[3 * idx + 1] = (float)((i2 + 0.5) * (double)dx[1] / nroot - (double)dx[1] / 2.);
+          }
+    }
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads > 0 ? nthreads : 1) reduction(+ : fails)
+    for (int i = 0; i < B.tile_dims[0]; ++i) {
+      int64_t hint = lo;
+      std::vector<double> stdv(3 * (size_t)std::max(NN, 1));
+      for (int j = 0; j < B.tile_dims[1]; ++j)
+        for (int k = 0; k < B.tile_dims[2]; ++k) {
+          const float x = xs[B.coord_offset[0] + i], y = ys[B.coord_offset[1] + j],
+                      z = zs[B.coord_offset[2] + k];
+          const int64_t cell = ((int64_t)(B.tile_origin[0] + i) * G1 + (B.tile_origin[1] + j)) * G2 +
+                               (B.tile_origin[2] + k);
+          double pc[3] = {(double)x, (double)y, (double)z};
+          int64_t tc = locate(g, pc, hint, lo, hi);
+          if (tc == -2) { ++fails; tc = -1; }
+          if (tc >= 0) hint = tc;
+          if (loc) loc[cell] = tc;
+          // accumulators: float in mode 0, double in mode 1
+          float fD = 0.f, fV[3] = {0, 0, 0}, fG[9] = {0}, fS[DTFE_MAX_SCALARS] = {0},
+                fSG[3 * DTFE_MAX_SCALARS] = {0};
+          double dD = 0, dV[3] = {0, 0, 0}, dG[9] = {0}, dS[DTFE_MAX_SCALARS] = {0},
+                 dSG[3 * DTFE_MAX_SCALARS] = {0};
+          for (size_t q = 0; q < stdv.size(); ++q) stdv[q] = 0.0;
+          for (int w = 0; w < NN; ++w) {
+            double p[3];
+            int64_t t;
+            if (method == DTFE_METHOD_CENTRE) {
+              p[0] = pc[0]; p[1] = pc[1]; p[2] = pc[2];
+              t = tc;
+            } else {
+              if (method == DTFE_METHOD_MONTE_CARLO) {
+                double u[3];
+                dtfe::mc_offsets(key, (uint64_t)cell, (uint32_t)w, u);
+                for (int c = 0; c < 3; ++c) p[c] = u[c] * (double)dx[c] + pc[c];
+              } else {
+                p[0] = (double)(x + eq[3 * w + 0]);
+                p[1] = (double)(y + eq[3 * w + 1]);
+                p[2] = (double)(z + eq[3 * w + 2]);
+              }
+              t = locate(g, p, tc >= 0 ? tc : hint, lo, hi);
+              if (t == -2) { ++fails; t = -1; }
+            }
+            if (t < 0) continue;  // infinite cell: contributes nothing
+            CellEval e{};
+            eval_cell(g, dens32, dens64, t, p, mode, fix, want_vel, want_sc, e);
+            if (mode == 0) {
+              fD += (float)e.dens;
+              for (int c = 0; c < 3; ++c) fV[c] += (float)e.vel[c];
+              for (int c = 0; c < 9; ++c) fG[c] += (float)e.grad[c];
+              for (int q = 0; q < S; ++q) {
+                fS[q] += (float)e.sc[q];
+                for (int c = 0; c < 3; ++c) fSG[3 * q + c] += (float)e.scg[3 * q + c];
+              }
+            } else {
+              dD += e.dens;
+              for (int c = 0; c < 3; ++c) dV[c] += e.vel[c];
+              for (int c = 0; c < 9; ++c) dG[c] += e.grad[c];
+              for (int q = 0; q < S; ++q) {
+                dS[q] += e.sc[q];
+                for (int c = 0; c < 3; ++c) dSG[3 * q + c] += e.scg[3 * q + c];
+              }
+            }
+            if (want_vel)
+              for (int c = 0; c < 3; ++c) stdv[3 * w + c] = e.vel[c];
+          }
+          double D, Vv[3], Gg[9], Ss[DTFE_MAX_SCALARS], SGg[3 * DTFE_MAX_SCALARS], sd = 0;
+          if (mode == 0) {
+            float fn = (float)NN;
+            D = (double)(fD / fn);
+            for (int c = 0; c < 3; ++c) Vv[c] = (double)(fV[c] / fn);
+            for (int c = 0; c < 9; ++c) Gg[c] = (double)(fG[c] / fn);
+            for (int q = 0; q < S; ++q) {
+              Ss[q] = (double)(fS[q] / fn);
+              for (int c = 0; c < 3; ++c) SGg[3 * q + c] = (double)(fSG[3 * q + c] / fn);
+            }
+            if (has(DTFE_VELOCITY_STD)) {
+              // standardDeviation for Pvector (triangulation_miscellaneous.cc:256-271)
+              float mean[3] = {0, 0, 0};
+              for (int w = 0; w < NN; ++w)
+                for (int c = 0; c < 3; ++c) mean[c] += (float)stdv[3 * w + c];
+              for (int c = 0; c < 3; ++c) mean[c] /= (float)NN;
+              float r = 0.f;
+              for (int w = 0; w < NN; ++w)
+                for (int c = 0; c < 3; ++c) {
+                  float d = (float)stdv[3 * w + c] - mean[c];
+                  r += d * d;
+                }
+              sd = (double)std::sqrt(r / (float)NN);
+            }
+          } else {
+            D = dD / NN;
+            for (int c = 0; c < 3; ++c) Vv[c] = dV[c] / NN;
+            for (int c = 0; c < 9; ++c) Gg[c] = dG[c] / NN;
+            for (int q = 0; q < S; ++q) {
+              Ss[q] = dS[q] / NN;
+              for (int c = 0; c < 3; ++c) SGg[3 * q + c] = dSG[3 * q + c] / NN;
+            }
+            if (has(DTFE_VELOCITY_STD)) {
+              double mean[3] = {0, 0, 0};
+              for (int w = 0; w < NN; ++w)
+                for (int c = 0; c < 3; ++c) mean[c] += stdv[3 * w + c];
+              for (int c = 0; c < 3; ++c) mean[c] /= NN;
+              double r = 0;
+              for (int w = 0; w < NN; ++w)
+                for (int c = 0; c < 3; ++c) {
+                  double d = stdv[3 * w + c] - mean[c];
+                  r += d * d;
+                }
+              sd = std::sqrt(r / NN);
+            }
+          }
+          if (has(DTFE_DENSITY)) out[DTFE_DENSITY][cell] = D;
+          if (has(DTFE_VELOCITY))
+            for (int c = 0; c < 3; ++c) out[DTFE_VELOCITY][3 * cell + c] = Vv[c];
+          if (has(DTFE_VELOCITY_GRADIENT))
+            for (int c = 0; c < 9; ++c) out[DTFE_VELOCITY_GRADIENT][9 * cell + c] = Gg[c];
+          if (has(DTFE_VELOCITY_DIVERGENCE) || has(DTFE_VELOCITY_SHEAR) ||
+              has(DTFE_VELOCITY_VORTICITY)) {
+            double dv, sh[5], vo[3];
+            derived(Gg, mode, &dv, sh, vo);
+            if (has(DTFE_VELOCITY_DIVERGENCE)) out[DTFE_VELOCITY_DIVERGENCE][cell] = dv;
+            if (has(DTFE_VELOCITY_SHEAR))
+              for (int c = 0; c < 5; ++c) out[DTFE_VELOCITY_SHEAR][5 * cell + c] = sh[c];
+            if (has(DTFE_VELOCITY_VORTICITY))
+              for (int c = 0; c < 3; ++c) out[DTFE_VELOCITY_VORTICITY][3 * cell + c] = vo[c];
+          }
+          if (has(DTFE_VELOCITY_STD)) out[DTFE_VELOCITY_STD][cell] = sd;
+          if (has(DTFE_SCALAR))
+            for (int q = 0; q < S; ++q) out[DTFE_SCALAR][(int64_t)S * cell + q] = Ss[q];
+          if (has(DTFE_SCALAR_GRADIENT))
+            for (int q = 0; q < 3 * S; ++q)
+              out[DTFE_SCALAR_GRADIENT][(int64_t)3 * S * cell + q] = SGg[q];
+        }
+    }
+  }
+  if (n_fail) *n_fail = fails;
+  return fails ? DTFE_ERR_WALK : DTFE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,97 @@
+"""Python access to the CPU oracle (liboracle.so) — TEST INFRASTRUCTURE ONLY.
+
+Used by tests/, the smoke check and bench.py's CPU-baseline leg as the
+checker; never by the product path.  See dtfe_oracle.cpp for what it
+restates and in which arithmetic modes.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_ROOT = os.path.dirname(_HERE)
+if _ROOT not in sys.path:
+    sys.path.insert(0, _ROOT)
+
+from dtfe_b200 import _native as N  # noqa: E402  (struct definitions only)
+
+MODE_REF, MODE_FP64 = 0, 1
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        from dtfe_b200 import build
+        path = build.build_oracle()
+        L = C.CDLL(path)
+        vp = C.c_void_p
+        L.oracle_vertex_density.argtypes = [C.c_int64, vp, vp, C.c_int64, vp, vp, C.c_double, vp, vp, vp]
+        L.oracle_locate.argtypes = [C.c_int64, vp, vp, vp, C.c_int64, C.c_int64, C.c_int64, vp, vp]
+        L.oracle_interpolate.argtypes = [C.c_int64, vp, vp, C.c_int64, vp, vp, vp, C.c_int, vp, vp, C.c_int,
+                                         vp, vp, vp, vp, vp, C.POINTER(N.InterpOpts), C.c_int,
+                                         C.POINTER(C.c_void_p), vp, C.c_int, vp]
+        _lib = L
+    return _lib
+
+
+def vertex_density(plan, rho_bar: float | None = None):
+    """(dens32 float32 (V,), dens64 float64 (V,), volsum float64 (V,))."""
+    rb = plan.rho_bar if rho_bar is None else rho_bar
+    V = plan.n_verts
+    d32 = np.empty(V, np.float32)
+    d64 = np.empty(V, np.float64)
+    vs = np.empty(V, np.float64)
+    lib().oracle_vertex_density(plan.n_tets, plan.tet_v.ctypes.data, plan.tet_n.ctypes.data, V,
+                                plan.xyz.ctypes.data, plan.weight.ctypes.data, rb,
+                                d32.ctypes.data, d64.ctypes.data, vs.ctypes.data)
+    return d32, d64, vs
+
+
+def locate(plan, pts: np.ndarray, box: int = 0) -> np.ndarray:
+    pts = np.ascontiguousarray(pts, np.float64)
+    b = plan.boxes[box]
+    out = np.empty(len(pts), np.int64)
+    lib().oracle_locate(plan.n_tets, plan.tet_v.ctypes.data, plan.tet_n.ctypes.data, plan.xyz.ctypes.data,
+                        b.tet_offset, b.tet_offset + b.n_tets, len(pts), pts.ctypes.data, out.ctypes.data)
+    return out
+
+
+def interpolate(plan, dens32, dens64, fields, method: int = 0, n_samples: int = 1, seed: int = 0,
+                mode: int = MODE_REF, fix: bool = False, nthreads: int = 1, want_loc: bool = False):
+    """Returns (dict field -> float64 array shaped (G, ncomp) or (G,), loc or None)."""
+    G = int(np.prod(plan.grid))
+    S = plan.n_scalars
+    mask = 0
+    outs = [None] * N.NUM_FIELDS
+    arrs = {}
+    for f in fields:
+        s = N.FIELD_SLOTS[f]
+        mask |= 1 << s
+        nc = N.field_components(s, S)
+        a = np.zeros((G, nc) if nc > 1 else G, np.float64)
+        arrs[f] = a
+        outs[s] = a.ctypes.data
+    optr = (C.c_void_p * N.NUM_FIELDS)(*[o if o else None for o in outs])
+    o = N.InterpOpts(method, n_samples, seed, mask, N.FLAG_FIX_VALUE_INTERP if fix else 0)
+    loc = np.full(G, -1, np.int64) if want_loc else None
+    nfail = C.c_int64(0)
+    vel = plan.velocity.ctypes.data if plan.velocity is not None else None
+    sc = plan.scalar.ctypes.data if plan.scalar is not None else None
+    grid = np.asarray(plan.grid, np.int32)
+    rc = lib().oracle_interpolate(plan.n_tets, plan.tet_v.ctypes.data, plan.tet_n.ctypes.data, plan.n_verts,
+                                  plan.xyz.ctypes.data, vel, sc, S,
+                                  None if dens32 is None else dens32.ctypes.data,
+                                  None if dens64 is None else dens64.ctypes.data,
+                                  plan.n_boxes, C.addressof(plan.boxes), plan.xs.ctypes.data, plan.ys.ctypes.data,
+                                  plan.zs.ctypes.data, grid.ctypes.data, C.byref(o), mode, optr,
+                                  None if loc is None else loc.ctypes.data, nthreads, C.byref(nfail))
+    if rc not in (0, 5):
+        raise RuntimeError(f"oracle_interpolate failed with status {rc}")
+    if nfail.value:
+        raise RuntimeError(f"oracle walk failed on {nfail.value} samples")
+    return arrs, loc

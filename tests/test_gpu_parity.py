@@ -1,0 +1,116 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
+
+Bars:
+  * point location: bit-exact tetrahedron ids (canonical tie rule);
+  * vertex densities: equal to the oracle's mode-"ref" float values up to one
+    float ulp (the FP64 volume sums are accumulated in a different order);
+  * interpolated fields vs the oracle in the reference's arithmetic (mode ref):
+    relative error <= 1e-6;
+  * interpolated fields vs the FP64 oracle: relative error <= 1e-5 (the
+    north-star tolerance), denominators floored at the field's RMS.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import rel_err
+from dtfe_b200 import plan as P
+from dtfe_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ["density", "velocity", "velocity_gradient", "velocity_divergence", "velocity_shear",
+          "velocity_vorticity", "scalar", "scalar_gradient"]
+
+
+def _plan(n=24, grid=(24, 24, 24), n_threads=1, rms=0.5, seed=0, n_scalars=1):
+    pos, psi = S.zeldovich_lattice(n, 100.0, rms, seed)
+    w = np.random.default_rng(seed + 10).uniform(0.5, 1.5, len(pos)).astype(np.float32)
+    vel = (100 * psi / (100.0 / n)).astype(np.float32)
+    sc = np.random.default_rng(seed + 20).standard_normal((len(pos), n_scalars)).astype(np.float32) \
+        if n_scalars else None
+    return P.make_plan(pos, w, vel, sc, grid=grid, n_threads=n_threads,
+                       average_density_value=float(w.sum()) / 1e6)
+
+
+@pytest.fixture(scope="module")
+def plan1(gpu_built):
+    return _plan()
+
+
+@pytest.fixture(scope="module")
+def plan8(gpu_built):
+    return _plan(n=20, grid=(20, 20, 20), n_threads=8, n_scalars=2)
+
+
+def _device(plan):
+    from dtfe_b200.device import DeviceDTFE
+    d = DeviceDTFE(0, plan.n_scalars)
+    d.load(plan)
+    d.vertex_density(plan.rho_bar)
+    return d
+
+
+def test_vertex_density(plan1):
+    d = _device(plan1)
+    g = d.download_vertex_density(plan1.n_verts)
+    d32, d64, _ = O.vertex_density(plan1)
+    ulps = np.abs(g.view(np.int32).astype(np.int64) - d32.view(np.int32).astype(np.int64))
+    assert ulps.max() <= 1
+    assert rel_err(g, d64) < 1e-6
+    d.close()
+
+
+def test_locate_bit_exact(plan1):
+    d = _device(plan1)
+    rng = np.random.default_rng(3)
+    pts = rng.random((20000, 3)) * 100.0
+    # include exact vertex positions and face/edge midpoints (ties)
+    tv = plan1.tet_v[:500]
+    X = plan1.xyz.astype(np.float64)
+    pts = np.concatenate([pts, X[tv[:, 0]], 0.5 * (X[tv[:, 0]] + X[tv[:, 1]]),
+                          (X[tv[:, 0]] + X[tv[:, 1]] + X[tv[:, 2]]) / 3.0])
+    g = d.locate_points(pts, start=0)
+    o = O.locate(plan1, pts)
+    assert (g == o).all(), np.flatnonzero(g != o)[:10]
+    d.close()
+
+
+@pytest.mark.parametrize("fix", [False, True])
+def test_centre_fields(plan1, fix):
+    d = _device(plan1)
+    g = d.interpolate(FIELDS, method=0, fix=fix)
+    assert d.last_status["n_walk_failures"] == 0
+    d32, d64, _ = O.vertex_density(plan1)
+    ref, _ = O.interpolate(plan1, d32, d64, FIELDS, mode=O.MODE_REF, fix=fix)
+    f64, _ = O.interpolate(plan1, d32, d64, FIELDS, mode=O.MODE_FP64, fix=fix)
+    for f in FIELDS:
+        assert rel_err(g[f], ref[f]) <= 1e-6, f
+        assert rel_err(g[f], f64[f]) <= 1e-5, f
+    d.close()
+
+
+@pytest.mark.parametrize("method,nn", [(2, 8), (3, 8)])
+def test_averaged_fields(plan1, method, nn):
+    d = _device(plan1)
+    fields = FIELDS + (["velocity_std"] if method == 2 else [])
+    g = d.interpolate(fields, method=method, n_samples=nn, seed=3)
+    d32, d64, _ = O.vertex_density(plan1)
+    ref, _ = O.interpolate(plan1, d32, d64, fields, method=method, n_samples=nn, seed=3, mode=O.MODE_REF)
+    f64, _ = O.interpolate(plan1, d32, d64, fields, method=method, n_samples=nn, seed=3, mode=O.MODE_FP64)
+    for f in fields:
+        assert rel_err(g[f], ref[f]) <= 1e-6, f
+        assert rel_err(g[f], f64[f]) <= 1e-5, f
+    d.close()
+
+
+def test_subboxes(plan8):
+    d = _device(plan8)
+    fields = FIELDS
+    g = d.interpolate(fields, method=0)
+    d32, d64, _ = O.vertex_density(plan8)
+    ref, loc = O.interpolate(plan8, d32, d64, fields, mode=O.MODE_REF, want_loc=True)
+    assert (loc >= 0).all()
+    for f in fields:
+        assert rel_err(g[f], ref[f]) <= 1e-6, f
+    d.close()

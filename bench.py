@@ -1,0 +1,417 @@
+#!/usr/bin/env python
+"""DTFE interpolation throughput on B200: grid samples/s.
+
+Workload (default): 256^3 Zel'dovich-displaced particles (rms displacement
+1.0 lattice spacing, velocities 100 km/s per unit displacement + N(0, 50
+km/s)) in a periodic 100 Mpc/h box, interpolated to a 256^3 grid.  A step is
+one pass of the hot path over the resident tessellation: vertex densities
+(FP64 volume reduction), seed bins, then one fused walk+interpolation launch
+producing cell-centre density, velocity, velocity gradient, divergence,
+shear and vorticity for every cell.  A grid sample is one fully evaluated
+output cell.  The host tessellation is built once before timing (the
+reference's CGAL step, excluded from the metric as it is cached).
+
+Keys beyond the base contract:
+  e2e          the same metric through the C ABI with host buffers: every step
+               uploads the tessellation and vertex data from pinned memory and
+               copies all output fields back
+  roofline     k_interpolate against the measured HBM copy bandwidth
+  cpu_baseline the CPU oracle (restated reference path) on the host cores,
+               on a bounded sample of the same workload
+  mc           Monte-Carlo cell average (8 points per cell) throughput
+
+--impl reference times the reference's CPU path (the oracle port: no CGAL or
+Boost exists here to build the reference itself) with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+FIELDS = ["density", "velocity", "velocity_gradient", "velocity_divergence", "velocity_shear",
+          "velocity_vorticity"]
+C_OUT = 1 + 3 + 9 + 1 + 5 + 3  # output floats per cell
+METRIC = "grid samples/s DTFE dens+vel-grad 256^3 vs plain GPU & CPU at ≤1e-5 rel; bwd/fwd"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256, help="particles per side (and grid cells per side)")
+    ap.add_argument("--threads", type=int, default=0, help="host threads (0 = all)")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mc", action="store_true")
+    return ap.parse_args()
+
+
+def host_threads(req: int) -> int:
+    if req > 0:
+        return req
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def build_workload(n: int, rank: int, threads: int):
+    from dtfe_b200 import plan as P
+    from dtfe_b200 import synthetic as S
+    t0 = time.time()
+    pos, psi = S.zeldovich_lattice(n, S.BOX, 1.0, seed=1 + 1000 * rank)
+    rng = np.random.default_rng(2 + 1000 * rank)
+    vel = (100.0 * psi / (S.BOX / n) + rng.normal(0.0, 50.0, psi.shape)).astype(np.float32)
+    del psi
+    w = np.ones(len(pos), np.float32)
+    t_ics = time.time() - t0
+    t0 = time.time()
+    plan = P.make_plan(pos, w, vel, None, grid=(n, n, n), n_threads=threads,
+                       average_density_value=float(len(pos)) / S.BOX ** 3)
+    plan.timings["ics_s"] = t_ics
+    plan.timings["plan_total_s"] = time.time() - t0
+    return plan
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """dram bytes per k_interpolate launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "interp_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def cpu_baseline(plan, threads: int, target_s: float) -> dict:
+    """The CPU oracle in the reference's arithmetic on the host cores: vertex
+    densities over the whole tessellation plus cell-centre interpolation of
+    the benchmark fields on the first x-slabs of sub-box 0, scaled to the
+    full grid."""
+    import copy
+    import oracle as O
+    from dtfe_b200 import _native as N
+    t0 = time.time()
+    d32, d64, _ = O.vertex_density(plan)
+    t_vd = time.time() - t0
+    b0 = plan.boxes[0]
+    per_slab = int(b0.tile_dims[1]) * int(b0.tile_dims[2])
+    # calibrate: one slab, then enough slabs for the target time
+    sub = copy.copy(plan)
+    boxes = (N.Subbox * 1)()
+    boxes[0] = b0
+    sub.boxes = boxes
+    slabs = 1
+    elapsed = 0.0
+    for _ in range(4):
+        boxes[0].tile_dims[0] = slabs
+        t0 = time.time()
+        O.interpolate(sub, d32, d64, FIELDS, mode=O.MODE_REF, nthreads=threads)
+        elapsed = time.time() - t0
+        if elapsed > 0.25 * target_s or slabs >= int(b0.tile_dims[0]):
+            break
+        slabs = min(int(b0.tile_dims[0]), max(slabs * 2, int(slabs * target_s / max(elapsed, 1e-3))))
+    cells = slabs * per_slab
+    G = int(np.prod(plan.grid))
+    t_step = t_vd + elapsed * G / cells
+    return {"value": G / t_step, "unit": "grid samples/s", "cores": threads, "kind": "port",
+            "sample": f"vertex densities of all {plan.n_verts} vertices ({t_vd:.2f} s) + cell-centre "
+                      f"interpolation of {cells} of {G} cells ({elapsed:.2f} s, x-slabs of sub-box 0), "
+                      f"scaled to the full grid",
+            "vertex_density_s": t_vd, "interp_cells_per_s": cells / elapsed}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = host_threads(args.threads)
+    plan = build_workload(args.n, 0, threads)
+    import copy
+    import oracle as O
+    from dtfe_b200 import _native as N
+    G = int(np.prod(plan.grid))
+    b0 = plan.boxes[0]
+    sub = copy.copy(plan)
+    boxes = (N.Subbox * 1)()
+    boxes[0] = b0
+    sub.boxes = boxes
+    per_slab = int(b0.tile_dims[1]) * int(b0.tile_dims[2])
+    slabs = max(1, min(int(b0.tile_dims[0]), 2))
+    boxes[0].tile_dims[0] = slabs
+    cells = slabs * per_slab
+    times = []
+    for it in range(args.warmup + args.steps):
+        t0 = time.time()
+        d32, d64, _ = O.vertex_density(plan)
+        t1 = time.time()
+        O.interpolate(sub, d32, d64, FIELDS, mode=O.MODE_REF, nthreads=threads)
+        t2 = time.time()
+        if it >= args.warmup:
+            times.append((t1 - t0) + (t2 - t1) * G / cells)
+    t_step = float(np.mean(times))
+    value = G / t_step
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "grid samples/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"zeldovich{args.n}: {args.n}^3 particles -> {args.n}^3 grid, cell-centre "
+                               "density+velocity+gradient+div/shear/vort", "grid": [args.n] * 3,
+                   "particles": args.n ** 3},
+        "cpu_baseline": {"value": value, "unit": "grid samples/s", "cores": threads, "kind": "port",
+                         "sample": f"per step: vertex densities of all {plan.n_verts} vertices + "
+                                   f"{cells} of {G} cells, scaled to the full grid"},
+        "e2e": {"value": value, "unit": "grid samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from dtfe_b200.device import DeviceDTFE
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    threads = max(1, host_threads(args.threads) // max(1, world if world > 1 else 1))
+    plan = build_workload(args.n, rank, threads)
+    G = int(np.prod(plan.grid))
+
+    dev = DeviceDTFE(local, 0)
+    dev.load(plan)
+    outs = {f: torch.empty((G, [1, 3, 9, 1, 5, 3][i]), dtype=torch.float32, device=f"cuda:{local}")
+            for i, f in enumerate(FIELDS)}
+    stream = torch.cuda.ExternalStream(dev.stream, device=f"cuda:{local}")
+
+    def step():
+        dev.vertex_density(plan.rho_bar)
+        return dev.interpolate_dev(FIELDS, outs, method=0)
+
+    for _ in range(args.warmup):
+        step()
+    dev.synchronize()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ki0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ki1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    status = None
+    for i in range(args.steps):
+        dev.vertex_density(plan.rho_bar)
+        ki0[i].record(stream)
+        status = dev.interpolate_dev(FIELDS, outs, method=0)
+        ki1[i].record(stream)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    t_total = ev0.elapsed_time(ev1) / 1e3
+    t_interp = float(np.mean([a.elapsed_time(b) for a, b in zip(ki0, ki1)])) / 1e3
+    if world > 1:
+        t = torch.tensor([t_total], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_total = float(t.item())
+        dist.barrier()
+    value = world * G * args.steps / t_total
+    ms_step = 1e3 * t_total / args.steps
+
+    # Monte-Carlo average (8 points per cell): point evaluations/s
+    mc = None
+    if not args.no_mc:
+        for _ in range(2):
+            dev.vertex_density(plan.rho_bar)
+            dev.interpolate_dev(FIELDS, outs, method=2, n_samples=8, seed=3)
+        dev.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            dev.vertex_density(plan.rho_bar)
+            dev.interpolate_dev(FIELDS, outs, method=2, n_samples=8, seed=3)
+        e1.record(stream)
+        e1.synchronize()
+        tm = e0.elapsed_time(e1) / 3e3
+        mc = {"cells_per_s": G / tm, "point_evals_per_s": 9 * G / tm, "ms_per_step": 1e3 * tm,
+              "n_samples": 8, "method": 2}
+
+    # end to end through the C ABI with host buffers (pinned)
+    e2e = None
+    if args.e2e_steps > 0:
+        from copy import copy as _copy
+        hp = _copy(plan)
+
+        def pin(a):
+            if a is None:
+                return None
+            t = torch.empty(a.shape, dtype={np.dtype("float32"): torch.float32,
+                                            np.dtype("int32"): torch.int32}[a.dtype], pin_memory=True)
+            t.numpy()[...] = a
+            return t.numpy()
+        hp.tet_v, hp.tet_n, hp.xyz = pin(plan.tet_v), pin(plan.tet_n), pin(plan.xyz)
+        hp.weight, hp.velocity = pin(plan.weight), pin(plan.velocity)
+        host_out = {f: pin(np.empty((G, [1, 3, 9, 1, 5, 3][i]), np.float32)) for i, f in enumerate(FIELDS)}
+        h2d = (hp.tet_v.nbytes + hp.tet_n.nbytes + hp.xyz.nbytes + hp.weight.nbytes + hp.velocity.nbytes
+               + 4 * (len(hp.xs) + len(hp.ys) + len(hp.zs)))
+        d2h = sum(a.nbytes for a in host_out.values())
+
+        def e2e_step():
+            dev.load(hp)
+            dev.vertex_density(hp.rho_bar)
+            dev.interpolate(FIELDS, method=0, out=host_out)
+        e2e_step()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        dev.synchronize()
+        te = (time.perf_counter() - t0) / args.e2e_steps
+        if world > 1:
+            t = torch.tensor([te], device=f"cuda:{local}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t.item())
+        e2e = {"value": world * G / te, "unit": "grid samples/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * te}
+
+    peak, peak_kind = measured_peak()
+    b_alg = 16 * plan.n_tets + plan.n_verts * (12 + 4 + 12) + 4 * C_OUT * G
+    achieved = b_alg / t_interp / 1e9
+    traffic = profile_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic.get("dram_bytes_per_launch_scaled") if traffic else None,
+                "kernel": "k_interpolate<centre>", "kernel_ms": 1e3 * t_interp,
+                "algorithmic_bytes": int(b_alg), "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(plan, host_threads(args.threads), args.cpu_seconds)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "grid samples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"zeldovich{args.n}: {args.n}^3 Zel'dovich particles (rms 1.0 spacing, "
+                               f"periodic 100 Mpc/h, padding 5) -> {args.n}^3 grid, cell-centre "
+                               "density+velocity+gradient+div/shear/vort per step, vertex densities included",
+                   "grid": list(plan.grid), "particles": args.n ** 3, "vertices": plan.n_verts,
+                   "tetrahedra": plan.n_tets, "subboxes": plan.n_boxes,
+                   "l2": "inputs larger than L2 (tessellation arrays > 126 MB)",
+                   "parallelism": f"dp{world} (independent boxes per GPU)"},
+        "gpu_launches": 4 * args.steps,
+        "clocks": clk,
+        "e2e": e2e,
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "mc": mc,
+        "walk": {k: status[k] for k in ("n_samples_located", "n_walk_steps", "n_exact_tests", "n_ties",
+                                        "n_outside")} if status else None,
+        "host_prep_s": plan.timings,
+    }
+    dev.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <map>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -416,22 +417,30 @@ struct dtfe_gpu_s {
   unsigned long long* counters = nullptr;
   float* out_buf[DTFE_NUM_FIELDS] = {};
   size_t out_cap[DTFE_NUM_FIELDS] = {};
+  std::map<void*, size_t> caps;  // bytes held by each device buffer
 };
 
 namespace {
 
+// Device allocation that keeps a buffer when it is already large enough, so
+// repeated uploads of same-sized inputs do not reallocate.
 template <typename Tp>
-int dev_alloc(Tp** p, size_t count) {
+int dev_alloc(dtfe_handle h, Tp** p, size_t count) {
+  size_t bytes = count * sizeof(Tp);
+  size_t& cap = h->caps[(void*)p];
+  if (*p && cap >= bytes) return DTFE_OK;
   if (*p) {
     cudaFree(*p);
     *p = nullptr;
+    cap = 0;
   }
   if (count == 0) return DTFE_OK;
-  cudaError_t e = cudaMalloc((void**)p, count * sizeof(Tp));
+  cudaError_t e = cudaMalloc((void**)p, bytes);
   if (e != cudaSuccess) {
     *p = nullptr;
     return set_error(DTFE_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e));
   }
+  cap = bytes;
   return DTFE_OK;
 }
 
@@ -502,7 +511,7 @@ int dtfe_gpu_create(const dtfe_config* cfg, dtfe_handle* out) {
     delete h;
     return set_error(DTFE_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
   }
-  int rc = dev_alloc(&h->counters, CNT_N);
+  int rc = dev_alloc(h, &h->counters, CNT_N);
   if (rc) {
     cudaStreamDestroy(h->stream);
     delete h;
@@ -546,11 +555,11 @@ int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n, i
   int rc;
   h->T = n_tets;
   h->V = n_verts;
-  if ((rc = dev_alloc(&h->tet_v, n_tets)) || (rc = dev_alloc(&h->tet_n, n_tets)) ||
-      (rc = dev_alloc(&h->posd, n_verts)) || (rc = dev_alloc(&h->vel4, n_verts)) ||
-      (rc = dev_alloc(&h->w, n_verts)) || (rc = dev_alloc(&h->volsum, n_verts)) ||
-      (rc = dev_alloc(&h->hull, n_verts)) || (rc = dev_alloc(&h->vtx_tet, n_verts)) ||
-      (rc = dev_alloc(&h->scal, (size_t)n_verts * h->S)))
+  if ((rc = dev_alloc(h, &h->tet_v, n_tets)) || (rc = dev_alloc(h, &h->tet_n, n_tets)) ||
+      (rc = dev_alloc(h, &h->posd, n_verts)) || (rc = dev_alloc(h, &h->vel4, n_verts)) ||
+      (rc = dev_alloc(h, &h->w, n_verts)) || (rc = dev_alloc(h, &h->volsum, n_verts)) ||
+      (rc = dev_alloc(h, &h->hull, n_verts)) || (rc = dev_alloc(h, &h->vtx_tet, n_verts)) ||
+      (rc = dev_alloc(h, &h->scal, (size_t)n_verts * h->S)))
     return rc;
   cudaStream_t st = h->stream;
   if (n_tets) {
@@ -616,10 +625,10 @@ int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* box
   tprefix[n_boxes] = cells;
   vprefix[n_boxes] = boxes[n_boxes - 1].vert_offset + boxes[n_boxes - 1].n_verts;
   int rc;
-  if ((rc = dev_alloc(&h->boxes, n_boxes)) || (rc = dev_alloc(&h->tile_prefix, n_boxes + 1)) ||
-      (rc = dev_alloc(&h->vprefix, n_boxes + 1)) || (rc = dev_alloc(&h->bin_offset, n_boxes)) ||
-      (rc = dev_alloc(&h->bins, cells)) || (rc = dev_alloc(&h->xs, n_xs)) ||
-      (rc = dev_alloc(&h->ys, n_ys)) || (rc = dev_alloc(&h->zs, n_zs)))
+  if ((rc = dev_alloc(h, &h->boxes, n_boxes)) || (rc = dev_alloc(h, &h->tile_prefix, n_boxes + 1)) ||
+      (rc = dev_alloc(h, &h->vprefix, n_boxes + 1)) || (rc = dev_alloc(h, &h->bin_offset, n_boxes)) ||
+      (rc = dev_alloc(h, &h->bins, cells)) || (rc = dev_alloc(h, &h->xs, n_xs)) ||
+      (rc = dev_alloc(h, &h->ys, n_ys)) || (rc = dev_alloc(h, &h->zs, n_zs)))
     return rc;
   cudaStream_t st = h->stream;
   DTFE_CUDA_TRY(cudaMemcpyAsync(h->boxes, boxes, sizeof(dtfe_subbox) * n_boxes, cudaMemcpyHostToDevice, st));
@@ -713,7 +722,7 @@ static int interpolate_impl(dtfe_handle h, const dtfe_interp_opts* o, float* con
               e[1] = (float)((i2 + 0.5) * (double)dx[1] / n - (double)dx[1] / 2.);
             }
       }
-      if ((rc = dev_alloc(&h->eq_off, eq.size()))) return rc;
+      if ((rc = dev_alloc(h, &h->eq_off, eq.size()))) return rc;
       DTFE_CUDA_TRY(cudaMemcpyAsync(h->eq_off, eq.data(), sizeof(float) * eq.size(), cudaMemcpyHostToDevice, st));
       DTFE_CUDA_TRY(cudaStreamSynchronize(st));
       h->eq_nn = NN;
@@ -785,7 +794,7 @@ int dtfe_gpu_interpolate(dtfe_handle h, const dtfe_interp_opts* opts, float* con
     if (!out[s]) return set_error(DTFE_ERR_ARG, "missing output buffer");
     size_t need = (size_t)G * field_components(s, h->S);
     if (h->out_cap[s] < need) {
-      int rc = dev_alloc(&h->out_buf[s], need);
+      int rc = dev_alloc(h, &h->out_buf[s], need);
       if (rc) return rc;
       h->out_cap[s] = need;
     }

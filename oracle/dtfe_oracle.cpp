@@ -318,28 +318,38 @@ extern "C" {
 // vertexDensity (triangulation.cpp:200-279): rho_v = w_v*(D+1)/(rho_bar*sum V),
 // 0 when any incident cell is infinite.  Volumes are the double determinant/6
 // (Tetrahedron_3::volume, triangulation_miscellaneous.cc:205-213), summed in
-// double in ascending tetrahedron order.  dens32: mode-0 result, float
+// double in ascending tetrahedron order within each sub-box.  dens32: mode-0 result, float
 // factor (D+1)/rho_bar (:220) times the weight, divided by the double sum;
 // dens64: all-double result.  Either output may be NULL.
 int oracle_vertex_density(int64_t T, const int32_t* tv, const int32_t* tn, int64_t V,
                           const float* xyz, const float* w, double rho_bar, float* dens32,
-                          double* dens64, double* volsum_out) {
+                          double* dens64, double* volsum_out, int K, const dtfe_subbox* boxes,
+                          int nthreads) {
   std::vector<double> vol(V, 0.0);
   std::vector<char> hull(V, 0);
-  for (int64_t t = 0; t < T; ++t) {
-    double X[4][3];
-    for (int a = 0; a < 4; ++a)
-      for (int k = 0; k < 3; ++k) X[a][k] = (double)xyz[3 * (int64_t)tv[4 * t + a] + k];
-    double v6 = dtfe::orient_det(X[0], X[1], X[2], X[3]);
-    double vt = v6 / 6.0;
-    for (int a = 0; a < 4; ++a) vol[tv[4 * t + a]] += vt;
-    for (int i = 0; i < 4; ++i)
-      if (tn[4 * t + i] < 0)
-        for (int a = 0; a < 4; ++a)
-          if (a != i) hull[tv[4 * t + a]] = 1;
+  // Sub-boxes own disjoint vertex and tetrahedron ranges, so they run in
+  // parallel (one host thread each, as the reference's OpenMP threads do).
+  const int nb = (K > 0 && boxes) ? K : 1;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads > 0 ? nthreads : 1)
+  for (int b = 0; b < nb; ++b) {
+    int64_t lo = (K > 0 && boxes) ? boxes[b].tet_offset : 0;
+    int64_t hi = (K > 0 && boxes) ? boxes[b].tet_offset + boxes[b].n_tets : T;
+    for (int64_t t = lo; t < hi; ++t) {
+      double X[4][3];
+      for (int a = 0; a < 4; ++a)
+        for (int k = 0; k < 3; ++k) X[a][k] = (double)xyz[3 * (int64_t)tv[4 * t + a] + k];
+      double v6 = dtfe::orient_det(X[0], X[1], X[2], X[3]);
+      double vt = v6 / 6.0;
+      for (int a = 0; a < 4; ++a) vol[tv[4 * t + a]] += vt;
+      for (int i = 0; i < 4; ++i)
+        if (tn[4 * t + i] < 0)
+          for (int a = 0; a < 4; ++a)
+            if (a != i) hull[tv[4 * t + a]] = 1;
+    }
   }
   float rb = (float)rho_bar;
   float factor = (float)(4.0 / (double)rb);
+#pragma omp parallel for schedule(static) num_threads(nthreads > 0 ? nthreads : 1)
   for (int64_t v = 0; v < V; ++v) {
     bool zero = hull[v] || vol[v] == 0.0;
     if (dens32) dens32[v] = zero ? 0.f : (float)((double)(w[v] * factor) / vol[v]);
@@ -410,11 +420,16 @@ int oracle_interpolate(int64_t T, const int32_t* tv, const int32_t* tn, int64_t 
             eq[3 * idx + 1] = (float)((i2 + 0.5) * (double)dx[1] / nroot - (double)dx[1] / 2.);
           }
     }
-#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads > 0 ? nthreads : 1) reduction(+ : fails)
-    for (int i = 0; i < B.tile_dims[0]; ++i) {
-      int64_t hint = lo;
+    // Pencils (i, j) run in parallel; each thread carries its walk hint from
+    // one pencil to the next (the reference carries it along its raster).
+#pragma omp parallel num_threads(nthreads > 0 ? nthreads : 1) reduction(+ : fails)
+    {
+      int64_t row_hint = lo;
       std::vector<double> stdv(3 * (size_t)std::max(NN, 1));
-      for (int j = 0; j < B.tile_dims[1]; ++j)
+#pragma omp for collapse(2) schedule(dynamic, 4)
+    for (int i = 0; i < B.tile_dims[0]; ++i) {
+      for (int j = 0; j < B.tile_dims[1]; ++j) {
+        int64_t hint = row_hint;
         for (int k = 0; k < B.tile_dims[2]; ++k) {
           const float x = xs[B.coord_offset[0] + i], y = ys[B.coord_offset[1] + j],
                       z = zs[B.coord_offset[2] + k];
@@ -423,7 +438,10 @@ int oracle_interpolate(int64_t T, const int32_t* tv, const int32_t* tn, int64_t 
           double pc[3] = {(double)x, (double)y, (double)z};
           int64_t tc = locate(g, pc, hint, lo, hi);
           if (tc == -2) { ++fails; tc = -1; }
-          if (tc >= 0) hint = tc;
+          if (tc >= 0) {
+            hint = tc;
+            if (k == 0) row_hint = tc;
+          }
           if (loc) loc[cell] = tc;
           // accumulators: float in mode 0, double in mode 1
           float fD = 0.f, fV[3] = {0, 0, 0}, fG[9] = {0}, fS[DTFE_MAX_SCALARS] = {0},
@@ -541,6 +559,8 @@ int oracle_interpolate(int64_t T, const int32_t* tv, const int32_t* tn, int64_t 
             for (int q = 0; q < 3 * S; ++q)
               out[DTFE_SCALAR_GRADIENT][(int64_t)3 * S * cell + q] = SGg[q];
         }
+      }
+    }
     }
   }
   if (n_fail) *n_fail = fails;

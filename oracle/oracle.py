@@ -30,7 +30,8 @@ def lib() -> C.CDLL:
         path = build.build_oracle()
         L = C.CDLL(path)
         vp = C.c_void_p
-        L.oracle_vertex_density.argtypes = [C.c_int64, vp, vp, C.c_int64, vp, vp, C.c_double, vp, vp, vp]
+        L.oracle_vertex_density.argtypes = [C.c_int64, vp, vp, C.c_int64, vp, vp, C.c_double, vp, vp, vp,
+                                            C.c_int, vp, C.c_int]
         L.oracle_locate.argtypes = [C.c_int64, vp, vp, vp, C.c_int64, C.c_int64, C.c_int64, vp, vp]
         L.oracle_interpolate.argtypes = [C.c_int64, vp, vp, C.c_int64, vp, vp, vp, C.c_int, vp, vp, C.c_int,
                                          vp, vp, vp, vp, vp, C.POINTER(N.InterpOpts), C.c_int,
@@ -39,8 +40,9 @@ def lib() -> C.CDLL:
     return _lib
 
 
-def vertex_density(plan, rho_bar: float | None = None):
-    """(dens32 float32 (V,), dens64 float64 (V,), volsum float64 (V,))."""
+def vertex_density(plan, rho_bar: float | None = None, nthreads: int = 0):
+    """(dens32 float32 (V,), dens64 float64 (V,), volsum float64 (V,)).
+    nthreads 0 = all host threads (parallel over sub-boxes)."""
     rb = plan.rho_bar if rho_bar is None else rho_bar
     V = plan.n_verts
     d32 = np.empty(V, np.float32)
@@ -48,7 +50,8 @@ def vertex_density(plan, rho_bar: float | None = None):
     vs = np.empty(V, np.float64)
     lib().oracle_vertex_density(plan.n_tets, plan.tet_v.ctypes.data, plan.tet_n.ctypes.data, V,
                                 plan.xyz.ctypes.data, plan.weight.ctypes.data, rb,
-                                d32.ctypes.data, d64.ctypes.data, vs.ctypes.data)
+                                d32.ctypes.data, d64.ctypes.data, vs.ctypes.data,
+                                plan.n_boxes, C.addressof(plan.boxes), nthreads or (os.cpu_count() or 1))
     return d32, d64, vs
 
 

@@ -58,6 +58,7 @@ class Config(C.Structure):
 # status codes (include/dtfe_gpu.h)
 OK, ERR_ARG, ERR_CUDA, ERR_ALLOC, ERR_STATE, ERR_WALK, ERR_DEGENERATE, ERR_NO_DEVICE, ERR_TOO_LARGE = range(9)
 NUM_FIELDS = 9
+NOALLOC_MAX_VERTS = 1 << 20
 FIELD_SLOTS = {
     "density": 0, "velocity": 1, "velocity_gradient": 2, "velocity_divergence": 3,
     "velocity_shear": 4, "velocity_vorticity": 5, "velocity_std": 6,
@@ -136,6 +137,8 @@ def gpu() -> C.CDLL:
         lib.dtfe_gpu_stream.argtypes = [H]
         lib.dtfe_gpu_stream.restype = C.c_void_p
         lib.dtfe_gpu_synchronize.argtypes = [H]
+        lib.dtfe_vertex_density_noalloc.argtypes = [vp, vp, C.c_int64, vp, vp, C.c_int64, C.c_double, vp, vp]
+        lib.dtfe_vertex_density_noalloc.restype = C.c_int
         _gpu = lib
     return _gpu
 

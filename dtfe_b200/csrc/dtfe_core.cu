@@ -490,6 +490,9 @@ extern "C" {
 
 const char* dtfe_last_error(void) { return g_last_error.c_str(); }
 
+// Records an error message for dtfe_last_error() from other translation units.
+int dtfe_internal_set_error(int code, const char* msg) { return set_error(code, msg ? msg : ""); }
+
 int dtfe_gpu_create(const dtfe_config* cfg, dtfe_handle* out) {
   if (!out) return set_error(DTFE_ERR_ARG, "null output handle");
   *out = nullptr;

@@ -25,10 +25,10 @@
 
 #if defined(__CUDACC__)
 #define DTFE_HD __host__ __device__ __forceinline__
-#define DTFE_HD_NOINLINE __host__ __device__ __noinline__
+#define DTFE_HD_NOINLINE static __host__ __device__ __noinline__
 #else
 #define DTFE_HD inline
-#define DTFE_HD_NOINLINE inline
+#define DTFE_HD_NOINLINE static inline
 #endif
 
 #if !defined(__CUDA_ARCH__)

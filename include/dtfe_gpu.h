@@ -170,6 +170,26 @@ int dtfe_gpu_download_vertex_density(dtfe_handle h, float* dens);
 int dtfe_gpu_locate_points(dtfe_handle h, int64_t np, const double* pts, int32_t start,
                            int32_t* out);
 
+/* Vertex densities without any device allocation, for callers that cannot
+ * let a library allocate: host applications that hand out all device memory
+ * from their own fixed-budget pool, or latency-critical loops where an
+ * allocation and the synchronisation it may imply are unacceptable.  No
+ * counterpart in the reference (it has no GPU path).
+ * Inputs and output are DEVICE pointers on the current device: tet_v/tet_n
+ * (4 int32 per tetrahedron, 16-byte aligned), xyz (3 floats per vertex), w
+ * (V floats); dens receives V floats, the same values as
+ * dtfe_gpu_vertex_density.  Scratch is a static device array for at most
+ * DTFE_NOALLOC_MAX_VERTS vertices (12 MiB, resident on every device that
+ * loads the library until exit); larger inputs return DTFE_ERR_TOO_LARGE.
+ * All calls share that scratch: calls that overlap on the GPU race.  The
+ * first call on a device looks up the scratch address; make it before any
+ * stream capture.  stream: a cudaStream_t (NULL = default stream); the call
+ * returns after the stream has finished it. */
+#define DTFE_NOALLOC_MAX_VERTS (1 << 20)
+int dtfe_vertex_density_noalloc(const int32_t* tet_v_dev, const int32_t* tet_n_dev, int64_t n_tets,
+                                const float* xyz_dev, const float* w_dev, int64_t n_verts,
+                                double rho_bar, float* dens_dev, void* stream);
+
 /* Stream the handle's work is ordered on (a cudaStream_t). */
 void* dtfe_gpu_stream(dtfe_handle h);
 /* Block until the handle's stream is idle. */

@@ -1,18 +1,22 @@
 // DTFE interpolation path on B200 (sm_100a): kernels and the C ABI of
 // include/dtfe_gpu.h.
 //
-// Pipeline per call (all on the handle's stream):
-//   k_volume_scatter   one thread per tetrahedron: signed volume in FP64,
-//                      scattered to its four vertices (FP64 reduction),
-//                      hull-face marks, lowest incident tetrahedron per vertex
+// Pipeline (all on the handle's stream):
+//   upload             tessellation and vertex data; k_hull_marks flags the
+//                      vertices of hull faces once (a topological property of
+//                      the tessellation: the reference's infinite cells)
+//   k_volume_bins      per step, one thread per tetrahedron: signed volume in
+//                      FP64 scattered to its four vertices and, per grid cell,
+//                      the lowest tetrahedron whose centroid lies in the cell
+//                      (the walk seeds).  Both reductions are first combined
+//                      in shared-memory hash tables per block (tetrahedra are
+//                      Morton-sorted, so a block touches few vertices and
+//                      cells) and then flushed with one global atomic each
 //   k_vertex_density   rho_v = w (D+1)/(rho_bar sum V), 0 on the hull
 //                      (vertexDensity, triangulation.cpp:200-279)
-//   k_seed_bins        lowest vertex id per grid cell of each tile: the walk
-//                      seed of a sample is an incident tetrahedron of a vertex
-//                      lying in the sample's own cell
-//   k_interpolate      one thread per grid cell: walk to the cell centre,
-//                      evaluate (or average over n points, each walked from
-//                      the centre's tetrahedron as in
+//   k_interpolate      one thread per grid cell: walk from the cell's seed to
+//                      the cell centre, evaluate (or average over n points,
+//                      each walked from the centre's tetrahedron as in
 //                      averaged_interpolation_2.cc:123,145), derive
 //                      divergence/shear/vorticity in the epilogue, write every
 //                      requested field once.
@@ -57,41 +61,17 @@ __global__ void k_pack_xyz(int64_t n, const float* __restrict__ xyz, float4* __r
   if (i < n) out[i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], wval);
 }
 
-__global__ void k_volume_scatter(int64_t T, const int4* __restrict__ tet_v, const int4* __restrict__ tet_n,
-                                 const float4* __restrict__ posd, double* __restrict__ volsum,
-                                 int* __restrict__ hull, int* __restrict__ vtx_tet) {
+__global__ void k_hull_marks(int64_t T, const int4* __restrict__ tet_v, const int4* __restrict__ tet_n,
+                             int* __restrict__ hull) {
   int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= T) return;
-  int4 v = __ldg(&tet_v[t]);
   int4 n = __ldg(&tet_n[t]);
-  double X[4][3];
-  load_pos(posd, v.x, X[0]);
-  load_pos(posd, v.y, X[1]);
-  load_pos(posd, v.z, X[2]);
-  load_pos(posd, v.w, X[3]);
-  double vt = orient_det(X[0], X[1], X[2], X[3]) / 6.0;
-  atomicAdd(&volsum[v.x], vt);
-  atomicAdd(&volsum[v.y], vt);
-  atomicAdd(&volsum[v.z], vt);
-  atomicAdd(&volsum[v.w], vt);
-  int ti = (int)t;
-  atomicMin(&vtx_tet[v.x], ti);
-  atomicMin(&vtx_tet[v.y], ti);
-  atomicMin(&vtx_tet[v.z], ti);
-  atomicMin(&vtx_tet[v.w], ti);
+  if (n.x >= 0 && n.y >= 0 && n.z >= 0 && n.w >= 0) return;
+  int4 v = __ldg(&tet_v[t]);
   if (n.x < 0) { hull[v.y] = 1; hull[v.z] = 1; hull[v.w] = 1; }
   if (n.y < 0) { hull[v.x] = 1; hull[v.z] = 1; hull[v.w] = 1; }
   if (n.z < 0) { hull[v.x] = 1; hull[v.y] = 1; hull[v.w] = 1; }
   if (n.w < 0) { hull[v.x] = 1; hull[v.y] = 1; hull[v.z] = 1; }
-}
-
-__global__ void k_vertex_density(int64_t V, const float* __restrict__ w, const double* __restrict__ volsum,
-                                 const int* __restrict__ hull, float factor, float4* __restrict__ posd) {
-  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= V) return;
-  double vol = volsum[i];
-  float d = (hull[i] || vol == 0.0) ? 0.f : (float)((double)(w[i] * factor) / vol);
-  posd[i].w = d;
 }
 
 __device__ __forceinline__ int find_box(const int64_t* __restrict__ prefix, int K, int64_t s) {
@@ -104,27 +84,185 @@ __device__ __forceinline__ int find_box(const int64_t* __restrict__ prefix, int 
   return lo;
 }
 
-__global__ void k_seed_bins(int64_t V, const float4* __restrict__ posd, const int* __restrict__ vtx_tet,
-                            const dtfe_subbox* __restrict__ boxes, const int64_t* __restrict__ vprefix,
-                            const int64_t* __restrict__ bin_offset, int K, int* __restrict__ bins) {
+// ---- vertex -> tetrahedron incidence (built once per upload) ------------
+__global__ void k_degree(int64_t T, const int4* __restrict__ tet_v, int* __restrict__ deg) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= T) return;
+  int4 v = __ldg(&tet_v[t]);
+  atomicAdd(&deg[v.x], 1);
+  atomicAdd(&deg[v.y], 1);
+  atomicAdd(&deg[v.z], 1);
+  atomicAdd(&deg[v.w], 1);
+}
+
+// Exclusive scan of n ints into int64 offsets (out has n+1 entries):
+// per-block scans of kScanBlock items, a single-block scan of the block
+// totals, then the block offsets are added.
+constexpr int kScanBlock = 1024;
+__global__ void k_scan_blocks(int64_t n, const int* __restrict__ in, int64_t* __restrict__ out,
+                              int64_t* __restrict__ block_sums) {
+  __shared__ int64_t sh[kScanBlock];
+  int64_t i = blockIdx.x * (int64_t)kScanBlock + threadIdx.x;
+  int64_t x = i < n ? (int64_t)in[i] : 0;
+  sh[threadIdx.x] = x;
+  __syncthreads();
+  for (int off = 1; off < kScanBlock; off <<= 1) {
+    int64_t y = threadIdx.x >= off ? sh[threadIdx.x - off] : 0;
+    __syncthreads();
+    sh[threadIdx.x] += y;
+    __syncthreads();
+  }
+  if (i < n) out[i] = sh[threadIdx.x] - x;  // exclusive
+  if (threadIdx.x == kScanBlock - 1) block_sums[blockIdx.x] = sh[threadIdx.x];
+}
+
+__global__ void k_scan_totals(int64_t nb, int64_t* __restrict__ block_sums, int64_t* __restrict__ total) {
+  // one block: sequential chunks, each scanned in shared memory
+  __shared__ int64_t sh[kScanBlock];
+  int64_t carry = 0;
+  for (int64_t base = 0; base < nb; base += kScanBlock) {
+    int64_t i = base + threadIdx.x;
+    int64_t x = i < nb ? block_sums[i] : 0;
+    sh[threadIdx.x] = x;
+    __syncthreads();
+    for (int off = 1; off < kScanBlock; off <<= 1) {
+      int64_t y = threadIdx.x >= off ? sh[threadIdx.x - off] : 0;
+      __syncthreads();
+      sh[threadIdx.x] += y;
+      __syncthreads();
+    }
+    if (i < nb) block_sums[i] = carry + sh[threadIdx.x] - x;
+    int64_t tot = sh[kScanBlock - 1];
+    __syncthreads();
+    carry += tot;
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void k_scan_add(int64_t n, int64_t* __restrict__ out, const int64_t* __restrict__ block_sums) {
+  int64_t i = blockIdx.x * (int64_t)kScanBlock + threadIdx.x;
+  if (i < n) out[i] += block_sums[blockIdx.x];
+}
+
+__global__ void k_fill_incidence(int64_t T, const int4* __restrict__ tet_v, const int64_t* __restrict__ off,
+                                 int* __restrict__ cursor, int* __restrict__ inc) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= T) return;
+  int4 q = __ldg(&tet_v[t]);
+  int v[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    int pos = atomicAdd(&cursor[v[a]], 1);
+    inc[off[v[a]] + pos] = (int)t;
+  }
+}
+
+// Ascending order inside every vertex's list: the FP64 volume sum then runs
+// in a fixed order (ascending tetrahedron id), independent of the atomics
+// that filled the lists.
+__global__ void k_sort_incidence(int64_t V, const int64_t* __restrict__ off, int* __restrict__ inc) {
   int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (v >= V) return;
-  int t = vtx_tet[v];
-  if (t < 0 || t >= kEmptyBin) return;  // not a vertex of any tetrahedron
-  int b = find_box(vprefix, K, v);
-  const dtfe_subbox& B = boxes[b];
-  float4 q = posd[v];
-  float c[3] = {q.x, q.y, q.z};
-  int idx[3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    float f = floorf((c[a] - B.lo[a]) / B.dx[a]);
-    if (!(f >= 0.f && f < (float)B.tile_dims[a])) return;
-    idx[a] = (int)f;
+  int64_t a = off[v], b = off[v + 1];
+  for (int64_t i = a + 1; i < b; ++i) {
+    int x = inc[i];
+    int64_t j = i - 1;
+    while (j >= a && inc[j] > x) {
+      inc[j + 1] = inc[j];
+      --j;
+    }
+    inc[j + 1] = x;
   }
-  int64_t local = ((int64_t)idx[0] * B.tile_dims[1] + idx[1]) * B.tile_dims[2] + idx[2];
-  atomicMin(&bins[bin_offset[b] + local], (int)v);
 }
+
+// ---- per step ------------------------------------------------------------
+constexpr int kVolBlock = 256;
+constexpr int kBinSlots = 512;  // >= 2 x kVolBlock: the table never fills
+
+__device__ __forceinline__ unsigned slot_hash(int key, unsigned mask) {
+  return ((unsigned)key * 2654435761u) & mask;
+}
+
+// Signed volume of every tetrahedron (FP64, streamed out once) and, when
+// DO_BINS, the walk seeds: per grid cell the lowest tetrahedron whose
+// centroid lies in it, combined per block in a shared-memory hash table
+// (tetrahedra are Morton-sorted, so a block covers few cells) and flushed
+// with one global atomicMin per cell.
+template <bool DO_BINS>
+__global__ void __launch_bounds__(kVolBlock) k_tet_volume_bins(
+    int64_t T, const int4* __restrict__ tet_v, const float4* __restrict__ posd, double* __restrict__ vol,
+    const dtfe_subbox* __restrict__ boxes, const int64_t* __restrict__ tprefix,
+    const int64_t* __restrict__ bin_offset, int K, int* __restrict__ bins) {
+  __shared__ int s_bkey[DO_BINS ? kBinSlots : 1];
+  __shared__ int s_bval[DO_BINS ? kBinSlots : 1];
+  if (DO_BINS) {
+    for (int i = threadIdx.x; i < kBinSlots; i += blockDim.x) { s_bkey[i] = -1; s_bval[i] = 0x7FFFFFFF; }
+    __syncthreads();
+  }
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t < T) {
+    int4 q = __ldg(&tet_v[t]);
+    int v[4] = {q.x, q.y, q.z, q.w};
+    float X[4][3];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) load_posf(posd, v[a], X[a]);
+    double D[4][3];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) D[a][c] = (double)X[a][c];
+    vol[t] = orient_det(D[0], D[1], D[2], D[3]) / 6.0;
+    if (DO_BINS) {
+      const int b = find_box(tprefix, K, t);
+      const dtfe_subbox& B = boxes[b];
+      int idx[3];
+      bool inside = true;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float cen = 0.25f * ((X[0][c] + X[1][c]) + (X[2][c] + X[3][c]));
+        float f = floorf((cen - B.lo[c]) / B.dx[c]);
+        inside = inside && (f >= 0.f && f < (float)B.tile_dims[c]);
+        idx[c] = inside ? (int)f : 0;
+      }
+      if (inside) {
+        int key = (int)(__ldg(&bin_offset[b]) +
+                        ((int64_t)idx[0] * B.tile_dims[1] + idx[1]) * B.tile_dims[2] + idx[2]);
+        unsigned h = slot_hash(key, kBinSlots - 1);
+        for (;;) {
+          int k = atomicCAS(&s_bkey[h], -1, key);
+          if (k == -1 || k == key) { atomicMin(&s_bval[h], (int)t); break; }
+          h = (h + 1) & (kBinSlots - 1);
+        }
+      }
+    }
+  }
+  if (DO_BINS) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < kBinSlots; i += blockDim.x)
+      if (s_bkey[i] >= 0) atomicMin(&bins[s_bkey[i]], s_bval[i]);
+  }
+}
+
+// rho_v = (w * factor) / sum of incident volumes, summed in ascending
+// tetrahedron order; 0 on the hull or without incident tetrahedra.
+__global__ void k_vertex_density(int64_t V, const float* __restrict__ w, const double* __restrict__ vol,
+                                 const int64_t* __restrict__ off, const int* __restrict__ inc,
+                                 const int* __restrict__ hull, float factor, float4* __restrict__ posd) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= V) return;
+  double sum = 0.0;
+  for (int64_t q = off[i], e = off[i + 1]; q < e; ++q) sum += __ldg(&vol[__ldg(&inc[q])]);
+  float d = (hull[i] || sum == 0.0) ? 0.f : (float)((double)(w[i] * factor) / sum);
+  posd[i].w = d;
+}
+
+// Offsets of the 26 neighbouring cells, nearest first (faces, edges, corners).
+__constant__ signed char c_nbr[26][3] = {
+    {0, 0, -1}, {0, 0, 1}, {0, -1, 0}, {0, 1, 0}, {-1, 0, 0}, {1, 0, 0},
+    {0, -1, -1}, {0, -1, 1}, {0, 1, -1}, {0, 1, 1}, {-1, 0, -1}, {-1, 0, 1},
+    {1, 0, -1}, {1, 0, 1}, {-1, -1, 0}, {-1, 1, 0}, {1, -1, 0}, {1, 1, 0},
+    {-1, -1, -1}, {-1, -1, 1}, {-1, 1, -1}, {-1, 1, 1}, {1, -1, -1}, {1, -1, 1},
+    {1, 1, -1}, {1, 1, 1}};
 
 struct InterpParams {
   const int4* tet_v;
@@ -132,7 +270,6 @@ struct InterpParams {
   const float4* posd;
   const float4* vel4;
   const float* scal;
-  const int* vtx_tet;
   const int* bins;
   const dtfe_subbox* boxes;
   const int64_t* tile_prefix;
@@ -155,8 +292,37 @@ struct InterpParams {
 
 __device__ __forceinline__ bool has_field(uint32_t f, int slot) { return (f >> slot) & 1u; }
 
+// Writes one C-component field of a warp's 32 cells.  When the cells are
+// consecutive in the grid (the usual case: k is the fastest index) the values
+// go through shared memory and leave as contiguous 16-byte stores; otherwise
+// each lane stores its own.
+template <int C>
+__device__ __forceinline__ void store_field(float* __restrict__ out, int64_t cell, bool valid,
+                                            const float* val, bool contig, int64_t c0, float* stage) {
+  const int lane = threadIdx.x & 31;
+  if (contig) {
+#pragma unroll
+    for (int c = 0; c < C; ++c) stage[lane * C + c] = val[c];
+    __syncwarp();
+    float4* dst = reinterpret_cast<float4*>(out + c0 * C);
+    const float4* src = reinterpret_cast<const float4*>(stage);
+#pragma unroll
+    for (int q = lane; q < 8 * C; q += 32) dst[q] = src[q];
+    __syncwarp();
+  } else if (valid) {
+#pragma unroll
+    for (int c = 0; c < C; ++c) out[cell * C + c] = val[c];
+  }
+}
+
+constexpr int kInterpBlock = 256;
+
 template <int METHOD, int S>
-__global__ void __launch_bounds__(256) k_interpolate(InterpParams P) {
+__global__ void __launch_bounds__(kInterpBlock) k_interpolate(InterpParams P) {
+  constexpr int CMAX = (3 * S > 9) ? 3 * S : 9;
+  __shared__ __align__(16) float s_stage[kInterpBlock / 32][32 * CMAX];
+  float* stage = s_stage[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
   const uint32_t F = P.fields;
   const bool want_grad = has_field(F, DTFE_VELOCITY_GRADIENT) || has_field(F, DTFE_VELOCITY_DIVERGENCE) ||
                          has_field(F, DTFE_VELOCITY_SHEAR) || has_field(F, DTFE_VELOCITY_VORTICITY);
@@ -168,201 +334,193 @@ __global__ void __launch_bounds__(256) k_interpolate(InterpParams P) {
   WalkStats st{0, 0, 0};
   unsigned n_loc = 0, n_out = 0, n_fail = 0;
 
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < P.n_total; s += stride) {
-    const int b = find_box(P.tile_prefix, P.K, s);
-    const dtfe_subbox& B = P.boxes[b];
-    const int64_t local = s - __ldg(&P.tile_prefix[b]);
-    const int nz = B.tile_dims[2], ny = B.tile_dims[1];
-    const int k = (int)(local % nz);
-    const int j = (int)((local / nz) % ny);
-    const int i = (int)(local / ((int64_t)nz * ny));
-    const float x = __ldg(&P.xs[B.coord_offset[0] + i]);
-    const float y = __ldg(&P.ys[B.coord_offset[1] + j]);
-    const float z = __ldg(&P.zs[B.coord_offset[2] + k]);
-    const int64_t cell = ((int64_t)(B.tile_origin[0] + i) * P.G1 + (B.tile_origin[1] + j)) * P.G2 +
-                         (B.tile_origin[2] + k);
-    // seed: a vertex in this cell, else in a neighbouring cell along z/y/x
-    const int* bins = P.bins + __ldg(&P.bin_offset[b]);
-    int sv = __ldg(&bins[local]);
-    if (sv >= kEmptyBin) {
-      const int64_t cand[6] = {k > 0 ? local - 1 : -1, k + 1 < nz ? local + 1 : -1,
-                               j > 0 ? local - nz : -1, j + 1 < ny ? local + nz : -1,
-                               i > 0 ? local - (int64_t)nz * ny : -1,
-                               i + 1 < B.tile_dims[0] ? local + (int64_t)nz * ny : -1};
-#pragma unroll
-      for (int c = 0; c < 6; ++c)
-        if (sv >= kEmptyBin && cand[c] >= 0) sv = __ldg(&bins[cand[c]]);
-    }
-    int t0 = sv < kEmptyBin ? __ldg(&P.vtx_tet[sv]) : (int)B.tet_offset;
-    if (t0 < B.tet_offset || t0 >= B.tet_offset + B.n_tets) t0 = (int)B.tet_offset;
-
-    const double pc[3] = {(double)x, (double)y, (double)z};
-    int v[4];
-    double X[4][3];
-    int tc = walk_locate(P.tet_v, P.tet_n, P.posd, pc, t0, P.max_steps, v, X, st);
-    ++n_loc;
-    if (tc == kWalkFail) { ++n_fail; tc = kOutside; }
-
+  const int64_t warp_stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t warp_base0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane;
+  for (int64_t base = warp_base0; base < P.n_total; base += warp_stride) {
+    const int64_t s = base + lane;
+    const bool valid = s < P.n_total;
+    int64_t cell = -1;
     float aD = 0.f, aV[3] = {0.f, 0.f, 0.f}, aG[9], aS[S > 0 ? S : 1], aSG[S > 0 ? 3 * S : 1];
+    float sdev = 0.f;
 #pragma unroll
     for (int c = 0; c < 9; ++c) aG[c] = 0.f;
 #pragma unroll
     for (int q = 0; q < (S > 0 ? S : 1); ++q) aS[q] = 0.f;
 #pragma unroll
     for (int q = 0; q < (S > 0 ? 3 * S : 1); ++q) aSG[q] = 0.f;
-    float stdacc[3] = {0.f, 0.f, 0.f};
 
-    if (METHOD == DTFE_METHOD_CENTRE) {
-      if (tc >= 0) {
-        CellOut e;
-        cell_eval<S>(v, X, pc, P.posd, P.vel4, P.scal, want_dens, want_vel, want_sc, fix, e);
-        aD = e.dens;
+    if (valid) {
+      const int b = find_box(P.tile_prefix, P.K, s);
+      const dtfe_subbox& B = P.boxes[b];
+      const int64_t local = s - __ldg(&P.tile_prefix[b]);
+      const int nz = B.tile_dims[2], ny = B.tile_dims[1];
+      const int k = (int)(local % nz);
+      const int j = (int)((local / nz) % ny);
+      const int i = (int)(local / ((int64_t)nz * ny));
+      const float x = __ldg(&P.xs[B.coord_offset[0] + i]);
+      const float y = __ldg(&P.ys[B.coord_offset[1] + j]);
+      const float z = __ldg(&P.zs[B.coord_offset[2] + k]);
+      cell = ((int64_t)(B.tile_origin[0] + i) * P.G1 + (B.tile_origin[1] + j)) * P.G2 + (B.tile_origin[2] + k);
+      // seed: the lowest tetrahedron whose centroid lies in this cell, else in
+      // the nearest cell of the surrounding 3x3x3 block that has one
+      const int* bins = P.bins + __ldg(&P.bin_offset[b]);
+      int t0 = __ldg(&bins[local]);
+      if (t0 >= kEmptyBin) {
+        const int nx = B.tile_dims[0];
+        for (int r = 0; r < 26 && t0 >= kEmptyBin; ++r) {
+          const int ii = i + c_nbr[r][0], jj = j + c_nbr[r][1], kk = k + c_nbr[r][2];
+          if (ii < 0 || jj < 0 || kk < 0 || ii >= nx || jj >= ny || kk >= nz) continue;
+          t0 = __ldg(&bins[((int64_t)ii * ny + jj) * nz + kk]);
+        }
+      }
+      if (t0 < B.tet_offset || t0 >= B.tet_offset + B.n_tets) t0 = (int)B.tet_offset;
+
+      const double pc[3] = {(double)x, (double)y, (double)z};
+      int v[4];
+      float X[4][3];
+      int tc = walk_locate(P.tet_v, P.tet_n, P.posd, pc, t0, P.max_steps, v, X, st);
+      ++n_loc;
+      if (tc == kWalkFail) { ++n_fail; tc = kOutside; }
+
+      if (METHOD == DTFE_METHOD_CENTRE) {
+        if (tc >= 0) {
+          CellOut e;
+          cell_eval<S>(v, X, pc, P.posd, P.vel4, P.scal, want_dens, want_vel, want_sc, fix, e);
+          aD = e.dens;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) aV[c] = e.vel[c];
+          for (int c = 0; c < 3; ++c) aV[c] = e.vel[c];
 #pragma unroll
-        for (int c = 0; c < 9; ++c) aG[c] = e.grad[c];
+          for (int c = 0; c < 9; ++c) aG[c] = e.grad[c];
 #pragma unroll
-        for (int q = 0; q < S; ++q) {
-          aS[q] = e.sc[q];
+          for (int q = 0; q < S; ++q) {
+            aS[q] = e.sc[q];
 #pragma unroll
-          for (int c = 0; c < 3; ++c) aSG[3 * q + c] = e.scg[3 * q + c];
+            for (int c = 0; c < 3; ++c) aSG[3 * q + c] = e.scg[3 * q + c];
+          }
+        } else {
+          ++n_out;
         }
       } else {
-        ++n_out;
-      }
-    } else {
-      if (tc < 0) ++n_out;
-      const int NN = P.NN;
-      const uint64_t key = mc_key(P.seed, B.part_no);
-      const int tstart = tc >= 0 ? tc : t0;
-      // velocity standard deviation: two passes over the sample velocities
-      // (standardDeviation, triangulation_miscellaneous.cc:256-271); the
-      // first pass accumulates the mean, the second re-walks the samples.
-      for (int w = 0; w < NN; ++w) {
-        double p[3];
-        if (METHOD == DTFE_METHOD_MONTE_CARLO) {
-          double u[3];
-          mc_offsets(key, (uint64_t)cell, (uint32_t)w, u);
-          p[0] = u[0] * (double)B.dx[0] + pc[0];
-          p[1] = u[1] * (double)B.dx[1] + pc[1];
-          p[2] = u[2] * (double)B.dx[2] + pc[2];
-        } else {
-          const float* eo = P.eq_off + ((int64_t)b * NN + w) * 3;
-          p[0] = (double)(x + __ldg(&eo[0]));
-          p[1] = (double)(y + __ldg(&eo[1]));
-          p[2] = (double)(z + __ldg(&eo[2]));
+        if (tc < 0) ++n_out;
+        const int NN = P.NN;
+        const uint64_t key = mc_key(P.seed, B.part_no);
+        const int tstart = tc >= 0 ? tc : t0;
+        float stdacc[3] = {0.f, 0.f, 0.f};
+        for (int w = 0; w < NN; ++w) {
+          double p[3];
+          if (METHOD == DTFE_METHOD_MONTE_CARLO) {
+            double u[3];
+            mc_offsets(key, (uint64_t)cell, (uint32_t)w, u);
+            p[0] = u[0] * (double)B.dx[0] + pc[0];
+            p[1] = u[1] * (double)B.dx[1] + pc[1];
+            p[2] = u[2] * (double)B.dx[2] + pc[2];
+          } else {
+            const float* eo = P.eq_off + ((int64_t)b * NN + w) * 3;
+            p[0] = (double)(x + __ldg(&eo[0]));
+            p[1] = (double)(y + __ldg(&eo[1]));
+            p[2] = (double)(z + __ldg(&eo[2]));
+          }
+          int vv[4];
+          float XX[4][3];
+          int t = walk_locate(P.tet_v, P.tet_n, P.posd, p, tstart, P.max_steps, vv, XX, st);
+          ++n_loc;
+          if (t == kWalkFail) { ++n_fail; t = kOutside; }
+          if (t < 0) continue;
+          CellOut e;
+          cell_eval<S>(vv, XX, p, P.posd, P.vel4, P.scal, want_dens, want_vel, want_sc, fix, e);
+          aD += e.dens;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) aV[c] += e.vel[c];
+#pragma unroll
+          for (int c = 0; c < 9; ++c) aG[c] += e.grad[c];
+#pragma unroll
+          for (int q = 0; q < S; ++q) {
+            aS[q] += e.sc[q];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) aSG[3 * q + c] += e.scg[3 * q + c];
+          }
+          if (want_std) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) stdacc[c] += e.vel[c];
+          }
         }
-        int vv[4];
-        double XX[4][3];
-        int t = walk_locate(P.tet_v, P.tet_n, P.posd, p, tstart, P.max_steps, vv, XX, st);
-        ++n_loc;
-        if (t == kWalkFail) { ++n_fail; t = kOutside; }
-        if (t < 0) continue;
-        CellOut e;
-        cell_eval<S>(vv, XX, p, P.posd, P.vel4, P.scal, want_dens, want_vel, want_sc, fix, e);
-        aD += e.dens;
+        const float fn = (float)NN;
+        aD = aD / fn;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) aV[c] += e.vel[c];
+        for (int c = 0; c < 3; ++c) aV[c] = aV[c] / fn;
 #pragma unroll
-        for (int c = 0; c < 9; ++c) aG[c] += e.grad[c];
+        for (int c = 0; c < 9; ++c) aG[c] = aG[c] / fn;
 #pragma unroll
         for (int q = 0; q < S; ++q) {
-          aS[q] += e.sc[q];
+          aS[q] = aS[q] / fn;
 #pragma unroll
-          for (int c = 0; c < 3; ++c) aSG[3 * q + c] += e.scg[3 * q + c];
+          for (int c = 0; c < 3; ++c) aSG[3 * q + c] = aSG[3 * q + c] / fn;
         }
         if (want_std) {
+          // standardDeviation (triangulation_miscellaneous.cc:256-271): the
+          // second pass re-walks the samples (their velocities are not kept)
+          float mean[3];
 #pragma unroll
-          for (int c = 0; c < 3; ++c) stdacc[c] += e.vel[c];
-        }
-      }
-      const float fn = (float)NN;
-      aD = aD / fn;
+          for (int c = 0; c < 3; ++c) mean[c] = stdacc[c] / fn;
+          float r = 0.f;
+          for (int w = 0; w < NN; ++w) {
+            float vel[3] = {0.f, 0.f, 0.f};
+            double u[3], p[3];
+            mc_offsets(key, (uint64_t)cell, (uint32_t)w, u);
+            p[0] = u[0] * (double)B.dx[0] + pc[0];
+            p[1] = u[1] * (double)B.dx[1] + pc[1];
+            p[2] = u[2] * (double)B.dx[2] + pc[2];
+            int vv[4];
+            float XX[4][3];
+            WalkStats st2{0, 0, 0};
+            int t = walk_locate(P.tet_v, P.tet_n, P.posd, p, tstart, P.max_steps, vv, XX, st2);
+            if (t >= 0) {
+              CellOut e;
+              cell_eval<0>(vv, XX, p, P.posd, P.vel4, P.scal, false, true, false, fix, e);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) aV[c] = aV[c] / fn;
+              for (int c = 0; c < 3; ++c) vel[c] = e.vel[c];
+            }
 #pragma unroll
-      for (int c = 0; c < 9; ++c) aG[c] = aG[c] / fn;
-#pragma unroll
-      for (int q = 0; q < S; ++q) {
-        aS[q] = aS[q] / fn;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) aSG[3 * q + c] = aSG[3 * q + c] / fn;
-      }
-      if (want_std) {
-        float mean[3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) mean[c] = stdacc[c] / fn;
-        float r = 0.f;
-        for (int w = 0; w < NN; ++w) {
-          float vel[3] = {0.f, 0.f, 0.f};
-          double u[3], p[3];
-          mc_offsets(key, (uint64_t)cell, (uint32_t)w, u);
-          p[0] = u[0] * (double)B.dx[0] + pc[0];
-          p[1] = u[1] * (double)B.dx[1] + pc[1];
-          p[2] = u[2] * (double)B.dx[2] + pc[2];
-          int vv[4];
-          double XX[4][3];
-          WalkStats st2{0, 0, 0};
-          int t = walk_locate(P.tet_v, P.tet_n, P.posd, p, tstart, P.max_steps, vv, XX, st2);
-          if (t >= 0) {
-            CellOut e;
-            cell_eval<0>(vv, XX, p, P.posd, P.vel4, P.scal, false, true, false, fix, e);
-#pragma unroll
-            for (int c = 0; c < 3; ++c) vel[c] = e.vel[c];
+            for (int c = 0; c < 3; ++c) {
+              float d = vel[c] - mean[c];
+              r += d * d;
+            }
           }
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            float d = vel[c] - mean[c];
-            r += d * d;
-          }
+          sdev = sqrtf(r / fn);
         }
-        P.out[DTFE_VELOCITY_STD][cell] = sqrtf(r / fn);
       }
     }
 
-    if (has_field(F, DTFE_DENSITY)) P.out[DTFE_DENSITY][cell] = aD;
-    if (has_field(F, DTFE_VELOCITY)) {
-      float* o = P.out[DTFE_VELOCITY] + 3 * cell;
-      o[0] = aV[0]; o[1] = aV[1]; o[2] = aV[2];
-    }
-    if (has_field(F, DTFE_VELOCITY_GRADIENT)) {
-      float* o = P.out[DTFE_VELOCITY_GRADIENT] + 9 * cell;
-#pragma unroll
-      for (int c = 0; c < 9; ++c) o[c] = aG[c];
-    }
+    // ---- stores: contiguous warps go through shared memory -----------------
+    const int64_t c0 = __shfl_sync(0xffffffffu, cell, 0);
+    const bool contig = __all_sync(0xffffffffu, valid && cell == c0 + lane) && (c0 % 4 == 0);
+    if (has_field(F, DTFE_DENSITY)) store_field<1>(P.out[DTFE_DENSITY], cell, valid, &aD, contig, c0, stage);
+    if (has_field(F, DTFE_VELOCITY)) store_field<3>(P.out[DTFE_VELOCITY], cell, valid, aV, contig, c0, stage);
+    if (has_field(F, DTFE_VELOCITY_GRADIENT))
+      store_field<9>(P.out[DTFE_VELOCITY_GRADIENT], cell, valid, aG, contig, c0, stage);
     if (has_field(F, DTFE_VELOCITY_DIVERGENCE) || has_field(F, DTFE_VELOCITY_SHEAR) ||
         has_field(F, DTFE_VELOCITY_VORTICITY)) {
       float dv, sh[5], vo[3];
       derived_fields(aG, dv, sh, vo);
-      if (has_field(F, DTFE_VELOCITY_DIVERGENCE)) P.out[DTFE_VELOCITY_DIVERGENCE][cell] = dv;
-      if (has_field(F, DTFE_VELOCITY_SHEAR)) {
-        float* o = P.out[DTFE_VELOCITY_SHEAR] + 5 * cell;
-#pragma unroll
-        for (int c = 0; c < 5; ++c) o[c] = sh[c];
-      }
-      if (has_field(F, DTFE_VELOCITY_VORTICITY)) {
-        float* o = P.out[DTFE_VELOCITY_VORTICITY] + 3 * cell;
-        o[0] = vo[0]; o[1] = vo[1]; o[2] = vo[2];
-      }
+      if (has_field(F, DTFE_VELOCITY_DIVERGENCE))
+        store_field<1>(P.out[DTFE_VELOCITY_DIVERGENCE], cell, valid, &dv, contig, c0, stage);
+      if (has_field(F, DTFE_VELOCITY_SHEAR))
+        store_field<5>(P.out[DTFE_VELOCITY_SHEAR], cell, valid, sh, contig, c0, stage);
+      if (has_field(F, DTFE_VELOCITY_VORTICITY))
+        store_field<3>(P.out[DTFE_VELOCITY_VORTICITY], cell, valid, vo, contig, c0, stage);
     }
-    if (S > 0 && has_field(F, DTFE_SCALAR)) {
-      float* o = P.out[DTFE_SCALAR] + (int64_t)S * cell;
-#pragma unroll
-      for (int q = 0; q < S; ++q) o[q] = aS[q];
-    }
-    if (S > 0 && has_field(F, DTFE_SCALAR_GRADIENT)) {
-      float* o = P.out[DTFE_SCALAR_GRADIENT] + (int64_t)3 * S * cell;
-#pragma unroll
-      for (int q = 0; q < 3 * S; ++q) o[q] = aSG[q];
-    }
+    if (want_std) store_field<1>(P.out[DTFE_VELOCITY_STD], cell, valid, &sdev, contig, c0, stage);
+    if (S > 0 && has_field(F, DTFE_SCALAR))
+      store_field<(S > 0 ? S : 1)>(P.out[DTFE_SCALAR], cell, valid, aS, contig, c0, stage);
+    if (S > 0 && has_field(F, DTFE_SCALAR_GRADIENT))
+      store_field<(S > 0 ? 3 * S : 1)>(P.out[DTFE_SCALAR_GRADIENT], cell, valid, aSG, contig, c0, stage);
   }
   // fold the per-thread counters into the global ones, one atomic per warp
   unsigned vals[CNT_N] = {n_loc, n_out, n_fail, (unsigned)st.steps, (unsigned)st.exact, (unsigned)st.tie};
 #pragma unroll
   for (int c = 0; c < CNT_N; ++c) {
     unsigned r = __reduce_add_sync(0xffffffffu, vals[c]);
-    if ((threadIdx.x & 31) == 0 && r) atomicAdd(&P.counters[c], (unsigned long long)r);
+    if (lane == 0 && r) atomicAdd(&P.counters[c], (unsigned long long)r);
   }
 }
 
@@ -374,7 +532,7 @@ __global__ void k_locate_points(int64_t np, const double* __restrict__ pts, cons
   if (i >= np) return;
   double p[3] = {pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
   int v[4];
-  double X[4][3];
+  float X[4][3];
   WalkStats st{0, 0, 0};
   out[i] = walk_locate(tet_v, tet_n, posd, p, start, max_steps, v, X, st);
 }
@@ -395,9 +553,12 @@ struct dtfe_gpu_s {
   float4* vel4 = nullptr;
   float* scal = nullptr;
   float* w = nullptr;
-  double* volsum = nullptr;
+  double* vol = nullptr;          // per-tetrahedron volume
+  int64_t* inc_off = nullptr;     // V+1 offsets into inc
+  int* inc = nullptr;             // incident tetrahedra per vertex, ascending
+  int* scratch_i = nullptr;       // V ints (degrees / fill cursors)
+  int64_t* scan_blocks = nullptr; // block totals of the offset scan
   int* hull = nullptr;
-  int* vtx_tet = nullptr;
   bool has_vel = false, has_scal = false;
   bool density_ready = false;
   // sub-boxes
@@ -405,7 +566,7 @@ struct dtfe_gpu_s {
   std::vector<dtfe_subbox> boxes_h;
   dtfe_subbox* boxes = nullptr;
   int64_t* tile_prefix = nullptr;
-  int64_t* vprefix = nullptr;
+  int64_t* tet_prefix = nullptr;  // K+1 tetrahedron range starts
   int64_t* bin_offset = nullptr;
   int* bins = nullptr;
   int64_t n_cells = 0;
@@ -463,10 +624,10 @@ int field_components(int slot, int S) {
 
 int prepare_bins(dtfe_handle h) {
   if (h->bins_ready) return DTFE_OK;
-  if (!h->density_ready) return set_error(DTFE_ERR_STATE, "vertex density not computed");
   DTFE_CUDA_TRY(cudaMemsetAsync(h->bins, 0x7F, sizeof(int) * h->n_cells, h->stream));
-  k_seed_bins<<<blocks_for(h->V, 256), 256, 0, h->stream>>>(h->V, h->posd, h->vtx_tet, h->boxes, h->vprefix,
-                                                           h->bin_offset, h->K, h->bins);
+  if (h->T > 0)
+    k_tet_volume_bins<true><<<blocks_for(h->T, kVolBlock), kVolBlock, 0, h->stream>>>(
+        h->T, h->tet_v, h->posd, h->vol, h->boxes, h->tet_prefix, h->bin_offset, h->K, h->bins);
   DTFE_CUDA_TRY(cudaGetLastError());
   h->bins_ready = true;
   return DTFE_OK;
@@ -528,8 +689,9 @@ int dtfe_gpu_destroy(dtfe_handle h) {
   if (!h) return DTFE_OK;
   cudaSetDevice(h->device);
   cudaStreamSynchronize(h->stream);
-  void* ptrs[] = {h->tet_v, h->tet_n, h->posd, h->vel4, h->scal, h->w, h->volsum, h->hull,
-                  h->vtx_tet, h->boxes, h->tile_prefix, h->vprefix, h->bin_offset, h->bins,
+  void* ptrs[] = {h->tet_v, h->tet_n, h->posd, h->vel4, h->scal, h->w, h->vol, h->inc_off, h->inc,
+                  h->scratch_i, h->scan_blocks, h->hull,
+                  h->boxes, h->tile_prefix, h->tet_prefix, h->bin_offset, h->bins,
                   h->xs, h->ys, h->zs, h->eq_off, h->counters};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -560,8 +722,11 @@ int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n, i
   h->V = n_verts;
   if ((rc = dev_alloc(h, &h->tet_v, n_tets)) || (rc = dev_alloc(h, &h->tet_n, n_tets)) ||
       (rc = dev_alloc(h, &h->posd, n_verts)) || (rc = dev_alloc(h, &h->vel4, n_verts)) ||
-      (rc = dev_alloc(h, &h->w, n_verts)) || (rc = dev_alloc(h, &h->volsum, n_verts)) ||
-      (rc = dev_alloc(h, &h->hull, n_verts)) || (rc = dev_alloc(h, &h->vtx_tet, n_verts)) ||
+      (rc = dev_alloc(h, &h->w, n_verts)) || (rc = dev_alloc(h, &h->vol, n_tets)) ||
+      (rc = dev_alloc(h, &h->inc_off, n_verts + 1)) || (rc = dev_alloc(h, &h->inc, 4 * n_tets)) ||
+      (rc = dev_alloc(h, &h->scratch_i, n_verts)) ||
+      (rc = dev_alloc(h, &h->scan_blocks, (n_verts + kScanBlock - 1) / kScanBlock + 1)) ||
+      (rc = dev_alloc(h, &h->hull, n_verts)) ||
       (rc = dev_alloc(h, &h->scal, (size_t)n_verts * h->S)))
     return rc;
   cudaStream_t st = h->stream;
@@ -591,6 +756,23 @@ int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n, i
         DTFE_CUDA_TRY(cudaMemsetAsync(h->scal, 0, sizeof(float) * h->S * n_verts, st));
     }
   }
+  // hull vertices (a property of the tessellation's topology)
+  if (n_verts) DTFE_CUDA_TRY(cudaMemsetAsync(h->hull, 0, sizeof(int) * n_verts, st));
+  if (n_tets) k_hull_marks<<<blocks_for(n_tets, 256), 256, 0, st>>>(n_tets, h->tet_v, h->tet_n, h->hull);
+  // vertex -> tetrahedron incidence lists (ascending tetrahedron ids)
+  if (n_verts) {
+    DTFE_CUDA_TRY(cudaMemsetAsync(h->scratch_i, 0, sizeof(int) * n_verts, st));
+    if (n_tets) k_degree<<<blocks_for(n_tets, 256), 256, 0, st>>>(n_tets, h->tet_v, h->scratch_i);
+    int64_t nb = (n_verts + kScanBlock - 1) / kScanBlock;
+    k_scan_blocks<<<(unsigned)nb, kScanBlock, 0, st>>>(n_verts, h->scratch_i, h->inc_off, h->scan_blocks);
+    k_scan_totals<<<1, kScanBlock, 0, st>>>(nb, h->scan_blocks, h->inc_off + n_verts);
+    k_scan_add<<<(unsigned)nb, kScanBlock, 0, st>>>(n_verts, h->inc_off, h->scan_blocks);
+    DTFE_CUDA_TRY(cudaMemsetAsync(h->scratch_i, 0, sizeof(int) * n_verts, st));
+    if (n_tets) {
+      k_fill_incidence<<<blocks_for(n_tets, 256), 256, 0, st>>>(n_tets, h->tet_v, h->inc_off, h->scratch_i, h->inc);
+      k_sort_incidence<<<blocks_for(n_verts, 256), 256, 0, st>>>(n_verts, h->inc_off, h->inc);
+    }
+  }
   DTFE_CUDA_TRY(cudaGetLastError());
   h->has_vel = vel != nullptr;
   h->has_scal = scal != nullptr;
@@ -605,7 +787,7 @@ int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* box
   if (!h || n_boxes <= 0 || !boxes || !xs || !ys || !zs || !grid)
     return set_error(DTFE_ERR_ARG, "null or empty sub-box description");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
-  std::vector<int64_t> tprefix(n_boxes + 1), vprefix(n_boxes + 1), boff(n_boxes);
+  std::vector<int64_t> tprefix(n_boxes + 1), tetpre(n_boxes + 1), boff(n_boxes);
   int64_t cells = 0;
   for (int b = 0; b < n_boxes; ++b) {
     const dtfe_subbox& B = boxes[b];
@@ -618,18 +800,20 @@ int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* box
     if (B.vert_offset < 0 || B.vert_offset + B.n_verts > h->V || B.tet_offset < 0 ||
         B.tet_offset + B.n_tets > h->T)
       return set_error(DTFE_ERR_ARG, "sub-box vertex/tetrahedron range outside the upload");
-    if (b > 0 && B.vert_offset != boxes[b - 1].vert_offset + boxes[b - 1].n_verts)
-      return set_error(DTFE_ERR_ARG, "sub-box vertex ranges must be consecutive");
+    if (b > 0 && (B.vert_offset != boxes[b - 1].vert_offset + boxes[b - 1].n_verts ||
+                  B.tet_offset != boxes[b - 1].tet_offset + boxes[b - 1].n_tets))
+      return set_error(DTFE_ERR_ARG, "sub-box vertex and tetrahedron ranges must be consecutive");
     tprefix[b] = cells;
     boff[b] = cells;
-    vprefix[b] = B.vert_offset;
+    tetpre[b] = B.tet_offset;
     cells += (int64_t)B.tile_dims[0] * B.tile_dims[1] * B.tile_dims[2];
   }
   tprefix[n_boxes] = cells;
-  vprefix[n_boxes] = boxes[n_boxes - 1].vert_offset + boxes[n_boxes - 1].n_verts;
+  tetpre[n_boxes] = boxes[n_boxes - 1].tet_offset + boxes[n_boxes - 1].n_tets;
+  if (cells >= (int64_t)kEmptyBin) return set_error(DTFE_ERR_TOO_LARGE, "more than 2^31 grid cells");
   int rc;
   if ((rc = dev_alloc(h, &h->boxes, n_boxes)) || (rc = dev_alloc(h, &h->tile_prefix, n_boxes + 1)) ||
-      (rc = dev_alloc(h, &h->vprefix, n_boxes + 1)) || (rc = dev_alloc(h, &h->bin_offset, n_boxes)) ||
+      (rc = dev_alloc(h, &h->tet_prefix, n_boxes + 1)) || (rc = dev_alloc(h, &h->bin_offset, n_boxes)) ||
       (rc = dev_alloc(h, &h->bins, cells)) || (rc = dev_alloc(h, &h->xs, n_xs)) ||
       (rc = dev_alloc(h, &h->ys, n_ys)) || (rc = dev_alloc(h, &h->zs, n_zs)))
     return rc;
@@ -637,7 +821,7 @@ int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* box
   DTFE_CUDA_TRY(cudaMemcpyAsync(h->boxes, boxes, sizeof(dtfe_subbox) * n_boxes, cudaMemcpyHostToDevice, st));
   DTFE_CUDA_TRY(cudaMemcpyAsync(h->tile_prefix, tprefix.data(), sizeof(int64_t) * (n_boxes + 1),
                                 cudaMemcpyHostToDevice, st));
-  DTFE_CUDA_TRY(cudaMemcpyAsync(h->vprefix, vprefix.data(), sizeof(int64_t) * (n_boxes + 1),
+  DTFE_CUDA_TRY(cudaMemcpyAsync(h->tet_prefix, tetpre.data(), sizeof(int64_t) * (n_boxes + 1),
                                 cudaMemcpyHostToDevice, st));
   DTFE_CUDA_TRY(cudaMemcpyAsync(h->bin_offset, boff.data(), sizeof(int64_t) * n_boxes, cudaMemcpyHostToDevice, st));
   DTFE_CUDA_TRY(cudaMemcpyAsync(h->xs, xs, sizeof(float) * n_xs, cudaMemcpyHostToDevice, st));
@@ -659,19 +843,23 @@ int dtfe_gpu_vertex_density(dtfe_handle h, double rho_bar) {
   if (h->V == 0) return set_error(DTFE_ERR_STATE, "nothing uploaded");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
   cudaStream_t st = h->stream;
-  DTFE_CUDA_TRY(cudaMemsetAsync(h->volsum, 0, sizeof(double) * h->V, st));
-  DTFE_CUDA_TRY(cudaMemsetAsync(h->hull, 0, sizeof(int) * h->V, st));
-  DTFE_CUDA_TRY(cudaMemsetAsync(h->vtx_tet, 0x7F, sizeof(int) * h->V, st));
-  if (h->T > 0)
-    k_volume_scatter<<<blocks_for(h->T, 256), 256, 0, st>>>(h->T, h->tet_v, h->tet_n, h->posd, h->volsum,
-                                                           h->hull, h->vtx_tet);
+  if (h->K > 0) DTFE_CUDA_TRY(cudaMemsetAsync(h->bins, 0x7F, sizeof(int) * h->n_cells, st));
+  if (h->T > 0) {
+    if (h->K > 0)
+      k_tet_volume_bins<true><<<blocks_for(h->T, kVolBlock), kVolBlock, 0, st>>>(
+          h->T, h->tet_v, h->posd, h->vol, h->boxes, h->tet_prefix, h->bin_offset, h->K, h->bins);
+    else
+      k_tet_volume_bins<false><<<blocks_for(h->T, kVolBlock), kVolBlock, 0, st>>>(
+          h->T, h->tet_v, h->posd, h->vol, h->boxes, h->tet_prefix, h->bin_offset, h->K, h->bins);
+  }
   // the reference's factor: (NO_DIM+1.)/averageDensity stored as Real
   float rb = (float)rho_bar;
   float factor = (float)(4.0 / (double)rb);
-  k_vertex_density<<<blocks_for(h->V, 256), 256, 0, st>>>(h->V, h->w, h->volsum, h->hull, factor, h->posd);
+  k_vertex_density<<<blocks_for(h->V, 256), 256, 0, st>>>(h->V, h->w, h->vol, h->inc_off, h->inc, h->hull,
+                                                           factor, h->posd);
   DTFE_CUDA_TRY(cudaGetLastError());
   h->density_ready = true;
-  h->bins_ready = false;
+  h->bins_ready = h->K > 0;
   return DTFE_OK;
 }
 
@@ -691,6 +879,7 @@ static int interpolate_impl(dtfe_handle h, const dtfe_interp_opts* o, float* con
   if (!h || !o) return set_error(DTFE_ERR_ARG, "null argument");
   if (h->K == 0) return set_error(DTFE_ERR_STATE, "sub-boxes not set");
   if (h->T == 0) return set_error(DTFE_ERR_DEGENERATE, "no tetrahedra");
+  if (!h->density_ready) return set_error(DTFE_ERR_STATE, "vertex density not computed");
   int method = o->method;
   if (method != DTFE_METHOD_CENTRE && method != DTFE_METHOD_MONTE_CARLO && method != DTFE_METHOD_EQUIDISTANT)
     return set_error(DTFE_ERR_ARG, "unknown method");
@@ -738,7 +927,6 @@ static int interpolate_impl(dtfe_handle h, const dtfe_interp_opts* o, float* con
   P.posd = h->posd;
   P.vel4 = h->vel4;
   P.scal = h->scal;
-  P.vtx_tet = h->vtx_tet;
   P.bins = h->bins;
   P.boxes = h->boxes;
   P.tile_prefix = h->tile_prefix;
@@ -758,8 +946,12 @@ static int interpolate_impl(dtfe_handle h, const dtfe_interp_opts* o, float* con
   P.max_steps = h->max_steps;
   for (int s = 0; s < DTFE_NUM_FIELDS; ++s) P.out[s] = (F >> s & 1u) ? out_dev[s] : nullptr;
   P.counters = h->counters;
-  const unsigned block = 256;
+  const unsigned block = kInterpBlock;
   unsigned grid = blocks_for(h->n_cells, block);
+  // every output must be 16-byte aligned for the staged stores
+  for (int q = 0; q < DTFE_NUM_FIELDS; ++q)
+    if (P.out[q] && ((uintptr_t)P.out[q] & 15))
+      return set_error(DTFE_ERR_ARG, "output buffers must be 16-byte aligned");
   if (method == DTFE_METHOD_CENTRE) launch_interp_s<DTFE_METHOD_CENTRE>(P, h->S, st, grid, block);
   else if (method == DTFE_METHOD_MONTE_CARLO) launch_interp_s<DTFE_METHOD_MONTE_CARLO>(P, h->S, st, grid, block);
   else launch_interp_s<DTFE_METHOD_EQUIDISTANT>(P, h->S, st, grid, block);

@@ -30,6 +30,13 @@ struct WalkStats {
   int tie;
 };
 
+__device__ __forceinline__ void load_posf(const float4* __restrict__ posd, int v, float X[3]) {
+  float4 q = __ldg(&posd[v]);
+  X[0] = q.x;
+  X[1] = q.y;
+  X[2] = q.z;
+}
+
 __device__ __forceinline__ void load_pos(const float4* __restrict__ posd, int v, double X[3]) {
   float4 q = __ldg(&posd[v]);
   X[0] = (double)q.x;
@@ -37,18 +44,38 @@ __device__ __forceinline__ void load_pos(const float4* __restrict__ posd, int v,
   X[2] = (double)q.z;
 }
 
-// Signs of the four face orientations of tetrahedron with vertices X[0..3]
-// for point p (o_i = orient with vertex i replaced by p), evaluating only the
-// faces in `need` (bit mask).  Returns the mask of evaluated faces.
-__device__ __forceinline__ void face_signs(const double X[4][3], const double p[3], int need,
-                                          int sgn[4], int& nexact) {
+// Sign of one face orientation from a determinant and its permanent; exact
+// re-evaluation (orient_exact with the definition's argument order) when the
+// filter cannot decide.
+__device__ __forceinline__ int filtered_sign(double det, double perm, int face, const float X[4][3],
+                                             const double p[3], int& nexact) {
+  double b = kOrientErr * perm;
+  if (det > b) return 1;
+  if (-det > b) return -1;
+  ++nexact;
+  double Q[4][3];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) Q[a][c] = (double)X[a][c];
+  const double* q[4] = {Q[0], Q[1], Q[2], Q[3]};
+  q[face] = p;
+  return orient_exact(q[0], q[1], q[2], q[3]);
+}
+
+// Face orientations o_i = orient(tetrahedron with vertex i replaced by p) for
+// the faces in `need`, evaluated in order 0..3 and stopping at the first
+// negative one (returned; -1 if none).  o_0 and o_1 share d2 x d3, o_2 and
+// o_3 share d0 x d1 (d_k = X_k - p).  zmask receives the faces through p.
+__device__ __forceinline__ int first_exit_face(const float X[4][3], const double p[3], int need,
+                                               int& zmask, int& nexact) {
   double d[4][3];
 #pragma unroll
   for (int k = 0; k < 4; ++k)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) d[k][c] = X[k][c] - p[c];
+    for (int c = 0; c < 3; ++c) d[k][c] = (double)X[k][c] - p[c];
+  zmask = 0;
   if (need & 3) {
-    // c23 = d2 x d3
     double m0 = d[2][1] * d[3][2], m1 = d[2][2] * d[3][1];
     double m2 = d[2][2] * d[3][0], m3 = d[2][0] * d[3][2];
     double m4 = d[2][0] * d[3][1], m5 = d[2][1] * d[3][0];
@@ -57,22 +84,19 @@ __device__ __forceinline__ void face_signs(const double X[4][3], const double p[
     if (need & 1) {
       double det = d[1][0] * cx + d[1][1] * cy + d[1][2] * cz;
       double perm = fabs(d[1][0]) * ax + fabs(d[1][1]) * ay + fabs(d[1][2]) * az;
-      double b = kOrientErr * perm;
-      if (det > b) sgn[0] = 1;
-      else if (-det > b) sgn[0] = -1;
-      else { sgn[0] = orient_exact(p, X[1], X[2], X[3]); ++nexact; }
+      int s = filtered_sign(det, perm, 0, X, p, nexact);
+      if (s < 0) return 0;
+      if (s == 0) zmask |= 1;
     }
     if (need & 2) {
       double det = -(d[0][0] * cx + d[0][1] * cy + d[0][2] * cz);
       double perm = fabs(d[0][0]) * ax + fabs(d[0][1]) * ay + fabs(d[0][2]) * az;
-      double b = kOrientErr * perm;
-      if (det > b) sgn[1] = 1;
-      else if (-det > b) sgn[1] = -1;
-      else { sgn[1] = orient_exact(X[0], p, X[2], X[3]); ++nexact; }
+      int s = filtered_sign(det, perm, 1, X, p, nexact);
+      if (s < 0) return 1;
+      if (s == 0) zmask |= 2;
     }
   }
   if (need & 12) {
-    // c01 = d0 x d1
     double m0 = d[0][1] * d[1][2], m1 = d[0][2] * d[1][1];
     double m2 = d[0][2] * d[1][0], m3 = d[0][0] * d[1][2];
     double m4 = d[0][0] * d[1][1], m5 = d[0][1] * d[1][0];
@@ -81,54 +105,45 @@ __device__ __forceinline__ void face_signs(const double X[4][3], const double p[
     if (need & 4) {
       double det = d[3][0] * cx + d[3][1] * cy + d[3][2] * cz;
       double perm = fabs(d[3][0]) * ax + fabs(d[3][1]) * ay + fabs(d[3][2]) * az;
-      double b = kOrientErr * perm;
-      if (det > b) sgn[2] = 1;
-      else if (-det > b) sgn[2] = -1;
-      else { sgn[2] = orient_exact(X[0], X[1], p, X[3]); ++nexact; }
+      int s = filtered_sign(det, perm, 2, X, p, nexact);
+      if (s < 0) return 2;
+      if (s == 0) zmask |= 4;
     }
     if (need & 8) {
       double det = -(d[2][0] * cx + d[2][1] * cy + d[2][2] * cz);
       double perm = fabs(d[2][0]) * ax + fabs(d[2][1]) * ay + fabs(d[2][2]) * az;
-      double b = kOrientErr * perm;
-      if (det > b) sgn[3] = 1;
-      else if (-det > b) sgn[3] = -1;
-      else { sgn[3] = orient_exact(X[0], X[1], X[2], p); ++nexact; }
+      int s = filtered_sign(det, perm, 3, X, p, nexact);
+      if (s < 0) return 3;
+      if (s == 0) zmask |= 8;
     }
   }
+  return -1;
 }
 
 __device__ __forceinline__ void load_tet(const int4* __restrict__ tet_v, const float4* __restrict__ posd,
-                                        int t, int v[4], double X[4][3]) {
+                                        int t, int v[4], float X[4][3]) {
   int4 q = __ldg(&tet_v[t]);
   v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
 #pragma unroll
-  for (int a = 0; a < 4; ++a) load_pos(posd, v[a], X[a]);
+  for (int a = 0; a < 4; ++a) load_posf(posd, v[a], X[a]);
 }
 
 __device__ __forceinline__ int nb_of(const int4& n, int i) {
   return i == 0 ? n.x : (i == 1 ? n.y : (i == 2 ? n.z : n.w));
 }
 
-// True if the closure of tetrahedron t holds p; zero[] marks faces through p.
+// True if the closure of tetrahedron t holds p; zmask marks faces through p.
 __device__ __noinline__ bool tet_contains(const int4* __restrict__ tet_v, const float4* __restrict__ posd,
                                           int t, const double p[3], int& zmask, int& nexact) {
   int v[4];
-  double X[4][3];
+  float X[4][3];
   load_tet(tet_v, posd, t, v, X);
-  int s[4];
-  face_signs(X, p, 15, s, nexact);
-  zmask = 0;
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    if (s[i] < 0) return false;
-    if (s[i] == 0) zmask |= 1 << i;
-  }
-  return true;
+  return first_exit_face(X, p, 15, zmask, nexact) < 0;
 }
 
 // Canonical tie rule: the lowest id among the tetrahedra whose closure holds
-// p, found by exploring across faces that pass through p.  Bounded: gives up
-// (keeps the best so far, sets overflow) after kTieMax tetrahedra.
+// p, found by exploring across faces that pass through p.  Bounded: keeps
+// the best so far after kTieMax tetrahedra.
 constexpr int kTieMax = 96;
 __device__ __noinline__ int canonical_tie(const int4* __restrict__ tet_v, const int4* __restrict__ tet_n,
                                           const float4* __restrict__ posd, int t, int zmask,
@@ -137,14 +152,10 @@ __device__ __noinline__ int canonical_tie(const int4* __restrict__ tet_v, const 
   int nseen = 1, head = 0;
   seen[0] = t;
   int best = t;
-  // seen[] doubles as the BFS queue (entries before head are expanded)
   int zm = zmask;
   while (head < nseen) {
     int u = seen[head];
-    if (head > 0) {
-      int dummy;
-      tet_contains(tet_v, posd, u, p, zm, dummy);
-    }
+    if (head > 0) tet_contains(tet_v, posd, u, p, zm, nexact);
     ++head;
     int4 n = __ldg(&tet_n[u]);
     for (int i = 0; i < 4; ++i) {
@@ -167,33 +178,20 @@ __device__ __noinline__ int canonical_tie(const int4* __restrict__ tet_v, const 
 
 // Visibility walk from tetrahedron t toward p.  Returns the canonical
 // containing tetrahedron, kOutside, or kWalkFail.  On success v/X hold the
-// vertices and positions of the returned tetrahedron.
+// vertices and positions of the returned tetrahedron.  Crossing a face keeps
+// the three shared vertices in registers and loads only the new one; the
+// face just crossed is not re-tested (p is strictly inside it).
 __device__ __forceinline__ int walk_locate(const int4* __restrict__ tet_v, const int4* __restrict__ tet_n,
                                            const float4* __restrict__ posd, const double p[3], int t,
-                                           int max_steps, int v[4], double X[4][3], WalkStats& st) {
+                                           int max_steps, int v[4], float X[4][3], WalkStats& st) {
+  load_tet(tet_v, posd, t, v, X);
   int came = -1;
-  int fv0 = -1, fv1 = -1, fv2 = -1;
   for (int step = 0; step < max_steps; ++step) {
     ++st.steps;
-    load_tet(tet_v, posd, t, v, X);
-    if (fv0 >= 0) {
-      came = -1;
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (v[j] != fv0 && v[j] != fv1 && v[j] != fv2) came = j;
-    }
     int need = 15 & ~(came >= 0 ? (1 << came) : 0);
-    int s[4] = {1, 1, 1, 1};
-    face_signs(X, p, need, s, st.exact);
-    int exit_face = -1;
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-      if (exit_face < 0 && (need & (1 << i)) && s[i] < 0) exit_face = i;
+    int zmask;
+    int exit_face = first_exit_face(X, p, need, zmask, st.exact);
     if (exit_face < 0) {
-      int zmask = 0;
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-        if ((need & (1 << i)) && s[i] == 0) zmask |= 1 << i;
       if (zmask) {
         ++st.tie;
         int b = canonical_tie(tet_v, tet_n, posd, t, zmask, p, st.exact);
@@ -204,16 +202,32 @@ __device__ __forceinline__ int walk_locate(const int4* __restrict__ tet_v, const
       }
       return t;
     }
-    int4 n = __ldg(&tet_n[t]);
-    int nb = nb_of(n, exit_face);
+    int nb = nb_of(__ldg(&tet_n[t]), exit_face);
     if (nb < 0) return kOutside;
-    // remember the face we cross to skip it in the next tetrahedron
-    int k = 0;
-    int f[3];
+    int4 q = __ldg(&tet_v[nb]);
+    int nv[4] = {q.x, q.y, q.z, q.w};
+    float NX[4][3];
+    came = 0;
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
-      if (j != exit_face) f[k++] = v[j];
-    fv0 = f[0]; fv1 = f[1]; fv2 = f[2];
+    for (int j = 0; j < 4; ++j) {
+      int src = -1;
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (k != exit_face && v[k] == nv[j]) src = k;
+      if (src >= 0) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) NX[j][c] = X[src][c];
+      } else {
+        load_posf(posd, nv[j], NX[j]);
+        came = j;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      v[j] = nv[j];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) X[j][c] = NX[j][c];
+    }
     t = nb;
   }
   return kWalkFail;
@@ -247,7 +261,7 @@ struct CellOut {
 
 // Evaluates the requested fields of the located tetrahedron at p.
 template <int S>
-__device__ __forceinline__ void cell_eval(const int v[4], const double X[4][3], const double p[3],
+__device__ __forceinline__ void cell_eval(const int v[4], const float X[4][3], const double p[3],
                                           const float4* __restrict__ posd,
                                           const float4* __restrict__ vel4,
                                           const float* __restrict__ scal, bool want_dens,
@@ -256,12 +270,12 @@ __device__ __forceinline__ void cell_eval(const int v[4], const double X[4][3], 
 #pragma unroll
   for (int r = 0; r < 3; ++r)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) A[r][c] = X[r + 1][c] - X[0][c];
+    for (int c = 0; c < 3; ++c) A[r][c] = (double)X[r + 1][c] - (double)X[0][c];
   float M[3][3];
   matrix_inverse_f(A, M);
   float rel[3];
 #pragma unroll
-  for (int c = 0; c < 3; ++c) rel[c] = (float)(p[c] - X[0][c]);
+  for (int c = 0; c < 3; ++c) rel[c] = (float)(p[c] - (double)X[0][c]);
   if (want_dens) {
     float d0 = __ldg(&posd[v[0]]).w;
     float dd[3];

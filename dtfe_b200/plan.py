@@ -152,6 +152,27 @@ def tessellate_many(point_sets: list, seed: int = 12345, sort_tets: bool = True)
     return out
 
 
+def _spread21(x: np.ndarray) -> np.ndarray:
+    x = x.astype(np.uint64) & np.uint64(0x1FFFFF)
+    x = (x | (x << np.uint64(32))) & np.uint64(0x1F00000000FFFF)
+    x = (x | (x << np.uint64(16))) & np.uint64(0x1F0000FF0000FF)
+    x = (x | (x << np.uint64(8))) & np.uint64(0x100F00F00F00F00F)
+    x = (x | (x << np.uint64(4))) & np.uint64(0x10C30C30C30C30C3)
+    x = (x | (x << np.uint64(2))) & np.uint64(0x1249249249249249)
+    return x
+
+
+def morton_order(pos: np.ndarray) -> np.ndarray:
+    """Permutation sorting points along a Morton (Z-order) curve."""
+    if len(pos) == 0:
+        return np.zeros(0, np.int64)
+    lo = pos.min(axis=0).astype(np.float64)
+    ext = np.maximum(pos.max(axis=0).astype(np.float64) - lo, 1e-30)
+    q = np.clip(((pos - lo) / ext * ((1 << 21) - 1)), 0, (1 << 21) - 1).astype(np.uint64)
+    key = _spread21(q[:, 0]) | (_spread21(q[:, 1]) << np.uint64(1)) | (_spread21(q[:, 2]) << np.uint64(2))
+    return np.argsort(key, kind="stable")
+
+
 def _make_box(voff, nv, toff, nt, origin, dims, coff, dx, lo, part_no):
     b = N.Subbox()
     b.vert_offset, b.n_verts, b.tet_offset, b.n_tets = voff, nv, toff, nt
@@ -170,6 +191,11 @@ def assemble(sets: list, tiles: list, weight, velocity, scalar, grid, rho_bar, p
 
     sets:  [(src_idx int32, pos float32 (n,3))]
     tiles: [(origin(3), dims(3), region(6) float32, part_no)]"""
+    t0 = time.time()
+    # vertices of each sub-box in Morton order: neighbouring tetrahedra then
+    # reference neighbouring vertex records
+    sets = [(src[o], pos[o]) for src, pos in sets for o in [morton_order(pos)]]
+    timings["vertex_sort_s"] = time.time() - t0
     t0 = time.time()
     tess = tessellate_many([p for _, p in sets])
     timings["tessellation_s"] = time.time() - t0

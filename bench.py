@@ -270,6 +270,9 @@ def run_ours(args):
         dev.vertex_density(plan.rho_bar)
         return dev.interpolate_dev(FIELDS, outs, method=0)
 
+    dev.vertex_density(plan.rho_bar)
+    variants = dev.autotune(FIELDS)
+
     for _ in range(args.warmup):
         step()
     dev.synchronize()
@@ -388,6 +391,7 @@ def run_ours(args):
                    "l2": "inputs larger than L2 (tessellation arrays > 126 MB)",
                    "parallelism": f"dp{world} (independent boxes per GPU)"},
         "gpu_launches": 4 * args.steps,
+        "launch_variants": {"locate": variants[0], "eval": variants[1]},
         "clocks": clk,
         "e2e": e2e,
         "roofline": roofline,

@@ -193,13 +193,8 @@ __global__ void __launch_bounds__(kVolBlock) k_tet_volume_bins(
     int64_t T, const int4* __restrict__ tet_v, const float4* __restrict__ posd, double* __restrict__ vol,
     const dtfe_subbox* __restrict__ boxes, const int64_t* __restrict__ tprefix,
     const int64_t* __restrict__ bin_offset, int K, int* __restrict__ bins) {
-  __shared__ int s_bkey[DO_BINS ? kBinSlots : 1];
-  __shared__ int s_bval[DO_BINS ? kBinSlots : 1];
-  if (DO_BINS) {
-    for (int i = threadIdx.x; i < kBinSlots; i += blockDim.x) { s_bkey[i] = -1; s_bval[i] = 0x7FFFFFFF; }
-    __syncthreads();
-  }
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int key = -1;
   if (t < T) {
     int4 q = __ldg(&tet_v[t]);
     int v[4] = {q.x, q.y, q.z, q.w};
@@ -224,36 +219,53 @@ __global__ void __launch_bounds__(kVolBlock) k_tet_volume_bins(
         inside = inside && (f >= 0.f && f < (float)B.tile_dims[c]);
         idx[c] = inside ? (int)f : 0;
       }
-      if (inside) {
-        int key = (int)(__ldg(&bin_offset[b]) +
-                        ((int64_t)idx[0] * B.tile_dims[1] + idx[1]) * B.tile_dims[2] + idx[2]);
-        unsigned h = slot_hash(key, kBinSlots - 1);
-        for (;;) {
-          int k = atomicCAS(&s_bkey[h], -1, key);
-          if (k == -1 || k == key) { atomicMin(&s_bval[h], (int)t); break; }
-          h = (h + 1) & (kBinSlots - 1);
-        }
-      }
+      if (inside)
+        key = (int)(__ldg(&bin_offset[b]) + ((int64_t)idx[0] * B.tile_dims[1] + idx[1]) * B.tile_dims[2] + idx[2]);
     }
   }
   if (DO_BINS) {
-    __syncthreads();
-    for (int i = threadIdx.x; i < kBinSlots; i += blockDim.x)
-      if (s_bkey[i] >= 0) atomicMin(&bins[s_bkey[i]], s_bval[i]);
+    // lanes of a warp that hit the same cell elect one leader, which stores
+    // the group's lowest tetrahedron id with a single atomicMin
+    const unsigned group = __match_any_sync(0xffffffffu, key);
+    const int tmin = __reduce_min_sync(group, t < T ? (int)t : 0x7FFFFFFF);
+    const int leader = __ffs(group) - 1;
+    if (key >= 0 && (int)(threadIdx.x & 31) == leader) atomicMin(&bins[key], tmin);
   }
 }
 
 // rho_v = (w * factor) / sum of incident volumes, summed in ascending
-// tetrahedron order; 0 on the hull or without incident tetrahedra.
-__global__ void k_vertex_density(int64_t V, const float* __restrict__ w, const double* __restrict__ vol,
-                                 const int64_t* __restrict__ off, const int* __restrict__ inc,
-                                 const int* __restrict__ hull, float factor, float4* __restrict__ posd) {
-  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= V) return;
+// tetrahedron order; 0 on the hull or without incident tetrahedra.  A warp
+// handles 32 consecutive vertices, whose incidence lists are contiguous: it
+// stages the lists' volumes in shared memory with coalesced loads (in chunks),
+// then every lane sums its own list sequentially.
+constexpr int kDensBlock = 256;
+constexpr int kDensChunk = 512;  // incidences staged per warp and pass
+__global__ void __launch_bounds__(kDensBlock) k_vertex_density(
+    int64_t V, const float* __restrict__ w, const double* __restrict__ vol, const int64_t* __restrict__ off,
+    const int* __restrict__ inc, const int* __restrict__ hull, float factor, float4* __restrict__ posd) {
+  __shared__ double s_vol[kDensBlock / 32][kDensChunk];
+  const int lane = threadIdx.x & 31;
+  double* sv = s_vol[threadIdx.x >> 5];
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t v0 = i - lane;
+  if (v0 >= V) return;
+  const int64_t vl = (v0 + 32 <= V) ? v0 + 32 : V;  // warp's vertex range [v0, vl)
+  const int64_t beg = __ldg(&off[v0]), end = __ldg(&off[vl]);
+  const bool mine = i < V;
+  const int64_t a = mine ? __ldg(&off[i]) : end, e = mine ? __ldg(&off[i + 1]) : end;
   double sum = 0.0;
-  for (int64_t q = off[i], e = off[i + 1]; q < e; ++q) sum += __ldg(&vol[__ldg(&inc[q])]);
-  float d = (hull[i] || sum == 0.0) ? 0.f : (float)((double)(w[i] * factor) / sum);
-  posd[i].w = d;
+  int64_t cur = a;  // next incidence of this lane to add
+  for (int64_t base = beg; base < end; base += kDensChunk) {
+    const int64_t lim = (end - base < kDensChunk) ? end : base + kDensChunk;
+    __syncwarp();
+    for (int64_t q = base + lane; q < lim; q += 32) sv[q - base] = __ldg(&vol[__ldg(&inc[q])]);
+    __syncwarp();
+    for (; cur < e && cur < lim; ++cur) sum += sv[cur - base];
+  }
+  if (mine) {
+    float d = (hull[i] || sum == 0.0) ? 0.f : (float)((double)(w[i] * factor) / sum);
+    posd[i].w = d;
+  }
 }
 
 // Offsets of the 26 neighbouring cells, nearest first (faces, edges, corners).
@@ -317,8 +329,174 @@ __device__ __forceinline__ void store_field(float* __restrict__ out, int64_t cel
 
 constexpr int kInterpBlock = 256;
 
+// Geometry of flattened sample s (tile order: sub-box, then x, y, z fastest).
+struct SampleCell {
+  int b, i, j, k;
+  int64_t local, cell;
+  float x, y, z;
+};
+
+__device__ __forceinline__ SampleCell sample_cell(const InterpParams& P, int64_t s) {
+  SampleCell c;
+  c.b = find_box(P.tile_prefix, P.K, s);
+  const dtfe_subbox& B = P.boxes[c.b];
+  c.local = s - __ldg(&P.tile_prefix[c.b]);
+  const int nz = B.tile_dims[2], ny = B.tile_dims[1];
+  c.k = (int)(c.local % nz);
+  c.j = (int)((c.local / nz) % ny);
+  c.i = (int)(c.local / ((int64_t)nz * ny));
+  c.x = __ldg(&P.xs[B.coord_offset[0] + c.i]);
+  c.y = __ldg(&P.ys[B.coord_offset[1] + c.j]);
+  c.z = __ldg(&P.zs[B.coord_offset[2] + c.k]);
+  c.cell = ((int64_t)(B.tile_origin[0] + c.i) * P.G1 + (B.tile_origin[1] + c.j)) * P.G2 + (B.tile_origin[2] + c.k);
+  return c;
+}
+
+__device__ __forceinline__ void fold_counters(const InterpParams& P, unsigned n_loc, unsigned n_out, unsigned n_fail,
+                                              const WalkStats& st) {
+  unsigned vals[CNT_N] = {n_loc, n_out, n_fail, (unsigned)st.steps, (unsigned)st.exact, (unsigned)st.tie};
+#pragma unroll
+  for (int c = 0; c < CNT_N; ++c) {
+    unsigned r = __reduce_add_sync(0xffffffffu, vals[c]);
+    if ((threadIdx.x & 31) == 0 && r) atomicAdd(&P.counters[c], (unsigned long long)r);
+  }
+}
+
+// Point location of every cell centre: seed from the cell's bin (the lowest
+// tetrahedron whose centroid lies in the cell, else in the nearest of the 26
+// neighbouring cells that has one), then the walk.  Writes the canonical
+// tetrahedron (or kOutside) per sample.  Each thread locates R consecutive
+// samples; within one z pencil the next sample starts from the previous hit
+// (the reference's raster hint) instead of its bin.
+template <int R>
+__device__ __forceinline__ void locate_cells_body(const InterpParams& P, int* __restrict__ tet_c) {
+  WalkStats st{0, 0, 0};
+  unsigned n_loc = 0, n_out = 0, n_fail = 0;
+  const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+  const int64_t n_groups = (P.n_total + R - 1) / R;
+  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  for (int64_t g0 = tid - (threadIdx.x & 31); g0 < n_groups; g0 += nthreads) {
+    const int64_t g = g0 + (threadIdx.x & 31);
+    int prev_hit = -1, prev_b = -1, prev_j = -1, prev_i = -1;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int64_t s = g * R + r;
+      if (g >= n_groups || s >= P.n_total) break;
+      const SampleCell c = sample_cell(P, s);
+      const dtfe_subbox& B = P.boxes[c.b];
+      int t0;
+      if (r > 0 && prev_hit >= 0 && prev_b == c.b && prev_j == c.j && prev_i == c.i) {
+        t0 = prev_hit;
+      } else {
+        const int* bins = P.bins + __ldg(&P.bin_offset[c.b]);
+        t0 = __ldg(&bins[c.local]);
+        if (t0 >= kEmptyBin) {
+          const int nx = B.tile_dims[0], ny = B.tile_dims[1], nz = B.tile_dims[2];
+          for (int q = 0; q < 26 && t0 >= kEmptyBin; ++q) {
+            const int ii = c.i + c_nbr[q][0], jj = c.j + c_nbr[q][1], kk = c.k + c_nbr[q][2];
+            if (ii < 0 || jj < 0 || kk < 0 || ii >= nx || jj >= ny || kk >= nz) continue;
+            t0 = __ldg(&bins[((int64_t)ii * ny + jj) * nz + kk]);
+          }
+        }
+        if (t0 < B.tet_offset || t0 >= B.tet_offset + B.n_tets) t0 = (int)B.tet_offset;
+      }
+      const double pc[3] = {(double)c.x, (double)c.y, (double)c.z};
+      int v[4];
+      float X[4][3];
+      int tc = walk_locate<true>(P.tet_v, P.tet_n, P.posd, pc, t0, P.max_steps, v, X, st);
+      ++n_loc;
+      if (tc == kWalkFail) { ++n_fail; tc = kOutside; }
+      if (tc < 0) ++n_out;
+      tet_c[s] = tc;
+      prev_hit = tc;
+      prev_b = c.b;
+      prev_j = c.j;
+      prev_i = c.i;
+    }
+  }
+  fold_counters(P, n_loc, n_out, n_fail, st);
+}
+
+template <int BS, int MINB, int R>
+__global__ void __launch_bounds__(BS, MINB) k_locate_cells(InterpParams P, int* __restrict__ tet_c) {
+  locate_cells_body<R>(P, tet_c);
+}
+
+// Field evaluation at the located cell centres (method 0): every lane does
+// the same work, so the warp stays converged.
+template <int S, int MINB>
+__global__ void __launch_bounds__(kInterpBlock, MINB) k_eval_centre(InterpParams P, const int* __restrict__ tet_c) {
+  constexpr int CMAX = (3 * S > 9) ? 3 * S : 9;
+  __shared__ __align__(16) float s_stage[kInterpBlock / 32][32 * CMAX];
+  float* stage = s_stage[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const uint32_t F = P.fields;
+  const bool want_grad = has_field(F, DTFE_VELOCITY_GRADIENT) || has_field(F, DTFE_VELOCITY_DIVERGENCE) ||
+                         has_field(F, DTFE_VELOCITY_SHEAR) || has_field(F, DTFE_VELOCITY_VORTICITY);
+  const bool want_vel = has_field(F, DTFE_VELOCITY) || want_grad;
+  const bool want_dens = has_field(F, DTFE_DENSITY);
+  const bool want_sc = S > 0 && (has_field(F, DTFE_SCALAR) || has_field(F, DTFE_SCALAR_GRADIENT));
+  const bool fix = P.fix != 0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t base0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane;
+  for (int64_t base = base0; base < P.n_total; base += stride) {
+    const int64_t s = base + lane;
+    const bool valid = s < P.n_total;
+    int64_t cell = -1;
+    CellOut e;
+    e.dens = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) e.vel[c] = 0.f;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) e.grad[c] = 0.f;
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+      e.sc[q] = 0.f;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) e.scg[3 * q + c] = 0.f;
+    }
+    if (valid) {
+      const SampleCell c = sample_cell(P, s);
+      cell = c.cell;
+      const int t = __ldg(&tet_c[s]);
+      if (t >= 0) {
+        int v[4];
+        float X[4][3];
+        load_tet(P.tet_v, P.posd, t, v, X);
+        const double pc[3] = {(double)c.x, (double)c.y, (double)c.z};
+        cell_eval<S>(v, X, pc, P.posd, P.vel4, P.scal, want_dens, want_vel, want_sc, fix, e);
+      }
+    }
+    const int64_t c0 = __shfl_sync(0xffffffffu, cell, 0);
+    const bool contig = __all_sync(0xffffffffu, valid && cell == c0 + lane) && (c0 % 4 == 0);
+    if (has_field(F, DTFE_DENSITY)) store_field<1>(P.out[DTFE_DENSITY], cell, valid, &e.dens, contig, c0, stage);
+    if (has_field(F, DTFE_VELOCITY)) store_field<3>(P.out[DTFE_VELOCITY], cell, valid, e.vel, contig, c0, stage);
+    if (has_field(F, DTFE_VELOCITY_GRADIENT))
+      store_field<9>(P.out[DTFE_VELOCITY_GRADIENT], cell, valid, e.grad, contig, c0, stage);
+    if (has_field(F, DTFE_VELOCITY_DIVERGENCE) || has_field(F, DTFE_VELOCITY_SHEAR) ||
+        has_field(F, DTFE_VELOCITY_VORTICITY)) {
+      float dv, sh[5], vo[3];
+      derived_fields(e.grad, dv, sh, vo);
+      if (has_field(F, DTFE_VELOCITY_DIVERGENCE))
+        store_field<1>(P.out[DTFE_VELOCITY_DIVERGENCE], cell, valid, &dv, contig, c0, stage);
+      if (has_field(F, DTFE_VELOCITY_SHEAR))
+        store_field<5>(P.out[DTFE_VELOCITY_SHEAR], cell, valid, sh, contig, c0, stage);
+      if (has_field(F, DTFE_VELOCITY_VORTICITY))
+        store_field<3>(P.out[DTFE_VELOCITY_VORTICITY], cell, valid, vo, contig, c0, stage);
+    }
+    if (S > 0 && has_field(F, DTFE_SCALAR))
+      store_field<(S > 0 ? S : 1)>(P.out[DTFE_SCALAR], cell, valid, e.sc, contig, c0, stage);
+    if (S > 0 && has_field(F, DTFE_SCALAR_GRADIENT))
+      store_field<(S > 0 ? 3 * S : 1)>(P.out[DTFE_SCALAR_GRADIENT], cell, valid, e.scg, contig, c0, stage);
+  }
+}
+
+// Cell averages (methods 2 and 3): n points per cell, each walked from the
+// cell centre's tetrahedron (averaged_interpolation_2.cc:123,145), summed in
+// sample order as the reference does, divided by n; infinite-cell points are
+// skipped but counted.
 template <int METHOD, int S>
-__global__ void __launch_bounds__(kInterpBlock) k_interpolate(InterpParams P) {
+__global__ void __launch_bounds__(kInterpBlock) k_average(InterpParams P, const int* __restrict__ tet_c) {
   constexpr int CMAX = (3 * S > 9) ? 3 * S : 9;
   __shared__ __align__(16) float s_stage[kInterpBlock / 32][32 * CMAX];
   float* stage = s_stage[threadIdx.x >> 5];
@@ -332,11 +510,11 @@ __global__ void __launch_bounds__(kInterpBlock) k_interpolate(InterpParams P) {
   const bool want_std = METHOD == DTFE_METHOD_MONTE_CARLO && has_field(F, DTFE_VELOCITY_STD);
   const bool fix = P.fix != 0;
   WalkStats st{0, 0, 0};
-  unsigned n_loc = 0, n_out = 0, n_fail = 0;
+  unsigned n_loc = 0, n_fail = 0;
 
-  const int64_t warp_stride = (int64_t)gridDim.x * blockDim.x;
-  const int64_t warp_base0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane;
-  for (int64_t base = warp_base0; base < P.n_total; base += warp_stride) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t base0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane;
+  for (int64_t base = base0; base < P.n_total; base += stride) {
     const int64_t s = base + lane;
     const bool valid = s < P.n_total;
     int64_t cell = -1;
@@ -350,148 +528,99 @@ __global__ void __launch_bounds__(kInterpBlock) k_interpolate(InterpParams P) {
     for (int q = 0; q < (S > 0 ? 3 * S : 1); ++q) aSG[q] = 0.f;
 
     if (valid) {
-      const int b = find_box(P.tile_prefix, P.K, s);
-      const dtfe_subbox& B = P.boxes[b];
-      const int64_t local = s - __ldg(&P.tile_prefix[b]);
-      const int nz = B.tile_dims[2], ny = B.tile_dims[1];
-      const int k = (int)(local % nz);
-      const int j = (int)((local / nz) % ny);
-      const int i = (int)(local / ((int64_t)nz * ny));
-      const float x = __ldg(&P.xs[B.coord_offset[0] + i]);
-      const float y = __ldg(&P.ys[B.coord_offset[1] + j]);
-      const float z = __ldg(&P.zs[B.coord_offset[2] + k]);
-      cell = ((int64_t)(B.tile_origin[0] + i) * P.G1 + (B.tile_origin[1] + j)) * P.G2 + (B.tile_origin[2] + k);
-      // seed: the lowest tetrahedron whose centroid lies in this cell, else in
-      // the nearest cell of the surrounding 3x3x3 block that has one
-      const int* bins = P.bins + __ldg(&P.bin_offset[b]);
-      int t0 = __ldg(&bins[local]);
-      if (t0 >= kEmptyBin) {
-        const int nx = B.tile_dims[0];
-        for (int r = 0; r < 26 && t0 >= kEmptyBin; ++r) {
-          const int ii = i + c_nbr[r][0], jj = j + c_nbr[r][1], kk = k + c_nbr[r][2];
-          if (ii < 0 || jj < 0 || kk < 0 || ii >= nx || jj >= ny || kk >= nz) continue;
-          t0 = __ldg(&bins[((int64_t)ii * ny + jj) * nz + kk]);
-        }
-      }
-      if (t0 < B.tet_offset || t0 >= B.tet_offset + B.n_tets) t0 = (int)B.tet_offset;
-
-      const double pc[3] = {(double)x, (double)y, (double)z};
-      int v[4];
-      float X[4][3];
-      int tc = walk_locate(P.tet_v, P.tet_n, P.posd, pc, t0, P.max_steps, v, X, st);
-      ++n_loc;
-      if (tc == kWalkFail) { ++n_fail; tc = kOutside; }
-
-      if (METHOD == DTFE_METHOD_CENTRE) {
-        if (tc >= 0) {
-          CellOut e;
-          cell_eval<S>(v, X, pc, P.posd, P.vel4, P.scal, want_dens, want_vel, want_sc, fix, e);
-          aD = e.dens;
-#pragma unroll
-          for (int c = 0; c < 3; ++c) aV[c] = e.vel[c];
-#pragma unroll
-          for (int c = 0; c < 9; ++c) aG[c] = e.grad[c];
-#pragma unroll
-          for (int q = 0; q < S; ++q) {
-            aS[q] = e.sc[q];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) aSG[3 * q + c] = e.scg[3 * q + c];
-          }
+      const SampleCell c = sample_cell(P, s);
+      const dtfe_subbox& B = P.boxes[c.b];
+      cell = c.cell;
+      const double pc[3] = {(double)c.x, (double)c.y, (double)c.z};
+      const int tc = __ldg(&tet_c[s]);
+      const int tstart = tc >= 0 ? tc : (int)B.tet_offset;
+      const int NN = P.NN;
+      const uint64_t key = mc_key(P.seed, B.part_no);
+      float stdacc[3] = {0.f, 0.f, 0.f};
+      for (int w = 0; w < NN; ++w) {
+        double p[3];
+        if (METHOD == DTFE_METHOD_MONTE_CARLO) {
+          double u[3];
+          mc_offsets(key, (uint64_t)cell, (uint32_t)w, u);
+          p[0] = u[0] * (double)B.dx[0] + pc[0];
+          p[1] = u[1] * (double)B.dx[1] + pc[1];
+          p[2] = u[2] * (double)B.dx[2] + pc[2];
         } else {
-          ++n_out;
+          const float* eo = P.eq_off + ((int64_t)c.b * NN + w) * 3;
+          p[0] = (double)(c.x + __ldg(&eo[0]));
+          p[1] = (double)(c.y + __ldg(&eo[1]));
+          p[2] = (double)(c.z + __ldg(&eo[2]));
         }
-      } else {
-        if (tc < 0) ++n_out;
-        const int NN = P.NN;
-        const uint64_t key = mc_key(P.seed, B.part_no);
-        const int tstart = tc >= 0 ? tc : t0;
-        float stdacc[3] = {0.f, 0.f, 0.f};
-        for (int w = 0; w < NN; ++w) {
-          double p[3];
-          if (METHOD == DTFE_METHOD_MONTE_CARLO) {
-            double u[3];
-            mc_offsets(key, (uint64_t)cell, (uint32_t)w, u);
-            p[0] = u[0] * (double)B.dx[0] + pc[0];
-            p[1] = u[1] * (double)B.dx[1] + pc[1];
-            p[2] = u[2] * (double)B.dx[2] + pc[2];
-          } else {
-            const float* eo = P.eq_off + ((int64_t)b * NN + w) * 3;
-            p[0] = (double)(x + __ldg(&eo[0]));
-            p[1] = (double)(y + __ldg(&eo[1]));
-            p[2] = (double)(z + __ldg(&eo[2]));
-          }
-          int vv[4];
-          float XX[4][3];
-          int t = walk_locate(P.tet_v, P.tet_n, P.posd, p, tstart, P.max_steps, vv, XX, st);
-          ++n_loc;
-          if (t == kWalkFail) { ++n_fail; t = kOutside; }
-          if (t < 0) continue;
-          CellOut e;
-          cell_eval<S>(vv, XX, p, P.posd, P.vel4, P.scal, want_dens, want_vel, want_sc, fix, e);
-          aD += e.dens;
+        int vv[4];
+        float XX[4][3];
+        int t = walk_locate(P.tet_v, P.tet_n, P.posd, p, tstart, P.max_steps, vv, XX, st);
+        ++n_loc;
+        if (t == kWalkFail) { ++n_fail; t = kOutside; }
+        if (t < 0) continue;
+        CellOut e;
+        cell_eval<S>(vv, XX, p, P.posd, P.vel4, P.scal, want_dens, want_vel, want_sc, fix, e);
+        aD += e.dens;
 #pragma unroll
-          for (int c = 0; c < 3; ++c) aV[c] += e.vel[c];
+        for (int q = 0; q < 3; ++q) aV[q] += e.vel[q];
 #pragma unroll
-          for (int c = 0; c < 9; ++c) aG[c] += e.grad[c];
-#pragma unroll
-          for (int q = 0; q < S; ++q) {
-            aS[q] += e.sc[q];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) aSG[3 * q + c] += e.scg[3 * q + c];
-          }
-          if (want_std) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c) stdacc[c] += e.vel[c];
-          }
-        }
-        const float fn = (float)NN;
-        aD = aD / fn;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) aV[c] = aV[c] / fn;
-#pragma unroll
-        for (int c = 0; c < 9; ++c) aG[c] = aG[c] / fn;
+        for (int q = 0; q < 9; ++q) aG[q] += e.grad[q];
 #pragma unroll
         for (int q = 0; q < S; ++q) {
-          aS[q] = aS[q] / fn;
+          aS[q] += e.sc[q];
 #pragma unroll
-          for (int c = 0; c < 3; ++c) aSG[3 * q + c] = aSG[3 * q + c] / fn;
+          for (int r = 0; r < 3; ++r) aSG[3 * q + r] += e.scg[3 * q + r];
         }
         if (want_std) {
-          // standardDeviation (triangulation_miscellaneous.cc:256-271): the
-          // second pass re-walks the samples (their velocities are not kept)
-          float mean[3];
 #pragma unroll
-          for (int c = 0; c < 3; ++c) mean[c] = stdacc[c] / fn;
-          float r = 0.f;
-          for (int w = 0; w < NN; ++w) {
-            float vel[3] = {0.f, 0.f, 0.f};
-            double u[3], p[3];
-            mc_offsets(key, (uint64_t)cell, (uint32_t)w, u);
-            p[0] = u[0] * (double)B.dx[0] + pc[0];
-            p[1] = u[1] * (double)B.dx[1] + pc[1];
-            p[2] = u[2] * (double)B.dx[2] + pc[2];
-            int vv[4];
-            float XX[4][3];
-            WalkStats st2{0, 0, 0};
-            int t = walk_locate(P.tet_v, P.tet_n, P.posd, p, tstart, P.max_steps, vv, XX, st2);
-            if (t >= 0) {
-              CellOut e;
-              cell_eval<0>(vv, XX, p, P.posd, P.vel4, P.scal, false, true, false, fix, e);
-#pragma unroll
-              for (int c = 0; c < 3; ++c) vel[c] = e.vel[c];
-            }
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-              float d = vel[c] - mean[c];
-              r += d * d;
-            }
-          }
-          sdev = sqrtf(r / fn);
+          for (int q = 0; q < 3; ++q) stdacc[q] += e.vel[q];
         }
+      }
+      const float fn = (float)NN;
+      aD = aD / fn;
+#pragma unroll
+      for (int q = 0; q < 3; ++q) aV[q] = aV[q] / fn;
+#pragma unroll
+      for (int q = 0; q < 9; ++q) aG[q] = aG[q] / fn;
+#pragma unroll
+      for (int q = 0; q < S; ++q) {
+        aS[q] = aS[q] / fn;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) aSG[3 * q + r] = aSG[3 * q + r] / fn;
+      }
+      if (want_std) {
+        // standardDeviation (triangulation_miscellaneous.cc:256-271); the
+        // second pass re-walks the samples (their velocities are not kept)
+        float mean[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) mean[q] = stdacc[q] / fn;
+        float r = 0.f;
+        for (int w = 0; w < NN; ++w) {
+          float vel[3] = {0.f, 0.f, 0.f};
+          double u[3], p[3];
+          mc_offsets(key, (uint64_t)cell, (uint32_t)w, u);
+          p[0] = u[0] * (double)B.dx[0] + pc[0];
+          p[1] = u[1] * (double)B.dx[1] + pc[1];
+          p[2] = u[2] * (double)B.dx[2] + pc[2];
+          int vv[4];
+          float XX[4][3];
+          WalkStats st2{0, 0, 0};
+          int t = walk_locate(P.tet_v, P.tet_n, P.posd, p, tstart, P.max_steps, vv, XX, st2);
+          if (t >= 0) {
+            CellOut e;
+            cell_eval<0>(vv, XX, p, P.posd, P.vel4, P.scal, false, true, false, fix, e);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) vel[q] = e.vel[q];
+          }
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            float d = vel[q] - mean[q];
+            r += d * d;
+          }
+        }
+        sdev = sqrtf(r / fn);
       }
     }
 
-    // ---- stores: contiguous warps go through shared memory -----------------
     const int64_t c0 = __shfl_sync(0xffffffffu, cell, 0);
     const bool contig = __all_sync(0xffffffffu, valid && cell == c0 + lane) && (c0 % 4 == 0);
     if (has_field(F, DTFE_DENSITY)) store_field<1>(P.out[DTFE_DENSITY], cell, valid, &aD, contig, c0, stage);
@@ -515,13 +644,7 @@ __global__ void __launch_bounds__(kInterpBlock) k_interpolate(InterpParams P) {
     if (S > 0 && has_field(F, DTFE_SCALAR_GRADIENT))
       store_field<(S > 0 ? 3 * S : 1)>(P.out[DTFE_SCALAR_GRADIENT], cell, valid, aSG, contig, c0, stage);
   }
-  // fold the per-thread counters into the global ones, one atomic per warp
-  unsigned vals[CNT_N] = {n_loc, n_out, n_fail, (unsigned)st.steps, (unsigned)st.exact, (unsigned)st.tie};
-#pragma unroll
-  for (int c = 0; c < CNT_N; ++c) {
-    unsigned r = __reduce_add_sync(0xffffffffu, vals[c]);
-    if (lane == 0 && r) atomicAdd(&P.counters[c], (unsigned long long)r);
-  }
+  fold_counters(P, n_loc, 0, n_fail, st);
 }
 
 // Locate arbitrary points (tests): canonical tetrahedron or -1 / -2.
@@ -569,6 +692,9 @@ struct dtfe_gpu_s {
   int64_t* tet_prefix = nullptr;  // K+1 tetrahedron range starts
   int64_t* bin_offset = nullptr;
   int* bins = nullptr;
+  int* tet_c = nullptr;   // located tetrahedron of every cell centre
+  int loc_variant = 0;    // launch variants (dtfe_gpu_autotune)
+  int eval_variant = 0;
   int64_t n_cells = 0;
   float *xs = nullptr, *ys = nullptr, *zs = nullptr;
   int32_t grid[3] = {0, 0, 0};
@@ -633,15 +759,52 @@ int prepare_bins(dtfe_handle h) {
   return DTFE_OK;
 }
 
-template <int METHOD>
-void launch_interp_s(const InterpParams& P, int S, cudaStream_t st, unsigned grid, unsigned block) {
+// Launch variants chosen by dtfe_gpu_autotune: register budget (blocks per
+// SM) and seeding schedule of the locate kernel; register budget of the
+// evaluation kernel.
+struct LocVariant { int block, minb, r; };
+constexpr LocVariant kLocVariants[] = {{256, 3, 1}, {256, 2, 1}, {256, 4, 1}, {256, 3, 2}, {256, 4, 2}, {256, 3, 4}};
+constexpr int kNumLocVariants = sizeof(kLocVariants) / sizeof(kLocVariants[0]);
+constexpr int kEvalMinBlocks[] = {3, 2, 4};
+constexpr int kNumEvalVariants = 3;
+
+void launch_locate(int variant, const InterpParams& P, int* tet_c, cudaStream_t st) {
+  const LocVariant& L = kLocVariants[variant];
+  const int64_t groups = (P.n_total + L.r - 1) / L.r;
+  const unsigned grid = (unsigned)((groups + L.block - 1) / L.block);
+  switch (variant) {
+    case 0: k_locate_cells<256, 3, 1><<<grid, 256, 0, st>>>(P, tet_c); break;
+    case 1: k_locate_cells<256, 2, 1><<<grid, 256, 0, st>>>(P, tet_c); break;
+    case 2: k_locate_cells<256, 4, 1><<<grid, 256, 0, st>>>(P, tet_c); break;
+    case 3: k_locate_cells<256, 3, 2><<<grid, 256, 0, st>>>(P, tet_c); break;
+    case 4: k_locate_cells<256, 4, 2><<<grid, 256, 0, st>>>(P, tet_c); break;
+    default: k_locate_cells<256, 3, 4><<<grid, 256, 0, st>>>(P, tet_c); break;
+  }
+}
+
+template <int S>
+void launch_eval(int method, int evariant, const InterpParams& P, const int* tet_c, cudaStream_t st, unsigned grid,
+                 unsigned block) {
+  if (method == DTFE_METHOD_CENTRE) {
+    if (evariant == 1) k_eval_centre<S, 2><<<grid, block, 0, st>>>(P, tet_c);
+    else if (evariant == 2) k_eval_centre<S, 4><<<grid, block, 0, st>>>(P, tet_c);
+    else k_eval_centre<S, 3><<<grid, block, 0, st>>>(P, tet_c);
+  } else if (method == DTFE_METHOD_MONTE_CARLO) {
+    k_average<DTFE_METHOD_MONTE_CARLO, S><<<grid, block, 0, st>>>(P, tet_c);
+  } else {
+    k_average<DTFE_METHOD_EQUIDISTANT, S><<<grid, block, 0, st>>>(P, tet_c);
+  }
+}
+
+void launch_eval_s(int method, int S, int evariant, const InterpParams& P, const int* tet_c, cudaStream_t st,
+                   unsigned grid, unsigned block) {
   switch (S) {
-    case 0: k_interpolate<METHOD, 0><<<grid, block, 0, st>>>(P); break;
-    case 1: k_interpolate<METHOD, 1><<<grid, block, 0, st>>>(P); break;
-    case 2: k_interpolate<METHOD, 2><<<grid, block, 0, st>>>(P); break;
-    case 3: k_interpolate<METHOD, 3><<<grid, block, 0, st>>>(P); break;
-    case 4: k_interpolate<METHOD, 4><<<grid, block, 0, st>>>(P); break;
-    default: k_interpolate<METHOD, 8><<<grid, block, 0, st>>>(P); break;
+    case 0: launch_eval<0>(method, evariant, P, tet_c, st, grid, block); break;
+    case 1: launch_eval<1>(method, evariant, P, tet_c, st, grid, block); break;
+    case 2: launch_eval<2>(method, evariant, P, tet_c, st, grid, block); break;
+    case 3: launch_eval<3>(method, evariant, P, tet_c, st, grid, block); break;
+    case 4: launch_eval<4>(method, evariant, P, tet_c, st, grid, block); break;
+    default: launch_eval<8>(method, evariant, P, tet_c, st, grid, block); break;
   }
 }
 
@@ -692,7 +855,7 @@ int dtfe_gpu_destroy(dtfe_handle h) {
   void* ptrs[] = {h->tet_v, h->tet_n, h->posd, h->vel4, h->scal, h->w, h->vol, h->inc_off, h->inc,
                   h->scratch_i, h->scan_blocks, h->hull,
                   h->boxes, h->tile_prefix, h->tet_prefix, h->bin_offset, h->bins,
-                  h->xs, h->ys, h->zs, h->eq_off, h->counters};
+                  h->xs, h->ys, h->zs, h->eq_off, h->counters, h->tet_c};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < DTFE_NUM_FIELDS; ++i)
@@ -855,8 +1018,8 @@ int dtfe_gpu_vertex_density(dtfe_handle h, double rho_bar) {
   // the reference's factor: (NO_DIM+1.)/averageDensity stored as Real
   float rb = (float)rho_bar;
   float factor = (float)(4.0 / (double)rb);
-  k_vertex_density<<<blocks_for(h->V, 256), 256, 0, st>>>(h->V, h->w, h->vol, h->inc_off, h->inc, h->hull,
-                                                           factor, h->posd);
+  k_vertex_density<<<blocks_for(h->V, kDensBlock), kDensBlock, 0, st>>>(h->V, h->w, h->vol, h->inc_off, h->inc,
+                                                                       h->hull, factor, h->posd);
   DTFE_CUDA_TRY(cudaGetLastError());
   h->density_ready = true;
   h->bins_ready = h->K > 0;
@@ -952,9 +1115,9 @@ static int interpolate_impl(dtfe_handle h, const dtfe_interp_opts* o, float* con
   for (int q = 0; q < DTFE_NUM_FIELDS; ++q)
     if (P.out[q] && ((uintptr_t)P.out[q] & 15))
       return set_error(DTFE_ERR_ARG, "output buffers must be 16-byte aligned");
-  if (method == DTFE_METHOD_CENTRE) launch_interp_s<DTFE_METHOD_CENTRE>(P, h->S, st, grid, block);
-  else if (method == DTFE_METHOD_MONTE_CARLO) launch_interp_s<DTFE_METHOD_MONTE_CARLO>(P, h->S, st, grid, block);
-  else launch_interp_s<DTFE_METHOD_EQUIDISTANT>(P, h->S, st, grid, block);
+  if ((rc = dev_alloc(h, &h->tet_c, h->n_cells))) return rc;
+  launch_locate(h->loc_variant, P, h->tet_c, st);
+  launch_eval_s(method, h->S, h->eval_variant, P, h->tet_c, st, grid, block);
   DTFE_CUDA_TRY(cudaGetLastError());
   unsigned long long cnt[CNT_N];
   DTFE_CUDA_TRY(cudaMemcpyAsync(cnt, h->counters, sizeof(cnt), cudaMemcpyDeviceToHost, st));
@@ -968,6 +1131,87 @@ static int interpolate_impl(dtfe_handle h, const dtfe_interp_opts* o, float* con
     status->n_ties = (int64_t)cnt[CNT_TIES];
   }
   if (cnt[CNT_FAIL]) return set_error(DTFE_ERR_WALK, "point-location walk hit its step limit");
+  return DTFE_OK;
+}
+
+// Times every launch variant of the locate and evaluation kernels on the
+// loaded data (cell-centre method, the given fields, into scratch outputs) and
+// keeps the fastest of each.  chosen (may be NULL) receives the two indices.
+static int autotune_impl(dtfe_handle h, uint32_t fields, int32_t* chosen) {
+  if (!h->density_ready) return set_error(DTFE_ERR_STATE, "vertex density not computed");
+  if (h->K == 0) return set_error(DTFE_ERR_STATE, "sub-boxes not set");
+  const int64_t G = (int64_t)h->grid[0] * h->grid[1] * h->grid[2];
+  float* dev[DTFE_NUM_FIELDS] = {};
+  for (int s = 0; s < DTFE_NUM_FIELDS; ++s) {
+    if (!(fields >> s & 1u)) continue;
+    size_t need = (size_t)G * field_components(s, h->S);
+    int rc = dev_alloc(h, &h->out_buf[s], need);
+    if (rc) return rc;
+    h->out_cap[s] = std::max(h->out_cap[s], need);
+    dev[s] = h->out_buf[s];
+  }
+  dtfe_interp_opts o = {DTFE_METHOD_CENTRE, 1, 0, fields, 0};
+  cudaEvent_t e0, e1;
+  DTFE_CUDA_TRY(cudaEventCreate(&e0));
+  DTFE_CUDA_TRY(cudaEventCreate(&e1));
+  auto time_call = [&](float* ms) -> int {
+    int rc = interpolate_impl(h, &o, dev, nullptr);  // warm
+    if (rc) return rc;
+    float best = 1e30f;
+    for (int rep = 0; rep < 3; ++rep) {
+      cudaEventRecord(e0, h->stream);
+      rc = interpolate_impl(h, &o, dev, nullptr);
+      if (rc) return rc;
+      cudaEventRecord(e1, h->stream);
+      cudaEventSynchronize(e1);
+      float t = 0.f;
+      cudaEventElapsedTime(&t, e0, e1);
+      best = std::min(best, t);
+    }
+    *ms = best;
+    return DTFE_OK;
+  };
+  int rc = DTFE_OK;
+  float best = 1e30f;
+  int best_loc = 0, best_eval = 0;
+  h->eval_variant = 0;
+  for (int v = 0; v < kNumLocVariants && !rc; ++v) {
+    h->loc_variant = v;
+    float t;
+    rc = time_call(&t);
+    if (!rc && t < best) { best = t; best_loc = v; }
+  }
+  h->loc_variant = best_loc;
+  best = 1e30f;
+  for (int v = 0; v < kNumEvalVariants && !rc; ++v) {
+    h->eval_variant = v;
+    float t;
+    rc = time_call(&t);
+    if (!rc && t < best) { best = t; best_eval = v; }
+  }
+  h->eval_variant = best_eval;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (chosen) {
+    chosen[0] = best_loc;
+    chosen[1] = best_eval;
+  }
+  return rc;
+}
+
+int dtfe_gpu_autotune(dtfe_handle h, uint32_t fields, int32_t* chosen) {
+  if (!h) return set_error(DTFE_ERR_ARG, "null handle");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  return autotune_impl(h, fields, chosen);
+}
+
+int dtfe_gpu_set_variants(dtfe_handle h, int32_t locate_variant, int32_t eval_variant) {
+  if (!h) return set_error(DTFE_ERR_ARG, "null handle");
+  if (locate_variant < 0 || locate_variant >= kNumLocVariants || eval_variant < 0 ||
+      eval_variant >= kNumEvalVariants)
+    return set_error(DTFE_ERR_ARG, "unknown launch variant");
+  h->loc_variant = locate_variant;
+  h->eval_variant = eval_variant;
   return DTFE_OK;
 }
 

@@ -44,6 +44,18 @@ __device__ __forceinline__ void load_pos(const float4* __restrict__ posd, int v,
   X[2] = (double)q.z;
 }
 
+// Exact sign of orient(tetrahedron with vertex `face` replaced by p).  All
+// arguments by value: the caller's arrays stay in registers.
+__device__ __noinline__ int exact_face_sign(float x0, float y0, float z0, float x1, float y1, float z1,
+                                            float x2, float y2, float z2, float x3, float y3, float z3,
+                                            double px, double py, double pz, int face) {
+  double Q[4][3] = {{x0, y0, z0}, {x1, y1, z1}, {x2, y2, z2}, {x3, y3, z3}};
+  Q[face][0] = px;
+  Q[face][1] = py;
+  Q[face][2] = pz;
+  return orient_exact(Q[0], Q[1], Q[2], Q[3]);
+}
+
 // Sign of one face orientation from a determinant and its permanent; exact
 // re-evaluation (orient_exact with the definition's argument order) when the
 // filter cannot decide.
@@ -53,14 +65,8 @@ __device__ __forceinline__ int filtered_sign(double det, double perm, int face, 
   if (det > b) return 1;
   if (-det > b) return -1;
   ++nexact;
-  double Q[4][3];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) Q[a][c] = (double)X[a][c];
-  const double* q[4] = {Q[0], Q[1], Q[2], Q[3]};
-  q[face] = p;
-  return orient_exact(q[0], q[1], q[2], q[3]);
+  return exact_face_sign(X[0][0], X[0][1], X[0][2], X[1][0], X[1][1], X[1][2], X[2][0], X[2][1], X[2][2],
+                         X[3][0], X[3][1], X[3][2], p[0], p[1], p[2], face);
 }
 
 // Face orientations o_i = orient(tetrahedron with vertex i replaced by p) for
@@ -120,6 +126,103 @@ __device__ __forceinline__ int first_exit_face(const float X[4][3], const double
   return -1;
 }
 
+// FP32 stage of the orientation filter for points that are exact floats
+// (cell centres, equidistant points).  Same evaluation as first_exit_face in
+// single precision; its forward error is below kOrientErr32 times the
+// permanent (the FP64 bound's constant applied to the float unit roundoff,
+// with a floor against underflow).  Faces the FP32 bound cannot decide are
+// re-evaluated by the FP64 filter and, if needed, exactly.
+constexpr float kOrientErr32 = 12.0f * 5.9604645e-8f;  // 12 * 2^-24
+constexpr float kPermFloor32 = 1e-30f;
+
+// Returns (sign + 1) | (4 if exact arithmetic was needed).
+__device__ __noinline__ int face_sign_fp64(float x0, float y0, float z0, float x1, float y1, float z1,
+                                           float x2, float y2, float z2, float x3, float y3, float z3,
+                                           double px, double py, double pz, int face) {
+  double Q[4][3] = {{x0, y0, z0}, {x1, y1, z1}, {x2, y2, z2}, {x3, y3, z3}};
+  Q[face][0] = px;
+  Q[face][1] = py;
+  Q[face][2] = pz;
+  double bax = Q[1][0] - Q[0][0], bay = Q[1][1] - Q[0][1], baz = Q[1][2] - Q[0][2];
+  double cax = Q[2][0] - Q[0][0], cay = Q[2][1] - Q[0][1], caz = Q[2][2] - Q[0][2];
+  double dax = Q[3][0] - Q[0][0], day = Q[3][1] - Q[0][1], daz = Q[3][2] - Q[0][2];
+  double m0 = cay * daz, m1 = caz * day, m2 = caz * dax, m3 = cax * daz, m4 = cax * day, m5 = cay * dax;
+  double det = bax * (m0 - m1) + bay * (m2 - m3) + baz * (m4 - m5);
+  double perm = fabs(bax) * (fabs(m0) + fabs(m1)) + fabs(bay) * (fabs(m2) + fabs(m3)) +
+                fabs(baz) * (fabs(m4) + fabs(m5));
+  double b = kOrientErr * perm;
+  if (det > b) return 2;
+  if (-det > b) return 0;
+  return (orient_exact(Q[0], Q[1], Q[2], Q[3]) + 1) | 4;
+}
+
+__device__ __forceinline__ int sign32(float det, float perm, int face, const float X[4][3], const float pf[3],
+                                      int& nexact) {
+  const float b = kOrientErr32 * perm;
+  if (perm > kPermFloor32) {
+    if (det > b) return 1;
+    if (-det > b) return -1;
+  }
+  const int r = face_sign_fp64(X[0][0], X[0][1], X[0][2], X[1][0], X[1][1], X[1][2], X[2][0], X[2][1],
+                               X[2][2], X[3][0], X[3][1], X[3][2], (double)pf[0], (double)pf[1], (double)pf[2],
+                               face);
+  nexact += r >> 2;
+  return (r & 3) - 1;
+}
+
+__device__ __forceinline__ int first_exit_face_f32(const float X[4][3], const float pf[3], int need, int& zmask,
+                                                   int& nexact) {
+  float d[4][3];
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) d[k][c] = X[k][c] - pf[c];
+  zmask = 0;
+  if (need & 3) {
+    float m0 = d[2][1] * d[3][2], m1 = d[2][2] * d[3][1];
+    float m2 = d[2][2] * d[3][0], m3 = d[2][0] * d[3][2];
+    float m4 = d[2][0] * d[3][1], m5 = d[2][1] * d[3][0];
+    float cx = m0 - m1, cy = m2 - m3, cz = m4 - m5;
+    float ax = fabsf(m0) + fabsf(m1), ay = fabsf(m2) + fabsf(m3), az = fabsf(m4) + fabsf(m5);
+    if (need & 1) {
+      float det = d[1][0] * cx + d[1][1] * cy + d[1][2] * cz;
+      float perm = fabsf(d[1][0]) * ax + fabsf(d[1][1]) * ay + fabsf(d[1][2]) * az;
+      int s = sign32(det, perm, 0, X, pf, nexact);
+      if (s < 0) return 0;
+      if (s == 0) zmask |= 1;
+    }
+    if (need & 2) {
+      float det = -(d[0][0] * cx + d[0][1] * cy + d[0][2] * cz);
+      float perm = fabsf(d[0][0]) * ax + fabsf(d[0][1]) * ay + fabsf(d[0][2]) * az;
+      int s = sign32(det, perm, 1, X, pf, nexact);
+      if (s < 0) return 1;
+      if (s == 0) zmask |= 2;
+    }
+  }
+  if (need & 12) {
+    float m0 = d[0][1] * d[1][2], m1 = d[0][2] * d[1][1];
+    float m2 = d[0][2] * d[1][0], m3 = d[0][0] * d[1][2];
+    float m4 = d[0][0] * d[1][1], m5 = d[0][1] * d[1][0];
+    float cx = m0 - m1, cy = m2 - m3, cz = m4 - m5;
+    float ax = fabsf(m0) + fabsf(m1), ay = fabsf(m2) + fabsf(m3), az = fabsf(m4) + fabsf(m5);
+    if (need & 4) {
+      float det = d[3][0] * cx + d[3][1] * cy + d[3][2] * cz;
+      float perm = fabsf(d[3][0]) * ax + fabsf(d[3][1]) * ay + fabsf(d[3][2]) * az;
+      int s = sign32(det, perm, 2, X, pf, nexact);
+      if (s < 0) return 2;
+      if (s == 0) zmask |= 4;
+    }
+    if (need & 8) {
+      float det = -(d[2][0] * cx + d[2][1] * cy + d[2][2] * cz);
+      float perm = fabsf(d[2][0]) * ax + fabsf(d[2][1]) * ay + fabsf(d[2][2]) * az;
+      int s = sign32(det, perm, 3, X, pf, nexact);
+      if (s < 0) return 3;
+      if (s == 0) zmask |= 8;
+    }
+  }
+  return -1;
+}
+
 __device__ __forceinline__ void load_tet(const int4* __restrict__ tet_v, const float4* __restrict__ posd,
                                         int t, int v[4], float X[4][3]) {
   int4 q = __ldg(&tet_v[t]);
@@ -134,10 +237,11 @@ __device__ __forceinline__ int nb_of(const int4& n, int i) {
 
 // True if the closure of tetrahedron t holds p; zmask marks faces through p.
 __device__ __noinline__ bool tet_contains(const int4* __restrict__ tet_v, const float4* __restrict__ posd,
-                                          int t, const double p[3], int& zmask, int& nexact) {
+                                          int t, double px, double py, double pz, int& zmask, int& nexact) {
   int v[4];
   float X[4][3];
   load_tet(tet_v, posd, t, v, X);
+  const double p[3] = {px, py, pz};
   return first_exit_face(X, p, 15, zmask, nexact) < 0;
 }
 
@@ -147,7 +251,8 @@ __device__ __noinline__ bool tet_contains(const int4* __restrict__ tet_v, const 
 constexpr int kTieMax = 96;
 __device__ __noinline__ int canonical_tie(const int4* __restrict__ tet_v, const int4* __restrict__ tet_n,
                                           const float4* __restrict__ posd, int t, int zmask,
-                                          const double p[3], int& nexact) {
+                                          double px, double py, double pz) {
+  int nexact = 0;  // exact tests inside tie resolution are not counted
   int seen[kTieMax];
   int nseen = 1, head = 0;
   seen[0] = t;
@@ -155,7 +260,7 @@ __device__ __noinline__ int canonical_tie(const int4* __restrict__ tet_v, const 
   int zm = zmask;
   while (head < nseen) {
     int u = seen[head];
-    if (head > 0) tet_contains(tet_v, posd, u, p, zm, nexact);
+    if (head > 0) tet_contains(tet_v, posd, u, px, py, pz, zm, nexact);
     ++head;
     int4 n = __ldg(&tet_n[u]);
     for (int i = 0; i < 4; ++i) {
@@ -167,7 +272,7 @@ __device__ __noinline__ int canonical_tie(const int4* __restrict__ tet_v, const 
         if (seen[q] == nb) { dup = true; break; }
       if (dup) continue;
       int zn;
-      if (!tet_contains(tet_v, posd, nb, p, zn, nexact)) continue;
+      if (!tet_contains(tet_v, posd, nb, px, py, pz, zn, nexact)) continue;
       if (nseen >= kTieMax) return best;
       seen[nseen++] = nb;
       if (nb < best) best = nb;
@@ -181,20 +286,24 @@ __device__ __noinline__ int canonical_tie(const int4* __restrict__ tet_v, const 
 // vertices and positions of the returned tetrahedron.  Crossing a face keeps
 // the three shared vertices in registers and loads only the new one; the
 // face just crossed is not re-tested (p is strictly inside it).
+template <bool FLOAT_POINT = false>
 __device__ __forceinline__ int walk_locate(const int4* __restrict__ tet_v, const int4* __restrict__ tet_n,
                                            const float4* __restrict__ posd, const double p[3], int t,
                                            int max_steps, int v[4], float X[4][3], WalkStats& st) {
+  // FLOAT_POINT: p holds exact float values, so the FP32 filter stage applies
+  const float pf[3] = {(float)p[0], (float)p[1], (float)p[2]};
   load_tet(tet_v, posd, t, v, X);
   int came = -1;
   for (int step = 0; step < max_steps; ++step) {
     ++st.steps;
     int need = 15 & ~(came >= 0 ? (1 << came) : 0);
     int zmask;
-    int exit_face = first_exit_face(X, p, need, zmask, st.exact);
+    int exit_face = FLOAT_POINT ? first_exit_face_f32(X, pf, need, zmask, st.exact)
+                                : first_exit_face(X, p, need, zmask, st.exact);
     if (exit_face < 0) {
       if (zmask) {
         ++st.tie;
-        int b = canonical_tie(tet_v, tet_n, posd, t, zmask, p, st.exact);
+        int b = canonical_tie(tet_v, tet_n, posd, t, zmask, p[0], p[1], p[2]);
         if (b != t) {
           t = b;
           load_tet(tet_v, posd, t, v, X);
@@ -210,14 +319,18 @@ __device__ __forceinline__ int walk_locate(const int4* __restrict__ tet_v, const
     came = 0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      int src = -1;
+      // predicated selection with compile-time indices keeps X in registers
+      bool found = false;
 #pragma unroll
-      for (int k = 0; k < 4; ++k)
-        if (k != exit_face && v[k] == nv[j]) src = k;
-      if (src >= 0) {
+      for (int c = 0; c < 3; ++c) NX[j][c] = 0.f;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) NX[j][c] = X[src][c];
-      } else {
+      for (int k = 0; k < 4; ++k) {
+        const bool m = (k != exit_face) && (v[k] == nv[j]);
+        found = found || m;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) NX[j][c] = m ? X[k][c] : NX[j][c];
+      }
+      if (!found) {
         load_posf(posd, nv[j], NX[j]);
         came = j;
       }

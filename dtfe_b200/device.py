@@ -110,6 +110,14 @@ class DeviceDTFE:
         self.last_status = st.as_dict()
         return self.last_status
 
+    def autotune(self, fields) -> tuple:
+        chosen = (C.c_int32 * 2)()
+        N.check(self.lib.dtfe_gpu_autotune(self.h, _mask(fields), chosen))
+        return int(chosen[0]), int(chosen[1])
+
+    def set_variants(self, locate: int, evaluate: int) -> None:
+        N.check(self.lib.dtfe_gpu_set_variants(self.h, locate, evaluate))
+
     def locate_points(self, pts: np.ndarray, start: int = 0) -> np.ndarray:
         pts = np.ascontiguousarray(pts, np.float64)
         out = np.empty(len(pts), np.int32)

@@ -161,6 +161,16 @@ int dtfe_gpu_interpolate(dtfe_handle h, const dtfe_interp_opts* opts,
 int dtfe_gpu_interpolate_dev(dtfe_handle h, const dtfe_interp_opts* opts,
                              float* const out_dev[DTFE_NUM_FIELDS], dtfe_status* st);
 
+/* Autotuner: times each launch variant of the point-location kernel
+ * (register budget per block, cells per thread seeded from the previous hit)
+ * and of the evaluation kernel on the loaded data, for the cell-centre method
+ * and the given field mask, and keeps the fastest.  chosen[0..1] (may be
+ * NULL) receive the selected variant indices.  No counterpart in the
+ * reference (its loops have no launch parameters). */
+int dtfe_gpu_autotune(dtfe_handle h, uint32_t fields, int32_t* chosen);
+/* Selects launch variants explicitly (indices as reported by autotune). */
+int dtfe_gpu_set_variants(dtfe_handle h, int32_t locate_variant, int32_t eval_variant);
+
 /* Copy the vertex densities (V floats) to the host. */
 int dtfe_gpu_download_vertex_density(dtfe_handle h, float* dens);
 

@@ -113,3 +113,20 @@ def test_subboxes(plan8):
     for f in fields:
         assert rel_err(g[f], ref[f]) <= 1e-6, f
     d.close()
+
+
+def test_launch_variants_identical(plan8):
+    """Every autotuner variant (register budget, cells per thread seeded from
+    the previous hit) produces bit-identical fields."""
+    d = _device(plan8)
+    chosen = d.autotune(FIELDS)
+    assert 0 <= chosen[0] < 6 and 0 <= chosen[1] < 3
+    d.set_variants(0, 0)
+    base = d.interpolate(FIELDS, method=0)
+    for loc in range(6):
+        for ev in range(3):
+            d.set_variants(loc, ev)
+            g = d.interpolate(FIELDS, method=0)
+            for f in FIELDS:
+                assert np.array_equal(g[f], base[f]), (loc, ev, f)
+    d.close()

@@ -1,0 +1,69 @@
+"""Python access to the reference-code harness (oracle/_ref/libdtfe_ref.so) —
+TEST INFRASTRUCTURE ONLY.
+
+The harness runs the reference's own interpolation sources
+(src/CGAL_triangulation/triangulation.cpp, compiled from the reference tree
+by oracle/Makefile) on a flat tessellation through a CGAL-API facade.  It is
+built only where the reference tree exists; ``available()`` says whether it
+was built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(_HERE, "_ref", "libdtfe_ref.so")
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB)
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        L = C.CDLL(LIB)
+        vp = C.c_void_p
+        L.ref_interpolate.argtypes = [C.c_int64, vp, vp, vp, vp, C.c_int64, vp, vp, vp, vp, C.c_int, C.c_int,
+                                      C.c_uint64, C.c_double, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.ref_interpolate.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def run(plan, box: int = 0, which: int = 0, n_points: int = 1, seed: int = 0, dens_override=None):
+    """Reference fields of one sub-box tile (tile-local grid, x slowest).
+
+    Returns dict with 'vertex_density' (local vertices) and the fields."""
+    b = plan.boxes[box]
+    v0, nv, t0, nt = b.vert_offset, b.n_verts, b.tet_offset, b.n_tets
+    xyz = np.ascontiguousarray(plan.xyz[v0:v0 + nv])
+    w = np.ascontiguousarray(plan.weight[v0:v0 + nv])
+    vel = None if plan.velocity is None else np.ascontiguousarray(plan.velocity[v0:v0 + nv])
+    sc = None if plan.scalar is None else np.ascontiguousarray(plan.scalar[v0:v0 + nv, 0])
+    tv = np.ascontiguousarray(plan.tet_v[t0:t0 + nt] - v0, dtype=np.int32)
+    tn = plan.tet_n[t0:t0 + nt]
+    tn = np.ascontiguousarray(np.where(tn >= 0, tn - t0, -1), dtype=np.int32)
+    dims = np.array([b.tile_dims[0], b.tile_dims[1], b.tile_dims[2]], np.int32)
+    region = np.array([b.lo[0], b.lo[0] + b.dx[0] * dims[0], b.lo[1], b.lo[1] + b.dx[1] * dims[1],
+                       b.lo[2], b.lo[2] + b.dx[2] * dims[2]], np.float32)
+    G = int(np.prod(dims))
+    out = {"vertex_density": np.zeros(nv, np.float32), "density": np.zeros(G, np.float32),
+           "velocity": np.zeros((G, 3), np.float32), "velocity_gradient": np.zeros((G, 9), np.float32),
+           "scalar": np.zeros(G, np.float32), "scalar_gradient": np.zeros((G, 3), np.float32),
+           "velocity_std": np.zeros(G, np.float32)}
+    dov = None if dens_override is None else np.ascontiguousarray(dens_override[v0:v0 + nv], np.float32)
+    p = lambda a: None if a is None else a.ctypes.data
+    rc = lib().ref_interpolate(nv, p(xyz), p(w), p(vel), p(sc), nt, p(tv), p(tn), p(region), p(dims), which,
+                               n_points, seed, plan.rho_bar, p(dov), p(out["vertex_density"]),
+                               p(out["density"]), p(out["velocity"]), p(out["velocity_gradient"]),
+                               p(out["scalar"]) if sc is not None else None,
+                               p(out["scalar_gradient"]) if sc is not None else None,
+                               p(out["velocity_std"]) if which == 2 else None)
+    if rc:
+        raise RuntimeError(f"ref_interpolate failed ({rc})")
+    return out

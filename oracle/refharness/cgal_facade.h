@@ -134,8 +134,19 @@ class Delaunay_triangulation_3 {
     Vertex* vertex(int i) const { return v[i]; }
     Cell* neighbor(int i) const { return n[i]; }
   };
-  typedef Vertex* Vertex_handle;
-  typedef Cell* Cell_handle;
+  // CGAL handles default-construct to null (the reference relies on it:
+  // `Cell_handle current;` is the first walk hint)
+  template <class T>
+  struct Handle {
+    T* p = nullptr;
+    Handle() = default;
+    Handle(T* q) : p(q) {}
+    T* operator->() const { return p; }
+    T& operator*() const { return *p; }
+    operator T*() const { return p; }
+  };
+  typedef Handle<Vertex> Vertex_handle;
+  typedef Handle<Cell> Cell_handle;
 
   // iterators over handles (dereference yields the object, -> the handle)
   template <class T>
@@ -150,6 +161,7 @@ class Delaunay_triangulation_3 {
     T* operator->() const { return *it; }
     T& operator*() const { return **it; }
     operator T*() const { return *it; }
+    operator Handle<T>() const { return Handle<T>(*it); }
     HIter& operator++() { ++it; return *this; }
     bool operator!=(const HIter& o) const { return it != o.it; }
     bool operator==(const HIter& o) const { return it == o.it; }
@@ -191,7 +203,7 @@ class Delaunay_triangulation_3 {
 
   // CGAL::insert: here the point is stored and the tessellation is (re)built
   // on the next query.
-  Vertex_handle insert(const Point& p, Vertex_handle = nullptr) {
+  Vertex_handle insert(const Point& p, Vertex_handle = Vertex_handle()) {
     Vertex* v = new Vertex();
     v->p = p;
     v->id = (int64_t)verts_.size();
@@ -244,14 +256,15 @@ class Delaunay_triangulation_3 {
     return t;
   }
 
-  Cell_handle locate(const Point& p, Locate_type& lt, int& li, int& lj, Cell_handle hint = nullptr) {
+  Cell_handle locate(const Point& p, Locate_type& lt, int& li, int& lj, Cell_handle hint = Cell_handle()) {
     ensure();
     li = lj = 0;
     if (finite_cells_.empty()) {
       lt = OUTSIDE_AFFINE_HULL;
-      return nullptr;
+      return Cell_handle();
     }
-    Cell* t = (hint && !hint->infinite) ? hint : (hint && hint->infinite ? hint->n[0] : finite_cells_[0]);
+    Cell* h = hint;
+    Cell* t = (h && !h->infinite) ? h : (h && h->infinite ? h->n[0] : finite_cells_[0]);
     for (size_t step = 0; step < 4 * finite_cells_.size() + 64; ++step) {
       int exit = -1;
       for (int i = 0; i < 4 && exit < 0; ++i)
@@ -285,7 +298,7 @@ class Delaunay_triangulation_3 {
     lt = CELL;
     return best;
   }
-  Cell_handle locate(const Point& p, Locate_type& lt, int& li, Cell_handle hint = nullptr) {
+  Cell_handle locate(const Point& p, Locate_type& lt, int& li, Cell_handle hint = Cell_handle()) {
     int lj;
     return locate(p, lt, li, lj, hint);
   }

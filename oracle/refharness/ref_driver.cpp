@@ -1,0 +1,149 @@
+// Driver of the reference-code harness — TEST INFRASTRUCTURE ONLY.
+//
+// Links against the reference's own src/CGAL_triangulation/triangulation.cpp
+// (compiled unmodified from the reference tree against cgal_facade.h and the
+// stand-in headers under include/) and exposes its interpolation functions
+// through a C entry point, so tests can run the reference's arithmetic on
+// exactly the tessellation the GPU path and the oracle use:
+//
+//   vertexDensity               triangulation.cpp:200-279
+//   interpolateGrid             unaveraged_interpolation.cc:209-369
+//   interpolateGrid_averaged_2  averaged_interpolation_2.cc:35-233
+//   interpolateGrid_averaged_3  averaged_interpolation_2.cc:664-866
+//
+// The reference's command-line layer (user_options.cc, boost::program_options)
+// is not built; the User_options constructor below sets the members those
+// functions read, with the reference's defaults (src/user_options.cc:39-92).
+
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include <gsl/gsl_qrng.h>
+
+#include "define.h"
+#include "CGAL_triangulation/CGAL_include_3D.h"
+#include "particle_data.h"
+#include "quantities.h"
+#include "user_options.h"
+
+void vertexDensity(DT& dt, User_options& userOptions);
+void interpolateGrid(DT& dt, User_options& userOptions, Quantities* quantities);
+void interpolateGrid_averaged_2(DT& dt, User_options& userOptions, Quantities* quantities);
+void interpolateGrid_averaged_3(DT& dt, User_options& userOptions, Quantities* quantities);
+
+User_options::User_options() {
+  periodic = false;
+  boxCoordinates.assign(0.);
+  userGivenBoxCoordinates = false;
+  inputFileType = 101;
+  outputFileType = 101;
+  regionOn = false;
+  regionMpcOn = false;
+  partitionOn = false;
+  partNo = -1;
+  paddingOn = false;
+  paddingMpcOn = false;
+  paddingParticles = Real(5.);
+  testPaddedBoundaries = false;
+  method = 1;
+  noPoints = 100;
+  noPointsOn = false;
+  averageDensity = Real(-1.);
+  randomSeed = 0;
+  redshiftConeOn = false;
+  DTFE = true;
+  NGP = CIC = TSC = SPH = false;
+  SPH_neighbors = 32;
+  MpcValue = Real(1.);
+  extensive = false;
+  verboseLevel = 0;
+  randomSample = Real(-1.);
+  poisson = 0;
+  transformToRedshiftSpaceOn = false;
+  paddedBox.assign(0.);
+  userDefinedSampling = false;
+  noProcessors = 1;
+  threadId = 0;
+  totalTime = Real(0.);
+}
+
+extern "C" {
+
+// GSL stand-ins (method 1 is never run by the harness)
+const gsl_qrng_type* gsl_qrng_sobol = nullptr;
+const gsl_qrng_type* gsl_qrng_niederreiter_2 = nullptr;
+gsl_qrng* gsl_qrng_alloc(const gsl_qrng_type*, unsigned int) {
+  std::fprintf(stderr, "reference harness: averaging method 1 is not available\n");
+  std::abort();
+}
+int gsl_qrng_get(const gsl_qrng*, double*) { std::abort(); }
+void gsl_qrng_free(gsl_qrng*) {}
+
+// Runs the reference on one (sub-box) tessellation with LOCAL indices.
+//   which: 0 cell-centre (interpolateGrid), 2 / 3 averaging methods.
+//   dens_override (may be NULL): vertex densities used for the interpolation
+//   instead of the reference's own (float-accumulated) ones.
+//   outputs (float, Quantities layout; NULL to skip): vertex densities,
+//   density, velocity, gradient, scalar (S = 1), scalar gradient, velocity std.
+int ref_interpolate(int64_t nv, const float* xyz, const float* w, const float* vel, const float* scal,
+                    int64_t nt, const int32_t* tv, const int32_t* tn, const float region[6],
+                    const int32_t grid[3], int which, int n_points, uint64_t seed, double rho_bar,
+                    const float* dens_override, float* out_vdens, float* out_density, float* out_velocity,
+                    float* out_gradient, float* out_scalar, float* out_scalar_gradient, float* out_std) {
+  DT dt;
+  const std::vector<DT::Vertex*>& verts = dt.load_flat(nv, xyz, nt, tv, tn);
+  for (int64_t i = 0; i < nv; ++i) {
+    vertexData& d = verts[i]->info();
+    d.weight() = w[i];
+    for (int c = 0; c < 3; ++c) d.velocity(c) = vel ? vel[3 * i + c] : 0.f;
+    d.scalar(0) = scal ? scal[i] : 0.f;
+  }
+  User_options opt;
+  opt.averageDensity = (Real)rho_bar;
+  opt.gridSize.assign(grid, grid + 3);
+  opt.region.coords.assign(region, region + 6);
+  opt.method = which;
+  opt.noPoints = n_points;
+  opt.randomSeed = (size_t)seed;
+  vertexDensity(dt, opt);
+  for (int64_t i = 0; i < nv; ++i) {
+    if (out_vdens) out_vdens[i] = verts[i]->info().density();
+    if (dens_override) verts[i]->info().setDensity(dens_override[i]);
+  }
+  Quantities q;
+  Field f;
+  f.density = out_density != nullptr;
+  f.velocity = out_velocity != nullptr;
+  f.velocity_gradient = out_gradient != nullptr;
+  f.scalar = out_scalar != nullptr;
+  f.scalar_gradient = out_scalar_gradient != nullptr;
+  f.velocity_std = out_std != nullptr && which == 2;
+  if (which == 0) {
+    opt.uField = f;
+    interpolateGrid(dt, opt, &q);
+  } else if (which == 2) {
+    opt.aField = f;
+    interpolateGrid_averaged_2(dt, opt, &q);
+  } else if (which == 3) {
+    opt.aField = f;
+    interpolateGrid_averaged_3(dt, opt, &q);
+  } else {
+    return 1;
+  }
+  const size_t G = (size_t)grid[0] * grid[1] * grid[2];
+  auto copy = [&](float* dst, const float* src, size_t n, size_t have) {
+    if (dst && have == G) std::memcpy(dst, src, n * sizeof(float));
+  };
+  copy(out_density, q.density.data(), G, q.density.size());
+  copy(out_velocity, (const float*)q.velocity.data(), 3 * G, q.velocity.size());
+  copy(out_gradient, (const float*)q.velocity_gradient.data(), 9 * G, q.velocity_gradient.size());
+  copy(out_scalar, (const float*)q.scalar.data(), G, q.scalar.size());
+  copy(out_scalar_gradient, (const float*)q.scalar_gradient.data(), 3 * G, q.scalar_gradient.size());
+  copy(out_std, q.velocity_std.data(), G, q.velocity_std.size());
+  return 0;
+}
+
+}  // extern "C"

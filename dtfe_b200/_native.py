@@ -33,6 +33,12 @@ class Subbox(C.Structure):
     ]
 
 
+class DepositBox(C.Structure):
+    """dtfe_deposit_box."""
+    _fields_ = [("particle_offset", C.c_int64), ("n_particles", C.c_int64), ("region", C.c_float * 6),
+                ("tile_origin", C.c_int32 * 3), ("tile_dims", C.c_int32 * 3)]
+
+
 class InterpOpts(C.Structure):
     """dtfe_interp_opts."""
     _fields_ = [("method", C.c_int32), ("n_samples", C.c_int32), ("seed", C.c_uint64),
@@ -137,6 +143,9 @@ def gpu() -> C.CDLL:
         lib.dtfe_gpu_stream.argtypes = [H]
         lib.dtfe_gpu_stream.restype = C.c_void_p
         lib.dtfe_gpu_synchronize.argtypes = [H]
+        lib.dtfe_gpu_deposit.argtypes = [H, C.c_int32, vp, vp, vp, C.c_int64, C.c_int32, vp, vp, C.c_double, vp, vp]
+        lib.dtfe_gpu_deposit_dev.argtypes = [H, C.c_int32, vp, vp, vp, C.c_int64, C.c_int32, vp, vp, C.c_double,
+                                             vp, vp]
         lib.dtfe_gpu_autotune.argtypes = [H, C.c_uint32, vp]
         lib.dtfe_gpu_set_variants.argtypes = [H, C.c_int32, C.c_int32]
         lib.dtfe_vertex_density_noalloc.argtypes = [vp, vp, C.c_int64, vp, vp, C.c_int64, C.c_double, vp, vp]

@@ -80,10 +80,23 @@ def build_oracle(force: bool = False) -> str:
     return out
 
 
+REFERENCE_TREE = "/root/reference"
+
+
+def build_ref() -> str | None:
+    """The reference-code harness (oracle/_ref), only where the reference tree
+    exists; elsewhere the prebuilt library, if any, is used as is."""
+    if not os.path.isdir(os.path.join(REFERENCE_TREE, "src")):
+        return None
+    _run(["make", "-s", "-C", ORACLE, "ref", "REF=" + REFERENCE_TREE])
+    return os.path.join(ORACLE, "_ref", "libdtfe_ref.so")
+
+
 def build_all(force: bool = False) -> None:
     build_host(force)
     build_gpu(force)
     build_oracle(force)
+    build_ref()
 
 
 if __name__ == "__main__":

@@ -1,0 +1,409 @@
+// NGP / CIC / TSC grid deposition on B200 (sm_100a) — the reference's
+// comparison estimators NGP_interpolation_regular_grid
+// (src/NGP_interpolation.cc:67-136), CIC_interpolation_regular_grid
+// (src/CIC_interpolation.cc:67-273) and TSC_interpolation_regular_grid
+// (src/TSC_interpolation.cc:67-254), per sub-box region.
+//
+// Each particle's stencil (cells and per-axis weights, clipped at the region
+// edges exactly as the reference clips them) and each contribution
+// result = w * wx * wy * wz are computed in the reference's float arithmetic.
+// The contributions are accumulated in 64-bit fixed point: every sum is exact,
+// so the grid is deterministic and independent of the order in which threads
+// add.  The fixed-point scales are powers of two chosen from the total |mass|
+// and |momentum| so that no cell can overflow.  A block of 256 particles
+// (Morton-ordered within its sub-box) whose stencils fit an 8x8x8 cell tile
+// accumulates in shared memory first and flushes each touched cell with one
+// global atomic per component; other blocks add to global memory directly.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/dtfe_gpu.h"
+
+extern "C" int dtfe_internal_set_error(int code, const char* msg);
+
+namespace {
+
+constexpr int kDepBlock = 256;
+constexpr int kTile = 8;  // shared tile edge in cells
+constexpr int kTileCells = kTile * kTile * kTile;
+
+struct DepBox {
+  int64_t off, n;         // particle range
+  float lo[3], dx[3];     // region lower corner and cell size (float, as the reference)
+  float inner[6], outer[6];
+  int32_t origin[3], dims[3];
+  int64_t tile_off;       // first flattened tile cell of this box
+  float factor;           // density normalisation of this region
+};
+
+struct DepParams {
+  const float4* pw;       // x, y, z, weight
+  const float4* vel;      // vx, vy, vz, 0 (may be null)
+  const DepBox* boxes;
+  const int64_t* prefix;  // K+1 particle offsets
+  int K;
+  int64_t n;
+  int64_t G1, G2;
+  double scale_m, scale_p;
+  unsigned long long* acc_m;  // per cell
+  unsigned long long* acc_p;  // 3 per cell (null: no velocity)
+};
+
+__device__ __forceinline__ int find_dep_box(const int64_t* __restrict__ prefix, int K, int64_t s) {
+  int lo = 0, hi = K;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (__ldg(&prefix[mid]) <= s) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ bool in_box(const float p[3], const float* b) {
+  return p[0] >= b[0] && p[0] <= b[1] && p[1] >= b[2] && p[1] <= b[3] && p[2] >= b[4] && p[2] <= b[5];
+}
+
+__device__ __forceinline__ float tsc_a(float t) { return (float)(.5 * (0.5 - (double)t) * (0.5 - (double)t)); }
+__device__ __forceinline__ float tsc_b(float t) { return (float)(.75 - (double)(t * t)); }
+__device__ __forceinline__ float tsc_c(float t) { return (float)(.5 * (0.5 + (double)t) * (0.5 + (double)t)); }
+
+// Stencil of one axis (cells local to the region, weights, count), as
+// axis_weights of the reference's CIC/TSC loops.
+template <int KIND>
+__device__ __forceinline__ void axis_stencil(bool inner, float temp, int n, int cell[3], float w[3], int& count) {
+  count = 0;
+  if (inner) {
+    cell[0] = (int)floorf(temp) - 1;
+    cell[1] = cell[0] + 1;
+    cell[2] = cell[1] + 1;
+    temp = (float)((double)temp - ((double)cell[1] + 0.5));
+    count = 3;
+    if (KIND == 1) {
+      if (temp < 0.f) { w[0] = -temp; w[1] = 1 + temp; w[2] = 0.f; }
+      else { w[0] = 0.f; w[1] = 1 - temp; w[2] = temp; }
+    } else {
+      w[0] = tsc_a(temp); w[1] = tsc_b(temp); w[2] = tsc_c(temp);
+    }
+    return;
+  }
+  int ti = (int)floorf(temp);
+  temp = (float)((double)temp - ((double)ti + 0.5));
+  if (ti == -1) {
+    cell[0] = 0; count = 1;
+    w[0] = KIND == 1 ? temp : tsc_c(temp);
+  } else if (ti == 0) {
+    cell[0] = 0; cell[1] = 1; count = 2;
+    if (KIND == 1) { w[0] = 1 - temp; w[1] = temp; }
+    else { w[0] = tsc_b(temp); w[1] = tsc_c(temp); }
+  } else if (ti == n - 1) {
+    cell[0] = n - 2; cell[1] = n - 1; count = 2;
+    if (KIND == 1) { w[0] = -temp; w[1] = 1 + temp; }
+    else { w[0] = tsc_a(temp); w[1] = tsc_b(temp); }
+  } else if (ti == n) {
+    cell[0] = n - 1; count = 1;
+    w[0] = KIND == 1 ? -temp : tsc_a(temp);
+  } else if (!(ti < -1 || ti > n)) {
+    cell[0] = ti - 1; cell[1] = ti; cell[2] = ti + 1; count = 3;
+    if (KIND == 1) {
+      if (temp < 0.f) { w[0] = -temp; w[1] = 1 + temp; w[2] = 0.f; }
+      else { w[0] = 0.f; w[1] = 1 - temp; w[2] = temp; }
+    } else {
+      w[0] = tsc_a(temp); w[1] = tsc_b(temp); w[2] = tsc_c(temp);
+    }
+  }
+}
+
+__device__ __forceinline__ unsigned long long to_fixed(float v, double scale) {
+  return (unsigned long long)llrint((double)v * scale);
+}
+
+// KIND: 0 NGP, 1 CIC, 2 TSC.
+template <int KIND>
+__global__ void __launch_bounds__(kDepBlock) k_deposit(DepParams P) {
+  __shared__ unsigned long long s_m[kTileCells];
+  __shared__ unsigned long long s_p[3][kTileCells];
+  __shared__ int s_box, s_lo[3], s_hi[3], s_ok;
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const bool valid = i < P.n;
+  const bool with_vel = P.acc_p != nullptr;
+
+  int b = 0;
+  int cell[3][3];
+  float w[3][3];
+  int count[3] = {0, 0, 0};
+  float wt = 0.f, v[3] = {0.f, 0.f, 0.f};
+  if (valid) {
+    b = find_dep_box(P.prefix, P.K, i);
+    const DepBox& B = P.boxes[b];
+    float4 q = __ldg(&P.pw[i]);
+    const float p[3] = {q.x, q.y, q.z};
+    wt = q.w;
+    if (with_vel && P.vel) {
+      float4 u = __ldg(&P.vel[i]);
+      v[0] = u.x; v[1] = u.y; v[2] = u.z;
+    }
+    if (KIND == 0) {
+      bool ok = true;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        cell[j][0] = (int)floorf((p[j] - B.lo[j]) / B.dx[j]);
+        w[j][0] = 1.f;
+        ok = ok && cell[j][0] >= 0 && cell[j][0] < B.dims[j];
+      }
+      if (ok) count[0] = count[1] = count[2] = 1;
+    } else {
+      const bool inner = in_box(p, B.inner);
+      if (inner || in_box(p, B.outer)) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          float temp = (p[j] - B.lo[j]) / B.dx[j];
+          axis_stencil<KIND>(inner, temp, B.dims[j], cell[j], w[j], count[j]);
+        }
+      }
+    }
+  }
+  const bool any = count[0] > 0 && count[1] > 0 && count[2] > 0;
+
+  // Does the whole block fit one shared tile of one sub-box?
+  if (threadIdx.x == 0) {
+    s_box = valid ? b : -1;
+    s_ok = 1;
+    for (int c = 0; c < 3; ++c) { s_lo[c] = 0x7FFFFFFF; s_hi[c] = -0x7FFFFFFF; }
+  }
+  __syncthreads();
+  if (valid && b != s_box) s_ok = 0;
+  if (any) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      atomicMin(&s_lo[c], cell[c][0]);
+      atomicMax(&s_hi[c], cell[c][count[c] - 1]);
+    }
+  }
+  __syncthreads();
+  bool staged = s_ok && s_box >= 0;
+  int tlo[3] = {s_lo[0], s_lo[1], s_lo[2]};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) staged = staged && s_hi[c] >= s_lo[c] && s_hi[c] - s_lo[c] < kTile;
+  if (staged) {
+    for (int k = threadIdx.x; k < kTileCells; k += blockDim.x) {
+      s_m[k] = 0ull;
+      s_p[0][k] = s_p[1][k] = s_p[2][k] = 0ull;
+    }
+    __syncthreads();
+  }
+
+  if (any) {
+    const DepBox& B = P.boxes[b];
+    for (int a = 0; a < count[0]; ++a)
+      for (int bb = 0; bb < count[1]; ++bb)
+        for (int c = 0; c < count[2]; ++c) {
+          const float result = wt * w[0][a] * w[1][bb] * w[2][c];
+          const unsigned long long fm = to_fixed(result, P.scale_m);
+          unsigned long long fp[3];
+          if (with_vel) {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) fp[q] = to_fixed(v[q] * result, P.scale_p);
+          }
+          if (staged) {
+            const int k = ((cell[0][a] - tlo[0]) * kTile + (cell[1][bb] - tlo[1])) * kTile + (cell[2][c] - tlo[2]);
+            atomicAdd(&s_m[k], fm);
+            if (with_vel) {
+#pragma unroll
+              for (int q = 0; q < 3; ++q) atomicAdd(&s_p[q][k], fp[q]);
+            }
+          } else {
+            const int64_t idx = ((int64_t)(B.origin[0] + cell[0][a]) * P.G1 + (B.origin[1] + cell[1][bb])) * P.G2 +
+                                (B.origin[2] + cell[2][c]);
+            atomicAdd(&P.acc_m[idx], fm);
+            if (with_vel) {
+#pragma unroll
+              for (int q = 0; q < 3; ++q) atomicAdd(&P.acc_p[3 * idx + q], fp[q]);
+            }
+          }
+        }
+  }
+  if (staged) {
+    __syncthreads();
+    const DepBox& B = P.boxes[s_box];
+    for (int k = threadIdx.x; k < kTileCells; k += blockDim.x) {
+      const int ci = k / (kTile * kTile), cj = (k / kTile) % kTile, ck = k % kTile;
+      const int gi = tlo[0] + ci, gj = tlo[1] + cj, gk = tlo[2] + ck;
+      if (gi >= B.dims[0] || gj >= B.dims[1] || gk >= B.dims[2]) continue;
+      const bool touched = s_m[k] != 0ull || (with_vel && (s_p[0][k] | s_p[1][k] | s_p[2][k]) != 0ull);
+      if (!touched) continue;
+      const int64_t idx = ((int64_t)(B.origin[0] + gi) * P.G1 + (B.origin[1] + gj)) * P.G2 + (B.origin[2] + gk);
+      atomicAdd(&P.acc_m[idx], s_m[k]);
+      if (with_vel) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) atomicAdd(&P.acc_p[3 * idx + q], s_p[q][k]);
+      }
+    }
+  }
+}
+
+// Fixed-point sums -> the reference's normalisation, per region: velocity =
+// momentum / mass (float division), density = mass * (region cells /
+// Box::volume() / rho_bar), Box::volume() being the hard-coded 35000^3.
+__global__ void k_deposit_finalize(int64_t n_tile_cells, const DepBox* __restrict__ boxes,
+                                   const int64_t* __restrict__ tile_prefix, int K, int64_t G1, int64_t G2,
+                                   const unsigned long long* __restrict__ acc_m,
+                                   const unsigned long long* __restrict__ acc_p, double inv_m, double inv_p,
+                                   float* __restrict__ density, float* __restrict__ velocity) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= n_tile_cells) return;
+  const int b = find_dep_box(tile_prefix, K, s);
+  const DepBox& B = boxes[b];
+  const int64_t local = s - B.tile_off;
+  const int k = (int)(local % B.dims[2]);
+  const int j = (int)((local / B.dims[2]) % B.dims[1]);
+  const int i = (int)(local / ((int64_t)B.dims[2] * B.dims[1]));
+  const int64_t idx = ((int64_t)(B.origin[0] + i) * G1 + (B.origin[1] + j)) * G2 + (B.origin[2] + k);
+  const float m = (float)((double)(long long)acc_m[idx] * inv_m);
+  if (velocity) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const float p = (float)((double)(long long)acc_p[3 * idx + q] * inv_p);
+      velocity[3 * idx + q] = m != 0.f ? p / m : 0.f;
+    }
+  }
+  if (density) density[idx] = m * B.factor;
+}
+
+__global__ void k_pack4(int64_t n, const float* __restrict__ a3, const float* __restrict__ b1, float4* __restrict__ out) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = make_float4(a3[3 * i], a3[3 * i + 1], a3[3 * i + 2], b1 ? b1[i] : 1.f);
+}
+
+}  // namespace
+
+extern "C" int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xyz, const float* w, const float* vel,
+                                     int64_t n, int32_t n_boxes, const dtfe_deposit_box* boxes,
+                                     const int32_t grid[3], double average_density, float* density_dev,
+                                     float* velocity_dev, void** scratch, size_t* scratch_bytes) {
+  if (kind < 0 || kind > 2) return dtfe_internal_set_error(DTFE_ERR_ARG, "deposit kind must be 0 (NGP), 1 (CIC), 2 (TSC)");
+  if (n < 0 || n_boxes <= 0 || !boxes || !grid) return dtfe_internal_set_error(DTFE_ERR_ARG, "bad deposit arguments");
+  if (!(average_density > 0.0)) return dtfe_internal_set_error(DTFE_ERR_ARG, "averageDensity must be positive");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t G = (int64_t)grid[0] * grid[1] * grid[2];
+  // host-side box records: the reference's float region arithmetic
+  std::vector<DepBox> hb(n_boxes);
+  std::vector<int64_t> prefix(n_boxes + 1);
+  double tot_m = 0.0, tot_p = 0.0;
+  for (int b = 0; b < n_boxes; ++b) {
+    const dtfe_deposit_box& in = boxes[b];
+    DepBox& B = hb[b];
+    B.off = in.particle_offset;
+    B.n = in.n_particles;
+    if (B.off < 0 || B.off + B.n > n || (b > 0 && B.off != hb[b - 1].off + hb[b - 1].n))
+      return dtfe_internal_set_error(DTFE_ERR_ARG, "deposit boxes must cover consecutive particle ranges");
+    for (int c = 0; c < 3; ++c) {
+      if (in.tile_dims[c] < (kind ? 3 : 1) || in.tile_origin[c] < 0 || in.tile_origin[c] + in.tile_dims[c] > grid[c])
+        return dtfe_internal_set_error(DTFE_ERR_ARG, "deposit tile outside the grid (CIC/TSC need >= 3 cells per axis)");
+      B.origin[c] = in.tile_origin[c];
+      B.dims[c] = in.tile_dims[c];
+      B.lo[c] = in.region[2 * c];
+      B.dx[c] = (in.region[2 * c + 1] - in.region[2 * c]) / (float)in.tile_dims[c];
+      const float pad = B.dx[c];
+      const float ipad = (float)(-1.1 * (double)pad);
+      B.outer[2 * c] = in.region[2 * c] - pad;
+      B.outer[2 * c + 1] = in.region[2 * c + 1] + pad;
+      B.inner[2 * c] = in.region[2 * c] - ipad;
+      B.inner[2 * c + 1] = in.region[2 * c + 1] + ipad;
+    }
+    prefix[b] = B.off;
+  }
+  prefix[n_boxes] = hb[n_boxes - 1].off + hb[n_boxes - 1].n;
+  std::vector<int64_t> tprefix(n_boxes + 1, 0);
+  float vol = 1.f;
+  for (int c = 0; c < 3; ++c) vol *= 35000;  // the reference's Box::volume()
+  for (int b = 0; b < n_boxes; ++b) {
+    DepBox& B = hb[b];
+    const int64_t cells = (int64_t)B.dims[0] * B.dims[1] * B.dims[2];
+    B.tile_off = tprefix[b];
+    tprefix[b + 1] = tprefix[b] + cells;
+    B.factor = (float)cells / vol / (float)average_density;
+  }
+  for (int64_t i = 0; i < n; ++i) {
+    const double wi = w ? std::fabs((double)w[i]) : 1.0;
+    tot_m += wi;
+    if (vel)
+      for (int q = 0; q < 3; ++q) tot_p = std::max(tot_p, 0.0) + wi * std::fabs((double)vel[3 * i + q]);
+  }
+  // scales: powers of two with the total below 2^61
+  auto scale_for = [](double tot) { return std::ldexp(1.0, 61 - (int)std::ceil(std::log2(std::max(tot, 1e-30)))); };
+  const double scale_m = scale_for(tot_m), scale_p = scale_for(tot_p);
+  // scratch: particles (2 float4), boxes, prefix, accumulators (4 per cell)
+  const size_t bytes_part = sizeof(float4) * 2 * (size_t)n;
+  const size_t bytes_box = sizeof(DepBox) * n_boxes + 2 * sizeof(int64_t) * (n_boxes + 1);
+  const size_t bytes_acc = sizeof(unsigned long long) * 4 * (size_t)G;
+  const size_t need = bytes_part + bytes_box + bytes_acc + 1024;
+  if (*scratch_bytes < need) {
+    if (*scratch) cudaFree(*scratch);
+    *scratch = nullptr;
+    *scratch_bytes = 0;
+    if (cudaMalloc(scratch, need) != cudaSuccess) return dtfe_internal_set_error(DTFE_ERR_ALLOC, "cudaMalloc (deposit)");
+    *scratch_bytes = need;
+  }
+  char* base = (char*)*scratch;
+  auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  float4* d_pw = (float4*)base;
+  float4* d_vel = d_pw + n;
+  size_t o = align(bytes_part);
+  unsigned long long* acc_m = (unsigned long long*)(base + o);
+  unsigned long long* acc_p = acc_m + G;
+  o = align(o + bytes_acc);
+  DepBox* d_boxes = (DepBox*)(base + o);
+  int64_t* d_prefix = (int64_t*)(base + o + sizeof(DepBox) * n_boxes);
+  int64_t* d_tprefix = d_prefix + (n_boxes + 1);
+  cudaError_t e;
+  float* tmp = nullptr;
+  if (n > 0) {
+    if ((e = cudaMallocAsync((void**)&tmp, sizeof(float) * 4 * (size_t)n, st)) != cudaSuccess)
+      return dtfe_internal_set_error(DTFE_ERR_ALLOC, cudaGetErrorString(e));
+    float* t3 = tmp;
+    float* t1 = tmp + 3 * n;
+    cudaMemcpyAsync(t3, xyz, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, st);
+    if (w) cudaMemcpyAsync(t1, w, sizeof(float) * n, cudaMemcpyHostToDevice, st);
+    k_pack4<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, t3, w ? t1 : nullptr, d_pw);
+    if (vel) {
+      cudaMemcpyAsync(t3, vel, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, st);
+      k_pack4<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, t3, nullptr, d_vel);
+    }
+    cudaFreeAsync(tmp, st);
+  }
+  cudaMemcpyAsync(d_boxes, hb.data(), sizeof(DepBox) * n_boxes, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_prefix, prefix.data(), sizeof(int64_t) * (n_boxes + 1), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_tprefix, tprefix.data(), sizeof(int64_t) * (n_boxes + 1), cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(acc_m, 0, bytes_acc, st);
+  DepParams P;
+  P.pw = d_pw;
+  P.vel = vel ? d_vel : nullptr;
+  P.boxes = d_boxes;
+  P.prefix = d_prefix;
+  P.K = n_boxes;
+  P.n = n;
+  P.G1 = grid[1];
+  P.G2 = grid[2];
+  P.scale_m = scale_m;
+  P.scale_p = scale_p;
+  P.acc_m = acc_m;
+  P.acc_p = velocity_dev ? acc_p : nullptr;
+  if (n > 0) {
+    const unsigned nb = (unsigned)((n + kDepBlock - 1) / kDepBlock);
+    if (kind == 0) k_deposit<0><<<nb, kDepBlock, 0, st>>>(P);
+    else if (kind == 1) k_deposit<1><<<nb, kDepBlock, 0, st>>>(P);
+    else k_deposit<2><<<nb, kDepBlock, 0, st>>>(P);
+  }
+  const int64_t nt = tprefix[n_boxes];
+  if (nt > 0)
+    k_deposit_finalize<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(nt, d_boxes, d_tprefix, n_boxes, grid[1], grid[2],
+                                                                     acc_m, acc_p, 1.0 / scale_m, 1.0 / scale_p,
+                                                                     density_dev, velocity_dev);
+  if ((e = cudaGetLastError()) != cudaSuccess) return dtfe_internal_set_error(DTFE_ERR_CUDA, cudaGetErrorString(e));
+  return DTFE_OK;
+}

@@ -705,6 +705,9 @@ struct dtfe_gpu_s {
   float* out_buf[DTFE_NUM_FIELDS] = {};
   size_t out_cap[DTFE_NUM_FIELDS] = {};
   std::map<void*, size_t> caps;  // bytes held by each device buffer
+  void* dep_scratch = nullptr;    // grid deposition scratch
+  size_t dep_bytes = 0;
+  float* dep_out = nullptr;       // host-output deposition staging (4 per cell)
 };
 
 namespace {
@@ -860,6 +863,8 @@ int dtfe_gpu_destroy(dtfe_handle h) {
     if (p) cudaFree(p);
   for (int i = 0; i < DTFE_NUM_FIELDS; ++i)
     if (h->out_buf[i]) cudaFree(h->out_buf[i]);
+  if (h->dep_scratch) cudaFree(h->dep_scratch);
+  if (h->dep_out) cudaFree(h->dep_out);
   cudaStreamDestroy(h->stream);
   delete h;
   return DTFE_OK;
@@ -1212,6 +1217,44 @@ int dtfe_gpu_set_variants(dtfe_handle h, int32_t locate_variant, int32_t eval_va
     return set_error(DTFE_ERR_ARG, "unknown launch variant");
   h->loc_variant = locate_variant;
   h->eval_variant = eval_variant;
+  return DTFE_OK;
+}
+
+int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xyz, const float* w, const float* vel, int64_t n,
+                          int32_t n_boxes, const dtfe_deposit_box* boxes, const int32_t grid[3],
+                          double average_density, float* density_dev, float* velocity_dev, void** scratch,
+                          size_t* scratch_bytes);
+
+int dtfe_gpu_deposit_dev(dtfe_handle h, int32_t kind, const float* xyz, const float* w, const float* vel, int64_t n,
+                         int32_t n_boxes, const dtfe_deposit_box* boxes, const int32_t grid[3],
+                         double average_density, float* density_dev, float* velocity_dev) {
+  if (!h || !grid || (n > 0 && !xyz)) return set_error(DTFE_ERR_ARG, "null argument");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  int64_t G = (int64_t)grid[0] * grid[1] * grid[2];
+  if (density_dev) DTFE_CUDA_TRY(cudaMemsetAsync(density_dev, 0, sizeof(float) * G, h->stream));
+  if (velocity_dev) DTFE_CUDA_TRY(cudaMemsetAsync(velocity_dev, 0, sizeof(float) * 3 * G, h->stream));
+  int rc = dtfe_gpu_deposit_impl(h->stream, kind, xyz, w, vel, n, n_boxes, boxes, grid, average_density,
+                                 density_dev, velocity_dev, &h->dep_scratch, &h->dep_bytes);
+  if (rc) return rc;
+  DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return DTFE_OK;
+}
+
+int dtfe_gpu_deposit(dtfe_handle h, int32_t kind, const float* xyz, const float* w, const float* vel, int64_t n,
+                     int32_t n_boxes, const dtfe_deposit_box* boxes, const int32_t grid[3], double average_density,
+                     float* density, float* velocity) {
+  if (!h || !grid) return set_error(DTFE_ERR_ARG, "null argument");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  int64_t G = (int64_t)grid[0] * grid[1] * grid[2];
+  int rc = dev_alloc(h, &h->dep_out, 4 * (size_t)G);
+  if (rc) return rc;
+  float* dd = density ? h->dep_out : nullptr;
+  float* dv = velocity ? h->dep_out + G : nullptr;
+  rc = dtfe_gpu_deposit_dev(h, kind, xyz, w, vel, n, n_boxes, boxes, grid, average_density, dd, dv);
+  if (rc) return rc;
+  if (density) DTFE_CUDA_TRY(cudaMemcpyAsync(density, dd, sizeof(float) * G, cudaMemcpyDeviceToHost, h->stream));
+  if (velocity) DTFE_CUDA_TRY(cudaMemcpyAsync(velocity, dv, sizeof(float) * 3 * G, cudaMemcpyDeviceToHost, h->stream));
+  DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return DTFE_OK;
 }
 

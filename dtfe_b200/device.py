@@ -110,6 +110,26 @@ class DeviceDTFE:
         self.last_status = st.as_dict()
         return self.last_status
 
+    def deposit(self, dplan, velocity: bool = True) -> dict:
+        """NGP / CIC / TSC density (and velocity) on the host."""
+        G = int(np.prod(dplan.grid))
+        dens = np.empty(G, np.float32)
+        vel = np.empty((G, 3), np.float32) if velocity and dplan.velocity is not None else None
+        grid = np.asarray(dplan.grid, np.int32)
+        N.check(self.lib.dtfe_gpu_deposit(self.h, dplan.kind, N.ptr(dplan.pos), N.ptr(dplan.weight),
+                                          N.ptr(dplan.velocity) if vel is not None else None, dplan.n,
+                                          len(dplan.boxes), C.addressof(dplan.boxes), grid.ctypes.data,
+                                          dplan.rho_bar, dens.ctypes.data, N.ptr(vel)))
+        return {"density": dens, "velocity": vel}
+
+    def deposit_dev(self, dplan, density_dev, velocity_dev=None) -> None:
+        grid = np.asarray(dplan.grid, np.int32)
+        N.check(self.lib.dtfe_gpu_deposit_dev(self.h, dplan.kind, N.ptr(dplan.pos), N.ptr(dplan.weight),
+                                              N.ptr(dplan.velocity) if velocity_dev is not None else None,
+                                              dplan.n, len(dplan.boxes), C.addressof(dplan.boxes),
+                                              grid.ctypes.data, dplan.rho_bar, N.ptr(density_dev),
+                                              N.ptr(velocity_dev)))
+
     def autotune(self, fields) -> tuple:
         chosen = (C.c_int32 * 2)()
         N.check(self.lib.dtfe_gpu_autotune(self.h, _mask(fields), chosen))

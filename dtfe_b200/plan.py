@@ -237,21 +237,13 @@ def assemble(sets: list, tiles: list, weight, velocity, scalar, grid, rho_bar, p
         padding=np.asarray(padding, np.float32), timings=timings)
 
 
-def make_plan(pos, weight, velocity=None, scalar=None, grid=(64, 64, 64), box=(0, 100, 0, 100, 0, 100),
-              periodic: bool = True, n_threads: int = 1, padding_particles: float = 5.0,
-              padding=None, average_density_value: float | None = None) -> Plan:
-    """Plans a single-box DTFE run split into parallelGrid(n_threads) sub-boxes.
+def decompose(pos, weight, grid, box, periodic: bool, n_threads: int, pad):
+    """The reference's particle selection and sub-box split (DTFE(),
+    src/DTFE.cpp:219-243, and DTFE_parallel, src/DTFE.cpp:298-356).
 
-    average_density_value=None reproduces the reference's automatic value
-    (sum of weights / 35000^3); pass sum(w)/L^3 for the physical normalisation."""
-    timings = {}
-    t0 = time.time()
+    Returns ([(source index, positions)], [(origin, dims, region, part_no)])."""
     pos = _f32(pos)
-    weight = _f32(weight) if weight is not None else np.ones(len(pos), np.float32)
     box = np.asarray(box, np.float32)
-    blen = np.array([box[1] - box[0], box[3] - box[2], box[5] - box[4]], np.float32)
-    pad = padding_length(len(pos), blen, grid, padding_particles) if padding is None else np.asarray(padding, np.float32)
-    rho_bar = average_density(weight) if average_density_value is None else float(np.float32(average_density_value))
     padded = np.array([box[0] - pad[0], box[1] + pad[1], box[2] - pad[2], box[3] + pad[3],
                        box[4] - pad[4], box[5] + pad[5]], np.float32)
     if periodic:
@@ -274,8 +266,81 @@ def make_plan(pos, weight, velocity=None, scalar=None, grid=(64, 64, 64), box=(0
             origin = (sub[k, 0], sub[k, 2], sub[k, 4])
             dims = (sub[k, 1] - sub[k, 0], sub[k, 3] - sub[k, 2], sub[k, 5] - sub[k, 4])
             tiles.append((origin, dims, region, k))
+    return sets, tiles
+
+
+def make_plan(pos, weight, velocity=None, scalar=None, grid=(64, 64, 64), box=(0, 100, 0, 100, 0, 100),
+              periodic: bool = True, n_threads: int = 1, padding_particles: float = 5.0,
+              padding=None, average_density_value: float | None = None) -> Plan:
+    """Plans a single-box DTFE run split into parallelGrid(n_threads) sub-boxes.
+
+    average_density_value=None reproduces the reference's automatic value
+    (sum of weights / 35000^3); pass sum(w)/L^3 for the physical normalisation."""
+    timings = {}
+    t0 = time.time()
+    pos = _f32(pos)
+    weight = _f32(weight) if weight is not None else np.ones(len(pos), np.float32)
+    box = np.asarray(box, np.float32)
+    blen = np.array([box[1] - box[0], box[3] - box[2], box[5] - box[4]], np.float32)
+    pad = padding_length(len(pos), blen, grid, padding_particles) if padding is None else np.asarray(padding, np.float32)
+    rho_bar = average_density(weight) if average_density_value is None else float(np.float32(average_density_value))
+    sets, tiles = decompose(pos, weight, grid, box, periodic, n_threads, pad)
     timings["selection_s"] = time.time() - t0
     return assemble(sets, tiles, weight, velocity, scalar, grid, rho_bar, pad, timings)
+
+
+@dataclass
+class DepositPlan:
+    """Particles of every region for the NGP / CIC / TSC estimators."""
+    pos: np.ndarray             # (n, 3) float32, regions concatenated
+    weight: np.ndarray          # (n,) float32
+    velocity: np.ndarray | None
+    boxes: C.Array              # dtfe_deposit_box[K]
+    grid: tuple
+    rho_bar: float
+    kind: int
+
+    @property
+    def n(self) -> int:
+        return int(self.pos.shape[0])
+
+
+DEPOSIT_KINDS = {"NGP": 0, "CIC": 1, "TSC": 2}
+
+
+def make_deposit_plan(pos, weight, velocity=None, grid=(64, 64, 64), box=(0, 100, 0, 100, 0, 100),
+                      periodic: bool = True, n_threads: int = 1, kind: str = "TSC",
+                      average_density_value: float | None = None) -> DepositPlan:
+    """The reference's flow for a grid-deposition run: padding of one cell for
+    NGP/TSC and none for CIC (updatePadding, src/user_options.cc:1073-1078),
+    periodic images, sub-box split; each region's particles Morton-ordered."""
+    k = DEPOSIT_KINDS[kind]
+    pos = _f32(pos)
+    weight = _f32(weight) if weight is not None else np.ones(len(pos), np.float32)
+    box = np.asarray(box, np.float32)
+    blen = np.array([box[1] - box[0], box[3] - box[2], box[5] - box[4]], np.float32)
+    pad = padding_length(len(pos), blen, grid, 5.0, kind=2 if k == 1 else 1)
+    rho_bar = average_density(weight) if average_density_value is None else float(np.float32(average_density_value))
+    sets, tiles = decompose(pos, weight, grid, box, periodic, n_threads, pad)
+    boxes = (N.DepositBox * len(sets))()
+    allp, srcs = [], []
+    off = 0
+    for i, ((src, p), (origin, dims, region, _)) in enumerate(zip(sets, tiles)):
+        o = morton_order(p)
+        allp.append(p[o])
+        srcs.append(src[o])
+        b = boxes[i]
+        b.particle_offset, b.n_particles = off, len(p)
+        for a in range(6):
+            b.region[a] = float(region[a])
+        for a in range(3):
+            b.tile_origin[a] = int(origin[a])
+            b.tile_dims[a] = int(dims[a])
+        off += len(p)
+    src = np.concatenate(srcs).astype(np.int64)
+    return DepositPlan(pos=np.ascontiguousarray(np.concatenate(allp)), weight=np.ascontiguousarray(weight[src]),
+                       velocity=None if velocity is None else np.ascontiguousarray(np.asarray(velocity, np.float32)[src]),
+                       boxes=boxes, grid=tuple(int(g) for g in grid), rho_bar=rho_bar, kind=k)
 
 
 def make_subbox_plan(subboxes: list, grid=(64, 64, 64), padding_fraction: float = 0.1,

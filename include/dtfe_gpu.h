@@ -161,6 +161,37 @@ int dtfe_gpu_interpolate(dtfe_handle h, const dtfe_interp_opts* opts,
 int dtfe_gpu_interpolate_dev(dtfe_handle h, const dtfe_interp_opts* opts,
                              float* const out_dev[DTFE_NUM_FIELDS], dtfe_status* st);
 
+/* ---- NGP / CIC / TSC comparison estimators ------------------------------
+ * One record per region (the reference deposits per sub-box region, with
+ * stencils clipped at the region's edges): the region's particles are
+ * [particle_offset, particle_offset + n_particles) of the particle arrays and
+ * its cells are the tile at tile_origin of the main grid. */
+typedef struct {
+  int64_t particle_offset, n_particles;
+  float region[6];          /* xmin, xmax, ymin, ymax, zmin, zmax */
+  int32_t tile_origin[3];
+  int32_t tile_dims[3];
+} dtfe_deposit_box;
+enum { DTFE_DEPOSIT_NGP = 0, DTFE_DEPOSIT_CIC = 1, DTFE_DEPOSIT_TSC = 2 };
+
+/* Deposits particle mass and momentum onto the grid and returns density
+ * (normalised as the reference: cells / Box::volume() / average_density, with
+ * the reference's fixed Box::volume() of 35000^3) and velocity = momentum /
+ * mass.  Host arrays: xyz 3n, w n (NULL: unit weights), vel 3n (NULL: no
+ * velocity); density (G floats) and velocity (3G floats, may be NULL) are host
+ * outputs; cells outside every tile are 0.  Sums are exact (64-bit fixed
+ * point) and so independent of thread order.
+ * (NGP_interpolation_regular_grid src/NGP_interpolation.cc:67-136,
+ *  CIC_interpolation_regular_grid src/CIC_interpolation.cc:67-273,
+ *  TSC_interpolation_regular_grid src/TSC_interpolation.cc:67-254.) */
+int dtfe_gpu_deposit(dtfe_handle h, int32_t kind, const float* xyz, const float* w, const float* vel,
+                     int64_t n, int32_t n_boxes, const dtfe_deposit_box* boxes, const int32_t grid[3],
+                     double average_density, float* density, float* velocity);
+/* Same with device outputs (density_dev: G floats, velocity_dev: 3G or NULL). */
+int dtfe_gpu_deposit_dev(dtfe_handle h, int32_t kind, const float* xyz, const float* w, const float* vel,
+                         int64_t n, int32_t n_boxes, const dtfe_deposit_box* boxes, const int32_t grid[3],
+                         double average_density, float* density_dev, float* velocity_dev);
+
 /* Autotuner: times each launch variant of the point-location kernel
  * (register budget per block, cells per thread seeded from the previous hit)
  * and of the evaluation kernel on the loaded data, for the cell-centre method

@@ -36,8 +36,37 @@ def lib() -> C.CDLL:
         L.oracle_interpolate.argtypes = [C.c_int64, vp, vp, C.c_int64, vp, vp, vp, C.c_int, vp, vp, C.c_int,
                                          vp, vp, vp, vp, vp, C.POINTER(N.InterpOpts), C.c_int,
                                          C.POINTER(C.c_void_p), vp, C.c_int, vp]
+        L.oracle_deposit.argtypes = [C.c_int, C.c_int, vp, vp, vp, C.c_int64, vp, vp, C.c_double, vp, vp]
         _lib = L
     return _lib
+
+
+def deposit(dplan, mode: int = MODE_REF, velocity: bool = True):
+    """NGP / CIC / TSC per region (NGP/CIC/TSC_interpolation_regular_grid),
+    placed into the main grid: (density (G,), velocity (G, 3) or None)."""
+    g = dplan.grid
+    dens = np.zeros(g, np.float64)
+    vel = np.zeros(g + (3,), np.float64) if velocity and dplan.velocity is not None else None
+    for b in dplan.boxes:
+        o, n = b.particle_offset, b.n_particles
+        dims = np.array([b.tile_dims[0], b.tile_dims[1], b.tile_dims[2]], np.int32)
+        region = np.array(list(b.region), np.float32)
+        td = np.zeros(int(np.prod(dims)), np.float64)
+        tv = np.zeros((int(np.prod(dims)), 3), np.float64) if vel is not None else None
+        pos = np.ascontiguousarray(dplan.pos[o:o + n])
+        w = np.ascontiguousarray(dplan.weight[o:o + n])
+        v = np.ascontiguousarray(dplan.velocity[o:o + n]) if vel is not None else None
+        rc = lib().oracle_deposit(dplan.kind, mode, pos.ctypes.data, w.ctypes.data,
+                                  None if v is None else v.ctypes.data, n, region.ctypes.data, dims.ctypes.data,
+                                  dplan.rho_bar, td.ctypes.data, None if tv is None else tv.ctypes.data)
+        if rc:
+            raise RuntimeError("oracle_deposit failed")
+        x0, y0, z0 = b.tile_origin[0], b.tile_origin[1], b.tile_origin[2]
+        dens[x0:x0 + dims[0], y0:y0 + dims[1], z0:z0 + dims[2]] = td.reshape(dims)
+        if vel is not None:
+            vel[x0:x0 + dims[0], y0:y0 + dims[1], z0:z0 + dims[2]] = tv.reshape(tuple(dims) + (3,))
+    G = int(np.prod(g))
+    return dens.reshape(G), None if vel is None else vel.reshape(G, 3)
 
 
 def vertex_density(plan, rho_bar: float | None = None, nthreads: int = 0):

@@ -43,3 +43,31 @@ def rel_err(a, b):
     if rms == 0:
         rms = 1.0
     return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), rms))) if b.size else 0.0
+
+
+GOLDEN = os.path.join(ROOT, "tests", "golden", "ref_zeldovich10.npz")
+
+
+def golden():
+    return dict(np.load(GOLDEN))
+
+
+def golden_plan(g):
+    """A single-box Plan rebuilt from the fixture's stored tessellation."""
+    import ctypes as C
+    from dtfe_b200 import _native as N
+    from dtfe_b200.plan import Plan
+    boxes = (N.Subbox * 1)()
+    b = boxes[0]
+    b.vert_offset, b.n_verts, b.tet_offset, b.n_tets = 0, len(g["xyz"]), 0, len(g["tet_v"])
+    for a in range(3):
+        b.tile_origin[a] = 0
+        b.tile_dims[a] = int(g["grid"][a])
+        b.dx[a] = float(g["box_dx"][a])
+        b.lo[a] = float(g["box_lo"][a])
+    b.coord_offset[0] = b.coord_offset[1] = b.coord_offset[2] = 0
+    b.part_no = -1
+    return Plan(tet_v=g["tet_v"], tet_n=g["tet_n"], xyz=g["xyz"], src=np.arange(len(g["xyz"]), dtype=np.int32),
+                weight=g["weight"], velocity=g["velocity"], scalar=g["scalar"], boxes=boxes, xs=g["xs"],
+                ys=g["ys"], zs=g["zs"], grid=tuple(int(x) for x in g["grid"]), rho_bar=float(g["rho_bar"]),
+                padding=g["padding"])

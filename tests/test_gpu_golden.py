@@ -1,0 +1,58 @@
+"""The CUDA path (through the C ABI) against the reference's own outputs
+(tests/golden/ref_zeldovich10.npz).  Bar: relative error <= 1e-6 (the GPU sums
+vertex volumes in FP64 where the reference sums them in float, which moves
+densities by ~1e-7)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import golden, golden_plan, rel_err
+from dtfe_b200 import _native as N
+
+pytestmark = pytest.mark.gpu
+FIELDS = ["density", "velocity", "velocity_gradient", "scalar", "scalar_gradient"]
+
+
+@pytest.fixture(scope="module")
+def g(gpu_built):
+    return golden()
+
+
+def test_gpu_vs_reference_fields(g):
+    from dtfe_b200.device import DeviceDTFE
+    plan = golden_plan(g)
+    with DeviceDTFE(0, 1) as d:
+        d.load(plan)
+        d.vertex_density(plan.rho_bar)
+        assert rel_err(d.download_vertex_density(plan.n_verts), g["ref_vertex_density"]) <= 1e-6
+        for method, nn, tag in ((0, 1, "centre"), (3, 8, "equidistant8")):
+            out = d.interpolate(FIELDS, method=method, n_samples=nn)
+            for f in FIELDS:
+                assert rel_err(out[f], g[f"ref_{tag}_{f}"].reshape(out[f].shape)) <= 1e-6, (tag, f)
+
+
+@pytest.mark.parametrize("kind,name", [(0, "ngp"), (1, "cic"), (2, "tsc")])
+def test_gpu_deposit_vs_reference(g, kind, name):
+    from dtfe_b200.device import DeviceDTFE
+    pos, w, vel = g["particles_pos"], g["particles_w"], g["particles_vel"]
+    boxes = (N.DepositBox * 1)()
+    b = boxes[0]
+    b.particle_offset, b.n_particles = 0, len(pos)
+    for a in range(6):
+        b.region[a] = float(g["deposit_region"][a])
+    for a in range(3):
+        b.tile_origin[a] = 0
+        b.tile_dims[a] = int(g["deposit_grid"][a])
+    grid = np.ascontiguousarray(g["deposit_grid"], np.int32)
+    G = int(np.prod(grid))
+    dens = np.zeros(G, np.float32)
+    v = np.zeros((G, 3), np.float32)
+    with DeviceDTFE(0, 0) as d:
+        N.check(d.lib.dtfe_gpu_deposit(d.h, kind, pos.ctypes.data, w.ctypes.data, vel.ctypes.data, len(pos), 1,
+                                       C.addressof(boxes), grid.ctypes.data, float(g["rho_bar"]),
+                                       dens.ctypes.data, v.ctypes.data))
+    ref_d, ref_v = g[f"ref_{name}_density"], g[f"ref_{name}_velocity"]
+    assert rel_err(dens, ref_d) <= 1e-6
+    m = ref_d != 0
+    assert rel_err(v[m], ref_v[m]) <= (1e-4 if kind == 1 else 1e-6)

@@ -41,6 +41,17 @@ struct DepBox {
   float factor;           // density normalisation of this region
 };
 
+struct DepSaved {
+  const float4* pw;
+  const DepBox* boxes;
+  const int64_t* prefix;
+  int K;
+  int64_t n;
+  int kind;
+  int64_t G1, G2, G;
+  int valid;
+};
+
 struct DepParams {
   const float4* pw;       // x, y, z, weight
   const float4* vel;      // vx, vy, vz, 0 (may be null)
@@ -274,6 +285,99 @@ __global__ void k_deposit_finalize(int64_t n_tile_cells, const DepBox* __restric
   if (density) density[idx] = m * B.factor;
 }
 
+// Adjoint of the deposited density for one particle: with loss weights
+// a_c = dL/d(density_c) and density_c = factor_b * sum_p m_p W_pc,
+//   dL/dm_p = factor_b sum_c a_c W_pc,  dL/dx_p = factor_b m_p sum_c a_c dW_pc/dx_p.
+// W_pc is the product of the per-axis stencil weights of the forward pass;
+// their derivatives follow the same clipped formulas (NGP: zero).
+template <int KIND>
+__device__ __forceinline__ void axis_stencil_grad(bool inner, float temp_in, int n, float dx, int cell[3],
+                                                  float w[3], float dw[3], int& count) {
+  axis_stencil<KIND>(inner, temp_in, n, cell, w, count);
+  float t;
+  if (inner) t = (float)((double)temp_in - ((double)((int)floorf(temp_in)) + 0.5));
+  else {
+    int ti = (int)floorf(temp_in);
+    t = (float)((double)temp_in - ((double)ti + 0.5));
+  }
+  const float s = 1.f / dx;
+  for (int q = 0; q < 3; ++q) dw[q] = 0.f;
+  if (KIND == 1) {
+    // every CIC branch is linear in t: recover the slope from the formulas
+    if (inner) {
+      if (t < 0.f) { dw[0] = -s; dw[1] = s; dw[2] = 0.f; }
+      else { dw[0] = 0.f; dw[1] = -s; dw[2] = s; }
+    } else {
+      int ti = (int)floorf(temp_in);
+      if (ti == -1) dw[0] = s;
+      else if (ti == 0) { dw[0] = -s; dw[1] = s; }
+      else if (ti == n - 1) { dw[0] = -s; dw[1] = s; }
+      else if (ti == n) dw[0] = -s;
+      else if (!(ti < -1 || ti > n)) {
+        if (t < 0.f) { dw[0] = -s; dw[1] = s; dw[2] = 0.f; }
+        else { dw[0] = 0.f; dw[1] = -s; dw[2] = s; }
+      }
+    }
+  } else if (KIND == 2) {
+    const float da = -(0.5f - t) * s, db = -2.f * t * s, dc = (0.5f + t) * s;
+    if (inner) { dw[0] = da; dw[1] = db; dw[2] = dc; }
+    else {
+      int ti = (int)floorf(temp_in);
+      if (ti == -1) dw[0] = dc;
+      else if (ti == 0) { dw[0] = db; dw[1] = dc; }
+      else if (ti == n - 1) { dw[0] = da; dw[1] = db; }
+      else if (ti == n) dw[0] = da;
+      else if (!(ti < -1 || ti > n)) { dw[0] = da; dw[1] = db; dw[2] = dc; }
+    }
+  }
+}
+
+template <int KIND>
+__global__ void k_deposit_adjoint(const float4* __restrict__ pw, const DepBox* __restrict__ boxes,
+                                  const int64_t* __restrict__ prefix, int K, int64_t n, int64_t G1, int64_t G2,
+                                  const float* __restrict__ a, float* __restrict__ gx, float* __restrict__ gw) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int b = find_dep_box(prefix, K, i);
+  const DepBox& B = boxes[b];
+  const float4 q = pw[i];
+  const float p[3] = {q.x, q.y, q.z};
+  int cell[3][3], count[3] = {0, 0, 0};
+  float w[3][3], dw[3][3];
+  if (KIND == 0) {
+    bool ok = true;
+    for (int j = 0; j < 3; ++j) {
+      cell[j][0] = (int)floorf((p[j] - B.lo[j]) / B.dx[j]);
+      w[j][0] = 1.f;
+      dw[j][0] = 0.f;
+      ok = ok && cell[j][0] >= 0 && cell[j][0] < B.dims[j];
+    }
+    if (ok) count[0] = count[1] = count[2] = 1;
+  } else {
+    const bool inner = in_box(p, B.inner);
+    if (inner || in_box(p, B.outer))
+      for (int j = 0; j < 3; ++j)
+        axis_stencil_grad<KIND>(inner, (p[j] - B.lo[j]) / B.dx[j], B.dims[j], B.dx[j], cell[j], w[j], dw[j],
+                                count[j]);
+  }
+  double sm = 0.0, sx[3] = {0.0, 0.0, 0.0};
+  for (int x0 = 0; x0 < count[0]; ++x0)
+    for (int x1 = 0; x1 < count[1]; ++x1)
+      for (int x2 = 0; x2 < count[2]; ++x2) {
+        const int64_t idx = ((int64_t)(B.origin[0] + cell[0][x0]) * G1 + (B.origin[1] + cell[1][x1])) * G2 +
+                            (B.origin[2] + cell[2][x2]);
+        const double ac = (double)a[idx];
+        if (ac == 0.0) continue;
+        sm += ac * (double)w[0][x0] * w[1][x1] * w[2][x2];
+        sx[0] += ac * (double)dw[0][x0] * w[1][x1] * w[2][x2];
+        sx[1] += ac * (double)w[0][x0] * dw[1][x1] * w[2][x2];
+        sx[2] += ac * (double)w[0][x0] * w[1][x1] * dw[2][x2];
+      }
+  if (gw) gw[i] = (float)(B.factor * sm);
+  if (gx)
+    for (int j = 0; j < 3; ++j) gx[3 * i + j] = (float)(B.factor * (double)q.w * sx[j]);
+}
+
 __global__ void k_pack4(int64_t n, const float* __restrict__ a3, const float* __restrict__ b1, float4* __restrict__ out) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) out[i] = make_float4(a3[3 * i], a3[3 * i + 1], a3[3 * i + 2], b1 ? b1[i] : 1.f);
@@ -281,10 +385,12 @@ __global__ void k_pack4(int64_t n, const float* __restrict__ a3, const float* __
 
 }  // namespace
 
+extern "C" size_t dtfe_internal_deposit_saved_size() { return sizeof(DepSaved); }
+
 extern "C" int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xyz, const float* w, const float* vel,
                                      int64_t n, int32_t n_boxes, const dtfe_deposit_box* boxes,
                                      const int32_t grid[3], double average_density, float* density_dev,
-                                     float* velocity_dev, void** scratch, size_t* scratch_bytes) {
+                                     float* velocity_dev, void** scratch, size_t* scratch_bytes, void* saved) {
   if (kind < 0 || kind > 2) return dtfe_internal_set_error(DTFE_ERR_ARG, "deposit kind must be 0 (NGP), 1 (CIC), 2 (TSC)");
   if (n < 0 || n_boxes <= 0 || !boxes || !grid) return dtfe_internal_set_error(DTFE_ERR_ARG, "bad deposit arguments");
   if (!(average_density > 0.0)) return dtfe_internal_set_error(DTFE_ERR_ARG, "averageDensity must be positive");
@@ -405,5 +511,34 @@ extern "C" int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xy
                                                                      acc_m, acc_p, 1.0 / scale_m, 1.0 / scale_p,
                                                                      density_dev, velocity_dev);
   if ((e = cudaGetLastError()) != cudaSuccess) return dtfe_internal_set_error(DTFE_ERR_CUDA, cudaGetErrorString(e));
+  // state for dtfe_gpu_deposit_adjoint (the scratch keeps particles and boxes)
+  DepSaved& sv = *(DepSaved*)saved;
+  sv.pw = d_pw;
+  sv.boxes = d_boxes;
+  sv.prefix = d_prefix;
+  sv.K = n_boxes;
+  sv.n = n;
+  sv.kind = kind;
+  sv.G1 = grid[1];
+  sv.G2 = grid[2];
+  sv.G = G;
+  sv.valid = 1;
   return DTFE_OK;
+}
+
+extern "C" int dtfe_gpu_deposit_adjoint_impl(void* stream, const void* saved, const float* a_dev, float* gx_dev,
+                                             float* gw_dev) {
+  const DepSaved& sv = *(const DepSaved*)saved;
+  if (!sv.valid) return dtfe_internal_set_error(DTFE_ERR_STATE, "no forward deposit on this handle");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (sv.n == 0) return DTFE_OK;
+  const unsigned nb = (unsigned)((sv.n + 255) / 256);
+  if (sv.kind == 0)
+    k_deposit_adjoint<0><<<nb, 256, 0, st>>>(sv.pw, sv.boxes, sv.prefix, sv.K, sv.n, sv.G1, sv.G2, a_dev, gx_dev, gw_dev);
+  else if (sv.kind == 1)
+    k_deposit_adjoint<1><<<nb, 256, 0, st>>>(sv.pw, sv.boxes, sv.prefix, sv.K, sv.n, sv.G1, sv.G2, a_dev, gx_dev, gw_dev);
+  else
+    k_deposit_adjoint<2><<<nb, 256, 0, st>>>(sv.pw, sv.boxes, sv.prefix, sv.K, sv.n, sv.G1, sv.G2, a_dev, gx_dev, gw_dev);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? DTFE_OK : dtfe_internal_set_error(DTFE_ERR_CUDA, cudaGetErrorString(e));
 }

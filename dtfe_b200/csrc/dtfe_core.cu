@@ -708,6 +708,13 @@ struct dtfe_gpu_s {
   void* dep_scratch = nullptr;    // grid deposition scratch
   size_t dep_bytes = 0;
   float* dep_out = nullptr;       // host-output deposition staging (4 per cell)
+  alignas(16) char dep_saved[128] = {};  // particle/box state of the last deposit (adjoint)
+  // adjoint state
+  bool tet_c_valid = false;       // tet_c holds the centres of the last centre interpolation
+  bool tet_c_fix = false;         // that interpolation used DTFE_FLAG_FIX_VALUE_INTERP
+  float factor = 0.f;             // (D+1)/rho_bar of the last vertex-density call
+  double *g_rho = nullptr, *g_x = nullptr, *g_v = nullptr, *g_S = nullptr, *g_m = nullptr, *vbar = nullptr;
+  float* adj_a = nullptr;         // device copies of host loss weights
 };
 
 namespace {
@@ -864,6 +871,9 @@ int dtfe_gpu_destroy(dtfe_handle h) {
   for (int i = 0; i < DTFE_NUM_FIELDS; ++i)
     if (h->out_buf[i]) cudaFree(h->out_buf[i]);
   if (h->dep_scratch) cudaFree(h->dep_scratch);
+  for (void* p : {(void*)h->g_rho, (void*)h->g_x, (void*)h->g_v, (void*)h->g_S, (void*)h->g_m, (void*)h->vbar,
+                  (void*)h->adj_a})
+    if (p) cudaFree(p);
   if (h->dep_out) cudaFree(h->dep_out);
   cudaStreamDestroy(h->stream);
   delete h;
@@ -946,6 +956,7 @@ int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n, i
   h->has_scal = scal != nullptr;
   h->density_ready = false;
   h->bins_ready = false;
+  h->tet_c_valid = false;
   return DTFE_OK;
 }
 
@@ -1023,6 +1034,7 @@ int dtfe_gpu_vertex_density(dtfe_handle h, double rho_bar) {
   // the reference's factor: (NO_DIM+1.)/averageDensity stored as Real
   float rb = (float)rho_bar;
   float factor = (float)(4.0 / (double)rb);
+  h->factor = factor;
   k_vertex_density<<<blocks_for(h->V, kDensBlock), kDensBlock, 0, st>>>(h->V, h->w, h->vol, h->inc_off, h->inc,
                                                                        h->hull, factor, h->posd);
   DTFE_CUDA_TRY(cudaGetLastError());
@@ -1123,6 +1135,8 @@ static int interpolate_impl(dtfe_handle h, const dtfe_interp_opts* o, float* con
   if ((rc = dev_alloc(h, &h->tet_c, h->n_cells))) return rc;
   launch_locate(h->loc_variant, P, h->tet_c, st);
   launch_eval_s(method, h->S, h->eval_variant, P, h->tet_c, st, grid, block);
+  h->tet_c_valid = method == DTFE_METHOD_CENTRE;  // the adjoint differentiates centre values only
+  h->tet_c_fix = (o->flags & DTFE_FLAG_FIX_VALUE_INTERP) != 0;
   DTFE_CUDA_TRY(cudaGetLastError());
   unsigned long long cnt[CNT_N];
   DTFE_CUDA_TRY(cudaMemcpyAsync(cnt, h->counters, sizeof(cnt), cudaMemcpyDeviceToHost, st));
@@ -1223,7 +1237,18 @@ int dtfe_gpu_set_variants(dtfe_handle h, int32_t locate_variant, int32_t eval_va
 int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xyz, const float* w, const float* vel, int64_t n,
                           int32_t n_boxes, const dtfe_deposit_box* boxes, const int32_t grid[3],
                           double average_density, float* density_dev, float* velocity_dev, void** scratch,
-                          size_t* scratch_bytes);
+                          size_t* scratch_bytes, void* saved);
+int dtfe_gpu_deposit_adjoint_impl(void* stream, const void* saved, const float* a_dev, float* gx_dev, float* gw_dev);
+int dtfe_internal_adjoint(void* stream, const void* cell_params, int64_t n_cells, int64_t V, int64_t T,
+                          const int4* tet_v, const float4* posd, const float* w, const int* hull, const double* vol,
+                          const int64_t* off, const int* inc, float factor, double* g_rho, double* g_x, double* g_v,
+                          double* g_S, double* g_m, double* vbar, float* out_x, float* out_v, float* out_w);
+size_t dtfe_internal_adjoint_params_size();
+void dtfe_internal_adjoint_fill_params(void* out, const int4* tet_v, const float4* posd, const float4* vel4,
+                                       const int* tet_c, const dtfe_subbox* boxes, const int64_t* tile_prefix,
+                                       const float* xs, const float* ys, const float* zs, int K, int64_t G1,
+                                       int64_t G2, int64_t n_total, const float* a, const float* b,
+                                       const float* c, int full_value);
 
 int dtfe_gpu_deposit_dev(dtfe_handle h, int32_t kind, const float* xyz, const float* w, const float* vel, int64_t n,
                          int32_t n_boxes, const dtfe_deposit_box* boxes, const int32_t grid[3],
@@ -1234,7 +1259,7 @@ int dtfe_gpu_deposit_dev(dtfe_handle h, int32_t kind, const float* xyz, const fl
   if (density_dev) DTFE_CUDA_TRY(cudaMemsetAsync(density_dev, 0, sizeof(float) * G, h->stream));
   if (velocity_dev) DTFE_CUDA_TRY(cudaMemsetAsync(velocity_dev, 0, sizeof(float) * 3 * G, h->stream));
   int rc = dtfe_gpu_deposit_impl(h->stream, kind, xyz, w, vel, n, n_boxes, boxes, grid, average_density,
-                                 density_dev, velocity_dev, &h->dep_scratch, &h->dep_bytes);
+                                 density_dev, velocity_dev, &h->dep_scratch, &h->dep_bytes, h->dep_saved);
   if (rc) return rc;
   DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return DTFE_OK;
@@ -1254,6 +1279,41 @@ int dtfe_gpu_deposit(dtfe_handle h, int32_t kind, const float* xyz, const float*
   if (rc) return rc;
   if (density) DTFE_CUDA_TRY(cudaMemcpyAsync(density, dd, sizeof(float) * G, cudaMemcpyDeviceToHost, h->stream));
   if (velocity) DTFE_CUDA_TRY(cudaMemcpyAsync(velocity, dv, sizeof(float) * 3 * G, cudaMemcpyDeviceToHost, h->stream));
+  DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return DTFE_OK;
+}
+
+int dtfe_gpu_adjoint_dev(dtfe_handle h, const float* grad_density_dev, const float* grad_velocity_dev,
+                         const float* grad_divergence_dev, float* grad_xyz_dev, float* grad_vel_dev,
+                         float* grad_w_dev) {
+  if (!h || !grad_xyz_dev) return set_error(DTFE_ERR_ARG, "null argument");
+  if (!h->density_ready || !h->tet_c_valid)
+    return set_error(DTFE_ERR_STATE, "adjoint needs a preceding vertex density and cell-centre interpolation");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  int rc;
+  if ((rc = dev_alloc(h, &h->g_rho, h->V)) || (rc = dev_alloc(h, &h->g_x, 3 * h->V)) ||
+      (rc = dev_alloc(h, &h->g_v, 3 * h->V)) || (rc = dev_alloc(h, &h->g_S, h->V)) ||
+      (rc = dev_alloc(h, &h->g_m, h->V)) || (rc = dev_alloc(h, &h->vbar, h->T)))
+    return rc;
+  alignas(16) char params[512];
+  if (dtfe_internal_adjoint_params_size() > sizeof(params)) return set_error(DTFE_ERR_STATE, "params size");
+  dtfe_internal_adjoint_fill_params(params, h->tet_v, h->posd, h->vel4, h->tet_c, h->boxes, h->tile_prefix, h->xs,
+                                    h->ys, h->zs, h->K, h->grid[1], h->grid[2], h->n_cells, grad_density_dev,
+                                    grad_divergence_dev, grad_velocity_dev, h->tet_c_fix ? 1 : 0);
+  rc = dtfe_internal_adjoint(h->stream, params, h->n_cells, h->V, h->T, h->tet_v, h->posd, h->w, h->hull, h->vol,
+                             h->inc_off, h->inc, h->factor, h->g_rho, h->g_x, h->g_v, h->g_S, h->g_m, h->vbar,
+                             grad_xyz_dev, grad_vel_dev, grad_w_dev);
+  if (rc) return set_error(rc, "adjoint kernels failed");
+  DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return DTFE_OK;
+}
+
+int dtfe_gpu_deposit_adjoint_dev(dtfe_handle h, const float* grad_density_dev, float* grad_xyz_dev,
+                                 float* grad_w_dev) {
+  if (!h || !grad_density_dev) return set_error(DTFE_ERR_ARG, "null argument");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  int rc = dtfe_gpu_deposit_adjoint_impl(h->stream, h->dep_saved, grad_density_dev, grad_xyz_dev, grad_w_dev);
+  if (rc) return rc;
   DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return DTFE_OK;
 }

@@ -130,6 +130,21 @@ class DeviceDTFE:
                                               grid.ctypes.data, dplan.rho_bar, N.ptr(density_dev),
                                               N.ptr(velocity_dev)))
 
+    def adjoint_dev(self, grad_xyz, grad_density=None, grad_velocity=None, grad_divergence=None,
+                    grad_vel=None, grad_w=None) -> None:
+        """Vertex gradients of sum(a*density + c.velocity + b*divergence) of the
+        last centre interpolation (device tensors: a, b (G,), c (G, 3);
+        outputs grad_xyz (V, 3), grad_vel (V, 3), grad_w (V,))."""
+        N.check(self.lib.dtfe_gpu_adjoint_dev(self.h, N.ptr(grad_density), N.ptr(grad_velocity),
+                                              N.ptr(grad_divergence), N.ptr(grad_xyz), N.ptr(grad_vel),
+                                              N.ptr(grad_w)))
+
+    def deposit_adjoint_dev(self, grad_density, grad_xyz, grad_w=None) -> None:
+        """Particle gradients of sum(a*density) of the last deposit on this
+        handle (device tensors: a (G,); outputs grad_xyz (n, 3), grad_w (n,))."""
+        N.check(self.lib.dtfe_gpu_deposit_adjoint_dev(self.h, N.ptr(grad_density), N.ptr(grad_xyz),
+                                                      N.ptr(grad_w)))
+
     def autotune(self, fields) -> tuple:
         chosen = (C.c_int32 * 2)()
         N.check(self.lib.dtfe_gpu_autotune(self.h, _mask(fields), chosen))

@@ -299,6 +299,7 @@ class DepositPlan:
     grid: tuple
     rho_bar: float
     kind: int
+    src: np.ndarray | None = None  # (n,) int64 input particle of each deposited copy
 
     @property
     def n(self) -> int:
@@ -340,7 +341,7 @@ def make_deposit_plan(pos, weight, velocity=None, grid=(64, 64, 64), box=(0, 100
     src = np.concatenate(srcs).astype(np.int64)
     return DepositPlan(pos=np.ascontiguousarray(np.concatenate(allp)), weight=np.ascontiguousarray(weight[src]),
                        velocity=None if velocity is None else np.ascontiguousarray(np.asarray(velocity, np.float32)[src]),
-                       boxes=boxes, grid=tuple(int(g) for g in grid), rho_bar=rho_bar, kind=k)
+                       boxes=boxes, grid=tuple(int(g) for g in grid), rho_bar=rho_bar, kind=k, src=src)
 
 
 def make_subbox_plan(subboxes: list, grid=(64, 64, 64), padding_fraction: float = 0.1,

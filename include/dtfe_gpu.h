@@ -192,6 +192,28 @@ int dtfe_gpu_deposit_dev(dtfe_handle h, int32_t kind, const float* xyz, const fl
                          int64_t n, int32_t n_boxes, const dtfe_deposit_box* boxes, const int32_t grid[3],
                          double average_density, float* density_dev, float* velocity_dev);
 
+/* ---- adjoints (no counterpart in the reference, which has no gradients) --
+ * Gradients of L = sum_c a_c density_c + c_c . velocity_c + b_c divergence_c
+ * (the grids of the preceding dtfe_gpu_interpolate* call on the same handle,
+ * which must have used DTFE_METHOD_CENTRE) with respect to the vertex
+ * positions (3V floats), velocities (3V, may be NULL) and weights (V, may be
+ * NULL), at fixed tessellation topology and fixed cell -> tetrahedron
+ * assignment.  a = grad_density_dev (G floats), c = grad_velocity_dev (3G),
+ * b = grad_divergence_dev (G); each may be NULL (zero).  The velocity value
+ * is differentiated as the forward call evaluated it (with or without
+ * DTFE_FLAG_FIX_VALUE_INTERP).  All pointers are device pointers.  Vertices
+ * that are periodic images of one particle each receive their own share; the
+ * particle's gradient is their sum.  DTFE_ERR_STATE without a preceding
+ * vertex density and centre interpolation. */
+int dtfe_gpu_adjoint_dev(dtfe_handle h, const float* grad_density_dev, const float* grad_velocity_dev,
+                         const float* grad_divergence_dev, float* grad_xyz_dev, float* grad_vel_dev,
+                         float* grad_w_dev);
+/* Gradient of L = sum_c a_c density_c for the density of the last
+ * dtfe_gpu_deposit* call on this handle, with respect to that call's particle
+ * positions (3n) and weights (n, may be NULL); device pointers. */
+int dtfe_gpu_deposit_adjoint_dev(dtfe_handle h, const float* grad_density_dev, float* grad_xyz_dev,
+                                 float* grad_w_dev);
+
 /* Autotuner: times each launch variant of the point-location kernel
  * (register budget per block, cells per thread seeded from the previous hit)
  * and of the evaluation kernel on the loaded data, for the cell-centre method

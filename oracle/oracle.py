@@ -37,6 +37,15 @@ def lib() -> C.CDLL:
                                          vp, vp, vp, vp, vp, C.POINTER(N.InterpOpts), C.c_int,
                                          C.POINTER(C.c_void_p), vp, C.c_int, vp]
         L.oracle_deposit.argtypes = [C.c_int, C.c_int, vp, vp, vp, C.c_int64, vp, vp, C.c_double, vp, vp]
+        L.oracle_dtfe_loss.argtypes = [C.c_int64, vp, C.c_int64, vp, vp, vp, vp, C.c_double, C.c_int64, vp, vp,
+                                       vp, vp, vp, C.c_int]
+        L.oracle_dtfe_loss.restype = C.c_double
+        L.oracle_dtfe_grad.argtypes = [C.c_int64, vp, C.c_int64, vp, vp, vp, vp, C.c_double, C.c_int64, vp, vp,
+                                       vp, vp, vp, C.c_int, vp, vp, vp]
+        L.oracle_dtfe_fd.argtypes = [C.c_int64, vp, C.c_int64, vp, vp, vp, vp, C.c_double, C.c_int64, vp, vp,
+                                     vp, vp, vp, C.c_int, C.c_int64, vp, vp, C.c_double, C.c_double, C.c_double, vp]
+        L.oracle_deposit_loss_grad.argtypes = [C.c_int, vp, vp, C.c_int64, vp, vp, C.c_double, vp, vp, vp]
+        L.oracle_deposit_loss_grad.restype = C.c_double
         _lib = L
     return _lib
 
@@ -127,3 +136,111 @@ def interpolate(plan, dens32, dens64, fields, method: int = 0, n_samples: int = 
     if nfail.value:
         raise RuntimeError(f"oracle walk failed on {nfail.value} samples")
     return arrs, loc
+
+
+# ---- adjoint checker -------------------------------------------------------
+
+def cell_points(plan) -> np.ndarray:
+    """(G, 3) float64 sample point of every main-grid cell (zeros outside
+    every tile), as the interpolation evaluates them."""
+    G1, G2 = plan.grid[1], plan.grid[2]
+    pts = np.zeros((int(np.prod(plan.grid)), 3), np.float64)
+    for b in plan.boxes:
+        d = [b.tile_dims[a] for a in range(3)]
+        i, j, k = np.meshgrid(np.arange(d[0]), np.arange(d[1]), np.arange(d[2]), indexing="ij")
+        cell = ((b.tile_origin[0] + i) * G1 + (b.tile_origin[1] + j)) * G2 + (b.tile_origin[2] + k)
+        pts[cell.ravel(), 0] = plan.xs[b.coord_offset[0] + i.ravel()]
+        pts[cell.ravel(), 1] = plan.ys[b.coord_offset[1] + j.ravel()]
+        pts[cell.ravel(), 2] = plan.zs[b.coord_offset[2] + k.ravel()]
+    return pts
+
+
+def hull_marks(plan) -> np.ndarray:
+    """(V,) int32: 1 for vertices of a hull face (a face without neighbour)."""
+    h = np.zeros(plan.n_verts, np.int32)
+    tv, tn = plan.tet_v, plan.tet_n
+    for f in range(4):
+        faces = tn[:, f] < 0
+        for a in range(4):
+            if a != f:
+                h[tv[faces, a]] = 1
+    return h
+
+
+class AdjointProblem:
+    """FP64 loss L = sum a*density + c.velocity + b*divergence over the cell
+    centres of a plan at frozen topology and frozen cell -> tetrahedron
+    assignment ``loc``; ``factor`` = 4 / rho_bar as the forward rounds it."""
+
+    def __init__(self, plan, loc, a=None, c=None, b=None, full_value: bool = False):
+        self.plan = plan
+        self.tv = np.ascontiguousarray(plan.tet_v, np.int32)
+        self.hull = hull_marks(plan)
+        self.pts = cell_points(plan)
+        self.loc = np.ascontiguousarray(loc, np.int64)
+        self.a = None if a is None else np.ascontiguousarray(a, np.float64)
+        self.c = None if c is None else np.ascontiguousarray(c, np.float64)
+        self.b = None if b is None else np.ascontiguousarray(b, np.float64)
+        self.full = 1 if full_value else 0
+        self.factor = float(np.float32(4.0 / float(np.float32(plan.rho_bar))))
+
+    def _args(self, x, w, v):
+        p = self.plan
+        return (p.n_tets, self.tv.ctypes.data, p.n_verts, x.ctypes.data, w.ctypes.data, v.ctypes.data,
+                self.hull.ctypes.data, self.factor, len(self.loc), self.loc.ctypes.data, self.pts.ctypes.data,
+                None if self.a is None else self.a.ctypes.data, None if self.c is None else self.c.ctypes.data,
+                None if self.b is None else self.b.ctypes.data, self.full)
+
+    def loss(self, x, w, v) -> float:
+        x, w, v = (np.ascontiguousarray(t, np.float64) for t in (x, w, v))
+        return float(lib().oracle_dtfe_loss(*self._args(x, w, v)))
+
+    def grad(self, x, w, v):
+        """(gx (V,3), gv (V,3), gw (V,)) float64."""
+        x, w, v = (np.ascontiguousarray(t, np.float64) for t in (x, w, v))
+        V = self.plan.n_verts
+        gx, gv, gw = np.zeros((V, 3)), np.zeros((V, 3)), np.zeros(V)
+        lib().oracle_dtfe_grad(*self._args(x, w, v), gx.ctypes.data, gv.ctypes.data, gw.ctypes.data)
+        return gx, gv, gw
+
+
+def images_of(src: np.ndarray, particles: np.ndarray):
+    """CSR (offsets, vertices) of the vertices that are images of each
+    selected particle."""
+    order = np.argsort(src, kind="stable")
+    ss = src[order]
+    lo = np.searchsorted(ss, particles, "left")
+    hi = np.searchsorted(ss, particles, "right")
+    off = np.zeros(len(particles) + 1, np.int64)
+    off[1:] = np.cumsum(hi - lo)
+    verts = np.concatenate([order[l:h] for l, h in zip(lo, hi)]).astype(np.int32) if len(particles) else \
+        np.zeros(0, np.int32)
+    return off, verts
+
+
+def dtfe_fd(prob: "AdjointProblem", x, w, v, particles, h_pos: float, h_vel: float = 1e-3, h_w: float = 1e-4):
+    """FP64 central differences of prob's loss for the selected particles:
+    (n, 7) = d/d(x, y, z, vx, vy, vz, w), every image of a particle moved."""
+    x, w, v = (np.ascontiguousarray(t, np.float64) for t in (x, w, v))
+    off, verts = images_of(np.asarray(prob.plan.src), np.asarray(particles))
+    out = np.zeros((len(particles), 7))
+    lib().oracle_dtfe_fd(*prob._args(x, w, v), len(particles), off.ctypes.data, verts.ctypes.data,
+                         float(h_pos), float(h_vel), float(h_w), out.ctypes.data)
+    return out
+
+
+def deposit_loss_grad(kind: int, pos, w, region, grid, rho_bar, a, want_grad: bool = True):
+    """FP64 L = sum a*density of one region's NGP/CIC/TSC deposition and its
+    gradient: (L, gx (n,3) or None, gw (n,) or None)."""
+    pos = np.ascontiguousarray(pos, np.float64)
+    w = np.ascontiguousarray(w, np.float64)
+    region = np.ascontiguousarray(region, np.float32)
+    grid = np.ascontiguousarray(grid, np.int32)
+    a = np.ascontiguousarray(a, np.float64)
+    gx = np.zeros((len(pos), 3)) if want_grad else None
+    gw = np.zeros(len(pos)) if want_grad else None
+    L = lib().oracle_deposit_loss_grad(kind, pos.ctypes.data, w.ctypes.data, len(pos), region.ctypes.data,
+                                       grid.ctypes.data, float(rho_bar), a.ctypes.data,
+                                       None if gx is None else gx.ctypes.data,
+                                       None if gw is None else gw.ctypes.data)
+    return float(L), gx, gw

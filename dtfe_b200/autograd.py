@@ -61,8 +61,8 @@ class _DTFEFunction(torch.autograd.Function):
         dens = torch.empty(G, dtype=torch.float32, device=o.cuda)
         vel = torch.empty((G, 3), dtype=torch.float32, device=o.cuda)
         div = torch.empty(G, dtype=torch.float32, device=o.cuda)
-        o.dev.interpolate_dev(["density", "velocity", "divergence"],
-                              {"density": dens, "velocity": vel, "divergence": div}, method=0, fix=mod.fix_value)
+        o.dev.interpolate_dev(["density", "velocity", "velocity_divergence"],
+                              {"density": dens, "velocity": vel, "velocity_divergence": div}, method=0, fix=mod.fix_value)
         o.generation += 1
         ctx.gen = o.generation
         ctx.mod = mod

@@ -53,8 +53,8 @@ def test_adjoint_matches_oracle(gpu_built, n, threads, full):
         dens = torch.empty(G, device=cuda)
         vg = torch.empty((G, 3), device=cuda)
         div = torch.empty(G, device=cuda)
-        dev.interpolate_dev(["density", "velocity", "divergence"], {"density": dens, "velocity": vg,
-                                                                    "divergence": div}, fix=full)
+        dev.interpolate_dev(["density", "velocity", "velocity_divergence"], {"density": dens, "velocity": vg,
+                                                                    "velocity_divergence": div}, fix=full)
         gx = torch.empty((V, 3), device=cuda)
         gv = torch.empty((V, 3), device=cuda)
         gw = torch.empty(V, device=cuda)

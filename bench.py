@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mc", action="store_true")
+    ap.add_argument("--bwd-n", type=int, default=128, help="particles per side of the backward workload")
+    ap.add_argument("--no-bwd", action="store_true")
+    ap.add_argument("--fd-particles", type=int, default=1000)
     return ap.parse_args()
 
 
@@ -195,6 +198,160 @@ def cpu_baseline(plan, threads: int, target_s: float) -> dict:
                       f"interpolation of {cells} of {G} cells ({elapsed:.2f} s, x-slabs of sub-box 0), "
                       f"scaled to the full grid",
             "vertex_density_s": t_vd, "interp_cells_per_s": cells / elapsed}
+
+
+def _events(stream, fn, steps):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / steps
+
+
+def backward_leg(args, local: int, threads: int) -> dict:
+    """Differentiation workload: 128^3 Zel'dovich particles (rms 0.5 spacing,
+    weights U[0.5, 1.5], velocities as the main workload) -> 128^3 grid.
+    Loss = sum a*density + b*divergence (DTFE) + sum a_cic*CIC + a_tsc*TSC
+    with seeded N(0, 1) weights.  Forward: vertex densities + cell-centre
+    density and divergence, CIC and TSC deposits; backward: the adjoints.
+    Gradients of 1000 random particles are checked against FP64 central
+    differences (h = 1e-6 box) of the oracle's loss."""
+    import torch
+    import oracle as O
+    from dtfe_b200 import plan as P
+    from dtfe_b200 import synthetic as S
+    from dtfe_b200.device import DeviceDTFE
+    n = args.bwd_n
+    cuda = torch.device("cuda", local)
+    pos, psi = S.zeldovich_lattice(n, S.BOX, 0.5, seed=17)
+    rng = np.random.default_rng(18)
+    w = rng.uniform(0.5, 1.5, len(pos)).astype(np.float32)
+    vel = (100.0 * psi / (S.BOX / n) + rng.normal(0.0, 50.0, psi.shape)).astype(np.float32)
+    del psi
+    avg = float(w.sum()) / S.BOX ** 3
+    t0 = time.time()
+    plan = P.make_plan(pos, w, vel, None, grid=(n, n, n), n_threads=threads, average_density_value=avg)
+    dplans = {k: P.make_deposit_plan(pos, w, None, grid=(n, n, n), n_threads=threads, kind=k,
+                                     average_density_value=avg) for k in ("CIC", "TSC")}
+    t_plan = time.time() - t0
+    G = int(np.prod(plan.grid))
+    V = plan.n_verts
+    a = torch.tensor(rng.standard_normal(G), dtype=torch.float32, device=cuda)
+    b = torch.tensor(rng.standard_normal(G), dtype=torch.float32, device=cuda)
+    ad = {k: torch.tensor(rng.standard_normal(G), dtype=torch.float32, device=cuda) for k in dplans}
+    dens = torch.empty(G, device=cuda)
+    div = torch.empty(G, device=cuda)
+    dd = {k: torch.empty(G, device=cuda) for k in dplans}
+    gx, gv, gw = (torch.empty((V, 3), device=cuda), torch.empty((V, 3), device=cuda), torch.empty(V, device=cuda))
+    dgx = {k: torch.empty((d.n, 3), device=cuda) for k, d in dplans.items()}
+    dgw = {k: torch.empty(d.n, device=cuda) for k, d in dplans.items()}
+    dev = DeviceDTFE(local)
+    ddev = {k: DeviceDTFE(local) for k in dplans}
+    dev.load(plan)
+    stream = torch.cuda.ExternalStream(dev.stream, device=cuda)
+    torch.cuda.synchronize()
+
+    def fwd():
+        dev.vertex_density(plan.rho_bar)
+        dev.interpolate_dev(["density", "velocity_divergence"], {"density": dens, "velocity_divergence": div})
+
+    def bwd():
+        dev.adjoint_dev(gx, grad_density=a, grad_divergence=b, grad_vel=gv, grad_w=gw)
+
+    for _ in range(3):
+        fwd()
+        bwd()
+    t_fwd = _events(stream, fwd, 5)
+    t_bwd = _events(stream, bwd, 5)
+    dep = {}
+    for k, d in dplans.items():
+        ds = torch.cuda.ExternalStream(ddev[k].stream, device=cuda)
+
+        def dfwd():
+            ddev[k].deposit_dev(d, dd[k])
+
+        def dbwd():
+            ddev[k].deposit_adjoint_dev(ad[k], dgx[k], dgw[k])
+        for _ in range(3):
+            dfwd()
+            dbwd()
+        dep[k] = {"fwd_ms": 1e3 * _events(ds, dfwd, 5), "bwd_ms": 1e3 * _events(ds, dbwd, 5),
+                  "particle_copies": d.n}
+    # finite-difference check on random particles
+    sel = np.random.default_rng(19).choice(len(pos), min(args.fd_particles, len(pos)), replace=False)
+    t0 = time.time()
+    d32, d64, _ = O.vertex_density(plan)
+    _, loc = O.interpolate(plan, d32, d64, ["density"], mode=O.MODE_FP64, want_loc=True, nthreads=threads)
+    prob = O.AdjointProblem(plan, loc, a=a.cpu().numpy().astype(np.float64), b=b.cpu().numpy().astype(np.float64))
+    fd = O.dtfe_fd(prob, plan.xyz, plan.weight, plan.velocity, sel, h_pos=1e-6 * S.BOX)
+
+    def per_particle(src, g):
+        out = np.zeros((len(pos),) + g.shape[1:])
+        np.add.at(out, src, g.astype(np.float64))
+        return out[sel]
+
+    def rel(x, y):
+        rms = max(float(np.sqrt(np.mean(y * y))), 1e-300)
+        return float(np.max(np.abs(x - y) / np.maximum(np.abs(y), rms)))
+    fd_err = {"dtfe_pos": rel(per_particle(plan.src, gx.cpu().numpy()), fd[:, :3]),
+              "dtfe_vel": rel(per_particle(plan.src, gv.cpu().numpy()), fd[:, 3:6]),
+              "dtfe_weight": rel(per_particle(plan.src, gw.cpu().numpy()), fd[:, 6])}
+    for k, d in dplans.items():
+        at = ad[k].cpu().numpy().astype(np.float64).reshape(plan.grid)
+        fdx = np.zeros((len(sel), 3))
+        fdw = np.zeros(len(sel))
+        order = np.argsort(d.src, kind="stable")
+        ss = d.src[order]
+        offs = np.array([bx.particle_offset for bx in d.boxes] + [d.n])
+        keep = np.ones(len(sel), bool)
+        for r, i in enumerate(sel):
+            for c in order[np.searchsorted(ss, i, "left"):np.searchsorted(ss, i, "right")]:
+                bi = int(np.searchsorted(offs, c, "right") - 1)
+                bx = d.boxes[bi]
+                dims = np.array([bx.tile_dims[q] for q in range(3)], np.int32)
+                org = [bx.tile_origin[q] for q in range(3)]
+                if d.kind == 1:
+                    # CIC weights have a kink at cell centres and the clipped edge
+                    # stencils jump at cell faces: a central difference that
+                    # straddles one is not a derivative, so such particles are left out
+                    lo = np.array([bx.region[0], bx.region[2], bx.region[4]], np.float64)
+                    dx = (np.array([bx.region[1], bx.region[3], bx.region[5]], np.float64) - lo) / dims
+                    fr = (d.pos[c].astype(np.float64) - lo) / dx
+                    fr -= np.floor(fr)
+                    if np.min(np.minimum(np.abs(fr - 0.5), np.minimum(fr, 1 - fr)) * dx) < 4e-6 * S.BOX:
+                        keep[r] = False
+                ta = np.ascontiguousarray(at[org[0]:org[0] + dims[0], org[1]:org[1] + dims[1],
+                                             org[2]:org[2] + dims[2]]).ravel()
+                reg = np.array(list(bx.region), np.float32)
+                h = 1e-6 * S.BOX
+                for q in range(3):
+                    pp, pm = d.pos[c:c + 1].astype(np.float64).copy(), d.pos[c:c + 1].astype(np.float64).copy()
+                    pp[0, q] += h
+                    pm[0, q] -= h
+                    lp = O.deposit_loss_grad(d.kind, pp, d.weight[c:c + 1], reg, dims, d.rho_bar, ta, False)[0]
+                    lm = O.deposit_loss_grad(d.kind, pm, d.weight[c:c + 1], reg, dims, d.rho_bar, ta, False)[0]
+                    fdx[r, q] += (lp - lm) / (2 * h)
+                fdw[r] += O.deposit_loss_grad(d.kind, d.pos[c:c + 1], np.ones(1), reg, dims, d.rho_bar, ta,
+                                              False)[0]
+        fd_err[f"{k.lower()}_pos"] = rel(per_particle(d.src, dgx[k].cpu().numpy())[keep], fdx[keep])
+        fd_err[f"{k.lower()}_weight"] = rel(per_particle(d.src, dgw[k].cpu().numpy()), fdw)
+        fd_err[f"{k.lower()}_pos_excluded_at_kinks"] = int((~keep).sum())
+    t_fd = time.time() - t0
+    dev.close()
+    for d in ddev.values():
+        d.close()
+    return {"workload": f"zeldovich{n}: {n}^3 particles (rms 0.5 spacing, weights U[0.5,1.5]) -> {n}^3 grid; "
+                        "loss = sum N(0,1)-weighted density + divergence grids (DTFE), CIC and TSC densities",
+            "dtfe_fwd_ms": 1e3 * t_fwd, "dtfe_bwd_ms": 1e3 * t_bwd, "bwd_over_fwd": t_bwd / t_fwd,
+            "deposit": dep,
+            "deposit_note": "deposit forward includes the host->device copy of the particles (host-input API)",
+            "fd_check": {"particles": int(len(sel)), "h": 1e-6 * S.BOX, "max_rel_err_rms_floor": fd_err,
+                         "seconds": t_fd},
+            "vertices": V, "tetrahedra": plan.n_tets, "host_plan_s": t_plan}
 
 
 def run_reference(args):
@@ -375,6 +532,10 @@ def run_ours(args):
                 "kernel": "k_interpolate<centre>", "kernel_ms": 1e3 * t_interp,
                 "algorithmic_bytes": int(b_alg), "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})"}
 
+    bwd = None
+    if not args.no_bwd:
+        bwd = backward_leg(args, local, threads)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(plan, host_threads(args.threads), args.cpu_seconds)
@@ -397,6 +558,7 @@ def run_ours(args):
         "roofline": roofline,
         "cpu_baseline": cpu,
         "mc": mc,
+        "backward": bwd,
         "walk": {k: status[k] for k in ("n_samples_located", "n_walk_steps", "n_exact_tests", "n_ties",
                                         "n_outside")} if status else None,
         "host_prep_s": plan.timings,

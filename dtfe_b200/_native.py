@@ -150,6 +150,7 @@ def gpu() -> C.CDLL:
         lib.dtfe_gpu_deposit_adjoint_dev.argtypes = [H, vp, vp, vp]
         lib.dtfe_gpu_autotune.argtypes = [H, C.c_uint32, vp]
         lib.dtfe_gpu_set_variants.argtypes = [H, C.c_int32, C.c_int32]
+        lib.dtfe_gpu_variant_counts.argtypes = [vp]
         lib.dtfe_vertex_density_noalloc.argtypes = [vp, vp, C.c_int64, vp, vp, C.c_int64, C.c_double, vp, vp]
         lib.dtfe_vertex_density_noalloc.restype = C.c_int
         _gpu = lib

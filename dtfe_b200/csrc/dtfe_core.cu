@@ -177,17 +177,14 @@ __global__ void k_sort_incidence(int64_t V, const int64_t* __restrict__ off, int
 
 // ---- per step ------------------------------------------------------------
 constexpr int kVolBlock = 256;
-constexpr int kBinSlots = 512;  // >= 2 x kVolBlock: the table never fills
-
-__device__ __forceinline__ unsigned slot_hash(int key, unsigned mask) {
-  return ((unsigned)key * 2654435761u) & mask;
-}
 
 // Signed volume of every tetrahedron (FP64, streamed out once) and, when
 // DO_BINS, the walk seeds: per grid cell the lowest tetrahedron whose
-// centroid lies in it, combined per block in a shared-memory hash table
-// (tetrahedra are Morton-sorted, so a block covers few cells) and flushed
-// with one global atomicMin per cell.
+// centroid lies in it.  Tetrahedra are Morton-sorted, so neighbouring lanes
+// often bin to the same cell; within such a run of lanes the first lane holds
+// the lowest tetrahedron id and alone issues the global atomicMin.  The seed
+// only starts the walk (its result does not depend on the seed), so the
+// centroid's cell is computed with a reciprocal instead of a division.
 template <bool DO_BINS>
 __global__ void __launch_bounds__(kVolBlock) k_tet_volume_bins(
     int64_t T, const int4* __restrict__ tet_v, const float4* __restrict__ posd, double* __restrict__ vol,
@@ -214,22 +211,20 @@ __global__ void __launch_bounds__(kVolBlock) k_tet_volume_bins(
       bool inside = true;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        float cen = 0.25f * ((X[0][c] + X[1][c]) + (X[2][c] + X[3][c]));
-        float f = floorf((cen - B.lo[c]) / B.dx[c]);
-        inside = inside && (f >= 0.f && f < (float)B.tile_dims[c]);
+        const float cen = 0.25f * ((X[0][c] + X[1][c]) + (X[2][c] + X[3][c]));
+        const float f = floorf((cen - __ldg(&B.lo[c])) * __frcp_rn(__ldg(&B.dx[c])));
+        const int n = __ldg(&B.tile_dims[c]);
+        inside = inside && (f >= 0.f && f < (float)n);
         idx[c] = inside ? (int)f : 0;
       }
       if (inside)
-        key = (int)(__ldg(&bin_offset[b]) + ((int64_t)idx[0] * B.tile_dims[1] + idx[1]) * B.tile_dims[2] + idx[2]);
+        key = (int)(__ldg(&bin_offset[b]) +
+                    ((int64_t)idx[0] * __ldg(&B.tile_dims[1]) + idx[1]) * __ldg(&B.tile_dims[2]) + idx[2]);
     }
   }
   if (DO_BINS) {
-    // lanes of a warp that hit the same cell elect one leader, which stores
-    // the group's lowest tetrahedron id with a single atomicMin
-    const unsigned group = __match_any_sync(0xffffffffu, key);
-    const int tmin = __reduce_min_sync(group, t < T ? (int)t : 0x7FFFFFFF);
-    const int leader = __ffs(group) - 1;
-    if (key >= 0 && (int)(threadIdx.x & 31) == leader) atomicMin(&bins[key], tmin);
+    const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+    if (key >= 0 && ((threadIdx.x & 31) == 0 || prev != key)) atomicMin(&bins[key], (int)t);
   }
 }
 
@@ -258,7 +253,18 @@ __global__ void __launch_bounds__(kDensBlock) k_vertex_density(
   for (int64_t base = beg; base < end; base += kDensChunk) {
     const int64_t lim = (end - base < kDensChunk) ? end : base + kDensChunk;
     __syncwarp();
-    for (int64_t q = base + lane; q < lim; q += 32) sv[q - base] = __ldg(&vol[__ldg(&inc[q])]);
+    // four independent index loads, then four independent volume gathers
+    for (int64_t q0 = base + lane; q0 < lim; q0 += 128) {
+      int id[4];
+      double x[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) id[u] = (q0 + 32 * u < lim) ? __ldg(&inc[q0 + 32 * u]) : -1;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) x[u] = id[u] >= 0 ? __ldg(&vol[id[u]]) : 0.0;
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (q0 + 32 * u < lim) sv[q0 + 32 * u - base] = x[u];
+    }
     __syncwarp();
     for (; cur < e && cur < lim; ++cur) sum += sv[cur - base];
   }
@@ -362,6 +368,24 @@ __device__ __forceinline__ void fold_counters(const InterpParams& P, unsigned n_
   }
 }
 
+// Seed tetrahedron of one sample: its cell's bin, else the nearest of the 26
+// neighbouring cells with one, else the sub-box's first tetrahedron.
+__device__ __forceinline__ int seed_of(const InterpParams& P, const SampleCell& c) {
+  const dtfe_subbox& B = P.boxes[c.b];
+  const int* bins = P.bins + __ldg(&P.bin_offset[c.b]);
+  int t0 = __ldg(&bins[c.local]);
+  if (t0 >= kEmptyBin) {
+    const int nx = B.tile_dims[0], ny = B.tile_dims[1], nz = B.tile_dims[2];
+    for (int q = 0; q < 26 && t0 >= kEmptyBin; ++q) {
+      const int ii = c.i + c_nbr[q][0], jj = c.j + c_nbr[q][1], kk = c.k + c_nbr[q][2];
+      if (ii < 0 || jj < 0 || kk < 0 || ii >= nx || jj >= ny || kk >= nz) continue;
+      t0 = __ldg(&bins[((int64_t)ii * ny + jj) * nz + kk]);
+    }
+  }
+  if (t0 < B.tet_offset || t0 >= B.tet_offset + B.n_tets) t0 = (int)B.tet_offset;
+  return t0;
+}
+
 // Point location of every cell centre: seed from the cell's bin (the lowest
 // tetrahedron whose centroid lies in the cell, else in the nearest of the 26
 // neighbouring cells that has one), then the walk.  Writes the canonical
@@ -383,23 +407,8 @@ __device__ __forceinline__ void locate_cells_body(const InterpParams& P, int* __
       const int64_t s = g * R + r;
       if (g >= n_groups || s >= P.n_total) break;
       const SampleCell c = sample_cell(P, s);
-      const dtfe_subbox& B = P.boxes[c.b];
-      int t0;
-      if (r > 0 && prev_hit >= 0 && prev_b == c.b && prev_j == c.j && prev_i == c.i) {
-        t0 = prev_hit;
-      } else {
-        const int* bins = P.bins + __ldg(&P.bin_offset[c.b]);
-        t0 = __ldg(&bins[c.local]);
-        if (t0 >= kEmptyBin) {
-          const int nx = B.tile_dims[0], ny = B.tile_dims[1], nz = B.tile_dims[2];
-          for (int q = 0; q < 26 && t0 >= kEmptyBin; ++q) {
-            const int ii = c.i + c_nbr[q][0], jj = c.j + c_nbr[q][1], kk = c.k + c_nbr[q][2];
-            if (ii < 0 || jj < 0 || kk < 0 || ii >= nx || jj >= ny || kk >= nz) continue;
-            t0 = __ldg(&bins[((int64_t)ii * ny + jj) * nz + kk]);
-          }
-        }
-        if (t0 < B.tet_offset || t0 >= B.tet_offset + B.n_tets) t0 = (int)B.tet_offset;
-      }
+      const int t0 = (r > 0 && prev_hit >= 0 && prev_b == c.b && prev_j == c.j && prev_i == c.i) ? prev_hit
+                                                                                             : seed_of(P, c);
       const double pc[3] = {(double)c.x, (double)c.y, (double)c.z};
       int v[4];
       float X[4][3];
@@ -412,6 +421,122 @@ __device__ __forceinline__ void locate_cells_body(const InterpParams& P, int* __
       prev_b = c.b;
       prev_j = c.j;
       prev_i = c.i;
+    }
+  }
+  fold_counters(P, n_loc, n_out, n_fail, st);
+}
+
+// Point location with lane refill: each lane owns R consecutive samples and
+// the warp advances every lane by one walk step per iteration; a lane whose
+// walk ends writes its result and starts its next sample at once (from the
+// previous hit within a z pencil, else from the bin), so lanes with short
+// walks do not wait for the warp's longest walk of every sample.  Results are
+// those of walk_locate (the tie rule makes them path-independent).
+template <int BS, int MINB, int R>
+__global__ void __launch_bounds__(BS, MINB) k_locate_refill(InterpParams P, int* __restrict__ tet_c) {
+  WalkStats st{0, 0, 0};
+  unsigned n_loc = 0, n_out = 0, n_fail = 0;
+  const int lane = threadIdx.x & 31;
+  const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+  const int64_t n_groups = (P.n_total + R - 1) / R;
+  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  for (int64_t g0 = tid - lane; g0 < n_groups; g0 += nthreads) {
+    const int64_t g = g0 + lane;
+    int64_t s = g * R;
+    int r = 0;
+    bool active = g < n_groups && s < P.n_total;
+    SampleCell c;
+    int t = 0, came = -1, nsteps = 0;
+    int v[4] = {0, 0, 0, 0};
+    float X[4][3];
+    float pf[3] = {0.f, 0.f, 0.f};
+    if (active) {
+      c = sample_cell(P, s);
+      pf[0] = c.x; pf[1] = c.y; pf[2] = c.z;
+      t = seed_of(P, c);
+      load_tet(P.tet_v, P.posd, t, v, X);
+    }
+    while (__any_sync(0xffffffffu, active)) {
+      if (!active) continue;
+      ++st.steps;
+      ++nsteps;
+      const int need = 15 & ~(came >= 0 ? (1 << came) : 0);
+      int zmask;
+      const int exit_face = first_exit_face_f32(X, pf, need, zmask, st.exact);
+      int result = kWalkFail - 1;  // none yet
+      if (exit_face < 0) {
+        if (zmask) {
+          ++st.tie;
+          const int b = canonical_tie(P.tet_v, P.tet_n, P.posd, t, zmask, (double)pf[0], (double)pf[1],
+                                      (double)pf[2]);
+          if (b != t) {
+            t = b;
+            load_tet(P.tet_v, P.posd, t, v, X);
+          }
+        }
+        result = t;
+      } else {
+        const int nb = nb_of(__ldg(&P.tet_n[t]), exit_face);
+        if (nb < 0) {
+          result = kOutside;
+        } else if (nsteps >= P.max_steps) {
+          result = kWalkFail;
+        } else {
+          const int4 q = __ldg(&P.tet_v[nb]);
+          const int nv[4] = {q.x, q.y, q.z, q.w};
+          float NX[4][3];
+          came = 0;
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            bool found = false;
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) NX[j][cc] = 0.f;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const bool m = (k != exit_face) && (v[k] == nv[j]);
+              found = found || m;
+#pragma unroll
+              for (int cc = 0; cc < 3; ++cc) NX[j][cc] = m ? X[k][cc] : NX[j][cc];
+            }
+            if (!found) {
+              load_posf(P.posd, nv[j], NX[j]);
+              came = j;
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            v[j] = nv[j];
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) X[j][cc] = NX[j][cc];
+          }
+          t = nb;
+        }
+      }
+      if (result >= kWalkFail) {
+        ++n_loc;
+        if (result == kWalkFail) {
+          ++n_fail;
+          result = kOutside;
+        }
+        if (result < 0) ++n_out;
+        tet_c[s] = result;
+        ++r;
+        ++s;
+        if (r >= R || s >= P.n_total) {
+          active = false;
+        } else {
+          const SampleCell c2 = sample_cell(P, s);
+          const bool hint = result >= 0 && c2.b == c.b && c2.j == c.j && c2.i == c.i;
+          c = c2;
+          pf[0] = c.x; pf[1] = c.y; pf[2] = c.z;
+          came = -1;
+          nsteps = 0;
+          if (!hint) {
+            t = seed_of(P, c);
+            load_tet(P.tet_v, P.posd, t, v, X);
+          }
+        }
+      }
     }
   }
   fold_counters(P, n_loc, n_out, n_fail, st);
@@ -773,7 +898,9 @@ int prepare_bins(dtfe_handle h) {
 // SM) and seeding schedule of the locate kernel; register budget of the
 // evaluation kernel.
 struct LocVariant { int block, minb, r; };
-constexpr LocVariant kLocVariants[] = {{256, 3, 1}, {256, 2, 1}, {256, 4, 1}, {256, 3, 2}, {256, 4, 2}, {256, 3, 4}};
+// 0-5: one full walk per sample and lane; 6-10: lane refill (k_locate_refill)
+constexpr LocVariant kLocVariants[] = {{256, 3, 1}, {256, 2, 1}, {256, 4, 1}, {256, 3, 2}, {256, 4, 2}, {256, 3, 4},
+                                       {256, 3, 4}, {256, 3, 8}, {256, 4, 8}, {256, 2, 8}, {256, 3, 16}};
 constexpr int kNumLocVariants = sizeof(kLocVariants) / sizeof(kLocVariants[0]);
 constexpr int kEvalMinBlocks[] = {3, 2, 4};
 constexpr int kNumEvalVariants = 3;
@@ -788,7 +915,12 @@ void launch_locate(int variant, const InterpParams& P, int* tet_c, cudaStream_t 
     case 2: k_locate_cells<256, 4, 1><<<grid, 256, 0, st>>>(P, tet_c); break;
     case 3: k_locate_cells<256, 3, 2><<<grid, 256, 0, st>>>(P, tet_c); break;
     case 4: k_locate_cells<256, 4, 2><<<grid, 256, 0, st>>>(P, tet_c); break;
-    default: k_locate_cells<256, 3, 4><<<grid, 256, 0, st>>>(P, tet_c); break;
+    case 5: k_locate_cells<256, 3, 4><<<grid, 256, 0, st>>>(P, tet_c); break;
+    case 6: k_locate_refill<256, 3, 4><<<grid, 256, 0, st>>>(P, tet_c); break;
+    case 7: k_locate_refill<256, 3, 8><<<grid, 256, 0, st>>>(P, tet_c); break;
+    case 8: k_locate_refill<256, 4, 8><<<grid, 256, 0, st>>>(P, tet_c); break;
+    case 9: k_locate_refill<256, 2, 8><<<grid, 256, 0, st>>>(P, tet_c); break;
+    default: k_locate_refill<256, 3, 16><<<grid, 256, 0, st>>>(P, tet_c); break;
   }
 }
 
@@ -1222,6 +1354,13 @@ int dtfe_gpu_autotune(dtfe_handle h, uint32_t fields, int32_t* chosen) {
   if (!h) return set_error(DTFE_ERR_ARG, "null handle");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
   return autotune_impl(h, fields, chosen);
+}
+
+int dtfe_gpu_variant_counts(int32_t counts[2]) {
+  if (!counts) return set_error(DTFE_ERR_ARG, "null argument");
+  counts[0] = kNumLocVariants;
+  counts[1] = kNumEvalVariants;
+  return DTFE_OK;
 }
 
 int dtfe_gpu_set_variants(dtfe_handle h, int32_t locate_variant, int32_t eval_variant) {

@@ -150,6 +150,11 @@ class DeviceDTFE:
         N.check(self.lib.dtfe_gpu_autotune(self.h, _mask(fields), chosen))
         return int(chosen[0]), int(chosen[1])
 
+    def variant_counts(self) -> tuple:
+        counts = (C.c_int32 * 2)()
+        N.check(self.lib.dtfe_gpu_variant_counts(counts))
+        return int(counts[0]), int(counts[1])
+
     def set_variants(self, locate: int, evaluate: int) -> None:
         N.check(self.lib.dtfe_gpu_set_variants(self.h, locate, evaluate))
 

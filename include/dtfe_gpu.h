@@ -222,6 +222,9 @@ int dtfe_gpu_deposit_adjoint_dev(dtfe_handle h, const float* grad_density_dev, f
  * reference (its loops have no launch parameters). */
 int dtfe_gpu_autotune(dtfe_handle h, uint32_t fields, int32_t* chosen);
 /* Selects launch variants explicitly (indices as reported by autotune). */
+/* Number of launch variants of the location (counts[0]) and evaluation
+ * (counts[1]) kernels that dtfe_gpu_autotune chooses among. */
+int dtfe_gpu_variant_counts(int32_t counts[2]);
 int dtfe_gpu_set_variants(dtfe_handle h, int32_t locate_variant, int32_t eval_variant);
 
 /* Copy the vertex densities (V floats) to the host. */

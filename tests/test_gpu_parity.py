@@ -120,13 +120,18 @@ def test_launch_variants_identical(plan8):
     the previous hit) produces bit-identical fields."""
     d = _device(plan8)
     chosen = d.autotune(FIELDS)
-    assert 0 <= chosen[0] < 6 and 0 <= chosen[1] < 3
+    n_loc, n_ev = d.variant_counts()
+    assert n_loc >= 11 and n_ev >= 3
+    assert 0 <= chosen[0] < n_loc and 0 <= chosen[1] < n_ev
     d.set_variants(0, 0)
     base = d.interpolate(FIELDS, method=0)
-    for loc in range(6):
-        for ev in range(3):
+    st0 = d.last_status
+    for loc in range(n_loc):
+        for ev in range(n_ev):
             d.set_variants(loc, ev)
             g = d.interpolate(FIELDS, method=0)
             for f in FIELDS:
                 assert np.array_equal(g[f], base[f]), (loc, ev, f)
+            assert d.last_status["n_samples_located"] == st0["n_samples_located"]
+            assert d.last_status["n_outside"] == st0["n_outside"]
     d.close()

@@ -253,18 +253,7 @@ __global__ void __launch_bounds__(kDensBlock) k_vertex_density(
   for (int64_t base = beg; base < end; base += kDensChunk) {
     const int64_t lim = (end - base < kDensChunk) ? end : base + kDensChunk;
     __syncwarp();
-    // four independent index loads, then four independent volume gathers
-    for (int64_t q0 = base + lane; q0 < lim; q0 += 128) {
-      int id[4];
-      double x[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) id[u] = (q0 + 32 * u < lim) ? __ldg(&inc[q0 + 32 * u]) : -1;
-#pragma unroll
-      for (int u = 0; u < 4; ++u) x[u] = id[u] >= 0 ? __ldg(&vol[id[u]]) : 0.0;
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-        if (q0 + 32 * u < lim) sv[q0 + 32 * u - base] = x[u];
-    }
+    for (int64_t q = base + lane; q < lim; q += 32) sv[q - base] = __ldg(&vol[__ldg(&inc[q])]);
     __syncwarp();
     for (; cur < e && cur < lim; ++cur) sum += sv[cur - base];
   }
@@ -421,122 +410,6 @@ __device__ __forceinline__ void locate_cells_body(const InterpParams& P, int* __
       prev_b = c.b;
       prev_j = c.j;
       prev_i = c.i;
-    }
-  }
-  fold_counters(P, n_loc, n_out, n_fail, st);
-}
-
-// Point location with lane refill: each lane owns R consecutive samples and
-// the warp advances every lane by one walk step per iteration; a lane whose
-// walk ends writes its result and starts its next sample at once (from the
-// previous hit within a z pencil, else from the bin), so lanes with short
-// walks do not wait for the warp's longest walk of every sample.  Results are
-// those of walk_locate (the tie rule makes them path-independent).
-template <int BS, int MINB, int R>
-__global__ void __launch_bounds__(BS, MINB) k_locate_refill(InterpParams P, int* __restrict__ tet_c) {
-  WalkStats st{0, 0, 0};
-  unsigned n_loc = 0, n_out = 0, n_fail = 0;
-  const int lane = threadIdx.x & 31;
-  const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
-  const int64_t n_groups = (P.n_total + R - 1) / R;
-  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  for (int64_t g0 = tid - lane; g0 < n_groups; g0 += nthreads) {
-    const int64_t g = g0 + lane;
-    int64_t s = g * R;
-    int r = 0;
-    bool active = g < n_groups && s < P.n_total;
-    SampleCell c;
-    int t = 0, came = -1, nsteps = 0;
-    int v[4] = {0, 0, 0, 0};
-    float X[4][3];
-    float pf[3] = {0.f, 0.f, 0.f};
-    if (active) {
-      c = sample_cell(P, s);
-      pf[0] = c.x; pf[1] = c.y; pf[2] = c.z;
-      t = seed_of(P, c);
-      load_tet(P.tet_v, P.posd, t, v, X);
-    }
-    while (__any_sync(0xffffffffu, active)) {
-      if (!active) continue;
-      ++st.steps;
-      ++nsteps;
-      const int need = 15 & ~(came >= 0 ? (1 << came) : 0);
-      int zmask;
-      const int exit_face = first_exit_face_f32(X, pf, need, zmask, st.exact);
-      int result = kWalkFail - 1;  // none yet
-      if (exit_face < 0) {
-        if (zmask) {
-          ++st.tie;
-          const int b = canonical_tie(P.tet_v, P.tet_n, P.posd, t, zmask, (double)pf[0], (double)pf[1],
-                                      (double)pf[2]);
-          if (b != t) {
-            t = b;
-            load_tet(P.tet_v, P.posd, t, v, X);
-          }
-        }
-        result = t;
-      } else {
-        const int nb = nb_of(__ldg(&P.tet_n[t]), exit_face);
-        if (nb < 0) {
-          result = kOutside;
-        } else if (nsteps >= P.max_steps) {
-          result = kWalkFail;
-        } else {
-          const int4 q = __ldg(&P.tet_v[nb]);
-          const int nv[4] = {q.x, q.y, q.z, q.w};
-          float NX[4][3];
-          came = 0;
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            bool found = false;
-#pragma unroll
-            for (int cc = 0; cc < 3; ++cc) NX[j][cc] = 0.f;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-              const bool m = (k != exit_face) && (v[k] == nv[j]);
-              found = found || m;
-#pragma unroll
-              for (int cc = 0; cc < 3; ++cc) NX[j][cc] = m ? X[k][cc] : NX[j][cc];
-            }
-            if (!found) {
-              load_posf(P.posd, nv[j], NX[j]);
-              came = j;
-            }
-          }
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            v[j] = nv[j];
-#pragma unroll
-            for (int cc = 0; cc < 3; ++cc) X[j][cc] = NX[j][cc];
-          }
-          t = nb;
-        }
-      }
-      if (result >= kWalkFail) {
-        ++n_loc;
-        if (result == kWalkFail) {
-          ++n_fail;
-          result = kOutside;
-        }
-        if (result < 0) ++n_out;
-        tet_c[s] = result;
-        ++r;
-        ++s;
-        if (r >= R || s >= P.n_total) {
-          active = false;
-        } else {
-          const SampleCell c2 = sample_cell(P, s);
-          const bool hint = result >= 0 && c2.b == c.b && c2.j == c.j && c2.i == c.i;
-          c = c2;
-          pf[0] = c.x; pf[1] = c.y; pf[2] = c.z;
-          came = -1;
-          nsteps = 0;
-          if (!hint) {
-            t = seed_of(P, c);
-            load_tet(P.tet_v, P.posd, t, v, X);
-          }
-        }
-      }
     }
   }
   fold_counters(P, n_loc, n_out, n_fail, st);
@@ -898,9 +771,7 @@ int prepare_bins(dtfe_handle h) {
 // SM) and seeding schedule of the locate kernel; register budget of the
 // evaluation kernel.
 struct LocVariant { int block, minb, r; };
-// 0-5: one full walk per sample and lane; 6-10: lane refill (k_locate_refill)
-constexpr LocVariant kLocVariants[] = {{256, 3, 1}, {256, 2, 1}, {256, 4, 1}, {256, 3, 2}, {256, 4, 2}, {256, 3, 4},
-                                       {256, 3, 4}, {256, 3, 8}, {256, 4, 8}, {256, 2, 8}, {256, 3, 16}};
+constexpr LocVariant kLocVariants[] = {{256, 3, 1}, {256, 2, 1}, {256, 4, 1}, {256, 3, 2}, {256, 4, 2}, {256, 3, 4}};
 constexpr int kNumLocVariants = sizeof(kLocVariants) / sizeof(kLocVariants[0]);
 constexpr int kEvalMinBlocks[] = {3, 2, 4};
 constexpr int kNumEvalVariants = 3;
@@ -915,12 +786,7 @@ void launch_locate(int variant, const InterpParams& P, int* tet_c, cudaStream_t 
     case 2: k_locate_cells<256, 4, 1><<<grid, 256, 0, st>>>(P, tet_c); break;
     case 3: k_locate_cells<256, 3, 2><<<grid, 256, 0, st>>>(P, tet_c); break;
     case 4: k_locate_cells<256, 4, 2><<<grid, 256, 0, st>>>(P, tet_c); break;
-    case 5: k_locate_cells<256, 3, 4><<<grid, 256, 0, st>>>(P, tet_c); break;
-    case 6: k_locate_refill<256, 3, 4><<<grid, 256, 0, st>>>(P, tet_c); break;
-    case 7: k_locate_refill<256, 3, 8><<<grid, 256, 0, st>>>(P, tet_c); break;
-    case 8: k_locate_refill<256, 4, 8><<<grid, 256, 0, st>>>(P, tet_c); break;
-    case 9: k_locate_refill<256, 2, 8><<<grid, 256, 0, st>>>(P, tet_c); break;
-    default: k_locate_refill<256, 3, 16><<<grid, 256, 0, st>>>(P, tet_c); break;
+    default: k_locate_cells<256, 3, 4><<<grid, 256, 0, st>>>(P, tet_c); break;
   }
 }
 

@@ -713,6 +713,9 @@ struct dtfe_gpu_s {
   float factor = 0.f;             // (D+1)/rho_bar of the last vertex-density call
   double *g_rho = nullptr, *g_x = nullptr, *g_v = nullptr, *g_S = nullptr, *g_m = nullptr, *vbar = nullptr;
   float* adj_a = nullptr;         // device copies of host loss weights
+  void* sph_scratch = nullptr;    // SPH cell grids, neighbour bookkeeping, FP64 sums
+  size_t sph_bytes = 0;
+  float* sph_out = nullptr;       // host-output SPH staging
 };
 
 namespace {
@@ -870,7 +873,7 @@ int dtfe_gpu_destroy(dtfe_handle h) {
     if (h->out_buf[i]) cudaFree(h->out_buf[i]);
   if (h->dep_scratch) cudaFree(h->dep_scratch);
   for (void* p : {(void*)h->g_rho, (void*)h->g_x, (void*)h->g_v, (void*)h->g_S, (void*)h->g_m, (void*)h->vbar,
-                  (void*)h->adj_a})
+                  (void*)h->adj_a, h->sph_scratch, (void*)h->sph_out})
     if (p) cudaFree(p);
   if (h->dep_out) cudaFree(h->dep_out);
   cudaStreamDestroy(h->stream);
@@ -1249,6 +1252,12 @@ int dtfe_internal_adjoint(void* stream, const void* cell_params, int64_t n_cells
                           const int64_t* off, const int* inc, float factor, double* g_rho, double* g_x, double* g_v,
                           double* g_S, double* g_m, double* vbar, float* out_x, float* out_v, float* out_w);
 size_t dtfe_internal_adjoint_params_size();
+int dtfe_internal_sph(void* stream, int K, const dtfe_subbox* boxes_h, const dtfe_subbox* boxes_d,
+                      const int64_t* tile_prefix_d, int64_t n_cells, int64_t G1, int64_t G2, const float* xs,
+                      const float* ys, const float* zs, int64_t V, const float4* posd, const float* w,
+                      const float4* vel4, const float* scal, int S, int k, uint32_t fields, int extensive,
+                      double average_density, float* dens_out, float* vel_out, float* scal_out, void** scratch,
+                      size_t* scratch_bytes);
 void dtfe_internal_adjoint_fill_params(void* out, const int4* tet_v, const float4* posd, const float4* vel4,
                                        const int* tet_c, const dtfe_subbox* boxes, const int64_t* tile_prefix,
                                        const float* xs, const float* ys, const float* zs, int K, int64_t G1,
@@ -1309,6 +1318,50 @@ int dtfe_gpu_adjoint_dev(dtfe_handle h, const float* grad_density_dev, const flo
                              h->inc_off, h->inc, h->factor, h->g_rho, h->g_x, h->g_v, h->g_S, h->g_m, h->vbar,
                              grad_xyz_dev, grad_vel_dev, grad_w_dev);
   if (rc) return set_error(rc, "adjoint kernels failed");
+  DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return DTFE_OK;
+}
+
+int dtfe_gpu_sph_dev(dtfe_handle h, int32_t n_neighbors, uint32_t fields, int32_t extensive,
+                     double average_density, float* density_dev, float* velocity_dev, float* scalar_dev) {
+  if (!h) return set_error(DTFE_ERR_ARG, "null handle");
+  if (h->K == 0 || h->V == 0) return set_error(DTFE_ERR_STATE, "upload and sub-boxes needed");
+  if (fields & ~(DTFE_FIELD_BIT(DTFE_DENSITY) | DTFE_FIELD_BIT(DTFE_VELOCITY) | DTFE_FIELD_BIT(DTFE_SCALAR)))
+    return set_error(DTFE_ERR_ARG, "SPH computes density, velocity and scalar fields only");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  const int64_t G = (int64_t)h->grid[0] * h->grid[1] * h->grid[2];
+  if (density_dev) DTFE_CUDA_TRY(cudaMemsetAsync(density_dev, 0, sizeof(float) * G, h->stream));
+  if (velocity_dev) DTFE_CUDA_TRY(cudaMemsetAsync(velocity_dev, 0, sizeof(float) * 3 * G, h->stream));
+  if (scalar_dev && h->S) DTFE_CUDA_TRY(cudaMemsetAsync(scalar_dev, 0, sizeof(float) * h->S * G, h->stream));
+  int rc = dtfe_internal_sph(h->stream, h->K, h->boxes_h.data(), h->boxes, h->tile_prefix, h->n_cells, h->grid[1],
+                             h->grid[2], h->xs, h->ys, h->zs, h->V, h->posd, h->w, h->vel4, h->scal, h->S,
+                             n_neighbors, fields, extensive, average_density,
+                             (fields & DTFE_FIELD_BIT(DTFE_DENSITY)) ? density_dev : nullptr, velocity_dev,
+                             scalar_dev, &h->sph_scratch, &h->sph_bytes);
+  if (rc) return rc;
+  DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return DTFE_OK;
+}
+
+int dtfe_gpu_sph(dtfe_handle h, int32_t n_neighbors, uint32_t fields, int32_t extensive, double average_density,
+                 float* density, float* velocity, float* scalar) {
+  if (!h) return set_error(DTFE_ERR_ARG, "null handle");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  const int64_t G = (int64_t)h->grid[0] * h->grid[1] * h->grid[2];
+  const bool wv = (fields & DTFE_FIELD_BIT(DTFE_VELOCITY)) != 0, ws = (fields & DTFE_FIELD_BIT(DTFE_SCALAR)) != 0;
+  if ((wv && !velocity) || (ws && !scalar) || ((fields & DTFE_FIELD_BIT(DTFE_DENSITY)) && !density))
+    return set_error(DTFE_ERR_ARG, "missing output buffer");
+  int rc = dev_alloc(h, &h->sph_out, (size_t)(1 + 3 + h->S) * G);
+  if (rc) return rc;
+  float* dd = h->sph_out;
+  float* dv = wv ? h->sph_out + G : nullptr;
+  float* ds = ws ? h->sph_out + 4 * G : nullptr;
+  rc = dtfe_gpu_sph_dev(h, n_neighbors, fields, extensive, average_density, dd, dv, ds);
+  if (rc) return rc;
+  if (density && (fields & DTFE_FIELD_BIT(DTFE_DENSITY)))
+    DTFE_CUDA_TRY(cudaMemcpyAsync(density, dd, sizeof(float) * G, cudaMemcpyDeviceToHost, h->stream));
+  if (dv) DTFE_CUDA_TRY(cudaMemcpyAsync(velocity, dv, sizeof(float) * 3 * G, cudaMemcpyDeviceToHost, h->stream));
+  if (ds) DTFE_CUDA_TRY(cudaMemcpyAsync(scalar, ds, sizeof(float) * h->S * G, cudaMemcpyDeviceToHost, h->stream));
   DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return DTFE_OK;
 }

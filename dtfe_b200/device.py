@@ -130,6 +130,25 @@ class DeviceDTFE:
                                               grid.ctypes.data, dplan.rho_bar, N.ptr(density_dev),
                                               N.ptr(velocity_dev)))
 
+    def sph(self, rho_bar: float, n_neighbors: int = 32, velocity: bool = True, scalars: bool = False,
+            extensive: bool = False) -> dict:
+        """SPH density (and velocity, scalars) on the host."""
+        G = int(np.prod(self.grid))
+        fields = ["density"] + (["velocity"] if velocity else []) + (["scalar"] if scalars else [])
+        dens = np.empty(G, np.float32)
+        vel = np.empty((G, 3), np.float32) if velocity else None
+        sc = np.empty((G, self.n_scalars), np.float32) if scalars else None
+        N.check(self.lib.dtfe_gpu_sph(self.h, int(n_neighbors), _mask(fields), int(extensive), float(rho_bar),
+                                      N.ptr(dens), N.ptr(vel), N.ptr(sc)))
+        return {"density": dens, "velocity": vel, "scalar": sc}
+
+    def sph_dev(self, rho_bar: float, density_dev, velocity_dev=None, scalar_dev=None, n_neighbors: int = 32,
+                extensive: bool = False) -> None:
+        fields = ["density"] + (["velocity"] if velocity_dev is not None else []) + \
+            (["scalar"] if scalar_dev is not None else [])
+        N.check(self.lib.dtfe_gpu_sph_dev(self.h, int(n_neighbors), _mask(fields), int(extensive), float(rho_bar),
+                                          N.ptr(density_dev), N.ptr(velocity_dev), N.ptr(scalar_dev)))
+
     def adjoint_dev(self, grad_xyz, grad_density=None, grad_velocity=None, grad_divergence=None,
                     grad_vel=None, grad_w=None) -> None:
         """Vertex gradients of sum(a*density + c.velocity + b*divergence) of the

@@ -192,6 +192,20 @@ int dtfe_gpu_deposit_dev(dtfe_handle h, int32_t kind, const float* xyz, const fl
                          int64_t n, int32_t n_boxes, const dtfe_deposit_box* boxes, const int32_t grid[3],
                          double average_density, float* density_dev, float* velocity_dev);
 
+/* SPH estimator (SPH_interpolation, src/SPH_interpolation.cc:252-474) on the
+ * uploaded vertices and sub-boxes: each sub-box's particles (its vertices,
+ * padding included) and grid tile, n_neighbors nearest neighbours (1..128,
+ * the particle itself counted), density normalised by average_density.
+ * fields: DTFE_FIELD_BIT(DTFE_DENSITY) | DTFE_FIELD_BIT(DTFE_VELOCITY) |
+ * DTFE_FIELD_BIT(DTFE_SCALAR); extensive selects the reference's extensive
+ * scalar convention.  Host outputs (G, 3G, S*G floats; NULL for fields not
+ * asked for).  The reference's float terms, FP64 sums, one rounding. */
+int dtfe_gpu_sph(dtfe_handle h, int32_t n_neighbors, uint32_t fields, int32_t extensive, double average_density,
+                 float* density, float* velocity, float* scalar);
+/* Same with device outputs. */
+int dtfe_gpu_sph_dev(dtfe_handle h, int32_t n_neighbors, uint32_t fields, int32_t extensive,
+                     double average_density, float* density_dev, float* velocity_dev, float* scalar_dev);
+
 /* ---- adjoints (no counterpart in the reference, which has no gradients) --
  * Gradients of L = sum_c a_c density_c + c_c . velocity_c + b_c divergence_c
  * (the grids of the preceding dtfe_gpu_interpolate* call on the same handle,

@@ -42,6 +42,8 @@ def lib() -> C.CDLL:
         L.oracle_dtfe_loss.restype = C.c_double
         L.oracle_dtfe_grad.argtypes = [C.c_int64, vp, C.c_int64, vp, vp, vp, vp, C.c_double, C.c_int64, vp, vp,
                                        vp, vp, vp, C.c_int, vp, vp, vp]
+        L.oracle_sph.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int64, vp, vp, vp, vp, C.c_double, C.c_int, C.c_int,
+                                 C.c_int, vp, vp, vp]
         L.oracle_dtfe_fd.argtypes = [C.c_int64, vp, C.c_int64, vp, vp, vp, vp, C.c_double, C.c_int64, vp, vp,
                                      vp, vp, vp, C.c_int, C.c_int64, vp, vp, C.c_double, C.c_double, C.c_double, vp]
         L.oracle_deposit_loss_grad.argtypes = [C.c_int, vp, vp, C.c_int64, vp, vp, C.c_double, vp, vp, vp]
@@ -76,6 +78,63 @@ def deposit(dplan, mode: int = MODE_REF, velocity: bool = True):
             vel[x0:x0 + dims[0], y0:y0 + dims[1], z0:z0 + dims[2]] = tv.reshape(tuple(dims) + (3,))
     G = int(np.prod(g))
     return dens.reshape(G), None if vel is None else vel.reshape(G, 3)
+
+
+def sph_region(pos, w, vel, scal, xs, ys, zs, avg: float, k: int = 32, extensive: bool = False,
+               mode: int = MODE_REF):
+    """SPH_interpolation for one region's particles and grid point tables:
+    (density (G,), velocity (G, 3) or None, scalars (G, S) or None), doubles."""
+    pos = np.ascontiguousarray(pos, np.float32)
+    w = np.ascontiguousarray(w, np.float32)
+    S = 0 if scal is None else int(np.asarray(scal).reshape(len(pos), -1).shape[1])
+    vel_a = None if vel is None else np.ascontiguousarray(vel, np.float32)
+    sc_a = None if scal is None else np.ascontiguousarray(np.asarray(scal, np.float32).reshape(len(pos), S))
+    xs, ys, zs = (np.ascontiguousarray(a, np.float32) for a in (xs, ys, zs))
+    dims = np.array([len(xs), len(ys), len(zs)], np.int32)
+    G = int(np.prod(dims))
+    dens = np.zeros(G)
+    vo = np.zeros((G, 3)) if vel is not None else None
+    so = np.zeros((G, S)) if S else None
+    rc = lib().oracle_sph(pos.ctypes.data, w.ctypes.data, None if vel_a is None else vel_a.ctypes.data,
+                          None if sc_a is None else sc_a.ctypes.data, S, len(pos), xs.ctypes.data, ys.ctypes.data,
+                          zs.ctypes.data, dims.ctypes.data, float(avg), int(k), int(extensive), int(mode),
+                          dens.ctypes.data, None if vo is None else vo.ctypes.data,
+                          None if so is None else so.ctypes.data)
+    if rc:
+        raise RuntimeError("oracle_sph failed")
+    return dens, vo, so
+
+
+def sph(plan, k: int = 32, velocity: bool = True, scalars: bool = False, extensive: bool = False,
+        mode: int = MODE_REF):
+    """SPH over every sub-box of a DTFE plan (its padded particle sets and
+    grid tiles), placed into the main grid: (density (G,), velocity (G, 3) or
+    None, scalars (G, S) or None)."""
+    g = plan.grid
+    G = int(np.prod(g))
+    S = plan.n_scalars if scalars else 0
+    dens = np.zeros(g)
+    vel = np.zeros(g + (3,)) if velocity else None
+    sc = np.zeros(g + (S,)) if S else None
+    for b in plan.boxes:
+        o, n = b.vert_offset, b.n_verts
+        d = [b.tile_dims[a] for a in range(3)]
+        org = [b.tile_origin[a] for a in range(3)]
+        co = [b.coord_offset[a] for a in range(3)]
+        xs = plan.xs[co[0]:co[0] + d[0]]
+        ys = plan.ys[co[1]:co[1] + d[1]]
+        zs = plan.zs[co[2]:co[2] + d[2]]
+        sv = plan.scalar[o:o + n] if S else None
+        dd, vv, ss = sph_region(plan.xyz[o:o + n], plan.weight[o:o + n],
+                                plan.velocity[o:o + n] if velocity else None, sv, xs, ys, zs, plan.rho_bar, k,
+                                extensive, mode)
+        sl = (slice(org[0], org[0] + d[0]), slice(org[1], org[1] + d[1]), slice(org[2], org[2] + d[2]))
+        dens[sl] = dd.reshape(d)
+        if vel is not None:
+            vel[sl] = vv.reshape(tuple(d) + (3,))
+        if sc is not None:
+            sc[sl] = ss.reshape(tuple(d) + (S,))
+    return dens.reshape(G), None if vel is None else vel.reshape(G, 3), None if sc is None else sc.reshape(G, S)
 
 
 def vertex_density(plan, rho_bar: float | None = None, nthreads: int = 0):

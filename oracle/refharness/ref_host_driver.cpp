@@ -10,6 +10,9 @@
 //   ref_select_in_box        findParticlesInBox      subpartition.h:79-154
 //   ref_average_density      averageDensity          subpartition.h:437-449
 //   ref_deposit              NGP/CIC/TSC_interpolation_regular_grid
+//   ref_sph                  SPH_interpolation (src/SPH_interpolation.cc:47-146,
+//                            252-474) over the reference's kd-tree
+//                            (src/kdtree/kdtree2.cpp, its own translation unit)
 
 #include <cmath>
 #include <cstdint>
@@ -31,6 +34,7 @@ using namespace std;
 #include "NGP_interpolation.cc"
 #include "CIC_interpolation.cc"
 #include "TSC_interpolation.cc"
+#include "SPH_interpolation.cc"
 
 namespace {
 
@@ -114,6 +118,38 @@ int ref_deposit(int kind, const float* pos, const float* w, const float* vel, in
   const size_t G = (size_t)grid[0] * grid[1] * grid[2];
   if (density && q.density.size() == G) std::memcpy(density, q.density.data(), G * sizeof(float));
   if (velocity && q.velocity.size() == G) std::memcpy(velocity, q.velocity.data(), 3 * G * sizeof(float));
+  return 0;
+}
+
+// SPH density (and velocity) of n particles on the grid of one region, with
+// n_neighbors neighbours, normalised by average_density.
+// scal: one scalar per particle (NO_SCALARS=1) or NULL; extensive selects
+// the reference's extensive-scalar convention.
+int ref_sph(const float* pos, const float* w, const float* vel, const float* scal, int extensive, int64_t n,
+            const float region[6], const int32_t grid[3], double average_density, int n_neighbors, float* density,
+            float* velocity, float* scalar) {
+  std::vector<Particle_data> p = make_particles(pos, w, vel, n);
+  if (scal)
+    for (int64_t i = 0; i < n; ++i) p[i].scalar(0) = scal[i];
+  User_options opt;
+  opt.extensive = extensive != 0;
+  opt.aField.scalar = scalar != nullptr;
+  opt.DTFE = false;
+  opt.SPH = true;
+  opt.SPH_neighbors = n_neighbors;
+  opt.gridSize.assign(grid, grid + 3);
+  opt.region.coords.assign(region, region + 6);
+  opt.averageDensity = (Real)average_density;
+  opt.aField.density = true;
+  opt.aField.velocity = velocity != nullptr;
+  std::vector<Sample_point> samples;
+  Quantities q;
+  SPH_interpolation(&p, samples, opt, &q);
+  const size_t G = (size_t)grid[0] * grid[1] * grid[2];
+  if (q.density.size() != G) return 2;
+  if (density) std::memcpy(density, q.density.data(), G * sizeof(float));
+  if (velocity && q.velocity.size() == G) std::memcpy(velocity, q.velocity.data(), 3 * G * sizeof(float));
+  if (scalar && q.scalar.size() == G) std::memcpy(scalar, q.scalar.data(), G * sizeof(float));
   return 0;
 }
 

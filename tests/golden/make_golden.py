@@ -16,6 +16,8 @@ fixture does not depend on it), then:
     scalar gradient on a 10^3 grid, with the reference's own vertex densities;
   * interpolateGrid_averaged_3 with 8 equidistant points per cell;
   * NGP / CIC / TSC density and velocity of the same particles in a region;
+  * SPH_interpolation (32 neighbours) density, velocity and intensive scalar
+    of the padded particle set on the 10^3 grid of the box;
   * parallelGrid for 1..64 threads on three grids, optimalPartitionSplit and
     findParticlesInBox on the particle set.
 """
@@ -45,6 +47,7 @@ def main():
     L.ref_select_in_box.argtypes = [vp, C.c_int64, vp, vp, C.c_int, vp]
     L.ref_select_in_box.restype = C.c_int64
     L.ref_deposit.argtypes = [C.c_int, vp, vp, vp, C.c_int64, vp, vp, C.c_double, vp, vp]
+    L.ref_sph.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int64, vp, vp, C.c_double, C.c_int, vp, vp, vp]
 
     n = 10
     pos, psi = S.zeldovich_lattice(n, 100.0, 0.5, seed=11)
@@ -82,6 +85,17 @@ def main():
                       dgrid.ctypes.data, plan.rho_bar, dd.ctypes.data, dv.ctypes.data)
         out[f"ref_{name}_density"], out[f"ref_{name}_velocity"] = dd, dv
 
+    box = np.array([0, 100, 0, 100, 0, 100], np.float32)
+    g3 = np.array(plan.grid, np.int32)
+    G3 = int(np.prod(g3))
+    sd, sv, ss = np.zeros(G3, np.float32), np.zeros((G3, 3), np.float32), np.zeros(G3, np.float32)
+    sc1 = np.ascontiguousarray(plan.scalar[:, 0])
+    rc = L.ref_sph(plan.xyz.ctypes.data, plan.weight.ctypes.data, plan.velocity.ctypes.data, sc1.ctypes.data, 0,
+                   plan.n_verts, box.ctypes.data, g3.ctypes.data, plan.rho_bar, 32, sd.ctypes.data, sv.ctypes.data,
+                   ss.ctypes.data)
+    assert rc == 0
+    out["ref_sph32_density"], out["ref_sph32_velocity"], out["ref_sph32_scalar"] = sd, sv, ss
+
     grids = np.array([[256, 256, 256], [8, 8, 8], [4, 16, 2]], np.int64)
     table = np.zeros((len(grids), 64, 3), np.int64)
     for gi, g in enumerate(grids):
@@ -103,7 +117,7 @@ def main():
     sel = np.zeros((cnt, 3), np.float32)
     L.ref_select_in_box(pos.ctypes.data, len(pos), full.ctypes.data, padded.ctypes.data, 1, sel.ctypes.data)
     out["select_padded"], out["select_pos"] = padded, sel
-    path = os.path.join(HERE, "ref_zeldovich10.npz")
+    path = os.path.join(HERE, "ref_zeldovich10.npz") if len(sys.argv) < 2 else sys.argv[1]
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path), "bytes")
 

@@ -72,3 +72,17 @@ def test_planning_bit_exact_vs_reference(g):
     _, sel = P.select_in_box(g["particles_pos"], np.array([0, 100, 0, 100, 0, 100], np.float32),
                              g["select_padded"], True)
     assert np.array_equal(sel, g["select_pos"])
+
+
+def test_sph_bit_exact_vs_reference(g):
+    """SPH_interpolation with 32 neighbours (density, velocity, intensive
+    scalar) of the fixture's padded particle set: the oracle in the
+    reference's float arithmetic equals the reference's own output."""
+    plan = golden_plan(g)
+    plan.scalar = g["scalar"]
+    dens, vel, sc = O.sph(plan, k=32, velocity=True, scalars=True, mode=O.MODE_REF)
+    assert np.array_equal(dens.astype(np.float32), g["ref_sph32_density"])
+    assert np.array_equal(vel.astype(np.float32), g["ref_sph32_velocity"])
+    assert np.array_equal(sc[:, 0].astype(np.float32), g["ref_sph32_scalar"])
+    d64, v64, _ = O.sph(plan, k=32, velocity=True, mode=O.MODE_FP64)
+    assert rel_err(d64, g["ref_sph32_density"]) < 1e-6

@@ -35,3 +35,32 @@ def test_live_interpolation(built, n_threads):
                 full = ora[f].reshape(plan.grid + ora[f].shape[1:])
                 tile = full[ox:ox + dims[0], oy:oy + dims[1], oz:oz + dims[2]].reshape(ref[f].shape)
                 assert np.array_equal(tile.astype(np.float32), ref[f]), (method, k, f)
+
+
+@pytest.mark.parametrize("k,extensive", [(32, 0), (16, 1), (7, 0)])
+def test_live_sph(built, k, extensive):
+    """SPH oracle (reference float mode) against the reference's own
+    SPH_interpolation and kd-tree on fresh particles in a region."""
+    import ctypes as C
+    L = R.lib()
+    vp = C.c_void_p
+    L.ref_sph.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int64, vp, vp, C.c_double, C.c_int, vp, vp, vp]
+    n = 18
+    pos, psi = S.zeldovich_lattice(n, 100.0, 0.8, seed=30 + k)
+    rng = np.random.default_rng(k)
+    w = rng.uniform(0.5, 1.5, len(pos)).astype(np.float32)
+    vel = (12 * psi).astype(np.float32)
+    sc = rng.standard_normal(len(pos)).astype(np.float32)
+    region = np.array([10, 90, 5, 95, 0, 100], np.float32)
+    grid = np.array([11, 9, 13], np.int32)
+    G = int(np.prod(grid))
+    d, v, s = np.zeros(G, np.float32), np.zeros((G, 3), np.float32), np.zeros(G, np.float32)
+    avg = float(w.sum()) / 1e6
+    assert L.ref_sph(pos.ctypes.data, w.ctypes.data, vel.ctypes.data, sc.ctypes.data, extensive, len(pos),
+                     region.ctypes.data, grid.ctypes.data, avg, k, d.ctypes.data, v.ctypes.data, s.ctypes.data) == 0
+    tabs = [P.axis_coords(region[2 * a], np.float32((region[2 * a + 1] - region[2 * a]) / np.float32(grid[a])),
+                          int(grid[a])) for a in range(3)]
+    od, ov, osc = O.sph_region(pos, w, vel, sc[:, None], *tabs, avg, k, extensive=bool(extensive), mode=O.MODE_REF)
+    assert np.array_equal(od.astype(np.float32), d)
+    assert np.array_equal(ov.astype(np.float32), v)
+    assert np.array_equal(osc[:, 0].astype(np.float32), s)

@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--bwd-n", type=int, default=128, help="particles per side of the backward workload")
     ap.add_argument("--no-bwd", action="store_true")
     ap.add_argument("--fd-particles", type=int, default=1000)
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-compare", action="store_true")
+    ap.add_argument("--batch-steps", type=int, default=10)
     return ap.parse_args()
 
 
@@ -354,6 +357,131 @@ def backward_leg(args, local: int, threads: int) -> dict:
             "vertices": V, "tetrahedra": plan.n_tets, "host_plan_s": t_plan}
 
 
+def compare_leg(args, plan, local: int, threads: int) -> dict:
+    """The comparison estimators on the main workload, device-timed: SPH with
+    32 neighbours on the same padded sub-box particle sets and grid tiles,
+    CIC and TSC deposition (their own paddings, the reference's sub-box
+    split) of density and velocity."""
+    import torch
+    from dtfe_b200 import plan as P
+    from dtfe_b200 import synthetic as S
+    from dtfe_b200.device import DeviceDTFE
+    cuda = torch.device("cuda", local)
+    G = int(np.prod(plan.grid))
+    res = {}
+    dev = DeviceDTFE(local)
+    dev.load(plan)
+    stream = torch.cuda.ExternalStream(dev.stream, device=cuda)
+    d = torch.empty(G, device=cuda)
+    v = torch.empty((G, 3), device=cuda)
+
+    def sph():
+        dev.sph_dev(plan.rho_bar, d, v, n_neighbors=32)
+    sph()
+    t = _events(stream, sph, 2)
+    res["SPH32"] = {"ms": 1e3 * t, "grid_samples_per_s": G / t}
+    dev.close()
+    n = args.n
+    pos, psi = S.zeldovich_lattice(n, S.BOX, 1.0, seed=1)
+    rng = np.random.default_rng(2)
+    vel = (100.0 * psi / (S.BOX / n) + rng.normal(0.0, 50.0, psi.shape)).astype(np.float32)
+    del psi
+    w = np.ones(len(pos), np.float32)
+    for kind in ("CIC", "TSC"):
+        dp = P.make_deposit_plan(pos, w, vel, grid=plan.grid, n_threads=threads, kind=kind,
+                                 average_density_value=float(len(pos)) / S.BOX ** 3)
+        dd = DeviceDTFE(local)
+        ds = torch.cuda.ExternalStream(dd.stream, device=cuda)
+
+        def dep():
+            dd.deposit_dev(dp, d, v)
+        dep()
+        t = _events(ds, dep, 3)
+        res[kind] = {"ms": 1e3 * t, "grid_samples_per_s": G / t, "particle_copies": dp.n,
+                     "note": "includes the host->device copy of the particles (host-input API)"}
+        dd.close()
+    return res
+
+
+def batch_leg(args, local: int, threads: int) -> dict:
+    """Batched sub-boxes: 64 periodic sub-boxes (side 25 Mpc/h) with
+    log-normal particle counts in [1e4, 1e6] (median 1e5), each a Zel'dovich
+    lattice plus an NFW cluster (20% of its particles, r_s = 0.05 side),
+    padding 10% of the side, each interpolated to its own 64^3 grid (density
+    + velocity).  A step: vertex densities + seeds + interpolation of all 64
+    tiles.  Timed three ways on the device: the captured CUDA graph replayed
+    back to back, the same step through the C ABI calls, and one handle and
+    launch sequence per sub-box (the unbatched loop)."""
+    import torch
+    from dtfe_b200 import plan as P
+    from dtfe_b200 import synthetic as S
+    from dtfe_b200.device import DeviceDTFE
+    cuda = torch.device("cuda", local)
+    t0 = time.time()
+    wl = S.workload("subboxes64_nfw")
+    plan = P.make_subbox_plan(wl["subboxes"], grid=wl["grid"], padding_fraction=wl["padding_fraction"])
+    t_plan = time.time() - t0
+    fields = ["density", "velocity"]
+    G = int(np.prod(plan.grid))
+    outs = {"density": torch.empty((G, 1), device=cuda), "velocity": torch.empty((G, 3), device=cuda)}
+    dev = DeviceDTFE(local)
+    dev.load(plan)
+    stream = torch.cuda.ExternalStream(dev.stream, device=cuda)
+    variants = dev.autotune(fields)
+
+    def plain():
+        dev.vertex_density(plan.rho_bar)
+        dev.interpolate_dev(fields, outs)
+    for _ in range(3):
+        plain()
+    t_plain = _events(stream, plain, args.batch_steps)
+    dev.graph_build(plan.rho_bar, fields, outs)
+    for _ in range(3):
+        dev.graph_launch()
+    dev.synchronize()
+    t_graph = _events(stream, dev.graph_launch, args.batch_steps)
+    st = dev.read_status()
+    # unbatched: one handle per sub-box, launches one sub-box at a time
+    parts = P.split_boxes(plan)
+    devs, pouts = [], []
+    for p in parts:
+        d = DeviceDTFE(local)
+        d.load(p)
+        d.set_variants(*variants)
+        g = int(np.prod(p.grid))
+        devs.append(d)
+        pouts.append({"density": torch.empty((g, 1), device=cuda), "velocity": torch.empty((g, 3), device=cuda)})
+
+    def loop():
+        for d, o, p in zip(devs, pouts, parts):
+            d.vertex_density(p.rho_bar)
+            d.interpolate_dev(fields, o)
+    for _ in range(2):
+        loop()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        loop()
+    torch.cuda.synchronize()
+    t_loop = (time.perf_counter() - t0) / 3
+    for d in devs:
+        d.close()
+    counts = [int(b.n_verts) for b in plan.box_list()]
+    dev.close()
+    return {"workload": "subboxes64_nfw: 64 periodic sub-boxes (side 25), log-normal counts in [1e4, 1e6] "
+                        "(median 1e5), lattice + NFW cluster, padding 10%, 64^3 grid each, density + velocity",
+            "grid_samples_per_step": G, "graph_ms": 1e3 * t_graph, "plain_ms": 1e3 * t_plain,
+            "per_subbox_loop_ms": 1e3 * t_loop, "graph_samples_per_s": G / t_graph,
+            "plain_samples_per_s": G / t_plain, "loop_samples_per_s": G / t_loop,
+            "launch_variants": {"locate": variants[0], "eval": variants[1]},
+            "vertices": plan.n_verts, "tetrahedra": plan.n_tets,
+            "vertices_per_subbox": {"min": min(counts), "median": int(np.median(counts)), "max": max(counts)},
+            "walk": {k: st[k] for k in ("n_samples_located", "n_walk_steps", "n_exact_tests", "n_ties", "n_outside")},
+            "host_plan_s": t_plan,
+            "note": "loop timed by wall clock around 64 synchronous C ABI call pairs (what one launch sequence "
+                    "per sub-box costs); graph and plain by CUDA events on the handle's stream"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -532,6 +660,14 @@ def run_ours(args):
                 "kernel": "k_interpolate<centre>", "kernel_ms": 1e3 * t_interp,
                 "algorithmic_bytes": int(b_alg), "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})"}
 
+    compare = None
+    if not args.no_compare:
+        compare = compare_leg(args, plan, local, threads)
+
+    batch = None
+    if not args.no_batch:
+        batch = batch_leg(args, local, threads)
+
     bwd = None
     if not args.no_bwd:
         bwd = backward_leg(args, local, threads)
@@ -559,6 +695,8 @@ def run_ours(args):
         "cpu_baseline": cpu,
         "mc": mc,
         "backward": bwd,
+        "batched_subboxes": batch,
+        "comparison_estimators": compare,
         "walk": {k: status[k] for k in ("n_samples_located", "n_walk_steps", "n_exact_tests", "n_ties",
                                         "n_outside")} if status else None,
         "host_prep_s": plan.timings,

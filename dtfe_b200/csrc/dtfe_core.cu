@@ -713,6 +713,7 @@ struct dtfe_gpu_s {
   float factor = 0.f;             // (D+1)/rho_bar of the last vertex-density call
   double *g_rho = nullptr, *g_x = nullptr, *g_v = nullptr, *g_S = nullptr, *g_m = nullptr, *vbar = nullptr;
   float* adj_a = nullptr;         // device copies of host loss weights
+  cudaGraphExec_t step_graph = nullptr;  // captured step (dtfe_gpu_graph_build)
   void* sph_scratch = nullptr;    // SPH cell grids, neighbour bookkeeping, FP64 sums
   size_t sph_bytes = 0;
   float* sph_out = nullptr;       // host-output SPH staging
@@ -757,6 +758,15 @@ int field_components(int slot, int S) {
     case DTFE_SCALAR_GRADIENT: return 3 * S;
   }
   return 0;
+}
+
+// A captured step refers to the handle's buffers as they were at capture.
+void drop_graph(dtfe_handle h) {
+  if (h->step_graph) {
+    cudaStreamSynchronize(h->stream);
+    cudaGraphExecDestroy(h->step_graph);
+    h->step_graph = nullptr;
+  }
 }
 
 int prepare_bins(dtfe_handle h) {
@@ -863,6 +873,7 @@ int dtfe_gpu_destroy(dtfe_handle h) {
   if (!h) return DTFE_OK;
   cudaSetDevice(h->device);
   cudaStreamSynchronize(h->stream);
+  if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
   void* ptrs[] = {h->tet_v, h->tet_n, h->posd, h->vel4, h->scal, h->w, h->vol, h->inc_off, h->inc,
                   h->scratch_i, h->scan_blocks, h->hull,
                   h->boxes, h->tile_prefix, h->tet_prefix, h->bin_offset, h->bins,
@@ -958,6 +969,7 @@ int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n, i
   h->density_ready = false;
   h->bins_ready = false;
   h->tet_c_valid = false;
+  drop_graph(h);
   return DTFE_OK;
 }
 
@@ -1014,6 +1026,7 @@ int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* box
   h->grid[0] = grid[0]; h->grid[1] = grid[1]; h->grid[2] = grid[2];
   h->bins_ready = false;
   h->eq_nn = 0;
+  drop_graph(h);
   return DTFE_OK;
 }
 
@@ -1055,8 +1068,10 @@ int dtfe_gpu_download_vertex_density(dtfe_handle h, float* dens) {
   return DTFE_OK;
 }
 
-static int interpolate_impl(dtfe_handle h, const dtfe_interp_opts* o, float* const out_dev[DTFE_NUM_FIELDS],
-                            dtfe_status* status) {
+// Validation, one-time set-up and every launch of one interpolation on the
+// handle's stream; nothing waits for the GPU after the set-up, so the
+// launches can be captured into a graph once the set-up has run.
+static int interp_enqueue(dtfe_handle h, const dtfe_interp_opts* o, float* const out_dev[DTFE_NUM_FIELDS]) {
   if (!h || !o) return set_error(DTFE_ERR_ARG, "null argument");
   if (h->K == 0) return set_error(DTFE_ERR_STATE, "sub-boxes not set");
   if (h->T == 0) return set_error(DTFE_ERR_DEGENERATE, "no tetrahedra");
@@ -1139,6 +1154,11 @@ static int interpolate_impl(dtfe_handle h, const dtfe_interp_opts* o, float* con
   h->tet_c_valid = method == DTFE_METHOD_CENTRE;  // the adjoint differentiates centre values only
   h->tet_c_fix = (o->flags & DTFE_FLAG_FIX_VALUE_INTERP) != 0;
   DTFE_CUDA_TRY(cudaGetLastError());
+  return DTFE_OK;
+}
+
+static int read_status(dtfe_handle h, dtfe_status* status) {
+  cudaStream_t st = h->stream;
   unsigned long long cnt[CNT_N];
   DTFE_CUDA_TRY(cudaMemcpyAsync(cnt, h->counters, sizeof(cnt), cudaMemcpyDeviceToHost, st));
   DTFE_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1152,6 +1172,13 @@ static int interpolate_impl(dtfe_handle h, const dtfe_interp_opts* o, float* con
   }
   if (cnt[CNT_FAIL]) return set_error(DTFE_ERR_WALK, "point-location walk hit its step limit");
   return DTFE_OK;
+}
+
+static int interpolate_impl(dtfe_handle h, const dtfe_interp_opts* o, float* const out_dev[DTFE_NUM_FIELDS],
+                            dtfe_status* status) {
+  int rc = interp_enqueue(h, o, out_dev);
+  if (rc) return rc;
+  return read_status(h, status);
 }
 
 // Times every launch variant of the locate and evaluation kernels on the
@@ -1381,6 +1408,49 @@ int dtfe_gpu_interpolate_dev(dtfe_handle h, const dtfe_interp_opts* opts,
   if (!h) return set_error(DTFE_ERR_ARG, "null handle");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
   return interpolate_impl(h, opts, out_dev, st);
+}
+
+int dtfe_gpu_graph_build(dtfe_handle h, double rho_bar, const dtfe_interp_opts* opts,
+                         float* const out_dev[DTFE_NUM_FIELDS]) {
+  if (!h || !opts) return set_error(DTFE_ERR_ARG, "null argument");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  drop_graph(h);
+  // one plain step first: allocations, equidistant offsets and the walk
+  // check happen here, so the captured launches need none of them
+  int rc = dtfe_gpu_vertex_density(h, rho_bar);
+  if (rc) return rc;
+  if ((rc = interpolate_impl(h, opts, out_dev, nullptr))) return rc;
+  cudaGraph_t g = nullptr;
+  DTFE_CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  rc = dtfe_gpu_vertex_density(h, rho_bar);
+  if (!rc) rc = interp_enqueue(h, opts, out_dev);
+  cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return set_error(DTFE_ERR_CUDA, cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&h->step_graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    h->step_graph = nullptr;
+    return set_error(DTFE_ERR_CUDA, cudaGetErrorString(e));
+  }
+  return DTFE_OK;
+}
+
+int dtfe_gpu_graph_launch(dtfe_handle h) {
+  if (!h) return set_error(DTFE_ERR_ARG, "null handle");
+  if (!h->step_graph) return set_error(DTFE_ERR_STATE, "no step graph built (or the handle changed since)");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  DTFE_CUDA_TRY(cudaGraphLaunch(h->step_graph, h->stream));
+  return DTFE_OK;
+}
+
+int dtfe_gpu_read_status(dtfe_handle h, dtfe_status* status) {
+  if (!h) return set_error(DTFE_ERR_ARG, "null handle");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  return read_status(h, status);
 }
 
 int dtfe_gpu_interpolate(dtfe_handle h, const dtfe_interp_opts* opts, float* const out[DTFE_NUM_FIELDS],

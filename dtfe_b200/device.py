@@ -110,6 +110,27 @@ class DeviceDTFE:
         self.last_status = st.as_dict()
         return self.last_status
 
+    def graph_build(self, rho_bar: float, fields, outs_dev: dict, method: int = 0, n_samples: int = 1,
+                    seed: int = 0, fix: bool = False) -> None:
+        """Captures one step (vertex densities + interpolation into outs_dev)
+        as a CUDA graph; graph_launch replays it."""
+        outs = [None] * N.NUM_FIELDS
+        for f in fields:
+            outs[N.FIELD_SLOTS[f]] = N.ptr(outs_dev[f]) if not isinstance(outs_dev[f], int) else outs_dev[f]
+        self._graph_outs = outs_dev  # keep the buffers alive with the graph
+        optr = (C.c_void_p * N.NUM_FIELDS)(*outs)
+        o = self._opts(fields, method, n_samples, seed, fix)
+        N.check(self.lib.dtfe_gpu_graph_build(self.h, float(rho_bar), C.byref(o), optr))
+
+    def graph_launch(self) -> None:
+        N.check(self.lib.dtfe_gpu_graph_launch(self.h))
+
+    def read_status(self) -> dict:
+        st = N.Status()
+        N.check(self.lib.dtfe_gpu_read_status(self.h, C.byref(st)))
+        self.last_status = st.as_dict()
+        return self.last_status
+
     def deposit(self, dplan, velocity: bool = True) -> dict:
         """NGP / CIC / TSC density (and velocity) on the host."""
         G = int(np.prod(dplan.grid))

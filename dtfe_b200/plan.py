@@ -372,3 +372,34 @@ def make_subbox_plan(subboxes: list, grid=(64, 64, 64), padding_fraction: float 
     rho_bar = float(np.float32(sum(float(p.weight.sum()) for p in subboxes) / (len(subboxes) * side ** 3)))
     main = (len(subboxes) * grid[0], grid[1], grid[2])
     return assemble(sets, tiles, weight, velocity, None, main, rho_bar, np.zeros(6, np.float32), timings)
+
+
+def split_boxes(plan: Plan) -> list:
+    """One single-box Plan per sub-box of ``plan`` (its vertices, tetrahedra
+    with re-based ids, its grid tile as the whole grid): the unbatched form,
+    one handle and one launch sequence per sub-box."""
+    out = []
+    for b in plan.box_list():
+        vo, nv, to, nt = int(b.vert_offset), int(b.n_verts), int(b.tet_offset), int(b.n_tets)
+        tv = np.ascontiguousarray(plan.tet_v[to:to + nt] - vo, np.int32)
+        tn = plan.tet_n[to:to + nt]
+        tn = np.ascontiguousarray(np.where(tn >= 0, tn - to, tn), np.int32)
+        one = (N.Subbox * 1)()
+        o = one[0]
+        C.memmove(C.addressof(o), C.addressof(b), C.sizeof(N.Subbox))
+        o.vert_offset, o.tet_offset = 0, 0
+        d = [int(b.tile_dims[a]) for a in range(3)]
+        co = [int(b.coord_offset[a]) for a in range(3)]
+        for a in range(3):
+            o.tile_origin[a] = 0
+            o.coord_offset[a] = 0
+        sl = slice(vo, vo + nv)
+        out.append(Plan(tet_v=tv, tet_n=tn, xyz=np.ascontiguousarray(plan.xyz[sl]), src=plan.src[sl],
+                        weight=np.ascontiguousarray(plan.weight[sl]),
+                        velocity=None if plan.velocity is None else np.ascontiguousarray(plan.velocity[sl]),
+                        scalar=None if plan.scalar is None else np.ascontiguousarray(plan.scalar[sl]),
+                        boxes=one, xs=np.ascontiguousarray(plan.xs[co[0]:co[0] + d[0]]),
+                        ys=np.ascontiguousarray(plan.ys[co[1]:co[1] + d[1]]),
+                        zs=np.ascontiguousarray(plan.zs[co[2]:co[2] + d[2]]), grid=tuple(d),
+                        rho_bar=plan.rho_bar, padding=plan.padding))
+    return out

@@ -83,18 +83,35 @@ def nfw_radii(n: int, rs: float, c: float, rng) -> np.ndarray:
     return np.interp(u, m, x) * rs
 
 
-def _lattice_plus_nfw(nk: int, side: float, seed: int) -> np.ndarray:
+def lattice_plus_nfw(nk: int, side: float, seed: int):
+    """One periodic sub-box of about nk particles: a Zel'dovich lattice (rms
+    0.5 spacing) holding 80% of them and an NFW-like cluster (r_s = 0.05 side,
+    truncated at 10 r_s, random centre) holding 20%.  Velocities: 100 km/s per
+    unit lattice displacement + N(0, 50 km/s) on the lattice, N(0, 300 km/s)
+    per component in the cluster.  Returns (pos, vel) float32."""
     rng = np.random.default_rng(seed)
     n_cl = int(round(0.2 * nk))
     n_lat = max(2, int(round((nk - n_cl) ** (1.0 / 3.0))))
-    lat, _ = zeldovich_lattice(n_lat, side, 0.5, seed + 1)
+    lat, psi = zeldovich_lattice(n_lat, side, 0.5, seed + 1)
+    v_lat = 100.0 * psi / (side / n_lat) + rng.normal(0.0, 50.0, psi.shape)
     r = nfw_radii(n_cl, 0.05 * side, 10.0, rng)
     d = rng.standard_normal((n_cl, 3))
     d /= np.linalg.norm(d, axis=1, keepdims=True)
     centre = rng.random(3) * side
     cl = np.mod(centre + d * r[:, None], side).astype(np.float32)
     cl[cl >= np.float32(side)] = np.float32(0.0)
-    return np.concatenate([lat, cl]).astype(np.float32)
+    v_cl = rng.normal(0.0, 300.0, (n_cl, 3))
+    return (np.concatenate([lat, cl]).astype(np.float32),
+            np.concatenate([v_lat, v_cl]).astype(np.float32))
+
+
+def subbox_set(counts, side: float, seed0: int = 1000) -> list:
+    """Periodic sub-boxes [0, side)^3 with the given particle counts."""
+    boxes = []
+    for i, nk in enumerate(counts):
+        pos, vel = lattice_plus_nfw(int(nk), side, seed=seed0 + i)
+        boxes.append(Particles(pos, np.ones(len(pos), np.float32), vel, box=(0.0, side, 0.0, side, 0.0, side)))
+    return boxes
 
 
 def workload(name: str) -> dict:
@@ -124,12 +141,7 @@ def workload(name: str) -> dict:
     if name == "subboxes64_nfw":
         rng = np.random.default_rng(7)
         counts = np.clip(np.exp(rng.normal(np.log(1e5), 1.0, 64)), 1e4, 1e6).astype(np.int64)
-        side = BOX / 4.0
-        boxes = []
-        for i, nk in enumerate(counts):
-            pos = _lattice_plus_nfw(int(nk), side, seed=1000 + i)
-            boxes.append(Particles(pos, np.ones(len(pos), np.float32),
-                                   box=(0.0, side, 0.0, side, 0.0, side)))
+        boxes = subbox_set(counts, BOX / 4.0)
         return dict(subboxes=boxes, grid=(64, 64, 64), fields=("density", "velocity"),
                     padding_fraction=0.1, name=name)
     raise KeyError(name)

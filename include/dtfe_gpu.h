@@ -192,6 +192,22 @@ int dtfe_gpu_deposit_dev(dtfe_handle h, int32_t kind, const float* xyz, const fl
                          int64_t n, int32_t n_boxes, const dtfe_deposit_box* boxes, const int32_t grid[3],
                          double average_density, float* density_dev, float* velocity_dev);
 
+/* ---- batched step as one CUDA graph --------------------------------------
+ * The reference loops over its sub-boxes (DTFE_parallel, src/DTFE.cpp:
+ * 287-385), one thread each.  Here every sub-box of the handle is one range
+ * of one launch per kernel; dtfe_gpu_graph_build runs one plain step
+ * (vertex densities with rho_bar, seeds, interpolation with *opts into the
+ * device buffers out_dev) and then captures the same launches into a CUDA
+ * graph; dtfe_gpu_graph_launch replays it on the handle's stream without
+ * waiting.  The graph holds the handle's buffers, the launch variants chosen
+ * at build time and the out_dev pointers: any later upload or set_subboxes
+ * drops it (DTFE_ERR_STATE on launch until rebuilt).  dtfe_gpu_read_status
+ * waits for the stream and returns the counters of the last step. */
+int dtfe_gpu_graph_build(dtfe_handle h, double rho_bar, const dtfe_interp_opts* opts,
+                         float* const out_dev[DTFE_NUM_FIELDS]);
+int dtfe_gpu_graph_launch(dtfe_handle h);
+int dtfe_gpu_read_status(dtfe_handle h, dtfe_status* status);
+
 /* SPH estimator (SPH_interpolation, src/SPH_interpolation.cc:252-474) on the
  * uploaded vertices and sub-boxes: each sub-box's particles (its vertices,
  * padding included) and grid tile, n_neighbors nearest neighbours (1..128,

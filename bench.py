@@ -427,6 +427,7 @@ def batch_leg(args, local: int, threads: int) -> dict:
     dev = DeviceDTFE(local)
     dev.load(plan)
     stream = torch.cuda.ExternalStream(dev.stream, device=cuda)
+    dev.vertex_density(plan.rho_bar)
     variants = dev.autotune(fields)
 
     def plain():

@@ -38,8 +38,8 @@ def test_graph_replay_matches_plain_and_oracle(bplan):
     outs = {f: torch.empty((G, NCOMP[f]), device=cuda) for f in FIELDS}
     with DeviceDTFE(0) as dev:
         dev.load(plan)
-        dev.autotune(FIELDS)
         dev.vertex_density(plan.rho_bar)
+        dev.autotune(FIELDS)
         st = dev.interpolate_dev(FIELDS, outs)
         plain = {f: outs[f].cpu().numpy().copy() for f in FIELDS}
         assert st["n_walk_failures"] == 0

@@ -658,7 +658,7 @@ def run_ours(args):
     traffic = profile_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic.get("dram_bytes_per_launch_scaled") if traffic else None,
-                "kernel": "k_interpolate<centre>", "kernel_ms": 1e3 * t_interp,
+                "kernel": "k_locate_cells + k_eval_centre (cell-centre interpolation)", "kernel_ms": 1e3 * t_interp,
                 "algorithmic_bytes": int(b_alg), "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})"}
 
     compare = None

@@ -428,18 +428,53 @@ void compact(Tessellator& T, bool sort_tets, Result& R) {
     if (v[0] < 0 || v[1] < 0 || v[2] < 0 || v[3] < 0) continue;  // infinite or freed
     finite.push_back((int32_t)t);
   }
+  // Canonical vertex order per tetrahedron: of the 12 orientation-preserving
+  // (even) permutations the lexicographically smallest vertex tuple.  With
+  // the sort below the output depends only on the point set (for a unique
+  // Delaunay tessellation), not on the insertion order.
+  static const int kEven[12][4] = {{0, 1, 2, 3}, {0, 2, 3, 1}, {0, 3, 1, 2}, {1, 0, 3, 2}, {1, 2, 0, 3},
+                                   {1, 3, 2, 0}, {2, 0, 1, 3}, {2, 1, 3, 0}, {2, 3, 0, 1}, {3, 0, 2, 1},
+                                   {3, 1, 0, 2}, {3, 2, 1, 0}};
+  std::vector<int8_t> perm(cap, 0);
+  for (int32_t t : finite) {
+    const int32_t* v = &T.tv[4 * (int64_t)t];
+    int best = 0;
+    for (int q = 1; q < 12; ++q)
+      for (int k = 0; k < 4; ++k) {
+        const int32_t a = v[kEven[q][k]], b = v[kEven[best][k]];
+        if (a != b) {
+          if (a < b) best = q;
+          break;
+        }
+      }
+    perm[t] = (int8_t)best;
+  }
+  auto vert = [&](int64_t t, int k) { return T.tv[4 * t + kEven[perm[t]][k]]; };
   if (sort_tets && !finite.empty()) {
     MortonFrame frame(T.P, T.n);
-    std::vector<std::pair<uint64_t, int32_t>> keyed(finite.size());
+    struct Key {
+      uint64_t m;
+      int32_t v[4];
+      int32_t t;
+      bool operator<(const Key& o) const {
+        if (m != o.m) return m < o.m;
+        for (int k = 0; k < 4; ++k)
+          if (v[k] != o.v[k]) return v[k] < o.v[k];
+        return false;
+      }
+    };
+    std::vector<Key> keyed(finite.size());
     for (size_t i = 0; i < finite.size(); ++i) {
-      const int32_t* v = &T.tv[4 * (int64_t)finite[i]];
+      const int64_t t = finite[i];
       double c[3] = {0, 0, 0};
       for (int a = 0; a < 4; ++a)
-        for (int k = 0; k < 3; ++k) c[k] += 0.25 * T.pt(v[a])[k];
-      keyed[i] = {frame.key(c), finite[i]};
+        for (int k = 0; k < 3; ++k) c[k] += 0.25 * T.pt(vert(t, a))[k];
+      keyed[i].m = frame.key(c);
+      for (int a = 0; a < 4; ++a) keyed[i].v[a] = vert(t, a);
+      keyed[i].t = (int32_t)t;
     }
     std::sort(keyed.begin(), keyed.end());
-    for (size_t i = 0; i < finite.size(); ++i) finite[i] = keyed[i].second;
+    for (size_t i = 0; i < finite.size(); ++i) finite[i] = keyed[i].t;
   }
   for (size_t i = 0; i < finite.size(); ++i) newid[finite[i]] = (int32_t)i;
   R.tet_v.resize(4 * finite.size());
@@ -447,8 +482,9 @@ void compact(Tessellator& T, bool sort_tets, Result& R) {
   for (size_t i = 0; i < finite.size(); ++i) {
     int64_t t = finite[i];
     for (int k = 0; k < 4; ++k) {
-      R.tet_v[4 * i + k] = T.tv[4 * t + k];
-      int32_t nb = T.tn[4 * t + k];
+      const int src = kEven[perm[t]][k];
+      R.tet_v[4 * i + k] = T.tv[4 * t + src];
+      int32_t nb = T.tn[4 * t + src];
       R.tet_n[4 * i + k] = newid[nb];  // -1 for an infinite neighbour
     }
   }
@@ -486,7 +522,7 @@ void dtfe_tessellate_batch(int k, const double* const* xyz, const int64_t* n,
                            int* rc) {
 #pragma omp parallel for schedule(dynamic, 1)
   for (int i = 0; i < k; ++i)
-    rc[i] = dtfe_tessellate(xyz[i], n[i], seed + (uint64_t)i, sort_tets, &handles[i]);
+    rc[i] = dtfe_tessellate(xyz[i], n[i], seed, sort_tets, &handles[i]);
 }
 
 void dtfe_tess_sizes(void* handle, int64_t* n_tets, int64_t* n_points,

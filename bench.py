@@ -595,8 +595,11 @@ def run_ours(args):
     ms_step = 1e3 * t_total / args.steps
 
     # Monte-Carlo average (8 points per cell): point evaluations/s
+    # the side legs (MC, comparison estimators, batched sub-boxes, backward)
+    # describe one GPU; at N > 1 only the step and its e2e are measured
+    side = world == 1
     mc = None
-    if not args.no_mc:
+    if side and not args.no_mc:
         for _ in range(2):
             dev.vertex_density(plan.rho_bar)
             dev.interpolate_dev(FIELDS, outs, method=2, n_samples=8, seed=3)
@@ -662,15 +665,15 @@ def run_ours(args):
                 "algorithmic_bytes": int(b_alg), "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})"}
 
     compare = None
-    if not args.no_compare:
+    if side and not args.no_compare:
         compare = compare_leg(args, plan, local, threads)
 
     batch = None
-    if not args.no_batch:
+    if side and not args.no_batch:
         batch = batch_leg(args, local, threads)
 
     bwd = None
-    if not args.no_bwd:
+    if side and not args.no_bwd:
         bwd = backward_leg(args, local, threads)
 
     cpu = None

@@ -39,6 +39,19 @@ class DepositBox(C.Structure):
                 ("tile_origin", C.c_int32 * 3), ("tile_dims", C.c_int32 * 3)]
 
 
+class PlanView(C.Structure):
+    """dtfe_plan_view (include/dtfe_host.h)."""
+    _fields_ = [("kind", C.c_int32), ("grid", C.c_int32 * 3), ("rho_bar", C.c_double), ("padding", C.c_float * 6),
+                ("n_verts", C.c_int64), ("n_tets", C.c_int64), ("n_boxes", C.c_int32), ("n_scalars", C.c_int32),
+                ("tet_v", C.c_void_p), ("tet_n", C.c_void_p), ("xyz", C.c_void_p), ("src", C.c_void_p),
+                ("weight", C.c_void_p), ("velocity", C.c_void_p), ("scalar", C.c_void_p),
+                ("boxes", C.c_void_p), ("xs", C.c_void_p), ("ys", C.c_void_p), ("zs", C.c_void_p),
+                ("n_xs", C.c_int64), ("n_ys", C.c_int64), ("n_zs", C.c_int64),
+                ("n_particles", C.c_int64), ("dep_pos", C.c_void_p), ("dep_weight", C.c_void_p),
+                ("dep_velocity", C.c_void_p), ("dep_src", C.c_void_p), ("n_dep_boxes", C.c_int32),
+                ("dep_boxes", C.c_void_p)]
+
+
 class InterpOpts(C.Structure):
     """dtfe_interp_opts."""
     _fields_ = [("method", C.c_int32), ("n_samples", C.c_int32), ("seed", C.c_uint64),
@@ -119,6 +132,10 @@ def host() -> C.CDLL:
         lib.dtfe_optimal_partition.argtypes = [vp, C.c_int64, vp, vp, vp, vp, vp]
         lib.dtfe_optimal_partition.restype = C.c_int
         lib.dtfe_axis_coords.argtypes = [C.c_float, C.c_float, C.c_int64, vp]
+        lib.dtfe_plan_build.argtypes = [C.c_int, vp, vp, vp, vp, C.c_int32, C.c_int64, vp, C.c_int, vp, C.c_int32,
+                                        C.c_float, C.c_double, C.POINTER(C.c_void_p)]
+        lib.dtfe_plan_get.argtypes = [C.c_void_p, C.POINTER(PlanView)]
+        lib.dtfe_plan_release.argtypes = [C.c_void_p]
         _host = lib
     return _host
 

@@ -403,3 +403,64 @@ def split_boxes(plan: Plan) -> list:
                         zs=np.ascontiguousarray(plan.zs[co[2]:co[2] + d[2]]), grid=tuple(d),
                         rho_bar=plan.rho_bar, padding=plan.padding))
     return out
+
+
+def _view_array(ptr, dtype, shape):
+    if not ptr or int(np.prod(shape)) == 0:
+        return np.zeros(shape, dtype)
+    n = int(np.prod(shape))
+    buf = (C.c_byte * (n * np.dtype(dtype).itemsize)).from_address(ptr)
+    return np.frombuffer(buf, dtype=dtype, count=n).reshape(shape).copy()
+
+
+def native_plan(kind: str, pos, weight, velocity=None, scalar=None, grid=(64, 64, 64),
+                box=(0, 100, 0, 100, 0, 100), periodic: bool = True, n_threads: int = 1,
+                padding_particles: float = 5.0, average_density_value: float | None = None):
+    """The same plan built by the C++ planner (dtfe_plan_build,
+    include/dtfe_host.h): a Plan for "DTFE", a DepositPlan for "NGP", "CIC",
+    "TSC"."""
+    kinds = {"DTFE": 0, "NGP": 1, "CIC": 2, "TSC": 3}
+    k = kinds[kind]
+    pos = _f32(pos)
+    w = None if weight is None else _f32(weight)
+    vel = None if velocity is None else _f32(velocity)
+    S = 0 if scalar is None else int(np.asarray(scalar).reshape(len(pos), -1).shape[1])
+    sc = None if scalar is None else np.ascontiguousarray(np.asarray(scalar, np.float32).reshape(len(pos), S))
+    bx = _f32(box)
+    g = np.ascontiguousarray(grid, np.int32)
+    lib = N.host()
+    h = C.c_void_p()
+    rc = lib.dtfe_plan_build(k, pos.ctypes.data, None if w is None else w.ctypes.data,
+                             None if vel is None else vel.ctypes.data, None if sc is None else sc.ctypes.data, S,
+                             len(pos), bx.ctypes.data, int(periodic), g.ctypes.data, int(n_threads),
+                             float(padding_particles),
+                             float(np.float32(average_density_value)) if average_density_value is not None else 0.0,
+                             C.byref(h))
+    if rc:
+        raise RuntimeError(f"dtfe_plan_build failed with status {rc}")
+    try:
+        v = N.PlanView()
+        lib.dtfe_plan_get(h, C.byref(v))
+        if k == 0:
+            V, T, K = v.n_verts, v.n_tets, v.n_boxes
+            boxes = (N.Subbox * K)()
+            C.memmove(C.addressof(boxes), v.boxes, C.sizeof(N.Subbox) * K)
+            return Plan(tet_v=_view_array(v.tet_v, np.int32, (T, 4)), tet_n=_view_array(v.tet_n, np.int32, (T, 4)),
+                        xyz=_view_array(v.xyz, np.float32, (V, 3)), src=_view_array(v.src, np.int32, (V,)),
+                        weight=_view_array(v.weight, np.float32, (V,)),
+                        velocity=_view_array(v.velocity, np.float32, (V, 3)) if v.velocity else None,
+                        scalar=_view_array(v.scalar, np.float32, (V, v.n_scalars)) if v.scalar else None,
+                        boxes=boxes, xs=_view_array(v.xs, np.float32, (v.n_xs,)),
+                        ys=_view_array(v.ys, np.float32, (v.n_ys,)), zs=_view_array(v.zs, np.float32, (v.n_zs,)),
+                        grid=tuple(int(x) for x in v.grid), rho_bar=float(v.rho_bar),
+                        padding=np.array(list(v.padding), np.float32))
+        n, K = v.n_particles, v.n_dep_boxes
+        boxes = (N.DepositBox * K)()
+        C.memmove(C.addressof(boxes), v.dep_boxes, C.sizeof(N.DepositBox) * K)
+        return DepositPlan(pos=_view_array(v.dep_pos, np.float32, (n, 3)),
+                           weight=_view_array(v.dep_weight, np.float32, (n,)),
+                           velocity=_view_array(v.dep_velocity, np.float32, (n, 3)) if v.dep_velocity else None,
+                           boxes=boxes, grid=tuple(int(x) for x in v.grid), rho_bar=float(v.rho_bar), kind=k - 1,
+                           src=_view_array(v.dep_src, np.int64, (n,)))
+    finally:
+        lib.dtfe_plan_release(h)

@@ -92,11 +92,46 @@ def build_ref() -> str | None:
     return os.path.join(ORACLE, "_ref", "libdtfe_ref.so")
 
 
+SHIM = os.path.join(PKG, "shim")
+
+
+def build_dropin(force: bool = False) -> str | None:
+    """The DTFE() drop-in (dtfe_b200/shim/dtfe_drop_in.cpp -> libdtfe_dropin.so),
+    compiled against the reference's own headers with the reference
+    Makefile's default macros (3-D, velocity, one scalar).  Only where the
+    reference tree exists; the boost headers its user_options.h includes come
+    from the harness stand-ins here (a real build uses the caller's boost).
+    Elsewhere the prebuilt library, if any, is used as is."""
+    src_dir = os.path.join(REFERENCE_TREE, "src")
+    if not os.path.isdir(src_dir):
+        return None
+    host, gpu = build_host(), build_gpu()
+    out = os.path.join(BUILD, "libdtfe_dropin.so")
+    src = os.path.join(SHIM, "dtfe_drop_in.cpp")
+    if force or _stale(out, [src, host, gpu] + _headers(INCLUDE)):
+        _run(["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-w",
+              "-DNO_DIM=3", "-DVELOCITY", "-DSCALAR", "-DNO_SCALARS=1",
+              "-I", INCLUDE, "-I", os.path.join(ORACLE, "refharness", "include"), "-I", src_dir,
+              "-o", out, src, "-L", BUILD, "-ldtfe_host", "-ldtfe_gpu", "-Wl,-rpath,$ORIGIN"])
+    return out
+
+
+def build_dropin_driver() -> str | None:
+    """Test driver of the drop-in (oracle/_ref/libdropin_driver.so): needs the
+    reference tree, like the harness it links."""
+    if not os.path.isdir(os.path.join(REFERENCE_TREE, "src")):
+        return None
+    _run(["make", "-s", "-C", ORACLE, "dropin", "REF=" + REFERENCE_TREE])
+    return os.path.join(ORACLE, "_ref", "libdropin_driver.so")
+
+
 def build_all(force: bool = False) -> None:
     build_host(force)
     build_gpu(force)
     build_oracle(force)
     build_ref()
+    if build_dropin(force):
+        build_dropin_driver()
 
 
 if __name__ == "__main__":

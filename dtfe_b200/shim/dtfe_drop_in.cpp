@@ -1,0 +1,207 @@
+// Drop-in replacement for the reference library's entry point
+//
+//   void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& samples,
+//             User_options& userOptions, Quantities* uQuantities, Quantities* aQuantities);
+//
+// (src/DTFE.h:36-40, src/DTFE.cpp:76-251).  It is compiled against the
+// caller's own reference headers (define.h, particle_data.h, user_options.h,
+// quantities.h and what they include), so the types are the caller's, and
+// it replaces src/DTFE.cpp in the caller's link.  The control flow of DTFE()
+// and DTFE_parallel() (average density, padding, periodic images, the
+// parallelGrid(omp_get_max_threads()) sub-box split, tessellation) runs on the
+// host through dtfe_plan_build (include/dtfe_host.h); vertex densities,
+// interpolation, the averaged methods, the velocity derivatives and the
+// NGP/CIC/TSC/SPH estimators run on the GPU through include/dtfe_gpu.h, and
+// the results are written straight into the caller's Quantities vectors
+// (cells x components, x slowest: the layout Quantities uses).
+//
+// As the reference: allParticles is cleared, userOptions.averageDensity is
+// set when it was negative (automatic), uQuantities receives the fields of
+// userOptions.uField (cell centres), aQuantities those of
+// userOptions.aField (method 2 or 3 averages, or the NGP/CIC/TSC/SPH grids).
+// Unlike the reference, failures throw std::runtime_error instead of calling
+// exit(), and options this path does not cover throw as well: user sampling
+// points, redshift cones, --region, --partition, random subsamples, Poisson
+// particles, explicit padding lengths, averaging method 1, scalar fields with
+// NGP/CIC/TSC.  The GPU is device 0 unless DTFE_GPU_DEVICE names another.
+
+#include <omp.h>
+
+#include <cstdlib>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "define.h"
+#include "particle_data.h"
+#include "quantities.h"
+#include "user_options.h"
+
+#include "dtfe_gpu.h"
+#include "dtfe_host.h"
+
+#if NO_DIM != 3
+#error "the GPU path is three-dimensional"
+#endif
+
+namespace {
+
+void check(int rc, const char* what) {
+  if (rc != DTFE_OK) {
+    const char* msg = dtfe_last_error();
+    throw std::runtime_error(std::string("DTFE (GPU): ") + what + ": " + (msg ? msg : "error"));
+  }
+}
+
+void unsupported(bool cond, const char* what) {
+  if (cond) throw std::runtime_error(std::string("DTFE (GPU): not supported: ") + what);
+}
+
+struct PlanGuard {
+  dtfe_plan p = nullptr;
+  ~PlanGuard() { dtfe_plan_release(p); }
+};
+
+struct HandleGuard {
+  dtfe_handle h = nullptr;
+  ~HandleGuard() { dtfe_gpu_destroy(h); }
+};
+
+template <class V>
+float* sized(V& vec, size_t G) {
+  vec.resize(G);
+  return reinterpret_cast<float*>(vec.data());
+}
+
+// Output pointers for the selected fields of one Quantities object.
+void outputs(const Field& f, Quantities* q, size_t G, float* out[DTFE_NUM_FIELDS], uint32_t* mask) {
+  for (int s = 0; s < DTFE_NUM_FIELDS; ++s) out[s] = nullptr;
+  *mask = 0;
+  auto set = [&](bool on, int slot, float* p) {
+    if (!on) return;
+    out[slot] = p;
+    *mask |= DTFE_FIELD_BIT(slot);
+  };
+  set(f.density, DTFE_DENSITY, f.density ? sized(q->density, G) : nullptr);
+  set(f.velocity, DTFE_VELOCITY, f.velocity ? sized(q->velocity, G) : nullptr);
+  set(f.velocity_gradient, DTFE_VELOCITY_GRADIENT, f.velocity_gradient ? sized(q->velocity_gradient, G) : nullptr);
+  set(f.velocity_divergence, DTFE_VELOCITY_DIVERGENCE,
+      f.velocity_divergence ? sized(q->velocity_divergence, G) : nullptr);
+  set(f.velocity_shear, DTFE_VELOCITY_SHEAR, f.velocity_shear ? sized(q->velocity_shear, G) : nullptr);
+  set(f.velocity_vorticity, DTFE_VELOCITY_VORTICITY, f.velocity_vorticity ? sized(q->velocity_vorticity, G) : nullptr);
+  set(f.velocity_std, DTFE_VELOCITY_STD, f.velocity_std ? sized(q->velocity_std, G) : nullptr);
+  set(f.scalar, DTFE_SCALAR, f.scalar ? sized(q->scalar, G) : nullptr);
+  set(f.scalar_gradient, DTFE_SCALAR_GRADIENT, f.scalar_gradient ? sized(q->scalar_gradient, G) : nullptr);
+}
+
+bool any(const Field& f) {
+  return f.density || f.velocity || f.velocity_gradient || f.velocity_divergence || f.velocity_shear ||
+         f.velocity_vorticity || f.velocity_std || f.scalar || f.scalar_gradient;
+}
+
+}  // namespace
+
+void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& samples, User_options& userOptions,
+          Quantities* uQuantities, Quantities* aQuantities) {
+  User_options& o = userOptions;
+  unsupported(!samples.empty() || o.userDefinedSampling, "user-defined sampling points");
+  unsupported(o.redshiftConeOn, "redshift-cone grids");
+  unsupported(o.regionOn, "--region");
+  unsupported(o.partitionOn, "--partition");
+  unsupported(o.randomSample >= Real(0.), "random subsamples");
+  unsupported(o.poisson != 0, "Poisson particles");
+  unsupported(o.paddingOn && !o.paddingLength.coords.empty() && o.paddingLength.coords[0] != Real(0.),
+              "explicit padding lengths");
+  unsupported(o.gridSize.size() != 3, "grids other than 3-D regular grids");
+  const bool dtfe = !(o.NGP || o.CIC || o.TSC || o.SPH);
+  unsupported(dtfe && any(o.aField) && o.method != 2 && o.method != 3, "averaging method 1");
+  unsupported(!dtfe && !o.SPH && (o.aField.scalar || o.aField.scalar_gradient), "scalar fields with NGP/CIC/TSC");
+
+  const int64_t n = (int64_t)allParticles->size();
+  std::vector<float> pos(3 * n), w(n), vel(3 * n), sc((size_t)noScalarComp * n);
+  for (int64_t i = 0; i < n; ++i) {
+    Particle_data& p = (*allParticles)[i];
+    for (int c = 0; c < 3; ++c) pos[3 * i + c] = p.pos[c];
+    w[i] = p.weight();
+#ifdef VELOCITY
+    for (int c = 0; c < 3; ++c) vel[3 * i + c] = p.velocity(c);
+#endif
+#ifdef SCALAR
+    for (size_t c = 0; c < noScalarComp; ++c) sc[noScalarComp * i + c] = p.scalar(c);
+#endif
+  }
+  allParticles->clear();  // the reference's contract (src/DTFE.cpp:75)
+#ifdef VELOCITY
+  const float* velp = vel.data();
+#else
+  const float* velp = nullptr;
+#endif
+#ifdef SCALAR
+  const float* scp = sc.data();
+  const int32_t S = (int32_t)noScalarComp;
+#else
+  const float* scp = nullptr;
+  const int32_t S = 0;
+#endif
+
+  float box[6];
+  for (int i = 0; i < 6; ++i) box[i] = o.boxCoordinates.coords[i];
+  const int32_t grid[3] = {(int32_t)o.gridSize[0], (int32_t)o.gridSize[1], (int32_t)o.gridSize[2]};
+  const size_t G = (size_t)grid[0] * grid[1] * grid[2];
+  if (o.averageDensity < Real(0.)) o.averageDensity = dtfe_average_density(w.data(), n);
+  const int kind = dtfe || o.SPH ? DTFE_PLAN_DTFE : (o.NGP ? DTFE_PLAN_NGP : (o.CIC ? DTFE_PLAN_CIC : DTFE_PLAN_TSC));
+
+  PlanGuard plan;
+  check(dtfe_plan_build(kind, pos.data(), w.data(), velp, scp, S, n, box, o.periodic ? 1 : 0, grid,
+                        omp_get_max_threads(), (float)o.paddingParticles, (double)o.averageDensity, &plan.p),
+        "planning");
+  dtfe_plan_view v;
+  check(dtfe_plan_get(plan.p, &v), "plan view");
+
+  dtfe_config cfg = {0, dtfe || o.SPH ? S : 0, 0, 0};
+  if (const char* d = std::getenv("DTFE_GPU_DEVICE")) cfg.device = std::atoi(d);
+  HandleGuard gpu;
+  check(dtfe_gpu_create(&cfg, &gpu.h), "create");
+
+  if (kind != DTFE_PLAN_DTFE) {
+    const int32_t k = kind == DTFE_PLAN_NGP ? DTFE_DEPOSIT_NGP : (kind == DTFE_PLAN_CIC ? DTFE_DEPOSIT_CIC : DTFE_DEPOSIT_TSC);
+    float* dens = o.aField.density ? sized(aQuantities->density, G) : nullptr;
+    float* velo = o.aField.velocity ? sized(aQuantities->velocity, G) : nullptr;
+    check(dtfe_gpu_deposit(gpu.h, k, v.dep_pos, v.dep_weight, velo ? v.dep_velocity : nullptr, v.n_particles,
+                           v.n_dep_boxes, v.dep_boxes, grid, v.rho_bar, dens ? dens : sized(aQuantities->density, G),
+                           velo),
+          "deposit");
+    if (!o.aField.density) aQuantities->density.clear();
+    return;
+  }
+
+  check(dtfe_gpu_upload(gpu.h, v.tet_v, v.tet_n, v.n_tets, v.xyz, v.weight, v.velocity, v.scalar, v.n_verts),
+        "upload");
+  check(dtfe_gpu_set_subboxes(gpu.h, v.n_boxes, v.boxes, v.xs, v.n_xs, v.ys, v.n_ys, v.zs, v.n_zs, grid),
+        "sub-boxes");
+  if (o.SPH) {
+    const bool wv = o.aField.velocity, ws = o.aField.scalar;
+    uint32_t f = DTFE_FIELD_BIT(DTFE_DENSITY) | (wv ? DTFE_FIELD_BIT(DTFE_VELOCITY) : 0u) |
+                 (ws ? DTFE_FIELD_BIT(DTFE_SCALAR) : 0u);
+    check(dtfe_gpu_sph(gpu.h, o.SPH_neighbors, f, o.extensive ? 1 : 0, v.rho_bar, sized(aQuantities->density, G),
+                       wv ? sized(aQuantities->velocity, G) : nullptr, ws ? sized(aQuantities->scalar, G) : nullptr),
+          "SPH");
+    if (!o.aField.density) aQuantities->density.clear();
+    return;
+  }
+  check(dtfe_gpu_vertex_density(gpu.h, v.rho_bar), "vertex density");
+  dtfe_status st;
+  if (any(o.uField)) {
+    float* out[DTFE_NUM_FIELDS];
+    dtfe_interp_opts io = {DTFE_METHOD_CENTRE, 1, 0, 0, 0};
+    outputs(o.uField, uQuantities, G, out, &io.fields);
+    check(dtfe_gpu_interpolate(gpu.h, &io, out, &st), "cell-centre interpolation");
+  }
+  if (any(o.aField)) {
+    float* out[DTFE_NUM_FIELDS];
+    dtfe_interp_opts io = {o.method == 2 ? DTFE_METHOD_MONTE_CARLO : DTFE_METHOD_EQUIDISTANT, o.noPoints,
+                           (uint64_t)o.randomSeed, 0, 0};
+    outputs(o.aField, aQuantities, G, out, &io.fields);
+    check(dtfe_gpu_interpolate(gpu.h, &io, out, &st), "averaged interpolation");
+  }
+}

@@ -1,0 +1,110 @@
+// Test driver of the DTFE() drop-in (dtfe_b200/shim) — TEST INFRASTRUCTURE
+// ONLY.  Builds the reference's own types (Particle_data, User_options with
+// the harness's default constructor, Quantities) from flat arrays, calls
+// DTFE() exactly as a reference caller would (src/DTFE.h:36-40), and copies
+// the Quantities vectors back out, so the Python tests can drive the drop-in.
+
+#include <omp.h>
+
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <string>
+#include <vector>
+
+#include "define.h"
+#include "particle_data.h"
+#include "quantities.h"
+#include "user_options.h"
+
+void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& samples, User_options& userOptions,
+          Quantities* uQuantities, Quantities* aQuantities);
+
+namespace {
+std::string g_error;
+
+void set_fields(Field& f, uint32_t m) {
+  f.density = m & 1u;
+  f.velocity = m & 2u;
+  f.velocity_gradient = m & 4u;
+  f.velocity_divergence = m & 8u;
+  f.velocity_shear = m & 16u;
+  f.velocity_vorticity = m & 32u;
+  f.velocity_std = m & 64u;
+  f.scalar = m & 128u;
+  f.scalar_gradient = m & 256u;
+}
+
+template <class V>
+void copy_out(const V& v, float* out, size_t G, size_t comps) {
+  if (out && v.size() == G) std::memcpy(out, v.data(), sizeof(float) * comps * G);
+}
+
+void copy_all(const Quantities& q, float* const* out, size_t G) {
+  if (!out) return;
+  copy_out(q.density, out[0], G, 1);
+  copy_out(q.velocity, out[1], G, 3);
+  copy_out(q.velocity_gradient, out[2], G, 9);
+  copy_out(q.velocity_divergence, out[3], G, 1);
+  copy_out(q.velocity_shear, out[4], G, 5);
+  copy_out(q.velocity_vorticity, out[5], G, 3);
+  copy_out(q.velocity_std, out[6], G, 1);
+  copy_out(q.scalar, out[7], G, noScalarComp);
+  copy_out(q.scalar_gradient, out[8], G, 3 * noScalarComp);
+}
+}  // namespace
+
+extern "C" {
+
+const char* dropin_error() { return g_error.c_str(); }
+
+// estimator: 0 DTFE, 1 NGP, 2 CIC, 3 TSC, 4 SPH.  u_fields / a_fields: bit
+// i = field slot i (density, velocity, gradient, divergence, shear,
+// vorticity, std, scalar, scalar gradient).  average_density < 0: automatic;
+// the value used comes back in *avg_out.  Returns 0, or 1 with
+// dropin_error() set when DTFE() threw.
+int dropin_run(int estimator, const float* pos, const float* w, const float* vel, const float* scal, int64_t n,
+               const float box[6], int periodic, const int32_t grid[3], double average_density, uint32_t u_fields,
+               uint32_t a_fields, int method, int n_points, uint64_t seed, int sph_neighbors, int n_threads,
+               float* const* u_out, float* const* a_out, double* avg_out, int64_t* particles_left) {
+  std::vector<Particle_data> p(n);
+  for (int64_t i = 0; i < n; ++i) {
+    for (int c = 0; c < 3; ++c) p[i].pos[c] = pos[3 * i + c];
+    p[i].weight() = w ? w[i] : 1.f;
+    for (int c = 0; c < 3; ++c) p[i].velocity(c) = vel ? vel[3 * i + c] : 0.f;
+    p[i].scalar(0) = scal ? scal[i] : 0.f;
+  }
+  User_options o;
+  o.gridSize.assign(grid, grid + 3);
+  o.boxCoordinates.coords.assign(box, box + 6);
+  o.periodic = periodic != 0;
+  o.averageDensity = (Real)average_density;
+  o.DTFE = estimator == 0;
+  o.NGP = estimator == 1;
+  o.CIC = estimator == 2;
+  o.TSC = estimator == 3;
+  o.SPH = estimator == 4;
+  o.SPH_neighbors = sph_neighbors;
+  o.method = method;
+  o.noPoints = n_points;
+  o.randomSeed = (size_t)seed;
+  set_fields(o.uField, u_fields);
+  set_fields(o.aField, a_fields);
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+  std::vector<Sample_point> samples;
+  Quantities uq, aq;
+  try {
+    DTFE(&p, samples, o, &uq, &aq);
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return 1;
+  }
+  const size_t G = (size_t)grid[0] * grid[1] * grid[2];
+  copy_all(uq, u_out, G);
+  copy_all(aq, a_out, G);
+  if (avg_out) *avg_out = (double)o.averageDensity;
+  if (particles_left) *particles_left = (int64_t)p.size();
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,63 @@
+"""ctypes access to the DTFE() drop-in's test driver (oracle/_ref/
+libdropin_driver.so, built where the reference's headers exist) — test
+infrastructure shared by test_dropin.py and test_gpu_dropin.py."""
+import ctypes as C
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PATH = os.path.join(ROOT, "oracle", "_ref", "libdropin_driver.so")
+NCOMP = [1, 3, 9, 1, 5, 3, 1, 1, 3]
+SLOTS = {"density": 0, "velocity": 1, "velocity_gradient": 2, "velocity_divergence": 3, "velocity_shear": 4,
+         "velocity_vorticity": 5, "velocity_std": 6, "scalar": 7, "scalar_gradient": 8}
+ESTIMATORS = {"DTFE": 0, "NGP": 1, "CIC": 2, "TSC": 3, "SPH": 4}
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(PATH)
+        vp = C.c_void_p
+        L.dropin_run.argtypes = [C.c_int, vp, vp, vp, vp, C.c_int64, vp, C.c_int, vp, C.c_double, C.c_uint32,
+                                 C.c_uint32, C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_int, vp, vp,
+                                 C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+        L.dropin_error.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def run(estimator, pos, w, vel, scal, grid, box=(0, 100, 0, 100, 0, 100), periodic=True, average_density=-1.0,
+        u_fields=(), a_fields=(), method=3, n_points=8, seed=0, sph_neighbors=32, n_threads=4):
+    """Calls DTFE() through the driver: (u dict, a dict, average density used,
+    particles left in the input vector).  Raises RuntimeError with DTFE()'s
+    message when it throws."""
+    pos = np.ascontiguousarray(pos, np.float32)
+    n = len(pos)
+    G = int(np.prod(grid))
+    arrs = []
+
+    def outs(fields):
+        d = {f: np.full((G, NCOMP[SLOTS[f]]), np.nan, np.float32) for f in fields}
+        arrs.append(d)
+        ptrs = (C.c_void_p * 9)(*[d[f].ctypes.data if f in d else None for f in SLOTS])
+        return d, ptrs, sum(1 << SLOTS[f] for f in fields)
+    ud, up, um = outs(u_fields)
+    ad, ap, am = outs(a_fields)
+    g = np.ascontiguousarray(grid, np.int32)
+    bx = np.ascontiguousarray(box, np.float32)
+    keep = [np.ascontiguousarray(a, np.float32) if a is not None else None for a in (w, vel, scal)]
+    avg = C.c_double()
+    left = C.c_int64()
+    rc = lib().dropin_run(ESTIMATORS[estimator], pos.ctypes.data, *[a.ctypes.data if a is not None else None
+                                                                    for a in keep], n, bx.ctypes.data, int(periodic),
+                          g.ctypes.data, float(average_density), um, am, method, n_points, seed, sph_neighbors,
+                          n_threads, up, ap, C.byref(avg), C.byref(left))
+    if rc:
+        raise RuntimeError(lib().dropin_error().decode())
+    return ud, ad, avg.value, left.value

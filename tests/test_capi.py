@@ -11,11 +11,11 @@ from dtfe_b200 import build
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def declared_functions():
+def declared_functions(header=None):
     names = set()
     inc = os.path.join(ROOT, "include")
     for f in os.listdir(inc):
-        if not f.endswith(".h"):
+        if not f.endswith(".h") or (header and f != header):
             continue
         text = open(os.path.join(inc, f)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
@@ -32,8 +32,28 @@ def test_header_declares_functions():
 
 def test_gpu_library_exports_all(built):
     lib = ctypes.CDLL(build.build_gpu())
-    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    missing = [n for n in declared_functions("dtfe_gpu.h") if not hasattr(lib, n)]
     assert not missing, missing
+
+
+def test_host_library_exports_all(built):
+    lib = ctypes.CDLL(build.build_host())
+    names = declared_functions("dtfe_host.h")
+    assert "dtfe_plan_build" in names and "dtfe_tessellate_batch" in names
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_dropin_exports_reference_entry_point(built):
+    """libdtfe_dropin.so defines the reference's C++ entry point
+    DTFE(std::vector<Particle_data>*, std::vector<Sample_point>&,
+    User_options&, Quantities*, Quantities*) (src/DTFE.h:36-40)."""
+    import subprocess
+    path = os.path.join(build.BUILD, "libdtfe_dropin.so")
+    if not os.path.exists(path):
+        pytest.skip("drop-in not built (needs the reference headers)")
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True).stdout
+    assert "_Z4DTFEPSt6vectorI13Particle_dataSaIS0_EERS_I12Sample_pointSaIS4_EER12User_optionsP10QuantitiesSB_" in out
 
 
 def test_create_without_device_fails_cleanly(built):

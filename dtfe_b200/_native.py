@@ -132,6 +132,9 @@ def host() -> C.CDLL:
         lib.dtfe_optimal_partition.argtypes = [vp, C.c_int64, vp, vp, vp, vp, vp]
         lib.dtfe_optimal_partition.restype = C.c_int
         lib.dtfe_axis_coords.argtypes = [C.c_float, C.c_float, C.c_int64, vp]
+        lib.dtfe_tets_pack.argtypes = [vp, vp, C.c_int64, vp]
+        lib.dtfe_tets_pack.restype = C.c_int64
+        lib.dtfe_tets_unpack.argtypes = [vp, C.c_int64, vp, vp]
         lib.dtfe_plan_build.argtypes = [C.c_int, vp, vp, vp, vp, C.c_int32, C.c_int64, vp, C.c_int, vp, C.c_int32,
                                         C.c_float, C.c_double, C.POINTER(C.c_void_p)]
         lib.dtfe_plan_get.argtypes = [C.c_void_p, C.POINTER(PlanView)]
@@ -150,6 +153,7 @@ def gpu() -> C.CDLL:
         lib.dtfe_gpu_create.argtypes = [C.POINTER(Config), C.POINTER(H)]
         lib.dtfe_gpu_destroy.argtypes = [H]
         lib.dtfe_gpu_upload.argtypes = [H, vp, vp, C.c_int64, vp, vp, vp, vp, C.c_int64]
+        lib.dtfe_gpu_upload_packed.argtypes = [H, vp, C.c_int64, vp, vp, vp, vp, C.c_int64]
         lib.dtfe_gpu_set_subboxes.argtypes = [H, C.c_int32, vp, vp, C.c_int64, vp, C.c_int64,
                                               vp, C.c_int64, vp]
         lib.dtfe_gpu_vertex_density.argtypes = [H, C.c_double]

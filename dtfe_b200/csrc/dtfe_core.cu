@@ -85,6 +85,61 @@ __device__ __forceinline__ int find_box(const int64_t* __restrict__ prefix, int 
 }
 
 // ---- vertex -> tetrahedron incidence (built once per upload) ------------
+// Decoder of the packed tessellation (dtfe_tets_pack, host_plan.cpp): one
+// thread per tetrahedron, one block per packing block of 256; the block scan
+// of escape counts gives every thread its first escaped value.
+constexpr int kPackBlock = 256;
+__global__ void __launch_bounds__(kPackBlock) k_unpack_tets(int64_t T, const int32_t* __restrict__ base,
+                                                            const int32_t* __restrict__ esc_off,
+                                                            const uint4* __restrict__ codes,
+                                                            const int32_t* __restrict__ esc, int4* __restrict__ tet_v,
+                                                            int4* __restrict__ tet_n) {
+  __shared__ int s_warp[kPackBlock / 32];
+  const int64_t t = blockIdx.x * (int64_t)kPackBlock + threadIdx.x;
+  const bool valid = t < T;
+  uint16_t c[8] = {0, 0, 0, 0, 0x8000, 0x8000, 0x8000, 0x8000};
+  if (valid) {
+    const uint4 q = __ldg(&codes[t]);
+    const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      c[2 * k] = (uint16_t)(w[k] & 0xFFFFu);
+      c[2 * k + 1] = (uint16_t)(w[k] >> 16);
+    }
+  }
+  int ne = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) ne += c[k] == 0xFFFF;
+#pragma unroll
+  for (int k = 4; k < 8; ++k) ne += (int16_t)c[k] == 32767;
+  // exclusive block scan of ne
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int inc = ne;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= d) inc += y;
+  }
+  if (lane == 31) s_warp[wid] = inc;
+  __syncthreads();
+  int before = 0;
+  for (int q = 0; q < wid; ++q) before += s_warp[q];
+  if (!valid) return;
+  const int32_t* e = esc + __ldg(&esc_off[blockIdx.x]) + before + inc - ne;
+  const int32_t b0 = __ldg(&base[blockIdx.x]);
+  int v[4], n[4];
+  v[0] = c[0] == 0xFFFF ? *e++ : b0 + (int)c[0];
+#pragma unroll
+  for (int k = 1; k < 4; ++k) v[k] = c[k] == 0xFFFF ? *e++ : v[0] + (int)c[k];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int d = (int16_t)c[4 + k];
+    n[k] = d == -32768 ? -1 : (d == 32767 ? *e++ : (int)(t + d));
+  }
+  tet_v[t] = make_int4(v[0], v[1], v[2], v[3]);
+  tet_n[t] = make_int4(n[0], n[1], n[2], n[3]);
+}
+
 __global__ void k_degree(int64_t T, const int4* __restrict__ tet_v, int* __restrict__ deg) {
   int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= T) return;
@@ -159,20 +214,54 @@ __global__ void k_fill_incidence(int64_t T, const int4* __restrict__ tet_v, cons
 
 // Ascending order inside every vertex's list: the FP64 volume sum then runs
 // in a fixed order (ascending tetrahedron id), independent of the atomics
-// that filled the lists.
-__global__ void k_sort_incidence(int64_t V, const int64_t* __restrict__ off, int* __restrict__ inc) {
-  int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (v >= V) return;
-  int64_t a = off[v], b = off[v + 1];
-  for (int64_t i = a + 1; i < b; ++i) {
-    int x = inc[i];
-    int64_t j = i - 1;
-    while (j >= a && inc[j] > x) {
-      inc[j + 1] = inc[j];
-      --j;
+// that filled the lists.  A warp loads the incidence lists of its 32
+// vertices (contiguous) into shared memory with coalesced loads, every lane
+// insertion-sorts its own list there, and the warp writes them back; warps
+// whose lists exceed the staging area sort in global memory, lane by lane.
+constexpr int kSortBlock = 256;
+constexpr int kSortChunk = 1536;  // incidences staged per warp (6 KB)
+__global__ void __launch_bounds__(kSortBlock) k_sort_incidence_staged(int64_t V, const int64_t* __restrict__ off,
+                                                                      int* __restrict__ inc) {
+  __shared__ int s_inc[kSortBlock / 32][kSortChunk];
+  const int lane = threadIdx.x & 31;
+  int* sv = s_inc[threadIdx.x >> 5];
+  const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t v0 = v - lane;
+  if (v0 >= V) return;
+  const int64_t vl = (v0 + 32 <= V) ? v0 + 32 : V;
+  const int64_t beg = off[v0], end = off[vl];
+  const bool mine = v < V;
+  if (end - beg > kSortChunk) {
+    if (!mine) return;
+    const int64_t a = off[v], b = off[v + 1];
+    for (int64_t i = a + 1; i < b; ++i) {
+      const int x = inc[i];
+      int64_t j = i - 1;
+      while (j >= a && inc[j] > x) {
+        inc[j + 1] = inc[j];
+        --j;
+      }
+      inc[j + 1] = x;
     }
-    inc[j + 1] = x;
+    return;
   }
+  const int n = (int)(end - beg);
+  for (int q = lane; q < n; q += 32) sv[q] = inc[beg + q];
+  __syncwarp();
+  if (mine) {
+    const int a = (int)(off[v] - beg), b = (int)(off[v + 1] - beg);
+    for (int i = a + 1; i < b; ++i) {
+      const int x = sv[i];
+      int j = i - 1;
+      while (j >= a && sv[j] > x) {
+        sv[j + 1] = sv[j];
+        --j;
+      }
+      sv[j + 1] = x;
+    }
+  }
+  __syncwarp();
+  for (int q = lane; q < n; q += 32) inc[beg + q] = sv[q];
 }
 
 // ---- per step ------------------------------------------------------------
@@ -900,10 +989,13 @@ int dtfe_gpu_synchronize(dtfe_handle h) {
   return DTFE_OK;
 }
 
-int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n, int64_t n_tets,
-                    const float* xyz, const float* w, const float* vel, const float* scal,
-                    int64_t n_verts) {
-  if (!h || !tet_v || !tet_n || !xyz || !w) return set_error(DTFE_ERR_ARG, "null argument");
+// Common body of the two uploads: tets(h) copies or decodes the
+// tetrahedron arrays into h->tet_v / h->tet_n on h->stream.
+extern "C++" {
+template <class TetCopy>
+static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const float* w, const float* vel,
+                       const float* scal, int64_t n_verts, TetCopy tets) {
+  if (!h || !xyz || !w) return set_error(DTFE_ERR_ARG, "null argument");
   if (n_tets < 0 || n_verts < 0 || n_tets > 0x7FFFFFFF || n_verts >= 0x7F7F7F7F)
     return set_error(DTFE_ERR_TOO_LARGE, "tetrahedron or vertex count beyond int32 indexing");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
@@ -920,10 +1012,7 @@ int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n, i
       (rc = dev_alloc(h, &h->scal, (size_t)n_verts * h->S)))
     return rc;
   cudaStream_t st = h->stream;
-  if (n_tets) {
-    DTFE_CUDA_TRY(cudaMemcpyAsync(h->tet_v, tet_v, 16 * n_tets, cudaMemcpyHostToDevice, st));
-    DTFE_CUDA_TRY(cudaMemcpyAsync(h->tet_n, tet_n, 16 * n_tets, cudaMemcpyHostToDevice, st));
-  }
+  if (n_tets && (rc = tets(h))) return rc;
   if (n_verts) {
     // positions and velocities arrive as 3 floats per vertex; pack them into
     // 16-byte records on the device
@@ -960,7 +1049,8 @@ int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n, i
     DTFE_CUDA_TRY(cudaMemsetAsync(h->scratch_i, 0, sizeof(int) * n_verts, st));
     if (n_tets) {
       k_fill_incidence<<<blocks_for(n_tets, 256), 256, 0, st>>>(n_tets, h->tet_v, h->inc_off, h->scratch_i, h->inc);
-      k_sort_incidence<<<blocks_for(n_verts, 256), 256, 0, st>>>(n_verts, h->inc_off, h->inc);
+      k_sort_incidence_staged<<<blocks_for(n_verts, kSortBlock), kSortBlock, 0, st>>>(n_verts, h->inc_off,
+                                                                                       h->inc);
     }
   }
   DTFE_CUDA_TRY(cudaGetLastError());
@@ -971,6 +1061,41 @@ int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n, i
   h->tet_c_valid = false;
   drop_graph(h);
   return DTFE_OK;
+}
+}  // extern "C++"
+
+int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n, int64_t n_tets,
+                    const float* xyz, const float* w, const float* vel, const float* scal,
+                    int64_t n_verts) {
+  if (!tet_v || !tet_n) return set_error(DTFE_ERR_ARG, "null argument");
+  return upload_impl(h, n_tets, xyz, w, vel, scal, n_verts, [&](dtfe_handle hh) -> int {
+    DTFE_CUDA_TRY(cudaMemcpyAsync(hh->tet_v, tet_v, 16 * n_tets, cudaMemcpyHostToDevice, hh->stream));
+    DTFE_CUDA_TRY(cudaMemcpyAsync(hh->tet_n, tet_n, 16 * n_tets, cudaMemcpyHostToDevice, hh->stream));
+    return DTFE_OK;
+  });
+}
+
+int dtfe_gpu_upload_packed(dtfe_handle h, const void* packed, int64_t packed_bytes, const float* xyz,
+                           const float* w, const float* vel, const float* scal, int64_t n_verts) {
+  // header: magic, T, n_blocks, n_escapes, offsets of base, escape offsets, codes, escapes
+  int64_t hd[8];
+  if (!packed || packed_bytes < (int64_t)sizeof(hd)) return set_error(DTFE_ERR_ARG, "null or short packed buffer");
+  std::memcpy(hd, packed, sizeof(hd));
+  const int64_t T = hd[1], nb = hd[2];
+  if (hd[0] != 0x31505444 || T < 0 || nb != (T + kPackBlock - 1) / kPackBlock || hd[7] + 4 * hd[3] > packed_bytes ||
+      hd[6] + 16 * T > packed_bytes)
+    return set_error(DTFE_ERR_ARG, "not a packed tessellation (dtfe_tets_pack)");
+  return upload_impl(h, T, xyz, w, vel, scal, n_verts, [&](dtfe_handle hh) -> int {
+    char* dev = nullptr;
+    DTFE_CUDA_TRY(cudaMallocAsync((void**)&dev, (size_t)packed_bytes, hh->stream));
+    DTFE_CUDA_TRY(cudaMemcpyAsync(dev, packed, (size_t)packed_bytes, cudaMemcpyHostToDevice, hh->stream));
+    k_unpack_tets<<<(unsigned)nb, kPackBlock, 0, hh->stream>>>(
+        T, (const int32_t*)(dev + hd[4]), (const int32_t*)(dev + hd[5]), (const uint4*)(dev + hd[6]),
+        (const int32_t*)(dev + hd[7]), hh->tet_v, hh->tet_n);
+    DTFE_CUDA_TRY(cudaGetLastError());
+    DTFE_CUDA_TRY(cudaFreeAsync(dev, hh->stream));
+    return DTFE_OK;
+  });
 }
 
 int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* boxes, const float* xs,

@@ -56,6 +56,12 @@ class DeviceDTFE:
             self.h, N.ptr(plan.tet_v), N.ptr(plan.tet_n), plan.n_tets, N.ptr(plan.xyz),
             N.ptr(plan.weight), N.ptr(plan.velocity), N.ptr(plan.scalar), plan.n_verts))
 
+    def upload_packed(self, plan, packed: np.ndarray) -> None:
+        """Upload with the tetrahedra in packed form (plan.pack_tets)."""
+        N.check(self.lib.dtfe_gpu_upload_packed(
+            self.h, packed.ctypes.data, packed.nbytes, N.ptr(plan.xyz), N.ptr(plan.weight), N.ptr(plan.velocity),
+            N.ptr(plan.scalar), plan.n_verts))
+
     def set_subboxes(self, plan) -> None:
         grid = np.asarray(plan.grid, np.int32)
         N.check(self.lib.dtfe_gpu_set_subboxes(

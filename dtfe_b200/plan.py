@@ -464,3 +464,26 @@ def native_plan(kind: str, pos, weight, velocity=None, scalar=None, grid=(64, 64
                            src=_view_array(v.dep_src, np.int64, (n,)))
     finally:
         lib.dtfe_plan_release(h)
+
+
+def pack_tets(tet_v: np.ndarray, tet_n: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
+    """The packed form of a tessellation (dtfe_tets_pack): uint8 bytes,
+    about 16 per tetrahedron.  ``out`` (e.g. pinned memory) is used when it
+    is large enough."""
+    tv = np.ascontiguousarray(tet_v, np.int32)
+    tn = np.ascontiguousarray(tet_n, np.int32)
+    lib = N.host()
+    n = int(lib.dtfe_tets_pack(tv.ctypes.data, tn.ctypes.data, len(tv), None))
+    if n < 0:
+        raise ValueError("cannot pack these arrays")
+    buf = out[:n] if out is not None and out.nbytes >= n else np.empty(n, np.uint8)
+    lib.dtfe_tets_pack(tv.ctypes.data, tn.ctypes.data, len(tv), buf.ctypes.data)
+    return buf
+
+
+def unpack_tets(packed: np.ndarray, n_tets: int):
+    tv = np.empty((n_tets, 4), np.int32)
+    tn = np.empty((n_tets, 4), np.int32)
+    if N.host().dtfe_tets_unpack(packed.ctypes.data, packed.nbytes, tv.ctypes.data, tn.ctypes.data):
+        raise ValueError("malformed packed tessellation")
+    return tv, tn

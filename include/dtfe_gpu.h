@@ -138,6 +138,12 @@ const char* dtfe_last_error(void);
 int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n,
                     int64_t n_tets, const float* xyz, const float* w,
                     const float* vel, const float* scal, int64_t n_verts);
+/* Same, with the tetrahedra in the packed form of dtfe_tets_pack
+ * (include/dtfe_host.h): about 16 bytes per tetrahedron instead of 32 cross
+ * to the device, where a kernel restores tet_v/tet_n.  No counterpart in the
+ * reference (its tessellation never leaves the host). */
+int dtfe_gpu_upload_packed(dtfe_handle h, const void* packed, int64_t packed_bytes, const float* xyz,
+                           const float* w, const float* vel, const float* scal, int64_t n_verts);
 
 /* Describe the sub-boxes and the main grid.  xs/ys/zs hold the sample
  * coordinates of every tile along each axis (the reference's running

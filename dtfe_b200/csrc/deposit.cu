@@ -447,7 +447,8 @@ extern "C" int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xy
   const size_t bytes_part = sizeof(float4) * 2 * (size_t)n;
   const size_t bytes_box = sizeof(DepBox) * n_boxes + 2 * sizeof(int64_t) * (n_boxes + 1);
   const size_t bytes_acc = sizeof(unsigned long long) * 4 * (size_t)G;
-  const size_t need = bytes_part + bytes_box + bytes_acc + 1024;
+  const size_t bytes_tmp = sizeof(float) * 4 * (size_t)n;  // 3-float records as they arrive
+  const size_t need = bytes_part + bytes_box + bytes_acc + bytes_tmp + 2048;
   if (*scratch_bytes < need) {
     if (*scratch) cudaFree(*scratch);
     *scratch = nullptr;
@@ -466,11 +467,9 @@ extern "C" int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xy
   DepBox* d_boxes = (DepBox*)(base + o);
   int64_t* d_prefix = (int64_t*)(base + o + sizeof(DepBox) * n_boxes);
   int64_t* d_tprefix = d_prefix + (n_boxes + 1);
+  float* tmp = (float*)(base + align(o + bytes_box));
   cudaError_t e;
-  float* tmp = nullptr;
   if (n > 0) {
-    if ((e = cudaMallocAsync((void**)&tmp, sizeof(float) * 4 * (size_t)n, st)) != cudaSuccess)
-      return dtfe_internal_set_error(DTFE_ERR_ALLOC, cudaGetErrorString(e));
     float* t3 = tmp;
     float* t1 = tmp + 3 * n;
     cudaMemcpyAsync(t3, xyz, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, st);
@@ -480,7 +479,6 @@ extern "C" int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xy
       cudaMemcpyAsync(t3, vel, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, st);
       k_pack4<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, t3, nullptr, d_vel);
     }
-    cudaFreeAsync(tmp, st);
   }
   cudaMemcpyAsync(d_boxes, hb.data(), sizeof(DepBox) * n_boxes, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(d_prefix, prefix.data(), sizeof(int64_t) * (n_boxes + 1), cudaMemcpyHostToDevice, st);

@@ -803,6 +803,7 @@ struct dtfe_gpu_s {
   double *g_rho = nullptr, *g_x = nullptr, *g_v = nullptr, *g_S = nullptr, *g_m = nullptr, *vbar = nullptr;
   float* adj_a = nullptr;         // device copies of host loss weights
   cudaGraphExec_t step_graph = nullptr;  // captured step (dtfe_gpu_graph_build)
+  char* upload_buf = nullptr;     // staging of packed tetrahedra and 3-float vertex records
   void* sph_scratch = nullptr;    // SPH cell grids, neighbour bookkeeping, FP64 sums
   size_t sph_bytes = 0;
   float* sph_out = nullptr;       // host-output SPH staging
@@ -973,7 +974,7 @@ int dtfe_gpu_destroy(dtfe_handle h) {
     if (h->out_buf[i]) cudaFree(h->out_buf[i]);
   if (h->dep_scratch) cudaFree(h->dep_scratch);
   for (void* p : {(void*)h->g_rho, (void*)h->g_x, (void*)h->g_v, (void*)h->g_S, (void*)h->g_m, (void*)h->vbar,
-                  (void*)h->adj_a, h->sph_scratch, (void*)h->sph_out})
+                  (void*)h->adj_a, h->sph_scratch, (void*)h->sph_out, (void*)h->upload_buf})
     if (p) cudaFree(p);
   if (h->dep_out) cudaFree(h->dep_out);
   cudaStreamDestroy(h->stream);
@@ -1016,8 +1017,10 @@ static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const fl
   if (n_verts) {
     // positions and velocities arrive as 3 floats per vertex; pack them into
     // 16-byte records on the device
-    float* tmp = nullptr;
-    DTFE_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(float) * 3 * n_verts, st));
+    // staging kept in the handle (an allocation per upload would map and
+    // unmap device memory every time)
+    if ((rc = dev_alloc(h, &h->upload_buf, sizeof(float) * 3 * n_verts))) return rc;
+    float* tmp = (float*)h->upload_buf;
     DTFE_CUDA_TRY(cudaMemcpyAsync(tmp, xyz, sizeof(float) * 3 * n_verts, cudaMemcpyHostToDevice, st));
     k_pack_xyz<<<blocks_for(n_verts, 256), 256, 0, st>>>(n_verts, tmp, h->posd, 0.f);
     if (vel) {
@@ -1026,7 +1029,6 @@ static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const fl
     } else {
       DTFE_CUDA_TRY(cudaMemsetAsync(h->vel4, 0, sizeof(float4) * n_verts, st));
     }
-    DTFE_CUDA_TRY(cudaFreeAsync(tmp, st));
     DTFE_CUDA_TRY(cudaMemcpyAsync(h->w, w, sizeof(float) * n_verts, cudaMemcpyHostToDevice, st));
     if (h->S > 0) {
       if (scal)
@@ -1086,14 +1088,14 @@ int dtfe_gpu_upload_packed(dtfe_handle h, const void* packed, int64_t packed_byt
       hd[6] + 16 * T > packed_bytes)
     return set_error(DTFE_ERR_ARG, "not a packed tessellation (dtfe_tets_pack)");
   return upload_impl(h, T, xyz, w, vel, scal, n_verts, [&](dtfe_handle hh) -> int {
-    char* dev = nullptr;
-    DTFE_CUDA_TRY(cudaMallocAsync((void**)&dev, (size_t)packed_bytes, hh->stream));
+    int rc2 = dev_alloc(hh, &hh->upload_buf, (size_t)packed_bytes);
+    if (rc2) return rc2;
+    char* dev = hh->upload_buf;
     DTFE_CUDA_TRY(cudaMemcpyAsync(dev, packed, (size_t)packed_bytes, cudaMemcpyHostToDevice, hh->stream));
     k_unpack_tets<<<(unsigned)nb, kPackBlock, 0, hh->stream>>>(
         T, (const int32_t*)(dev + hd[4]), (const int32_t*)(dev + hd[5]), (const uint4*)(dev + hd[6]),
         (const int32_t*)(dev + hd[7]), hh->tet_v, hh->tet_n);
     DTFE_CUDA_TRY(cudaGetLastError());
-    DTFE_CUDA_TRY(cudaFreeAsync(dev, hh->stream));
     return DTFE_OK;
   });
 }

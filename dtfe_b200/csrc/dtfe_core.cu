@@ -1580,13 +1580,13 @@ int dtfe_gpu_read_status(dtfe_handle h, dtfe_status* status) {
   return read_status(h, status);
 }
 
-int dtfe_gpu_interpolate(dtfe_handle h, const dtfe_interp_opts* opts, float* const out[DTFE_NUM_FIELDS],
-                         dtfe_status* st) {
-  if (!h || !opts || !out) return set_error(DTFE_ERR_ARG, "null argument");
-  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+// Device buffers for host-output calls: one per requested field, zeroed
+// (cells outside every tile keep zeros, as the reference's reserved vectors).
+static int host_out_buffers(dtfe_handle h, const dtfe_interp_opts* opts, float* const out[DTFE_NUM_FIELDS],
+                            float* dev[DTFE_NUM_FIELDS]) {
   int64_t G = (int64_t)h->grid[0] * h->grid[1] * h->grid[2];
-  float* dev[DTFE_NUM_FIELDS] = {};
   for (int s = 0; s < DTFE_NUM_FIELDS; ++s) {
+    dev[s] = nullptr;
     if (!(opts->fields >> s & 1u)) continue;
     if (!out[s]) return set_error(DTFE_ERR_ARG, "missing output buffer");
     size_t need = (size_t)G * field_components(s, h->S);
@@ -1596,17 +1596,38 @@ int dtfe_gpu_interpolate(dtfe_handle h, const dtfe_interp_opts* opts, float* con
       h->out_cap[s] = need;
     }
     dev[s] = h->out_buf[s];
-    // cells outside every tile keep zeros, as the reference's reserved vectors
     DTFE_CUDA_TRY(cudaMemsetAsync(dev[s], 0, need * sizeof(float), h->stream));
   }
-  int rc = interpolate_impl(h, opts, dev, st);
-  if (rc) return rc;
+  return DTFE_OK;
+}
+
+static int copy_out(dtfe_handle h, float* const out[DTFE_NUM_FIELDS], float* const dev[DTFE_NUM_FIELDS]) {
+  int64_t G = (int64_t)h->grid[0] * h->grid[1] * h->grid[2];
   for (int s = 0; s < DTFE_NUM_FIELDS; ++s) {
     if (!dev[s]) continue;
     size_t need = (size_t)G * field_components(s, h->S);
     DTFE_CUDA_TRY(cudaMemcpyAsync(out[s], dev[s], need * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
   }
+  return DTFE_OK;
+}
+
+int dtfe_gpu_interpolate(dtfe_handle h, const dtfe_interp_opts* opts, float* const out[DTFE_NUM_FIELDS],
+                         dtfe_status* st) {
+  if (!h || !opts || !out) return set_error(DTFE_ERR_ARG, "null argument");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  float* dev[DTFE_NUM_FIELDS];
+  int rc = host_out_buffers(h, opts, out, dev);
+  if (rc || (rc = interpolate_impl(h, opts, dev, st)) || (rc = copy_out(h, out, dev))) return rc;
   DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return DTFE_OK;
+}
+
+int dtfe_gpu_interpolate_async(dtfe_handle h, const dtfe_interp_opts* opts, float* const out[DTFE_NUM_FIELDS]) {
+  if (!h || !opts || !out) return set_error(DTFE_ERR_ARG, "null argument");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  float* dev[DTFE_NUM_FIELDS];
+  int rc = host_out_buffers(h, opts, out, dev);
+  if (rc || (rc = interp_enqueue(h, opts, dev)) || (rc = copy_out(h, out, dev))) return rc;
   return DTFE_OK;
 }
 

@@ -103,6 +103,18 @@ class DeviceDTFE:
         self.last_status = st.as_dict()
         return res
 
+    def interpolate_async(self, fields, out: dict, method: int = 0, n_samples: int = 1, seed: int = 0,
+                          fix: bool = False) -> None:
+        """Queues the interpolation and the copies into the host arrays of
+        ``out`` (field -> float32 array, best pinned); valid after
+        synchronize()."""
+        outs = [None] * N.NUM_FIELDS
+        for f in fields:
+            outs[N.FIELD_SLOTS[f]] = N.ptr(out[f])
+        optr = (C.c_void_p * N.NUM_FIELDS)(*outs)
+        o = self._opts(fields, method, n_samples, seed, fix)
+        N.check(self.lib.dtfe_gpu_interpolate_async(self.h, C.byref(o), optr))
+
     def interpolate_dev(self, fields, outs_dev: dict, method: int = 0, n_samples: int = 1, seed: int = 0,
                         fix: bool = False) -> dict:
         """Device outputs: dict field -> device pointer or tensor."""

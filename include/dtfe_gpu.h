@@ -166,6 +166,12 @@ int dtfe_gpu_interpolate(dtfe_handle h, const dtfe_interp_opts* opts,
 /* Same, writing into device buffers. */
 int dtfe_gpu_interpolate_dev(dtfe_handle h, const dtfe_interp_opts* opts,
                              float* const out_dev[DTFE_NUM_FIELDS], dtfe_status* st);
+/* Same as dtfe_gpu_interpolate, but returns once the work and the copies
+ * into the host buffers are queued on the handle's stream: the buffers (best
+ * pinned) are valid after dtfe_gpu_synchronize; the walk counters come from
+ * dtfe_gpu_read_status.  Lets a caller overlap one handle's transfers with
+ * another's (double buffering across snapshots). */
+int dtfe_gpu_interpolate_async(dtfe_handle h, const dtfe_interp_opts* opts, float* const out[DTFE_NUM_FIELDS]);
 
 /* ---- NGP / CIC / TSC comparison estimators ------------------------------
  * One record per region (the reference deposits per sub-box region, with

@@ -31,3 +31,40 @@ def test_packed_upload_identical(gpu_built):
     for f in FIELDS:
         assert np.array_equal(out[0][0][f], out[1][0][f]), f
     assert np.array_equal(out[0][1], out[1][1])
+
+
+def test_async_double_buffered_matches_sync(gpu_built):
+    """Two handles used alternately with dtfe_gpu_interpolate_async (the
+    double-buffered e2e loop) give the synchronous call's fields."""
+    from dtfe_b200.device import DeviceDTFE
+    pos, psi = S.zeldovich_lattice(16, 100.0, 1.0, seed=13)
+    vel = (50 * psi).astype(np.float32)
+    plan = P.make_plan(pos, np.ones(len(pos), np.float32), vel, None, grid=(16, 16, 16), n_threads=4)
+    packed = P.pack_tets(plan.tet_v, plan.tet_n)
+    G = int(np.prod(plan.grid))
+    nc = {"density": 1, "velocity": 3, "velocity_gradient": 9, "velocity_divergence": 1}
+    with DeviceDTFE(0) as ref_dev:
+        ref_dev.load(plan)
+        ref_dev.vertex_density(plan.rho_bar)
+        ref = ref_dev.interpolate(FIELDS, method=0)
+    devs = [DeviceDTFE(0), DeviceDTFE(0)]
+    outs = [{f: np.full((G, nc[f]), np.nan, np.float32) for f in FIELDS} for _ in range(2)]
+    try:
+        for d in devs:
+            d.upload_packed(plan, packed)
+            d.set_subboxes(plan)
+        for step in range(4):
+            d = devs[step % 2]
+            d.synchronize()
+            d.upload_packed(plan, packed)
+            d.vertex_density(plan.rho_bar)
+            d.interpolate_async(FIELDS, outs[step % 2], method=0)
+        for d in devs:
+            d.synchronize()
+        for o in outs:
+            for f in FIELDS:
+                assert np.array_equal(o[f].reshape(ref[f].shape), ref[f]), f
+        assert devs[0].read_status()["n_samples_located"] == G
+    finally:
+        for d in devs:
+            d.close()

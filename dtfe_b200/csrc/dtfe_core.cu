@@ -2,24 +2,25 @@
 // include/dtfe_gpu.h.
 //
 // Pipeline (all on the handle's stream):
-//   upload             tessellation and vertex data; k_hull_marks flags the
-//                      vertices of hull faces once (a topological property of
-//                      the tessellation: the reference's infinite cells)
-//   k_volume_bins      per step, one thread per tetrahedron: signed volume in
-//                      FP64 scattered to its four vertices and, per grid cell,
-//                      the lowest tetrahedron whose centroid lies in the cell
-//                      (the walk seeds).  Both reductions are first combined
-//                      in shared-memory hash tables per block (tetrahedra are
-//                      Morton-sorted, so a block touches few vertices and
-//                      cells) and then flushed with one global atomic each
-//   k_vertex_density   rho_v = w (D+1)/(rho_bar sum V), 0 on the hull
-//                      (vertexDensity, triangulation.cpp:200-279)
-//   k_interpolate      one thread per grid cell: walk from the cell's seed to
-//                      the cell centre, evaluate (or average over n points,
-//                      each walked from the centre's tetrahedron as in
-//                      averaged_interpolation_2.cc:123,145), derive
-//                      divergence/shear/vorticity in the epilogue, write every
-//                      requested field once.
+//   upload              tessellation (plain or packed) and vertex data;
+//                       k_hull_marks flags the vertices of hull faces (the
+//                       reference's infinite cells); incidence lists per
+//                       vertex (k_degree, scan, k_fill_incidence, sorted by
+//                       k_sort_incidence_staged)
+//   k_tet_volume_bins   per step, one thread per tetrahedron: signed FP64
+//                       volume, and per grid cell the walk seed: the
+//                       tetrahedron whose centroid is nearest the cell's
+//                       sample point among those whose centroid lies in it
+//   k_vertex_density    rho_v = w (D+1)/(rho_bar sum V), 0 on the hull
+//                       (vertexDensity, triangulation.cpp:200-279), summed
+//                       over the incidence list in ascending tetrahedron order
+//   k_locate_cells      one thread per cell: walk from the seed to the cell
+//                       centre (canonical tetrahedron, bit-exact location)
+//   k_eval_centre       the reference's per-sample arithmetic and the
+//                       divergence/shear/vorticity epilogue, every requested
+//                       field written once
+//   k_average           methods 2/3: n points per cell, each walked from the
+//                       centre's tetrahedron (averaged_interpolation_2.cc:123,145)
 
 #include <cuda_runtime.h>
 
@@ -52,7 +53,7 @@ int set_error(int code, const std::string& msg) {
       return set_error(DTFE_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
   } while (0)
 
-constexpr int kEmptyBin = 0x7F7F7F7F;  // memset(0x7F) value; above any vertex id
+constexpr int64_t kMaxCells = 0x7FFFFFFF;  // cell keys are int32
 enum { CNT_LOCATED, CNT_OUTSIDE, CNT_FAIL, CNT_STEPS, CNT_EXACT, CNT_TIES, CNT_N };
 
 // ---------------------------------------------------------------------------
@@ -268,19 +269,24 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_incidence_staged(int64_t V,
 constexpr int kVolBlock = 256;
 
 // Signed volume of every tetrahedron (FP64, streamed out once) and, when
-// DO_BINS, the walk seeds: per grid cell the lowest tetrahedron whose
-// centroid lies in it.  Tetrahedra are Morton-sorted, so neighbouring lanes
-// often bin to the same cell; within such a run of lanes the first lane holds
-// the lowest tetrahedron id and alone issues the global atomicMin.  The seed
-// only starts the walk (its result does not depend on the seed), so the
-// centroid's cell is computed with a reciprocal instead of a division.
+// DO_BINS, the walk seeds: per grid cell, among the tetrahedra whose
+// centroid lies in the cell, the one whose centroid is nearest the cell's
+// sample point (squared distance in float, ties to the lower id), kept as
+// (distance bits << 32 | id) by a 64-bit atomicMin.  Tetrahedra are
+// Morton-sorted, so neighbouring lanes often bin to the same cell: a
+// segmented minimum over each run of equal cells in the warp leaves one
+// atomic per run.  The seed only starts the walk (the located tetrahedron
+// does not depend on it), so the centroid's cell uses a reciprocal.
+constexpr unsigned long long kEmptySeed = ~0ull;
 template <bool DO_BINS>
 __global__ void __launch_bounds__(kVolBlock) k_tet_volume_bins(
     int64_t T, const int4* __restrict__ tet_v, const float4* __restrict__ posd, double* __restrict__ vol,
     const dtfe_subbox* __restrict__ boxes, const int64_t* __restrict__ tprefix,
-    const int64_t* __restrict__ bin_offset, int K, int* __restrict__ bins) {
+    const int64_t* __restrict__ bin_offset, int K, const float* __restrict__ xs, const float* __restrict__ ys,
+    const float* __restrict__ zs, unsigned long long* __restrict__ bins) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   int key = -1;
+  unsigned long long val = kEmptySeed;
   if (t < T) {
     int4 q = __ldg(&tet_v[t]);
     int v[4] = {q.x, q.y, q.z, q.w};
@@ -297,23 +303,38 @@ __global__ void __launch_bounds__(kVolBlock) k_tet_volume_bins(
       const int b = find_box(tprefix, K, t);
       const dtfe_subbox& B = boxes[b];
       int idx[3];
+      float cen[3];
       bool inside = true;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const float cen = 0.25f * ((X[0][c] + X[1][c]) + (X[2][c] + X[3][c]));
-        const float f = floorf((cen - __ldg(&B.lo[c])) * __frcp_rn(__ldg(&B.dx[c])));
+        cen[c] = 0.25f * ((X[0][c] + X[1][c]) + (X[2][c] + X[3][c]));
+        const float f = floorf((cen[c] - __ldg(&B.lo[c])) * __frcp_rn(__ldg(&B.dx[c])));
         const int n = __ldg(&B.tile_dims[c]);
         inside = inside && (f >= 0.f && f < (float)n);
         idx[c] = inside ? (int)f : 0;
       }
-      if (inside)
+      if (inside) {
         key = (int)(__ldg(&bin_offset[b]) +
                     ((int64_t)idx[0] * __ldg(&B.tile_dims[1]) + idx[1]) * __ldg(&B.tile_dims[2]) + idx[2]);
+        const float dxs = cen[0] - __ldg(&xs[B.coord_offset[0] + idx[0]]);
+        const float dys = cen[1] - __ldg(&ys[B.coord_offset[1] + idx[1]]);
+        const float dzs = cen[2] - __ldg(&zs[B.coord_offset[2] + idx[2]]);
+        const float d2 = dxs * dxs + dys * dys + dzs * dzs;
+        val = ((unsigned long long)__float_as_uint(d2) << 32) | (unsigned)t;
+      }
     }
   }
   if (DO_BINS) {
+    // segmented minimum over runs of equal keys; the run's first lane issues
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long ov = __shfl_down_sync(0xffffffffu, val, o);
+      const int ok = __shfl_down_sync(0xffffffffu, key, o);
+      if (lane + o < 32 && ok == key && ov < val) val = ov;
+    }
     const int prev = __shfl_up_sync(0xffffffffu, key, 1);
-    if (key >= 0 && ((threadIdx.x & 31) == 0 || prev != key)) atomicMin(&bins[key], (int)t);
+    if (key >= 0 && (lane == 0 || prev != key)) atomicMin(&bins[key], val);
   }
 }
 
@@ -366,7 +387,7 @@ struct InterpParams {
   const float4* posd;
   const float4* vel4;
   const float* scal;
-  const int* bins;
+  const unsigned long long* bins;  // walk seeds (distance bits << 32 | tetrahedron)
   const dtfe_subbox* boxes;
   const int64_t* tile_prefix;
   const int64_t* bin_offset;
@@ -450,16 +471,17 @@ __device__ __forceinline__ void fold_counters(const InterpParams& P, unsigned n_
 // neighbouring cells with one, else the sub-box's first tetrahedron.
 __device__ __forceinline__ int seed_of(const InterpParams& P, const SampleCell& c) {
   const dtfe_subbox& B = P.boxes[c.b];
-  const int* bins = P.bins + __ldg(&P.bin_offset[c.b]);
-  int t0 = __ldg(&bins[c.local]);
-  if (t0 >= kEmptyBin) {
+  const unsigned long long* bins = P.bins + __ldg(&P.bin_offset[c.b]);
+  unsigned long long s0 = __ldg(&bins[c.local]);
+  if (s0 == kEmptySeed) {
     const int nx = B.tile_dims[0], ny = B.tile_dims[1], nz = B.tile_dims[2];
-    for (int q = 0; q < 26 && t0 >= kEmptyBin; ++q) {
+    for (int q = 0; q < 26 && s0 == kEmptySeed; ++q) {
       const int ii = c.i + c_nbr[q][0], jj = c.j + c_nbr[q][1], kk = c.k + c_nbr[q][2];
       if (ii < 0 || jj < 0 || kk < 0 || ii >= nx || jj >= ny || kk >= nz) continue;
-      t0 = __ldg(&bins[((int64_t)ii * ny + jj) * nz + kk]);
+      s0 = __ldg(&bins[((int64_t)ii * ny + jj) * nz + kk]);
     }
   }
+  int t0 = s0 == kEmptySeed ? -1 : (int)(unsigned)(s0 & 0xFFFFFFFFull);
   if (t0 < B.tet_offset || t0 >= B.tet_offset + B.n_tets) t0 = (int)B.tet_offset;
   return t0;
 }
@@ -778,7 +800,7 @@ struct dtfe_gpu_s {
   int64_t* tile_prefix = nullptr;
   int64_t* tet_prefix = nullptr;  // K+1 tetrahedron range starts
   int64_t* bin_offset = nullptr;
-  int* bins = nullptr;
+  unsigned long long* bins = nullptr;
   int* tet_c = nullptr;   // located tetrahedron of every cell centre
   int loc_variant = 0;    // launch variants (dtfe_gpu_autotune)
   int eval_variant = 0;
@@ -861,10 +883,11 @@ void drop_graph(dtfe_handle h) {
 
 int prepare_bins(dtfe_handle h) {
   if (h->bins_ready) return DTFE_OK;
-  DTFE_CUDA_TRY(cudaMemsetAsync(h->bins, 0x7F, sizeof(int) * h->n_cells, h->stream));
+  DTFE_CUDA_TRY(cudaMemsetAsync(h->bins, 0xFF, sizeof(unsigned long long) * h->n_cells, h->stream));
   if (h->T > 0)
     k_tet_volume_bins<true><<<blocks_for(h->T, kVolBlock), kVolBlock, 0, h->stream>>>(
-        h->T, h->tet_v, h->posd, h->vol, h->boxes, h->tet_prefix, h->bin_offset, h->K, h->bins);
+        h->T, h->tet_v, h->posd, h->vol, h->boxes, h->tet_prefix, h->bin_offset, h->K, h->xs, h->ys, h->zs,
+        h->bins);
   DTFE_CUDA_TRY(cudaGetLastError());
   h->bins_ready = true;
   return DTFE_OK;
@@ -1129,7 +1152,7 @@ int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* box
   }
   tprefix[n_boxes] = cells;
   tetpre[n_boxes] = boxes[n_boxes - 1].tet_offset + boxes[n_boxes - 1].n_tets;
-  if (cells >= (int64_t)kEmptyBin) return set_error(DTFE_ERR_TOO_LARGE, "more than 2^31 grid cells");
+  if (cells >= kMaxCells) return set_error(DTFE_ERR_TOO_LARGE, "more than 2^31 grid cells");
   int rc;
   if ((rc = dev_alloc(h, &h->boxes, n_boxes)) || (rc = dev_alloc(h, &h->tile_prefix, n_boxes + 1)) ||
       (rc = dev_alloc(h, &h->tet_prefix, n_boxes + 1)) || (rc = dev_alloc(h, &h->bin_offset, n_boxes)) ||
@@ -1163,14 +1186,16 @@ int dtfe_gpu_vertex_density(dtfe_handle h, double rho_bar) {
   if (h->V == 0) return set_error(DTFE_ERR_STATE, "nothing uploaded");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
   cudaStream_t st = h->stream;
-  if (h->K > 0) DTFE_CUDA_TRY(cudaMemsetAsync(h->bins, 0x7F, sizeof(int) * h->n_cells, st));
+  if (h->K > 0) DTFE_CUDA_TRY(cudaMemsetAsync(h->bins, 0xFF, sizeof(unsigned long long) * h->n_cells, st));
   if (h->T > 0) {
     if (h->K > 0)
       k_tet_volume_bins<true><<<blocks_for(h->T, kVolBlock), kVolBlock, 0, st>>>(
-          h->T, h->tet_v, h->posd, h->vol, h->boxes, h->tet_prefix, h->bin_offset, h->K, h->bins);
+          h->T, h->tet_v, h->posd, h->vol, h->boxes, h->tet_prefix, h->bin_offset, h->K, h->xs, h->ys, h->zs,
+          h->bins);
     else
       k_tet_volume_bins<false><<<blocks_for(h->T, kVolBlock), kVolBlock, 0, st>>>(
-          h->T, h->tet_v, h->posd, h->vol, h->boxes, h->tet_prefix, h->bin_offset, h->K, h->bins);
+          h->T, h->tet_v, h->posd, h->vol, h->boxes, h->tet_prefix, h->bin_offset, h->K, h->xs, h->ys, h->zs,
+          h->bins);
   }
   // the reference's factor: (NO_DIM+1.)/averageDensity stored as Real
   float rb = (float)rho_bar;

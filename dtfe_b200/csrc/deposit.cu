@@ -60,7 +60,7 @@ struct DepParams {
   int K;
   int64_t n;
   int64_t G1, G2;
-  double scale_m, scale_p;
+  const double* scales;   // device: fixed-point scales of mass and momentum, then their inverses
   unsigned long long* acc_m;  // per cell
   unsigned long long* acc_p;  // 3 per cell (null: no velocity)
 };
@@ -142,6 +142,7 @@ __global__ void __launch_bounds__(kDepBlock) k_deposit(DepParams P) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const bool valid = i < P.n;
   const bool with_vel = P.acc_p != nullptr;
+  const double scale_m = __ldg(&P.scales[0]), scale_p = __ldg(&P.scales[1]);
 
   int b = 0;
   int cell[3][3];
@@ -214,11 +215,11 @@ __global__ void __launch_bounds__(kDepBlock) k_deposit(DepParams P) {
       for (int bb = 0; bb < count[1]; ++bb)
         for (int c = 0; c < count[2]; ++c) {
           const float result = wt * w[0][a] * w[1][bb] * w[2][c];
-          const unsigned long long fm = to_fixed(result, P.scale_m);
+          const unsigned long long fm = to_fixed(result, scale_m);
           unsigned long long fp[3];
           if (with_vel) {
 #pragma unroll
-            for (int q = 0; q < 3; ++q) fp[q] = to_fixed(v[q] * result, P.scale_p);
+            for (int q = 0; q < 3; ++q) fp[q] = to_fixed(v[q] * result, scale_p);
           }
           if (staged) {
             const int k = ((cell[0][a] - tlo[0]) * kTile + (cell[1][bb] - tlo[1])) * kTile + (cell[2][c] - tlo[2]);
@@ -263,7 +264,7 @@ __global__ void __launch_bounds__(kDepBlock) k_deposit(DepParams P) {
 __global__ void k_deposit_finalize(int64_t n_tile_cells, const DepBox* __restrict__ boxes,
                                    const int64_t* __restrict__ tile_prefix, int K, int64_t G1, int64_t G2,
                                    const unsigned long long* __restrict__ acc_m,
-                                   const unsigned long long* __restrict__ acc_p, double inv_m, double inv_p,
+                                   const unsigned long long* __restrict__ acc_p, const double* __restrict__ scales,
                                    float* __restrict__ density, float* __restrict__ velocity) {
   int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (s >= n_tile_cells) return;
@@ -274,6 +275,7 @@ __global__ void k_deposit_finalize(int64_t n_tile_cells, const DepBox* __restric
   const int j = (int)((local / B.dims[2]) % B.dims[1]);
   const int i = (int)(local / ((int64_t)B.dims[2] * B.dims[1]));
   const int64_t idx = ((int64_t)(B.origin[0] + i) * G1 + (B.origin[1] + j)) * G2 + (B.origin[2] + k);
+  const double inv_m = __ldg(&scales[2]), inv_p = __ldg(&scales[3]);
   const float m = (float)((double)(long long)acc_m[idx] * inv_m);
   if (velocity) {
 #pragma unroll
@@ -378,6 +380,44 @@ __global__ void k_deposit_adjoint(const float4* __restrict__ pw, const DepBox* _
     for (int j = 0; j < 3; ++j) gx[3 * i + j] = (float)(B.factor * (double)q.w * sx[j]);
 }
 
+// Fixed-point scales from order-independent bounds: n x max|w| for the mass
+// and n x max(|w| (|vx| + |vy| + |vz|)) for the momentum, times 8 (the
+// clipped edge stencils' weights sum to at most 8 in magnitude), each scaled
+// to stay below 2^61.  Maxima of non-negative floats by integer atomicMax on
+// their bits.
+__global__ void k_deposit_bounds(int64_t n, const float4* __restrict__ pw, const float4* __restrict__ vel,
+                                 unsigned* __restrict__ maxbits) {
+  float mw = 0.f, mp = 0.f;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float4 q = __ldg(&pw[i]);
+    const float a = fabsf(q.w);
+    mw = fmaxf(mw, a);
+    if (vel) {
+      const float4 u = __ldg(&vel[i]);
+      mp = fmaxf(mp, a * (fabsf(u.x) + fabsf(u.y) + fabsf(u.z)));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mw = fmaxf(mw, __shfl_xor_sync(0xffffffffu, mw, o));
+    mp = fmaxf(mp, __shfl_xor_sync(0xffffffffu, mp, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&maxbits[0], __float_as_uint(mw));
+    atomicMax(&maxbits[1], __float_as_uint(mp));
+  }
+}
+
+__global__ void k_deposit_scales(int64_t n, const unsigned* __restrict__ maxbits, double* __restrict__ scales) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int q = 0; q < 2; ++q) {
+    const double bound = 8.0 * (double)n * (double)__uint_as_float(maxbits[q]);
+    const double s = ldexp(1.0, 61 - (int)ceil(log2(fmax(bound, 1e-30))));
+    scales[q] = s;
+    scales[2 + q] = 1.0 / s;
+  }
+}
+
 __global__ void k_pack4(int64_t n, const float* __restrict__ a3, const float* __restrict__ b1, float4* __restrict__ out) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) out[i] = make_float4(a3[3 * i], a3[3 * i + 1], a3[3 * i + 2], b1 ? b1[i] : 1.f);
@@ -399,7 +439,6 @@ extern "C" int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xy
   // host-side box records: the reference's float region arithmetic
   std::vector<DepBox> hb(n_boxes);
   std::vector<int64_t> prefix(n_boxes + 1);
-  double tot_m = 0.0, tot_p = 0.0;
   for (int b = 0; b < n_boxes; ++b) {
     const dtfe_deposit_box& in = boxes[b];
     DepBox& B = hb[b];
@@ -434,21 +473,12 @@ extern "C" int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xy
     tprefix[b + 1] = tprefix[b] + cells;
     B.factor = (float)cells / vol / (float)average_density;
   }
-  for (int64_t i = 0; i < n; ++i) {
-    const double wi = w ? std::fabs((double)w[i]) : 1.0;
-    tot_m += wi;
-    if (vel)
-      for (int q = 0; q < 3; ++q) tot_p = std::max(tot_p, 0.0) + wi * std::fabs((double)vel[3 * i + q]);
-  }
-  // scales: powers of two with the total below 2^61
-  auto scale_for = [](double tot) { return std::ldexp(1.0, 61 - (int)std::ceil(std::log2(std::max(tot, 1e-30)))); };
-  const double scale_m = scale_for(tot_m), scale_p = scale_for(tot_p);
   // scratch: particles (2 float4), boxes, prefix, accumulators (4 per cell)
   const size_t bytes_part = sizeof(float4) * 2 * (size_t)n;
   const size_t bytes_box = sizeof(DepBox) * n_boxes + 2 * sizeof(int64_t) * (n_boxes + 1);
   const size_t bytes_acc = sizeof(unsigned long long) * 4 * (size_t)G;
   const size_t bytes_tmp = sizeof(float) * 4 * (size_t)n;  // 3-float records as they arrive
-  const size_t need = bytes_part + bytes_box + bytes_acc + bytes_tmp + 2048;
+  const size_t need = bytes_part + bytes_box + bytes_acc + bytes_tmp + 4096;
   if (*scratch_bytes < need) {
     if (*scratch) cudaFree(*scratch);
     *scratch = nullptr;
@@ -468,6 +498,8 @@ extern "C" int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xy
   int64_t* d_prefix = (int64_t*)(base + o + sizeof(DepBox) * n_boxes);
   int64_t* d_tprefix = d_prefix + (n_boxes + 1);
   float* tmp = (float*)(base + align(o + bytes_box));
+  double* d_scales = (double*)(base + align(align(o + bytes_box) + bytes_tmp));
+  unsigned* d_maxbits = (unsigned*)(d_scales + 4);
   cudaError_t e;
   if (n > 0) {
     float* t3 = tmp;
@@ -493,8 +525,13 @@ extern "C" int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xy
   P.n = n;
   P.G1 = grid[1];
   P.G2 = grid[2];
-  P.scale_m = scale_m;
-  P.scale_p = scale_p;
+  cudaMemsetAsync(d_maxbits, 0, 2 * sizeof(unsigned), st);
+  if (n > 0)
+    k_deposit_bounds<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4 * 148), 256, 0, st>>>(n, d_pw,
+                                                                                          vel ? d_vel : nullptr,
+                                                                                          d_maxbits);
+  k_deposit_scales<<<1, 32, 0, st>>>(n, d_maxbits, d_scales);
+  P.scales = d_scales;
   P.acc_m = acc_m;
   P.acc_p = velocity_dev ? acc_p : nullptr;
   if (n > 0) {
@@ -506,7 +543,7 @@ extern "C" int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xy
   const int64_t nt = tprefix[n_boxes];
   if (nt > 0)
     k_deposit_finalize<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(nt, d_boxes, d_tprefix, n_boxes, grid[1], grid[2],
-                                                                     acc_m, acc_p, 1.0 / scale_m, 1.0 / scale_p,
+                                                                     acc_m, acc_p, d_scales,
                                                                      density_dev, velocity_dev);
   if ((e = cudaGetLastError()) != cudaSuccess) return dtfe_internal_set_error(DTFE_ERR_CUDA, cudaGetErrorString(e));
   // state for dtfe_gpu_deposit_adjoint (the scratch keeps particles and boxes)

@@ -77,17 +77,44 @@ __device__ __forceinline__ float dist2(float ax, float ay, float az, const float
   return d;
 }
 
+// Per sub-box bounding box of its particles.  Vertices of a sub-box are
+// contiguous, so a warp's lanes usually share one sub-box: they reduce in
+// registers first and the first lane of each run of equal sub-boxes issues
+// the six atomics.
 __global__ void k_sph_bounds(int64_t v0, int64_t v1, const int64_t* __restrict__ vprefix, int K,
                              const float4* __restrict__ posd, int* __restrict__ bounds) {
   const int64_t i = v0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= v1) return;
-  const int b = find_range(vprefix, K, i);
-  const float4 p = __ldg(&posd[i]);
-  const float x[3] = {p.x, p.y, p.z};
+  const int lane = threadIdx.x & 31;
+  const bool valid = i < v1;
+  int b = -1;
+  int lo[3] = {0x7FFFFFFF, 0x7FFFFFFF, 0x7FFFFFFF}, hi[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
+  if (valid) {
+    b = find_range(vprefix, K, i);
+    const float4 p = __ldg(&posd[i]);
+    const float x[3] = {p.x, p.y, p.z};
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    atomicMin(&bounds[6 * b + 2 * c], ordered(x[c]));
-    atomicMax(&bounds[6 * b + 2 * c + 1], ordered(x[c]));
+    for (int c = 0; c < 3; ++c) lo[c] = hi[c] = ordered(x[c]);
+  }
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int ob = __shfl_down_sync(0xffffffffu, b, o);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int ol = __shfl_down_sync(0xffffffffu, lo[c], o);
+      const int oh = __shfl_down_sync(0xffffffffu, hi[c], o);
+      if (lane + o < 32 && ob == b) {
+        lo[c] = min(lo[c], ol);
+        hi[c] = max(hi[c], oh);
+      }
+    }
+  }
+  const int prev = __shfl_up_sync(0xffffffffu, b, 1);
+  if (b >= 0 && (lane == 0 || prev != b)) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      atomicMin(&bounds[6 * b + 2 * c], lo[c]);
+      atomicMax(&bounds[6 * b + 2 * c + 1], hi[c]);
+    }
   }
 }
 
@@ -166,6 +193,18 @@ __global__ void k_sph_place(int64_t v0, int64_t v1, const int64_t* __restrict__ 
 
 __device__ __forceinline__ bool before(float d, int i, float e, int j) { return d < e || (d == e && i < j); }
 
+// Distance from coordinate x to cell c's slab along axis a (0 inside).
+// Boundary cells are open towards the outside (particles beyond the box
+// are clamped into them), so their outer side counts as no gap.
+__device__ __forceinline__ float cell_gap(const SphGrid& g, float x, int c, int a) {
+  const float e = 1.f / g.inv[a];
+  const float lo = g.lo[a] + (float)c * e, hi = lo + e;
+  const float slack = 1e-3f * e;  // cell assignment rounds in float
+  if (x < lo && c > 0) return fmaxf(lo - x - slack, 0.f);
+  if (x > hi && c < g.n[a] - 1) return fmaxf(x - hi - slack, 0.f);
+  return 0.f;
+}
+
 // The k nearest particles of q in one sub-box's cell grid, ascending by
 // (squared distance, index), in this thread's shared-memory columns
 // ld[slot * kSphBlock], li[slot * kSphBlock].  Returns the list length.
@@ -186,6 +225,12 @@ __device__ int knn(const SphGrid& g, const int* __restrict__ start, const int* _
         for (int dz = -r; dz <= r; dz += step) {
           const int z = c0[2] + dz;
           if (z < 0 || z >= g.n[2]) continue;
+          if (m == k) {
+            // skip cells wholly farther than the current k-th neighbour
+            const float gap[3] = {cell_gap(g, q[0], x, 0), cell_gap(g, q[1], y, 1), cell_gap(g, q[2], z, 2)};
+            const float md = gap[0] * gap[0] + gap[1] * gap[1] + gap[2] * gap[2];
+            if (md > ld[(k - 1) * kSphBlock]) continue;
+          }
           const int64_t cell = g.cell_off + ((int64_t)x * g.n[1] + y) * g.n[2] + z;
           const int a = __ldg(&start[cell]), e = __ldg(&start[cell + 1]);
           for (int u = a; u < e; ++u) {

@@ -181,14 +181,15 @@ __global__ void k_sph_count(int64_t v0, int64_t v1, const int64_t* __restrict__ 
 
 __global__ void k_sph_place(int64_t v0, int64_t v1, const int64_t* __restrict__ vprefix, int K,
                             const SphGrid* __restrict__ grids, const float4* __restrict__ posd,
-                            const int* __restrict__ start, const int* __restrict__ rank, int* __restrict__ sorted) {
+                            const int* __restrict__ start, const int* __restrict__ rank, float4* __restrict__ sorted) {
   const int64_t i = v0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= v1) return;
   const SphGrid g = grids[find_range(vprefix, K, i)];
   const float4 p = __ldg(&posd[i]);
   const int64_t cell = g.cell_off + ((int64_t)cell_axis(g, p.x, 0) * g.n[1] + cell_axis(g, p.y, 1)) * g.n[2] +
                        cell_axis(g, p.z, 2);
-  sorted[start[cell] + rank[i - v0]] = (int)i;
+  // position and particle index in one record, in cell order
+  sorted[start[cell] + rank[i - v0]] = make_float4(p.x, p.y, p.z, __int_as_float((int)i));
 }
 
 __device__ __forceinline__ bool before(float d, int i, float e, int j) { return d < e || (d == e && i < j); }
@@ -208,8 +209,8 @@ __device__ __forceinline__ float cell_gap(const SphGrid& g, float x, int c, int 
 // The k nearest particles of q in one sub-box's cell grid, ascending by
 // (squared distance, index), in this thread's shared-memory columns
 // ld[slot * kSphBlock], li[slot * kSphBlock].  Returns the list length.
-__device__ int knn(const SphGrid& g, const int* __restrict__ start, const int* __restrict__ sorted,
-                   const float4* __restrict__ posd, const float q[3], int k, float* ld, int* li) {
+__device__ int knn(const SphGrid& g, const int* __restrict__ start, const float4* __restrict__ sorted,
+                   const float q[3], int k, float* ld, int* li) {
   const int c0[3] = {cell_axis(g, q[0], 0), cell_axis(g, q[1], 1), cell_axis(g, q[2], 2)};
   const int rmax = max(g.n[0], max(g.n[1], g.n[2]));
   int m = 0;
@@ -234,8 +235,8 @@ __device__ int knn(const SphGrid& g, const int* __restrict__ start, const int* _
           const int64_t cell = g.cell_off + ((int64_t)x * g.n[1] + y) * g.n[2] + z;
           const int a = __ldg(&start[cell]), e = __ldg(&start[cell + 1]);
           for (int u = a; u < e; ++u) {
-            const int p = __ldg(&sorted[u]);
-            const float4 pp = __ldg(&posd[p]);
+            const float4 pp = __ldg(&sorted[u]);
+            const int p = __float_as_int(pp.w);
             const float d = dist2(pp.x, pp.y, pp.z, q);
             if (m == k && !before(d, p, ld[(k - 1) * kSphBlock], li[(k - 1) * kSphBlock])) continue;
             int j = m < k ? m++ : k - 1;
@@ -264,7 +265,7 @@ struct SphParams {
   const int64_t* vprefix;
   const SphGrid* grids;
   const int* start;
-  const int* sorted;
+  const float4* sorted;  // x, y, z, particle index (as int bits) in cell order
   const float4* posd;
   const float* w;
   const float4* vel;
@@ -296,7 +297,7 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_particles(SphParams P, int64_
   const SphGrid g = P.grids[b];
   const float4 pi = __ldg(&P.posd[i]);
   const float q[3] = {pi.x, pi.y, pi.z};
-  const int m = knn(g, P.start, P.sorted, P.posd, q, P.k, ld, li);
+  const int m = knn(g, P.start, P.sorted, q, P.k, ld, li);
   const float h = (float)((double)sqrtf(ld[(m - 1) * kSphBlock]) / 2.);
   P.h[i] = h;
   if (!P.d) return;
@@ -341,7 +342,7 @@ __global__ void __launch_bounds__(kSphBlock) k_sph_gather(SphParams P) {
   const float q[3] = {__ldg(&P.xs[B.coord_offset[0] + c.i]), __ldg(&P.ys[B.coord_offset[1] + c.j]),
                       __ldg(&P.zs[B.coord_offset[2] + c.k])};
   const SphGrid g = P.grids[c.b];
-  const int m = knn(g, P.start, P.sorted, P.posd, q, P.k, ld, li);
+  const int m = knn(g, P.start, P.sorted, q, P.k, ld, li);
   const float h = (float)((double)sqrtf(ld[(m - 1) * kSphBlock]) / 2.);
   const float c1 = 1.f / (h * h * h);
   double rd = 0.0, rv[3] = {0.0, 0.0, 0.0}, rs[DTFE_MAX_SCALARS];
@@ -492,7 +493,7 @@ extern "C" int dtfe_internal_sph(void* stream, int K, const dtfe_subbox* boxes_h
   size_t cub_bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, cub_bytes, (int*)nullptr, (int*)nullptr, (int)(cmax + 1), st);
   const size_t sizes[] = {sizeof(int64_t) * (K + 1), sizeof(int) * 6 * K, sizeof(SphGrid) * K, sizeof(int64_t),
-                          sizeof(int) * (cmax + 1), sizeof(int) * (cmax + 1), sizeof(int) * nv, sizeof(int) * nv,
+                          sizeof(int) * (cmax + 1), sizeof(int) * (cmax + 1), sizeof(int) * nv, sizeof(float4) * nv,
                           sizeof(float) * V, want_sc ? sizeof(double) * V : 0, sizeof(double) * AC * n_cells,
                           cub_bytes};
   constexpr int NB = sizeof(sizes) / sizeof(sizes[0]);
@@ -518,7 +519,7 @@ extern "C" int dtfe_internal_sph(void* stream, int K, const dtfe_subbox* boxes_h
   int* d_count = (int*)part[4];
   int* d_start = (int*)part[5];
   int* d_rank = (int*)part[6];
-  int* d_sorted = (int*)part[7];
+  float4* d_sorted = (float4*)part[7];
   float* d_h = (float*)part[8];
   double* d_d = want_sc ? (double*)part[9] : nullptr;
   double* d_acc = (double*)part[10];

@@ -825,12 +825,6 @@ struct dtfe_gpu_s {
   double *g_rho = nullptr, *g_x = nullptr, *g_v = nullptr, *g_S = nullptr, *g_m = nullptr, *vbar = nullptr;
   float* adj_a = nullptr;         // device copies of host loss weights
   cudaGraphExec_t step_graph = nullptr;  // captured step (dtfe_gpu_graph_build)
-  // vertex densities run on a side stream, concurrently with the walk (which
-  // needs positions and seeds, not densities); the main stream waits for
-  // ev_density before anything reads or rewrites vertex data
-  cudaStream_t side = nullptr;
-  cudaEvent_t ev_bins = nullptr, ev_density = nullptr;
-  bool density_pending = false;
   char* upload_buf = nullptr;     // staging of packed tetrahedra and 3-float vertex records
   void* sph_scratch = nullptr;    // SPH cell grids, neighbour bookkeeping, FP64 sums
   size_t sph_bytes = 0;
@@ -885,15 +879,6 @@ void drop_graph(dtfe_handle h) {
     cudaGraphExecDestroy(h->step_graph);
     h->step_graph = nullptr;
   }
-}
-
-// The main stream waits for a vertex-density pass still running on the side
-// stream.  Every entry point calls it before touching device data.
-int join_side(dtfe_handle h) {
-  if (!h->density_pending) return DTFE_OK;
-  h->density_pending = false;
-  DTFE_CUDA_TRY(cudaStreamWaitEvent(h->stream, h->ev_density, 0));
-  return DTFE_OK;
 }
 
 int prepare_bins(dtfe_handle h) {
@@ -983,22 +968,13 @@ int dtfe_gpu_create(const dtfe_config* cfg, dtfe_handle* out) {
   h->S = c.n_scalars;
   h->max_steps = c.max_walk_steps > 0 ? c.max_walk_steps : 65536;
   cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_bins, cudaEventDisableTiming);
-  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_density, cudaEventDisableTiming);
   if (e != cudaSuccess) {
-    if (h->stream) cudaStreamDestroy(h->stream);
-    if (h->side) cudaStreamDestroy(h->side);
-    if (h->ev_bins) cudaEventDestroy(h->ev_bins);
     delete h;
     return set_error(DTFE_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
   }
   int rc = dev_alloc(h, &h->counters, CNT_N);
   if (rc) {
     cudaStreamDestroy(h->stream);
-    cudaStreamDestroy(h->side);
-    cudaEventDestroy(h->ev_bins);
-    cudaEventDestroy(h->ev_density);
     delete h;
     return rc;
   }
@@ -1009,7 +985,6 @@ int dtfe_gpu_create(const dtfe_config* cfg, dtfe_handle* out) {
 int dtfe_gpu_destroy(dtfe_handle h) {
   if (!h) return DTFE_OK;
   cudaSetDevice(h->device);
-  cudaStreamSynchronize(h->side);
   cudaStreamSynchronize(h->stream);
   if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
   void* ptrs[] = {h->tet_v, h->tet_n, h->posd, h->vel4, h->scal, h->w, h->vol, h->inc_off, h->inc,
@@ -1025,26 +1000,15 @@ int dtfe_gpu_destroy(dtfe_handle h) {
                   (void*)h->adj_a, h->sph_scratch, (void*)h->sph_out, (void*)h->upload_buf})
     if (p) cudaFree(p);
   if (h->dep_out) cudaFree(h->dep_out);
-  cudaEventDestroy(h->ev_bins);
-  cudaEventDestroy(h->ev_density);
-  cudaStreamDestroy(h->side);
   cudaStreamDestroy(h->stream);
   delete h;
   return DTFE_OK;
 }
 
-void* dtfe_gpu_stream(dtfe_handle h) {
-  if (!h) return nullptr;
-  cudaSetDevice(h->device);
-  join_side(h);  // work queued on the returned stream follows every earlier call
-  return (void*)h->stream;
-}
+void* dtfe_gpu_stream(dtfe_handle h) { return h ? (void*)h->stream : nullptr; }
 
 int dtfe_gpu_synchronize(dtfe_handle h) {
   if (!h) return set_error(DTFE_ERR_ARG, "null handle");
-  DTFE_CUDA_TRY(cudaSetDevice(h->device));
-  int rc = join_side(h);
-  if (rc) return rc;
   DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return DTFE_OK;
 }
@@ -1059,7 +1023,6 @@ static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const fl
   if (n_tets < 0 || n_verts < 0 || n_tets > 0x7FFFFFFF || n_verts >= 0x7F7F7F7F)
     return set_error(DTFE_ERR_TOO_LARGE, "tetrahedron or vertex count beyond int32 indexing");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
-  if (int jr = join_side(h)) return jr;
   int rc;
   h->T = n_tets;
   h->V = n_verts;
@@ -1166,7 +1129,6 @@ int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* box
   if (!h || n_boxes <= 0 || !boxes || !xs || !ys || !zs || !grid)
     return set_error(DTFE_ERR_ARG, "null or empty sub-box description");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
-  if (int jr = join_side(h)) return jr;
   std::vector<int64_t> tprefix(n_boxes + 1), tetpre(n_boxes + 1), boff(n_boxes);
   int64_t cells = 0;
   for (int b = 0; b < n_boxes; ++b) {
@@ -1223,8 +1185,6 @@ int dtfe_gpu_vertex_density(dtfe_handle h, double rho_bar) {
   if (!(rho_bar > 0.0)) return set_error(DTFE_ERR_ARG, "averageDensity must be positive");
   if (h->V == 0) return set_error(DTFE_ERR_STATE, "nothing uploaded");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
-  int rc = join_side(h);  // the previous pass reads vol, which this one rewrites
-  if (rc) return rc;
   cudaStream_t st = h->stream;
   if (h->K > 0) DTFE_CUDA_TRY(cudaMemsetAsync(h->bins, 0xFF, sizeof(unsigned long long) * h->n_cells, st));
   if (h->T > 0) {
@@ -1241,15 +1201,9 @@ int dtfe_gpu_vertex_density(dtfe_handle h, double rho_bar) {
   float rb = (float)rho_bar;
   float factor = (float)(4.0 / (double)rb);
   h->factor = factor;
-  // densities on the side stream: the walk (main stream) needs the seeds,
-  // not the densities, and runs meanwhile; the evaluation joins
-  DTFE_CUDA_TRY(cudaEventRecord(h->ev_bins, st));
-  DTFE_CUDA_TRY(cudaStreamWaitEvent(h->side, h->ev_bins, 0));
-  k_vertex_density<<<blocks_for(h->V, kDensBlock), kDensBlock, 0, h->side>>>(h->V, h->w, h->vol, h->inc_off,
-                                                                             h->inc, h->hull, factor, h->posd);
+  k_vertex_density<<<blocks_for(h->V, kDensBlock), kDensBlock, 0, st>>>(h->V, h->w, h->vol, h->inc_off, h->inc,
+                                                                       h->hull, factor, h->posd);
   DTFE_CUDA_TRY(cudaGetLastError());
-  DTFE_CUDA_TRY(cudaEventRecord(h->ev_density, h->side));
-  h->density_pending = true;
   h->density_ready = true;
   h->bins_ready = h->K > 0;
   return DTFE_OK;
@@ -1259,7 +1213,6 @@ int dtfe_gpu_download_vertex_density(dtfe_handle h, float* dens) {
   if (!h || !dens) return set_error(DTFE_ERR_ARG, "null argument");
   if (!h->density_ready) return set_error(DTFE_ERR_STATE, "vertex density not computed");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
-  if (int jr = join_side(h)) return jr;
   // .w of each float4: strided copy
   DTFE_CUDA_TRY(cudaMemcpy2DAsync(dens, sizeof(float), (const char*)h->posd + 12, sizeof(float4),
                                   sizeof(float), h->V, cudaMemcpyDeviceToHost, h->stream));
@@ -1349,7 +1302,6 @@ static int interp_enqueue(dtfe_handle h, const dtfe_interp_opts* o, float* const
       return set_error(DTFE_ERR_ARG, "output buffers must be 16-byte aligned");
   if ((rc = dev_alloc(h, &h->tet_c, h->n_cells))) return rc;
   launch_locate(h->loc_variant, P, h->tet_c, st);
-  if ((rc = join_side(h))) return rc;
   launch_eval_s(method, h->S, h->eval_variant, P, h->tet_c, st, grid, block);
   h->tet_c_valid = method == DTFE_METHOD_CENTRE;  // the adjoint differentiates centre values only
   h->tet_c_fix = (o->flags & DTFE_FLAG_FIX_VALUE_INTERP) != 0;
@@ -1531,7 +1483,6 @@ int dtfe_gpu_adjoint_dev(dtfe_handle h, const float* grad_density_dev, const flo
   if (!h->density_ready || !h->tet_c_valid)
     return set_error(DTFE_ERR_STATE, "adjoint needs a preceding vertex density and cell-centre interpolation");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
-  if (int jr = join_side(h)) return jr;
   int rc;
   if ((rc = dev_alloc(h, &h->g_rho, h->V)) || (rc = dev_alloc(h, &h->g_x, 3 * h->V)) ||
       (rc = dev_alloc(h, &h->g_v, 3 * h->V)) || (rc = dev_alloc(h, &h->g_S, h->V)) ||
@@ -1557,7 +1508,6 @@ int dtfe_gpu_sph_dev(dtfe_handle h, int32_t n_neighbors, uint32_t fields, int32_
   if (fields & ~(DTFE_FIELD_BIT(DTFE_DENSITY) | DTFE_FIELD_BIT(DTFE_VELOCITY) | DTFE_FIELD_BIT(DTFE_SCALAR)))
     return set_error(DTFE_ERR_ARG, "SPH computes density, velocity and scalar fields only");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
-  if (int jr = join_side(h)) return jr;
   const int64_t G = (int64_t)h->grid[0] * h->grid[1] * h->grid[2];
   if (density_dev) DTFE_CUDA_TRY(cudaMemsetAsync(density_dev, 0, sizeof(float) * G, h->stream));
   if (velocity_dev) DTFE_CUDA_TRY(cudaMemsetAsync(velocity_dev, 0, sizeof(float) * 3 * G, h->stream));
@@ -1616,7 +1566,6 @@ int dtfe_gpu_graph_build(dtfe_handle h, double rho_bar, const dtfe_interp_opts* 
                          float* const out_dev[DTFE_NUM_FIELDS]) {
   if (!h || !opts) return set_error(DTFE_ERR_ARG, "null argument");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
-  if (int jr = join_side(h)) return jr;
   drop_graph(h);
   // one plain step first: allocations, equidistant offsets and the walk
   // check happen here, so the captured launches need none of them
@@ -1646,7 +1595,6 @@ int dtfe_gpu_graph_launch(dtfe_handle h) {
   if (!h) return set_error(DTFE_ERR_ARG, "null handle");
   if (!h->step_graph) return set_error(DTFE_ERR_STATE, "no step graph built (or the handle changed since)");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
-  if (int jr = join_side(h)) return jr;
   DTFE_CUDA_TRY(cudaGraphLaunch(h->step_graph, h->stream));
   return DTFE_OK;
 }
@@ -1654,7 +1602,6 @@ int dtfe_gpu_graph_launch(dtfe_handle h) {
 int dtfe_gpu_read_status(dtfe_handle h, dtfe_status* status) {
   if (!h) return set_error(DTFE_ERR_ARG, "null handle");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
-  if (int jr = join_side(h)) return jr;
   return read_status(h, status);
 }
 
@@ -1718,7 +1665,6 @@ int dtfe_gpu_locate_points(dtfe_handle h, int64_t np, const double* pts, int32_t
   if (start < 0 || start >= h->T) return set_error(DTFE_ERR_ARG, "start tetrahedron out of range");
   if (np == 0) return DTFE_OK;
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
-  if (int jr = join_side(h)) return jr;
   cudaStream_t st = h->stream;
   double* dp = nullptr;
   int* dout = nullptr;

@@ -31,6 +31,8 @@ def lib() -> C.CDLL:
         L.ref_interpolate.argtypes = [C.c_int64, vp, vp, vp, vp, C.c_int64, vp, vp, vp, vp, C.c_int, C.c_int,
                                       C.c_uint64, C.c_double, vp, vp, vp, vp, vp, vp, vp, vp]
         L.ref_interpolate.restype = C.c_int
+        L.ref_interpolate_timed.argtypes = L.ref_interpolate.argtypes + [C.c_uint32, C.POINTER(C.c_double)]
+        L.ref_interpolate_timed.restype = C.c_int
         _lib = L
     return _lib
 
@@ -67,3 +69,53 @@ def run(plan, box: int = 0, which: int = 0, n_points: int = 1, seed: int = 0, de
     if rc:
         raise RuntimeError(f"ref_interpolate failed ({rc})")
     return out
+
+
+def _box_args(plan, box):
+    b = plan.boxes[box]
+    v0, nv, t0, nt = b.vert_offset, b.n_verts, b.tet_offset, b.n_tets
+    xyz = np.ascontiguousarray(plan.xyz[v0:v0 + nv])
+    w = np.ascontiguousarray(plan.weight[v0:v0 + nv])
+    vel = None if plan.velocity is None else np.ascontiguousarray(plan.velocity[v0:v0 + nv])
+    tv = np.ascontiguousarray(plan.tet_v[t0:t0 + nt] - v0, dtype=np.int32)
+    tn = plan.tet_n[t0:t0 + nt]
+    tn = np.ascontiguousarray(np.where(tn >= 0, tn - t0, -1), dtype=np.int32)
+    dims = np.array([b.tile_dims[0], b.tile_dims[1], b.tile_dims[2]], np.int32)
+    region = np.array([b.lo[0], b.lo[0] + b.dx[0] * dims[0], b.lo[1], b.lo[1] + b.dx[1] * dims[1],
+                       b.lo[2], b.lo[2] + b.dx[2] * dims[2]], np.float32)
+    return xyz, w, vel, tv, tn, dims, region
+
+
+def time_boxes(plan, threads: int):
+    """Times the reference's own per-thread work of DTFE_parallel
+    (src/DTFE.cpp:331-356): vertexDensity + interpolateGrid of density,
+    velocity and velocity gradient on every sub-box, the sub-boxes spread
+    over ``threads`` host threads as the reference's OpenMP team would.
+    Returns (seconds of the slowest thread, per-box seconds); only the
+    reference's calls are timed, not loading the tessellation."""
+    from concurrent.futures import ThreadPoolExecutor
+    L = lib()
+
+    def one(box):
+        xyz, w, vel, tv, tn, dims, region = _box_args(plan, box)
+        G = int(np.prod(dims))
+        dens = np.zeros(G, np.float32)
+        velo = np.zeros((G, 3), np.float32)
+        grad = np.zeros((G, 9), np.float32)
+        sec = C.c_double(0.0)
+        p = lambda a: None if a is None else a.ctypes.data
+        rc = L.ref_interpolate_timed(len(xyz), p(xyz), p(w), p(vel), None, len(tv), p(tv), p(tn), p(region),
+                                     p(dims), 0, 1, 0, plan.rho_bar, None, None, p(dens), p(velo), p(grad),
+                                     None, None, None, 7, C.byref(sec))
+        if rc:
+            raise RuntimeError(f"ref_interpolate_timed failed ({rc})")
+        return sec.value
+    K = plan.n_boxes
+    with ThreadPoolExecutor(max_workers=max(1, min(threads, K))) as ex:
+        per_box = list(ex.map(one, range(K)))
+    # the reference gives each OpenMP thread one sub-box; with more boxes than
+    # threads, boxes are dealt round-robin
+    loads = [0.0] * max(1, min(threads, K))
+    for k, t in enumerate(per_box):
+        loads[k % len(loads)] += t
+    return max(loads), per_box

@@ -15,6 +15,7 @@
 // is not built; the User_options constructor below sets the members those
 // functions read, with the reference's defaults (src/user_options.cc:39-92).
 
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -88,11 +89,14 @@ void gsl_qrng_free(gsl_qrng*) {}
 //   instead of the reference's own (float-accumulated) ones.
 //   outputs (float, Quantities layout; NULL to skip): vertex densities,
 //   density, velocity, gradient, scalar (S = 1), scalar gradient, velocity std.
-int ref_interpolate(int64_t nv, const float* xyz, const float* w, const float* vel, const float* scal,
-                    int64_t nt, const int32_t* tv, const int32_t* tn, const float region[6],
-                    const int32_t grid[3], int which, int n_points, uint64_t seed, double rho_bar,
-                    const float* dens_override, float* out_vdens, float* out_density, float* out_velocity,
-                    float* out_gradient, float* out_scalar, float* out_scalar_gradient, float* out_std) {
+// seconds (may be NULL) receives the wall time of the reference's own work:
+// vertexDensity + the interpolation call (not the facade's loading).
+int ref_interpolate_timed(int64_t nv, const float* xyz, const float* w, const float* vel, const float* scal,
+                          int64_t nt, const int32_t* tv, const int32_t* tn, const float region[6],
+                          const int32_t grid[3], int which, int n_points, uint64_t seed, double rho_bar,
+                          const float* dens_override, float* out_vdens, float* out_density, float* out_velocity,
+                          float* out_gradient, float* out_scalar, float* out_scalar_gradient, float* out_std,
+                          uint32_t extra_fields, double* seconds) {
   DT dt;
   const std::vector<DT::Vertex*>& verts = dt.load_flat(nv, xyz, nt, tv, tn);
   for (int64_t i = 0; i < nv; ++i) {
@@ -108,7 +112,9 @@ int ref_interpolate(int64_t nv, const float* xyz, const float* w, const float* v
   opt.method = which;
   opt.noPoints = n_points;
   opt.randomSeed = (size_t)seed;
+  const auto t0 = std::chrono::steady_clock::now();
   vertexDensity(dt, opt);
+  const auto t1 = std::chrono::steady_clock::now();
   for (int64_t i = 0; i < nv; ++i) {
     if (out_vdens) out_vdens[i] = verts[i]->info().density();
     if (dens_override) verts[i]->info().setDensity(dens_override[i]);
@@ -121,6 +127,10 @@ int ref_interpolate(int64_t nv, const float* xyz, const float* w, const float* v
   f.scalar = out_scalar != nullptr;
   f.scalar_gradient = out_scalar_gradient != nullptr;
   f.velocity_std = out_std != nullptr && which == 2;
+  // extra_fields bit 0..2: velocity divergence, shear, vorticity (computed by
+  // the reference from the gradient, src/DTFE.cpp:394-475, outside the timing)
+  if (extra_fields & 7u) f.velocity_gradient = true;
+  const auto t2 = std::chrono::steady_clock::now();
   if (which == 0) {
     opt.uField = f;
     interpolateGrid(dt, opt, &q);
@@ -133,6 +143,9 @@ int ref_interpolate(int64_t nv, const float* xyz, const float* w, const float* v
   } else {
     return 1;
   }
+  const auto t3 = std::chrono::steady_clock::now();
+  if (seconds)
+    *seconds = std::chrono::duration<double>(t1 - t0).count() + std::chrono::duration<double>(t3 - t2).count();
   const size_t G = (size_t)grid[0] * grid[1] * grid[2];
   auto copy = [&](float* dst, const float* src, size_t n, size_t have) {
     if (dst && have == G) std::memcpy(dst, src, n * sizeof(float));
@@ -144,6 +157,16 @@ int ref_interpolate(int64_t nv, const float* xyz, const float* w, const float* v
   copy(out_scalar_gradient, (const float*)q.scalar_gradient.data(), 3 * G, q.scalar_gradient.size());
   copy(out_std, q.velocity_std.data(), G, q.velocity_std.size());
   return 0;
+}
+
+int ref_interpolate(int64_t nv, const float* xyz, const float* w, const float* vel, const float* scal,
+                    int64_t nt, const int32_t* tv, const int32_t* tn, const float region[6],
+                    const int32_t grid[3], int which, int n_points, uint64_t seed, double rho_bar,
+                    const float* dens_override, float* out_vdens, float* out_density, float* out_velocity,
+                    float* out_gradient, float* out_scalar, float* out_scalar_gradient, float* out_std) {
+  return ref_interpolate_timed(nv, xyz, w, vel, scal, nt, tv, tn, region, grid, which, n_points, seed, rho_bar,
+                               dens_override, out_vdens, out_density, out_velocity, out_gradient, out_scalar,
+                               out_scalar_gradient, out_std, 0u, nullptr);
 }
 
 }  // extern "C"

@@ -64,3 +64,15 @@ def test_live_sph(built, k, extensive):
     assert np.array_equal(od.astype(np.float32), d)
     assert np.array_equal(ov.astype(np.float32), v)
     assert np.array_equal(osc[:, 0].astype(np.float32), s)
+
+
+def test_timed_reference_matches_untimed(built):
+    """The timed harness entry the CPU baseline uses runs the same reference
+    code (same outputs) and reports a positive time per sub-box."""
+    pos, psi = S.zeldovich_lattice(12, 100.0, 0.8, seed=3)
+    w = np.ones(len(pos), np.float32)
+    vel = (20 * psi).astype(np.float32)
+    plan = P.make_plan(pos, w, vel, None, grid=(10, 10, 10), n_threads=4, average_density_value=float(len(pos)) / 1e6)
+    tmax, per_box = R.time_boxes(plan, 2)
+    assert len(per_box) == plan.n_boxes and all(t > 0 for t in per_box)
+    assert tmax >= max(per_box) - 1e-12

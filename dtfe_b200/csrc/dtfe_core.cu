@@ -826,6 +826,8 @@ struct dtfe_gpu_s {
   float* adj_a = nullptr;         // device copies of host loss weights
   cudaGraphExec_t step_graph = nullptr;  // captured step (dtfe_gpu_graph_build)
   char* upload_buf = nullptr;     // staging of packed tetrahedra and 3-float vertex records
+  cudaEvent_t ev_h2d = nullptr;   // recorded when an upload's copies have crossed
+  dtfe_gpu_s* upload_after = nullptr;  // uploads wait for this handle's latest copies
   void* sph_scratch = nullptr;    // SPH cell grids, neighbour bookkeeping, FP64 sums
   size_t sph_bytes = 0;
   float* sph_out = nullptr;       // host-output SPH staging
@@ -968,12 +970,15 @@ int dtfe_gpu_create(const dtfe_config* cfg, dtfe_handle* out) {
   h->S = c.n_scalars;
   h->max_steps = c.max_walk_steps > 0 ? c.max_walk_steps : 65536;
   cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_h2d, cudaEventDisableTiming);
   if (e != cudaSuccess) {
+    if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return set_error(DTFE_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
   }
   int rc = dev_alloc(h, &h->counters, CNT_N);
   if (rc) {
+    cudaEventDestroy(h->ev_h2d);
     cudaStreamDestroy(h->stream);
     delete h;
     return rc;
@@ -1000,6 +1005,7 @@ int dtfe_gpu_destroy(dtfe_handle h) {
                   (void*)h->adj_a, h->sph_scratch, (void*)h->sph_out, (void*)h->upload_buf})
     if (p) cudaFree(p);
   if (h->dep_out) cudaFree(h->dep_out);
+  cudaEventDestroy(h->ev_h2d);
   cudaStreamDestroy(h->stream);
   delete h;
   return DTFE_OK;
@@ -1016,9 +1022,16 @@ int dtfe_gpu_synchronize(dtfe_handle h) {
 // Common body of the two uploads: tets(h) copies or decodes the
 // tetrahedron arrays into h->tet_v / h->tet_n on h->stream.
 extern "C++" {
-template <class TetCopy>
+// tets_bytes: staging the tetrahedra need on the device (0: they are copied
+// straight into tet_v / tet_n); tets_h2d(h, stage) queues their host->device
+// copies, tets_finish(h, stage) the kernels that complete them.  All copies
+// of an upload are queued before any of its kernels, so that a chained
+// handle's upload (dtfe_gpu_chain_uploads) can start on the copy engine as
+// soon as these have crossed.
+template <class TetH2D, class TetFinish>
 static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const float* w, const float* vel,
-                       const float* scal, int64_t n_verts, TetCopy tets) {
+                       const float* scal, int64_t n_verts, size_t tets_bytes, TetH2D tets_h2d,
+                       TetFinish tets_finish) {
   if (!h || !xyz || !w) return set_error(DTFE_ERR_ARG, "null argument");
   if (n_tets < 0 || n_verts < 0 || n_tets > 0x7FFFFFFF || n_verts >= 0x7F7F7F7F)
     return set_error(DTFE_ERR_TOO_LARGE, "tetrahedron or vertex count beyond int32 indexing");
@@ -1026,6 +1039,8 @@ static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const fl
   int rc;
   h->T = n_tets;
   h->V = n_verts;
+  const size_t tets_stage = (tets_bytes + 255) & ~(size_t)255;
+  const size_t vert_stage = sizeof(float) * 3 * (size_t)n_verts;
   if ((rc = dev_alloc(h, &h->tet_v, n_tets)) || (rc = dev_alloc(h, &h->tet_n, n_tets)) ||
       (rc = dev_alloc(h, &h->posd, n_verts)) || (rc = dev_alloc(h, &h->vel4, n_verts)) ||
       (rc = dev_alloc(h, &h->w, n_verts)) || (rc = dev_alloc(h, &h->vol, n_tets)) ||
@@ -1033,32 +1048,34 @@ static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const fl
       (rc = dev_alloc(h, &h->scratch_i, n_verts)) ||
       (rc = dev_alloc(h, &h->scan_blocks, (n_verts + kScanBlock - 1) / kScanBlock + 1)) ||
       (rc = dev_alloc(h, &h->hull, n_verts)) ||
-      (rc = dev_alloc(h, &h->scal, (size_t)n_verts * h->S)))
+      (rc = dev_alloc(h, &h->scal, (size_t)n_verts * h->S)) ||
+      // staging kept in the handle (an allocation per upload would map and
+      // unmap device memory every time): tetrahedra, positions, velocities
+      (rc = dev_alloc(h, &h->upload_buf, tets_stage + 2 * vert_stage)))
     return rc;
   cudaStream_t st = h->stream;
-  if (n_tets && (rc = tets(h))) return rc;
+  char* stage = h->upload_buf;
+  float* sx = (float*)(stage + tets_stage);
+  float* sv = (float*)(stage + tets_stage + vert_stage);
+  // copies first: wait for the chained handle's transfers, queue ours, mark them
+  if (h->upload_after) DTFE_CUDA_TRY(cudaStreamWaitEvent(st, h->upload_after->ev_h2d, 0));
+  if (n_tets && (rc = tets_h2d(h, stage))) return rc;
   if (n_verts) {
-    // positions and velocities arrive as 3 floats per vertex; pack them into
-    // 16-byte records on the device
-    // staging kept in the handle (an allocation per upload would map and
-    // unmap device memory every time)
-    if ((rc = dev_alloc(h, &h->upload_buf, sizeof(float) * 3 * n_verts))) return rc;
-    float* tmp = (float*)h->upload_buf;
-    DTFE_CUDA_TRY(cudaMemcpyAsync(tmp, xyz, sizeof(float) * 3 * n_verts, cudaMemcpyHostToDevice, st));
-    k_pack_xyz<<<blocks_for(n_verts, 256), 256, 0, st>>>(n_verts, tmp, h->posd, 0.f);
-    if (vel) {
-      DTFE_CUDA_TRY(cudaMemcpyAsync(tmp, vel, sizeof(float) * 3 * n_verts, cudaMemcpyHostToDevice, st));
-      k_pack_xyz<<<blocks_for(n_verts, 256), 256, 0, st>>>(n_verts, tmp, h->vel4, 0.f);
-    } else {
-      DTFE_CUDA_TRY(cudaMemsetAsync(h->vel4, 0, sizeof(float4) * n_verts, st));
-    }
+    DTFE_CUDA_TRY(cudaMemcpyAsync(sx, xyz, vert_stage, cudaMemcpyHostToDevice, st));
+    if (vel) DTFE_CUDA_TRY(cudaMemcpyAsync(sv, vel, vert_stage, cudaMemcpyHostToDevice, st));
     DTFE_CUDA_TRY(cudaMemcpyAsync(h->w, w, sizeof(float) * n_verts, cudaMemcpyHostToDevice, st));
-    if (h->S > 0) {
-      if (scal)
-        DTFE_CUDA_TRY(cudaMemcpyAsync(h->scal, scal, sizeof(float) * h->S * n_verts, cudaMemcpyHostToDevice, st));
-      else
-        DTFE_CUDA_TRY(cudaMemsetAsync(h->scal, 0, sizeof(float) * h->S * n_verts, st));
-    }
+    if (h->S > 0 && scal)
+      DTFE_CUDA_TRY(cudaMemcpyAsync(h->scal, scal, sizeof(float) * h->S * n_verts, cudaMemcpyHostToDevice, st));
+  }
+  DTFE_CUDA_TRY(cudaEventRecord(h->ev_h2d, st));
+  // then the kernels: decode the tetrahedra, pack positions and velocities
+  // into 16-byte records
+  if (n_tets && (rc = tets_finish(h, stage))) return rc;
+  if (n_verts) {
+    k_pack_xyz<<<blocks_for(n_verts, 256), 256, 0, st>>>(n_verts, sx, h->posd, 0.f);
+    if (vel) k_pack_xyz<<<blocks_for(n_verts, 256), 256, 0, st>>>(n_verts, sv, h->vel4, 0.f);
+    else DTFE_CUDA_TRY(cudaMemsetAsync(h->vel4, 0, sizeof(float4) * n_verts, st));
+    if (h->S > 0 && !scal) DTFE_CUDA_TRY(cudaMemsetAsync(h->scal, 0, sizeof(float) * h->S * n_verts, st));
   }
   // hull vertices (a property of the tessellation's topology)
   if (n_verts) DTFE_CUDA_TRY(cudaMemsetAsync(h->hull, 0, sizeof(int) * n_verts, st));
@@ -1093,11 +1110,14 @@ int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n, i
                     const float* xyz, const float* w, const float* vel, const float* scal,
                     int64_t n_verts) {
   if (!tet_v || !tet_n) return set_error(DTFE_ERR_ARG, "null argument");
-  return upload_impl(h, n_tets, xyz, w, vel, scal, n_verts, [&](dtfe_handle hh) -> int {
-    DTFE_CUDA_TRY(cudaMemcpyAsync(hh->tet_v, tet_v, 16 * n_tets, cudaMemcpyHostToDevice, hh->stream));
-    DTFE_CUDA_TRY(cudaMemcpyAsync(hh->tet_n, tet_n, 16 * n_tets, cudaMemcpyHostToDevice, hh->stream));
-    return DTFE_OK;
-  });
+  return upload_impl(
+      h, n_tets, xyz, w, vel, scal, n_verts, 0,
+      [&](dtfe_handle hh, char*) -> int {
+        DTFE_CUDA_TRY(cudaMemcpyAsync(hh->tet_v, tet_v, 16 * n_tets, cudaMemcpyHostToDevice, hh->stream));
+        DTFE_CUDA_TRY(cudaMemcpyAsync(hh->tet_n, tet_n, 16 * n_tets, cudaMemcpyHostToDevice, hh->stream));
+        return DTFE_OK;
+      },
+      [&](dtfe_handle, char*) -> int { return DTFE_OK; });
 }
 
 int dtfe_gpu_upload_packed(dtfe_handle h, const void* packed, int64_t packed_bytes, const float* xyz,
@@ -1110,17 +1130,26 @@ int dtfe_gpu_upload_packed(dtfe_handle h, const void* packed, int64_t packed_byt
   if (hd[0] != 0x31505444 || T < 0 || nb != (T + kPackBlock - 1) / kPackBlock || hd[7] + 4 * hd[3] > packed_bytes ||
       hd[6] + 16 * T > packed_bytes)
     return set_error(DTFE_ERR_ARG, "not a packed tessellation (dtfe_tets_pack)");
-  return upload_impl(h, T, xyz, w, vel, scal, n_verts, [&](dtfe_handle hh) -> int {
-    int rc2 = dev_alloc(hh, &hh->upload_buf, (size_t)packed_bytes);
-    if (rc2) return rc2;
-    char* dev = hh->upload_buf;
-    DTFE_CUDA_TRY(cudaMemcpyAsync(dev, packed, (size_t)packed_bytes, cudaMemcpyHostToDevice, hh->stream));
-    k_unpack_tets<<<(unsigned)nb, kPackBlock, 0, hh->stream>>>(
-        T, (const int32_t*)(dev + hd[4]), (const int32_t*)(dev + hd[5]), (const uint4*)(dev + hd[6]),
-        (const int32_t*)(dev + hd[7]), hh->tet_v, hh->tet_n);
-    DTFE_CUDA_TRY(cudaGetLastError());
-    return DTFE_OK;
-  });
+  return upload_impl(
+      h, T, xyz, w, vel, scal, n_verts, (size_t)packed_bytes,
+      [&](dtfe_handle hh, char* dev) -> int {
+        DTFE_CUDA_TRY(cudaMemcpyAsync(dev, packed, (size_t)packed_bytes, cudaMemcpyHostToDevice, hh->stream));
+        return DTFE_OK;
+      },
+      [&](dtfe_handle hh, char* dev) -> int {
+        k_unpack_tets<<<(unsigned)nb, kPackBlock, 0, hh->stream>>>(
+            T, (const int32_t*)(dev + hd[4]), (const int32_t*)(dev + hd[5]), (const uint4*)(dev + hd[6]),
+            (const int32_t*)(dev + hd[7]), hh->tet_v, hh->tet_n);
+        DTFE_CUDA_TRY(cudaGetLastError());
+        return DTFE_OK;
+      });
+}
+
+int dtfe_gpu_chain_uploads(dtfe_handle h, dtfe_handle after) {
+  if (!h || after == h) return set_error(DTFE_ERR_ARG, "bad handles");
+  if (after && after->device != h->device) return set_error(DTFE_ERR_ARG, "handles on different devices");
+  h->upload_after = after;
+  return DTFE_OK;
 }
 
 int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* boxes, const float* xs,

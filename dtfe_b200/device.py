@@ -62,6 +62,11 @@ class DeviceDTFE:
             self.h, packed.ctypes.data, packed.nbytes, N.ptr(plan.xyz), N.ptr(plan.weight), N.ptr(plan.velocity),
             N.ptr(plan.scalar), plan.n_verts))
 
+    def chain_uploads(self, after: "DeviceDTFE | None") -> None:
+        """Uploads on this handle wait for ``after``'s latest transfers
+        (dtfe_gpu_chain_uploads); None removes the link."""
+        N.check(self.lib.dtfe_gpu_chain_uploads(self.h, after.h if after is not None else None))
+
     def set_subboxes(self, plan) -> None:
         grid = np.asarray(plan.grid, np.int32)
         N.check(self.lib.dtfe_gpu_set_subboxes(

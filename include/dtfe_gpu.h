@@ -144,6 +144,14 @@ int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n,
  * reference (its tessellation never leaves the host). */
 int dtfe_gpu_upload_packed(dtfe_handle h, const void* packed, int64_t packed_bytes, const float* xyz,
                            const float* w, const float* vel, const float* scal, int64_t n_verts);
+/* Orders uploads between two handles used alternately (double buffering
+ * across snapshots): every later upload on h waits until the host->device
+ * copies of after's most recent upload have crossed, so the two handles'
+ * inputs use the copy engine one after the other instead of sharing it
+ * (their kernels and downloads still overlap).  after = NULL removes the
+ * link; remove it before destroying `after`.  No counterpart in the
+ * reference. */
+int dtfe_gpu_chain_uploads(dtfe_handle h, dtfe_handle after);
 
 /* Describe the sub-boxes and the main grid.  xs/ys/zs hold the sample
  * coordinates of every tile along each axis (the reference's running

@@ -53,6 +53,8 @@ def test_async_double_buffered_matches_sync(gpu_built):
         for d in devs:
             d.upload_packed(plan, packed)
             d.set_subboxes(plan)
+        devs[0].chain_uploads(devs[1])
+        devs[1].chain_uploads(devs[0])
         for step in range(4):
             d = devs[step % 2]
             d.synchronize()
@@ -66,5 +68,7 @@ def test_async_double_buffered_matches_sync(gpu_built):
                 assert np.array_equal(o[f].reshape(ref[f].shape), ref[f]), f
         assert devs[0].read_status()["n_samples_located"] == G
     finally:
+        for d in devs:
+            d.chain_uploads(None)
         for d in devs:
             d.close()

@@ -54,7 +54,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256, help="particles per side (and grid cells per side)")
     ap.add_argument("--threads", type=int, default=0, help="host threads (0 = all)")
-    ap.add_argument("--e2e-steps", type=int, default=6)
+    ap.add_argument("--e2e-steps", type=int, default=9)
+    ap.add_argument("--e2e-buffers", type=int, default=3,
+                    help="handles used in turn by the end-to-end loop (2 = double buffering)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mc", action="store_true")
@@ -709,52 +711,57 @@ def run_ours(args):
             return te
         te_lat = time_e2e(e2e_packed)
         te_plain = time_e2e(e2e_plain)
-        # double buffering across steps: two handles, each step's transfers
-        # and kernels queued asynchronously, so one handle's downloads and
-        # kernels overlap the other's uploads (every step still moves its
-        # inputs in and all its fields out)
-        dev2 = DeviceDTFE(local, 0)
-        dev2.set_variants(*variants)
-        pair = [dev, dev2]
-        outs2 = [host_out, {f: pin(np.empty_like(a)) for f, a in host_out.items()}]
-        for d in pair:
+        # multiple buffering across steps: a ring of handles, each step's
+        # transfers and kernels queued asynchronously, so one handle's
+        # downloads and kernels overlap the next one's uploads (every step
+        # still moves its inputs in and all its fields out); with three, a
+        # step's upload no longer waits for the download two steps back
+        nbuf = max(2, args.e2e_buffers)
+        ring = [dev]
+        for _ in range(nbuf - 1):
+            d = DeviceDTFE(local, 0)
+            d.set_variants(*variants)
+            ring.append(d)
+        outs2 = [host_out] + [{f: pin(np.empty_like(a)) for f, a in host_out.items()} for _ in range(nbuf - 1)]
+        for d in ring:
             d.upload_packed(hp, packed)
             d.set_subboxes(hp)
-        # the two handles' inputs cross PCIe one after the other
-        dev.chain_uploads(dev2)
-        dev2.chain_uploads(dev)
+        # the handles' inputs cross PCIe one after the other, in step order
+        for i, d in enumerate(ring):
+            d.chain_uploads(ring[i - 1])
 
         def e2e_pipelined(k):
-            d = pair[k % 2]
+            d = ring[k % nbuf]
             d.synchronize()
             d.upload_packed(hp, packed)
             d.vertex_density(hp.rho_bar)
-            d.interpolate_async(FIELDS, outs2[k % 2], method=0)
-        for k in range(2):
+            d.interpolate_async(FIELDS, outs2[k % nbuf], method=0)
+        for k in range(nbuf):
             e2e_pipelined(k)
-        for d in pair:
+        for d in ring:
             d.synchronize()
         if world > 1:
             dist.barrier()
         t0 = time.perf_counter()
         for k in range(args.e2e_steps):
             e2e_pipelined(k)
-        for d in pair:
+        for d in ring:
             d.synchronize()
         te = (time.perf_counter() - t0) / args.e2e_steps
         if world > 1:
             t = torch.tensor([te], device=f"cuda:{local}", dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             te = float(t.item())
-        st2 = dev2.read_status()
-        dev.chain_uploads(None)
-        dev2.chain_uploads(None)
-        dev2.close()
+        st2 = ring[(args.e2e_steps - 1) % nbuf].read_status()
+        for d in ring:
+            d.chain_uploads(None)
+        for d in ring[1:]:
+            d.close()
         e2e = {"value": world * G / te, "unit": "grid samples/s", "h2d_bytes_per_step": int(packed.nbytes + h_vert),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * te,
                "path": "per step: dtfe_gpu_upload_packed + vertex_density + interpolate_async into pinned host "
-                       "buffers, two handles alternating (double buffering, uploads chained); sub-box geometry set "
-                       "once per handle",
+                       f"buffers, {nbuf} handles in turn (uploads chained in step order); sub-box geometry set "
+                       "once per handle", "buffers": nbuf,
                "samples_located_last_step": st2["n_samples_located"],
                "single_step_latency_ms": 1e3 * te_lat,
                "unpacked_single_step": {"value": world * G / te_plain, "ms_per_step": 1e3 * te_plain,

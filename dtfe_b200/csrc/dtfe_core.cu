@@ -55,6 +55,9 @@ int set_error(int code, const std::string& msg) {
 
 constexpr int64_t kMaxCells = 0x7FFFFFFF;  // cell keys are int32
 enum { CNT_LOCATED, CNT_OUTSIDE, CNT_FAIL, CNT_STEPS, CNT_EXACT, CNT_TIES, CNT_N };
+// after the per-step counters, kept across steps: tetrahedra a packed upload
+// could not decode (cleared by every upload)
+constexpr int CNT_DECODE = CNT_N;
 
 // ---------------------------------------------------------------------------
 __global__ void k_pack_xyz(int64_t n, const float* __restrict__ xyz, float4* __restrict__ out, float wval) {
@@ -87,35 +90,21 @@ __device__ __forceinline__ int find_box(const int64_t* __restrict__ prefix, int 
 
 // ---- vertex -> tetrahedron incidence (built once per upload) ------------
 // Decoder of the packed tessellation (dtfe_tets_pack, host_plan.cpp): one
-// thread per tetrahedron, one block per packing block of 256; the block scan
-// of escape counts gives every thread its first escaped value.
+// thread per tetrahedron, one block per packing block of 256.  The block's
+// bytes are staged in shared memory with coalesced 4-byte loads; a block scan
+// of the tetrahedra's sizes (8 bytes + one per bit of the flag byte) places
+// each thread's fields, a second scan of the escaped fields its first escaped
+// value.  Every read is checked against the buffer and every decoded index
+// against the vertex and tetrahedron counts: a violation counts into *err
+// (reported by the next status read) and stores vertex 0 / no neighbour, so
+// that a malformed buffer cannot send later kernels out of range.
 constexpr int kPackBlock = 256;
-__global__ void __launch_bounds__(kPackBlock) k_unpack_tets(int64_t T, const int32_t* __restrict__ base,
-                                                            const int32_t* __restrict__ esc_off,
-                                                            const uint4* __restrict__ codes,
-                                                            const int32_t* __restrict__ esc, int4* __restrict__ tet_v,
-                                                            int4* __restrict__ tet_n) {
-  __shared__ int s_warp[kPackBlock / 32];
-  const int64_t t = blockIdx.x * (int64_t)kPackBlock + threadIdx.x;
-  const bool valid = t < T;
-  uint16_t c[8] = {0, 0, 0, 0, 0x8000, 0x8000, 0x8000, 0x8000};
-  if (valid) {
-    const uint4 q = __ldg(&codes[t]);
-    const uint32_t w[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      c[2 * k] = (uint16_t)(w[k] & 0xFFFFu);
-      c[2 * k + 1] = (uint16_t)(w[k] >> 16);
-    }
-  }
-  int ne = 0;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) ne += c[k] == 0xFFFF;
-#pragma unroll
-  for (int k = 4; k < 8; ++k) ne += (int16_t)c[k] == 32767;
-  // exclusive block scan of ne
+constexpr int kPackMaxBlockBytes = kPackBlock * 16;
+
+// Exclusive block-wide prefix sum of x over kPackBlock threads (all must call).
+__device__ __forceinline__ int pack_block_scan(int x, int* s_warp, int* total) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int inc = ne;
+  int inc = x;
 #pragma unroll
   for (int d = 1; d < 32; d <<= 1) {
     const int y = __shfl_up_sync(0xffffffffu, inc, d);
@@ -123,19 +112,82 @@ __global__ void __launch_bounds__(kPackBlock) k_unpack_tets(int64_t T, const int
   }
   if (lane == 31) s_warp[wid] = inc;
   __syncthreads();
-  int before = 0;
-  for (int q = 0; q < wid; ++q) before += s_warp[q];
+  int before = 0, all = 0;
+#pragma unroll
+  for (int q = 0; q < kPackBlock / 32; ++q) {
+    const int v = s_warp[q];
+    before += q < wid ? v : 0;
+    all += v;
+  }
+  if (total) *total = all;
+  return before + inc - x;
+}
+
+__global__ void __launch_bounds__(kPackBlock)
+    k_unpack_tets(int64_t T, int64_t V, const int32_t* __restrict__ base, const int32_t* __restrict__ esc_off,
+                  const int64_t* __restrict__ boff, const uint8_t* __restrict__ flags,
+                  const uint32_t* __restrict__ data, int64_t data_bytes, const int32_t* __restrict__ esc,
+                  int64_t n_esc, int4* __restrict__ tet_v, int4* __restrict__ tet_n, unsigned long long* err) {
+  __shared__ uint32_t s_data[kPackMaxBlockBytes / 4 + 2];
+  __shared__ int s_scan[2][kPackBlock / 32];
+  const int64_t b = blockIdx.x;
+  const int64_t t = b * kPackBlock + threadIdx.x;
+  const bool valid = t < T;
+  const int flag = valid ? (int)__ldg(&flags[t]) : 0;
+  const int size = valid ? 8 + __popc(flag) : 0;
+  int block_bytes;
+  const int off = pack_block_scan(size, s_scan[0], &block_bytes);
+  const int64_t b0 = __ldg(&boff[b]), b1 = __ldg(&boff[b + 1]);
+  const bool block_ok = b0 >= 0 && b1 - b0 == block_bytes && b1 <= data_bytes;
+  // stage the block from the 4-byte word holding its first byte; data_bytes
+  // is a multiple of 16, so rounding b1 up to a word stays inside the data
+  const int64_t w0 = block_ok ? b0 >> 2 : 0;
+  const int nw = block_ok ? (int)(((b1 + 3) >> 2) - w0) : 0;
+  for (int i = threadIdx.x; i < nw; i += kPackBlock) s_data[i] = __ldg(&data[w0 + i]);
+  __syncthreads();
+  // off + size <= block_bytes <= kPackMaxBlockBytes: in s_data even when the
+  // block is rejected (its bytes are then unused)
+  const uint8_t* sb = (const uint8_t*)s_data + (block_ok ? (b0 & 3) : 0);
+  uint32_t raw[8];
+  int p = off, ne = 0;
+#pragma unroll
+  for (int f = 0; f < 8; ++f) {
+    const bool wide = (flag >> f) & 1;
+    raw[f] = sb[p++];
+    if (wide) raw[f] |= (uint32_t)sb[p++] << 8;
+    if (f < 4) ne += raw[f] == (wide ? 0xFFFFu : 0xFFu);
+    else ne += (wide ? (int)(int16_t)raw[f] : (int)(int8_t)raw[f]) == (wide ? 32767 : 127);
+  }
+  if (!valid) ne = 0;
+  const int e_in = pack_block_scan(ne, s_scan[1], nullptr);
   if (!valid) return;
-  const int32_t* e = esc + __ldg(&esc_off[blockIdx.x]) + before + inc - ne;
-  const int32_t b0 = __ldg(&base[blockIdx.x]);
-  int v[4], n[4];
-  v[0] = c[0] == 0xFFFF ? *e++ : b0 + (int)c[0];
+  const int64_t e0 = (int64_t)__ldg(&esc_off[b]) + e_in;
+  bool ok = block_ok && e0 >= 0 && e0 + ne <= n_esc;
+  int v[4] = {0, 0, 0, 0}, n[4] = {-1, -1, -1, -1};
+  if (ok) {
+    const int32_t* e = esc + e0;
+    const int32_t b_base = __ldg(&base[b]);
 #pragma unroll
-  for (int k = 1; k < 4; ++k) v[k] = c[k] == 0xFFFF ? *e++ : v[0] + (int)c[k];
+    for (int k = 0; k < 4; ++k) {
+      const bool wide = (flag >> k) & 1;
+      const bool escaped = raw[k] == (wide ? 0xFFFFu : 0xFFu);
+      v[k] = escaped ? __ldg(e++) : (k ? v[0] : b_base) + (int)raw[k];
+      ok = ok && v[k] >= 0 && v[k] < V;
+    }
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const int d = (int16_t)c[4 + k];
-    n[k] = d == -32768 ? -1 : (d == 32767 ? *e++ : (int)(t + d));
+    for (int k = 0; k < 4; ++k) {
+      const bool wide = (flag >> (4 + k)) & 1;
+      const int sv = wide ? (int)(int16_t)raw[4 + k] : (int)(int8_t)raw[4 + k];
+      const int lo = wide ? -32768 : -128, hi = wide ? 32767 : 127;
+      const int64_t m = sv == lo ? -1 : (sv == hi ? (int64_t)__ldg(e++) : t + sv);
+      ok = ok && m >= -1 && m < T;
+      n[k] = (int)m;
+    }
+  }
+  if (!ok) {
+    atomicAdd(err, 1ull);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] = 0, n[k] = -1;
   }
   tet_v[t] = make_int4(v[0], v[1], v[2], v[3]);
   tet_n[t] = make_int4(n[0], n[1], n[2], n[3]);
@@ -976,7 +1028,9 @@ int dtfe_gpu_create(const dtfe_config* cfg, dtfe_handle* out) {
     delete h;
     return set_error(DTFE_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
   }
-  int rc = dev_alloc(h, &h->counters, CNT_N);
+  int rc = dev_alloc(h, &h->counters, CNT_N + 1);
+  if (!rc && cudaMemsetAsync(h->counters, 0, sizeof(unsigned long long) * (CNT_N + 1), h->stream) != cudaSuccess)
+    rc = set_error(DTFE_ERR_CUDA, "clearing the status counters");
   if (rc) {
     cudaEventDestroy(h->ev_h2d);
     cudaStreamDestroy(h->stream);
@@ -1070,6 +1124,7 @@ static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const fl
   DTFE_CUDA_TRY(cudaEventRecord(h->ev_h2d, st));
   // then the kernels: decode the tetrahedra, pack positions and velocities
   // into 16-byte records
+  DTFE_CUDA_TRY(cudaMemsetAsync(h->counters + CNT_DECODE, 0, sizeof(unsigned long long), st));
   if (n_tets && (rc = tets_finish(h, stage))) return rc;
   if (n_verts) {
     k_pack_xyz<<<blocks_for(n_verts, 256), 256, 0, st>>>(n_verts, sx, h->posd, 0.f);
@@ -1122,14 +1177,18 @@ int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n, i
 
 int dtfe_gpu_upload_packed(dtfe_handle h, const void* packed, int64_t packed_bytes, const float* xyz,
                            const float* w, const float* vel, const float* scal, int64_t n_verts) {
-  // header: magic, T, n_blocks, n_escapes, offsets of base, escape offsets, codes, escapes
-  int64_t hd[8];
+  // header: magic "DTP2", T, n_blocks, n_escapes, then the byte offsets of
+  // block bases, escape prefix, block byte offsets, flags, data, escapes
+  int64_t hd[10];
   if (!packed || packed_bytes < (int64_t)sizeof(hd)) return set_error(DTFE_ERR_ARG, "null or short packed buffer");
   std::memcpy(hd, packed, sizeof(hd));
-  const int64_t T = hd[1], nb = hd[2];
-  if (hd[0] != 0x31505444 || T < 0 || nb != (T + kPackBlock - 1) / kPackBlock || hd[7] + 4 * hd[3] > packed_bytes ||
-      hd[6] + 16 * T > packed_bytes)
-    return set_error(DTFE_ERR_ARG, "not a packed tessellation (dtfe_tets_pack)");
+  const int64_t T = hd[1], nb = hd[2], n_esc = hd[3];
+  bool ok = hd[0] == 0x32505444 && T >= 0 && nb == (T + kPackBlock - 1) / kPackBlock && n_esc >= 0 &&
+            hd[4] >= (int64_t)sizeof(hd) && hd[5] >= hd[4] + 4 * nb && hd[6] >= hd[5] + 4 * (nb + 1) &&
+            hd[7] >= hd[6] + 8 * (nb + 1) && hd[8] >= hd[7] + T && hd[9] >= hd[8] &&
+            hd[9] + 4 * n_esc <= packed_bytes;
+  for (int k = 4; k < 10; ++k) ok = ok && hd[k] % 16 == 0;
+  if (!ok) return set_error(DTFE_ERR_ARG, "not a packed tessellation (dtfe_tets_pack)");
   return upload_impl(
       h, T, xyz, w, vel, scal, n_verts, (size_t)packed_bytes,
       [&](dtfe_handle hh, char* dev) -> int {
@@ -1138,8 +1197,9 @@ int dtfe_gpu_upload_packed(dtfe_handle h, const void* packed, int64_t packed_byt
       },
       [&](dtfe_handle hh, char* dev) -> int {
         k_unpack_tets<<<(unsigned)nb, kPackBlock, 0, hh->stream>>>(
-            T, (const int32_t*)(dev + hd[4]), (const int32_t*)(dev + hd[5]), (const uint4*)(dev + hd[6]),
-            (const int32_t*)(dev + hd[7]), hh->tet_v, hh->tet_n);
+            T, n_verts, (const int32_t*)(dev + hd[4]), (const int32_t*)(dev + hd[5]),
+            (const int64_t*)(dev + hd[6]), (const uint8_t*)(dev + hd[7]), (const uint32_t*)(dev + hd[8]),
+            hd[9] - hd[8], (const int32_t*)(dev + hd[9]), n_esc, hh->tet_v, hh->tet_n, hh->counters + CNT_DECODE);
         DTFE_CUDA_TRY(cudaGetLastError());
         return DTFE_OK;
       });
@@ -1340,7 +1400,7 @@ static int interp_enqueue(dtfe_handle h, const dtfe_interp_opts* o, float* const
 
 static int read_status(dtfe_handle h, dtfe_status* status) {
   cudaStream_t st = h->stream;
-  unsigned long long cnt[CNT_N];
+  unsigned long long cnt[CNT_N + 1];
   DTFE_CUDA_TRY(cudaMemcpyAsync(cnt, h->counters, sizeof(cnt), cudaMemcpyDeviceToHost, st));
   DTFE_CUDA_TRY(cudaStreamSynchronize(st));
   if (status) {
@@ -1351,6 +1411,7 @@ static int read_status(dtfe_handle h, dtfe_status* status) {
     status->n_exact_tests = (int64_t)cnt[CNT_EXACT];
     status->n_ties = (int64_t)cnt[CNT_TIES];
   }
+  if (cnt[CNT_DECODE]) return set_error(DTFE_ERR_ARG, "packed tessellation did not decode (malformed buffer)");
   if (cnt[CNT_FAIL]) return set_error(DTFE_ERR_WALK, "point-location walk hit its step limit");
   return DTFE_OK;
 }

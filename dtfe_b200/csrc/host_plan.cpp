@@ -322,55 +322,61 @@ void dtfe_axis_coords(float lo, float dx, int64_t n, float* out) {
 // ---- packed tessellation (dtfe_tets_pack / dtfe_tets_unpack) ----------------
 // The flat arrays are mostly small differences: with Morton-ordered
 // vertices and tetrahedra (and the smallest vertex first in every
-// tetrahedron) a tetrahedron's vertices lie within 2^16 of its first one, its
-// first vertex within 2^16 of the smallest first vertex of its block of 256,
-// and its neighbours within 2^15 of itself.  Packed, a tetrahedron takes 16
-// bytes instead of 32, which halves what crosses PCIe.  Layout:
-//   header          8 x int64: magic, T, n_blocks, n_escapes, and the byte
-//                   offsets of block_base, block_esc, codes, escapes
-//   block_base      int32 per block of 256: smallest first vertex
-//   block_esc       int32 per block + 1: escapes before the block
-//   codes           8 x uint16 per tetrahedron: v0 - base, v1 - v0,
-//                   v2 - v0, v3 - v0 (0xFFFF: escaped); n_k - t as int16
-//                   (-32768: no neighbour, 32767: escaped)
-//   escapes         int32 values of the escaped fields, in (tetrahedron,
-//                   field) order
+// tetrahedron) a tetrahedron's vertices lie close to its first one, its first
+// vertex close to the smallest first vertex of its block of 256, and its
+// neighbours close to itself.  Every one of a tetrahedron's 8 fields (first
+// vertex - block base, three vertex offsets, four neighbour deltas) takes 1
+// or 2 bytes, a flag bit per field says which; values that fit neither are
+// escaped to a 32-bit list.  About 10-11 bytes per tetrahedron instead of 32.
+// Layout:
+//   header       10 x int64: magic, T, n_blocks, n_escapes, and the byte
+//                offsets of block_base, block_esc, block_off, flags, data, escapes
+//   block_base   int32 per block: smallest first vertex of its tetrahedra
+//   block_esc    int32 per block + 1: escapes before the block
+//   block_off    int64 per block + 1: byte offset of the block in data
+//   flags        uint8 per tetrahedron: bit f set = field f takes 2 bytes
+//   data         the fields, tetrahedron after tetrahedron, little endian:
+//                vertex fields unsigned (all ones: escaped), neighbour
+//                fields signed (minimum: no neighbour, maximum: escaped)
+//   escapes      int32 values of the escaped fields, in (tetrahedron, field)
+//                order
 namespace {
 constexpr int64_t kPackBlock = 256;
-constexpr int64_t kPackMagic = 0x31505444;  // "DTP1"
-constexpr uint16_t kVEsc = 0xFFFF;
-constexpr int16_t kNHull = -32768, kNEsc = 32767;
+constexpr int64_t kPackMagic = 0x32505444;  // "DTP2"
 
 struct PackHeader {
-  int64_t magic, T, n_blocks, n_esc, off_base, off_esc, off_codes, off_escapes;
+  int64_t magic, T, n_blocks, n_esc, off_base, off_esc, off_boff, off_flags, off_data, off_escapes;
 };
 
 inline size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
 
-// Codes of one tetrahedron; escaped values appended to esc (if non-null),
-// returns the number of escapes.
-inline int encode_tet(int64_t t, const int32_t* v, const int32_t* n, int32_t base, uint16_t c[8],
-                      int32_t* esc) {
-  int ne = 0;
-  auto put_esc = [&](int32_t x) {
-    if (esc) esc[ne] = x;
-    ++ne;
+struct TetCode {
+  uint8_t flag;
+  int nbytes, nesc;
+  uint16_t val[8];   // field codes (1 or 2 bytes each)
+  int32_t esc[8];
+};
+
+// Field codes of one tetrahedron against block base `base`.
+inline void encode_tet(int64_t t, const int32_t* v, const int32_t* n, int32_t base, TetCode& c) {
+  c.flag = 0;
+  c.nbytes = 0;
+  c.nesc = 0;
+  auto unsigned_field = [&](int f, int64_t o, int32_t full) {
+    if (o >= 0 && o < 0xFF) { c.val[f] = (uint16_t)o; c.nbytes += 1; }
+    else if (o >= 0 && o < 0xFFFF) { c.val[f] = (uint16_t)o; c.flag |= (uint8_t)(1u << f); c.nbytes += 2; }
+    else { c.val[f] = 0xFF; c.nbytes += 1; c.esc[c.nesc++] = full; }
   };
-  const int64_t o0 = (int64_t)v[0] - base;
-  if (o0 >= 0 && o0 < kVEsc) c[0] = (uint16_t)o0;
-  else { c[0] = kVEsc; put_esc(v[0]); }
-  for (int k = 1; k < 4; ++k) {
-    const int64_t o = (int64_t)v[k] - v[0];
-    if (o >= 0 && o < kVEsc) c[k] = (uint16_t)o;
-    else { c[k] = kVEsc; put_esc(v[k]); }
-  }
+  unsigned_field(0, (int64_t)v[0] - base, v[0]);
+  for (int k = 1; k < 4; ++k) unsigned_field(k, (int64_t)v[k] - v[0], v[k]);
   for (int k = 0; k < 4; ++k) {
-    if (n[k] < 0) { c[4 + k] = (uint16_t)kNHull; continue; }
+    const int f = 4 + k;
+    if (n[k] < 0) { c.val[f] = (uint16_t)(uint8_t)(int8_t)-128; c.nbytes += 1; continue; }
     const int64_t d = (int64_t)n[k] - t;
-    if (d >= -32767 && d <= 32766) c[4 + k] = (uint16_t)(int16_t)d;
-    else { c[4 + k] = (uint16_t)kNEsc; put_esc(n[k]); }
+    if (d >= -127 && d <= 126) { c.val[f] = (uint16_t)(uint8_t)(int8_t)d; c.nbytes += 1; }
+    else if (d >= -32767 && d <= 32766) { c.val[f] = (uint16_t)(int16_t)d; c.flag |= (uint8_t)(1u << f); c.nbytes += 2; }
+    else { c.val[f] = 127; c.nbytes += 1; c.esc[c.nesc++] = n[k]; }
   }
-  return ne;
 }
 }  // namespace
 
@@ -383,18 +389,28 @@ int64_t dtfe_tets_pack(const int32_t* tet_v, const int32_t* tet_n, int64_t T, vo
   if (T < 0 || (T > 0 && (!tet_v || !tet_n))) return -1;
   const int64_t nb = (T + kPackBlock - 1) / kPackBlock;
   std::vector<int32_t> base(nb), cnt(nb + 1, 0);
+  std::vector<int64_t> boff(nb + 1, 0);
 #pragma omp parallel for schedule(static)
   for (int64_t b = 0; b < nb; ++b) {
     const int64_t t0 = b * kPackBlock, t1 = std::min(T, t0 + kPackBlock);
     int32_t m = tet_v[4 * t0];
     for (int64_t t = t0; t < t1; ++t) m = std::min(m, tet_v[4 * t]);
     base[b] = m;
-    int c = 0;
-    uint16_t codes[8];
-    for (int64_t t = t0; t < t1; ++t) c += encode_tet(t, tet_v + 4 * t, tet_n + 4 * t, m, codes, nullptr);
-    cnt[b + 1] = c;
+    int ne = 0;
+    int64_t bytes = 0;
+    TetCode c;
+    for (int64_t t = t0; t < t1; ++t) {
+      encode_tet(t, tet_v + 4 * t, tet_n + 4 * t, m, c);
+      ne += c.nesc;
+      bytes += c.nbytes;
+    }
+    cnt[b + 1] = ne;
+    boff[b + 1] = bytes;
   }
-  for (int64_t b = 0; b < nb; ++b) cnt[b + 1] += cnt[b];
+  for (int64_t b = 0; b < nb; ++b) {
+    cnt[b + 1] += cnt[b];
+    boff[b + 1] += boff[b];
+  }
   PackHeader hd;
   hd.magic = kPackMagic;
   hd.T = T;
@@ -402,21 +418,36 @@ int64_t dtfe_tets_pack(const int32_t* tet_v, const int32_t* tet_n, int64_t T, vo
   hd.n_esc = cnt[nb];
   hd.off_base = (int64_t)align16(sizeof(PackHeader));
   hd.off_esc = hd.off_base + (int64_t)align16(sizeof(int32_t) * nb);
-  hd.off_codes = hd.off_esc + (int64_t)align16(sizeof(int32_t) * (nb + 1));
-  hd.off_escapes = hd.off_codes + (int64_t)align16(sizeof(uint16_t) * 8 * T);
+  hd.off_boff = hd.off_esc + (int64_t)align16(sizeof(int32_t) * (nb + 1));
+  hd.off_flags = hd.off_boff + (int64_t)align16(sizeof(int64_t) * (nb + 1));
+  hd.off_data = hd.off_flags + (int64_t)align16((size_t)T);
+  hd.off_escapes = hd.off_data + (int64_t)align16((size_t)boff[nb] + 16);
   const int64_t total = hd.off_escapes + (int64_t)align16(sizeof(int32_t) * hd.n_esc);
   if (!out) return total;
   char* o = (char*)out;
+  std::memset(o, 0, (size_t)total);
   std::memcpy(o, &hd, sizeof(hd));
   std::memcpy(o + hd.off_base, base.data(), sizeof(int32_t) * nb);
   std::memcpy(o + hd.off_esc, cnt.data(), sizeof(int32_t) * (nb + 1));
-  uint16_t* codes = (uint16_t*)(o + hd.off_codes);
+  std::memcpy(o + hd.off_boff, boff.data(), sizeof(int64_t) * (nb + 1));
+  uint8_t* flags = (uint8_t*)(o + hd.off_flags);
+  uint8_t* data = (uint8_t*)(o + hd.off_data);
   int32_t* esc = (int32_t*)(o + hd.off_escapes);
 #pragma omp parallel for schedule(static)
   for (int64_t b = 0; b < nb; ++b) {
     const int64_t t0 = b * kPackBlock, t1 = std::min(T, t0 + kPackBlock);
+    uint8_t* d = data + boff[b];
     int32_t* e = esc + cnt[b];
-    for (int64_t t = t0; t < t1; ++t) e += encode_tet(t, tet_v + 4 * t, tet_n + 4 * t, base[b], codes + 8 * t, e);
+    TetCode c;
+    for (int64_t t = t0; t < t1; ++t) {
+      encode_tet(t, tet_v + 4 * t, tet_n + 4 * t, base[b], c);
+      flags[t] = c.flag;
+      for (int f = 0; f < 8; ++f) {
+        *d++ = (uint8_t)(c.val[f] & 0xFF);
+        if (c.flag >> f & 1) *d++ = (uint8_t)(c.val[f] >> 8);
+      }
+      for (int q = 0; q < c.nesc; ++q) *e++ = c.esc[q];
+    }
   }
   return total;
 }
@@ -431,18 +462,33 @@ int dtfe_tets_unpack(const void* packed, int64_t bytes, int32_t* tet_v, int32_t*
   const char* p = (const char*)packed;
   const int32_t* base = (const int32_t*)(p + hd.off_base);
   const int32_t* cnt = (const int32_t*)(p + hd.off_esc);
-  const uint16_t* codes = (const uint16_t*)(p + hd.off_codes);
+  const int64_t* boff = (const int64_t*)(p + hd.off_boff);
+  const uint8_t* flags = (const uint8_t*)(p + hd.off_flags);
+  const uint8_t* data = (const uint8_t*)(p + hd.off_data);
   const int32_t* esc = (const int32_t*)(p + hd.off_escapes);
   for (int64_t b = 0; b < hd.n_blocks; ++b) {
+    const uint8_t* d = data + boff[b];
     const int32_t* e = esc + cnt[b];
     for (int64_t t = b * kPackBlock; t < std::min(hd.T, (b + 1) * kPackBlock); ++t) {
-      const uint16_t* c = codes + 8 * t;
+      uint32_t raw[8];
+      bool wide[8];
+      for (int f = 0; f < 8; ++f) {
+        wide[f] = flags[t] >> f & 1;
+        raw[f] = *d++;
+        if (wide[f]) raw[f] |= (uint32_t)(*d++) << 8;
+      }
       int32_t* v = tet_v + 4 * t;
-      v[0] = c[0] == kVEsc ? *e++ : base[b] + (int32_t)c[0];
-      for (int k = 1; k < 4; ++k) v[k] = c[k] == kVEsc ? *e++ : v[0] + (int32_t)c[k];
+      auto uval = [&](int f, int32_t ref) -> int32_t {
+        const bool escaped = wide[f] ? raw[f] == 0xFFFF : raw[f] == 0xFF;
+        return escaped ? *e++ : ref + (int32_t)raw[f];
+      };
+      v[0] = uval(0, base[b]);
+      for (int k = 1; k < 4; ++k) v[k] = uval(k, v[0]);
       for (int k = 0; k < 4; ++k) {
-        const int16_t d = (int16_t)c[4 + k];
-        tet_n[4 * t + k] = d == kNHull ? -1 : (d == kNEsc ? *e++ : (int32_t)(t + d));
+        const int f = 4 + k;
+        const int32_t sv = wide[f] ? (int32_t)(int16_t)raw[f] : (int32_t)(int8_t)raw[f];
+        const int32_t lo = wide[f] ? -32768 : -128, hi = wide[f] ? 32767 : 127;
+        tet_n[4 * t + k] = sv == lo ? -1 : (sv == hi ? *e++ : (int32_t)(t + sv));
       }
     }
   }

@@ -43,12 +43,14 @@ void dtfe_tess_sizes(void* handle, int64_t* n_tets, int64_t* n_points, int64_t* 
 void dtfe_tess_export(void* handle, int32_t* tet_v, int32_t* tet_n, int32_t* vmap);
 void dtfe_tess_release(void* handle);
 
-/* Packed tessellation for the PCIe transfer (dtfe_gpu_upload_packed):
- * 16-bit differences (vertices from the block's smallest first vertex and
- * from the tetrahedron's first vertex, neighbours from the tetrahedron's own
- * id) with 32-bit escapes.  out == NULL returns the size in bytes;
- * otherwise writes the buffer and returns its size (negative: bad
- * arguments).  dtfe_tets_unpack restores the arrays (0 on success). */
+/* Packed tessellation for the PCIe transfer (dtfe_gpu_upload_packed), about
+ * 11 bytes per tetrahedron instead of 32: per tetrahedron a flag byte and
+ * eight 1- or 2-byte fields (first vertex from the smallest first vertex of
+ * its block of 256, the other vertices from the first, neighbours from the
+ * tetrahedron's own id), values that fit neither escaped to 32 bits.
+ * out == NULL returns the size in bytes; otherwise writes the buffer and
+ * returns its size (negative: bad arguments).  dtfe_tets_unpack restores
+ * the arrays (0 on success, 1 for a malformed buffer). */
 int64_t dtfe_tets_pack(const int32_t* tet_v, const int32_t* tet_n, int64_t T, void* out);
 int dtfe_tets_unpack(const void* packed, int64_t bytes, int32_t* tet_v, int32_t* tet_n);
 

@@ -72,3 +72,32 @@ def test_async_double_buffered_matches_sync(gpu_built):
             d.chain_uploads(None)
         for d in devs:
             d.close()
+
+
+def test_packed_malformed_is_reported(gpu_built):
+    """A packed buffer whose block sizes no longer add up (one flag byte
+    changed) or whose header is not a packed tessellation is refused: the
+    host rejects a bad header at upload, the device decoder's own bounds
+    checks count the bad block and the next status read raises."""
+    from dtfe_b200 import _native as N
+    from dtfe_b200.device import DeviceDTFE
+    pos, _ = S.zeldovich_lattice(12, 100.0, 1.0, seed=14)
+    plan = P.make_plan(pos, np.ones(len(pos), np.float32), None, None, grid=(12, 12, 12), n_threads=2)
+    packed = P.pack_tets(plan.tet_v, plan.tet_n)
+    hd = packed[:80].view(np.int64)
+    with DeviceDTFE(0) as dev:
+        bad = packed.copy()
+        bad[:8].view(np.int64)[0] = 0x31505444     # an older magic
+        with pytest.raises(N.DTFEError):
+            dev.upload_packed(plan, bad)
+        bad = packed.copy()
+        bad[int(hd[7]) + 3] ^= 0x01               # a flag byte of block 0: its bytes no longer add up
+        dev.upload_packed(plan, bad)
+        dev.set_subboxes(plan)
+        dev.vertex_density(plan.rho_bar)
+        with pytest.raises(N.DTFEError, match="did not decode"):
+            dev.interpolate(["density"], method=0)
+        # a good upload clears it
+        dev.upload_packed(plan, packed)
+        dev.vertex_density(plan.rho_bar)
+        dev.interpolate(["density"], method=0)

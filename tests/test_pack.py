@@ -28,3 +28,22 @@ def test_pack_roundtrip_escapes(built):
     e = P.pack_tets(np.zeros((0, 4), np.int32), np.zeros((0, 4), np.int32))
     a, b = P.unpack_tets(e, 0)
     assert a.shape == (0, 4)
+
+
+def test_pack_layout_header(built):
+    """The header's offsets are 16-byte aligned and in order, the format the
+    device decoder checks before a packed upload."""
+    pos, _ = S.zeldovich_lattice(10, 100.0, 1.0, seed=4)
+    plan = P.make_plan(pos, np.ones(len(pos), np.float32), None, None, grid=(10, 10, 10), n_threads=2)
+    packed = P.pack_tets(plan.tet_v, plan.tet_n)
+    hd = packed[:80].view(np.int64)
+    T, nb, ne = int(hd[1]), int(hd[2]), int(hd[3])
+    assert hd[0] == 0x32505444 and T == plan.n_tets and nb == (T + 255) // 256
+    off = [int(x) for x in hd[4:10]]
+    assert all(o % 16 == 0 for o in off) and off == sorted(off)
+    assert off[-1] + 4 * ne <= packed.nbytes
+    flags = packed[off[3]:off[3] + T]
+    boff = packed[off[2]:off[2] + 8 * (nb + 1)].view(np.int64)
+    sizes = 8 + np.unpackbits(flags[:, None], axis=1).sum(1)
+    per_block = np.add.reduceat(sizes, np.arange(0, T, 256))
+    assert np.array_equal(np.diff(boff), per_block)

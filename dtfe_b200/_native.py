@@ -45,7 +45,8 @@ class PlanView(C.Structure):
                 ("n_verts", C.c_int64), ("n_tets", C.c_int64), ("n_boxes", C.c_int32), ("n_scalars", C.c_int32),
                 ("tet_v", C.c_void_p), ("tet_n", C.c_void_p), ("xyz", C.c_void_p), ("src", C.c_void_p),
                 ("weight", C.c_void_p), ("velocity", C.c_void_p), ("scalar", C.c_void_p),
-                ("boxes", C.c_void_p), ("xs", C.c_void_p), ("ys", C.c_void_p), ("zs", C.c_void_p),
+                ("boxes", C.c_void_p), ("regions", C.c_void_p), ("xs", C.c_void_p), ("ys", C.c_void_p),
+                ("zs", C.c_void_p),
                 ("n_xs", C.c_int64), ("n_ys", C.c_int64), ("n_zs", C.c_int64),
                 ("n_particles", C.c_int64), ("dep_pos", C.c_void_p), ("dep_weight", C.c_void_p),
                 ("dep_velocity", C.c_void_p), ("dep_src", C.c_void_p), ("n_dep_boxes", C.c_int32),

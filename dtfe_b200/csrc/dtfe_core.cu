@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <map>
 #include <cstring>
@@ -56,8 +57,12 @@ int set_error(int code, const std::string& msg) {
 constexpr int64_t kMaxCells = 0x7FFFFFFF;  // cell keys are int32
 enum { CNT_LOCATED, CNT_OUTSIDE, CNT_FAIL, CNT_STEPS, CNT_EXACT, CNT_TIES, CNT_N };
 // after the per-step counters, kept across steps: tetrahedra a packed upload
-// could not decode (cleared by every upload)
+// could not decode (cleared by every upload); exact orientation tests and
+// boundary hits of the centre raster (cleared by every raster)
 constexpr int CNT_DECODE = CNT_N;
+constexpr int CNT_RASTER_EXACT = CNT_N + 1;
+constexpr int CNT_RASTER_TIES = CNT_N + 2;
+constexpr int CNT_ALL = CNT_N + 3;
 
 // ---------------------------------------------------------------------------
 __global__ void k_pack_xyz(int64_t n, const float* __restrict__ xyz, float4* __restrict__ out, float wval) {
@@ -390,6 +395,129 @@ __global__ void __launch_bounds__(kVolBlock) k_tet_volume_bins(
   }
 }
 
+// Signed FP64 volume of every tetrahedron (as k_tet_volume_bins) and the
+// location of every cell centre, without a walk: a centre lies in the closure
+// of a tetrahedron only inside its bounding box, so each thread finds the
+// centres of its sub-box's tile in its box (index ranges from the tile's
+// raster formula x_i = lo + (i + 1/2) dx, widened by the largest deviation of
+// the coordinate tables from it, measured on the host: conservative), the
+// block scans its threads' counts and its 256 threads test the block's
+// candidates in turn (owner by binary search over the scan) with the exact
+// orientation predicates.  Every tetrahedron whose closure holds the centre
+// takes part in an atomicMin on its slot (preset to 0xFFFFFFFF = outside),
+// which leaves the lowest such id: the canonical tie rule.
+constexpr int kRasterBlock = 256;
+struct RasterAxis {
+  double lo, inv_dx, margin;
+};
+template <int MINB>
+__global__ void __launch_bounds__(kRasterBlock, MINB) k_tet_volume_raster(
+    int64_t T, const int4* __restrict__ tet_v, const float4* __restrict__ posd, double* __restrict__ vol,
+    const dtfe_subbox* __restrict__ boxes, const int64_t* __restrict__ tprefix,
+    const int64_t* __restrict__ tile_prefix, const RasterAxis* __restrict__ axes, int K,
+    const float* __restrict__ xs, const float* __restrict__ ys, const float* __restrict__ zs,
+    unsigned* __restrict__ tet_c, unsigned long long* __restrict__ counters) {
+  __shared__ float s_X[kRasterBlock][13];
+  __shared__ int s_meta[kRasterBlock][7];  // i0, j0, k0, nj, nk, box, tetrahedron
+  __shared__ long long s_scan[kRasterBlock];
+  __shared__ long long s_warp[kRasterBlock / 32];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int64_t t = blockIdx.x * (int64_t)kRasterBlock + tid;
+  long long cnt = 0;
+  if (t < T) {
+    int4 q = __ldg(&tet_v[t]);
+    int v[4] = {q.x, q.y, q.z, q.w};
+    float X[4][3];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) load_posf(posd, v[a], X[a]);
+    double D[4][3];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) D[a][c] = (double)X[a][c];
+    vol[t] = orient_det(D[0], D[1], D[2], D[3]) / 6.0;
+    if (t >= __ldg(&tprefix[0]) && t < __ldg(&tprefix[K])) {
+      const int b = find_box(tprefix, K, t);
+      int r0[3], nr[3];
+      cnt = 1;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float lo = fminf(fminf(X[0][c], X[1][c]), fminf(X[2][c], X[3][c]));
+        const float hi = fmaxf(fmaxf(X[0][c], X[1][c]), fmaxf(X[2][c], X[3][c]));
+        const RasterAxis A = axes[3 * b + c];
+        const double n = (double)__ldg(&boxes[b].tile_dims[c]);
+        const double f0 = fmax(ceil(((double)lo - A.lo) * A.inv_dx - 0.5 - A.margin), 0.0);
+        const double f1 = fmin(floor(((double)hi - A.lo) * A.inv_dx - 0.5 + A.margin), n - 1.0);
+        r0[c] = f1 >= f0 ? (int)f0 : 0;
+        nr[c] = f1 >= f0 ? (int)(f1 - f0) + 1 : 0;
+        cnt *= nr[c];
+      }
+      if (cnt) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) s_X[tid][3 * a + c] = X[a][c];
+        s_meta[tid][0] = r0[0];
+        s_meta[tid][1] = r0[1];
+        s_meta[tid][2] = r0[2];
+        s_meta[tid][3] = nr[1];
+        s_meta[tid][4] = nr[2];
+        s_meta[tid][5] = b;
+        s_meta[tid][6] = (int)t;
+      }
+    }
+  }
+  // inclusive block scan of the candidate counts
+  long long inc = cnt;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const long long y = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= d) inc += y;
+  }
+  if (lane == 31) s_warp[wid] = inc;
+  __syncthreads();
+  long long before = 0;
+#pragma unroll
+  for (int w = 0; w < kRasterBlock / 32; ++w) before += w < wid ? s_warp[w] : 0;
+  s_scan[tid] = before + inc;
+  __syncthreads();
+  const long long total = s_scan[kRasterBlock - 1];
+  int nexact = 0, nties = 0;
+  for (long long qi = tid; qi < total; qi += kRasterBlock) {
+    int lo = 0, hi = kRasterBlock - 1;  // first owner with s_scan > qi
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (s_scan[mid] > qi) hi = mid;
+      else lo = mid + 1;
+    }
+    const int o = lo;
+    const int local = (int)(qi - (o ? s_scan[o - 1] : 0));
+    const int nj = s_meta[o][3], nk = s_meta[o][4], b = s_meta[o][5];
+    const int k = s_meta[o][2] + local % nk;
+    const int j = s_meta[o][1] + (local / nk) % nj;
+    const int i = s_meta[o][0] + local / (nk * nj);
+    const dtfe_subbox& B = boxes[b];
+    const float pf[3] = {__ldg(&xs[B.coord_offset[0] + i]), __ldg(&ys[B.coord_offset[1] + j]),
+                         __ldg(&zs[B.coord_offset[2] + k])};
+    float X[4][3];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) X[a][c] = s_X[o][3 * a + c];
+    int zmask;
+    if (first_exit_face_f32(X, pf, 15, zmask, nexact) < 0) {
+      const int64_t slot =
+          __ldg(&tile_prefix[b]) + ((int64_t)i * __ldg(&B.tile_dims[1]) + j) * __ldg(&B.tile_dims[2]) + k;
+      atomicMin(&tet_c[slot], (unsigned)s_meta[o][6]);
+      nties += zmask != 0;
+    }
+  }
+  const unsigned re = __reduce_add_sync(0xffffffffu, (unsigned)nexact);
+  const unsigned rt = __reduce_add_sync(0xffffffffu, (unsigned)nties);
+  if (lane == 0 && re) atomicAdd(&counters[0], (unsigned long long)re);
+  if (lane == 0 && rt) atomicAdd(&counters[1], (unsigned long long)rt);
+}
+
 // rho_v = (w * factor) / sum of incident volumes, summed in ascending
 // tetrahedron order; 0 on the hull or without incident tetrahedra.  A warp
 // handles 32 consecutive vertices, whose incidence lists are contiguous: it
@@ -455,6 +583,7 @@ struct InterpParams {
   uint32_t fields;
   int fix;
   int max_steps;
+  int count_centres;  // the centres were placed by the raster: the evaluation counts them
   float* out[DTFE_NUM_FIELDS];
   unsigned long long* counters;
 };
@@ -600,6 +729,7 @@ __global__ void __launch_bounds__(kInterpBlock, MINB) k_eval_centre(InterpParams
   const bool fix = P.fix != 0;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t base0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane;
+  unsigned n_loc = 0, n_out = 0;  // centres placed by the raster
   for (int64_t base = base0; base < P.n_total; base += stride) {
     const int64_t s = base + lane;
     const bool valid = s < P.n_total;
@@ -620,6 +750,8 @@ __global__ void __launch_bounds__(kInterpBlock, MINB) k_eval_centre(InterpParams
       const SampleCell c = sample_cell(P, s);
       cell = c.cell;
       const int t = __ldg(&tet_c[s]);
+      n_loc += 1;
+      n_out += t < 0;
       if (t >= 0) {
         int v[4];
         float X[4][3];
@@ -650,6 +782,7 @@ __global__ void __launch_bounds__(kInterpBlock, MINB) k_eval_centre(InterpParams
     if (S > 0 && has_field(F, DTFE_SCALAR_GRADIENT))
       store_field<(S > 0 ? 3 * S : 1)>(P.out[DTFE_SCALAR_GRADIENT], cell, valid, e.scg, contig, c0, stage);
   }
+  if (P.count_centres) fold_counters(P, n_loc, n_out, 0, WalkStats{0, 0, 0});
 }
 
 // Cell averages (methods 2 and 3): n points per cell, each walked from the
@@ -671,7 +804,7 @@ __global__ void __launch_bounds__(kInterpBlock) k_average(InterpParams P, const 
   const bool want_std = METHOD == DTFE_METHOD_MONTE_CARLO && has_field(F, DTFE_VELOCITY_STD);
   const bool fix = P.fix != 0;
   WalkStats st{0, 0, 0};
-  unsigned n_loc = 0, n_fail = 0;
+  unsigned n_loc = 0, n_fail = 0, n_out_c = 0;
 
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t base0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane;
@@ -694,6 +827,10 @@ __global__ void __launch_bounds__(kInterpBlock) k_average(InterpParams P, const 
       cell = c.cell;
       const double pc[3] = {(double)c.x, (double)c.y, (double)c.z};
       const int tc = __ldg(&tet_c[s]);
+      if (P.count_centres) {
+        ++n_loc;
+        n_out_c += tc < 0;
+      }
       const int tstart = tc >= 0 ? tc : (int)B.tet_offset;
       const int NN = P.NN;
       const uint64_t key = mc_key(P.seed, B.part_no);
@@ -805,7 +942,7 @@ __global__ void __launch_bounds__(kInterpBlock) k_average(InterpParams P, const 
     if (S > 0 && has_field(F, DTFE_SCALAR_GRADIENT))
       store_field<(S > 0 ? 3 * S : 1)>(P.out[DTFE_SCALAR_GRADIENT], cell, valid, aSG, contig, c0, stage);
   }
-  fold_counters(P, n_loc, 0, n_fail, st);
+  fold_counters(P, n_loc, n_out_c, n_fail, st);
 }
 
 // Locate arbitrary points (tests): canonical tetrahedron or -1 / -2.
@@ -859,7 +996,10 @@ struct dtfe_gpu_s {
   int64_t n_cells = 0;
   float *xs = nullptr, *ys = nullptr, *zs = nullptr;
   int32_t grid[3] = {0, 0, 0};
-  bool bins_ready = false;
+  bool prep_ready = false;        // volumes and centre locations (raster) or walk seeds are current
+  bool prep_raster = false;       // ... prepared by the raster
+  int prep_variant = 0;           // ... with this locate variant
+  RasterAxis* raster_axes = nullptr;  // per sub-box and axis: raster formula and its margin
   float* eq_off = nullptr;
   int eq_nn = 0;
   unsigned long long* counters = nullptr;
@@ -935,37 +1075,73 @@ void drop_graph(dtfe_handle h) {
   }
 }
 
-int prepare_bins(dtfe_handle h) {
-  if (h->bins_ready) return DTFE_OK;
-  DTFE_CUDA_TRY(cudaMemsetAsync(h->bins, 0xFF, sizeof(unsigned long long) * h->n_cells, h->stream));
-  if (h->T > 0)
-    k_tet_volume_bins<true><<<blocks_for(h->T, kVolBlock), kVolBlock, 0, h->stream>>>(
-        h->T, h->tet_v, h->posd, h->vol, h->boxes, h->tet_prefix, h->bin_offset, h->K, h->xs, h->ys, h->zs,
-        h->bins);
-  DTFE_CUDA_TRY(cudaGetLastError());
-  h->bins_ready = true;
-  return DTFE_OK;
-}
-
-// Launch variants chosen by dtfe_gpu_autotune: register budget (blocks per
-// SM) and seeding schedule of the locate kernel; register budget of the
-// evaluation kernel.
+// Launch variants chosen by dtfe_gpu_autotune.  Locate variants 0..2 place
+// the cell centres with the raster fused into the volume kernel (3, 2 or 4
+// blocks per SM); variants 3..8 walk from seeds (blocks per SM, samples per
+// thread).  Evaluation variants: register budget of the evaluation kernel.
+constexpr int kNumRasterVariants = 3;
 struct LocVariant { int block, minb, r; };
-constexpr LocVariant kLocVariants[] = {{256, 3, 1}, {256, 2, 1}, {256, 4, 1}, {256, 3, 2}, {256, 4, 2}, {256, 3, 4}};
-constexpr int kNumLocVariants = sizeof(kLocVariants) / sizeof(kLocVariants[0]);
+constexpr LocVariant kWalkVariants[] = {{256, 3, 1}, {256, 2, 1}, {256, 4, 1}, {256, 3, 2}, {256, 4, 2}, {256, 3, 4}};
+constexpr int kNumLocVariants = kNumRasterVariants + sizeof(kWalkVariants) / sizeof(kWalkVariants[0]);
+inline bool is_raster(int loc_variant) { return loc_variant < kNumRasterVariants; }
 constexpr int kEvalMinBlocks[] = {3, 2, 4};
 constexpr int kNumEvalVariants = 3;
 
+// Per step, before the interpolation: tetrahedron volumes and either the
+// cell centres' tetrahedra (raster) or the walk seeds.  Without sub-boxes,
+// volumes only.
+int launch_prep(dtfe_handle h) {
+  cudaStream_t st = h->stream;
+  const bool raster = is_raster(h->loc_variant);
+  DTFE_CUDA_TRY(cudaMemsetAsync(h->counters + CNT_RASTER_EXACT, 0, 2 * sizeof(unsigned long long), st));
+  if (h->K > 0 && raster) {
+    int rc = dev_alloc(h, &h->tet_c, h->n_cells);
+    if (rc) return rc;
+    DTFE_CUDA_TRY(cudaMemsetAsync(h->tet_c, 0xFF, sizeof(int) * h->n_cells, st));
+    if (h->T > 0) {
+      const unsigned nb = blocks_for(h->T, kRasterBlock);
+      auto* k = h->loc_variant == 1 ? k_tet_volume_raster<2>
+                                    : (h->loc_variant == 2 ? k_tet_volume_raster<4> : k_tet_volume_raster<3>);
+      k<<<nb, kRasterBlock, 0, st>>>(h->T, h->tet_v, h->posd, h->vol, h->boxes, h->tet_prefix, h->tile_prefix,
+                                     h->raster_axes, h->K, h->xs, h->ys, h->zs, (unsigned*)h->tet_c,
+                                     h->counters + CNT_RASTER_EXACT);
+    }
+  } else if (h->K > 0) {
+    DTFE_CUDA_TRY(cudaMemsetAsync(h->bins, 0xFF, sizeof(unsigned long long) * h->n_cells, st));
+    if (h->T > 0)
+      k_tet_volume_bins<true><<<blocks_for(h->T, kVolBlock), kVolBlock, 0, st>>>(
+          h->T, h->tet_v, h->posd, h->vol, h->boxes, h->tet_prefix, h->bin_offset, h->K, h->xs, h->ys, h->zs,
+          h->bins);
+  } else if (h->T > 0) {
+    k_tet_volume_bins<false><<<blocks_for(h->T, kVolBlock), kVolBlock, 0, st>>>(
+        h->T, h->tet_v, h->posd, h->vol, h->boxes, h->tet_prefix, h->bin_offset, h->K, h->xs, h->ys, h->zs,
+        h->bins);
+  }
+  DTFE_CUDA_TRY(cudaGetLastError());
+  h->prep_ready = h->K > 0;
+  h->prep_raster = raster;
+  h->prep_variant = h->loc_variant;
+  return DTFE_OK;
+}
+
+int prepare_centres(dtfe_handle h) {
+  if (h->prep_ready && h->prep_raster == is_raster(h->loc_variant) &&
+      (!h->prep_raster || h->prep_variant == h->loc_variant))
+    return DTFE_OK;
+  return launch_prep(h);
+}
+
 void launch_locate(int variant, const InterpParams& P, int* tet_c, cudaStream_t st) {
-  const LocVariant& L = kLocVariants[variant];
+  if (is_raster(variant)) return;
+  const LocVariant& L = kWalkVariants[variant - kNumRasterVariants];
   const int64_t groups = (P.n_total + L.r - 1) / L.r;
   const unsigned grid = (unsigned)((groups + L.block - 1) / L.block);
   switch (variant) {
-    case 0: k_locate_cells<256, 3, 1><<<grid, 256, 0, st>>>(P, tet_c); break;
-    case 1: k_locate_cells<256, 2, 1><<<grid, 256, 0, st>>>(P, tet_c); break;
-    case 2: k_locate_cells<256, 4, 1><<<grid, 256, 0, st>>>(P, tet_c); break;
-    case 3: k_locate_cells<256, 3, 2><<<grid, 256, 0, st>>>(P, tet_c); break;
-    case 4: k_locate_cells<256, 4, 2><<<grid, 256, 0, st>>>(P, tet_c); break;
+    case 3: k_locate_cells<256, 3, 1><<<grid, 256, 0, st>>>(P, tet_c); break;
+    case 4: k_locate_cells<256, 2, 1><<<grid, 256, 0, st>>>(P, tet_c); break;
+    case 5: k_locate_cells<256, 4, 1><<<grid, 256, 0, st>>>(P, tet_c); break;
+    case 6: k_locate_cells<256, 3, 2><<<grid, 256, 0, st>>>(P, tet_c); break;
+    case 7: k_locate_cells<256, 4, 2><<<grid, 256, 0, st>>>(P, tet_c); break;
     default: k_locate_cells<256, 3, 4><<<grid, 256, 0, st>>>(P, tet_c); break;
   }
 }
@@ -1028,8 +1204,8 @@ int dtfe_gpu_create(const dtfe_config* cfg, dtfe_handle* out) {
     delete h;
     return set_error(DTFE_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
   }
-  int rc = dev_alloc(h, &h->counters, CNT_N + 1);
-  if (!rc && cudaMemsetAsync(h->counters, 0, sizeof(unsigned long long) * (CNT_N + 1), h->stream) != cudaSuccess)
+  int rc = dev_alloc(h, &h->counters, CNT_ALL);
+  if (!rc && cudaMemsetAsync(h->counters, 0, sizeof(unsigned long long) * CNT_ALL, h->stream) != cudaSuccess)
     rc = set_error(DTFE_ERR_CUDA, "clearing the status counters");
   if (rc) {
     cudaEventDestroy(h->ev_h2d);
@@ -1049,7 +1225,7 @@ int dtfe_gpu_destroy(dtfe_handle h) {
   void* ptrs[] = {h->tet_v, h->tet_n, h->posd, h->vel4, h->scal, h->w, h->vol, h->inc_off, h->inc,
                   h->scratch_i, h->scan_blocks, h->hull,
                   h->boxes, h->tile_prefix, h->tet_prefix, h->bin_offset, h->bins,
-                  h->xs, h->ys, h->zs, h->eq_off, h->counters, h->tet_c};
+                  h->xs, h->ys, h->zs, h->eq_off, h->counters, h->tet_c, h->raster_axes};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < DTFE_NUM_FIELDS; ++i)
@@ -1154,7 +1330,7 @@ static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const fl
   h->has_vel = vel != nullptr;
   h->has_scal = scal != nullptr;
   h->density_ready = false;
-  h->bins_ready = false;
+  h->prep_ready = false;
   h->tet_c_valid = false;
   drop_graph(h);
   return DTFE_OK;
@@ -1242,8 +1418,26 @@ int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* box
   tprefix[n_boxes] = cells;
   tetpre[n_boxes] = boxes[n_boxes - 1].tet_offset + boxes[n_boxes - 1].n_tets;
   if (cells >= kMaxCells) return set_error(DTFE_ERR_TOO_LARGE, "more than 2^31 grid cells");
+  // raster formula of every tile axis, x_i ~ lo + (i + 1/2) dx, and the
+  // largest deviation of its coordinate table from it (in cells): the
+  // raster's index ranges widened by it cannot miss a centre
+  std::vector<RasterAxis> axes((size_t)3 * n_boxes);
+  for (int b = 0; b < n_boxes; ++b)
+    for (int a = 0; a < 3; ++a) {
+      const dtfe_subbox& B = boxes[b];
+      const float* tab = (a == 0 ? xs : (a == 1 ? ys : zs)) + B.coord_offset[a];
+      RasterAxis& A = axes[3 * b + a];
+      A.lo = (double)B.lo[a];
+      A.inv_dx = 1.0 / (double)B.dx[a];
+      double dev = 0.0;
+      for (int i = 0; i < B.tile_dims[a]; ++i)
+        dev = std::max(dev, std::fabs(((double)tab[i] - A.lo) * A.inv_dx - 0.5 - (double)i));
+      if (!(dev < 1e6)) return set_error(DTFE_ERR_ARG, "coordinate table far from the tile's raster");
+      A.margin = dev + 1e-6;
+    }
   int rc;
-  if ((rc = dev_alloc(h, &h->boxes, n_boxes)) || (rc = dev_alloc(h, &h->tile_prefix, n_boxes + 1)) ||
+  if ((rc = dev_alloc(h, &h->raster_axes, (size_t)3 * n_boxes)) ||
+      (rc = dev_alloc(h, &h->boxes, n_boxes)) || (rc = dev_alloc(h, &h->tile_prefix, n_boxes + 1)) ||
       (rc = dev_alloc(h, &h->tet_prefix, n_boxes + 1)) || (rc = dev_alloc(h, &h->bin_offset, n_boxes)) ||
       (rc = dev_alloc(h, &h->bins, cells)) || (rc = dev_alloc(h, &h->xs, n_xs)) ||
       (rc = dev_alloc(h, &h->ys, n_ys)) || (rc = dev_alloc(h, &h->zs, n_zs)))
@@ -1258,12 +1452,14 @@ int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* box
   DTFE_CUDA_TRY(cudaMemcpyAsync(h->xs, xs, sizeof(float) * n_xs, cudaMemcpyHostToDevice, st));
   DTFE_CUDA_TRY(cudaMemcpyAsync(h->ys, ys, sizeof(float) * n_ys, cudaMemcpyHostToDevice, st));
   DTFE_CUDA_TRY(cudaMemcpyAsync(h->zs, zs, sizeof(float) * n_zs, cudaMemcpyHostToDevice, st));
+  DTFE_CUDA_TRY(cudaMemcpyAsync(h->raster_axes, axes.data(), sizeof(RasterAxis) * axes.size(),
+                                cudaMemcpyHostToDevice, st));
   DTFE_CUDA_TRY(cudaStreamSynchronize(st));  // host vectors go out of scope
   h->K = n_boxes;
   h->boxes_h.assign(boxes, boxes + n_boxes);
   h->n_cells = cells;
   h->grid[0] = grid[0]; h->grid[1] = grid[1]; h->grid[2] = grid[2];
-  h->bins_ready = false;
+  h->prep_ready = false;
   h->eq_nn = 0;
   drop_graph(h);
   return DTFE_OK;
@@ -1275,17 +1471,8 @@ int dtfe_gpu_vertex_density(dtfe_handle h, double rho_bar) {
   if (h->V == 0) return set_error(DTFE_ERR_STATE, "nothing uploaded");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
   cudaStream_t st = h->stream;
-  if (h->K > 0) DTFE_CUDA_TRY(cudaMemsetAsync(h->bins, 0xFF, sizeof(unsigned long long) * h->n_cells, st));
-  if (h->T > 0) {
-    if (h->K > 0)
-      k_tet_volume_bins<true><<<blocks_for(h->T, kVolBlock), kVolBlock, 0, st>>>(
-          h->T, h->tet_v, h->posd, h->vol, h->boxes, h->tet_prefix, h->bin_offset, h->K, h->xs, h->ys, h->zs,
-          h->bins);
-    else
-      k_tet_volume_bins<false><<<blocks_for(h->T, kVolBlock), kVolBlock, 0, st>>>(
-          h->T, h->tet_v, h->posd, h->vol, h->boxes, h->tet_prefix, h->bin_offset, h->K, h->xs, h->ys, h->zs,
-          h->bins);
-  }
+  int rc = launch_prep(h);
+  if (rc) return rc;
   // the reference's factor: (NO_DIM+1.)/averageDensity stored as Real
   float rb = (float)rho_bar;
   float factor = (float)(4.0 / (double)rb);
@@ -1294,7 +1481,6 @@ int dtfe_gpu_vertex_density(dtfe_handle h, double rho_bar) {
                                                                        h->hull, factor, h->posd);
   DTFE_CUDA_TRY(cudaGetLastError());
   h->density_ready = true;
-  h->bins_ready = h->K > 0;
   return DTFE_OK;
 }
 
@@ -1330,7 +1516,7 @@ static int interp_enqueue(dtfe_handle h, const dtfe_interp_opts* o, float* const
     return set_error(DTFE_ERR_ARG, "scalar fields requested but n_scalars == 0");
   for (int s = 0; s < DTFE_NUM_FIELDS; ++s)
     if ((F >> s & 1u) && !out_dev[s]) return set_error(DTFE_ERR_ARG, "missing output buffer");
-  int rc = prepare_bins(h);
+  int rc = prepare_centres(h);
   if (rc) return rc;
   cudaStream_t st = h->stream;
   if (method == DTFE_METHOD_EQUIDISTANT) {
@@ -1381,6 +1567,7 @@ static int interp_enqueue(dtfe_handle h, const dtfe_interp_opts* o, float* const
   P.fields = F;
   P.fix = (o->flags & DTFE_FLAG_FIX_VALUE_INTERP) ? 1 : 0;
   P.max_steps = h->max_steps;
+  P.count_centres = is_raster(h->loc_variant) ? 1 : 0;
   for (int s = 0; s < DTFE_NUM_FIELDS; ++s) P.out[s] = (F >> s & 1u) ? out_dev[s] : nullptr;
   P.counters = h->counters;
   const unsigned block = kInterpBlock;
@@ -1400,7 +1587,7 @@ static int interp_enqueue(dtfe_handle h, const dtfe_interp_opts* o, float* const
 
 static int read_status(dtfe_handle h, dtfe_status* status) {
   cudaStream_t st = h->stream;
-  unsigned long long cnt[CNT_N + 1];
+  unsigned long long cnt[CNT_ALL];
   DTFE_CUDA_TRY(cudaMemcpyAsync(cnt, h->counters, sizeof(cnt), cudaMemcpyDeviceToHost, st));
   DTFE_CUDA_TRY(cudaStreamSynchronize(st));
   if (status) {
@@ -1408,8 +1595,8 @@ static int read_status(dtfe_handle h, dtfe_status* status) {
     status->n_outside = (int64_t)cnt[CNT_OUTSIDE];
     status->n_walk_failures = (int64_t)cnt[CNT_FAIL];
     status->n_walk_steps = (int64_t)cnt[CNT_STEPS];
-    status->n_exact_tests = (int64_t)cnt[CNT_EXACT];
-    status->n_ties = (int64_t)cnt[CNT_TIES];
+    status->n_exact_tests = (int64_t)(cnt[CNT_EXACT] + cnt[CNT_RASTER_EXACT]);
+    status->n_ties = (int64_t)(cnt[CNT_TIES] + cnt[CNT_RASTER_TIES]);
   }
   if (cnt[CNT_DECODE]) return set_error(DTFE_ERR_ARG, "packed tessellation did not decode (malformed buffer)");
   if (cnt[CNT_FAIL]) return set_error(DTFE_ERR_WALK, "point-location walk hit its step limit");
@@ -1443,11 +1630,15 @@ static int autotune_impl(dtfe_handle h, uint32_t fields, int32_t* chosen) {
   cudaEvent_t e0, e1;
   DTFE_CUDA_TRY(cudaEventCreate(&e0));
   DTFE_CUDA_TRY(cudaEventCreate(&e1));
+  // every timed call redoes the per-step preparation (volumes and centre
+  // raster or walk seeds), so that the locate variants compare whole steps
   auto time_call = [&](float* ms) -> int {
+    h->prep_ready = false;
     int rc = interpolate_impl(h, &o, dev, nullptr);  // warm
     if (rc) return rc;
     float best = 1e30f;
     for (int rep = 0; rep < 3; ++rep) {
+      h->prep_ready = false;
       cudaEventRecord(e0, h->stream);
       rc = interpolate_impl(h, &o, dev, nullptr);
       if (rc) return rc;

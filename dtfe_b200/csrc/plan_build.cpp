@@ -24,6 +24,7 @@ struct dtfe_plan_s {
   std::vector<int32_t> tet_v, tet_n, src;
   std::vector<float> xyz, weight, velocity, scalar, xs, ys, zs;
   std::vector<dtfe_subbox> boxes;
+  std::vector<float> regions;  // 6 per sub-box: the tile region (xmin, xmax, ymin, ymax, zmin, zmax)
   std::vector<float> dep_pos, dep_weight, dep_velocity;
   std::vector<int64_t> dep_src;
   std::vector<dtfe_deposit_box> dep_boxes;
@@ -179,6 +180,7 @@ int assemble(dtfe_plan_s& P, std::vector<PointSet>& sets, const std::vector<Tile
   int64_t voff = 0, toff = 0, coff[3] = {0, 0, 0};
   int status = 0;
   P.boxes.resize(k);
+  P.regions.resize(6 * k);
   for (int i = 0; i < k; ++i) {
     int64_t nt = 0, npt = 0, nd = 0;
     if (handles[i]) dtfe_tess_sizes(handles[i], &nt, &npt, &nd);
@@ -196,6 +198,7 @@ int assemble(dtfe_plan_s& P, std::vector<PointSet>& sets, const std::vector<Tile
     P.xyz.insert(P.xyz.end(), sets[i].pos.begin(), sets[i].pos.end());
     P.src.insert(P.src.end(), sets[i].src.begin(), sets[i].src.end());
     const Tile& t = tiles[i];
+    std::memcpy(&P.regions[6 * i], t.region, sizeof(t.region));
     dtfe_subbox& b = P.boxes[i];
     std::memset(&b, 0, sizeof(b));
     b.vert_offset = voff;
@@ -305,6 +308,7 @@ int dtfe_plan_build(int kind, const float* pos, const float* w, const float* vel
   v.velocity = P->velocity.empty() ? nullptr : P->velocity.data();
   v.scalar = P->scalar.empty() ? nullptr : P->scalar.data();
   v.boxes = P->boxes.data();
+  v.regions = P->regions.empty() ? nullptr : P->regions.data();
   v.xs = P->xs.data();
   v.ys = P->ys.data();
   v.zs = P->zs.data();

@@ -46,6 +46,7 @@ class Plan:
     rho_bar: float
     padding: np.ndarray        # (6,) float32
     timings: dict = field(default_factory=dict)
+    regions: np.ndarray | None = None  # (K, 6) float32 tile regions (xmin, xmax, ymin, ymax, zmin, zmax)
 
     @property
     def n_tets(self) -> int:
@@ -58,6 +59,18 @@ class Plan:
     @property
     def n_boxes(self) -> int:
         return len(self.boxes)
+
+    def region_array(self) -> np.ndarray:
+        """(K, 6) float32 tile regions; without stored regions, the upper
+        corners lo + dx * dims of each tile."""
+        if self.regions is not None:
+            return np.ascontiguousarray(self.regions, np.float32).reshape(-1, 6)
+        out = np.empty((self.n_boxes, 6), np.float32)
+        for k, b in enumerate(self.boxes):
+            for a in range(3):
+                out[k, 2 * a] = b.lo[a]
+                out[k, 2 * a + 1] = np.float32(b.lo[a] + b.dx[a] * b.tile_dims[a])
+        return out
 
     @property
     def n_scalars(self) -> int:
@@ -200,7 +213,7 @@ def assemble(sets: list, tiles: list, weight, velocity, scalar, grid, rho_bar, p
     tess = tessellate_many([p for _, p in sets])
     timings["tessellation_s"] = time.time() - t0
     tv_all, tn_all, xyz_all, src_all = [], [], [], []
-    xs, ys, zs = [], [], []
+    xs, ys, zs, regions = [], [], [], []
     boxes = (N.Subbox * len(sets))()
     voff = toff = 0
     coff = [0, 0, 0]
@@ -211,6 +224,7 @@ def assemble(sets: list, tiles: list, weight, velocity, scalar, grid, rho_bar, p
         xyz_all.append(pos)
         src_all.append(src)
         region = np.asarray(region, np.float32)
+        regions.append(region)
         dx = np.empty(3, np.float32)
         for a in range(3):
             length = np.float32(region[2 * a + 1] - region[2 * a])
@@ -234,7 +248,8 @@ def assemble(sets: list, tiles: list, weight, velocity, scalar, grid, rho_bar, p
         boxes=boxes,
         xs=np.concatenate(xs), ys=np.concatenate(ys), zs=np.concatenate(zs),
         grid=tuple(int(g) for g in grid), rho_bar=float(rho_bar),
-        padding=np.asarray(padding, np.float32), timings=timings)
+        padding=np.asarray(padding, np.float32), timings=timings,
+        regions=np.ascontiguousarray(np.stack(regions), np.float32) if regions else None)
 
 
 def decompose(pos, weight, grid, box, periodic: bool, n_threads: int, pad):
@@ -379,7 +394,8 @@ def split_boxes(plan: Plan) -> list:
     with re-based ids, its grid tile as the whole grid): the unbatched form,
     one handle and one launch sequence per sub-box."""
     out = []
-    for b in plan.box_list():
+    regions = plan.region_array()
+    for k, b in enumerate(plan.box_list()):
         vo, nv, to, nt = int(b.vert_offset), int(b.n_verts), int(b.tet_offset), int(b.n_tets)
         tv = np.ascontiguousarray(plan.tet_v[to:to + nt] - vo, np.int32)
         tn = plan.tet_n[to:to + nt]
@@ -401,7 +417,7 @@ def split_boxes(plan: Plan) -> list:
                         boxes=one, xs=np.ascontiguousarray(plan.xs[co[0]:co[0] + d[0]]),
                         ys=np.ascontiguousarray(plan.ys[co[1]:co[1] + d[1]]),
                         zs=np.ascontiguousarray(plan.zs[co[2]:co[2] + d[2]]), grid=tuple(d),
-                        rho_bar=plan.rho_bar, padding=plan.padding))
+                        rho_bar=plan.rho_bar, padding=plan.padding, regions=regions[k:k + 1].copy()))
     return out
 
 
@@ -453,7 +469,8 @@ def native_plan(kind: str, pos, weight, velocity=None, scalar=None, grid=(64, 64
                         boxes=boxes, xs=_view_array(v.xs, np.float32, (v.n_xs,)),
                         ys=_view_array(v.ys, np.float32, (v.n_ys,)), zs=_view_array(v.zs, np.float32, (v.n_zs,)),
                         grid=tuple(int(x) for x in v.grid), rho_bar=float(v.rho_bar),
-                        padding=np.array(list(v.padding), np.float32))
+                        padding=np.array(list(v.padding), np.float32),
+                        regions=_view_array(v.regions, np.float32, (K, 6)) if v.regions else None)
         n, K = v.n_particles, v.n_dep_boxes
         boxes = (N.DepositBox * K)()
         C.memmove(C.addressof(boxes), v.dep_boxes, C.sizeof(N.DepositBox) * K)

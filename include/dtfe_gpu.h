@@ -264,17 +264,20 @@ int dtfe_gpu_adjoint_dev(dtfe_handle h, const float* grad_density_dev, const flo
 int dtfe_gpu_deposit_adjoint_dev(dtfe_handle h, const float* grad_density_dev, float* grad_xyz_dev,
                                  float* grad_w_dev);
 
-/* Autotuner: times each launch variant of the point-location kernel
- * (register budget per block, cells per thread seeded from the previous hit)
- * and of the evaluation kernel on the loaded data, for the cell-centre method
- * and the given field mask, and keeps the fastest.  chosen[0..1] (may be
- * NULL) receive the selected variant indices.  No counterpart in the
- * reference (its loops have no launch parameters). */
+/* Autotuner: times each way of locating the cell centres — variants 0..2:
+ * every tetrahedron tests the centres inside its bounding box while its
+ * volume is computed (the default, 0); variants 3..8: a walk per centre from
+ * a seed tetrahedron — with its register budgets, and each register budget
+ * of the evaluation kernel, on the loaded data for the cell-centre method
+ * and the given field mask (whole steps: volumes, location, evaluation), and
+ * keeps the fastest.  All variants locate the same canonical tetrahedra.
+ * chosen[0..1] (may be NULL) receive the selected variant indices.  No
+ * counterpart in the reference (its loops have no launch parameters). */
 int dtfe_gpu_autotune(dtfe_handle h, uint32_t fields, int32_t* chosen);
-/* Selects launch variants explicitly (indices as reported by autotune). */
 /* Number of launch variants of the location (counts[0]) and evaluation
  * (counts[1]) kernels that dtfe_gpu_autotune chooses among. */
 int dtfe_gpu_variant_counts(int32_t counts[2]);
+/* Selects launch variants explicitly (indices as reported by autotune). */
 int dtfe_gpu_set_variants(dtfe_handle h, int32_t locate_variant, int32_t eval_variant);
 
 /* Copy the vertex densities (V floats) to the host. */

@@ -82,6 +82,7 @@ typedef struct {
   const float* velocity;  /* 3 V or NULL */
   const float* scalar;    /* S V or NULL */
   const dtfe_subbox* boxes;
+  const float* regions;   /* 6 per sub-box: its tile region (dtfe_gpu_set_regions) */
   const float *xs, *ys, *zs;
   int64_t n_xs, n_ys, n_zs;
   /* DTFE_PLAN_NGP/CIC/TSC: particle copies per region for dtfe_gpu_deposit */

@@ -41,6 +41,7 @@
 #include "../include/dtfe_gpu.h"
 #include "../dtfe_b200/csrc/philox.h"
 #include "../dtfe_b200/csrc/predicates.h"
+#include "../dtfe_b200/csrc/sobol.h"
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -566,5 +567,274 @@ int oracle_interpolate(int64_t T, const int32_t* tv, const int32_t* tn, int64_t 
   if (n_fail) *n_fail = fails;
   return fails ? DTFE_ERR_WALK : DTFE_OK;
 }
+
+// Averaging method 1: interpolateGrid_averaged_1
+// (src/CGAL_triangulation/averaged_interpolation_1.cc:197-421), per sub-box
+// over its tetrahedra in order.
+//   * quasi-random table: the first 100 NN Sobol points of the corner
+//     simplex, as floats (quasiRandomSequence :32-50);
+//   * a tetrahedron whose bounding box misses the region is skipped
+//     (cellOutsideRegion :67-77; closed boxes, double coordinates);
+//   * checkCellPosition (:84-118): base = vertex 0, basePosition =
+//     float(base - region lo), its cell floor(basePosition / dx) in float,
+//     that cell's box [i dx + lo, i dx + lo + dx] in float, one cell when
+//     vertices 1..3 lie in it (closed, isPointInBox box.h:63-73);
+//     vertexMatrix = double differences to the base;
+//   * volume = float(determinant / 6) (triangulation_miscellaneous.cc:205-213),
+//     inverse edge matrix as matrixInverse;
+//   * one valid cell: vertex averages (float sums / 4) times the volume and
+//     the gradients times the volume are added to it (:292-318);
+//   * otherwise n = size_t(NN vol / vcell) + 1 points (at most 100 NN) when
+//     vol / vcell > 1/6, else NN/6 + 1; point i = q_i vertexMatrix (double);
+//     its cell floor((basePosition + p) / dx) (double); densityValue,
+//     velocityValue, scalarValue at p and the gradients, each times vol / n,
+//     added to that cell (:322-364);
+//   * every cell divided by the cell volume dx0 dx1 dx2 (:371-393);
+//     divergence, shear and vorticity from the averaged gradient
+//     (src/DTFE.cpp:394-475).
+// mode 0 is the reference's float arithmetic and accumulation order; mode 1
+// evaluates values, volumes and sums in double over the same points and
+// cells.
+int oracle_method1(int64_t T, const int32_t* tv, int64_t V, const float* xyz, const float* vel,
+                   const float* scal, int S, const float* dens32, const double* dens64, int K,
+                   const dtfe_subbox* boxes, const float* regions, const int32_t grid[3], int NN,
+                   uint32_t fields, int fix, int mode, double* const out[DTFE_NUM_FIELDS]) {
+  (void)T;
+  (void)V;
+  auto has = [&](int s) { return (fields & DTFE_FIELD_BIT(s)) != 0 && out[s] != nullptr; };
+  if (NN < 1 || has(DTFE_VELOCITY_STD)) return DTFE_ERR_ARG;
+  const bool want_grad = has(DTFE_VELOCITY_GRADIENT) || has(DTFE_VELOCITY_DIVERGENCE) ||
+                         has(DTFE_VELOCITY_SHEAR) || has(DTFE_VELOCITY_VORTICITY);
+  const bool want_sc = S > 0 && scal && (has(DTFE_SCALAR) || has(DTFE_SCALAR_GRADIENT));
+  const size_t maxNN = 100 * (size_t)NN, minNN = (size_t)NN / 6 + 1;
+  const float minRatio = (float)(1. / 6.);
+  std::vector<float> q(3 * maxNN);
+  dtfe::sobol_simplex_table(maxNN, q.data());
+  const int64_t G1 = grid[1], G2 = grid[2];
+  for (int b = 0; b < K; ++b) {
+    const dtfe_subbox& B = boxes[b];
+    const float* reg = regions + 6 * b;
+    const float lo[3] = {reg[0], reg[2], reg[4]}, hi[3] = {reg[1], reg[3], reg[5]};
+    const float dx[3] = {B.dx[0], B.dx[1], B.dx[2]};
+    const int n[3] = {B.tile_dims[0], B.tile_dims[1], B.tile_dims[2]};
+    const int64_t Gb = (int64_t)n[0] * n[1] * n[2];
+    const float gcv = dx[0] * dx[1] * dx[2];
+    // accumulators of the tile: float (mode 0) or double (mode 1)
+    std::vector<float> fD(Gb, 0.f), fV(3 * Gb, 0.f), fG(9 * Gb, 0.f), fS(S * Gb, 0.f), fSG(3 * S * Gb, 0.f);
+    std::vector<double> dD(Gb, 0.), dV(3 * Gb, 0.), dG(9 * Gb, 0.), dS(S * Gb, 0.), dSG(3 * S * Gb, 0.);
+    for (int64_t t = B.tet_offset; t < B.tet_offset + B.n_tets; ++t) {
+      const int32_t* v = &tv[4 * t];
+      double X[4][3];
+      for (int a = 0; a < 4; ++a)
+        for (int c = 0; c < 3; ++c) X[a][c] = (double)xyz[3 * (int64_t)v[a] + c];
+      bool outside = false;
+      for (int c = 0; c < 3; ++c) {
+        const double mn = std::min(std::min(X[0][c], X[1][c]), std::min(X[2][c], X[3][c]));
+        const double mx = std::max(std::max(X[0][c], X[1][c]), std::max(X[2][c], X[3][c]));
+        outside = outside || mn > (double)hi[c] || mx < (double)lo[c];
+      }
+      if (outside) continue;
+      float bp[3];
+      int bc[3];
+      float gl[3], gh[3];
+      for (int c = 0; c < 3; ++c) {
+        bp[c] = (float)(X[0][c] - (double)lo[c]);
+        bc[c] = (int)std::floor(bp[c] / dx[c]);
+        gl[c] = (float)bc[c] * dx[c] + lo[c];
+        gh[c] = gl[c] + dx[c];
+      }
+      bool one = true;
+      for (int a = 1; a < 4 && one; ++a)
+        for (int c = 0; c < 3; ++c)
+          one = one && X[a][c] >= (double)gl[c] && X[a][c] <= (double)gh[c];
+      double vM[3][3];
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) vM[r][c] = X[r + 1][c] - X[0][c];
+      const double vol64 = dtfe::orient_det(X[0], X[1], X[2], X[3]) / 6.0;
+      const float vol = (float)vol64;
+      // gradients (densityGrad, velocityGrad, scalarGrad): float in mode 0
+      float Mf[3][3];
+      double Md[3][3];
+      matrix_inverse<float>(vM, Mf);
+      matrix_inverse<double>(vM, Md);
+      float d0 = dens32[v[0]], grf[3], VGf[3][3] = {}, SGf[DTFE_MAX_SCALARS][3] = {};
+      double e0 = dens64[v[0]], grd[3], VGd[3][3] = {}, SGd[DTFE_MAX_SCALARS][3] = {};
+      for (int i = 0; i < 3; ++i) {
+        float acc = 0.f;
+        double accd = 0.;
+        for (int j = 0; j < 3; ++j) {
+          acc += Mf[i][j] * (dens32[v[j + 1]] - d0);
+          accd += Md[i][j] * (dens64[v[j + 1]] - e0);
+        }
+        grf[i] = acc;
+        grd[i] = accd;
+      }
+      const float* v0 = vel ? &vel[3 * (int64_t)v[0]] : nullptr;
+      if (vel)
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) {
+            float acc = 0.f;
+            double accd = 0.;
+            for (int k = 0; k < 3; ++k) {
+              acc += Mf[i][k] * (vel[3 * (int64_t)v[k + 1] + j] - v0[j]);
+              accd += Md[i][k] * ((double)vel[3 * (int64_t)v[k + 1] + j] - (double)v0[j]);
+            }
+            VGf[i][j] = acc;
+            VGd[i][j] = accd;
+          }
+      const float* s0 = want_sc ? &scal[(int64_t)S * v[0]] : nullptr;
+      if (want_sc)
+        for (int qq = 0; qq < S; ++qq)
+          for (int i = 0; i < 3; ++i) {
+            float acc = 0.f;
+            double accd = 0.;
+            for (int k = 0; k < 3; ++k) {
+              acc += Mf[i][k] * (scal[(int64_t)S * v[k + 1] + qq] - s0[qq]);
+              accd += Md[i][k] * ((double)scal[(int64_t)S * v[k + 1] + qq] - (double)s0[qq]);
+            }
+            SGf[qq][i] = acc;
+            SGd[qq][i] = accd;
+          }
+      const bool valid_one =
+          one && bc[0] >= 0 && bc[0] < n[0] && bc[1] >= 0 && bc[1] < n[1] && bc[2] >= 0 && bc[2] < n[2];
+      if (valid_one) {
+        const int64_t idx = ((int64_t)bc[0] * n[1] + bc[1]) * n[2] + bc[2];
+        if (mode == 0) {
+          float a = 0.f;
+          for (int i = 0; i < 4; ++i) a += dens32[v[i]];
+          fD[idx] += (a / 4.f) * vol;
+          if (vel)
+            for (int c = 0; c < 3; ++c) {
+              float av = 0.f;
+              for (int i = 0; i < 4; ++i) av += vel[3 * (int64_t)v[i] + c];
+              fV[3 * idx + c] += (av / 4.f) * vol;
+            }
+          for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) fG[9 * idx + j * 3 + i] += VGf[i][j] * vol;
+          if (want_sc)
+            for (int qq = 0; qq < S; ++qq) {
+              float as = 0.f;
+              for (int i = 0; i < 4; ++i) as += scal[(int64_t)S * v[i] + qq];
+              fS[S * idx + qq] += (as / 4.f) * vol;
+              for (int i = 0; i < 3; ++i) fSG[3 * S * idx + 3 * qq + i] += SGf[qq][i] * vol;
+            }
+        } else {
+          double a = 0.;
+          for (int i = 0; i < 4; ++i) a += dens64[v[i]];
+          dD[idx] += a / 4. * vol64;
+          if (vel)
+            for (int c = 0; c < 3; ++c) {
+              double av = 0.;
+              for (int i = 0; i < 4; ++i) av += vel[3 * (int64_t)v[i] + c];
+              dV[3 * idx + c] += av / 4. * vol64;
+            }
+          for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) dG[9 * idx + j * 3 + i] += VGd[i][j] * vol64;
+          if (want_sc)
+            for (int qq = 0; qq < S; ++qq) {
+              double as = 0.;
+              for (int i = 0; i < 4; ++i) as += scal[(int64_t)S * v[i] + qq];
+              dS[S * idx + qq] += as / 4. * vol64;
+              for (int i = 0; i < 3; ++i) dSG[3 * S * idx + 3 * qq + i] += SGd[qq][i] * vol64;
+            }
+        }
+        continue;
+      }
+      const size_t tempInt = (size_t)((float)NN * vol / gcv) + 1;
+      const size_t np = (vol / gcv > minRatio) ? (tempInt > maxNN ? maxNN : tempInt) : minNN;
+      const float factor = vol / (float)np;
+      const double factor64 = vol64 / (double)np;
+      for (size_t i = 0; i < np; ++i) {
+        double p[3];
+        for (int c = 0; c < 3; ++c)
+          p[c] = (double)q[3 * i] * vM[0][c] + (double)q[3 * i + 1] * vM[1][c] + (double)q[3 * i + 2] * vM[2][c];
+        int pos[3];
+        bool ok = true;
+        for (int c = 0; c < 3 && ok; ++c) {
+          pos[c] = (int)std::floor(((double)bp[c] + p[c]) / (double)dx[c]);
+          ok = pos[c] >= 0 && pos[c] < n[c];
+        }
+        if (!ok) continue;
+        const int64_t idx = ((int64_t)pos[0] * n[1] + pos[1]) * n[2] + pos[2];
+        if (mode == 0) {
+          const float temp = (float)(p[0] * grf[0] + p[1] * grf[1] + p[2] * grf[2]);
+          fD[idx] += (d0 + temp) * factor;
+          if (vel)
+            for (int c = 0; c < 3; ++c) {
+              float tmp = 0.f;
+              for (int j = 0; j < 3; ++j)
+                tmp = fix ? (float)((double)tmp + (double)VGf[j][c] * p[j]) : (float)((double)VGf[j][c] * p[j]);
+              fV[3 * idx + c] += (tmp + v0[c]) * factor;
+            }
+          for (int j = 0; j < 3; ++j)
+            for (int c = 0; c < 3; ++c) fG[9 * idx + j * 3 + c] += VGf[c][j] * factor;
+          if (want_sc)
+            for (int qq = 0; qq < S; ++qq) {
+              float tmp = 0.f;
+              for (int j = 0; j < 3; ++j)
+                tmp = fix ? (float)((double)tmp + (double)SGf[qq][j] * p[j]) : (float)((double)SGf[qq][j] * p[j]);
+              fS[S * idx + qq] += (tmp + s0[qq]) * factor;
+              for (int c = 0; c < 3; ++c) fSG[3 * S * idx + 3 * qq + c] += SGf[qq][c] * factor;
+            }
+        } else {
+          dD[idx] += (e0 + p[0] * grd[0] + p[1] * grd[1] + p[2] * grd[2]) * factor64;
+          if (vel)
+            for (int c = 0; c < 3; ++c) {
+              double tmp = 0.;
+              if (fix) for (int j = 0; j < 3; ++j) tmp += VGd[j][c] * p[j];
+              else tmp = VGd[2][c] * p[2];
+              dV[3 * idx + c] += (tmp + (double)v0[c]) * factor64;
+            }
+          for (int j = 0; j < 3; ++j)
+            for (int c = 0; c < 3; ++c) dG[9 * idx + j * 3 + c] += VGd[c][j] * factor64;
+          if (want_sc)
+            for (int qq = 0; qq < S; ++qq) {
+              double tmp = 0.;
+              if (fix) for (int j = 0; j < 3; ++j) tmp += SGd[qq][j] * p[j];
+              else tmp = SGd[qq][2] * p[2];
+              dS[S * idx + qq] += (tmp + (double)s0[qq]) * factor64;
+              for (int c = 0; c < 3; ++c) dSG[3 * S * idx + 3 * qq + c] += SGd[qq][c] * factor64;
+            }
+        }
+      }
+    }
+    // divide by the cell volume and write the tile into the grid
+    for (int i = 0; i < n[0]; ++i)
+      for (int j = 0; j < n[1]; ++j)
+        for (int k = 0; k < n[2]; ++k) {
+          const int64_t idx = ((int64_t)i * n[1] + j) * n[2] + k;
+          const int64_t cell = ((int64_t)(B.tile_origin[0] + i) * G1 + (B.tile_origin[1] + j)) * G2 +
+                               (B.tile_origin[2] + k);
+          auto val = [&](const std::vector<float>& f, const std::vector<double>& d, int64_t at) {
+            return mode == 0 ? (double)(f[at] / gcv) : d[at] / (double)gcv;
+          };
+          double g9[9];
+          for (int c = 0; c < 9; ++c) g9[c] = val(fG, dG, 9 * idx + c);
+          if (has(DTFE_DENSITY)) out[DTFE_DENSITY][cell] = val(fD, dD, idx);
+          if (has(DTFE_VELOCITY))
+            for (int c = 0; c < 3; ++c) out[DTFE_VELOCITY][3 * cell + c] = val(fV, dV, 3 * idx + c);
+          if (has(DTFE_VELOCITY_GRADIENT))
+            for (int c = 0; c < 9; ++c) out[DTFE_VELOCITY_GRADIENT][9 * cell + c] = g9[c];
+          if (want_grad) {
+            double dv, sh[5], vo[3];
+            derived(g9, mode, &dv, sh, vo);
+            if (has(DTFE_VELOCITY_DIVERGENCE)) out[DTFE_VELOCITY_DIVERGENCE][cell] = dv;
+            if (has(DTFE_VELOCITY_SHEAR))
+              for (int c = 0; c < 5; ++c) out[DTFE_VELOCITY_SHEAR][5 * cell + c] = sh[c];
+            if (has(DTFE_VELOCITY_VORTICITY))
+              for (int c = 0; c < 3; ++c) out[DTFE_VELOCITY_VORTICITY][3 * cell + c] = vo[c];
+          }
+          if (want_sc && has(DTFE_SCALAR))
+            for (int qq = 0; qq < S; ++qq) out[DTFE_SCALAR][(int64_t)S * cell + qq] = val(fS, dS, S * idx + qq);
+          if (want_sc && has(DTFE_SCALAR_GRADIENT))
+            for (int c = 0; c < 3 * S; ++c)
+              out[DTFE_SCALAR_GRADIENT][(int64_t)3 * S * cell + c] = val(fSG, dSG, 3 * S * idx + c);
+        }
+  }
+  return DTFE_OK;
+}
+
+// The method-1 quasi-random table (3 floats per point).
+void oracle_sobol_simplex(int64_t n, float* out) { dtfe::sobol_simplex_table((size_t)n, out); }
 
 }  // extern "C"

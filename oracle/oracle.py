@@ -48,6 +48,10 @@ def lib() -> C.CDLL:
                                      vp, vp, vp, C.c_int, C.c_int64, vp, vp, C.c_double, C.c_double, C.c_double, vp]
         L.oracle_deposit_loss_grad.argtypes = [C.c_int, vp, vp, C.c_int64, vp, vp, C.c_double, vp, vp, vp]
         L.oracle_deposit_loss_grad.restype = C.c_double
+        L.oracle_method1.argtypes = [C.c_int64, vp, C.c_int64, vp, vp, vp, C.c_int, vp, vp, C.c_int, vp, vp, vp,
+                                     C.c_int, C.c_uint32, C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+        L.oracle_sobol_simplex.argtypes = [C.c_int64, vp]
+        L.oracle_sobol_simplex.restype = None
         _lib = L
     return _lib
 
@@ -195,6 +199,41 @@ def interpolate(plan, dens32, dens64, fields, method: int = 0, n_samples: int = 
     if nfail.value:
         raise RuntimeError(f"oracle walk failed on {nfail.value} samples")
     return arrs, loc
+
+
+def method1(plan, dens32, dens64, fields, n_points: int = 100, mode: int = MODE_REF, fix: bool = False):
+    """Averaging method 1 (points inside each tetrahedron scattered to the
+    grid, interpolateGrid_averaged_1): dict field -> float64 array."""
+    G = int(np.prod(plan.grid))
+    S = plan.n_scalars
+    mask = 0
+    outs = [None] * N.NUM_FIELDS
+    arrs = {}
+    for f in fields:
+        s = N.FIELD_SLOTS[f]
+        mask |= 1 << s
+        nc = N.field_components(s, S)
+        a = np.zeros((G, nc) if nc > 1 else G, np.float64)
+        arrs[f] = a
+        outs[s] = a.ctypes.data
+    optr = (C.c_void_p * N.NUM_FIELDS)(*[o if o else None for o in outs])
+    vel = plan.velocity.ctypes.data if plan.velocity is not None else None
+    sc = plan.scalar.ctypes.data if plan.scalar is not None else None
+    grid = np.asarray(plan.grid, np.int32)
+    regions = plan.region_array()
+    rc = lib().oracle_method1(plan.n_tets, plan.tet_v.ctypes.data, plan.n_verts, plan.xyz.ctypes.data, vel, sc, S,
+                              dens32.ctypes.data, dens64.ctypes.data, plan.n_boxes, C.addressof(plan.boxes),
+                              regions.ctypes.data, grid.ctypes.data, n_points, mask, 1 if fix else 0, mode, optr)
+    if rc:
+        raise RuntimeError(f"oracle_method1 failed with status {rc}")
+    return arrs
+
+
+def sobol_simplex(n: int) -> np.ndarray:
+    """(n, 3) float32: the method-1 quasi-random table."""
+    out = np.zeros((n, 3), np.float32)
+    lib().oracle_sobol_simplex(n, out.ctypes.data)
+    return out
 
 
 # ---- adjoint checker -------------------------------------------------------

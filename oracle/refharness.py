@@ -51,8 +51,7 @@ def run(plan, box: int = 0, which: int = 0, n_points: int = 1, seed: int = 0, de
     tn = plan.tet_n[t0:t0 + nt]
     tn = np.ascontiguousarray(np.where(tn >= 0, tn - t0, -1), dtype=np.int32)
     dims = np.array([b.tile_dims[0], b.tile_dims[1], b.tile_dims[2]], np.int32)
-    region = np.array([b.lo[0], b.lo[0] + b.dx[0] * dims[0], b.lo[1], b.lo[1] + b.dx[1] * dims[1],
-                       b.lo[2], b.lo[2] + b.dx[2] * dims[2]], np.float32)
+    region = np.ascontiguousarray(plan.region_array()[box])
     G = int(np.prod(dims))
     out = {"vertex_density": np.zeros(nv, np.float32), "density": np.zeros(G, np.float32),
            "velocity": np.zeros((G, 3), np.float32), "velocity_gradient": np.zeros((G, 9), np.float32),
@@ -81,8 +80,7 @@ def _box_args(plan, box):
     tn = plan.tet_n[t0:t0 + nt]
     tn = np.ascontiguousarray(np.where(tn >= 0, tn - t0, -1), dtype=np.int32)
     dims = np.array([b.tile_dims[0], b.tile_dims[1], b.tile_dims[2]], np.int32)
-    region = np.array([b.lo[0], b.lo[0] + b.dx[0] * dims[0], b.lo[1], b.lo[1] + b.dx[1] * dims[1],
-                       b.lo[2], b.lo[2] + b.dx[2] * dims[2]], np.float32)
+    region = np.ascontiguousarray(plan.region_array()[box])
     return xyz, w, vel, tv, tn, dims, region
 
 

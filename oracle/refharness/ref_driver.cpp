@@ -10,6 +10,8 @@
 //   interpolateGrid             unaveraged_interpolation.cc:209-369
 //   interpolateGrid_averaged_2  averaged_interpolation_2.cc:35-233
 //   interpolateGrid_averaged_3  averaged_interpolation_2.cc:664-866
+//   interpolateGrid_averaged_1  averaged_interpolation_1.cc:197-421 (Sobol points
+//                               from dtfe_b200/csrc/sobol.h behind the GSL API)
 //
 // The reference's command-line layer (user_options.cc, boost::program_options)
 // is not built; the User_options constructor below sets the members those
@@ -24,6 +26,8 @@
 
 #include <gsl/gsl_qrng.h>
 
+#include "../../dtfe_b200/csrc/sobol.h"
+
 #include "define.h"
 #include "CGAL_triangulation/CGAL_include_3D.h"
 #include "particle_data.h"
@@ -34,6 +38,7 @@ void vertexDensity(DT& dt, User_options& userOptions);
 void interpolateGrid(DT& dt, User_options& userOptions, Quantities* quantities);
 void interpolateGrid_averaged_2(DT& dt, User_options& userOptions, Quantities* quantities);
 void interpolateGrid_averaged_3(DT& dt, User_options& userOptions, Quantities* quantities);
+void interpolateGrid_averaged_1(DT& dt, User_options& userOptions, Quantities* quantities);
 
 User_options::User_options() {
   periodic = false;
@@ -73,18 +78,30 @@ User_options::User_options() {
 
 extern "C" {
 
-// GSL stand-ins (method 1 is never run by the harness)
-const gsl_qrng_type* gsl_qrng_sobol = nullptr;
-const gsl_qrng_type* gsl_qrng_niederreiter_2 = nullptr;
-gsl_qrng* gsl_qrng_alloc(const gsl_qrng_type*, unsigned int) {
-  std::fprintf(stderr, "reference harness: averaging method 1 is not available\n");
-  std::abort();
+// GSL stand-ins: gsl_qrng_sobol as the Bratley-Fox construction of
+// dtfe_b200/csrc/sobol.h (the only generator averaging method 1 uses).
+struct gsl_qrng_type_s {
+  int id;
+};
+struct gsl_qrng_s {
+  mutable dtfe::Sobol3 seq;
+};
+static const gsl_qrng_type kSobolType{1};
+static const gsl_qrng_type kNiederreiterType{2};
+const gsl_qrng_type* gsl_qrng_sobol = &kSobolType;
+const gsl_qrng_type* gsl_qrng_niederreiter_2 = &kNiederreiterType;
+gsl_qrng* gsl_qrng_alloc(const gsl_qrng_type* T, unsigned int d) {
+  if (T != gsl_qrng_sobol || d != 3) {
+    std::fprintf(stderr, "reference harness: only the 3-dimensional Sobol generator is available\n");
+    std::abort();
+  }
+  return new gsl_qrng;
 }
-int gsl_qrng_get(const gsl_qrng*, double*) { std::abort(); }
-void gsl_qrng_free(gsl_qrng*) {}
+int gsl_qrng_get(const gsl_qrng* q, double* x) { return q->seq.next(x) ? 0 : 1; }
+void gsl_qrng_free(gsl_qrng* q) { delete q; }
 
 // Runs the reference on one (sub-box) tessellation with LOCAL indices.
-//   which: 0 cell-centre (interpolateGrid), 2 / 3 averaging methods.
+//   which: 0 cell-centre (interpolateGrid), 1 / 2 / 3 averaging methods.
 //   dens_override (may be NULL): vertex densities used for the interpolation
 //   instead of the reference's own (float-accumulated) ones.
 //   outputs (float, Quantities layout; NULL to skip): vertex densities,
@@ -134,6 +151,9 @@ int ref_interpolate_timed(int64_t nv, const float* xyz, const float* w, const fl
   if (which == 0) {
     opt.uField = f;
     interpolateGrid(dt, opt, &q);
+  } else if (which == 1) {
+    opt.aField = f;
+    interpolateGrid_averaged_1(dt, opt, &q);
   } else if (which == 2) {
     opt.aField = f;
     interpolateGrid_averaged_2(dt, opt, &q);

@@ -70,4 +70,4 @@ def golden_plan(g):
     return Plan(tet_v=g["tet_v"], tet_n=g["tet_n"], xyz=g["xyz"], src=np.arange(len(g["xyz"]), dtype=np.int32),
                 weight=g["weight"], velocity=g["velocity"], scalar=g["scalar"], boxes=boxes, xs=g["xs"],
                 ys=g["ys"], zs=g["zs"], grid=tuple(int(x) for x in g["grid"]), rho_bar=float(g["rho_bar"]),
-                padding=g["padding"])
+                padding=g["padding"], regions=g["region"].reshape(1, 6) if "region" in g else None)

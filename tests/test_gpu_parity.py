@@ -135,3 +135,41 @@ def test_launch_variants_identical(plan8):
             assert d.last_status["n_samples_located"] == st0["n_samples_located"]
             assert d.last_status["n_outside"] == st0["n_outside"]
     d.close()
+
+
+def test_centre_ties_lattice(gpu_built):
+    """Particles exactly on every second sample coordinate: every cell centre
+    is a vertex, an edge midpoint, a face centre or a cube centre of the
+    lattice, so most centres lie on shared faces, edges or vertices.  The
+    raster variants (lowest id among the tetrahedra whose closure holds the
+    centre) and the walk variants (walk, then the tie rule) must both give
+    the oracle's canonical tetrahedra: fields equal to the oracle's."""
+    from dtfe_b200.device import DeviceDTFE
+    g = (24, 24, 24)
+    rng = np.random.default_rng(1)
+    probe = P.make_plan(rng.random((100, 3)).astype(np.float32) * 100, np.ones(100, np.float32), None, None,
+                        grid=g, n_threads=1, average_density_value=1e-3)
+    X, Y, Z = np.meshgrid(probe.xs[::2], probe.ys[::2], probe.zs[::2], indexing="ij")
+    pos = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1).astype(np.float32)
+    vel = rng.standard_normal(pos.shape).astype(np.float32)
+    w = rng.uniform(0.5, 1.5, len(pos)).astype(np.float32)
+    plan = P.make_plan(pos, w, vel, None, grid=g, n_threads=1, average_density_value=float(w.sum()) / 1e6)
+    assert np.array_equal(plan.xs, probe.xs)
+    fields = ["density", "velocity", "velocity_gradient"]
+    d32, d64, _ = O.vertex_density(plan)
+    ref, _ = O.interpolate(plan, d32, d64, fields, mode=O.MODE_REF)
+    with DeviceDTFE(0) as d:
+        d.load(plan)
+        d.vertex_density(plan.rho_bar)
+        n_loc, _ = d.variant_counts()
+        outs = []
+        for loc in (0, 1, 2, n_loc - 6):     # the three raster budgets and the first walk variant
+            d.set_variants(loc, 0)
+            outs.append(d.interpolate(fields, method=0))
+            assert d.last_status["n_outside"] == 0
+            assert d.last_status["n_samples_located"] == int(np.prod(g))
+        assert d.last_status["n_ties"] > 0
+    for got in outs:
+        for f in fields:
+            assert np.array_equal(got[f], outs[0][f]), f
+            assert rel_err(got[f], ref[f]) <= 1e-6, f

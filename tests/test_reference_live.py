@@ -76,3 +76,34 @@ def test_timed_reference_matches_untimed(built):
     tmax, per_box = R.time_boxes(plan, 2)
     assert len(per_box) == plan.n_boxes and all(t > 0 for t in per_box)
     assert tmax >= max(per_box) - 1e-12
+
+
+@pytest.mark.parametrize("n_threads,nn", [(1, 100), (4, 8)])
+def test_live_method1(built, n_threads, nn):
+    """Averaging method 1 (Sobol points inside every tetrahedron scattered to
+    the grid): the reference's own interpolateGrid_averaged_1, run through the
+    harness on each sub-box, against the oracle's float mode bit for bit, and
+    the oracle's FP64 mode within 1e-5 of it."""
+    pos, psi = S.zeldovich_lattice(12, 100.0, 0.9, seed=41)
+    rng = np.random.default_rng(42)
+    w = rng.uniform(0.5, 1.5, len(pos)).astype(np.float32)
+    vel = (60 * psi).astype(np.float32)
+    sc = rng.standard_normal((len(pos), 1)).astype(np.float32)
+    # grid finer than the particles: tetrahedra spanning several cells and
+    # tetrahedra inside one cell both occur
+    plan = P.make_plan(pos, w, vel, sc, grid=(17, 15, 19), n_threads=n_threads,
+                       average_density_value=float(w.sum()) / 1e6)
+    d32, d64, _ = O.vertex_density(plan)
+    ora = O.method1(plan, d32, d64, FIELDS, n_points=nn, mode=O.MODE_REF)
+    o64 = O.method1(plan, d32, d64, FIELDS, n_points=nn, mode=O.MODE_FP64)
+    for k, b in enumerate(plan.box_list()):
+        ref = R.run(plan, k, which=1, n_points=nn, dens_override=d32)
+        ox, oy, oz = b.tile_origin[0], b.tile_origin[1], b.tile_origin[2]
+        dims = (b.tile_dims[0], b.tile_dims[1], b.tile_dims[2])
+        for f in FIELDS:
+            full = ora[f].reshape(plan.grid + ora[f].shape[1:])
+            tile = full[ox:ox + dims[0], oy:oy + dims[1], oz:oz + dims[2]].reshape(ref[f].shape)
+            assert np.array_equal(tile.astype(np.float32), ref[f]), (k, f)
+    for f in FIELDS:
+        assert rel_err(ora[f], o64[f]) <= 1e-5, f
+    assert np.abs(ora["density"]).max() > 0

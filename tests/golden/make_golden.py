@@ -15,6 +15,9 @@ fixture does not depend on it), then:
   * interpolateGrid (cell centres) of density, velocity, gradient, scalar,
     scalar gradient on a 10^3 grid, with the reference's own vertex densities;
   * interpolateGrid_averaged_3 with 8 equidistant points per cell;
+  * interpolateGrid_averaged_1 with 100 points per cell (the reference's
+    default method and count; its GSL Sobol generator stood in by
+    dtfe_b200/csrc/sobol.h);
   * NGP / CIC / TSC density and velocity of the same particles in a region;
   * SPH_interpolation (32 neighbours) density, velocity and intensive scalar
     of the padded particle set on the 10^3 grid of the box;
@@ -66,6 +69,7 @@ def main():
     b = plan.boxes[0]
     out["box_lo"] = np.array(list(b.lo), np.float32)
     out["box_dx"] = np.array(list(b.dx), np.float32)
+    out["region"] = plan.region_array()[0]
     centre = R.run(plan, 0, which=0)
     out["ref_vertex_density"] = centre["vertex_density"]
     for f in ("density", "velocity", "velocity_gradient", "scalar", "scalar_gradient"):
@@ -73,6 +77,9 @@ def main():
     eq = R.run(plan, 0, which=3, n_points=8)
     for f in ("density", "velocity", "velocity_gradient", "scalar", "scalar_gradient"):
         out["ref_equidistant8_" + f] = eq[f]
+    m1 = R.run(plan, 0, which=1, n_points=100)
+    for f in ("density", "velocity", "velocity_gradient", "scalar", "scalar_gradient"):
+        out["ref_method1_100_" + f] = m1[f]
 
     region = np.array([10, 90, 5, 95, 0, 100], np.float32)
     dgrid = np.array([8, 9, 10], np.int32)

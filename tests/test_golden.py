@@ -46,6 +46,19 @@ def test_interpolation_bit_exact_vs_reference(g, method, nn, tag):
         assert np.array_equal(out[f].astype(np.float32), want), f
 
 
+def test_method1_bit_exact_vs_reference(g):
+    """Averaging method 1 with the reference's default 100 points per cell
+    (its own vertex densities): the oracle's float mode reproduces the
+    reference's interpolateGrid_averaged_1 bit for bit."""
+    plan = golden_plan(g)
+    _, d64, _ = O.vertex_density(plan)
+    ref_dens = np.ascontiguousarray(g["ref_vertex_density"])
+    out = O.method1(plan, ref_dens, d64, FIELDS, n_points=100, mode=O.MODE_REF)
+    for f in FIELDS:
+        want = g[f"ref_method1_100_{f}"].reshape(out[f].shape)
+        assert np.array_equal(out[f].astype(np.float32), want), f
+
+
 @pytest.mark.parametrize("kind,name", [(0, "ngp"), (1, "cic"), (2, "tsc")])
 def test_deposit_bit_exact_vs_reference(g, kind, name):
     import ctypes as C

@@ -84,7 +84,7 @@ FIELD_SLOTS = {
     "velocity_shear": 4, "velocity_vorticity": 5, "velocity_std": 6,
     "scalar": 7, "scalar_gradient": 8,
 }
-METHOD_CENTRE, METHOD_MONTE_CARLO, METHOD_EQUIDISTANT = 0, 2, 3
+METHOD_CENTRE, METHOD_TETRAHEDRA, METHOD_MONTE_CARLO, METHOD_EQUIDISTANT = 0, 1, 2, 3
 FLAG_FIX_VALUE_INTERP = 1
 
 
@@ -158,6 +158,7 @@ def gpu() -> C.CDLL:
         lib.dtfe_gpu_upload_packed.argtypes = [H, vp, C.c_int64, vp, vp, vp, vp, C.c_int64]
         lib.dtfe_gpu_set_subboxes.argtypes = [H, C.c_int32, vp, vp, C.c_int64, vp, C.c_int64,
                                               vp, C.c_int64, vp]
+        lib.dtfe_gpu_set_regions.argtypes = [H, C.c_int32, vp]
         lib.dtfe_gpu_vertex_density.argtypes = [H, C.c_double]
         lib.dtfe_gpu_interpolate.argtypes = [H, C.POINTER(InterpOpts), C.POINTER(vp), C.POINTER(Status)]
         lib.dtfe_gpu_interpolate_async.argtypes = [H, C.POINTER(InterpOpts), C.POINTER(vp)]

@@ -1022,6 +1022,13 @@ struct dtfe_gpu_s {
   dtfe_gpu_s* upload_after = nullptr;  // uploads wait for this handle's latest copies
   void* sph_scratch = nullptr;    // SPH cell grids, neighbour bookkeeping, FP64 sums
   size_t sph_bytes = 0;
+  std::vector<float> regions_h;   // 6 per sub-box: tile regions (averaging method 1)
+  float* m1_table = nullptr;      // method-1 Sobol points (100 NN x 3)
+  int m1_table_nn = 0;
+  void* m1_scratch = nullptr;     // method-1 counts, offsets, scan scratch
+  size_t m1_bytes = 0;
+  void* m1_lists = nullptr;       // method-1 tetrahedra of every cell
+  size_t m1_lists_bytes = 0;
   float* sph_out = nullptr;       // host-output SPH staging
 };
 
@@ -1084,7 +1091,6 @@ struct LocVariant { int block, minb, r; };
 constexpr LocVariant kWalkVariants[] = {{256, 3, 1}, {256, 2, 1}, {256, 4, 1}, {256, 3, 2}, {256, 4, 2}, {256, 3, 4}};
 constexpr int kNumLocVariants = kNumRasterVariants + sizeof(kWalkVariants) / sizeof(kWalkVariants[0]);
 inline bool is_raster(int loc_variant) { return loc_variant < kNumRasterVariants; }
-constexpr int kEvalMinBlocks[] = {3, 2, 4};
 constexpr int kNumEvalVariants = 3;
 
 // Per step, before the interpolation: tetrahedron volumes and either the
@@ -1168,6 +1174,9 @@ void launch_eval_s(int method, int S, int evariant, const InterpParams& P, const
     case 2: launch_eval<2>(method, evariant, P, tet_c, st, grid, block); break;
     case 3: launch_eval<3>(method, evariant, P, tet_c, st, grid, block); break;
     case 4: launch_eval<4>(method, evariant, P, tet_c, st, grid, block); break;
+    case 5: launch_eval<5>(method, evariant, P, tet_c, st, grid, block); break;
+    case 6: launch_eval<6>(method, evariant, P, tet_c, st, grid, block); break;
+    case 7: launch_eval<7>(method, evariant, P, tet_c, st, grid, block); break;
     default: launch_eval<8>(method, evariant, P, tet_c, st, grid, block); break;
   }
 }
@@ -1232,7 +1241,8 @@ int dtfe_gpu_destroy(dtfe_handle h) {
     if (h->out_buf[i]) cudaFree(h->out_buf[i]);
   if (h->dep_scratch) cudaFree(h->dep_scratch);
   for (void* p : {(void*)h->g_rho, (void*)h->g_x, (void*)h->g_v, (void*)h->g_S, (void*)h->g_m, (void*)h->vbar,
-                  (void*)h->adj_a, h->sph_scratch, (void*)h->sph_out, (void*)h->upload_buf})
+                  (void*)h->adj_a, h->sph_scratch, (void*)h->sph_out, (void*)h->upload_buf, (void*)h->m1_table,
+                  h->m1_scratch, h->m1_lists})
     if (p) cudaFree(p);
   if (h->dep_out) cudaFree(h->dep_out);
   cudaEventDestroy(h->ev_h2d);
@@ -1457,11 +1467,30 @@ int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* box
   DTFE_CUDA_TRY(cudaStreamSynchronize(st));  // host vectors go out of scope
   h->K = n_boxes;
   h->boxes_h.assign(boxes, boxes + n_boxes);
+  h->regions_h.resize((size_t)6 * n_boxes);
+  for (int b = 0; b < n_boxes; ++b)
+    for (int a = 0; a < 3; ++a) {
+      h->regions_h[6 * b + 2 * a] = boxes[b].lo[a];
+      h->regions_h[6 * b + 2 * a + 1] = boxes[b].lo[a] + boxes[b].dx[a] * (float)boxes[b].tile_dims[a];
+    }
   h->n_cells = cells;
   h->grid[0] = grid[0]; h->grid[1] = grid[1]; h->grid[2] = grid[2];
   h->prep_ready = false;
   h->eq_nn = 0;
   drop_graph(h);
+  return DTFE_OK;
+}
+
+int dtfe_gpu_set_regions(dtfe_handle h, int32_t n_boxes, const float* regions) {
+  if (!h || !regions) return set_error(DTFE_ERR_ARG, "null argument");
+  if (n_boxes != h->K) return set_error(DTFE_ERR_STATE, "regions must follow dtfe_gpu_set_subboxes, one per sub-box");
+  for (int b = 0; b < n_boxes; ++b)
+    for (int a = 0; a < 3; ++a) {
+      const float lo = regions[6 * b + 2 * a], hi = regions[6 * b + 2 * a + 1];
+      if (lo != h->boxes_h[b].lo[a] || !(hi >= lo))
+        return set_error(DTFE_ERR_ARG, "region lower corner differs from the sub-box's lo, or hi < lo");
+    }
+  h->regions_h.assign(regions, regions + (size_t)6 * n_boxes);
   return DTFE_OK;
 }
 
@@ -1498,13 +1527,20 @@ int dtfe_gpu_download_vertex_density(dtfe_handle h, float* dens) {
 // Validation, one-time set-up and every launch of one interpolation on the
 // handle's stream; nothing waits for the GPU after the set-up, so the
 // launches can be captured into a graph once the set-up has run.
+int dtfe_internal_method1(void* stream, int K, const dtfe_subbox* boxes_h, const dtfe_subbox* boxes_d,
+                          const float* regions_h, int64_t n_cells, int64_t G1, int64_t G2, int64_t T,
+                          const int4* tet_v, const float4* posd, const float4* vel4, const float* scal, int S, int NN,
+                          uint32_t fields, int fix, float* const out[DTFE_NUM_FIELDS], float** table, int* table_nn,
+                          void** scratch, size_t* scratch_bytes, void** lists, size_t* lists_bytes);
+
 static int interp_enqueue(dtfe_handle h, const dtfe_interp_opts* o, float* const out_dev[DTFE_NUM_FIELDS]) {
   if (!h || !o) return set_error(DTFE_ERR_ARG, "null argument");
   if (h->K == 0) return set_error(DTFE_ERR_STATE, "sub-boxes not set");
   if (h->T == 0) return set_error(DTFE_ERR_DEGENERATE, "no tetrahedra");
   if (!h->density_ready) return set_error(DTFE_ERR_STATE, "vertex density not computed");
   int method = o->method;
-  if (method != DTFE_METHOD_CENTRE && method != DTFE_METHOD_MONTE_CARLO && method != DTFE_METHOD_EQUIDISTANT)
+  if (method != DTFE_METHOD_CENTRE && method != DTFE_METHOD_TETRAHEDRA && method != DTFE_METHOD_MONTE_CARLO &&
+      method != DTFE_METHOD_EQUIDISTANT)
     return set_error(DTFE_ERR_ARG, "unknown method");
   int NN = method == DTFE_METHOD_CENTRE ? 1 : o->n_samples;
   if (NN < 1) return set_error(DTFE_ERR_ARG, "n_samples must be >= 1");
@@ -1516,6 +1552,20 @@ static int interp_enqueue(dtfe_handle h, const dtfe_interp_opts* o, float* const
     return set_error(DTFE_ERR_ARG, "scalar fields requested but n_scalars == 0");
   for (int s = 0; s < DTFE_NUM_FIELDS; ++s)
     if ((F >> s & 1u) && !out_dev[s]) return set_error(DTFE_ERR_ARG, "missing output buffer");
+  if (method == DTFE_METHOD_TETRAHEDRA) {
+    // points inside the tetrahedra, gathered per cell (method1.cu)
+    DTFE_CUDA_TRY(cudaMemsetAsync(h->counters, 0, sizeof(unsigned long long) * CNT_N, h->stream));
+    float* outs[DTFE_NUM_FIELDS];
+    for (int s = 0; s < DTFE_NUM_FIELDS; ++s) outs[s] = (F >> s & 1u) ? out_dev[s] : nullptr;
+    const int rc1 = dtfe_internal_method1(h->stream, h->K, h->boxes_h.data(), h->boxes, h->regions_h.data(),
+                                          h->n_cells, h->grid[1], h->grid[2], h->T, h->tet_v, h->posd,
+                                          h->has_vel ? h->vel4 : nullptr, h->S > 0 ? h->scal : nullptr, h->S, NN,
+                                          F, (o->flags & DTFE_FLAG_FIX_VALUE_INTERP) ? 1 : 0, outs, &h->m1_table,
+                                          &h->m1_table_nn, &h->m1_scratch, &h->m1_bytes, &h->m1_lists,
+                                          &h->m1_lists_bytes);
+    h->tet_c_valid = false;
+    return rc1;
+  }
   int rc = prepare_centres(h);
   if (rc) return rc;
   cudaStream_t st = h->stream;
@@ -1846,6 +1896,8 @@ int dtfe_gpu_interpolate_dev(dtfe_handle h, const dtfe_interp_opts* opts,
 int dtfe_gpu_graph_build(dtfe_handle h, double rho_bar, const dtfe_interp_opts* opts,
                          float* const out_dev[DTFE_NUM_FIELDS]) {
   if (!h || !opts) return set_error(DTFE_ERR_ARG, "null argument");
+  if (opts->method == DTFE_METHOD_TETRAHEDRA)
+    return set_error(DTFE_ERR_ARG, "averaging method 1 sizes its lists on the host: not capturable");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
   drop_graph(h);
   // one plain step first: allocations, equidistant offsets and the walk

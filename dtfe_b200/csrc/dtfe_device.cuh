@@ -46,7 +46,7 @@ __device__ __forceinline__ void load_pos(const float4* __restrict__ posd, int v,
 
 // Exact sign of orient(tetrahedron with vertex `face` replaced by p).  All
 // arguments by value: the caller's arrays stay in registers.
-__device__ __noinline__ int exact_face_sign(float x0, float y0, float z0, float x1, float y1, float z1,
+static __device__ __noinline__ int exact_face_sign(float x0, float y0, float z0, float x1, float y1, float z1,
                                             float x2, float y2, float z2, float x3, float y3, float z3,
                                             double px, double py, double pz, int face) {
   double Q[4][3] = {{x0, y0, z0}, {x1, y1, z1}, {x2, y2, z2}, {x3, y3, z3}};
@@ -136,7 +136,7 @@ constexpr float kOrientErr32 = 12.0f * 5.9604645e-8f;  // 12 * 2^-24
 constexpr float kPermFloor32 = 1e-30f;
 
 // Returns (sign + 1) | (4 if exact arithmetic was needed).
-__device__ __noinline__ int face_sign_fp64(float x0, float y0, float z0, float x1, float y1, float z1,
+static __device__ __noinline__ int face_sign_fp64(float x0, float y0, float z0, float x1, float y1, float z1,
                                            float x2, float y2, float z2, float x3, float y3, float z3,
                                            double px, double py, double pz, int face) {
   double Q[4][3] = {{x0, y0, z0}, {x1, y1, z1}, {x2, y2, z2}, {x3, y3, z3}};
@@ -236,7 +236,7 @@ __device__ __forceinline__ int nb_of(const int4& n, int i) {
 }
 
 // True if the closure of tetrahedron t holds p; zmask marks faces through p.
-__device__ __noinline__ bool tet_contains(const int4* __restrict__ tet_v, const float4* __restrict__ posd,
+static __device__ __noinline__ bool tet_contains(const int4* __restrict__ tet_v, const float4* __restrict__ posd,
                                           int t, double px, double py, double pz, int& zmask, int& nexact) {
   int v[4];
   float X[4][3];
@@ -249,7 +249,7 @@ __device__ __noinline__ bool tet_contains(const int4* __restrict__ tet_v, const 
 // p, found by exploring across faces that pass through p.  Bounded: keeps
 // the best so far after kTieMax tetrahedra.
 constexpr int kTieMax = 96;
-__device__ __noinline__ int canonical_tie(const int4* __restrict__ tet_v, const int4* __restrict__ tet_n,
+static __device__ __noinline__ int canonical_tie(const int4* __restrict__ tet_v, const int4* __restrict__ tet_n,
                                           const float4* __restrict__ posd, int t, int zmask,
                                           double px, double py, double pz) {
   int nexact = 0;  // exact tests inside tie resolution are not counted

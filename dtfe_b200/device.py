@@ -73,6 +73,13 @@ class DeviceDTFE:
             self.h, plan.n_boxes, C.addressof(plan.boxes), N.ptr(plan.xs), len(plan.xs),
             N.ptr(plan.ys), len(plan.ys), N.ptr(plan.zs), len(plan.zs), grid.ctypes.data))
         self.grid = tuple(plan.grid)
+        if getattr(plan, "regions", None) is not None:
+            self.set_regions(plan.regions)
+
+    def set_regions(self, regions: np.ndarray) -> None:
+        """Tile regions (K, 6) for averaging method 1 (dtfe_gpu_set_regions)."""
+        r = np.ascontiguousarray(regions, np.float32).reshape(-1, 6)
+        N.check(self.lib.dtfe_gpu_set_regions(self.h, len(r), r.ctypes.data))
 
     def load(self, plan) -> None:
         self.upload(plan)

@@ -68,6 +68,10 @@ enum {
 /* ---- interpolation methods (User_options::method, plus plain sampling) -- */
 enum {
   DTFE_METHOD_CENTRE = 0,       /* field at the cell centre (uQuantities) */
+  DTFE_METHOD_TETRAHEDRA = 1,   /* n points per cell on average, placed in
+                                   the tetrahedra (Sobol) and scattered to
+                                   the cells (interpolateGrid_averaged_1,
+                                   averaged_interpolation_1.cc:197-421)   */
   DTFE_METHOD_MONTE_CARLO = 2,  /* mean of n random points per cell       */
   DTFE_METHOD_EQUIDISTANT = 3   /* mean of n = m^3 equidistant points     */
 };
@@ -155,10 +159,19 @@ int dtfe_gpu_chain_uploads(dtfe_handle h, dtfe_handle after);
 
 /* Describe the sub-boxes and the main grid.  xs/ys/zs hold the sample
  * coordinates of every tile along each axis (the reference's running
- * float sums x += dx, unaveraged_interpolation.cc:270-358). */
+ * float sums x += dx, unaveraged_interpolation.cc:270-358).  The tile
+ * regions default to lo + dx * tile_dims; dtfe_gpu_set_regions gives the
+ * exact ones. */
 int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* boxes,
                           const float* xs, int64_t n_xs, const float* ys, int64_t n_ys,
                           const float* zs, int64_t n_zs, const int32_t grid[3]);
+/* The region of every sub-box's tile (6 floats per sub-box: xmin, xmax,
+ * ymin, ymax, zmin, zmax; the reference's per-thread userOptions.region,
+ * src/DTFE.cpp:331-356), after dtfe_gpu_set_subboxes.  Averaging method 1
+ * skips tetrahedra whose bounding box misses it
+ * (averaged_interpolation_1.cc:67-77).  Each xmin/ymin/zmin must equal the
+ * sub-box's lo. */
+int dtfe_gpu_set_regions(dtfe_handle h, int32_t n_boxes, const float* regions);
 
 /* Vertex densities rho_v = w_v (D+1) / (rho_bar * sum of incident volumes),
  * 0 on the hull (vertexDensity, triangulation.cpp:200-279). */

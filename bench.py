@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mc", action="store_true")
+    ap.add_argument("--no-m1", action="store_true")
+    ap.add_argument("--m1-points", type=int, default=100, help="method-1 points per cell (reference default 100)")
     ap.add_argument("--bwd-n", type=int, default=128, help="particles per side of the backward workload")
     ap.add_argument("--no-bwd", action="store_true")
     ap.add_argument("--fd-particles", type=int, default=1000)
@@ -662,6 +664,26 @@ def run_ours(args):
         mc = {"cells_per_s": G / tm, "point_evals_per_s": 9 * G / tm, "ms_per_step": 1e3 * tm,
               "n_samples": 8, "method": 2}
 
+    # averaging method 1 (the reference's default: 100 points per cell on
+    # average, placed in the tetrahedra): grid cells/s of whole steps
+    m1 = None
+    if side and not args.no_m1:
+        from dtfe_b200 import _native as N1
+        for _ in range(2):
+            dev.vertex_density(plan.rho_bar)
+            dev.interpolate_dev(FIELDS, outs, method=N1.METHOD_TETRAHEDRA, n_samples=args.m1_points)
+        dev.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            dev.vertex_density(plan.rho_bar)
+            dev.interpolate_dev(FIELDS, outs, method=N1.METHOD_TETRAHEDRA, n_samples=args.m1_points)
+        e1.record(stream)
+        e1.synchronize()
+        tm = e0.elapsed_time(e1) / 3e3
+        m1 = {"cells_per_s": G / tm, "ms_per_step": 1e3 * tm, "n_points": args.m1_points, "method": 1}
+
     # end to end through the C ABI with host buffers (pinned)
     e2e = None
     if args.e2e_steps > 0:
@@ -809,7 +831,7 @@ def run_ours(args):
         "e2e": e2e,
         "roofline": roofline,
         "cpu_baseline": cpu,
-        "mc": mc,
+        "mc": mc, "method1": m1,
         "backward": bwd,
         "batched_subboxes": batch,
         "comparison_estimators": compare,

@@ -40,6 +40,7 @@ inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct M1Box {
   float lo[3], hi[3], dx[3];
+  double inv_dx[3];  // 1 / dx in double (cell test fast path)
   int n[3];
   float gcv;  // dx0 dx1 dx2 in float
   int64_t tile;  // first flattened sample of the tile
@@ -136,12 +137,22 @@ __device__ __forceinline__ void m1_point(const M1Tet& m, const float* __restrict
   for (int c = 0; c < 3; ++c) p[c] = q0 * m.vM[0][c] + q1 * m.vM[1][c] + q2 * m.vM[2][c];
 }
 
+// floor(x / d) with x / d rounded as IEEE division: from x * (1/d) unless
+// that product lies within 1e-9 (relative) of an integer, where the rounded
+// quotient could fall on the other side; then by the division itself.
+__device__ __forceinline__ double floor_div(double x, double d, double inv) {
+  const double q = x * inv;
+  const double r = rint(q);
+  if (fabs(q - r) <= 1e-9 * fmax(fabs(q), 1.0)) return floor(x / d);
+  return floor(q);
+}
+
 // isGridCellIndex (:140-157): floor((basePosition + p) / dx) per axis
 __device__ __forceinline__ bool m1_cell(const M1Tet& m, const M1Box& B, const double p[3], int cell[3]) {
   bool ok = true;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const double f = floor(((double)m.bp[c] + p[c]) / (double)B.dx[c]);
+    const double f = floor_div((double)m.bp[c] + p[c], (double)B.dx[c], B.inv_dx[c]);
     ok = ok && f >= 0.0 && f < (double)B.n[c];
     cell[c] = ok ? (int)f : 0;
   }
@@ -163,55 +174,74 @@ __device__ __forceinline__ void load_tet_f(const M1Params& P, int64_t t, int v[4
   }
 }
 
-// Cells receiving a tetrahedron's contributions; calls emit(flattened sample)
-// once per cell (a superset only for tetrahedra wider than the window).
+// Cells receiving a tetrahedron's contributions: emit(flattened sample,
+// point mask) once per cell.  The mask marks the points (of at most 32) that
+// fall in the cell; 0 means "test every point" (single-cell tetrahedra, more
+// than 32 points, or a tetrahedron wider than the 4x4x4 window, whose range
+// of hit cells is emitted: a superset).
+constexpr int kMaskPoints = 32;
 template <class Emit>
 __device__ __forceinline__ void m1_for_cells(const M1Params& P, int b, const M1Tet& m, Emit emit) {
   const M1Box& B = P.boxes[b];
   if (m.np == 0) {
-    emit(B.tile + ((int64_t)m.one[0] * B.n[1] + m.one[1]) * B.n[2] + m.one[2]);
+    emit(B.tile + ((int64_t)m.one[0] * B.n[1] + m.one[1]) * B.n[2] + m.one[2], 0u);
     return;
   }
-  unsigned long long mask = 0ull;
+  unsigned long long cells = 0ull;
+  unsigned char win[kMaskPoints];
   int ref[3] = {0, 0, 0}, lo[3] = {0, 0, 0}, hi[3] = {-1, -1, -1};
   bool any = false, wide = false;
+  const bool masks = m.np <= kMaskPoints;
   for (int i = 0; i < m.np; ++i) {
     double p[3];
     m1_point(m, P.table, i, p);
     int c[3];
-    if (!m1_cell(m, B, p, c)) continue;
-    if (!any) {
-      any = true;
+    unsigned char w = 0xFF;
+    if (m1_cell(m, B, p, c)) {
+      if (!any) {
+        any = true;
 #pragma unroll
-      for (int a = 0; a < 3; ++a) ref[a] = lo[a] = hi[a] = c[a];
-    }
+        for (int a = 0; a < 3; ++a) ref[a] = lo[a] = hi[a] = c[a];
+      }
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      lo[a] = min(lo[a], c[a]);
-      hi[a] = max(hi[a], c[a]);
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = min(lo[a], c[a]);
+        hi[a] = max(hi[a], c[a]);
+      }
+      const int ox = c[0] - ref[0] + 1, oy = c[1] - ref[1] + 1, oz = c[2] - ref[2] + 1;
+      if (ox < 0 || ox > 3 || oy < 0 || oy > 3 || oz < 0 || oz > 3) {
+        wide = true;
+      } else {
+        w = (unsigned char)(ox * 16 + oy * 4 + oz);
+        cells |= 1ull << w;
+      }
     }
-    const int ox = c[0] - ref[0] + 1, oy = c[1] - ref[1] + 1, oz = c[2] - ref[2] + 1;
-    if (ox < 0 || ox > 3 || oy < 0 || oy > 3 || oz < 0 || oz > 3) wide = true;
-    else mask |= 1ull << (ox * 16 + oy * 4 + oz);
+    if (masks) win[i] = w;
   }
   if (!any) return;
   if (!wide) {
-    while (mask) {
-      const int bit = __ffsll((long long)mask) - 1;
-      mask &= mask - 1;
+    while (cells) {
+      const int bit = __ffsll((long long)cells) - 1;
+      cells &= cells - 1;
+      unsigned pm = 0u;
+      if (masks)
+        for (int i = 0; i < m.np; ++i) pm |= (win[i] == bit ? 1u : 0u) << i;
       const int ci = ref[0] + (bit >> 4) - 1, cj = ref[1] + ((bit >> 2) & 3) - 1, ck = ref[2] + (bit & 3) - 1;
-      emit(B.tile + ((int64_t)ci * B.n[1] + cj) * B.n[2] + ck);
+      emit(B.tile + ((int64_t)ci * B.n[1] + cj) * B.n[2] + ck, pm);
     }
     return;
   }
   for (int ci = lo[0]; ci <= hi[0]; ++ci)
     for (int cj = lo[1]; cj <= hi[1]; ++cj)
-      for (int ck = lo[2]; ck <= hi[2]; ++ck) emit(B.tile + ((int64_t)ci * B.n[1] + cj) * B.n[2] + ck);
+      for (int ck = lo[2]; ck <= hi[2]; ++ck) emit(B.tile + ((int64_t)ci * B.n[1] + cj) * B.n[2] + ck, 0u);
 }
 
+// list entries: tetrahedron << 32 | point mask (sorting them orders by
+// tetrahedron)
 template <int FILL>
 __global__ void __launch_bounds__(256) k_m1_cells(M1Params P, unsigned long long* __restrict__ cnt,
-                                                  const int64_t* __restrict__ off, int* __restrict__ list) {
+                                                  const int64_t* __restrict__ off,
+                                                  unsigned long long* __restrict__ list) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= P.T) return;
   if (t < __ldg(&P.tet_prefix[0]) || t >= __ldg(&P.tet_prefix[P.K])) return;
@@ -221,22 +251,22 @@ __global__ void __launch_bounds__(256) k_m1_cells(M1Params P, unsigned long long
   load_tet_f(P, t, v, X);
   M1Tet m;
   if (!m1_setup(X, P.boxes[b], P.NN, m)) return;
-  m1_for_cells(P, b, m, [&](int64_t s) {
+  m1_for_cells(P, b, m, [&](int64_t s, unsigned pm) {
     if (FILL) {
       const unsigned long long k = atomicAdd(&cnt[s], 1ull);
-      list[off[s] + (int64_t)k] = (int)t;
+      list[off[s] + (int64_t)k] = ((unsigned long long)t << 32) | pm;
     } else {
       atomicAdd(&cnt[s], 1ull);
     }
   });
 }
 
-__global__ void k_m1_sort(int64_t n, const int64_t* __restrict__ off, int* __restrict__ list) {
+__global__ void k_m1_sort(int64_t n, const int64_t* __restrict__ off, unsigned long long* __restrict__ list) {
   const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (s >= n) return;
   const int64_t a = off[s], e = off[s + 1];
   for (int64_t i = a + 1; i < e; ++i) {
-    const int x = list[i];
+    const unsigned long long x = list[i];
     int64_t j = i - 1;
     while (j >= a && list[j] > x) {
       list[j + 1] = list[j];
@@ -248,7 +278,7 @@ __global__ void k_m1_sort(int64_t n, const int64_t* __restrict__ off, int* __res
 
 template <int S>
 __global__ void __launch_bounds__(128) k_m1_gather(M1Params P, const int64_t* __restrict__ off,
-                                                   const int* __restrict__ list) {
+                                                   const unsigned long long* __restrict__ list) {
   const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (s >= P.n_cells) return;
   // the cell of flattened sample s (tile order: sub-box, then x, y, z fastest)
@@ -275,7 +305,9 @@ __global__ void __launch_bounds__(128) k_m1_gather(M1Params P, const int64_t* __
 #pragma unroll
   for (int q = 0; q < (S > 0 ? 3 * S : 1); ++q) aSG[q] = 0.f;
   for (int64_t e = off[s]; e < off[s + 1]; ++e) {
-    const int t = list[e];
+    const unsigned long long pair = list[e];
+    const int t = (int)(pair >> 32);
+    const unsigned pm = (unsigned)pair;
     int v[4];
     float X[4][3];
     load_tet_f(P, t, v, X);
@@ -357,11 +389,9 @@ __global__ void __launch_bounds__(128) k_m1_gather(M1Params P, const int64_t* __
       }
       continue;
     }
-    for (int i = 0; i < m.np; ++i) {
-      double p[3];
-      m1_point(m, P.table, i, p);
-      int c[3];
-      if (!m1_cell(m, B, p, c) || c[0] != ci || c[1] != cj || c[2] != ck) continue;
+    // one point's contribution (densityValue, velocityValue, scalarValue and
+    // the gradients, each times vol / n; :336-355)
+    auto add_point = [&](const double p[3]) {
       const float f = m.factor;
       const float temp = (float)(p[0] * (double)gr[0] + p[1] * (double)gr[1] + p[2] * (double)gr[2]);
       aD += (dn[0] + temp) * f;
@@ -392,6 +422,22 @@ __global__ void __launch_bounds__(128) k_m1_gather(M1Params P, const int64_t* __
         aS[q] += (tmp + ss[0][q]) * f;
 #pragma unroll
         for (int cc = 0; cc < 3; ++cc) aSG[3 * q + cc] += SG[q][cc] * f;
+      }
+    };
+    // the points in this cell, in ascending order: the mask's, else every
+    // point that tests into the cell
+    if (pm) {
+      for (unsigned r = pm; r; r &= r - 1) {
+        double p[3];
+        m1_point(m, P.table, __ffs(r) - 1, p);
+        add_point(p);
+      }
+    } else {
+      for (int i = 0; i < m.np; ++i) {
+        double p[3];
+        m1_point(m, P.table, i, p);
+        int c[3];
+        if (m1_cell(m, B, p, c) && c[0] == ci && c[1] == cj && c[2] == ck) add_point(p);
       }
     }
   }
@@ -432,7 +478,7 @@ __global__ void __launch_bounds__(128) k_m1_gather(M1Params P, const int64_t* __
 }
 
 template <int S>
-void launch_gather(const M1Params& P, const int64_t* off, const int* list, cudaStream_t st) {
+void launch_gather(const M1Params& P, const int64_t* off, const unsigned long long* list, cudaStream_t st) {
   const unsigned nb = (unsigned)((P.n_cells + 127) / 128);
   k_m1_gather<S><<<nb, 128, 0, st>>>(P, off, list);
 }
@@ -483,6 +529,7 @@ extern "C" int dtfe_internal_method1(void* stream, int K, const dtfe_subbox* box
       B.n[c] = s.tile_dims[c];
     }
     B.gcv = B.dx[0] * B.dx[1] * B.dx[2];
+    for (int c = 0; c < 3; ++c) B.inv_dx[c] = 1.0 / (double)B.dx[c];
     B.tile = tile;
     B.G = (int64_t)B.n[0] * B.n[1] * B.n[2];
     tile += B.G;
@@ -548,7 +595,7 @@ extern "C" int dtfe_internal_method1(void* stream, int K, const dtfe_subbox* box
       cudaStreamSynchronize(st) != cudaSuccess)
     return dtfe_internal_set_error(DTFE_ERR_CUDA, "method-1 pair count");
   // the (cell, tetrahedron) lists in their own buffer
-  const size_t list_bytes = sizeof(int) * (size_t)(pairs > 0 ? pairs : 1);
+  const size_t list_bytes = sizeof(unsigned long long) * (size_t)(pairs > 0 ? pairs : 1);
   if (*lists_bytes < list_bytes) {
     if (*lists) cudaFree(*lists);
     *lists = nullptr;
@@ -557,7 +604,7 @@ extern "C" int dtfe_internal_method1(void* stream, int K, const dtfe_subbox* box
       return dtfe_internal_set_error(DTFE_ERR_ALLOC, "cudaMalloc (method-1 lists)");
     *lists_bytes = list_bytes;
   }
-  int* d_list = (int*)*lists;
+  unsigned long long* d_list = (unsigned long long*)*lists;
   if (cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * (n_cells + 1), st) != cudaSuccess)
     return dtfe_internal_set_error(DTFE_ERR_CUDA, "method-1 fill reset");
   if (T > 0) k_m1_cells<1><<<tb, 256, 0, st>>>(P, d_cnt, d_off, d_list);

@@ -18,12 +18,12 @@
 // As the reference: allParticles is cleared, userOptions.averageDensity is
 // set when it was negative (automatic), uQuantities receives the fields of
 // userOptions.uField (cell centres), aQuantities those of
-// userOptions.aField (method 2 or 3 averages, or the NGP/CIC/TSC/SPH grids).
+// userOptions.aField (method 1, 2 or 3 averages, or the NGP/CIC/TSC/SPH grids;
+// method 1 computes no velocity standard deviation, as the reference).
 // Unlike the reference, failures throw std::runtime_error instead of calling
 // exit(), and options this path does not cover throw as well: user sampling
 // points, redshift cones, --region, --partition, random subsamples, Poisson
-// particles, explicit padding lengths, averaging method 1, scalar fields with
-// NGP/CIC/TSC.  The GPU is device 0 unless DTFE_GPU_DEVICE names another.
+// particles, explicit padding lengths, scalar fields with NGP/CIC/TSC.  The GPU is device 0 unless DTFE_GPU_DEVICE names another.
 
 #include <omp.h>
 
@@ -114,7 +114,7 @@ void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& s
               "explicit padding lengths");
   unsupported(o.gridSize.size() != 3, "grids other than 3-D regular grids");
   const bool dtfe = !(o.NGP || o.CIC || o.TSC || o.SPH);
-  unsupported(dtfe && any(o.aField) && o.method != 2 && o.method != 3, "averaging method 1");
+  unsupported(dtfe && any(o.aField) && (o.method < 1 || o.method > 3), "averaging methods other than 1, 2, 3");
   unsupported(!dtfe && !o.SPH && (o.aField.scalar || o.aField.scalar_gradient), "scalar fields with NGP/CIC/TSC");
 
   const int64_t n = (int64_t)allParticles->size();
@@ -179,6 +179,7 @@ void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& s
         "upload");
   check(dtfe_gpu_set_subboxes(gpu.h, v.n_boxes, v.boxes, v.xs, v.n_xs, v.ys, v.n_ys, v.zs, v.n_zs, grid),
         "sub-boxes");
+  if (v.regions) check(dtfe_gpu_set_regions(gpu.h, v.n_boxes, v.regions), "sub-box regions");
   if (o.SPH) {
     const bool wv = o.aField.velocity, ws = o.aField.scalar;
     uint32_t f = DTFE_FIELD_BIT(DTFE_DENSITY) | (wv ? DTFE_FIELD_BIT(DTFE_VELOCITY) : 0u) |
@@ -199,9 +200,14 @@ void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& s
   }
   if (any(o.aField)) {
     float* out[DTFE_NUM_FIELDS];
-    dtfe_interp_opts io = {o.method == 2 ? DTFE_METHOD_MONTE_CARLO : DTFE_METHOD_EQUIDISTANT, o.noPoints,
-                           (uint64_t)o.randomSeed, 0, 0};
-    outputs(o.aField, aQuantities, G, out, &io.fields);
+    const int method = o.method == 1 ? DTFE_METHOD_TETRAHEDRA
+                                     : (o.method == 2 ? DTFE_METHOD_MONTE_CARLO : DTFE_METHOD_EQUIDISTANT);
+    dtfe_interp_opts io = {method, (int32_t)o.noPoints, (uint64_t)o.randomSeed, 0, 0};
+    Field f = o.aField;
+    // interpolateGrid_averaged_1 warns and leaves the standard deviation out
+    // (averaged_interpolation_1.cc:234-238)
+    if (method == DTFE_METHOD_TETRAHEDRA) f.velocity_std = false;
+    outputs(f, aQuantities, G, out, &io.fields);
     check(dtfe_gpu_interpolate(gpu.h, &io, out, &st), "averaged interpolation");
   }
 }

@@ -14,7 +14,7 @@ def _particles():
 
 def test_unsupported_options_throw(built):
     pos, w = _particles()
-    with pytest.raises(RuntimeError, match="averaging method 1"):
-        D.run("DTFE", pos, w, None, None, (8, 8, 8), a_fields=("density",), method=1)
+    with pytest.raises(RuntimeError, match="averaging methods other than 1, 2, 3"):
+        D.run("DTFE", pos, w, None, None, (8, 8, 8), a_fields=("density",), method=4)
     with pytest.raises(RuntimeError, match="scalar fields with NGP/CIC/TSC"):
         D.run("CIC", pos, w, None, None, (8, 8, 8), a_fields=("density", "scalar"))

@@ -86,3 +86,22 @@ def test_dropin_sph(particles):
         ref = dev.sph(plan.rho_bar, n_neighbors=32, velocity=True)
     assert np.array_equal(a["density"][:, 0], ref["density"])
     assert np.array_equal(a["velocity"], ref["velocity"])
+
+
+def test_dropin_method1(particles):
+    """The reference's default averaging (method 1, 100 points per cell)
+    through DTFE(): the device API's method 1 on the same plan, bit for bit;
+    no velocity standard deviation, as the reference."""
+    from dtfe_b200 import _native as N
+    from dtfe_b200.device import DeviceDTFE
+    pos, w, vel, sc = particles
+    _, a, _, _ = D.run("DTFE", pos, w, vel, sc, GRID, a_fields=["density", "velocity", "velocity_gradient", "scalar"],
+                       method=1, n_points=100)
+    plan = P.make_plan(pos, w, vel, sc[:, None], grid=GRID, n_threads=4)
+    with DeviceDTFE(0, 1) as dev:
+        dev.load(plan)
+        dev.vertex_density(plan.rho_bar)
+        ref = dev.interpolate(["density", "velocity", "velocity_gradient", "scalar"], method=N.METHOD_TETRAHEDRA,
+                              n_samples=100)
+    for f in ("density", "velocity", "velocity_gradient", "scalar"):
+        assert np.array_equal(a[f].reshape(ref[f].shape), ref[f]), f

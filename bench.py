@@ -182,6 +182,22 @@ def reference_code_step(plan, threads: int):
     return R.time_boxes(plan, threads)
 
 
+def reference_method1(plan, threads: int, n_points: int):
+    """The reference's own vertexDensity + interpolateGrid_averaged_1 on all
+    sub-boxes, one host thread each (the harness; None without it)."""
+    try:
+        import refharness as R
+    except ImportError:
+        return None
+    if not R.available():
+        return None
+    t, per_box = R.time_boxes(plan, threads, which=1, n_points=n_points)
+    G = int(np.prod(plan.grid))
+    return {"cells_per_s": G / t, "cores": min(threads, plan.n_boxes), "kind": "reference",
+            "step_s": t, "sample": f"the whole workload, {plan.n_boxes} sub-boxes on one host thread each; "
+                                   f"sub-boxes {min(per_box):.2f}-{max(per_box):.2f} s"}
+
+
 def cpu_baseline(plan, threads: int, target_s: float) -> dict:
     """The reference's own code on the host cores (reference_code_step) on
     the whole workload; without the harness, the CPU oracle in the
@@ -683,6 +699,8 @@ def run_ours(args):
         e1.synchronize()
         tm = e0.elapsed_time(e1) / 3e3
         m1 = {"cells_per_s": G / tm, "ms_per_step": 1e3 * tm, "n_points": args.m1_points, "method": 1}
+        if rank == 0 and not args.no_cpu:
+            m1["reference"] = reference_method1(plan, host_threads(args.threads), args.m1_points)
 
     # end to end through the C ABI with host buffers (pinned)
     e2e = None

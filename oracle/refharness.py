@@ -84,11 +84,12 @@ def _box_args(plan, box):
     return xyz, w, vel, tv, tn, dims, region
 
 
-def time_boxes(plan, threads: int):
+def time_boxes(plan, threads: int, which: int = 0, n_points: int = 1):
     """Times the reference's own per-thread work of DTFE_parallel
-    (src/DTFE.cpp:331-356): vertexDensity + interpolateGrid of density,
-    velocity and velocity gradient on every sub-box, the sub-boxes spread
-    over ``threads`` host threads as the reference's OpenMP team would.
+    (src/DTFE.cpp:331-356): vertexDensity + the interpolation ``which``
+    (0 interpolateGrid, 1/2/3 the averaging methods with ``n_points``) of
+    density, velocity and velocity gradient on every sub-box, the sub-boxes
+    spread over ``threads`` host threads as the reference's OpenMP team would.
     Returns (seconds of the slowest thread, per-box seconds); only the
     reference's calls are timed, not loading the tessellation."""
     from concurrent.futures import ThreadPoolExecutor
@@ -103,7 +104,8 @@ def time_boxes(plan, threads: int):
         sec = C.c_double(0.0)
         p = lambda a: None if a is None else a.ctypes.data
         rc = L.ref_interpolate_timed(len(xyz), p(xyz), p(w), p(vel), None, len(tv), p(tv), p(tn), p(region),
-                                     p(dims), 0, 1, 0, plan.rho_bar, None, None, p(dens), p(velo), p(grad),
+                                     p(dims), which, n_points, 0, plan.rho_bar, None, None, p(dens), p(velo),
+                                     p(grad),
                                      None, None, None, 7, C.byref(sec))
         if rc:
             raise RuntimeError(f"ref_interpolate_timed failed ({rc})")

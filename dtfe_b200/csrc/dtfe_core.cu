@@ -1023,7 +1023,7 @@ struct dtfe_gpu_s {
   void* sph_scratch = nullptr;    // SPH cell grids, neighbour bookkeeping, FP64 sums
   size_t sph_bytes = 0;
   std::vector<float> regions_h;   // 6 per sub-box: tile regions (averaging method 1)
-  float* m1_table = nullptr;      // method-1 Sobol points (100 NN x 3)
+  double* m1_table = nullptr;     // method-1 Sobol points (100 NN x 3)
   int m1_table_nn = 0;
   void* m1_scratch = nullptr;     // method-1 counts, offsets, scan scratch
   size_t m1_bytes = 0;
@@ -1530,7 +1530,7 @@ int dtfe_gpu_download_vertex_density(dtfe_handle h, float* dens) {
 int dtfe_internal_method1(void* stream, int K, const dtfe_subbox* boxes_h, const dtfe_subbox* boxes_d,
                           const float* regions_h, int64_t n_cells, int64_t G1, int64_t G2, int64_t T,
                           const int4* tet_v, const float4* posd, const float4* vel4, const float* scal, int S, int NN,
-                          uint32_t fields, int fix, float* const out[DTFE_NUM_FIELDS], float** table, int* table_nn,
+                          uint32_t fields, int fix, float* const out[DTFE_NUM_FIELDS], double** table, int* table_nn,
                           void** scratch, size_t* scratch_bytes, void** lists, size_t* lists_bytes);
 
 static int interp_enqueue(dtfe_handle h, const dtfe_interp_opts* o, float* const out_dev[DTFE_NUM_FIELDS]) {

@@ -55,7 +55,7 @@ struct M1Params {
   const M1Box* boxes;
   const int64_t* tet_prefix;  // K + 1
   const dtfe_subbox* sub;
-  const float* table;  // 3 per point
+  const double* table;  // 3 per point: the float Sobol values, held as doubles
   int K, NN, fix;
   int64_t T, n_cells, G1, G2;
   uint32_t fields;
@@ -130,9 +130,8 @@ __device__ __forceinline__ bool m1_setup(const float X[4][3], const M1Box& B, in
   return true;
 }
 
-__device__ __forceinline__ void m1_point(const M1Tet& m, const float* __restrict__ table, int i, double p[3]) {
-  const double q0 = (double)__ldg(&table[3 * i]), q1 = (double)__ldg(&table[3 * i + 1]),
-               q2 = (double)__ldg(&table[3 * i + 2]);
+__device__ __forceinline__ void m1_point(const M1Tet& m, const double* __restrict__ table, int i, double p[3]) {
+  const double q0 = __ldg(&table[3 * i]), q1 = __ldg(&table[3 * i + 1]), q2 = __ldg(&table[3 * i + 2]);
 #pragma unroll
   for (int c = 0; c < 3; ++c) p[c] = q0 * m.vM[0][c] + q1 * m.vM[1][c] + q2 * m.vM[2][c];
 }
@@ -142,9 +141,11 @@ __device__ __forceinline__ void m1_point(const M1Tet& m, const float* __restrict
 // quotient could fall on the other side; then by the division itself.
 __device__ __forceinline__ double floor_div(double x, double d, double inv) {
   const double q = x * inv;
-  const double r = rint(q);
-  if (fabs(q - r) <= 1e-9 * fmax(fabs(q), 1.0)) return floor(x / d);
-  return floor(q);
+  const double f = floor(q);
+  const double frac = q - f;  // exact
+  const double tol = 1e-9 * fmax(fabs(q), 1.0);
+  if (frac <= tol || frac >= 1.0 - tol) return floor(x / d);
+  return f;
 }
 
 // isGridCellIndex (:140-157): floor((basePosition + p) / dx) per axis
@@ -175,16 +176,16 @@ __device__ __forceinline__ void load_tet_f(const M1Params& P, int64_t t, int v[4
 }
 
 // Cells receiving a tetrahedron's contributions: emit(flattened sample,
-// point mask) once per cell.  The mask marks the points (of at most 32) that
+// point mask) once per cell.  The mask marks the points (of at most 64) that
 // fall in the cell; 0 means "test every point" (single-cell tetrahedra, more
-// than 32 points, or a tetrahedron wider than the 4x4x4 window, whose range
+// than 64 points, or a tetrahedron wider than the 4x4x4 window, whose range
 // of hit cells is emitted: a superset).
-constexpr int kMaskPoints = 32;
+constexpr int kMaskPoints = 64;
 template <class Emit>
 __device__ __forceinline__ void m1_for_cells(const M1Params& P, int b, const M1Tet& m, Emit emit) {
   const M1Box& B = P.boxes[b];
   if (m.np == 0) {
-    emit(B.tile + ((int64_t)m.one[0] * B.n[1] + m.one[1]) * B.n[2] + m.one[2], 0u);
+    emit(B.tile + ((int64_t)m.one[0] * B.n[1] + m.one[1]) * B.n[2] + m.one[2], 0ull);
     return;
   }
   unsigned long long cells = 0ull;
@@ -223,9 +224,9 @@ __device__ __forceinline__ void m1_for_cells(const M1Params& P, int b, const M1T
     while (cells) {
       const int bit = __ffsll((long long)cells) - 1;
       cells &= cells - 1;
-      unsigned pm = 0u;
+      unsigned long long pm = 0ull;
       if (masks)
-        for (int i = 0; i < m.np; ++i) pm |= (win[i] == bit ? 1u : 0u) << i;
+        for (int i = 0; i < m.np; ++i) pm |= (win[i] == bit ? 1ull : 0ull) << i;
       const int ci = ref[0] + (bit >> 4) - 1, cj = ref[1] + ((bit >> 2) & 3) - 1, ck = ref[2] + (bit & 3) - 1;
       emit(B.tile + ((int64_t)ci * B.n[1] + cj) * B.n[2] + ck, pm);
     }
@@ -233,15 +234,13 @@ __device__ __forceinline__ void m1_for_cells(const M1Params& P, int b, const M1T
   }
   for (int ci = lo[0]; ci <= hi[0]; ++ci)
     for (int cj = lo[1]; cj <= hi[1]; ++cj)
-      for (int ck = lo[2]; ck <= hi[2]; ++ck) emit(B.tile + ((int64_t)ci * B.n[1] + cj) * B.n[2] + ck, 0u);
+      for (int ck = lo[2]; ck <= hi[2]; ++ck) emit(B.tile + ((int64_t)ci * B.n[1] + cj) * B.n[2] + ck, 0ull);
 }
 
-// list entries: tetrahedron << 32 | point mask (sorting them orders by
-// tetrahedron)
+// list entries: {tetrahedron, point mask}, sorted by tetrahedron
 template <int FILL>
 __global__ void __launch_bounds__(256) k_m1_cells(M1Params P, unsigned long long* __restrict__ cnt,
-                                                  const int64_t* __restrict__ off,
-                                                  unsigned long long* __restrict__ list) {
+                                                  const int64_t* __restrict__ off, ulonglong2* __restrict__ list) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= P.T) return;
   if (t < __ldg(&P.tet_prefix[0]) || t >= __ldg(&P.tet_prefix[P.K])) return;
@@ -251,24 +250,24 @@ __global__ void __launch_bounds__(256) k_m1_cells(M1Params P, unsigned long long
   load_tet_f(P, t, v, X);
   M1Tet m;
   if (!m1_setup(X, P.boxes[b], P.NN, m)) return;
-  m1_for_cells(P, b, m, [&](int64_t s, unsigned pm) {
+  m1_for_cells(P, b, m, [&](int64_t s, unsigned long long pm) {
     if (FILL) {
       const unsigned long long k = atomicAdd(&cnt[s], 1ull);
-      list[off[s] + (int64_t)k] = ((unsigned long long)t << 32) | pm;
+      list[off[s] + (int64_t)k] = make_ulonglong2((unsigned long long)t, pm);
     } else {
       atomicAdd(&cnt[s], 1ull);
     }
   });
 }
 
-__global__ void k_m1_sort(int64_t n, const int64_t* __restrict__ off, unsigned long long* __restrict__ list) {
+__global__ void k_m1_sort(int64_t n, const int64_t* __restrict__ off, ulonglong2* __restrict__ list) {
   const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (s >= n) return;
   const int64_t a = off[s], e = off[s + 1];
   for (int64_t i = a + 1; i < e; ++i) {
-    const unsigned long long x = list[i];
+    const ulonglong2 x = list[i];
     int64_t j = i - 1;
-    while (j >= a && list[j] > x) {
+    while (j >= a && list[j].x > x.x) {
       list[j + 1] = list[j];
       --j;
     }
@@ -278,7 +277,7 @@ __global__ void k_m1_sort(int64_t n, const int64_t* __restrict__ off, unsigned l
 
 template <int S>
 __global__ void __launch_bounds__(128) k_m1_gather(M1Params P, const int64_t* __restrict__ off,
-                                                   const unsigned long long* __restrict__ list) {
+                                                   const ulonglong2* __restrict__ list) {
   const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (s >= P.n_cells) return;
   // the cell of flattened sample s (tile order: sub-box, then x, y, z fastest)
@@ -305,9 +304,9 @@ __global__ void __launch_bounds__(128) k_m1_gather(M1Params P, const int64_t* __
 #pragma unroll
   for (int q = 0; q < (S > 0 ? 3 * S : 1); ++q) aSG[q] = 0.f;
   for (int64_t e = off[s]; e < off[s + 1]; ++e) {
-    const unsigned long long pair = list[e];
-    const int t = (int)(pair >> 32);
-    const unsigned pm = (unsigned)pair;
+    const ulonglong2 pair = list[e];
+    const int t = (int)pair.x;
+    const unsigned long long pm = pair.y;
     int v[4];
     float X[4][3];
     load_tet_f(P, t, v, X);
@@ -389,20 +388,33 @@ __global__ void __launch_bounds__(128) k_m1_gather(M1Params P, const int64_t* __
       }
       continue;
     }
+    // the gradients in double once per tetrahedron (the point products below
+    // are double products of these float values)
+    const double grd[3] = {(double)gr[0], (double)gr[1], (double)gr[2]};
+    double VGd[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) VGd[i][j] = (double)VG[i][j];
+    double SGd[S > 0 ? S : 1][3];
+#pragma unroll
+    for (int q = 0; q < S; ++q)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) SGd[q][j] = (double)SG[q][j];
     // one point's contribution (densityValue, velocityValue, scalarValue and
     // the gradients, each times vol / n; :336-355)
     auto add_point = [&](const double p[3]) {
       const float f = m.factor;
-      const float temp = (float)(p[0] * (double)gr[0] + p[1] * (double)gr[1] + p[2] * (double)gr[2]);
+      const float temp = (float)(p[0] * grd[0] + p[1] * grd[1] + p[2] * grd[2]);
       aD += (dn[0] + temp) * f;
 #pragma unroll
       for (int cc = 0; cc < 3; ++cc) {
         float tmp = 0.f;
         if (fix) {
 #pragma unroll
-          for (int j = 0; j < 3; ++j) tmp = (float)((double)tmp + (double)VG[j][cc] * p[j]);
+          for (int j = 0; j < 3; ++j) tmp = (float)((double)tmp + VGd[j][cc] * p[j]);
         } else {
-          tmp = (float)((double)VG[2][cc] * p[2]);
+          tmp = (float)(VGd[2][cc] * p[2]);
         }
         aV[cc] += (tmp + vv[0][cc]) * f;
       }
@@ -415,9 +427,9 @@ __global__ void __launch_bounds__(128) k_m1_gather(M1Params P, const int64_t* __
         float tmp = 0.f;
         if (fix) {
 #pragma unroll
-          for (int j = 0; j < 3; ++j) tmp = (float)((double)tmp + (double)SG[q][j] * p[j]);
+          for (int j = 0; j < 3; ++j) tmp = (float)((double)tmp + SGd[q][j] * p[j]);
         } else {
-          tmp = (float)((double)SG[q][2] * p[2]);
+          tmp = (float)(SGd[q][2] * p[2]);
         }
         aS[q] += (tmp + ss[0][q]) * f;
 #pragma unroll
@@ -427,9 +439,9 @@ __global__ void __launch_bounds__(128) k_m1_gather(M1Params P, const int64_t* __
     // the points in this cell, in ascending order: the mask's, else every
     // point that tests into the cell
     if (pm) {
-      for (unsigned r = pm; r; r &= r - 1) {
+      for (unsigned long long r = pm; r; r &= r - 1) {
         double p[3];
-        m1_point(m, P.table, __ffs(r) - 1, p);
+        m1_point(m, P.table, __ffsll((long long)r) - 1, p);
         add_point(p);
       }
     } else {
@@ -478,7 +490,7 @@ __global__ void __launch_bounds__(128) k_m1_gather(M1Params P, const int64_t* __
 }
 
 template <int S>
-void launch_gather(const M1Params& P, const int64_t* off, const unsigned long long* list, cudaStream_t st) {
+void launch_gather(const M1Params& P, const int64_t* off, const ulonglong2* list, cudaStream_t st) {
   const unsigned nb = (unsigned)((P.n_cells + 127) / 128);
   k_m1_gather<S><<<nb, 128, 0, st>>>(P, off, list);
 }
@@ -496,7 +508,7 @@ extern "C" int dtfe_internal_method1(void* stream, int K, const dtfe_subbox* box
                                      const float* regions_h, int64_t n_cells, int64_t G1, int64_t G2, int64_t T,
                                      const int4* tet_v, const float4* posd, const float4* vel4, const float* scal,
                                      int S, int NN, uint32_t fields, int fix, float* const out[DTFE_NUM_FIELDS],
-                                     float** table, int* table_nn, void** scratch, size_t* scratch_bytes,
+                                     double** table, int* table_nn, void** scratch, size_t* scratch_bytes,
                                      void** lists, size_t* lists_bytes) {
   cudaStream_t st = (cudaStream_t)stream;
   if (NN < 1 || NN > (1 << 20)) return dtfe_internal_set_error(DTFE_ERR_ARG, "method 1 needs 1..2^20 points per cell");
@@ -504,14 +516,15 @@ extern "C" int dtfe_internal_method1(void* stream, int K, const dtfe_subbox* box
   // point table (first 100 NN simplex points)
   if (*table_nn != NN) {
     const size_t np = 100 * (size_t)NN;
-    std::vector<float> h(3 * np);
-    sobol_simplex_table(np, h.data());
+    std::vector<float> hf(3 * np);
+    sobol_simplex_table(np, hf.data());
+    std::vector<double> h(hf.begin(), hf.end());  // exact: the reference multiplies these floats in double
     if (*table) cudaFree(*table);
     *table = nullptr;
     *table_nn = 0;
-    if (cudaMalloc((void**)table, sizeof(float) * h.size()) != cudaSuccess)
+    if (cudaMalloc((void**)table, sizeof(double) * h.size()) != cudaSuccess)
       return dtfe_internal_set_error(DTFE_ERR_ALLOC, "cudaMalloc (method-1 points)");
-    if (cudaMemcpyAsync(*table, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+    if (cudaMemcpyAsync(*table, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
       return dtfe_internal_set_error(DTFE_ERR_CUDA, "uploading the method-1 points");
     *table_nn = NN;
@@ -595,7 +608,7 @@ extern "C" int dtfe_internal_method1(void* stream, int K, const dtfe_subbox* box
       cudaStreamSynchronize(st) != cudaSuccess)
     return dtfe_internal_set_error(DTFE_ERR_CUDA, "method-1 pair count");
   // the (cell, tetrahedron) lists in their own buffer
-  const size_t list_bytes = sizeof(unsigned long long) * (size_t)(pairs > 0 ? pairs : 1);
+  const size_t list_bytes = sizeof(ulonglong2) * (size_t)(pairs > 0 ? pairs : 1);
   if (*lists_bytes < list_bytes) {
     if (*lists) cudaFree(*lists);
     *lists = nullptr;
@@ -604,7 +617,7 @@ extern "C" int dtfe_internal_method1(void* stream, int K, const dtfe_subbox* box
       return dtfe_internal_set_error(DTFE_ERR_ALLOC, "cudaMalloc (method-1 lists)");
     *lists_bytes = list_bytes;
   }
-  unsigned long long* d_list = (unsigned long long*)*lists;
+  ulonglong2* d_list = (ulonglong2*)*lists;
   if (cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * (n_cells + 1), st) != cudaSuccess)
     return dtfe_internal_set_error(DTFE_ERR_CUDA, "method-1 fill reset");
   if (T > 0) k_m1_cells<1><<<tb, 256, 0, st>>>(P, d_cnt, d_off, d_list);

@@ -31,6 +31,7 @@
 #include <cstdint>
 
 #include "../../include/dtfe_gpu.h"
+#include "tile_index.cuh"
 #include "predicates.h"
 
 namespace {
@@ -102,7 +103,8 @@ __global__ void k_adjoint_cells(AdjCellParams P) {
   const dtfe_subbox& B = P.boxes[b];
   const int64_t local = s - P.tile_prefix[b];
   const int nz = B.tile_dims[2], ny = B.tile_dims[1];
-  const int k = (int)(local % nz), j = (int)((local / nz) % ny), i = (int)(local / ((int64_t)nz * ny));
+  int i, j, k;
+  tile_ijk(local, ny, nz, i, j, k);
   const int64_t cell = ((int64_t)(B.tile_origin[0] + i) * P.G1 + (B.tile_origin[1] + j)) * P.G2 + (B.tile_origin[2] + k);
   const double wa = P.a ? (double)P.a[cell] : 0.0;
   const double wb = P.b ? (double)P.b[cell] : 0.0;

@@ -35,6 +35,7 @@
 #include "../../include/dtfe_gpu.h"
 #include "dtfe_device.cuh"
 #include "philox.h"
+#include "tile_index.cuh"
 
 using namespace dtfe;
 
@@ -333,7 +334,8 @@ constexpr int kVolBlock = 256;
 // Morton-sorted, so neighbouring lanes often bin to the same cell: a
 // segmented minimum over each run of equal cells in the warp leaves one
 // atomic per run.  The seed only starts the walk (the located tetrahedron
-// does not depend on it), so the centroid's cell uses a reciprocal.
+// does not depend on it), so the centroid's cell uses a fast approximate
+// division (the range checks keep the index in the tile).
 constexpr unsigned long long kEmptySeed = ~0ull;
 template <bool DO_BINS>
 __global__ void __launch_bounds__(kVolBlock) k_tet_volume_bins(
@@ -365,7 +367,7 @@ __global__ void __launch_bounds__(kVolBlock) k_tet_volume_bins(
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         cen[c] = 0.25f * ((X[0][c] + X[1][c]) + (X[2][c] + X[3][c]));
-        const float f = floorf((cen[c] - __ldg(&B.lo[c])) * __frcp_rn(__ldg(&B.dx[c])));
+        const float f = floorf(__fdividef(cen[c] - __ldg(&B.lo[c]), __ldg(&B.dx[c])));
         const int n = __ldg(&B.tile_dims[c]);
         inside = inside && (f >= 0.f && f < (float)n);
         idx[c] = inside ? (int)f : 0;
@@ -628,9 +630,7 @@ __device__ __forceinline__ SampleCell sample_cell(const InterpParams& P, int64_t
   const dtfe_subbox& B = P.boxes[c.b];
   c.local = s - __ldg(&P.tile_prefix[c.b]);
   const int nz = B.tile_dims[2], ny = B.tile_dims[1];
-  c.k = (int)(c.local % nz);
-  c.j = (int)((c.local / nz) % ny);
-  c.i = (int)(c.local / ((int64_t)nz * ny));
+  tile_ijk(c.local, ny, nz, c.i, c.j, c.k);
   c.x = __ldg(&P.xs[B.coord_offset[0] + c.i]);
   c.y = __ldg(&P.ys[B.coord_offset[1] + c.j]);
   c.z = __ldg(&P.zs[B.coord_offset[2] + c.k]);

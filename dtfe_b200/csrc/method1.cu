@@ -29,6 +29,7 @@
 #include "../../include/dtfe_gpu.h"
 #include "dtfe_device.cuh"
 #include "sobol.h"
+#include "tile_index.cuh"
 
 extern "C" int dtfe_internal_set_error(int code, const char* msg);
 
@@ -293,8 +294,8 @@ __global__ void __launch_bounds__(128) k_m1_gather(M1Params P, const int64_t* __
   }
   const M1Box& B = P.boxes[b];
   const int64_t local = s - B.tile;
-  const int ck = (int)(local % B.n[2]), cj = (int)((local / B.n[2]) % B.n[1]),
-            ci = (int)(local / ((int64_t)B.n[2] * B.n[1]));
+  int ci, cj, ck;
+  tile_ijk(local, B.n[1], B.n[2], ci, cj, ck);
   const bool fix = P.fix != 0;
   const bool has_vel = P.vel4 != nullptr;
   float aD = 0.f, aV[3] = {0.f, 0.f, 0.f}, aG[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};

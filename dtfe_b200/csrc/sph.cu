@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "../../include/dtfe_gpu.h"
+#include "tile_index.cuh"
 
 extern "C" int dtfe_internal_set_error(int code, const char* msg);
 
@@ -325,9 +326,7 @@ __device__ __forceinline__ Sample sample_of(const SphParams& P, int64_t s) {
   const dtfe_subbox& B = P.boxes[c.b];
   c.local = s - P.tile_prefix[c.b];
   const int nz = B.tile_dims[2], ny = B.tile_dims[1];
-  c.k = (int)(c.local % nz);
-  c.j = (int)((c.local / nz) % ny);
-  c.i = (int)(c.local / ((int64_t)nz * ny));
+  tile_ijk(c.local, ny, nz, c.i, c.j, c.k);
   return c;
 }
 

@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mc", action="store_true")
     ap.add_argument("--no-m1", action="store_true")
+    ap.add_argument("--variants", default="", help="locate,eval launch variants (default: autotune)")
     ap.add_argument("--m1-points", type=int, default=100, help="method-1 points per cell (reference default 100)")
     ap.add_argument("--bwd-n", type=int, default=128, help="particles per side of the backward workload")
     ap.add_argument("--no-bwd", action="store_true")
@@ -621,7 +622,11 @@ def run_ours(args):
         return dev.interpolate_dev(FIELDS, outs, method=0)
 
     dev.vertex_density(plan.rho_bar)
-    variants = dev.autotune(FIELDS)
+    if args.variants:
+        variants = tuple(int(x) for x in args.variants.split(","))
+        dev.set_variants(*variants)
+    else:
+        variants = dev.autotune(FIELDS)
 
     for _ in range(args.warmup):
         step()

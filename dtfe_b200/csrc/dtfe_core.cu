@@ -991,8 +991,11 @@ struct dtfe_gpu_s {
   int64_t* bin_offset = nullptr;
   unsigned long long* bins = nullptr;
   int* tet_c = nullptr;   // located tetrahedron of every cell centre
-  int loc_variant = 0;    // launch variants (dtfe_gpu_autotune)
-  int eval_variant = 0;
+  // launch variants (dtfe_gpu_autotune); the defaults are the ones it picks
+  // on the 128^3 and 256^3 Zel'dovich workloads: seeded walk at 4 blocks
+  // per SM, evaluation at 4 blocks per SM
+  int loc_variant = 5;
+  int eval_variant = 2;
   int64_t n_cells = 0;
   float *xs = nullptr, *ys = nullptr, *zs = nullptr;
   int32_t grid[3] = {0, 0, 0};

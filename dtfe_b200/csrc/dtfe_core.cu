@@ -785,6 +785,87 @@ __global__ void __launch_bounds__(kInterpBlock, MINB) k_eval_centre(InterpParams
   if (P.count_centres) fold_counters(P, n_loc, n_out, 0, WalkStats{0, 0, 0});
 }
 
+// Cell centres located and evaluated in one pass (locate variants 9..11):
+// each lane walks from its seed as k_locate_cells does, then evaluates with
+// the tetrahedron the walk ends in, whose vertices and positions are still
+// in registers; the warp is converged again after the walk, so the
+// evaluation and the staged stores run as in k_eval_centre.
+template <int S, int MINB>
+__global__ void __launch_bounds__(kInterpBlock, MINB) k_locate_eval(InterpParams P, int* __restrict__ tet_c) {
+  constexpr int CMAX = (3 * S > 9) ? 3 * S : 9;
+  __shared__ __align__(16) float s_stage[kInterpBlock / 32][32 * CMAX];
+  float* stage = s_stage[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const uint32_t F = P.fields;
+  const bool want_grad = has_field(F, DTFE_VELOCITY_GRADIENT) || has_field(F, DTFE_VELOCITY_DIVERGENCE) ||
+                         has_field(F, DTFE_VELOCITY_SHEAR) || has_field(F, DTFE_VELOCITY_VORTICITY);
+  const bool want_vel = has_field(F, DTFE_VELOCITY) || want_grad;
+  const bool want_dens = has_field(F, DTFE_DENSITY);
+  const bool want_sc = S > 0 && (has_field(F, DTFE_SCALAR) || has_field(F, DTFE_SCALAR_GRADIENT));
+  const bool fix = P.fix != 0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t base0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane;
+  WalkStats wst{0, 0, 0};
+  unsigned n_loc = 0, n_out = 0, n_fail = 0;
+  for (int64_t base = base0; base < P.n_total; base += stride) {
+    const int64_t s = base + lane;
+    const bool valid = s < P.n_total;
+    int64_t cell = -1;
+    CellOut e;
+    e.dens = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) e.vel[c] = 0.f;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) e.grad[c] = 0.f;
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+      e.sc[q] = 0.f;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) e.scg[3 * q + c] = 0.f;
+    }
+    if (valid) {
+      const SampleCell c = sample_cell(P, s);
+      cell = c.cell;
+      // the walk ends with the located tetrahedron's vertices and positions
+      // in registers: the evaluation uses them directly
+      const double pc[3] = {(double)c.x, (double)c.y, (double)c.z};
+      int v[4];
+      float X[4][3];
+      int t = walk_locate<true>(P.tet_v, P.tet_n, P.posd, pc, seed_of(P, c), P.max_steps, v, X, wst);
+      ++n_loc;
+      if (t == kWalkFail) {
+        ++n_fail;
+        t = kOutside;
+      }
+      n_out += t < 0;
+      tet_c[s] = t;
+      if (t >= 0) cell_eval<S>(v, X, pc, P.posd, P.vel4, P.scal, want_dens, want_vel, want_sc, fix, e);
+    }
+    const int64_t c0 = __shfl_sync(0xffffffffu, cell, 0);
+    const bool contig = __all_sync(0xffffffffu, valid && cell == c0 + lane) && (c0 % 4 == 0);
+    if (has_field(F, DTFE_DENSITY)) store_field<1>(P.out[DTFE_DENSITY], cell, valid, &e.dens, contig, c0, stage);
+    if (has_field(F, DTFE_VELOCITY)) store_field<3>(P.out[DTFE_VELOCITY], cell, valid, e.vel, contig, c0, stage);
+    if (has_field(F, DTFE_VELOCITY_GRADIENT))
+      store_field<9>(P.out[DTFE_VELOCITY_GRADIENT], cell, valid, e.grad, contig, c0, stage);
+    if (has_field(F, DTFE_VELOCITY_DIVERGENCE) || has_field(F, DTFE_VELOCITY_SHEAR) ||
+        has_field(F, DTFE_VELOCITY_VORTICITY)) {
+      float dv, sh[5], vo[3];
+      derived_fields(e.grad, dv, sh, vo);
+      if (has_field(F, DTFE_VELOCITY_DIVERGENCE))
+        store_field<1>(P.out[DTFE_VELOCITY_DIVERGENCE], cell, valid, &dv, contig, c0, stage);
+      if (has_field(F, DTFE_VELOCITY_SHEAR))
+        store_field<5>(P.out[DTFE_VELOCITY_SHEAR], cell, valid, sh, contig, c0, stage);
+      if (has_field(F, DTFE_VELOCITY_VORTICITY))
+        store_field<3>(P.out[DTFE_VELOCITY_VORTICITY], cell, valid, vo, contig, c0, stage);
+    }
+    if (S > 0 && has_field(F, DTFE_SCALAR))
+      store_field<(S > 0 ? S : 1)>(P.out[DTFE_SCALAR], cell, valid, e.sc, contig, c0, stage);
+    if (S > 0 && has_field(F, DTFE_SCALAR_GRADIENT))
+      store_field<(S > 0 ? 3 * S : 1)>(P.out[DTFE_SCALAR_GRADIENT], cell, valid, e.scg, contig, c0, stage);
+  }
+  fold_counters(P, n_loc, n_out, n_fail, wst);
+}
+
 // Cell averages (methods 2 and 3): n points per cell, each walked from the
 // cell centre's tetrahedron (averaged_interpolation_2.cc:123,145), summed in
 // sample order as the reference does, divided by n; infinite-cell points are
@@ -991,10 +1072,10 @@ struct dtfe_gpu_s {
   int64_t* bin_offset = nullptr;
   unsigned long long* bins = nullptr;
   int* tet_c = nullptr;   // located tetrahedron of every cell centre
-  // launch variants (dtfe_gpu_autotune); the defaults are the ones it picks
-  // on the 128^3 and 256^3 Zel'dovich workloads: seeded walk at 4 blocks
-  // per SM, evaluation at 4 blocks per SM
-  int loc_variant = 5;
+  // launch variants (dtfe_gpu_autotune); the defaults are the fastest on
+  // the 256^3 Zel'dovich workload: seeded walk and evaluation in one kernel
+  // at 4 blocks per SM (evaluation variant 2 for the averaging methods)
+  int loc_variant = 11;
   int eval_variant = 2;
   int64_t n_cells = 0;
   float *xs = nullptr, *ys = nullptr, *zs = nullptr;
@@ -1088,12 +1169,18 @@ void drop_graph(dtfe_handle h) {
 // Launch variants chosen by dtfe_gpu_autotune.  Locate variants 0..2 place
 // the cell centres with the raster fused into the volume kernel (3, 2 or 4
 // blocks per SM); variants 3..8 walk from seeds (blocks per SM, samples per
-// thread).  Evaluation variants: register budget of the evaluation kernel.
+// thread); variants 9..11 walk and evaluate in one kernel (3, 2 or 4 blocks
+// per SM; for the averaging methods they walk as variant 3).  Evaluation
+// variants: register budget of the evaluation kernel.
 constexpr int kNumRasterVariants = 3;
 struct LocVariant { int block, minb, r; };
 constexpr LocVariant kWalkVariants[] = {{256, 3, 1}, {256, 2, 1}, {256, 4, 1}, {256, 3, 2}, {256, 4, 2}, {256, 3, 4}};
-constexpr int kNumLocVariants = kNumRasterVariants + sizeof(kWalkVariants) / sizeof(kWalkVariants[0]);
+constexpr int kNumWalkVariants = sizeof(kWalkVariants) / sizeof(kWalkVariants[0]);
+constexpr int kFusedMinBlocks[] = {3, 2, 4};
+constexpr int kFirstFused = kNumRasterVariants + kNumWalkVariants;
+constexpr int kNumLocVariants = kFirstFused + sizeof(kFusedMinBlocks) / sizeof(kFusedMinBlocks[0]);
 inline bool is_raster(int loc_variant) { return loc_variant < kNumRasterVariants; }
+inline bool is_fused(int loc_variant) { return loc_variant >= kFirstFused; }
 constexpr int kNumEvalVariants = 3;
 
 // Per step, before the interpolation: tetrahedron volumes and either the
@@ -1166,6 +1253,28 @@ void launch_eval(int method, int evariant, const InterpParams& P, const int* tet
     k_average<DTFE_METHOD_MONTE_CARLO, S><<<grid, block, 0, st>>>(P, tet_c);
   } else {
     k_average<DTFE_METHOD_EQUIDISTANT, S><<<grid, block, 0, st>>>(P, tet_c);
+  }
+}
+
+template <int S>
+void launch_fused(int fv, const InterpParams& P, int* tet_c, cudaStream_t st, unsigned grid, unsigned block) {
+  if (kFusedMinBlocks[fv] == 2) k_locate_eval<S, 2><<<grid, block, 0, st>>>(P, tet_c);
+  else if (kFusedMinBlocks[fv] == 4) k_locate_eval<S, 4><<<grid, block, 0, st>>>(P, tet_c);
+  else k_locate_eval<S, 3><<<grid, block, 0, st>>>(P, tet_c);
+}
+
+void launch_fused_s(int S, int fv, const InterpParams& P, int* tet_c, cudaStream_t st, unsigned grid,
+                    unsigned block) {
+  switch (S) {
+    case 0: launch_fused<0>(fv, P, tet_c, st, grid, block); break;
+    case 1: launch_fused<1>(fv, P, tet_c, st, grid, block); break;
+    case 2: launch_fused<2>(fv, P, tet_c, st, grid, block); break;
+    case 3: launch_fused<3>(fv, P, tet_c, st, grid, block); break;
+    case 4: launch_fused<4>(fv, P, tet_c, st, grid, block); break;
+    case 5: launch_fused<5>(fv, P, tet_c, st, grid, block); break;
+    case 6: launch_fused<6>(fv, P, tet_c, st, grid, block); break;
+    case 7: launch_fused<7>(fv, P, tet_c, st, grid, block); break;
+    default: launch_fused<8>(fv, P, tet_c, st, grid, block); break;
   }
 }
 
@@ -1630,8 +1739,13 @@ static int interp_enqueue(dtfe_handle h, const dtfe_interp_opts* o, float* const
     if (P.out[q] && ((uintptr_t)P.out[q] & 15))
       return set_error(DTFE_ERR_ARG, "output buffers must be 16-byte aligned");
   if ((rc = dev_alloc(h, &h->tet_c, h->n_cells))) return rc;
-  launch_locate(h->loc_variant, P, h->tet_c, st);
-  launch_eval_s(method, h->S, h->eval_variant, P, h->tet_c, st, grid, block);
+  const bool fused = is_fused(h->loc_variant) && method == DTFE_METHOD_CENTRE;
+  if (fused) {
+    launch_fused_s(h->S, h->loc_variant - kFirstFused, P, h->tet_c, st, grid, block);
+  } else {
+    launch_locate(is_fused(h->loc_variant) ? kNumRasterVariants : h->loc_variant, P, h->tet_c, st);
+    launch_eval_s(method, h->S, h->eval_variant, P, h->tet_c, st, grid, block);
+  }
   h->tet_c_valid = method == DTFE_METHOD_CENTRE;  // the adjoint differentiates centre values only
   h->tet_c_fix = (o->flags & DTFE_FLAG_FIX_VALUE_INTERP) != 0;
   DTFE_CUDA_TRY(cudaGetLastError());
@@ -1894,6 +2008,13 @@ int dtfe_gpu_interpolate_dev(dtfe_handle h, const dtfe_interp_opts* opts,
   if (!h) return set_error(DTFE_ERR_ARG, "null handle");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
   return interpolate_impl(h, opts, out_dev, st);
+}
+
+int dtfe_gpu_interpolate_dev_async(dtfe_handle h, const dtfe_interp_opts* opts,
+                                   float* const out_dev[DTFE_NUM_FIELDS]) {
+  if (!h) return set_error(DTFE_ERR_ARG, "null handle");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  return interp_enqueue(h, opts, out_dev);
 }
 
 int dtfe_gpu_graph_build(dtfe_handle h, double rho_bar, const dtfe_interp_opts* opts,

@@ -140,6 +140,17 @@ class DeviceDTFE:
         self.last_status = st.as_dict()
         return self.last_status
 
+    def interpolate_dev_async(self, fields, outs_dev: dict, method: int = 0, n_samples: int = 1, seed: int = 0,
+                              fix: bool = False) -> None:
+        """Queues the interpolation into device outputs without waiting
+        (dtfe_gpu_interpolate_dev_async); read_status() reports it."""
+        outs = [None] * N.NUM_FIELDS
+        for f in fields:
+            outs[N.FIELD_SLOTS[f]] = N.ptr(outs_dev[f]) if not isinstance(outs_dev[f], int) else outs_dev[f]
+        optr = (C.c_void_p * N.NUM_FIELDS)(*outs)
+        o = self._opts(fields, method, n_samples, seed, fix)
+        N.check(self.lib.dtfe_gpu_interpolate_dev_async(self.h, C.byref(o), optr))
+
     def graph_build(self, rho_bar: float, fields, outs_dev: dict, method: int = 0, n_samples: int = 1,
                     seed: int = 0, fix: bool = False) -> None:
         """Captures one step (vertex densities + interpolation into outs_dev)

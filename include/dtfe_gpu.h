@@ -193,6 +193,12 @@ int dtfe_gpu_interpolate_dev(dtfe_handle h, const dtfe_interp_opts* opts,
  * dtfe_gpu_read_status.  Lets a caller overlap one handle's transfers with
  * another's (double buffering across snapshots). */
 int dtfe_gpu_interpolate_async(dtfe_handle h, const dtfe_interp_opts* opts, float* const out[DTFE_NUM_FIELDS]);
+/* Same as dtfe_gpu_interpolate_dev, but only queues the work on the handle's
+ * stream and returns without waiting: consecutive steps (vertex densities,
+ * interpolation, ...) then run back to back on the device; the walk counters
+ * and a walk failure are reported by dtfe_gpu_read_status. */
+int dtfe_gpu_interpolate_dev_async(dtfe_handle h, const dtfe_interp_opts* opts,
+                                   float* const out_dev[DTFE_NUM_FIELDS]);
 
 /* ---- NGP / CIC / TSC comparison estimators ------------------------------
  * One record per region (the reference deposits per sub-box region, with

@@ -86,6 +86,7 @@ FIELD_SLOTS = {
 }
 METHOD_CENTRE, METHOD_TETRAHEDRA, METHOD_MONTE_CARLO, METHOD_EQUIDISTANT = 0, 1, 2, 3
 FLAG_FIX_VALUE_INTERP = 1
+FLAG_FIX_OUTSIDE_RASTER = 2
 
 
 def field_components(slot: int, n_scalars: int) -> int:

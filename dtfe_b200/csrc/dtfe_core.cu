@@ -586,6 +586,8 @@ struct InterpParams {
   int fix;
   int max_steps;
   int count_centres;  // the centres were placed by the raster: the evaluation counts them
+  const int64_t* pencil_prefix;  // K + 1: z pencils (tile x by y) before each sub-box
+  int S;                         // scalars per vertex
   float* out[DTFE_NUM_FIELDS];
   unsigned long long* counters;
 };
@@ -650,8 +652,12 @@ __device__ __forceinline__ void fold_counters(const InterpParams& P, unsigned n_
 
 // Seed tetrahedron of one sample: its cell's bin, else the nearest of the 26
 // neighbouring cells with one, else the sub-box's first tetrahedron.
+// -1 when the sub-box has no tetrahedra (fewer than four non-coplanar
+// particles): its samples are outside, as the reference's zeros for such a
+// triangulation (triangulation_miscellaneous.cc:121-138).
 __device__ __forceinline__ int seed_of(const InterpParams& P, const SampleCell& c) {
   const dtfe_subbox& B = P.boxes[c.b];
+  if (B.n_tets == 0) return -1;
   const unsigned long long* bins = P.bins + __ldg(&P.bin_offset[c.b]);
   unsigned long long s0 = __ldg(&bins[c.local]);
   if (s0 == kEmptySeed) {
@@ -693,7 +699,7 @@ __device__ __forceinline__ void locate_cells_body(const InterpParams& P, int* __
       const double pc[3] = {(double)c.x, (double)c.y, (double)c.z};
       int v[4];
       float X[4][3];
-      int tc = walk_locate<true>(P.tet_v, P.tet_n, P.posd, pc, t0, P.max_steps, v, X, st);
+      int tc = t0 < 0 ? kOutside : walk_locate<true>(P.tet_v, P.tet_n, P.posd, pc, t0, P.max_steps, v, X, st);
       ++n_loc;
       if (tc == kWalkFail) { ++n_fail; tc = kOutside; }
       if (tc < 0) ++n_out;
@@ -831,7 +837,8 @@ __global__ void __launch_bounds__(kInterpBlock, MINB) k_locate_eval(InterpParams
       const double pc[3] = {(double)c.x, (double)c.y, (double)c.z};
       int v[4];
       float X[4][3];
-      int t = walk_locate<true>(P.tet_v, P.tet_n, P.posd, pc, seed_of(P, c), P.max_steps, v, X, wst);
+      const int t0 = seed_of(P, c);
+      int t = t0 < 0 ? kOutside : walk_locate<true>(P.tet_v, P.tet_n, P.posd, pc, t0, P.max_steps, v, X, wst);
       ++n_loc;
       if (t == kWalkFail) {
         ++n_fail;
@@ -864,6 +871,47 @@ __global__ void __launch_bounds__(kInterpBlock, MINB) k_locate_eval(InterpParams
       store_field<(S > 0 ? 3 * S : 1)>(P.out[DTFE_SCALAR_GRADIENT], cell, valid, e.scg, contig, c0, stage);
   }
   fold_counters(P, n_loc, n_out, n_fail, wst);
+}
+
+// The reference's cell-centre raster after an outside sample: it skips
+// `z += dx` (unaveraged_interpolation.cc:304 jumps over :353), so the rest of
+// the z pencil re-locates that outside point and gets zeros.  One warp per
+// pencil reads its located tetrahedra 32 at a time; every cell after the
+// pencil's first outside one is marked outside and its fields zeroed.
+__global__ void __launch_bounds__(256) k_outside_pencils(InterpParams P, int* __restrict__ tet_c, int64_t n_pencils) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t q = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; q < n_pencils; q += nw) {
+    const int b = find_box(P.pencil_prefix, P.K, q);
+    const dtfe_subbox& B = P.boxes[b];
+    const int ny = B.tile_dims[1], nz = B.tile_dims[2];
+    const uint32_t local = (uint32_t)(q - __ldg(&P.pencil_prefix[b]));
+    const int i = (int)(local / (uint32_t)ny), j = (int)(local - (uint32_t)i * (uint32_t)ny);
+    const int64_t s0 = __ldg(&P.tile_prefix[b]) + (int64_t)local * nz;
+    const int64_t c0 = ((int64_t)(B.tile_origin[0] + i) * P.G1 + (B.tile_origin[1] + j)) * P.G2 + B.tile_origin[2];
+    bool seen = false;
+    for (int k0 = 0; k0 < nz; k0 += 32) {
+      const int k = k0 + lane;
+      const bool valid = k < nz;
+      const int t = valid ? tet_c[s0 + k] : 0;
+      const unsigned outside = __ballot_sync(0xffffffffu, valid && t < 0);
+      const bool poison = seen || (outside & ((1u << lane) - 1u)) != 0;
+      if (valid && poison && t >= 0) {
+        tet_c[s0 + k] = kOutside;
+        const int64_t cell = c0 + k;
+        for (int slot = 0; slot < DTFE_NUM_FIELDS; ++slot) {
+          if (!has_field(P.fields, slot) || !P.out[slot]) continue;
+          const int nc = slot == DTFE_VELOCITY || slot == DTFE_VELOCITY_VORTICITY ? 3
+                       : slot == DTFE_VELOCITY_GRADIENT ? 9
+                       : slot == DTFE_VELOCITY_SHEAR ? 5
+                       : slot == DTFE_SCALAR ? P.S
+                       : slot == DTFE_SCALAR_GRADIENT ? 3 * P.S : 1;
+          for (int c = 0; c < nc; ++c) P.out[slot][cell * nc + c] = 0.f;
+        }
+      }
+      seen = seen || outside != 0u;
+    }
+  }
 }
 
 // Cell averages (methods 2 and 3): n points per cell, each walked from the
@@ -932,7 +980,8 @@ __global__ void __launch_bounds__(kInterpBlock) k_average(InterpParams P, const 
         }
         int vv[4];
         float XX[4][3];
-        int t = walk_locate(P.tet_v, P.tet_n, P.posd, p, tstart, P.max_steps, vv, XX, st);
+        // a sub-box without tetrahedra: every point outside
+        int t = B.n_tets > 0 ? walk_locate(P.tet_v, P.tet_n, P.posd, p, tstart, P.max_steps, vv, XX, st) : kOutside;
         ++n_loc;
         if (t == kWalkFail) { ++n_fail; t = kOutside; }
         if (t < 0) continue;
@@ -983,7 +1032,8 @@ __global__ void __launch_bounds__(kInterpBlock) k_average(InterpParams P, const 
           int vv[4];
           float XX[4][3];
           WalkStats st2{0, 0, 0};
-          int t = walk_locate(P.tet_v, P.tet_n, P.posd, p, tstart, P.max_steps, vv, XX, st2);
+          int t = B.n_tets > 0 ? walk_locate(P.tet_v, P.tet_n, P.posd, p, tstart, P.max_steps, vv, XX, st2)
+                               : kOutside;
           if (t >= 0) {
             CellOut e;
             cell_eval<0>(vv, XX, p, P.posd, P.vel4, P.scal, false, true, false, fix, e);
@@ -1068,6 +1118,8 @@ struct dtfe_gpu_s {
   std::vector<dtfe_subbox> boxes_h;
   dtfe_subbox* boxes = nullptr;
   int64_t* tile_prefix = nullptr;
+  int64_t* pencil_prefix = nullptr;  // K + 1: z pencils before each sub-box
+  int64_t n_pencils = 0;
   int64_t* tet_prefix = nullptr;  // K+1 tetrahedron range starts
   int64_t* bin_offset = nullptr;
   unsigned long long* bins = nullptr;
@@ -1345,7 +1397,7 @@ int dtfe_gpu_destroy(dtfe_handle h) {
   if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
   void* ptrs[] = {h->tet_v, h->tet_n, h->posd, h->vel4, h->scal, h->w, h->vol, h->inc_off, h->inc,
                   h->scratch_i, h->scan_blocks, h->hull,
-                  h->boxes, h->tile_prefix, h->tet_prefix, h->bin_offset, h->bins,
+                  h->boxes, h->tile_prefix, h->pencil_prefix, h->tet_prefix, h->bin_offset, h->bins,
                   h->xs, h->ys, h->zs, h->eq_off, h->counters, h->tet_c, h->raster_axes};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -1516,7 +1568,7 @@ int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* box
   if (!h || n_boxes <= 0 || !boxes || !xs || !ys || !zs || !grid)
     return set_error(DTFE_ERR_ARG, "null or empty sub-box description");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
-  std::vector<int64_t> tprefix(n_boxes + 1), tetpre(n_boxes + 1), boff(n_boxes);
+  std::vector<int64_t> tprefix(n_boxes + 1), tetpre(n_boxes + 1), boff(n_boxes), ppre(n_boxes + 1);
   int64_t cells = 0;
   for (int b = 0; b < n_boxes; ++b) {
     const dtfe_subbox& B = boxes[b];
@@ -1534,6 +1586,7 @@ int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* box
       return set_error(DTFE_ERR_ARG, "sub-box vertex and tetrahedron ranges must be consecutive");
     tprefix[b] = cells;
     boff[b] = cells;
+    ppre[b + 1] = ppre[b] + (int64_t)B.tile_dims[0] * B.tile_dims[1];
     tetpre[b] = B.tet_offset;
     cells += (int64_t)B.tile_dims[0] * B.tile_dims[1] * B.tile_dims[2];
   }
@@ -1560,6 +1613,7 @@ int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* box
   int rc;
   if ((rc = dev_alloc(h, &h->raster_axes, (size_t)3 * n_boxes)) ||
       (rc = dev_alloc(h, &h->boxes, n_boxes)) || (rc = dev_alloc(h, &h->tile_prefix, n_boxes + 1)) ||
+      (rc = dev_alloc(h, &h->pencil_prefix, n_boxes + 1)) ||
       (rc = dev_alloc(h, &h->tet_prefix, n_boxes + 1)) || (rc = dev_alloc(h, &h->bin_offset, n_boxes)) ||
       (rc = dev_alloc(h, &h->bins, cells)) || (rc = dev_alloc(h, &h->xs, n_xs)) ||
       (rc = dev_alloc(h, &h->ys, n_ys)) || (rc = dev_alloc(h, &h->zs, n_zs)))
@@ -1567,6 +1621,8 @@ int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* box
   cudaStream_t st = h->stream;
   DTFE_CUDA_TRY(cudaMemcpyAsync(h->boxes, boxes, sizeof(dtfe_subbox) * n_boxes, cudaMemcpyHostToDevice, st));
   DTFE_CUDA_TRY(cudaMemcpyAsync(h->tile_prefix, tprefix.data(), sizeof(int64_t) * (n_boxes + 1),
+                                cudaMemcpyHostToDevice, st));
+  DTFE_CUDA_TRY(cudaMemcpyAsync(h->pencil_prefix, ppre.data(), sizeof(int64_t) * (n_boxes + 1),
                                 cudaMemcpyHostToDevice, st));
   DTFE_CUDA_TRY(cudaMemcpyAsync(h->tet_prefix, tetpre.data(), sizeof(int64_t) * (n_boxes + 1),
                                 cudaMemcpyHostToDevice, st));
@@ -1586,6 +1642,7 @@ int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* box
       h->regions_h[6 * b + 2 * a + 1] = boxes[b].lo[a] + boxes[b].dx[a] * (float)boxes[b].tile_dims[a];
     }
   h->n_cells = cells;
+  h->n_pencils = ppre[n_boxes];
   h->grid[0] = grid[0]; h->grid[1] = grid[1]; h->grid[2] = grid[2];
   h->prep_ready = false;
   h->eq_nn = 0;
@@ -1721,6 +1778,8 @@ static int interp_enqueue(dtfe_handle h, const dtfe_interp_opts* o, float* const
   P.ys = h->ys;
   P.zs = h->zs;
   P.K = h->K;
+  P.pencil_prefix = h->pencil_prefix;
+  P.S = h->S;
   P.G1 = h->grid[1];
   P.G2 = h->grid[2];
   P.n_total = h->n_cells;
@@ -1745,6 +1804,11 @@ static int interp_enqueue(dtfe_handle h, const dtfe_interp_opts* o, float* const
   } else {
     launch_locate(is_fused(h->loc_variant) ? kNumRasterVariants : h->loc_variant, P, h->tet_c, st);
     launch_eval_s(method, h->S, h->eval_variant, P, h->tet_c, st, grid, block);
+  }
+  // the reference's raster after an outside sample (DTFE_FLAG_FIX_OUTSIDE_RASTER: off)
+  if (method == DTFE_METHOD_CENTRE && !(o->flags & DTFE_FLAG_FIX_OUTSIDE_RASTER) && h->n_pencils > 0) {
+    const int64_t want = (h->n_pencils * 32 + 255) / 256;
+    k_outside_pencils<<<(unsigned)std::min<int64_t>(want, 148 * 16), 256, 0, st>>>(P, h->tet_c, h->n_pencils);
   }
   h->tet_c_valid = method == DTFE_METHOD_CENTRE;  // the adjoint differentiates centre values only
   h->tet_c_fix = (o->flags & DTFE_FLAG_FIX_VALUE_INTERP) != 0;

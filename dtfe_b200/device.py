@@ -93,11 +93,12 @@ class DeviceDTFE:
         N.check(self.lib.dtfe_gpu_download_vertex_density(self.h, out.ctypes.data))
         return out
 
-    def _opts(self, fields, method, n_samples, seed, fix):
-        return N.InterpOpts(method, n_samples, seed, _mask(fields), N.FLAG_FIX_VALUE_INTERP if fix else 0)
+    def _opts(self, fields, method, n_samples, seed, fix, fix_outside=False):
+        flags = (N.FLAG_FIX_VALUE_INTERP if fix else 0) | (N.FLAG_FIX_OUTSIDE_RASTER if fix_outside else 0)
+        return N.InterpOpts(method, n_samples, seed, _mask(fields), flags)
 
     def interpolate(self, fields, method: int = 0, n_samples: int = 1, seed: int = 0, fix: bool = False,
-                    out: dict | None = None) -> dict:
+                    out: dict | None = None, fix_outside: bool = False) -> dict:
         """Host outputs: dict field -> float32 array (G, ncomp) or (G,)."""
         G = int(np.prod(self.grid))
         outs = [None] * N.NUM_FIELDS
@@ -110,7 +111,7 @@ class DeviceDTFE:
             outs[s] = N.ptr(a)
         optr = (C.c_void_p * N.NUM_FIELDS)(*outs)
         st = N.Status()
-        o = self._opts(fields, method, n_samples, seed, fix)
+        o = self._opts(fields, method, n_samples, seed, fix, fix_outside)
         N.check(self.lib.dtfe_gpu_interpolate(self.h, C.byref(o), optr, C.byref(st)))
         self.last_status = st.as_dict()
         return res

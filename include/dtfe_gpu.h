@@ -81,6 +81,12 @@ enum {
  * gradient product (unaveraged_interpolation.cc:116,159).  Default: keep that
  * behaviour for parity; this flag evaluates the full dot product instead. */
 #define DTFE_FLAG_FIX_VALUE_INTERP 1u
+/* Reference interpolateGrid() skips its `z += dx` after a sample outside the
+ * hull (the `continue` at unaveraged_interpolation.cc:304 jumps over :353),
+ * so every later sample of that z pencil re-locates the same outside point
+ * and gets zeros.  Default (cell centres only): the same zeros, for parity;
+ * this flag evaluates those samples at their own centres instead. */
+#define DTFE_FLAG_FIX_OUTSIDE_RASTER 2u
 
 /* ---- limits -------------------------------------------------------------- */
 #define DTFE_MAX_SCALARS 8

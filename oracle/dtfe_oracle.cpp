@@ -85,6 +85,9 @@ bool contains(const Tess& g, int64_t t, const double* p, int zero[4]) {
 // contains p.  Returns -1 when p is outside the hull (an infinite cell in the
 // reference), -2 when the walk fails.
 int64_t locate(const Tess& g, const double* p, int64_t start, int64_t lo, int64_t hi) {
+  // no tetrahedra in the sub-box (fewer than four non-coplanar points): the
+  // reference interpolates zeros (triangulation_miscellaneous.cc:121-138)
+  if (hi <= lo) return -1;
   int64_t t = start;
   if (t < lo || t >= hi) t = lo;
   int64_t limit = 4 * (hi - lo) + 64;
@@ -387,6 +390,9 @@ int oracle_interpolate(int64_t T, const int32_t* tv, const int32_t* tn, int64_t 
   Tess g{T, V, tv, tn, xyz, vel, scal, S};
   const uint32_t f = o->fields;
   const bool fix = (o->flags & DTFE_FLAG_FIX_VALUE_INTERP) != 0;
+  // the reference's cell-centre raster stays on an outside point for the
+  // rest of its z pencil (unaveraged_interpolation.cc:304 skips :353)
+  const bool stale_after_outside = o->method == DTFE_METHOD_CENTRE && !(o->flags & DTFE_FLAG_FIX_OUTSIDE_RASTER);
   auto has = [&](int s) { return (f & DTFE_FIELD_BIT(s)) != 0 && out[s] != nullptr; };
   const bool want_grad = has(DTFE_VELOCITY_GRADIENT) || has(DTFE_VELOCITY_DIVERGENCE) ||
                          has(DTFE_VELOCITY_SHEAR) || has(DTFE_VELOCITY_VORTICITY);
@@ -431,14 +437,16 @@ int oracle_interpolate(int64_t T, const int32_t* tv, const int32_t* tn, int64_t 
     for (int i = 0; i < B.tile_dims[0]; ++i) {
       for (int j = 0; j < B.tile_dims[1]; ++j) {
         int64_t hint = row_hint;
+        bool stale = false;  // an earlier sample of this pencil was outside
         for (int k = 0; k < B.tile_dims[2]; ++k) {
           const float x = xs[B.coord_offset[0] + i], y = ys[B.coord_offset[1] + j],
                       z = zs[B.coord_offset[2] + k];
           const int64_t cell = ((int64_t)(B.tile_origin[0] + i) * G1 + (B.tile_origin[1] + j)) * G2 +
                                (B.tile_origin[2] + k);
           double pc[3] = {(double)x, (double)y, (double)z};
-          int64_t tc = locate(g, pc, hint, lo, hi);
+          int64_t tc = stale ? -1 : locate(g, pc, hint, lo, hi);
           if (tc == -2) { ++fails; tc = -1; }
+          if (tc < 0 && stale_after_outside) stale = true;
           if (tc >= 0) {
             hint = tc;
             if (k == 0) row_hint = tc;

@@ -166,7 +166,8 @@ def locate(plan, pts: np.ndarray, box: int = 0) -> np.ndarray:
 
 
 def interpolate(plan, dens32, dens64, fields, method: int = 0, n_samples: int = 1, seed: int = 0,
-                mode: int = MODE_REF, fix: bool = False, nthreads: int = 1, want_loc: bool = False):
+                mode: int = MODE_REF, fix: bool = False, nthreads: int = 1, want_loc: bool = False,
+                fix_outside: bool = False):
     """Returns (dict field -> float64 array shaped (G, ncomp) or (G,), loc or None)."""
     G = int(np.prod(plan.grid))
     S = plan.n_scalars
@@ -181,7 +182,8 @@ def interpolate(plan, dens32, dens64, fields, method: int = 0, n_samples: int = 
         arrs[f] = a
         outs[s] = a.ctypes.data
     optr = (C.c_void_p * N.NUM_FIELDS)(*[o if o else None for o in outs])
-    o = N.InterpOpts(method, n_samples, seed, mask, N.FLAG_FIX_VALUE_INTERP if fix else 0)
+    o = N.InterpOpts(method, n_samples, seed, mask, (N.FLAG_FIX_VALUE_INTERP if fix else 0) |
+                     (N.FLAG_FIX_OUTSIDE_RASTER if fix_outside else 0))
     loc = np.full(G, -1, np.int64) if want_loc else None
     nfail = C.c_int64(0)
     vel = plan.velocity.ctypes.data if plan.velocity is not None else None

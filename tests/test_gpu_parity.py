@@ -173,3 +173,40 @@ def test_centre_ties_lattice(gpu_built):
         for f in fields:
             assert np.array_equal(got[f], outs[0][f]), f
             assert rel_err(got[f], ref[f]) <= 1e-6, f
+
+
+def test_sparse_subboxes(gpu_built):
+    """Sub-boxes without tetrahedra, one-tetrahedron sub-boxes and cell centres
+    outside the hulls (the reference's stale raster after an outside sample,
+    and DTFE_FLAG_FIX_OUTSIDE_RASTER): every locate variant, methods 0, 3, 1,
+    bit-identical to the oracle's float mode (itself pinned to the reference
+    in tests/test_reference_live.py)."""
+    from dtfe_b200 import _native as N
+    from dtfe_b200.device import DeviceDTFE
+    rng = np.random.default_rng(1)
+    pos = (rng.random((40, 3)) * 100).astype(np.float32)
+    vel = rng.standard_normal((40, 3)).astype(np.float32)
+    plan = P.make_plan(pos, rng.uniform(0.5, 1.5, 40).astype(np.float32), vel, None, grid=(16, 16, 16),
+                       n_threads=16, periodic=False, padding=np.ones(6, np.float32), average_density_value=1e-3)
+    fields = ["density", "velocity", "velocity_gradient", "velocity_divergence"]
+    d32, d64, _ = O.vertex_density(plan)
+    with DeviceDTFE(0) as d:
+        d.load(plan)
+        d.vertex_density(plan.rho_bar)
+        n_loc, _ = d.variant_counts()
+        for fix_outside in (False, True):
+            want, _ = O.interpolate(plan, d32, d64, fields, method=0, mode=O.MODE_REF, fix_outside=fix_outside)
+            for loc in range(n_loc):
+                d.set_variants(loc, 0)
+                got = d.interpolate(fields, method=0, fix_outside=fix_outside)
+                for f in fields:
+                    assert np.array_equal(got[f].reshape(want[f].shape), want[f].astype(np.float32)), \
+                        (fix_outside, loc, f)
+        want, _ = O.interpolate(plan, d32, d64, fields, method=3, n_samples=8, mode=O.MODE_REF)
+        got = d.interpolate(fields, method=3, n_samples=8)
+        for f in fields:
+            assert rel_err(got[f].reshape(want[f].shape), want[f]) <= 1e-6, f
+        want = O.method1(plan, d32, d64, fields, n_points=100, mode=O.MODE_REF)
+        got = d.interpolate(fields, method=N.METHOD_TETRAHEDRA, n_samples=100)
+        for f in fields:
+            assert np.array_equal(got[f].reshape(want[f].shape), want[f].astype(np.float32)), f

@@ -576,6 +576,65 @@ int oracle_interpolate(int64_t T, const int32_t* tv, const int32_t* tn, int64_t 
   return fails ? DTFE_ERR_WALK : DTFE_OK;
 }
 
+// Fields at user sampling points: interpolateUserSampling
+// (src/CGAL_triangulation/unaveraged_interpolation.cc:560-691).  Points
+// outside `region` (closed, isPointInBox) are dropped; the rest, in order,
+// are located (walk hinted by the previous hit, canonical tie rule) in the
+// tetrahedra [lo, hi) and evaluated as cell centres are; outside the hull
+// zeros.  Divergence, shear and vorticity from the gradient
+// (src/DTFE.cpp:394-475).  Returns the number of points kept in *n_out.
+int oracle_interpolate_points(int64_t T, const int32_t* tv, const int32_t* tn, int64_t V, const float* xyz,
+                              const float* vel, const float* scal, int S, const float* dens32, const double* dens64,
+                              int64_t lo, int64_t hi, int64_t n, const float* pts, const float region[6],
+                              uint32_t fields, int mode, int fix, double* const out[DTFE_NUM_FIELDS],
+                              int64_t* n_out) {
+  (void)T;
+  (void)V;
+  Tess g{T, V, tv, tn, xyz, vel, scal, S};
+  auto has = [&](int s) { return (fields & DTFE_FIELD_BIT(s)) != 0 && out[s] != nullptr; };
+  if (has(DTFE_VELOCITY_STD)) return DTFE_ERR_ARG;
+  const bool want_vel = has(DTFE_VELOCITY) || has(DTFE_VELOCITY_GRADIENT) || has(DTFE_VELOCITY_DIVERGENCE) ||
+                        has(DTFE_VELOCITY_SHEAR) || has(DTFE_VELOCITY_VORTICITY);
+  const bool want_sc = has(DTFE_SCALAR) || has(DTFE_SCALAR_GRADIENT);
+  int64_t m = 0, hint = lo;
+  for (int64_t i = 0; i < n; ++i) {
+    const float* q = pts + 3 * i;
+    bool in = true;
+    for (int c = 0; c < 3; ++c) in = in && q[c] >= region[2 * c] && q[c] <= region[2 * c + 1];
+    if (!in) continue;
+    const double p[3] = {(double)q[0], (double)q[1], (double)q[2]};
+    int64_t t = locate(g, p, hint, lo, hi);
+    if (t == -2) return DTFE_ERR_WALK;
+    CellEval e;
+    std::memset(&e, 0, sizeof(e));
+    if (t >= 0) {
+      hint = t;
+      eval_cell(g, dens32, dens64, t, p, mode, fix != 0, want_vel, want_sc, e);
+    }
+    if (has(DTFE_DENSITY)) out[DTFE_DENSITY][m] = e.dens;
+    if (has(DTFE_VELOCITY))
+      for (int c = 0; c < 3; ++c) out[DTFE_VELOCITY][3 * m + c] = e.vel[c];
+    if (has(DTFE_VELOCITY_GRADIENT))
+      for (int c = 0; c < 9; ++c) out[DTFE_VELOCITY_GRADIENT][9 * m + c] = e.grad[c];
+    if (has(DTFE_VELOCITY_DIVERGENCE) || has(DTFE_VELOCITY_SHEAR) || has(DTFE_VELOCITY_VORTICITY)) {
+      double dv, sh[5], vo[3];
+      derived(e.grad, mode, &dv, sh, vo);
+      if (has(DTFE_VELOCITY_DIVERGENCE)) out[DTFE_VELOCITY_DIVERGENCE][m] = dv;
+      if (has(DTFE_VELOCITY_SHEAR))
+        for (int c = 0; c < 5; ++c) out[DTFE_VELOCITY_SHEAR][5 * m + c] = sh[c];
+      if (has(DTFE_VELOCITY_VORTICITY))
+        for (int c = 0; c < 3; ++c) out[DTFE_VELOCITY_VORTICITY][3 * m + c] = vo[c];
+    }
+    if (has(DTFE_SCALAR))
+      for (int c = 0; c < S; ++c) out[DTFE_SCALAR][(int64_t)S * m + c] = e.sc[c];
+    if (has(DTFE_SCALAR_GRADIENT))
+      for (int c = 0; c < 3 * S; ++c) out[DTFE_SCALAR_GRADIENT][(int64_t)3 * S * m + c] = e.scg[c];
+    ++m;
+  }
+  *n_out = m;
+  return DTFE_OK;
+}
+
 // Averaging method 1: interpolateGrid_averaged_1
 // (src/CGAL_triangulation/averaged_interpolation_1.cc:197-421), per sub-box
 // over its tetrahedra in order.

@@ -50,6 +50,9 @@ def lib() -> C.CDLL:
         L.oracle_deposit_loss_grad.restype = C.c_double
         L.oracle_method1.argtypes = [C.c_int64, vp, C.c_int64, vp, vp, vp, C.c_int, vp, vp, C.c_int, vp, vp, vp,
                                      C.c_int, C.c_uint32, C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+        L.oracle_interpolate_points.argtypes = [C.c_int64, vp, vp, C.c_int64, vp, vp, vp, C.c_int, vp, vp,
+                                                C.c_int64, C.c_int64, C.c_int64, vp, vp, C.c_uint32, C.c_int,
+                                                C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]
         L.oracle_sobol_simplex.argtypes = [C.c_int64, vp]
         L.oracle_sobol_simplex.restype = None
         _lib = L
@@ -229,6 +232,39 @@ def method1(plan, dens32, dens64, fields, n_points: int = 100, mode: int = MODE_
     if rc:
         raise RuntimeError(f"oracle_method1 failed with status {rc}")
     return arrs
+
+
+def interpolate_points(plan, dens32, dens64, fields, pts, region, mode: int = MODE_REF, fix: bool = False,
+                       box: int = 0):
+    """Fields at user sampling points (interpolateUserSampling) in the
+    tessellation of sub-box `box`: dict field -> float64 array of the points
+    inside `region`, in order."""
+    pts = np.ascontiguousarray(pts, np.float32)
+    n = len(pts)
+    S = plan.n_scalars
+    mask = 0
+    outs = [None] * N.NUM_FIELDS
+    arrs = {}
+    for f in fields:
+        s = N.FIELD_SLOTS[f]
+        mask |= 1 << s
+        nc = N.field_components(s, S)
+        a = np.zeros((n, nc) if nc > 1 else n, np.float64)
+        arrs[f] = a
+        outs[s] = a.ctypes.data
+    optr = (C.c_void_p * N.NUM_FIELDS)(*[o if o else None for o in outs])
+    vel = plan.velocity.ctypes.data if plan.velocity is not None else None
+    sc = plan.scalar.ctypes.data if plan.scalar is not None else None
+    b = plan.boxes[box]
+    reg = np.ascontiguousarray(region, np.float32)
+    n_out = C.c_int64(0)
+    rc = lib().oracle_interpolate_points(plan.n_tets, plan.tet_v.ctypes.data, plan.tet_n.ctypes.data, plan.n_verts,
+                                         plan.xyz.ctypes.data, vel, sc, S, dens32.ctypes.data, dens64.ctypes.data,
+                                         b.tet_offset, b.tet_offset + b.n_tets, n, pts.ctypes.data,
+                                         reg.ctypes.data, mask, mode, 1 if fix else 0, optr, C.byref(n_out))
+    if rc:
+        raise RuntimeError(f"oracle_interpolate_points failed with status {rc}")
+    return {f: a[:n_out.value] for f, a in arrs.items()}
 
 
 def sobol_simplex(n: int) -> np.ndarray:

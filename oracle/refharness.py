@@ -70,6 +70,36 @@ def run(plan, box: int = 0, which: int = 0, n_points: int = 1, seed: int = 0, de
     return out
 
 
+def run_points(plan, pts, region, dens, box: int = 0):
+    """The reference's interpolateUserSampling on sub-box `box`'s
+    tessellation with vertex densities `dens`: density, velocity, gradient,
+    scalar, scalar gradient of the points inside `region`, in order."""
+    xyz, w, vel, tv, tn, dims, _ = _box_args(plan, box)
+    b = plan.boxes[box]
+    v0, nv = b.vert_offset, b.n_verts
+    sc = None if plan.scalar is None else np.ascontiguousarray(plan.scalar[v0:v0 + nv, 0])
+    d = np.ascontiguousarray(dens[v0:v0 + nv], np.float32)
+    pts = np.ascontiguousarray(pts, np.float32)
+    n = len(pts)
+    out = {"density": np.zeros(n, np.float32), "velocity": np.zeros((n, 3), np.float32),
+           "velocity_gradient": np.zeros((n, 9), np.float32), "scalar": np.zeros(n, np.float32),
+           "scalar_gradient": np.zeros((n, 3), np.float32)}
+    reg = np.ascontiguousarray(region, np.float32)
+    L = lib()
+    vp = C.c_void_p
+    L.ref_interpolate_points.argtypes = [C.c_int64, vp, vp, vp, vp, C.c_int64, vp, vp, vp, C.c_int64, vp, vp,
+                                         vp, vp, vp, vp, vp, C.POINTER(C.c_int64)]
+    p = lambda a: None if a is None else a.ctypes.data
+    m = C.c_int64(0)
+    rc = L.ref_interpolate_points(len(xyz), p(xyz), p(w), p(vel), p(sc), len(tv), p(tv), p(tn), p(reg), n,
+                                  p(pts), p(d), p(out["density"]), p(out["velocity"]), p(out["velocity_gradient"]),
+                                  p(out["scalar"]) if sc is not None else None,
+                                  p(out["scalar_gradient"]) if sc is not None else None, C.byref(m))
+    if rc:
+        raise RuntimeError(f"ref_interpolate_points failed ({rc})")
+    return {k: a[:m.value] for k, a in out.items()}
+
+
 def _box_args(plan, box):
     b = plan.boxes[box]
     v0, nv, t0, nt = b.vert_offset, b.n_verts, b.tet_offset, b.n_tets

@@ -10,6 +10,7 @@
 //   interpolateGrid             unaveraged_interpolation.cc:209-369
 //   interpolateGrid_averaged_2  averaged_interpolation_2.cc:35-233
 //   interpolateGrid_averaged_3  averaged_interpolation_2.cc:664-866
+//   interpolateUserSampling     unaveraged_interpolation.cc:560-691
 //   interpolateGrid_averaged_1  averaged_interpolation_1.cc:197-421 (Sobol points
 //                               from dtfe_b200/csrc/sobol.h behind the GSL API)
 //
@@ -39,6 +40,8 @@ void interpolateGrid(DT& dt, User_options& userOptions, Quantities* quantities);
 void interpolateGrid_averaged_2(DT& dt, User_options& userOptions, Quantities* quantities);
 void interpolateGrid_averaged_3(DT& dt, User_options& userOptions, Quantities* quantities);
 void interpolateGrid_averaged_1(DT& dt, User_options& userOptions, Quantities* quantities);
+void interpolateUserSampling(DT& dt, std::vector<Sample_point>& samples, User_options& userOptions,
+                             Quantities* quantities);
 
 User_options::User_options() {
   periodic = false;
@@ -176,6 +179,51 @@ int ref_interpolate_timed(int64_t nv, const float* xyz, const float* w, const fl
   copy(out_scalar, (const float*)q.scalar.data(), G, q.scalar.size());
   copy(out_scalar_gradient, (const float*)q.scalar_gradient.data(), 3 * G, q.scalar_gradient.size());
   copy(out_std, q.velocity_std.data(), G, q.velocity_std.size());
+  return 0;
+}
+
+// The reference's interpolateUserSampling (unaveraged_interpolation.cc:560-691)
+// at n points (3 floats each) in `region`, with the given vertex densities:
+// the fields of the points inside the region, in order (*n_out of them).
+int ref_interpolate_points(int64_t nv, const float* xyz, const float* w, const float* vel, const float* scal,
+                           int64_t nt, const int32_t* tv, const int32_t* tn, const float region[6], int64_t n,
+                           const float* pts, const float* dens, float* out_density, float* out_velocity,
+                           float* out_gradient, float* out_scalar, float* out_scalar_gradient, int64_t* n_out) {
+  DT dt;
+  const std::vector<DT::Vertex*>& verts = dt.load_flat(nv, xyz, nt, tv, tn);
+  for (int64_t i = 0; i < nv; ++i) {
+    vertexData& d = verts[i]->info();
+    d.weight() = w[i];
+    for (int c = 0; c < 3; ++c) d.velocity(c) = vel ? vel[3 * i + c] : 0.f;
+    d.scalar(0) = scal ? scal[i] : 0.f;
+    d.setDensity(dens[i]);
+  }
+  User_options opt;
+  opt.region.coords.assign(region, region + 6);
+  opt.userDefinedSampling = true;
+  std::vector<Sample_point> samples((size_t)n);
+  for (int64_t i = 0; i < n; ++i) {
+    float p[3] = {pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
+    samples[i].setPosition(p);
+  }
+  Quantities q;
+  Field f;
+  f.density = out_density != nullptr;
+  f.velocity = out_velocity != nullptr;
+  f.velocity_gradient = out_gradient != nullptr;
+  f.scalar = out_scalar != nullptr;
+  f.scalar_gradient = out_scalar_gradient != nullptr;
+  opt.uField = f;
+  interpolateUserSampling(dt, samples, opt, &q);
+  const size_t m = f.density ? q.density.size() : (f.velocity ? q.velocity.size() : q.velocity_gradient.size());
+  *n_out = (int64_t)m;
+  if (out_density && q.density.size() == m) std::memcpy(out_density, q.density.data(), m * sizeof(float));
+  if (out_velocity && q.velocity.size() == m) std::memcpy(out_velocity, q.velocity.data(), 3 * m * sizeof(float));
+  if (out_gradient && q.velocity_gradient.size() == m)
+    std::memcpy(out_gradient, q.velocity_gradient.data(), 9 * m * sizeof(float));
+  if (out_scalar && q.scalar.size() == m) std::memcpy(out_scalar, q.scalar.data(), m * sizeof(float));
+  if (out_scalar_gradient && q.scalar_gradient.size() == m)
+    std::memcpy(out_scalar_gradient, q.scalar_gradient.data(), 3 * m * sizeof(float));
   return 0;
 }
 

@@ -147,3 +147,29 @@ def test_live_sparse_subboxes(built):
     compat, _ = O.interpolate(plan, d32, d64, fields, method=0, mode=O.MODE_REF)
     moved = np.abs(fixed["velocity"] - compat["velocity"]).sum(1) > 0
     assert moved.any() and not (np.abs(compat["velocity"][moved]).sum(1) > 0).any()
+
+
+def test_live_user_sampling(built):
+    """Fields at user sampling points: the reference's interpolateUserSampling
+    (one box, as DTFE() runs user samples) against the oracle's float mode,
+    bit for bit: points outside the region dropped, points outside the hull
+    zeros, the rest evaluated as cell centres are."""
+    pos, psi = S.zeldovich_lattice(12, 100.0, 0.9, seed=51)
+    rng = np.random.default_rng(52)
+    w = rng.uniform(0.5, 1.5, len(pos)).astype(np.float32)
+    vel = (60 * psi).astype(np.float32)
+    sc = rng.standard_normal((len(pos), 1)).astype(np.float32)
+    plan = P.make_plan(pos, w, vel, sc, grid=(12, 12, 12), n_threads=1, average_density_value=float(w.sum()) / 1e6)
+    d32, d64, _ = O.vertex_density(plan)
+    # the padded hull reaches about 40 beyond the box: points up to 80 beyond
+    pts = np.concatenate([rng.uniform(-80, 180, (3000, 3)), rng.uniform(0, 100, (2000, 3))]).astype(np.float32)
+    pts[:20] = plan.xyz[:20]                       # on vertices (ties)
+    region = np.array([-70, 170, -60, 160, -70, 150], np.float32)
+    fields = ["density", "velocity", "velocity_gradient", "scalar", "scalar_gradient"]
+    ora = O.interpolate_points(plan, d32, d64, fields, pts, region, mode=O.MODE_REF)
+    ref = R.run_points(plan, pts, region, d32)
+    keep = np.all((pts >= region[0::2]) & (pts <= region[1::2]), axis=1)
+    assert len(ref["density"]) == keep.sum() == len(ora["density"])
+    for f in fields:
+        assert np.array_equal(ora[f].astype(np.float32), ref[f]), f
+    assert (ora["density"] == 0).any() and (ora["density"] != 0).any()

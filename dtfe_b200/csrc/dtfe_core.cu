@@ -914,6 +914,117 @@ __global__ void __launch_bounds__(256) k_outside_pencils(InterpParams P, int* __
   }
 }
 
+// Fields at user sampling points (interpolateUserSampling,
+// unaveraged_interpolation.cc:560-691), one thread per point of a single
+// sub-box's tessellation.  keep[i]: the point lies in the region (closed);
+// idx: exclusive prefix of keep, the point's output row.  Seed: the bin of the
+// tile cell holding the point (when the seeds are built and the point lies in
+// the tile), else the sub-box's first tetrahedron; then the walk and the
+// cell-centre arithmetic at the point.
+struct Region6 {
+  float r[6];
+};
+__global__ void k_points_keep(int64_t n, const float* __restrict__ pts, Region6 R, int* __restrict__ keep) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  bool in = true;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float q = pts[3 * i + c];
+    in = in && q >= R.r[2 * c] && q <= R.r[2 * c + 1];
+  }
+  keep[i] = in ? 1 : 0;
+}
+
+template <int S>
+__global__ void __launch_bounds__(256) k_points_eval(InterpParams P, int64_t n, const float* __restrict__ pts,
+                                                     const int* __restrict__ keep, const int64_t* __restrict__ idx,
+                                                     int use_bins) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const bool active = i < n && keep[i];
+  WalkStats st{0, 0, 0};
+  unsigned n_loc = 0, n_out = 0, n_fail = 0;
+  if (active) {
+    const float pf[3] = {pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
+    const double p[3] = {(double)pf[0], (double)pf[1], (double)pf[2]};
+    const dtfe_subbox& B = P.boxes[0];
+    int t0 = B.n_tets > 0 ? (int)B.tet_offset : -1;
+    if (use_bins && t0 >= 0) {
+      SampleCell c;
+      bool in = true;
+      int ijk[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const float f = floorf((pf[a] - B.lo[a]) / B.dx[a]);
+        in = in && f >= 0.f && f < (float)B.tile_dims[a];
+        ijk[a] = in ? (int)f : 0;
+      }
+      if (in) {
+        c.b = 0;
+        c.i = ijk[0];
+        c.j = ijk[1];
+        c.k = ijk[2];
+        c.local = ((int64_t)ijk[0] * B.tile_dims[1] + ijk[1]) * B.tile_dims[2] + ijk[2];
+        t0 = seed_of(P, c);
+      }
+    }
+    int v[4];
+    float X[4][3];
+    int t = t0 < 0 ? kOutside : walk_locate<true>(P.tet_v, P.tet_n, P.posd, p, t0, P.max_steps, v, X, st);
+    ++n_loc;
+    if (t == kWalkFail) {
+      ++n_fail;
+      t = kOutside;
+    }
+    n_out += t < 0;
+    CellOut e;
+    e.dens = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) e.vel[c] = 0.f;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) e.grad[c] = 0.f;
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+      e.sc[q] = 0.f;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) e.scg[3 * q + c] = 0.f;
+    }
+    const uint32_t F = P.fields;
+    const bool want_grad = has_field(F, DTFE_VELOCITY_GRADIENT) || has_field(F, DTFE_VELOCITY_DIVERGENCE) ||
+                           has_field(F, DTFE_VELOCITY_SHEAR) || has_field(F, DTFE_VELOCITY_VORTICITY);
+    const bool want_vel = has_field(F, DTFE_VELOCITY) || want_grad;
+    const bool want_sc = S > 0 && (has_field(F, DTFE_SCALAR) || has_field(F, DTFE_SCALAR_GRADIENT));
+    if (t >= 0) cell_eval<S>(v, X, p, P.posd, P.vel4, P.scal, has_field(F, DTFE_DENSITY), want_vel, want_sc, P.fix != 0, e);
+    const int64_t o = idx[i];
+    if (has_field(F, DTFE_DENSITY)) P.out[DTFE_DENSITY][o] = e.dens;
+    if (has_field(F, DTFE_VELOCITY))
+#pragma unroll
+      for (int c = 0; c < 3; ++c) P.out[DTFE_VELOCITY][3 * o + c] = e.vel[c];
+    if (has_field(F, DTFE_VELOCITY_GRADIENT))
+#pragma unroll
+      for (int c = 0; c < 9; ++c) P.out[DTFE_VELOCITY_GRADIENT][9 * o + c] = e.grad[c];
+    if (has_field(F, DTFE_VELOCITY_DIVERGENCE) || has_field(F, DTFE_VELOCITY_SHEAR) ||
+        has_field(F, DTFE_VELOCITY_VORTICITY)) {
+      float dv, sh[5], vo[3];
+      derived_fields(e.grad, dv, sh, vo);
+      if (has_field(F, DTFE_VELOCITY_DIVERGENCE)) P.out[DTFE_VELOCITY_DIVERGENCE][o] = dv;
+      if (has_field(F, DTFE_VELOCITY_SHEAR))
+#pragma unroll
+        for (int c = 0; c < 5; ++c) P.out[DTFE_VELOCITY_SHEAR][5 * o + c] = sh[c];
+      if (has_field(F, DTFE_VELOCITY_VORTICITY))
+#pragma unroll
+        for (int c = 0; c < 3; ++c) P.out[DTFE_VELOCITY_VORTICITY][3 * o + c] = vo[c];
+    }
+    if (S > 0 && has_field(F, DTFE_SCALAR))
+#pragma unroll
+      for (int q = 0; q < S; ++q) P.out[DTFE_SCALAR][(int64_t)S * o + q] = e.sc[q];
+    if (S > 0 && has_field(F, DTFE_SCALAR_GRADIENT))
+#pragma unroll
+      for (int q = 0; q < 3 * S; ++q) P.out[DTFE_SCALAR_GRADIENT][(int64_t)3 * S * o + q] = e.scg[q];
+  }
+  fold_counters(P, n_loc, n_out, n_fail, st);
+}
+
 // Cell averages (methods 2 and 3): n points per cell, each walked from the
 // cell centre's tetrahedron (averaged_interpolation_2.cc:123,145), summed in
 // sample order as the reference does, divided by n; infinite-cell points are
@@ -1159,6 +1270,11 @@ struct dtfe_gpu_s {
   void* sph_scratch = nullptr;    // SPH cell grids, neighbour bookkeeping, FP64 sums
   size_t sph_bytes = 0;
   std::vector<float> regions_h;   // 6 per sub-box: tile regions (averaging method 1)
+  float* pts_buf = nullptr;       // user sampling points: positions, then the output rows
+  int* pts_keep = nullptr;
+  int64_t* pts_idx = nullptr;
+  int64_t* pts_blocks = nullptr;
+  float* pts_out = nullptr;
   double* m1_table = nullptr;     // method-1 Sobol points (100 NN x 3)
   int m1_table_nn = 0;
   void* m1_scratch = nullptr;     // method-1 counts, offsets, scan scratch
@@ -1396,7 +1512,8 @@ int dtfe_gpu_destroy(dtfe_handle h) {
   cudaStreamSynchronize(h->stream);
   if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
   void* ptrs[] = {h->tet_v, h->tet_n, h->posd, h->vel4, h->scal, h->w, h->vol, h->inc_off, h->inc,
-                  h->scratch_i, h->scan_blocks, h->hull,
+                  h->scratch_i, h->scan_blocks, h->hull, h->pts_buf, h->pts_keep, h->pts_idx, h->pts_blocks,
+                  h->pts_out,
                   h->boxes, h->tile_prefix, h->pencil_prefix, h->tet_prefix, h->bin_offset, h->bins,
                   h->xs, h->ys, h->zs, h->eq_off, h->counters, h->tet_c, h->raster_axes};
   for (void* p : ptrs)
@@ -2072,6 +2189,93 @@ int dtfe_gpu_interpolate_dev(dtfe_handle h, const dtfe_interp_opts* opts,
   if (!h) return set_error(DTFE_ERR_ARG, "null handle");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
   return interpolate_impl(h, opts, out_dev, st);
+}
+
+int dtfe_gpu_interpolate_points(dtfe_handle h, int64_t n, const float* xyz, const float region[6],
+                                const dtfe_interp_opts* o, float* const out[DTFE_NUM_FIELDS], int64_t* n_out) {
+  if (!h || !o || !region || !n_out || (n > 0 && !xyz) || n < 0) return set_error(DTFE_ERR_ARG, "null argument");
+  if (o->method != DTFE_METHOD_CENTRE) return set_error(DTFE_ERR_ARG, "user sampling points take the centre method");
+  if (h->K != 1)
+    return set_error(DTFE_ERR_STATE, "user sampling points need one sub-box (the reference runs them without the split)");
+  if (!h->density_ready) return set_error(DTFE_ERR_STATE, "vertex density not computed");
+  const uint32_t F = o->fields;
+  if ((F >> DTFE_NUM_FIELDS) || (F & DTFE_FIELD_BIT(DTFE_VELOCITY_STD)))
+    return set_error(DTFE_ERR_ARG, "unknown field bits or velocity_std at user points");
+  if (h->S == 0 && (F & (DTFE_FIELD_BIT(DTFE_SCALAR) | DTFE_FIELD_BIT(DTFE_SCALAR_GRADIENT))))
+    return set_error(DTFE_ERR_ARG, "scalar fields requested but n_scalars == 0");
+  for (int q = 0; q < DTFE_NUM_FIELDS; ++q)
+    if ((F >> q & 1u) && !out[q]) return set_error(DTFE_ERR_ARG, "missing output buffer");
+  *n_out = 0;
+  if (n == 0) return DTFE_OK;
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  int rc = prepare_centres(h);
+  if (rc) return rc;
+  cudaStream_t st = h->stream;
+  size_t comps = 0;
+  for (int q = 0; q < DTFE_NUM_FIELDS; ++q)
+    if (F >> q & 1u) comps += (size_t)field_components(q, h->S);
+  const int64_t nb = (n + kScanBlock - 1) / kScanBlock;
+  if ((rc = dev_alloc(h, &h->pts_buf, (size_t)3 * n)) || (rc = dev_alloc(h, &h->pts_keep, (size_t)n)) ||
+      (rc = dev_alloc(h, &h->pts_idx, (size_t)n + 1)) || (rc = dev_alloc(h, &h->pts_blocks, (size_t)nb + 1)) ||
+      (rc = dev_alloc(h, &h->pts_out, std::max<size_t>(comps, 1) * (size_t)n)))
+    return rc;
+  DTFE_CUDA_TRY(cudaMemcpyAsync(h->pts_buf, xyz, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, st));
+  Region6 R;
+  for (int c = 0; c < 6; ++c) R.r[c] = region[c];
+  k_points_keep<<<blocks_for(n, 256), 256, 0, st>>>(n, h->pts_buf, R, h->pts_keep);
+  k_scan_blocks<<<(unsigned)nb, kScanBlock, 0, st>>>(n, h->pts_keep, h->pts_idx, h->pts_blocks);
+  k_scan_totals<<<1, kScanBlock, 0, st>>>(nb, h->pts_blocks, h->pts_idx + n);
+  k_scan_add<<<(unsigned)nb, kScanBlock, 0, st>>>(n, h->pts_idx, h->pts_blocks);
+  DTFE_CUDA_TRY(cudaMemsetAsync(h->counters, 0, sizeof(unsigned long long) * CNT_N, st));
+  InterpParams P;
+  std::memset(&P, 0, sizeof(P));
+  P.tet_v = h->tet_v;
+  P.tet_n = h->tet_n;
+  P.posd = h->posd;
+  P.vel4 = h->vel4;
+  P.scal = h->scal;
+  P.bins = h->bins;
+  P.boxes = h->boxes;
+  P.tile_prefix = h->tile_prefix;
+  P.bin_offset = h->bin_offset;
+  P.K = h->K;
+  P.G1 = h->grid[1];
+  P.G2 = h->grid[2];
+  P.fields = F;
+  P.fix = (o->flags & DTFE_FLAG_FIX_VALUE_INTERP) ? 1 : 0;
+  P.max_steps = h->max_steps;
+  P.counters = h->counters;
+  P.S = h->S;
+  size_t at = 0;
+  for (int q = 0; q < DTFE_NUM_FIELDS; ++q) {
+    if (!(F >> q & 1u)) continue;
+    P.out[q] = h->pts_out + at * (size_t)n;
+    at += (size_t)field_components(q, h->S);
+  }
+  const int use_bins = h->prep_ready && !h->prep_raster ? 1 : 0;
+  const unsigned g = blocks_for(n, 256);
+  switch (h->S) {
+    case 0: k_points_eval<0><<<g, 256, 0, st>>>(P, n, h->pts_buf, h->pts_keep, h->pts_idx, use_bins); break;
+    case 1: k_points_eval<1><<<g, 256, 0, st>>>(P, n, h->pts_buf, h->pts_keep, h->pts_idx, use_bins); break;
+    case 2: k_points_eval<2><<<g, 256, 0, st>>>(P, n, h->pts_buf, h->pts_keep, h->pts_idx, use_bins); break;
+    case 3: k_points_eval<3><<<g, 256, 0, st>>>(P, n, h->pts_buf, h->pts_keep, h->pts_idx, use_bins); break;
+    case 4: k_points_eval<4><<<g, 256, 0, st>>>(P, n, h->pts_buf, h->pts_keep, h->pts_idx, use_bins); break;
+    case 5: k_points_eval<5><<<g, 256, 0, st>>>(P, n, h->pts_buf, h->pts_keep, h->pts_idx, use_bins); break;
+    case 6: k_points_eval<6><<<g, 256, 0, st>>>(P, n, h->pts_buf, h->pts_keep, h->pts_idx, use_bins); break;
+    case 7: k_points_eval<7><<<g, 256, 0, st>>>(P, n, h->pts_buf, h->pts_keep, h->pts_idx, use_bins); break;
+    default: k_points_eval<8><<<g, 256, 0, st>>>(P, n, h->pts_buf, h->pts_keep, h->pts_idx, use_bins); break;
+  }
+  DTFE_CUDA_TRY(cudaGetLastError());
+  int64_t m = 0;
+  DTFE_CUDA_TRY(cudaMemcpyAsync(&m, h->pts_idx + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  DTFE_CUDA_TRY(cudaStreamSynchronize(st));
+  for (int q = 0; q < DTFE_NUM_FIELDS; ++q)
+    if ((F >> q & 1u) && m > 0)
+      DTFE_CUDA_TRY(cudaMemcpyAsync(out[q], P.out[q], sizeof(float) * (size_t)field_components(q, h->S) * m,
+                                    cudaMemcpyDeviceToHost, st));
+  *n_out = m;
+  h->tet_c_valid = false;
+  return read_status(h, nullptr);
 }
 
 int dtfe_gpu_interpolate_dev_async(dtfe_handle h, const dtfe_interp_opts* opts,

@@ -141,6 +141,27 @@ class DeviceDTFE:
         self.last_status = st.as_dict()
         return self.last_status
 
+    def interpolate_points(self, fields, pts: np.ndarray, region, fix: bool = False) -> dict:
+        """Fields at user sampling points (dtfe_gpu_interpolate_points): dict
+        field -> float32 array of the points inside `region`, in order."""
+        pts = np.ascontiguousarray(pts, np.float32).reshape(-1, 3)
+        n = len(pts)
+        reg = np.ascontiguousarray(region, np.float32)
+        outs = [None] * N.NUM_FIELDS
+        res = {}
+        for f in fields:
+            s = N.FIELD_SLOTS[f]
+            nc = N.field_components(s, self.n_scalars)
+            a = np.zeros((n, nc) if nc > 1 else n, np.float32)
+            res[f] = a
+            outs[s] = N.ptr(a)
+        optr = (C.c_void_p * N.NUM_FIELDS)(*outs)
+        o = self._opts(fields, N.METHOD_CENTRE, 1, 0, fix)
+        m = C.c_int64(0)
+        N.check(self.lib.dtfe_gpu_interpolate_points(self.h, n, pts.ctypes.data, reg.ctypes.data, C.byref(o), optr,
+                                                     C.byref(m)))
+        return {f: a[:m.value] for f, a in res.items()}
+
     def interpolate_dev_async(self, fields, outs_dev: dict, method: int = 0, n_samples: int = 1, seed: int = 0,
                               fix: bool = False) -> None:
         """Queues the interpolation into device outputs without waiting

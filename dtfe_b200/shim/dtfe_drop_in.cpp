@@ -20,9 +20,11 @@
 // userOptions.uField (cell centres), aQuantities those of
 // userOptions.aField (method 1, 2 or 3 averages, or the NGP/CIC/TSC/SPH grids;
 // method 1 computes no velocity standard deviation, as the reference).
+// User sampling points (the samples vector) give uQuantities at the samples
+// inside the box, in order (interpolateUserSampling).
 // Unlike the reference, failures throw std::runtime_error instead of calling
-// exit(), and options this path does not cover throw as well: user sampling
-// points, redshift cones, --region, --partition, random subsamples, Poisson
+// exit(), and options this path does not cover throw as well: volume
+// averages at user sampling points, redshift cones, --region, --partition, random subsamples, Poisson
 // particles, explicit padding lengths, scalar fields with NGP/CIC/TSC.  The GPU is device 0 unless DTFE_GPU_DEVICE names another.
 
 #include <omp.h>
@@ -104,7 +106,7 @@ bool any(const Field& f) {
 void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& samples, User_options& userOptions,
           Quantities* uQuantities, Quantities* aQuantities) {
   User_options& o = userOptions;
-  unsupported(!samples.empty() || o.userDefinedSampling, "user-defined sampling points");
+  const bool user_points = !samples.empty() || o.userDefinedSampling;
   unsupported(o.redshiftConeOn, "redshift-cone grids");
   unsupported(o.regionOn, "--region");
   unsupported(o.partitionOn, "--partition");
@@ -114,6 +116,8 @@ void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& s
               "explicit padding lengths");
   unsupported(o.gridSize.size() != 3, "grids other than 3-D regular grids");
   const bool dtfe = !(o.NGP || o.CIC || o.TSC || o.SPH);
+  unsupported(user_points && (!dtfe || any(o.aField)),
+              "volume averages or NGP/CIC/TSC/SPH at user-defined sampling points");
   unsupported(dtfe && any(o.aField) && (o.method < 1 || o.method > 3), "averaging methods other than 1, 2, 3");
   unsupported(!dtfe && !o.SPH && (o.aField.scalar || o.aField.scalar_gradient), "scalar fields with NGP/CIC/TSC");
 
@@ -153,7 +157,8 @@ void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& s
 
   PlanGuard plan;
   check(dtfe_plan_build(kind, pos.data(), w.data(), velp, scp, S, n, box, o.periodic ? 1 : 0, grid,
-                        omp_get_max_threads(), (float)o.paddingParticles, (double)o.averageDensity, &plan.p),
+                        user_points ? 1 : omp_get_max_threads(),  // user samples: no split (src/DTFE.cpp:301)
+                        (float)o.paddingParticles, (double)o.averageDensity, &plan.p),
         "planning");
   dtfe_plan_view v;
   check(dtfe_plan_get(plan.p, &v), "plan view");
@@ -192,7 +197,29 @@ void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& s
   }
   check(dtfe_gpu_vertex_density(gpu.h, v.rho_bar), "vertex density");
   dtfe_status st;
-  if (any(o.uField)) {
+  if (any(o.uField) && user_points) {
+    // interpolateUserSampling: the samples inside the region (the box), in order
+    const size_t m = samples.size();
+    std::vector<float> pts(3 * m);
+    for (size_t i = 0; i < m; ++i)
+      for (int c = 0; c < 3; ++c) pts[3 * i + c] = samples[i].position(c);
+    float* out[DTFE_NUM_FIELDS];
+    dtfe_interp_opts io = {DTFE_METHOD_CENTRE, 1, 0, 0, 0};
+    outputs(o.uField, uQuantities, m, out, &io.fields);
+    int64_t kept = 0;
+    check(dtfe_gpu_interpolate_points(gpu.h, (int64_t)m, pts.data(), box, &io, out, &kept),
+          "interpolation at user sampling points");
+    Quantities* q = uQuantities;
+    const Field& f = o.uField;
+    if (f.density) q->density.resize(kept);
+    if (f.velocity) q->velocity.resize(kept);
+    if (f.velocity_gradient) q->velocity_gradient.resize(kept);
+    if (f.velocity_divergence) q->velocity_divergence.resize(kept);
+    if (f.velocity_shear) q->velocity_shear.resize(kept);
+    if (f.velocity_vorticity) q->velocity_vorticity.resize(kept);
+    if (f.scalar) q->scalar.resize(kept);
+    if (f.scalar_gradient) q->scalar_gradient.resize(kept);
+  } else if (any(o.uField)) {
     float* out[DTFE_NUM_FIELDS];
     dtfe_interp_opts io = {DTFE_METHOD_CENTRE, 1, 0, 0, 0};
     outputs(o.uField, uQuantities, G, out, &io.fields);

@@ -199,6 +199,16 @@ int dtfe_gpu_interpolate_dev(dtfe_handle h, const dtfe_interp_opts* opts,
  * dtfe_gpu_read_status.  Lets a caller overlap one handle's transfers with
  * another's (double buffering across snapshots). */
 int dtfe_gpu_interpolate_async(dtfe_handle h, const dtfe_interp_opts* opts, float* const out[DTFE_NUM_FIELDS]);
+/* Fields at user sampling points (interpolateUserSampling,
+ * unaveraged_interpolation.cc:560-691; DTFE() runs user samples without the
+ * sub-box split, src/DTFE.cpp:301): n points (xyz, 3 floats each, host);
+ * those outside region[6] (closed box) are dropped, the rest are located and
+ * evaluated as cell centres are (zeros outside the hull), in order.  The
+ * handle must hold one sub-box and its vertex densities; opts->method must be
+ * DTFE_METHOD_CENTRE.  out[slot] (host) receives *n_out rows of the field's
+ * components (size them for n). */
+int dtfe_gpu_interpolate_points(dtfe_handle h, int64_t n, const float* xyz, const float region[6],
+                                const dtfe_interp_opts* opts, float* const out[DTFE_NUM_FIELDS], int64_t* n_out);
 /* Same as dtfe_gpu_interpolate_dev, but only queues the work on the handle's
  * stream and returns without waiting: consecutive steps (vertex densities,
  * interpolation, ...) then run back to back on the device; the walk counters

@@ -107,4 +107,43 @@ int dropin_run(int estimator, const float* pos, const float* w, const float* vel
   return 0;
 }
 
+// DTFE() with user sampling points (n_samples, xyz 3 each) for the fields
+// u_fields: *n_kept rows (the samples inside the box) land in u_out.
+int dropin_run_points(const float* pos, const float* w, const float* vel, const float* scal, int64_t n,
+                      const float box[6], int periodic, const int32_t grid[3], double average_density,
+                      uint32_t u_fields, int64_t n_samples, const float* sxyz, int n_threads, float* const* u_out,
+                      int64_t* n_kept) {
+  std::vector<Particle_data> p(n);
+  for (int64_t i = 0; i < n; ++i) {
+    for (int c = 0; c < 3; ++c) p[i].pos[c] = pos[3 * i + c];
+    p[i].weight() = w ? w[i] : 1.f;
+    for (int c = 0; c < 3; ++c) p[i].velocity(c) = vel ? vel[3 * i + c] : 0.f;
+    p[i].scalar(0) = scal ? scal[i] : 0.f;
+  }
+  User_options o;
+  o.gridSize.assign(grid, grid + 3);
+  o.boxCoordinates.coords.assign(box, box + 6);
+  o.periodic = periodic != 0;
+  o.averageDensity = (Real)average_density;
+  o.userDefinedSampling = true;
+  set_fields(o.uField, u_fields);
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+  std::vector<Sample_point> samples((size_t)n_samples);
+  for (int64_t i = 0; i < n_samples; ++i) {
+    float q[3] = {sxyz[3 * i], sxyz[3 * i + 1], sxyz[3 * i + 2]};
+    samples[i].setPosition(q);
+  }
+  Quantities uq, aq;
+  try {
+    DTFE(&p, samples, o, &uq, &aq);
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return 1;
+  }
+  const size_t m = uq.density.size() ? uq.density.size() : uq.velocity.size();
+  *n_kept = (int64_t)m;
+  copy_all(uq, u_out, m);
+  return 0;
+}
+
 }  // extern "C"

@@ -27,6 +27,8 @@ def lib():
         L.dropin_run.argtypes = [C.c_int, vp, vp, vp, vp, C.c_int64, vp, C.c_int, vp, C.c_double, C.c_uint32,
                                  C.c_uint32, C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_int, vp, vp,
                                  C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+        L.dropin_run_points.argtypes = [vp, vp, vp, vp, C.c_int64, vp, C.c_int, vp, C.c_double, C.c_uint32,
+                                        C.c_int64, vp, C.c_int, vp, C.POINTER(C.c_int64)]
         L.dropin_error.restype = C.c_char_p
         _lib = L
     return _lib
@@ -61,3 +63,25 @@ def run(estimator, pos, w, vel, scal, grid, box=(0, 100, 0, 100, 0, 100), period
     if rc:
         raise RuntimeError(lib().dropin_error().decode())
     return ud, ad, avg.value, left.value
+
+
+def run_points(pos, w, vel, scal, grid, samples, box=(0, 100, 0, 100, 0, 100), periodic=True,
+               average_density=-1.0, u_fields=("density",), n_threads=4):
+    """DTFE() with user sampling points: dict field -> rows of the samples
+    inside the box, in order."""
+    pos = np.ascontiguousarray(pos, np.float32)
+    samples = np.ascontiguousarray(samples, np.float32)
+    m = len(samples)
+    d = {f: np.full((m, NCOMP[SLOTS[f]]), np.nan, np.float32) for f in u_fields}
+    ptrs = (C.c_void_p * 9)(*[d[f].ctypes.data if f in d else None for f in SLOTS])
+    mask = sum(1 << SLOTS[f] for f in u_fields)
+    g = np.ascontiguousarray(grid, np.int32)
+    bx = np.ascontiguousarray(box, np.float32)
+    keep = [np.ascontiguousarray(a, np.float32) if a is not None else None for a in (w, vel, scal)]
+    kept = C.c_int64()
+    rc = lib().dropin_run_points(pos.ctypes.data, *[a.ctypes.data if a is not None else None for a in keep],
+                                 len(pos), bx.ctypes.data, int(periodic), g.ctypes.data, float(average_density),
+                                 mask, m, samples.ctypes.data, n_threads, ptrs, C.byref(kept))
+    if rc:
+        raise RuntimeError(lib().dropin_error().decode())
+    return {f: a[:kept.value] for f, a in d.items()}

@@ -105,3 +105,23 @@ def test_dropin_method1(particles):
                               n_samples=100)
     for f in ("density", "velocity", "velocity_gradient", "scalar"):
         assert np.array_equal(a[f].reshape(ref[f].shape), ref[f]), f
+
+
+def test_dropin_user_sampling(particles):
+    """DTFE() with user sampling points (the samples vector): the samples
+    inside the box, in order, equal the device API's user-point interpolation
+    on the reference's single-box plan."""
+    from dtfe_b200.device import DeviceDTFE
+    pos, w, vel, sc = particles
+    rng = np.random.default_rng(11)
+    samples = rng.uniform(-10, 110, (3000, 3)).astype(np.float32)
+    fields = ["density", "velocity", "velocity_gradient", "velocity_divergence", "scalar"]
+    u = D.run_points(pos, w, vel, sc, GRID, samples, u_fields=fields)
+    plan = P.make_plan(pos, w, vel, sc[:, None], grid=GRID, n_threads=1)
+    with DeviceDTFE(0, 1) as dev:
+        dev.load(plan)
+        dev.vertex_density(plan.rho_bar)
+        ref = dev.interpolate_points(fields, samples, [0, 100, 0, 100, 0, 100])
+    for f in fields:
+        assert len(u[f]) == len(ref[f]) < len(samples)
+        assert np.array_equal(u[f].reshape(ref[f].shape), ref[f]), f

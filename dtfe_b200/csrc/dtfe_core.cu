@@ -873,11 +873,40 @@ __global__ void __launch_bounds__(kInterpBlock, MINB) k_locate_eval(InterpParams
   fold_counters(P, n_loc, n_out, n_fail, wst);
 }
 
+// Zeroes every sample of a pencil of nz samples after its first outside one
+// (tet_c[s0 + k] < 0): the pencil's samples are tet_c[s0 .. s0 + nz), its
+// cells P.out rows c0 .. c0 + nz.  One warp reads the located tetrahedra 32 at
+// a time; later inside samples are marked outside and their fields zeroed.
+__device__ __forceinline__ void zero_after_outside(const InterpParams& P, int* __restrict__ tet_c, int64_t s0,
+                                                   int64_t c0, int nz, int lane) {
+  bool seen = false;
+  for (int k0 = 0; k0 < nz; k0 += 32) {
+    const int k = k0 + lane;
+    const bool valid = k < nz;
+    const int t = valid ? tet_c[s0 + k] : 0;
+    const unsigned outside = __ballot_sync(0xffffffffu, valid && t < 0);
+    const bool poison = seen || (outside & ((1u << lane) - 1u)) != 0;
+    if (valid && poison && t >= 0) {
+      tet_c[s0 + k] = kOutside;
+      const int64_t cell = c0 + k;
+      for (int slot = 0; slot < DTFE_NUM_FIELDS; ++slot) {
+        if (!has_field(P.fields, slot) || !P.out[slot]) continue;
+        const int nc = slot == DTFE_VELOCITY || slot == DTFE_VELOCITY_VORTICITY ? 3
+                     : slot == DTFE_VELOCITY_GRADIENT ? 9
+                     : slot == DTFE_VELOCITY_SHEAR ? 5
+                     : slot == DTFE_SCALAR ? P.S
+                     : slot == DTFE_SCALAR_GRADIENT ? 3 * P.S : 1;
+        for (int c = 0; c < nc; ++c) P.out[slot][cell * nc + c] = 0.f;
+      }
+    }
+    seen = seen || outside != 0u;
+  }
+}
+
 // The reference's cell-centre raster after an outside sample: it skips
 // `z += dx` (unaveraged_interpolation.cc:304 jumps over :353), so the rest of
 // the z pencil re-locates that outside point and gets zeros.  One warp per
-// pencil reads its located tetrahedra 32 at a time; every cell after the
-// pencil's first outside one is marked outside and its fields zeroed.
+// pencil of the sub-box tiles.
 __global__ void __launch_bounds__(256) k_outside_pencils(InterpParams P, int* __restrict__ tet_c, int64_t n_pencils) {
   const int lane = threadIdx.x & 31;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -889,29 +918,18 @@ __global__ void __launch_bounds__(256) k_outside_pencils(InterpParams P, int* __
     const int i = (int)(local / (uint32_t)ny), j = (int)(local - (uint32_t)i * (uint32_t)ny);
     const int64_t s0 = __ldg(&P.tile_prefix[b]) + (int64_t)local * nz;
     const int64_t c0 = ((int64_t)(B.tile_origin[0] + i) * P.G1 + (B.tile_origin[1] + j)) * P.G2 + B.tile_origin[2];
-    bool seen = false;
-    for (int k0 = 0; k0 < nz; k0 += 32) {
-      const int k = k0 + lane;
-      const bool valid = k < nz;
-      const int t = valid ? tet_c[s0 + k] : 0;
-      const unsigned outside = __ballot_sync(0xffffffffu, valid && t < 0);
-      const bool poison = seen || (outside & ((1u << lane) - 1u)) != 0;
-      if (valid && poison && t >= 0) {
-        tet_c[s0 + k] = kOutside;
-        const int64_t cell = c0 + k;
-        for (int slot = 0; slot < DTFE_NUM_FIELDS; ++slot) {
-          if (!has_field(P.fields, slot) || !P.out[slot]) continue;
-          const int nc = slot == DTFE_VELOCITY || slot == DTFE_VELOCITY_VORTICITY ? 3
-                       : slot == DTFE_VELOCITY_GRADIENT ? 9
-                       : slot == DTFE_VELOCITY_SHEAR ? 5
-                       : slot == DTFE_SCALAR ? P.S
-                       : slot == DTFE_SCALAR_GRADIENT ? 3 * P.S : 1;
-          for (int c = 0; c < nc; ++c) P.out[slot][cell * nc + c] = 0.f;
-        }
-      }
-      seen = seen || outside != 0u;
-    }
+    zero_after_outside(P, tet_c, s0, c0, nz, lane);
   }
+}
+
+// The same on a redshift-cone grid: an outside sample skips `psi += dx`
+// (unaveraged_interpolation.cc:466 jumps over :527), so the rest of its psi
+// row repeats it.  Rows of nz samples, sample index = output row.
+__global__ void __launch_bounds__(256) k_cone_rows(InterpParams P, int* __restrict__ tet_c, int64_t n_rows, int nz) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t q = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; q < n_rows; q += nw)
+    zero_after_outside(P, tet_c, q * nz, q * nz, nz, lane);
 }
 
 // Fields at user sampling points (interpolateUserSampling,
@@ -936,16 +954,58 @@ __global__ void k_points_keep(int64_t n, const float* __restrict__ pts, Region6 
   keep[i] = in ? 1 : 0;
 }
 
-template <int S>
-__global__ void __launch_bounds__(256) k_points_eval(InterpParams P, int64_t n, const float* __restrict__ pts,
-                                                     const int* __restrict__ keep, const int64_t* __restrict__ idx,
-                                                     int use_bins) {
+// Where k_points_eval takes its points.  User sampling points: those kept,
+// each written to its prefix row.
+struct PointList {
+  const float* pts;
+  const int* keep;
+  const int64_t* idx;
+  __device__ __forceinline__ bool get(int64_t i, float pf[3], int64_t& row) const {
+    if (!keep[i]) return false;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) pf[c] = pts[3 * i + c];
+    row = idx[i];
+    return true;
+  }
+};
+// Redshift-cone bins (unaveraged_interpolation.cc:441-447): sample
+// (i, j, k) = row (i n1 + j) n2 + k at o + (r st cp, r st sp, r ct), each
+// product and sum rounded in float left to right as the reference's
+// expression is (no contraction).  Tables: r[n0], st/ct[n1], cp/sp[n2].
+struct ConeGrid {
+  const float* r;
+  const float* st;
+  const float* ct;
+  const float* cp;
+  const float* sp;
+  float o[3];
+  uint32_t n1, n2;
+  __device__ __forceinline__ bool get(int64_t s, float pf[3], int64_t& row) const {
+    const uint64_t ij = (uint64_t)s / n2;
+    const uint32_t k = (uint32_t)((uint64_t)s - ij * n2);
+    const uint32_t i = (uint32_t)(ij / n1), j = (uint32_t)(ij - (uint64_t)i * n1);
+    const float ri = __ldg(&r[i]);
+    const float rs = __fmul_rn(ri, __ldg(&st[j]));
+    pf[0] = __fadd_rn(o[0], __fmul_rn(rs, __ldg(&cp[k])));
+    pf[1] = __fadd_rn(o[1], __fmul_rn(rs, __ldg(&sp[k])));
+    pf[2] = __fadd_rn(o[2], __fmul_rn(ri, __ldg(&ct[j])));
+    row = s;
+    return true;
+  }
+};
+
+// tet_out (may be null): the located tetrahedron of each row, kOutside when
+// outside the hull.
+template <int S, class Src>
+__global__ void __launch_bounds__(256) k_points_eval(InterpParams P, int64_t n, Src src, int use_bins,
+                                                     int* __restrict__ tet_out) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const bool active = i < n && keep[i];
+  float pf[3];
+  int64_t o = 0;
+  const bool active = i < n && src.get(i, pf, o);
   WalkStats st{0, 0, 0};
   unsigned n_loc = 0, n_out = 0, n_fail = 0;
   if (active) {
-    const float pf[3] = {pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
     const double p[3] = {(double)pf[0], (double)pf[1], (double)pf[2]};
     const dtfe_subbox& B = P.boxes[0];
     int t0 = B.n_tets > 0 ? (int)B.tet_offset : -1;
@@ -995,7 +1055,7 @@ __global__ void __launch_bounds__(256) k_points_eval(InterpParams P, int64_t n, 
     const bool want_vel = has_field(F, DTFE_VELOCITY) || want_grad;
     const bool want_sc = S > 0 && (has_field(F, DTFE_SCALAR) || has_field(F, DTFE_SCALAR_GRADIENT));
     if (t >= 0) cell_eval<S>(v, X, p, P.posd, P.vel4, P.scal, has_field(F, DTFE_DENSITY), want_vel, want_sc, P.fix != 0, e);
-    const int64_t o = idx[i];
+    if (tet_out) tet_out[o] = t;
     if (has_field(F, DTFE_DENSITY)) P.out[DTFE_DENSITY][o] = e.dens;
     if (has_field(F, DTFE_VELOCITY))
 #pragma unroll
@@ -2191,42 +2251,39 @@ int dtfe_gpu_interpolate_dev(dtfe_handle h, const dtfe_interp_opts* opts,
   return interpolate_impl(h, opts, out_dev, st);
 }
 
-int dtfe_gpu_interpolate_points(dtfe_handle h, int64_t n, const float* xyz, const float region[6],
-                                const dtfe_interp_opts* o, float* const out[DTFE_NUM_FIELDS], int64_t* n_out) {
-  if (!h || !o || !region || !n_out || (n > 0 && !xyz) || n < 0) return set_error(DTFE_ERR_ARG, "null argument");
-  if (o->method != DTFE_METHOD_CENTRE) return set_error(DTFE_ERR_ARG, "user sampling points take the centre method");
+}  // extern "C"
+
+namespace {
+
+// Argument checks shared by the point-sample entry points (user points,
+// redshift cones): one sub-box with its vertex densities, the centre method,
+// known fields with their output buffers.
+int check_point_call(dtfe_handle h, const dtfe_interp_opts* o, float* const out[DTFE_NUM_FIELDS], const char* what) {
+  if (o->method != DTFE_METHOD_CENTRE) return set_error(DTFE_ERR_ARG, std::string(what) + " take the centre method");
   if (h->K != 1)
-    return set_error(DTFE_ERR_STATE, "user sampling points need one sub-box (the reference runs them without the split)");
+    return set_error(DTFE_ERR_STATE,
+                     std::string(what) + " need one sub-box (the reference runs them without the split)");
   if (!h->density_ready) return set_error(DTFE_ERR_STATE, "vertex density not computed");
   const uint32_t F = o->fields;
   if ((F >> DTFE_NUM_FIELDS) || (F & DTFE_FIELD_BIT(DTFE_VELOCITY_STD)))
-    return set_error(DTFE_ERR_ARG, "unknown field bits or velocity_std at user points");
+    return set_error(DTFE_ERR_ARG, std::string("unknown field bits or velocity_std at ") + what);
   if (h->S == 0 && (F & (DTFE_FIELD_BIT(DTFE_SCALAR) | DTFE_FIELD_BIT(DTFE_SCALAR_GRADIENT))))
     return set_error(DTFE_ERR_ARG, "scalar fields requested but n_scalars == 0");
   for (int q = 0; q < DTFE_NUM_FIELDS; ++q)
     if ((F >> q & 1u) && !out[q]) return set_error(DTFE_ERR_ARG, "missing output buffer");
-  *n_out = 0;
-  if (n == 0) return DTFE_OK;
-  DTFE_CUDA_TRY(cudaSetDevice(h->device));
-  int rc = prepare_centres(h);
-  if (rc) return rc;
-  cudaStream_t st = h->stream;
+  return DTFE_OK;
+}
+
+size_t point_components(dtfe_handle h, uint32_t F) {
   size_t comps = 0;
   for (int q = 0; q < DTFE_NUM_FIELDS; ++q)
     if (F >> q & 1u) comps += (size_t)field_components(q, h->S);
-  const int64_t nb = (n + kScanBlock - 1) / kScanBlock;
-  if ((rc = dev_alloc(h, &h->pts_buf, (size_t)3 * n)) || (rc = dev_alloc(h, &h->pts_keep, (size_t)n)) ||
-      (rc = dev_alloc(h, &h->pts_idx, (size_t)n + 1)) || (rc = dev_alloc(h, &h->pts_blocks, (size_t)nb + 1)) ||
-      (rc = dev_alloc(h, &h->pts_out, std::max<size_t>(comps, 1) * (size_t)n)))
-    return rc;
-  DTFE_CUDA_TRY(cudaMemcpyAsync(h->pts_buf, xyz, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, st));
-  Region6 R;
-  for (int c = 0; c < 6; ++c) R.r[c] = region[c];
-  k_points_keep<<<blocks_for(n, 256), 256, 0, st>>>(n, h->pts_buf, R, h->pts_keep);
-  k_scan_blocks<<<(unsigned)nb, kScanBlock, 0, st>>>(n, h->pts_keep, h->pts_idx, h->pts_blocks);
-  k_scan_totals<<<1, kScanBlock, 0, st>>>(nb, h->pts_blocks, h->pts_idx + n);
-  k_scan_add<<<(unsigned)nb, kScanBlock, 0, st>>>(n, h->pts_idx, h->pts_blocks);
-  DTFE_CUDA_TRY(cudaMemsetAsync(h->counters, 0, sizeof(unsigned long long) * CNT_N, st));
+  return comps;
+}
+
+// Interpolation parameters of a point-sample launch: the handle's single
+// sub-box, outputs staged field after field in h->pts_out (`rows` rows each).
+InterpParams point_params(dtfe_handle h, const dtfe_interp_opts* o, int64_t rows) {
   InterpParams P;
   std::memset(&P, 0, sizeof(P));
   P.tet_v = h->tet_v;
@@ -2241,39 +2298,170 @@ int dtfe_gpu_interpolate_points(dtfe_handle h, int64_t n, const float* xyz, cons
   P.K = h->K;
   P.G1 = h->grid[1];
   P.G2 = h->grid[2];
-  P.fields = F;
+  P.fields = o->fields;
   P.fix = (o->flags & DTFE_FLAG_FIX_VALUE_INTERP) ? 1 : 0;
   P.max_steps = h->max_steps;
   P.counters = h->counters;
   P.S = h->S;
   size_t at = 0;
   for (int q = 0; q < DTFE_NUM_FIELDS; ++q) {
-    if (!(F >> q & 1u)) continue;
-    P.out[q] = h->pts_out + at * (size_t)n;
+    if (!(o->fields >> q & 1u)) continue;
+    P.out[q] = h->pts_out + at * (size_t)rows;
     at += (size_t)field_components(q, h->S);
   }
-  const int use_bins = h->prep_ready && !h->prep_raster ? 1 : 0;
+  return P;
+}
+
+template <class Src>
+void launch_points_eval(dtfe_handle h, const InterpParams& P, int64_t n, const Src& src, int use_bins,
+                        int* tet_out) {
   const unsigned g = blocks_for(n, 256);
+  cudaStream_t st = h->stream;
   switch (h->S) {
-    case 0: k_points_eval<0><<<g, 256, 0, st>>>(P, n, h->pts_buf, h->pts_keep, h->pts_idx, use_bins); break;
-    case 1: k_points_eval<1><<<g, 256, 0, st>>>(P, n, h->pts_buf, h->pts_keep, h->pts_idx, use_bins); break;
-    case 2: k_points_eval<2><<<g, 256, 0, st>>>(P, n, h->pts_buf, h->pts_keep, h->pts_idx, use_bins); break;
-    case 3: k_points_eval<3><<<g, 256, 0, st>>>(P, n, h->pts_buf, h->pts_keep, h->pts_idx, use_bins); break;
-    case 4: k_points_eval<4><<<g, 256, 0, st>>>(P, n, h->pts_buf, h->pts_keep, h->pts_idx, use_bins); break;
-    case 5: k_points_eval<5><<<g, 256, 0, st>>>(P, n, h->pts_buf, h->pts_keep, h->pts_idx, use_bins); break;
-    case 6: k_points_eval<6><<<g, 256, 0, st>>>(P, n, h->pts_buf, h->pts_keep, h->pts_idx, use_bins); break;
-    case 7: k_points_eval<7><<<g, 256, 0, st>>>(P, n, h->pts_buf, h->pts_keep, h->pts_idx, use_bins); break;
-    default: k_points_eval<8><<<g, 256, 0, st>>>(P, n, h->pts_buf, h->pts_keep, h->pts_idx, use_bins); break;
+    case 0: k_points_eval<0, Src><<<g, 256, 0, st>>>(P, n, src, use_bins, tet_out); break;
+    case 1: k_points_eval<1, Src><<<g, 256, 0, st>>>(P, n, src, use_bins, tet_out); break;
+    case 2: k_points_eval<2, Src><<<g, 256, 0, st>>>(P, n, src, use_bins, tet_out); break;
+    case 3: k_points_eval<3, Src><<<g, 256, 0, st>>>(P, n, src, use_bins, tet_out); break;
+    case 4: k_points_eval<4, Src><<<g, 256, 0, st>>>(P, n, src, use_bins, tet_out); break;
+    case 5: k_points_eval<5, Src><<<g, 256, 0, st>>>(P, n, src, use_bins, tet_out); break;
+    case 6: k_points_eval<6, Src><<<g, 256, 0, st>>>(P, n, src, use_bins, tet_out); break;
+    case 7: k_points_eval<7, Src><<<g, 256, 0, st>>>(P, n, src, use_bins, tet_out); break;
+    default: k_points_eval<8, Src><<<g, 256, 0, st>>>(P, n, src, use_bins, tet_out); break;
   }
+}
+
+// Per-axis tables of a redshift-cone grid in the reference's float arithmetic
+// (checkAngles, triangulation_miscellaneous.cc:162-197; the bin loops of
+// interpolateRedshiftCone, unaveraged_interpolation.cc:387-447; the checks of
+// src/user_options.cc:1000-1009).  tab: r[n0], st[n1], ct[n1], cp[n2], sp[n2].
+int cone_tables(const float cone[6], const int32_t dims[3], std::vector<float>& tab) {
+  float b[6];
+  for (int i = 0; i < 6; ++i) b[i] = cone[i];
+  for (int a = 0; a < 3; ++a)
+    if (dims[a] <= 0) return set_error(DTFE_ERR_ARG, "redshift-cone bins must be positive");
+  if (!(b[2] >= 0.f && b[2] <= 180.f && b[3] >= 0.f && b[3] <= 180.f))
+    return set_error(DTFE_ERR_ARG, "redshift-cone theta limits must lie in [0, 180] degrees");
+  if (!(b[5] - b[4] < 360.f)) return set_error(DTFE_ERR_ARG, "the psi range of a redshift cone spans 360 degrees or more");
+  for (int i = 4; i < 6; ++i) b[i] -= std::floor(b[i] / 360.f) * 360.f;  // psi into [0, 360)
+  if (b[4] > b[5]) b[5] += 360.f;
+  const float rad = (float)(3.14159265 / 180.);  // the reference's PI (define.h:47)
+  for (int i = 2; i < 6; ++i) b[i] *= rad;
+  float dx[3];
+  for (int a = 0; a < 3; ++a) dx[a] = (b[2 * a + 1] - b[2 * a]) / (float)dims[a];
+  const size_t n0 = (size_t)dims[0], n1 = (size_t)dims[1], n2 = (size_t)dims[2];
+  tab.assign(n0 + 2 * n1 + 2 * n2, 0.f);
+  float* r = tab.data();
+  float* st = r + n0;
+  float* ct = st + n1;
+  float* cp = ct + n1;
+  float* sp = cp + n2;
+  float x = (float)((double)b[0] + (double)dx[0] / 2.);
+  for (size_t i = 0; i < n0; ++i, x += dx[0]) r[i] = x;
+  x = (float)((double)b[2] + (double)dx[1] / 2.);
+  for (size_t j = 0; j < n1; ++j, x += dx[1]) {
+    st[j] = std::sin(x);
+    ct[j] = std::cos(x);
+  }
+  x = (float)((double)b[4] + (double)dx[2] / 2.);
+  for (size_t k = 0; k < n2; ++k, x += dx[2]) {
+    cp[k] = std::cos(x);
+    sp[k] = std::sin(x);
+  }
+  return DTFE_OK;
+}
+
+// Copies the staged rows of every requested field into the caller's host
+// buffers and waits for them.
+int copy_point_rows(dtfe_handle h, const InterpParams& P, uint32_t F, int64_t m, float* const out[DTFE_NUM_FIELDS]) {
+  for (int q = 0; q < DTFE_NUM_FIELDS; ++q)
+    if ((F >> q & 1u) && m > 0)
+      DTFE_CUDA_TRY(cudaMemcpyAsync(out[q], P.out[q], sizeof(float) * (size_t)field_components(q, h->S) * m,
+                                    cudaMemcpyDeviceToHost, h->stream));
+  DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return DTFE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dtfe_gpu_interpolate_points(dtfe_handle h, int64_t n, const float* xyz, const float region[6],
+                                const dtfe_interp_opts* o, float* const out[DTFE_NUM_FIELDS], int64_t* n_out) {
+  if (!h || !o || !region || !out || !n_out || (n > 0 && !xyz) || n < 0) return set_error(DTFE_ERR_ARG, "null argument");
+  int rc = check_point_call(h, o, out, "user sampling points");
+  if (rc) return rc;
+  *n_out = 0;
+  if (n == 0) return DTFE_OK;
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  if ((rc = prepare_centres(h))) return rc;
+  cudaStream_t st = h->stream;
+  const uint32_t F = o->fields;
+  const size_t comps = point_components(h, F);
+  const int64_t nb = (n + kScanBlock - 1) / kScanBlock;
+  if ((rc = dev_alloc(h, &h->pts_buf, (size_t)3 * n)) || (rc = dev_alloc(h, &h->pts_keep, (size_t)n)) ||
+      (rc = dev_alloc(h, &h->pts_idx, (size_t)n + 1)) || (rc = dev_alloc(h, &h->pts_blocks, (size_t)nb + 1)) ||
+      (rc = dev_alloc(h, &h->pts_out, std::max<size_t>(comps, 1) * (size_t)n)))
+    return rc;
+  DTFE_CUDA_TRY(cudaMemcpyAsync(h->pts_buf, xyz, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, st));
+  Region6 R;
+  for (int c = 0; c < 6; ++c) R.r[c] = region[c];
+  k_points_keep<<<blocks_for(n, 256), 256, 0, st>>>(n, h->pts_buf, R, h->pts_keep);
+  k_scan_blocks<<<(unsigned)nb, kScanBlock, 0, st>>>(n, h->pts_keep, h->pts_idx, h->pts_blocks);
+  k_scan_totals<<<1, kScanBlock, 0, st>>>(nb, h->pts_blocks, h->pts_idx + n);
+  k_scan_add<<<(unsigned)nb, kScanBlock, 0, st>>>(n, h->pts_idx, h->pts_blocks);
+  DTFE_CUDA_TRY(cudaMemsetAsync(h->counters, 0, sizeof(unsigned long long) * CNT_N, st));
+  const InterpParams P = point_params(h, o, n);
+  const int use_bins = h->prep_ready && !h->prep_raster ? 1 : 0;
+  launch_points_eval(h, P, n, PointList{h->pts_buf, h->pts_keep, h->pts_idx}, use_bins, nullptr);
   DTFE_CUDA_TRY(cudaGetLastError());
   int64_t m = 0;
   DTFE_CUDA_TRY(cudaMemcpyAsync(&m, h->pts_idx + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   DTFE_CUDA_TRY(cudaStreamSynchronize(st));
-  for (int q = 0; q < DTFE_NUM_FIELDS; ++q)
-    if ((F >> q & 1u) && m > 0)
-      DTFE_CUDA_TRY(cudaMemcpyAsync(out[q], P.out[q], sizeof(float) * (size_t)field_components(q, h->S) * m,
-                                    cudaMemcpyDeviceToHost, st));
+  if ((rc = copy_point_rows(h, P, F, m, out))) return rc;
   *n_out = m;
+  h->tet_c_valid = false;
+  return read_status(h, nullptr);
+}
+
+int dtfe_gpu_interpolate_cone(dtfe_handle h, const float cone[6], const float origin[3], const int32_t dims[3],
+                              const dtfe_interp_opts* o, float* const out[DTFE_NUM_FIELDS]) {
+  if (!h || !o || !cone || !origin || !dims || !out) return set_error(DTFE_ERR_ARG, "null argument");
+  int rc = check_point_call(h, o, out, "redshift-cone grids");
+  if (rc) return rc;
+  std::vector<float> tab;
+  if ((rc = cone_tables(cone, dims, tab))) return rc;
+  const int64_t n = (int64_t)dims[0] * dims[1] * dims[2];
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  if ((rc = prepare_centres(h))) return rc;
+  cudaStream_t st = h->stream;
+  const uint32_t F = o->fields;
+  const size_t comps = point_components(h, F);
+  // pts_buf holds the cone's tables, pts_keep the located tetrahedra
+  if ((rc = dev_alloc(h, &h->pts_buf, tab.size())) || (rc = dev_alloc(h, &h->pts_keep, (size_t)n)) ||
+      (rc = dev_alloc(h, &h->pts_out, std::max<size_t>(comps, 1) * (size_t)n)))
+    return rc;
+  DTFE_CUDA_TRY(cudaMemcpyAsync(h->pts_buf, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice, st));
+  DTFE_CUDA_TRY(cudaMemsetAsync(h->counters, 0, sizeof(unsigned long long) * CNT_N, st));
+  const InterpParams P = point_params(h, o, n);
+  ConeGrid src;
+  src.r = h->pts_buf;
+  src.st = src.r + dims[0];
+  src.ct = src.st + dims[1];
+  src.cp = src.ct + dims[1];
+  src.sp = src.cp + dims[2];
+  for (int c = 0; c < 3; ++c) src.o[c] = origin[c];
+  src.n1 = (uint32_t)dims[1];
+  src.n2 = (uint32_t)dims[2];
+  const int use_bins = h->prep_ready && !h->prep_raster ? 1 : 0;
+  launch_points_eval(h, P, n, src, use_bins, h->pts_keep);
+  DTFE_CUDA_TRY(cudaGetLastError());
+  if (!(o->flags & DTFE_FLAG_FIX_OUTSIDE_RASTER)) {
+    const int64_t rows = (int64_t)dims[0] * dims[1];
+    const int64_t want = (rows + 7) / 8;  // 8 warps per block
+    k_cone_rows<<<(unsigned)std::min<int64_t>(want, 148 * 16), 256, 0, st>>>(P, h->pts_keep, rows, dims[2]);
+    DTFE_CUDA_TRY(cudaGetLastError());
+  }
+  if ((rc = copy_point_rows(h, P, F, n, out))) return rc;
   h->tet_c_valid = false;
   return read_status(h, nullptr);
 }

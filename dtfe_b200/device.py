@@ -162,6 +162,28 @@ class DeviceDTFE:
                                                      C.byref(m)))
         return {f: a[:m.value] for f, a in res.items()}
 
+    def interpolate_cone(self, fields, cone, origin, dims, fix: bool = False, fix_outside: bool = False) -> dict:
+        """Fields on a redshift-cone grid (dtfe_gpu_interpolate_cone): dict
+        field -> float32 array of dims[0] * dims[1] * dims[2] rows, r slowest
+        and psi fastest."""
+        d = np.ascontiguousarray(dims, np.int32)
+        c = np.ascontiguousarray(cone, np.float32)
+        org = np.ascontiguousarray(origin, np.float32)
+        n = int(np.prod(d.astype(np.int64)))
+        outs = [None] * N.NUM_FIELDS
+        res = {}
+        for f in fields:
+            s = N.FIELD_SLOTS[f]
+            nc = N.field_components(s, self.n_scalars)
+            a = np.zeros((n, nc) if nc > 1 else n, np.float32)
+            res[f] = a
+            outs[s] = N.ptr(a)
+        optr = (C.c_void_p * N.NUM_FIELDS)(*outs)
+        o = self._opts(fields, N.METHOD_CENTRE, 1, 0, fix, fix_outside)
+        N.check(self.lib.dtfe_gpu_interpolate_cone(self.h, c.ctypes.data, org.ctypes.data, d.ctypes.data, C.byref(o),
+                                                   optr))
+        return res
+
     def interpolate_dev_async(self, fields, outs_dev: dict, method: int = 0, n_samples: int = 1, seed: int = 0,
                               fix: bool = False) -> None:
         """Queues the interpolation into device outputs without waiting

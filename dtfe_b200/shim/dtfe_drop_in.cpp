@@ -21,11 +21,13 @@
 // userOptions.aField (method 1, 2 or 3 averages, or the NGP/CIC/TSC/SPH grids;
 // method 1 computes no velocity standard deviation, as the reference).
 // User sampling points (the samples vector) give uQuantities at the samples
-// inside the box, in order (interpolateUserSampling).
+// inside the box, in order (interpolateUserSampling); a redshift cone
+// (redshiftConeOn) gives them on its gridSize bins (interpolateRedshiftCone).
 // Unlike the reference, failures throw std::runtime_error instead of calling
 // exit(), and options this path does not cover throw as well: volume
-// averages at user sampling points, redshift cones, --region, --partition, random subsamples, Poisson
-// particles, explicit padding lengths, scalar fields with NGP/CIC/TSC.  The GPU is device 0 unless DTFE_GPU_DEVICE names another.
+// averages at user sampling points or on redshift cones, --region,
+// --partition, random subsamples, Poisson particles, explicit padding
+// lengths, scalar fields with NGP/CIC/TSC.  The GPU is device 0 unless DTFE_GPU_DEVICE names another.
 
 #include <omp.h>
 
@@ -107,7 +109,11 @@ void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& s
           Quantities* uQuantities, Quantities* aQuantities) {
   User_options& o = userOptions;
   const bool user_points = !samples.empty() || o.userDefinedSampling;
-  unsupported(o.redshiftConeOn, "redshift-cone grids");
+  const bool cone = o.redshiftConeOn && !user_points;  // user samples switch the cone off (user_options.cc:962-964)
+  unsupported(cone && (o.NGP || o.CIC || o.TSC || o.SPH || any(o.aField)),
+              "volume averages or NGP/CIC/TSC/SPH on redshift-cone grids");
+  unsupported(cone && (o.redshiftCone.coords.size() != 6 || o.originPosition.size() != 3),
+              "redshift cones without 6 limits and a 3-D origin");
   unsupported(o.regionOn, "--region");
   unsupported(o.partitionOn, "--partition");
   unsupported(o.randomSample >= Real(0.), "random subsamples");
@@ -157,7 +163,7 @@ void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& s
 
   PlanGuard plan;
   check(dtfe_plan_build(kind, pos.data(), w.data(), velp, scp, S, n, box, o.periodic ? 1 : 0, grid,
-                        user_points ? 1 : omp_get_max_threads(),  // user samples: no split (src/DTFE.cpp:301)
+                        user_points || cone ? 1 : omp_get_max_threads(),  // no split (src/DTFE.cpp:301)
                         (float)o.paddingParticles, (double)o.averageDensity, &plan.p),
         "planning");
   dtfe_plan_view v;
@@ -219,6 +225,15 @@ void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& s
     if (f.velocity_vorticity) q->velocity_vorticity.resize(kept);
     if (f.scalar) q->scalar.resize(kept);
     if (f.scalar_gradient) q->scalar_gradient.resize(kept);
+  } else if (any(o.uField) && cone) {
+    // interpolateRedshiftCone: gridSize bins in (r, theta, psi)
+    float* out[DTFE_NUM_FIELDS];
+    dtfe_interp_opts io = {DTFE_METHOD_CENTRE, 1, 0, 0, 0};
+    outputs(o.uField, uQuantities, G, out, &io.fields);
+    float lim[6], org[3];
+    for (int i = 0; i < 6; ++i) lim[i] = o.redshiftCone.coords[i];
+    for (int i = 0; i < 3; ++i) org[i] = o.originPosition[i];
+    check(dtfe_gpu_interpolate_cone(gpu.h, lim, org, grid, &io, out), "redshift-cone interpolation");
   } else if (any(o.uField)) {
     float* out[DTFE_NUM_FIELDS];
     dtfe_interp_opts io = {DTFE_METHOD_CENTRE, 1, 0, 0, 0};

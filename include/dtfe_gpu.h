@@ -209,6 +209,24 @@ int dtfe_gpu_interpolate_async(dtfe_handle h, const dtfe_interp_opts* opts, floa
  * components (size them for n). */
 int dtfe_gpu_interpolate_points(dtfe_handle h, int64_t n, const float* xyz, const float region[6],
                                 const dtfe_interp_opts* opts, float* const out[DTFE_NUM_FIELDS], int64_t* n_out);
+/* Fields on a redshift-cone grid (interpolateRedshiftCone,
+ * unaveraged_interpolation.cc:381-547; DTFE() runs cones without the sub-box
+ * split, src/DTFE.cpp:301).  cone = (r_min, r_max, theta_min, theta_max,
+ * psi_min, psi_max), distances in the particles' units and angles in degrees
+ * (User_options::redshiftCone); origin = the cone's apex
+ * (User_options::originPosition); dims = bins in r, theta, psi
+ * (User_options::gridSize).  Sample (i, j, k) is the centre of its bin,
+ * (o0 + r sin(theta) cos(psi), o1 + r sin(theta) sin(psi), o2 + r cos(theta))
+ * in the reference's float arithmetic, written to row (i dims[1] + j) dims[2]
+ * + k of out[slot] (host, dims[0] dims[1] dims[2] rows); outside the hull
+ * zeros.  As in the reference, a sample outside the hull leaves psi where it
+ * was, so the rest of its psi row repeats that sample (zeros);
+ * DTFE_FLAG_FIX_OUTSIDE_RASTER advances psi regardless.  Theta limits outside
+ * [0, 180] or a psi range of 360 degrees or more are refused (DTFE_ERR_ARG,
+ * src/user_options.cc:1000-1009).  The handle must hold one sub-box and its
+ * vertex densities; opts->method must be DTFE_METHOD_CENTRE. */
+int dtfe_gpu_interpolate_cone(dtfe_handle h, const float cone[6], const float origin[3], const int32_t dims[3],
+                              const dtfe_interp_opts* opts, float* const out[DTFE_NUM_FIELDS]);
 /* Same as dtfe_gpu_interpolate_dev, but only queues the work on the handle's
  * stream and returns without waiting: consecutive steps (vertex densities,
  * interpolation, ...) then run back to back on the device; the walk counters

@@ -635,6 +635,112 @@ int oracle_interpolate_points(int64_t T, const int32_t* tv, const int32_t* tn, i
   return DTFE_OK;
 }
 
+// Sample coordinates of a redshift-cone grid (interpolateRedshiftCone,
+// unaveraged_interpolation.cc:381-455) in the reference's float arithmetic:
+//   * checkAngles (triangulation_miscellaneous.cc:162-197, 3-D): theta limits
+//     must lie in [0, 180]; psi limits wrapped by a -= floor(a / 360) 360;
+//     psi_max += 360 when psi_min > psi_max; angles times float(PI / 180)
+//     with PI = 3.14159265 (define.h:47);
+//   * user_options.cc:1000-1009: a psi span of 360 degrees or more is refused;
+//   * dx = (hi - lo) / n in float; first value float(lo + dx / 2.) (double
+//     sum), then sequential float adds of dx (:435-447, 505-509);
+//   * per-axis tables: r, sin(theta), cos(theta), cos(psi), sin(psi) through
+//     the float overloads of <cmath> (the reference's `using namespace std`).
+// The point is (o0 + r st cp, o1 + r st sp, o2 + r ct), left to right in float.
+int oracle_cone_tables(const float cone[6], const int32_t dims[3], float* r, float* st, float* ct, float* cp,
+                       float* sp) {
+  float b[6];
+  for (int i = 0; i < 6; ++i) b[i] = cone[i];
+  for (int a = 0; a < 3; ++a)
+    if (dims[a] <= 0) return DTFE_ERR_ARG;
+  if (b[2] < 0.f || b[2] > 180.f || b[3] < 0.f || b[3] > 180.f) return DTFE_ERR_ARG;
+  if (b[5] - b[4] >= 360.f) return DTFE_ERR_ARG;
+  b[4] -= std::floor(b[4] / 360.f) * 360.f;
+  b[5] -= std::floor(b[5] / 360.f) * 360.f;
+  if (b[4] > b[5]) b[5] += 360.f;
+  const float rad = (float)(3.14159265 / 180.);
+  for (int i = 2; i < 6; ++i) b[i] *= rad;
+  float dx[3];
+  for (int a = 0; a < 3; ++a) dx[a] = (b[2 * a + 1] - b[2 * a]) / (float)dims[a];
+  float x = (float)((double)b[0] + (double)dx[0] / 2.);
+  for (int i = 0; i < dims[0]; ++i, x += dx[0]) r[i] = x;
+  x = (float)((double)b[2] + (double)dx[1] / 2.);
+  for (int j = 0; j < dims[1]; ++j, x += dx[1]) {
+    st[j] = std::sin(x);
+    ct[j] = std::cos(x);
+  }
+  x = (float)((double)b[4] + (double)dx[2] / 2.);
+  for (int k = 0; k < dims[2]; ++k, x += dx[2]) {
+    cp[k] = std::cos(x);
+    sp[k] = std::sin(x);
+  }
+  return DTFE_OK;
+}
+
+// Fields on a redshift-cone grid: interpolateRedshiftCone
+// (unaveraged_interpolation.cc:381-547).  Raster r slowest, psi fastest; each
+// sample located from the previous hit (canonical tie rule) in the
+// tetrahedra [lo, hi) and evaluated as a cell centre; outside the hull
+// zeros.  An outside sample skips `psi += dx` (the `continue` at :466 jumps
+// over :527), so the rest of that psi pencil re-locates the same outside
+// point: zeros to its end.  fix_outside advances psi regardless.  Derived
+// fields from the gradient (src/DTFE.cpp:394-475).
+int oracle_interpolate_cone(int64_t T, const int32_t* tv, const int32_t* tn, int64_t V, const float* xyz,
+                            const float* vel, const float* scal, int S, const float* dens32, const double* dens64,
+                            int64_t lo, int64_t hi, const float cone[6], const float origin[3],
+                            const int32_t dims[3], uint32_t fields, int mode, int fix, int fix_outside,
+                            double* const out[DTFE_NUM_FIELDS]) {
+  Tess g{T, V, tv, tn, xyz, vel, scal, S};
+  auto has = [&](int s) { return (fields & DTFE_FIELD_BIT(s)) != 0 && out[s] != nullptr; };
+  if (has(DTFE_VELOCITY_STD)) return DTFE_ERR_ARG;
+  std::vector<float> r(dims[0] > 0 ? dims[0] : 1), st(dims[1] > 0 ? dims[1] : 1), ct(st.size()),
+      cp(dims[2] > 0 ? dims[2] : 1), sp(cp.size());
+  int rc = oracle_cone_tables(cone, dims, r.data(), st.data(), ct.data(), cp.data(), sp.data());
+  if (rc) return rc;
+  const bool want_vel = has(DTFE_VELOCITY) || has(DTFE_VELOCITY_GRADIENT) || has(DTFE_VELOCITY_DIVERGENCE) ||
+                        has(DTFE_VELOCITY_SHEAR) || has(DTFE_VELOCITY_VORTICITY);
+  const bool want_sc = has(DTFE_SCALAR) || has(DTFE_SCALAR_GRADIENT);
+  int64_t m = 0, hint = lo;
+  for (int i = 0; i < dims[0]; ++i)
+    for (int j = 0; j < dims[1]; ++j) {
+      const float rs = r[i] * st[j];
+      const float z = origin[2] + r[i] * ct[j];
+      int kp = 0;  // the psi bin the reference's running `psi` holds
+      for (int k = 0; k < dims[2]; ++k, ++m) {
+        const float q[3] = {origin[0] + rs * cp[kp], origin[1] + rs * sp[kp], z};
+        const double p[3] = {(double)q[0], (double)q[1], (double)q[2]};
+        const int64_t t = hi > lo ? locate(g, p, hint, lo, hi) : -1;
+        if (t == -2) return DTFE_ERR_WALK;
+        CellEval e;
+        std::memset(&e, 0, sizeof(e));
+        if (t >= 0) {
+          hint = t;
+          eval_cell(g, dens32, dens64, t, p, mode, fix != 0, want_vel, want_sc, e);
+        }
+        if (t >= 0 || fix_outside) ++kp;
+        if (has(DTFE_DENSITY)) out[DTFE_DENSITY][m] = e.dens;
+        if (has(DTFE_VELOCITY))
+          for (int c = 0; c < 3; ++c) out[DTFE_VELOCITY][3 * m + c] = e.vel[c];
+        if (has(DTFE_VELOCITY_GRADIENT))
+          for (int c = 0; c < 9; ++c) out[DTFE_VELOCITY_GRADIENT][9 * m + c] = e.grad[c];
+        if (has(DTFE_VELOCITY_DIVERGENCE) || has(DTFE_VELOCITY_SHEAR) || has(DTFE_VELOCITY_VORTICITY)) {
+          double dv, sh[5], vo[3];
+          derived(e.grad, mode, &dv, sh, vo);
+          if (has(DTFE_VELOCITY_DIVERGENCE)) out[DTFE_VELOCITY_DIVERGENCE][m] = dv;
+          if (has(DTFE_VELOCITY_SHEAR))
+            for (int c = 0; c < 5; ++c) out[DTFE_VELOCITY_SHEAR][5 * m + c] = sh[c];
+          if (has(DTFE_VELOCITY_VORTICITY))
+            for (int c = 0; c < 3; ++c) out[DTFE_VELOCITY_VORTICITY][3 * m + c] = vo[c];
+        }
+        if (has(DTFE_SCALAR))
+          for (int c = 0; c < S; ++c) out[DTFE_SCALAR][(int64_t)S * m + c] = e.sc[c];
+        if (has(DTFE_SCALAR_GRADIENT))
+          for (int c = 0; c < 3 * S; ++c) out[DTFE_SCALAR_GRADIENT][(int64_t)3 * S * m + c] = e.scg[c];
+      }
+    }
+  return DTFE_OK;
+}
+
 // Averaging method 1: interpolateGrid_averaged_1
 // (src/CGAL_triangulation/averaged_interpolation_1.cc:197-421), per sub-box
 // over its tetrahedra in order.

@@ -53,6 +53,10 @@ def lib() -> C.CDLL:
         L.oracle_interpolate_points.argtypes = [C.c_int64, vp, vp, C.c_int64, vp, vp, vp, C.c_int, vp, vp,
                                                 C.c_int64, C.c_int64, C.c_int64, vp, vp, C.c_uint32, C.c_int,
                                                 C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]
+        L.oracle_cone_tables.argtypes = [vp, vp, vp, vp, vp, vp, vp]
+        L.oracle_interpolate_cone.argtypes = [C.c_int64, vp, vp, C.c_int64, vp, vp, vp, C.c_int, vp, vp,
+                                              C.c_int64, C.c_int64, vp, vp, vp, C.c_uint32, C.c_int, C.c_int,
+                                              C.c_int, C.POINTER(C.c_void_p)]
         L.oracle_sobol_simplex.argtypes = [C.c_int64, vp]
         L.oracle_sobol_simplex.restype = None
         _lib = L
@@ -265,6 +269,54 @@ def interpolate_points(plan, dens32, dens64, fields, pts, region, mode: int = MO
     if rc:
         raise RuntimeError(f"oracle_interpolate_points failed with status {rc}")
     return {f: a[:n_out.value] for f, a in arrs.items()}
+
+
+def cone_tables(cone, dims):
+    """Per-axis tables of a redshift-cone grid: r, sin(theta), cos(theta),
+    cos(psi), sin(psi) as float32 arrays, in the reference's arithmetic."""
+    c = np.ascontiguousarray(cone, np.float32)
+    d = np.ascontiguousarray(dims, np.int32)
+    r = np.zeros(max(int(d[0]), 1), np.float32)
+    st, ct = np.zeros(max(int(d[1]), 1), np.float32), np.zeros(max(int(d[1]), 1), np.float32)
+    cp, sp = np.zeros(max(int(d[2]), 1), np.float32), np.zeros(max(int(d[2]), 1), np.float32)
+    rc = lib().oracle_cone_tables(c.ctypes.data, d.ctypes.data, r.ctypes.data, st.ctypes.data, ct.ctypes.data,
+                                  cp.ctypes.data, sp.ctypes.data)
+    if rc:
+        raise ValueError(f"oracle_cone_tables refused the cone {list(cone)} (status {rc})")
+    return r, st, ct, cp, sp
+
+
+def interpolate_cone(plan, dens32, dens64, fields, cone, origin, dims, mode: int = MODE_REF, fix: bool = False,
+                     fix_outside: bool = False, box: int = 0):
+    """Fields on a redshift-cone grid (interpolateRedshiftCone) in the
+    tessellation of sub-box `box`: dict field -> float64 array of
+    dims[0] * dims[1] * dims[2] rows, r slowest and psi fastest."""
+    n = int(np.prod(dims))
+    S = plan.n_scalars
+    mask = 0
+    outs = [None] * N.NUM_FIELDS
+    arrs = {}
+    for f in fields:
+        s = N.FIELD_SLOTS[f]
+        mask |= 1 << s
+        nc = N.field_components(s, S)
+        a = np.zeros((n, nc) if nc > 1 else n, np.float64)
+        arrs[f] = a
+        outs[s] = a.ctypes.data
+    optr = (C.c_void_p * N.NUM_FIELDS)(*[o if o else None for o in outs])
+    vel = plan.velocity.ctypes.data if plan.velocity is not None else None
+    sc = plan.scalar.ctypes.data if plan.scalar is not None else None
+    b = plan.boxes[box]
+    c = np.ascontiguousarray(cone, np.float32)
+    o = np.ascontiguousarray(origin, np.float32)
+    d = np.ascontiguousarray(dims, np.int32)
+    rc = lib().oracle_interpolate_cone(plan.n_tets, plan.tet_v.ctypes.data, plan.tet_n.ctypes.data, plan.n_verts,
+                                       plan.xyz.ctypes.data, vel, sc, S, dens32.ctypes.data, dens64.ctypes.data,
+                                       b.tet_offset, b.tet_offset + b.n_tets, c.ctypes.data, o.ctypes.data,
+                                       d.ctypes.data, mask, mode, 1 if fix else 0, 1 if fix_outside else 0, optr)
+    if rc:
+        raise RuntimeError(f"oracle_interpolate_cone failed with status {rc}")
+    return arrs
 
 
 def sobol_simplex(n: int) -> np.ndarray:

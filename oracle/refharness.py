@@ -100,6 +100,36 @@ def run_points(plan, pts, region, dens, box: int = 0):
     return {k: a[:m.value] for k, a in out.items()}
 
 
+def run_cone(plan, cone, origin, dims, dens, box: int = 0):
+    """The reference's interpolateRedshiftCone on sub-box `box`'s
+    tessellation with vertex densities `dens`: density, velocity, gradient,
+    scalar, scalar gradient of the dims[0] * dims[1] * dims[2] cone samples."""
+    xyz, w, vel, tv, tn, _, _ = _box_args(plan, box)
+    b = plan.boxes[box]
+    v0, nv = b.vert_offset, b.n_verts
+    sc = None if plan.scalar is None else np.ascontiguousarray(plan.scalar[v0:v0 + nv, 0])
+    d = np.ascontiguousarray(dens[v0:v0 + nv], np.float32)
+    n = int(np.prod(dims))
+    out = {"density": np.zeros(n, np.float32), "velocity": np.zeros((n, 3), np.float32),
+           "velocity_gradient": np.zeros((n, 9), np.float32), "scalar": np.zeros(n, np.float32),
+           "scalar_gradient": np.zeros((n, 3), np.float32)}
+    c = np.ascontiguousarray(cone, np.float32)
+    o = np.ascontiguousarray(origin, np.float32)
+    dd = np.ascontiguousarray(dims, np.int32)
+    L = lib()
+    vp = C.c_void_p
+    L.ref_interpolate_cone.argtypes = [C.c_int64, vp, vp, vp, vp, C.c_int64, vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                                       vp, vp]
+    p = lambda a: None if a is None else a.ctypes.data
+    rc = L.ref_interpolate_cone(len(xyz), p(xyz), p(w), p(vel), p(sc), len(tv), p(tv), p(tn), p(c), p(o), p(dd),
+                                p(d), p(out["density"]), p(out["velocity"]), p(out["velocity_gradient"]),
+                                p(out["scalar"]) if sc is not None else None,
+                                p(out["scalar_gradient"]) if sc is not None else None)
+    if rc:
+        raise RuntimeError(f"ref_interpolate_cone failed ({rc})")
+    return out
+
+
 def _box_args(plan, box):
     b = plan.boxes[box]
     v0, nv, t0, nt = b.vert_offset, b.n_verts, b.tet_offset, b.n_tets

@@ -146,4 +146,40 @@ int dropin_run_points(const float* pos, const float* w, const float* vel, const 
   return 0;
 }
 
+// DTFE() on a redshift-cone grid: cone = (r_min, r_max, theta_min,
+// theta_max, psi_min, psi_max), origin = the apex, grid = bins in r, theta,
+// psi; u_out receive grid[0] grid[1] grid[2] rows.
+int dropin_run_cone(const float* pos, const float* w, const float* vel, const float* scal, int64_t n,
+                    const float box[6], int periodic, const int32_t grid[3], double average_density,
+                    uint32_t u_fields, const float cone[6], const float origin[3], int n_threads,
+                    float* const* u_out) {
+  std::vector<Particle_data> p(n);
+  for (int64_t i = 0; i < n; ++i) {
+    for (int c = 0; c < 3; ++c) p[i].pos[c] = pos[3 * i + c];
+    p[i].weight() = w ? w[i] : 1.f;
+    for (int c = 0; c < 3; ++c) p[i].velocity(c) = vel ? vel[3 * i + c] : 0.f;
+    p[i].scalar(0) = scal ? scal[i] : 0.f;
+  }
+  User_options o;
+  o.gridSize.assign(grid, grid + 3);
+  o.boxCoordinates.coords.assign(box, box + 6);
+  o.periodic = periodic != 0;
+  o.averageDensity = (Real)average_density;
+  o.redshiftConeOn = true;
+  o.redshiftCone.coords.assign(cone, cone + 6);
+  o.originPosition.assign(origin, origin + 3);
+  set_fields(o.uField, u_fields);
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+  std::vector<Sample_point> samples;
+  Quantities uq, aq;
+  try {
+    DTFE(&p, samples, o, &uq, &aq);
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return 1;
+  }
+  copy_all(uq, u_out, (size_t)grid[0] * grid[1] * grid[2]);
+  return 0;
+}
+
 }  // extern "C"

@@ -11,6 +11,7 @@
 //   interpolateGrid_averaged_2  averaged_interpolation_2.cc:35-233
 //   interpolateGrid_averaged_3  averaged_interpolation_2.cc:664-866
 //   interpolateUserSampling     unaveraged_interpolation.cc:560-691
+//   interpolateRedshiftCone     unaveraged_interpolation.cc:381-547
 //   interpolateGrid_averaged_1  averaged_interpolation_1.cc:197-421 (Sobol points
 //                               from dtfe_b200/csrc/sobol.h behind the GSL API)
 //
@@ -42,6 +43,7 @@ void interpolateGrid_averaged_3(DT& dt, User_options& userOptions, Quantities* q
 void interpolateGrid_averaged_1(DT& dt, User_options& userOptions, Quantities* quantities);
 void interpolateUserSampling(DT& dt, std::vector<Sample_point>& samples, User_options& userOptions,
                              Quantities* quantities);
+void interpolateRedshiftCone(DT& dt, User_options& userOptions, Quantities* quantities);
 
 User_options::User_options() {
   periodic = false;
@@ -217,6 +219,48 @@ int ref_interpolate_points(int64_t nv, const float* xyz, const float* w, const f
   interpolateUserSampling(dt, samples, opt, &q);
   const size_t m = f.density ? q.density.size() : (f.velocity ? q.velocity.size() : q.velocity_gradient.size());
   *n_out = (int64_t)m;
+  if (out_density && q.density.size() == m) std::memcpy(out_density, q.density.data(), m * sizeof(float));
+  if (out_velocity && q.velocity.size() == m) std::memcpy(out_velocity, q.velocity.data(), 3 * m * sizeof(float));
+  if (out_gradient && q.velocity_gradient.size() == m)
+    std::memcpy(out_gradient, q.velocity_gradient.data(), 9 * m * sizeof(float));
+  if (out_scalar && q.scalar.size() == m) std::memcpy(out_scalar, q.scalar.data(), m * sizeof(float));
+  if (out_scalar_gradient && q.scalar_gradient.size() == m)
+    std::memcpy(out_scalar_gradient, q.scalar_gradient.data(), 3 * m * sizeof(float));
+  return 0;
+}
+
+// interpolateRedshiftCone on one tessellation (LOCAL indices) with the given
+// vertex densities: cone = (r_min, r_max, theta_min, theta_max, psi_min,
+// psi_max) in Mpc and degrees, dims = (n_r, n_theta, n_psi).  Outputs hold
+// dims[0] dims[1] dims[2] rows (NULL to skip a field).
+int ref_interpolate_cone(int64_t nv, const float* xyz, const float* w, const float* vel, const float* scal,
+                         int64_t nt, const int32_t* tv, const int32_t* tn, const float cone[6],
+                         const float origin[3], const int32_t dims[3], const float* dens, float* out_density,
+                         float* out_velocity, float* out_gradient, float* out_scalar, float* out_scalar_gradient) {
+  DT dt;
+  const std::vector<DT::Vertex*>& verts = dt.load_flat(nv, xyz, nt, tv, tn);
+  for (int64_t i = 0; i < nv; ++i) {
+    vertexData& d = verts[i]->info();
+    d.weight() = w[i];
+    for (int c = 0; c < 3; ++c) d.velocity(c) = vel ? vel[3 * i + c] : 0.f;
+    d.scalar(0) = scal ? scal[i] : 0.f;
+    d.setDensity(dens[i]);
+  }
+  User_options opt;
+  opt.redshiftConeOn = true;
+  opt.redshiftCone.coords.assign(cone, cone + 6);
+  opt.originPosition.assign(origin, origin + 3);
+  opt.gridSize.assign({(size_t)dims[0], (size_t)dims[1], (size_t)dims[2]});
+  Quantities q;
+  Field f;
+  f.density = out_density != nullptr;
+  f.velocity = out_velocity != nullptr;
+  f.velocity_gradient = out_gradient != nullptr;
+  f.scalar = out_scalar != nullptr;
+  f.scalar_gradient = out_scalar_gradient != nullptr;
+  opt.uField = f;
+  interpolateRedshiftCone(dt, opt, &q);
+  const size_t m = (size_t)dims[0] * dims[1] * dims[2];
   if (out_density && q.density.size() == m) std::memcpy(out_density, q.density.data(), m * sizeof(float));
   if (out_velocity && q.velocity.size() == m) std::memcpy(out_velocity, q.velocity.data(), 3 * m * sizeof(float));
   if (out_gradient && q.velocity_gradient.size() == m)

@@ -29,6 +29,8 @@ def lib():
                                  C.POINTER(C.c_double), C.POINTER(C.c_int64)]
         L.dropin_run_points.argtypes = [vp, vp, vp, vp, C.c_int64, vp, C.c_int, vp, C.c_double, C.c_uint32,
                                         C.c_int64, vp, C.c_int, vp, C.POINTER(C.c_int64)]
+        L.dropin_run_cone.argtypes = [vp, vp, vp, vp, C.c_int64, vp, C.c_int, vp, C.c_double, C.c_uint32, vp, vp,
+                                      C.c_int, vp]
         L.dropin_error.restype = C.c_char_p
         _lib = L
     return _lib
@@ -85,3 +87,25 @@ def run_points(pos, w, vel, scal, grid, samples, box=(0, 100, 0, 100, 0, 100), p
     if rc:
         raise RuntimeError(lib().dropin_error().decode())
     return {f: a[:kept.value] for f, a in d.items()}
+
+
+def run_cone(pos, w, vel, scal, grid, cone, origin, box=(0, 100, 0, 100, 0, 100), periodic=True,
+             average_density=-1.0, u_fields=("density",), n_threads=4):
+    """DTFE() on a redshift-cone grid: dict field -> grid[0] grid[1] grid[2]
+    rows, r slowest and psi fastest."""
+    pos = np.ascontiguousarray(pos, np.float32)
+    G = int(np.prod(grid))
+    d = {f: np.full((G, NCOMP[SLOTS[f]]), np.nan, np.float32) for f in u_fields}
+    ptrs = (C.c_void_p * 9)(*[d[f].ctypes.data if f in d else None for f in SLOTS])
+    mask = sum(1 << SLOTS[f] for f in u_fields)
+    g = np.ascontiguousarray(grid, np.int32)
+    bx = np.ascontiguousarray(box, np.float32)
+    c = np.ascontiguousarray(cone, np.float32)
+    o = np.ascontiguousarray(origin, np.float32)
+    keep = [np.ascontiguousarray(a, np.float32) if a is not None else None for a in (w, vel, scal)]
+    rc = lib().dropin_run_cone(pos.ctypes.data, *[a.ctypes.data if a is not None else None for a in keep],
+                               len(pos), bx.ctypes.data, int(periodic), g.ctypes.data, float(average_density),
+                               mask, c.ctypes.data, o.ctypes.data, n_threads, ptrs)
+    if rc:
+        raise RuntimeError(lib().dropin_error().decode())
+    return d

@@ -1,0 +1,75 @@
+"""Fields on a redshift-cone grid on the GPU (dtfe_gpu_interpolate_cone),
+bit-identical to the oracle's float mode (itself bit-identical to the
+reference's interpolateRedshiftCone, tests/test_reference_live.py): shells
+leaving the padded hull (zeros), the reference's stuck psi after an outside
+sample and its fix, a psi range wrapping through 360 degrees, seeds from the
+grid bins and from the sub-box's first tetrahedron."""
+import numpy as np
+import pytest
+
+import oracle as O
+from dtfe_b200 import _native as N
+from dtfe_b200 import plan as P
+from dtfe_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+FIELDS = ["density", "velocity", "velocity_gradient", "velocity_divergence", "velocity_shear",
+          "velocity_vorticity", "scalar", "scalar_gradient"]
+CONES = [((1.0, 120.0, 10.0, 170.0, 300.0, 60.0), (50.0, 50.0, 50.0), (9, 7, 45)),
+         ((0.5, 60.0, 0.0, 180.0, 0.0, 359.0), (20.0, 70.0, 40.0), (6, 5, 13)),
+         ((30.0, 31.0, 90.0, 90.0, 10.0, 10.0), (50.0, 50.0, 50.0), (1, 1, 1))]
+
+
+def _plan(seed):
+    pos, psi = S.zeldovich_lattice(12, 100.0, 0.9, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    w = rng.uniform(0.5, 1.5, len(pos)).astype(np.float32)
+    vel = (60 * psi).astype(np.float32)
+    sc = rng.standard_normal((len(pos), 1)).astype(np.float32)
+    return P.make_plan(pos, w, vel, sc, grid=(12, 12, 12), n_threads=1, average_density_value=float(w.sum()) / 1e6)
+
+
+def test_cone_vs_oracle(gpu_built):
+    from dtfe_b200.device import DeviceDTFE
+    plan = _plan(53)
+    d32, d64, _ = O.vertex_density(plan)
+    with DeviceDTFE(0, 1) as d:
+        d.load(plan)
+        for cone, origin, dims in CONES:
+            for fix, fix_outside in ((False, False), (True, False), (False, True)):
+                want = O.interpolate_cone(plan, d32, d64, FIELDS, cone, origin, dims, mode=O.MODE_REF, fix=fix,
+                                          fix_outside=fix_outside)
+                for loc in (11, 3, 0):        # fused (seeded), walk (seeded), raster (no seeds)
+                    d.set_variants(loc, 2)
+                    d.vertex_density(plan.rho_bar)
+                    got = d.interpolate_cone(FIELDS, cone, origin, dims, fix=fix, fix_outside=fix_outside)
+                    for f in FIELDS:
+                        assert got[f].shape[0] == int(np.prod(dims))
+                        assert np.array_equal(got[f], want[f].astype(np.float32)), (cone, fix, fix_outside, loc, f)
+    # the first cone leaves the hull and its stuck psi zeroes inside samples
+    cone, origin, dims = CONES[0]
+    a = O.interpolate_cone(plan, d32, d64, ["density"], cone, origin, dims, mode=O.MODE_REF)["density"]
+    b = O.interpolate_cone(plan, d32, d64, ["density"], cone, origin, dims, mode=O.MODE_REF,
+                           fix_outside=True)["density"]
+    assert (a == 0).any() and (a != 0).any() and ((a == 0) & (b != 0)).any()
+
+
+def test_cone_errors(gpu_built):
+    from dtfe_b200.device import DeviceDTFE
+    plan = _plan(55)
+    with DeviceDTFE(0) as d:
+        d.load(plan)
+        d.vertex_density(plan.rho_bar)
+        with pytest.raises(N.DTFEError, match="theta"):
+            d.interpolate_cone(["density"], (1, 10, -5, 90, 0, 90), (50, 50, 50), (2, 2, 2))
+        with pytest.raises(N.DTFEError, match="360"):
+            d.interpolate_cone(["density"], (1, 10, 0, 90, 0, 360), (50, 50, 50), (2, 2, 2))
+        with pytest.raises(N.DTFEError, match="bins"):
+            d.interpolate_cone(["density"], (1, 10, 0, 90, 0, 90), (50, 50, 50), (2, 0, 2))
+    pos, _ = S.zeldovich_lattice(8, 100.0, 0.5, seed=3)
+    split = P.make_plan(pos, np.ones(len(pos), np.float32), None, None, grid=(8, 8, 8), n_threads=2)
+    with DeviceDTFE(0) as d:
+        d.load(split)
+        d.vertex_density(split.rho_bar)
+        with pytest.raises(N.DTFEError, match="one sub-box"):
+            d.interpolate_cone(["density"], (1, 10, 0, 90, 0, 90), (50, 50, 50), (2, 2, 2))

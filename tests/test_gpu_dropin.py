@@ -125,3 +125,21 @@ def test_dropin_user_sampling(particles):
     for f in fields:
         assert len(u[f]) == len(ref[f]) < len(samples)
         assert np.array_equal(u[f].reshape(ref[f].shape), ref[f]), f
+
+
+def test_dropin_redshift_cone(particles):
+    """DTFE() on a redshift-cone grid (redshiftConeOn): the gridSize bins in
+    (r, theta, psi), equal to the oracle's interpolateRedshiftCone on the
+    reference's single-box plan, bit for bit, shells beyond the padded hull
+    included."""
+    import oracle as O
+    pos, w, vel, sc = particles
+    fields = ["density", "velocity", "velocity_gradient", "velocity_divergence", "scalar"]
+    cone, origin = (2.0, 110.0, 5.0, 175.0, 200.0, 100.0), (50.0, 40.0, 60.0)
+    u = D.run_cone(pos, w, vel, sc, GRID, cone, origin, u_fields=fields)
+    plan = P.make_plan(pos, w, vel, sc[:, None], grid=GRID, n_threads=1)
+    d32, d64, _ = O.vertex_density(plan)
+    ref = O.interpolate_cone(plan, d32, d64, fields, cone, origin, GRID, mode=O.MODE_REF)
+    for f in fields:
+        assert np.array_equal(u[f].reshape(ref[f].shape), ref[f].astype(np.float32)), f
+    assert (ref["density"] == 0).any() and (ref["density"] != 0).any()

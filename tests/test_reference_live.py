@@ -173,3 +173,32 @@ def test_live_user_sampling(built):
     for f in fields:
         assert np.array_equal(ora[f].astype(np.float32), ref[f]), f
     assert (ora["density"] == 0).any() and (ora["density"] != 0).any()
+
+
+def test_live_redshift_cone(built):
+    """Fields on a redshift-cone grid: the reference's interpolateRedshiftCone
+    (one box, as DTFE() runs cones) against the oracle's float mode, bit for
+    bit, on a cone whose outer shells leave the padded hull (zeros, and the
+    reference's stuck psi: the rest of such a psi pencil stays zero) and whose
+    psi range wraps through 360 degrees."""
+    pos, psi = S.zeldovich_lattice(12, 100.0, 0.9, seed=53)
+    rng = np.random.default_rng(54)
+    w = rng.uniform(0.5, 1.5, len(pos)).astype(np.float32)
+    vel = (60 * psi).astype(np.float32)
+    sc = rng.standard_normal((len(pos), 1)).astype(np.float32)
+    plan = P.make_plan(pos, w, vel, sc, grid=(12, 12, 12), n_threads=1, average_density_value=float(w.sum()) / 1e6)
+    d32, d64, _ = O.vertex_density(plan)
+    fields = ["density", "velocity", "velocity_gradient", "scalar", "scalar_gradient"]
+    for cone, origin, dims in [((1.0, 120.0, 10.0, 170.0, 300.0, 60.0), (50.0, 50.0, 50.0), (9, 7, 11)),
+                               ((0.5, 60.0, 0.0, 180.0, 0.0, 359.0), (20.0, 70.0, 40.0), (6, 5, 13))]:
+        ora = O.interpolate_cone(plan, d32, d64, fields, cone, origin, dims, mode=O.MODE_REF)
+        ref = R.run_cone(plan, cone, origin, dims, d32)
+        for f in fields:
+            assert np.array_equal(ora[f].astype(np.float32), ref[f]), (cone, f)
+    # the first cone reaches outside the hull, and the stuck psi zeroes samples
+    # that would have been inside
+    cone, origin, dims = (1.0, 120.0, 10.0, 170.0, 300.0, 60.0), (50.0, 50.0, 50.0), (9, 7, 11)
+    ora = O.interpolate_cone(plan, d32, d64, ["density"], cone, origin, dims, mode=O.MODE_REF)
+    fixed = O.interpolate_cone(plan, d32, d64, ["density"], cone, origin, dims, mode=O.MODE_REF, fix_outside=True)
+    assert (ora["density"] == 0).any() and (ora["density"] != 0).any()
+    assert ((ora["density"] == 0) & (fixed["density"] != 0)).any()

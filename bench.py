@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-compare", action="store_true")
     ap.add_argument("--batch-steps", type=int, default=10)
+    ap.add_argument("--sampling-n", type=int, default=128,
+                    help="particles per side of the redshift-cone / user-point workload (one box)")
+    ap.add_argument("--no-sampling", action="store_true")
     return ap.parse_args()
 
 
@@ -535,6 +538,102 @@ def batch_leg(args, local: int, threads: int) -> dict:
                     "per sub-box costs); graph and plain by CUDA events on the handle's stream"}
 
 
+def sampling_leg(args, local: int, threads: int, cpu: bool) -> dict:
+    """Redshift-cone bins and user sampling points (interpolateRedshiftCone,
+    interpolateUserSampling).  DTFE() runs both on one tessellation of the
+    whole padded box (no sub-box split, src/DTFE.cpp:301), so this leg builds
+    a single-box plan: n^3 Zel'dovich particles (n = --sampling-n, rms 1.0
+    spacing, velocities as the main workload, periodic 100 Mpc/h, padding 5).
+    Cone: apex at the box centre, r in [1, 86.6] (the box corner), theta
+    [0, 180], psi [0, 359], n^3 bins.  Points: n^3 uniform points in the box.
+    Density, velocity and velocity gradient.  GPU: the cone into device
+    outputs (dtfe_gpu_interpolate_cone_dev) and, end to end with host
+    buffers, the cone and the points (dtfe_gpu_interpolate_cone /
+    _points); CUDA events on the handle's stream.  Reference: the harness's
+    interpolateRedshiftCone on every 8th r bin's worth (n/8 bins over the same
+    r range) and interpolateUserSampling on the first n^3/8 points, one host
+    thread as DTFE() runs them, given the GPU's vertex densities; the GPU
+    runs the same reduced cone and points and must match them bit for bit."""
+    import torch
+    from dtfe_b200 import plan as P
+    from dtfe_b200 import synthetic as S
+    from dtfe_b200.device import DeviceDTFE
+    n = args.sampling_n
+    fields = ["density", "velocity", "velocity_gradient"]
+    pos, psi = S.zeldovich_lattice(n, S.BOX, 1.0, seed=21)
+    rng = np.random.default_rng(22)
+    vel = (100.0 * psi / (S.BOX / n) + rng.normal(0.0, 50.0, psi.shape)).astype(np.float32)
+    del psi
+    w = np.ones(len(pos), np.float32)
+    t0 = time.time()
+    plan = P.make_plan(pos, w, vel, None, grid=(n, n, n), n_threads=1,
+                       average_density_value=float(len(pos)) / S.BOX ** 3)
+    t_plan = time.time() - t0
+    half = S.BOX / 2
+    cone = (1.0, float(np.sqrt(3.0) * half), 0.0, 180.0, 0.0, 359.0)
+    origin = (half, half, half)
+    dims = (n, n, n)
+    G = n ** 3
+    pts = rng.uniform(0.0, S.BOX, (G, 3)).astype(np.float32)
+    region = [0.0, S.BOX, 0.0, S.BOX, 0.0, S.BOX]
+    cuda = f"cuda:{local}"
+    outs = {f: torch.empty((G, [1, 3, 9][i]), dtype=torch.float32, device=cuda) for i, f in enumerate(fields)}
+    res = {"workload": f"zeldovich{n} single box: {n}^3 particles, {plan.n_verts} vertices, {plan.n_tets} "
+                       f"tetrahedra; cone r [1, 86.6] theta [0, 180] psi [0, 359] from the box centre, "
+                       f"{n}^3 bins; {G} uniform user points",
+           "fields": fields, "plan_s": t_plan}
+    with DeviceDTFE(local, 0) as dev:
+        dev.load(plan)
+        dev.vertex_density(plan.rho_bar)
+        stream = torch.cuda.ExternalStream(dev.stream, device=cuda)
+
+        def timed(fn, k=5):
+            for _ in range(2):
+                fn()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(k):
+                fn()
+            e1.record(stream)
+            e1.synchronize()
+            return e0.elapsed_time(e1) / 1e3 / k
+
+        t_dev = timed(lambda: dev.interpolate_cone_dev(fields, cone, origin, dims, outs))
+        t_cone = timed(lambda: dev.interpolate_cone(fields, cone, origin, dims), 3)
+        t_pts = timed(lambda: dev.interpolate_points(fields, pts, region), 3)
+        res["cone"] = {"samples_per_s": G / t_dev, "ms": 1e3 * t_dev, "gpu_launches_per_call": 2,
+                       "e2e_samples_per_s": G / t_cone, "e2e_ms": 1e3 * t_cone,
+                       "d2h_bytes": 4 * 13 * G}
+        res["points"] = {"e2e_points_per_s": G / t_pts, "e2e_ms": 1e3 * t_pts, "h2d_bytes": 12 * G,
+                         "d2h_bytes": 4 * 13 * G}
+        if cpu:
+            try:
+                import refharness as R
+                have = R.available()
+            except ImportError:
+                have = False
+            if have:
+                dens = dev.download_vertex_density(plan.n_verts)
+                rdims = (max(1, n // 8), n, n)
+                ref_c, sec_c = R.run_cone(plan, cone, origin, rdims, dens, timing=True)
+                m = G // 8
+                ref_p, sec_p = R.run_points(plan, pts[:m], region, dens, timing=True)
+                got_c = dev.interpolate_cone(fields, cone, origin, rdims)
+                got_p = dev.interpolate_points(fields, pts[:m], region)
+                same = all(np.array_equal(got_c[f].reshape(ref_c[f].shape), ref_c[f]) and
+                           np.array_equal(got_p[f].reshape(ref_p[f].shape), ref_p[f]) for f in fields)
+                nc = int(np.prod(rdims))
+                res["reference"] = {
+                    "kind": "reference", "cores": 1,
+                    "cone_samples_per_s": nc / sec_c, "points_per_s": m / sec_p,
+                    "sample": f"cone with {rdims[0]} r bins over the same range ({nc} bins), the first {m} "
+                              "points; the reference's own functions on one host thread",
+                    "bit_exact_vs_gpu": bool(same)}
+    return res
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -841,6 +940,10 @@ def run_ours(args):
     if side and not args.no_bwd:
         bwd = backward_leg(args, local, threads)
 
+    sampling = None
+    if side and not args.no_sampling:
+        sampling = sampling_leg(args, local, threads, rank == 0 and not args.no_cpu)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(plan, host_threads(args.threads), args.cpu_seconds)
@@ -865,6 +968,7 @@ def run_ours(args):
         "mc": mc, "method1": m1,
         "backward": bwd,
         "batched_subboxes": batch,
+        "sampling": sampling,
         "comparison_estimators": compare,
         "walk": {k: status[k] for k in ("n_samples_located", "n_walk_steps", "n_exact_tests", "n_ties",
                                         "n_outside")} if status else None,

@@ -168,6 +168,7 @@ def gpu() -> C.CDLL:
         lib.dtfe_gpu_interpolate_points.argtypes = [H, C.c_int64, vp, vp, C.POINTER(InterpOpts), C.POINTER(vp),
                                                     C.POINTER(C.c_int64)]
         lib.dtfe_gpu_interpolate_cone.argtypes = [H, vp, vp, vp, C.POINTER(InterpOpts), C.POINTER(vp)]
+        lib.dtfe_gpu_interpolate_cone_dev.argtypes = [H, vp, vp, vp, C.POINTER(InterpOpts), C.POINTER(vp)]
         lib.dtfe_gpu_download_vertex_density.argtypes = [H, vp]
         lib.dtfe_gpu_locate_points.argtypes = [H, C.c_int64, vp, C.c_int32, vp]
         lib.dtfe_gpu_stream.argtypes = [H]

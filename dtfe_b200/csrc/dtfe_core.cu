@@ -995,9 +995,10 @@ struct ConeGrid {
 };
 
 // tet_out (may be null): the located tetrahedron of each row, kOutside when
-// outside the hull.
+// outside the hull.  Four blocks per SM (64 registers), as the fused
+// cell-centre kernel's default: the walks are latency-bound.
 template <int S, class Src>
-__global__ void __launch_bounds__(256) k_points_eval(InterpParams P, int64_t n, Src src, int use_bins,
+__global__ void __launch_bounds__(256, 4) k_points_eval(InterpParams P, int64_t n, Src src, int use_bins,
                                                      int* __restrict__ tet_out) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   float pf[3];
@@ -2423,26 +2424,26 @@ int dtfe_gpu_interpolate_points(dtfe_handle h, int64_t n, const float* xyz, cons
   return read_status(h, nullptr);
 }
 
-int dtfe_gpu_interpolate_cone(dtfe_handle h, const float cone[6], const float origin[3], const int32_t dims[3],
-                              const dtfe_interp_opts* o, float* const out[DTFE_NUM_FIELDS]) {
-  if (!h || !o || !cone || !origin || !dims || !out) return set_error(DTFE_ERR_ARG, "null argument");
-  int rc = check_point_call(h, o, out, "redshift-cone grids");
-  if (rc) return rc;
+}  // extern "C"
+
+namespace {
+
+// Queues a redshift-cone interpolation into the device rows outp[slot]
+// (dims[0] dims[1] dims[2] rows each); P receives the launch parameters.
+int cone_enqueue(dtfe_handle h, const float cone[6], const float origin[3], const int32_t dims[3],
+                 const dtfe_interp_opts* o, float* const outp[DTFE_NUM_FIELDS], InterpParams& P) {
   std::vector<float> tab;
-  if ((rc = cone_tables(cone, dims, tab))) return rc;
+  int rc = cone_tables(cone, dims, tab);
+  if (rc) return rc;
   const int64_t n = (int64_t)dims[0] * dims[1] * dims[2];
-  DTFE_CUDA_TRY(cudaSetDevice(h->device));
   if ((rc = prepare_centres(h))) return rc;
   cudaStream_t st = h->stream;
-  const uint32_t F = o->fields;
-  const size_t comps = point_components(h, F);
   // pts_buf holds the cone's tables, pts_keep the located tetrahedra
-  if ((rc = dev_alloc(h, &h->pts_buf, tab.size())) || (rc = dev_alloc(h, &h->pts_keep, (size_t)n)) ||
-      (rc = dev_alloc(h, &h->pts_out, std::max<size_t>(comps, 1) * (size_t)n)))
-    return rc;
+  if ((rc = dev_alloc(h, &h->pts_buf, tab.size())) || (rc = dev_alloc(h, &h->pts_keep, (size_t)n))) return rc;
   DTFE_CUDA_TRY(cudaMemcpyAsync(h->pts_buf, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice, st));
   DTFE_CUDA_TRY(cudaMemsetAsync(h->counters, 0, sizeof(unsigned long long) * CNT_N, st));
-  const InterpParams P = point_params(h, o, n);
+  P = point_params(h, o, n);
+  for (int q = 0; q < DTFE_NUM_FIELDS; ++q) P.out[q] = (o->fields >> q & 1u) ? outp[q] : nullptr;
   ConeGrid src;
   src.r = h->pts_buf;
   src.st = src.r + dims[0];
@@ -2461,8 +2462,46 @@ int dtfe_gpu_interpolate_cone(dtfe_handle h, const float cone[6], const float or
     k_cone_rows<<<(unsigned)std::min<int64_t>(want, 148 * 16), 256, 0, st>>>(P, h->pts_keep, rows, dims[2]);
     DTFE_CUDA_TRY(cudaGetLastError());
   }
-  if ((rc = copy_point_rows(h, P, F, n, out))) return rc;
   h->tet_c_valid = false;
+  return DTFE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dtfe_gpu_interpolate_cone(dtfe_handle h, const float cone[6], const float origin[3], const int32_t dims[3],
+                              const dtfe_interp_opts* o, float* const out[DTFE_NUM_FIELDS]) {
+  if (!h || !o || !cone || !origin || !dims || !out) return set_error(DTFE_ERR_ARG, "null argument");
+  int rc = check_point_call(h, o, out, "redshift-cone grids");
+  if (rc) return rc;
+  for (int a = 0; a < 3; ++a)
+    if (dims[a] <= 0) return set_error(DTFE_ERR_ARG, "redshift-cone bins must be positive");
+  const int64_t n = (int64_t)dims[0] * dims[1] * dims[2];
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  const size_t comps = point_components(h, o->fields);
+  if ((rc = dev_alloc(h, &h->pts_out, std::max<size_t>(comps, 1) * (size_t)n))) return rc;
+  float* stage[DTFE_NUM_FIELDS] = {};
+  size_t at = 0;
+  for (int q = 0; q < DTFE_NUM_FIELDS; ++q) {
+    if (!(o->fields >> q & 1u)) continue;
+    stage[q] = h->pts_out + at * (size_t)n;
+    at += (size_t)field_components(q, h->S);
+  }
+  InterpParams P;
+  if ((rc = cone_enqueue(h, cone, origin, dims, o, stage, P))) return rc;
+  if ((rc = copy_point_rows(h, P, o->fields, n, out))) return rc;
+  return read_status(h, nullptr);
+}
+
+int dtfe_gpu_interpolate_cone_dev(dtfe_handle h, const float cone[6], const float origin[3], const int32_t dims[3],
+                                  const dtfe_interp_opts* o, float* const out_dev[DTFE_NUM_FIELDS]) {
+  if (!h || !o || !cone || !origin || !dims || !out_dev) return set_error(DTFE_ERR_ARG, "null argument");
+  int rc = check_point_call(h, o, out_dev, "redshift-cone grids");
+  if (rc) return rc;
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  InterpParams P;
+  if ((rc = cone_enqueue(h, cone, origin, dims, o, out_dev, P))) return rc;
   return read_status(h, nullptr);
 }
 

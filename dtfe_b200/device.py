@@ -184,6 +184,21 @@ class DeviceDTFE:
                                                    optr))
         return res
 
+    def interpolate_cone_dev(self, fields, cone, origin, dims, outs_dev: dict, fix: bool = False,
+                             fix_outside: bool = False) -> None:
+        """Same as interpolate_cone into device outputs (torch tensors or
+        device pointers) of dims[0] * dims[1] * dims[2] rows."""
+        d = np.ascontiguousarray(dims, np.int32)
+        c = np.ascontiguousarray(cone, np.float32)
+        org = np.ascontiguousarray(origin, np.float32)
+        outs = [None] * N.NUM_FIELDS
+        for f in fields:
+            outs[N.FIELD_SLOTS[f]] = N.ptr(outs_dev[f]) if not isinstance(outs_dev[f], int) else outs_dev[f]
+        optr = (C.c_void_p * N.NUM_FIELDS)(*outs)
+        o = self._opts(fields, N.METHOD_CENTRE, 1, 0, fix, fix_outside)
+        N.check(self.lib.dtfe_gpu_interpolate_cone_dev(self.h, c.ctypes.data, org.ctypes.data, d.ctypes.data,
+                                                       C.byref(o), optr))
+
     def interpolate_dev_async(self, fields, outs_dev: dict, method: int = 0, n_samples: int = 1, seed: int = 0,
                               fix: bool = False) -> None:
         """Queues the interpolation into device outputs without waiting

@@ -84,8 +84,10 @@ enum {
 /* Reference interpolateGrid() skips its `z += dx` after a sample outside the
  * hull (the `continue` at unaveraged_interpolation.cc:304 jumps over :353),
  * so every later sample of that z pencil re-locates the same outside point
- * and gets zeros.  Default (cell centres only): the same zeros, for parity;
- * this flag evaluates those samples at their own centres instead. */
+ * and gets zeros; interpolateRedshiftCone() does the same with `psi += dx`
+ * (:466 jumps over :527).  Default (cell centres and cone bins): the same
+ * zeros, for parity; this flag evaluates those samples at their own centres
+ * instead. */
 #define DTFE_FLAG_FIX_OUTSIDE_RASTER 2u
 
 /* ---- limits -------------------------------------------------------------- */
@@ -227,6 +229,9 @@ int dtfe_gpu_interpolate_points(dtfe_handle h, int64_t n, const float* xyz, cons
  * vertex densities; opts->method must be DTFE_METHOD_CENTRE. */
 int dtfe_gpu_interpolate_cone(dtfe_handle h, const float cone[6], const float origin[3], const int32_t dims[3],
                               const dtfe_interp_opts* opts, float* const out[DTFE_NUM_FIELDS]);
+/* Same, writing into device buffers (dims[0] dims[1] dims[2] rows each). */
+int dtfe_gpu_interpolate_cone_dev(dtfe_handle h, const float cone[6], const float origin[3], const int32_t dims[3],
+                                  const dtfe_interp_opts* opts, float* const out_dev[DTFE_NUM_FIELDS]);
 /* Same as dtfe_gpu_interpolate_dev, but only queues the work on the handle's
  * stream and returns without waiting: consecutive steps (vertex densities,
  * interpolation, ...) then run back to back on the device; the walk counters

@@ -70,10 +70,11 @@ def run(plan, box: int = 0, which: int = 0, n_points: int = 1, seed: int = 0, de
     return out
 
 
-def run_points(plan, pts, region, dens, box: int = 0):
+def run_points(plan, pts, region, dens, box: int = 0, timing: bool = False):
     """The reference's interpolateUserSampling on sub-box `box`'s
     tessellation with vertex densities `dens`: density, velocity, gradient,
-    scalar, scalar gradient of the points inside `region`, in order."""
+    scalar, scalar gradient of the points inside `region`, in order.  With
+    `timing`, (that dict, seconds of the interpolateUserSampling call)."""
     xyz, w, vel, tv, tn, dims, _ = _box_args(plan, box)
     b = plan.boxes[box]
     v0, nv = b.vert_offset, b.n_verts
@@ -88,22 +89,25 @@ def run_points(plan, pts, region, dens, box: int = 0):
     L = lib()
     vp = C.c_void_p
     L.ref_interpolate_points.argtypes = [C.c_int64, vp, vp, vp, vp, C.c_int64, vp, vp, vp, C.c_int64, vp, vp,
-                                         vp, vp, vp, vp, vp, C.POINTER(C.c_int64)]
+                                         vp, vp, vp, vp, vp, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
     p = lambda a: None if a is None else a.ctypes.data
     m = C.c_int64(0)
+    secs = C.c_double(0.0)
     rc = L.ref_interpolate_points(len(xyz), p(xyz), p(w), p(vel), p(sc), len(tv), p(tv), p(tn), p(reg), n,
                                   p(pts), p(d), p(out["density"]), p(out["velocity"]), p(out["velocity_gradient"]),
                                   p(out["scalar"]) if sc is not None else None,
-                                  p(out["scalar_gradient"]) if sc is not None else None, C.byref(m))
+                                  p(out["scalar_gradient"]) if sc is not None else None, C.byref(m), C.byref(secs))
     if rc:
         raise RuntimeError(f"ref_interpolate_points failed ({rc})")
-    return {k: a[:m.value] for k, a in out.items()}
+    res = {k: a[:m.value] for k, a in out.items()}
+    return (res, secs.value) if timing else res
 
 
-def run_cone(plan, cone, origin, dims, dens, box: int = 0):
+def run_cone(plan, cone, origin, dims, dens, box: int = 0, timing: bool = False):
     """The reference's interpolateRedshiftCone on sub-box `box`'s
     tessellation with vertex densities `dens`: density, velocity, gradient,
-    scalar, scalar gradient of the dims[0] * dims[1] * dims[2] cone samples."""
+    scalar, scalar gradient of the dims[0] * dims[1] * dims[2] cone samples.
+    With `timing`, (that dict, seconds of the interpolateRedshiftCone call)."""
     xyz, w, vel, tv, tn, _, _ = _box_args(plan, box)
     b = plan.boxes[box]
     v0, nv = b.vert_offset, b.n_verts
@@ -119,15 +123,16 @@ def run_cone(plan, cone, origin, dims, dens, box: int = 0):
     L = lib()
     vp = C.c_void_p
     L.ref_interpolate_cone.argtypes = [C.c_int64, vp, vp, vp, vp, C.c_int64, vp, vp, vp, vp, vp, vp, vp, vp, vp,
-                                       vp, vp]
+                                       vp, vp, C.POINTER(C.c_double)]
     p = lambda a: None if a is None else a.ctypes.data
+    secs = C.c_double(0.0)
     rc = L.ref_interpolate_cone(len(xyz), p(xyz), p(w), p(vel), p(sc), len(tv), p(tv), p(tn), p(c), p(o), p(dd),
                                 p(d), p(out["density"]), p(out["velocity"]), p(out["velocity_gradient"]),
                                 p(out["scalar"]) if sc is not None else None,
-                                p(out["scalar_gradient"]) if sc is not None else None)
+                                p(out["scalar_gradient"]) if sc is not None else None, C.byref(secs))
     if rc:
         raise RuntimeError(f"ref_interpolate_cone failed ({rc})")
-    return out
+    return (out, secs.value) if timing else out
 
 
 def _box_args(plan, box):

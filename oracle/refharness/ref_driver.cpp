@@ -190,7 +190,8 @@ int ref_interpolate_timed(int64_t nv, const float* xyz, const float* w, const fl
 int ref_interpolate_points(int64_t nv, const float* xyz, const float* w, const float* vel, const float* scal,
                            int64_t nt, const int32_t* tv, const int32_t* tn, const float region[6], int64_t n,
                            const float* pts, const float* dens, float* out_density, float* out_velocity,
-                           float* out_gradient, float* out_scalar, float* out_scalar_gradient, int64_t* n_out) {
+                           float* out_gradient, float* out_scalar, float* out_scalar_gradient, int64_t* n_out,
+                           double* seconds) {
   DT dt;
   const std::vector<DT::Vertex*>& verts = dt.load_flat(nv, xyz, nt, tv, tn);
   for (int64_t i = 0; i < nv; ++i) {
@@ -216,7 +217,9 @@ int ref_interpolate_points(int64_t nv, const float* xyz, const float* w, const f
   f.scalar = out_scalar != nullptr;
   f.scalar_gradient = out_scalar_gradient != nullptr;
   opt.uField = f;
+  const auto t0 = std::chrono::steady_clock::now();
   interpolateUserSampling(dt, samples, opt, &q);
+  if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   const size_t m = f.density ? q.density.size() : (f.velocity ? q.velocity.size() : q.velocity_gradient.size());
   *n_out = (int64_t)m;
   if (out_density && q.density.size() == m) std::memcpy(out_density, q.density.data(), m * sizeof(float));
@@ -232,11 +235,13 @@ int ref_interpolate_points(int64_t nv, const float* xyz, const float* w, const f
 // interpolateRedshiftCone on one tessellation (LOCAL indices) with the given
 // vertex densities: cone = (r_min, r_max, theta_min, theta_max, psi_min,
 // psi_max) in Mpc and degrees, dims = (n_r, n_theta, n_psi).  Outputs hold
-// dims[0] dims[1] dims[2] rows (NULL to skip a field).
+// dims[0] dims[1] dims[2] rows (NULL to skip a field); *seconds (if not NULL)
+// = the wall time of the interpolateRedshiftCone call alone.
 int ref_interpolate_cone(int64_t nv, const float* xyz, const float* w, const float* vel, const float* scal,
                          int64_t nt, const int32_t* tv, const int32_t* tn, const float cone[6],
                          const float origin[3], const int32_t dims[3], const float* dens, float* out_density,
-                         float* out_velocity, float* out_gradient, float* out_scalar, float* out_scalar_gradient) {
+                         float* out_velocity, float* out_gradient, float* out_scalar, float* out_scalar_gradient,
+                         double* seconds) {
   DT dt;
   const std::vector<DT::Vertex*>& verts = dt.load_flat(nv, xyz, nt, tv, tn);
   for (int64_t i = 0; i < nv; ++i) {
@@ -259,7 +264,9 @@ int ref_interpolate_cone(int64_t nv, const float* xyz, const float* w, const flo
   f.scalar = out_scalar != nullptr;
   f.scalar_gradient = out_scalar_gradient != nullptr;
   opt.uField = f;
+  const auto t0 = std::chrono::steady_clock::now();
   interpolateRedshiftCone(dt, opt, &q);
+  if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   const size_t m = (size_t)dims[0] * dims[1] * dims[2];
   if (out_density && q.density.size() == m) std::memcpy(out_density, q.density.data(), m * sizeof(float));
   if (out_velocity && q.velocity.size() == m) std::memcpy(out_velocity, q.velocity.data(), 3 * m * sizeof(float));

@@ -54,6 +54,26 @@ def test_cone_vs_oracle(gpu_built):
     assert (a == 0).any() and (a != 0).any() and ((a == 0) & (b != 0)).any()
 
 
+def test_cone_device_outputs(gpu_built):
+    """dtfe_gpu_interpolate_cone_dev writes the same rows into device
+    buffers as the host-buffer call."""
+    import torch
+    from dtfe_b200.device import DeviceDTFE
+    plan = _plan(57)
+    cone, origin, dims = CONES[0]
+    n = int(np.prod(dims))
+    with DeviceDTFE(0, 1) as d:
+        d.load(plan)
+        d.vertex_density(plan.rho_bar)
+        want = d.interpolate_cone(FIELDS, cone, origin, dims)
+        outs = {f: torch.full((n, N.field_components(N.FIELD_SLOTS[f], 1)), float("nan"), device="cuda")
+                for f in FIELDS}
+        d.interpolate_cone_dev(FIELDS, cone, origin, dims, outs)
+        d.synchronize()
+        for f in FIELDS:
+            assert np.array_equal(outs[f].cpu().numpy().reshape(want[f].shape), want[f]), f
+
+
 def test_cone_errors(gpu_built):
     from dtfe_b200.device import DeviceDTFE
     plan = _plan(55)

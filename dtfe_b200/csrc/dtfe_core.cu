@@ -936,9 +936,9 @@ __global__ void __launch_bounds__(256) k_cone_rows(InterpParams P, int* __restri
 // unaveraged_interpolation.cc:560-691), one thread per point of a single
 // sub-box's tessellation.  keep[i]: the point lies in the region (closed);
 // idx: exclusive prefix of keep, the point's output row.  Seed: the bin of the
-// tile cell holding the point (when the seeds are built and the point lies in
-// the tile), else the sub-box's first tetrahedron; then the walk and the
-// cell-centre arithmetic at the point.
+// tile cell nearest the point (when the seeds are built), else the sub-box's
+// first tetrahedron; then the walk and the cell-centre arithmetic at the
+// point.
 struct Region6 {
   float r[6];
 };
@@ -1010,24 +1010,24 @@ __global__ void __launch_bounds__(256, 4) k_points_eval(InterpParams P, int64_t 
     const double p[3] = {(double)pf[0], (double)pf[1], (double)pf[2]};
     const dtfe_subbox& B = P.boxes[0];
     int t0 = B.n_tets > 0 ? (int)B.tet_offset : -1;
-    if (use_bins && t0 >= 0) {
+    if (use_bins && t0 >= 0 && B.tile_dims[0] > 0 && B.tile_dims[1] > 0 && B.tile_dims[2] > 0) {
+      // the bin of the tile cell nearest the point: points beyond the tile
+      // (padding zone, outside the hull) start at the tile's edge rather than
+      // at the first tetrahedron (the located tetrahedron does not depend on
+      // the start)
       SampleCell c;
-      bool in = true;
       int ijk[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         const float f = floorf((pf[a] - B.lo[a]) / B.dx[a]);
-        in = in && f >= 0.f && f < (float)B.tile_dims[a];
-        ijk[a] = in ? (int)f : 0;
+        ijk[a] = (int)fminf(fmaxf(f, 0.f), (float)(B.tile_dims[a] - 1));
       }
-      if (in) {
-        c.b = 0;
-        c.i = ijk[0];
-        c.j = ijk[1];
-        c.k = ijk[2];
-        c.local = ((int64_t)ijk[0] * B.tile_dims[1] + ijk[1]) * B.tile_dims[2] + ijk[2];
-        t0 = seed_of(P, c);
-      }
+      c.b = 0;
+      c.i = ijk[0];
+      c.j = ijk[1];
+      c.k = ijk[2];
+      c.local = ((int64_t)ijk[0] * B.tile_dims[1] + ijk[1]) * B.tile_dims[2] + ijk[2];
+      t0 = seed_of(P, c);
     }
     int v[4];
     float X[4][3];

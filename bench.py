@@ -72,6 +72,7 @@ def parse():
     ap.add_argument("--sampling-n", type=int, default=128,
                     help="particles per side of the redshift-cone / user-point workload (one box)")
     ap.add_argument("--no-sampling", action="store_true")
+    ap.add_argument("--no-output", action="store_true", help="skip the binary output-file leg")
     return ap.parse_args()
 
 
@@ -634,6 +635,55 @@ def sampling_leg(args, local: int, threads: int, cpu: bool) -> dict:
     return res
 
 
+def output_leg(dev, outs: dict, cpu: bool) -> dict:
+    """Binary output files (outputFileType 101): the step's device fields
+    written as writeOutputData names them, streamed from HBM through pinned
+    buffers (dtfe_gpu_write_binary_dev), into a temporary directory; beside
+    it the reference's own writeOutputData (harness) writing the same fields
+    from host Quantities.  Wall-clock seconds around the whole write (file
+    I/O is the bound); the files are compared byte for byte and removed."""
+    import shutil
+    import tempfile
+    import torch
+    from dtfe_b200 import output as OUT
+    d = tempfile.mkdtemp(prefix="dtfe_out_")
+    try:
+        torch.cuda.synchronize()
+        nbytes = sum(t.numel() * 4 for t in outs.values())
+        t0 = time.time()
+        mine = OUT.write_fields(os.path.join(d, "gpu"), outs, device=dev)
+        t_gpu = time.time() - t0
+        res = {"fields": list(outs), "bytes": nbytes, "gpu_s": t_gpu, "gpu_gbs": nbytes / t_gpu / 1e9,
+               "files": [os.path.basename(p) for p in mine], "timing": "wall clock (file I/O)"}
+        if cpu:
+            try:
+                import refharness as R
+                have = R.available()
+            except ImportError:
+                have = False
+            if have:
+                host = {f: t.cpu().numpy() for f, t in outs.items()}
+                n = next(iter(host.values())).shape[0]
+                t0 = time.time()
+                R.write_output(os.path.join(d, "ref"), n, host, {})
+                t_ref = time.time() - t0
+                same = True
+                for p in mine:
+                    q = os.path.join(d, os.path.basename(p).replace("gpu", "ref", 1))
+                    with open(p, "rb") as f1, open(q, "rb") as f2:
+                        while same:
+                            a, b = f1.read(1 << 24), f2.read(1 << 24)
+                            same = a == b
+                            if not a:
+                                break
+                res["reference"] = {"s": t_ref, "gbs": nbytes / t_ref / 1e9, "kind": "reference", "cores": 1,
+                                    "sample": "the same fields from host vectors (writeOutputData, binary)",
+                                    "bytes_identical": bool(same)}
+        return res
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -940,6 +990,11 @@ def run_ours(args):
     if side and not args.no_bwd:
         bwd = backward_leg(args, local, threads)
 
+    output = None
+    if side and not args.no_output:
+        output = output_leg(dev, {f: outs[f] for f in ("density", "velocity", "velocity_gradient")},
+                            rank == 0 and not args.no_cpu)
+
     sampling = None
     if side and not args.no_sampling:
         sampling = sampling_leg(args, local, threads, rank == 0 and not args.no_cpu)
@@ -969,6 +1024,7 @@ def run_ours(args):
         "backward": bwd,
         "batched_subboxes": batch,
         "sampling": sampling,
+        "output_files": output,
         "comparison_estimators": compare,
         "walk": {k: status[k] for k in ("n_samples_located", "n_walk_steps", "n_exact_tests", "n_ties",
                                         "n_outside")} if status else None,

@@ -76,7 +76,7 @@ class Config(C.Structure):
 
 
 # status codes (include/dtfe_gpu.h)
-OK, ERR_ARG, ERR_CUDA, ERR_ALLOC, ERR_STATE, ERR_WALK, ERR_DEGENERATE, ERR_NO_DEVICE, ERR_TOO_LARGE = range(9)
+OK, ERR_ARG, ERR_CUDA, ERR_ALLOC, ERR_STATE, ERR_WALK, ERR_DEGENERATE, ERR_NO_DEVICE, ERR_TOO_LARGE, ERR_IO = range(10)
 NUM_FIELDS = 9
 NOALLOC_MAX_VERTS = 1 << 20
 FIELD_SLOTS = {
@@ -131,6 +131,10 @@ def host() -> C.CDLL:
         lib.dtfe_select_in_box.argtypes = [vp, C.c_int64, vp, vp, C.c_int, vp, vp]
         lib.dtfe_select_in_box.restype = C.c_int64
         lib.dtfe_parallel_grid.argtypes = [C.c_int64, vp, vp]
+        lib.dtfe_write_binary.argtypes = [C.c_char_p, vp, C.c_int64]
+        lib.dtfe_write_binary.restype = C.c_int
+        lib.dtfe_field_suffix.argtypes = [C.c_int32, C.c_int32]
+        lib.dtfe_field_suffix.restype = C.c_char_p
         lib.dtfe_optimal_partition.argtypes = [vp, C.c_int64, vp, vp, vp, vp, vp]
         lib.dtfe_optimal_partition.restype = C.c_int
         lib.dtfe_axis_coords.argtypes = [C.c_float, C.c_float, C.c_int64, vp]
@@ -169,6 +173,7 @@ def gpu() -> C.CDLL:
                                                     C.POINTER(C.c_int64)]
         lib.dtfe_gpu_interpolate_cone.argtypes = [H, vp, vp, vp, C.POINTER(InterpOpts), C.POINTER(vp)]
         lib.dtfe_gpu_interpolate_cone_dev.argtypes = [H, vp, vp, vp, C.POINTER(InterpOpts), C.POINTER(vp)]
+        lib.dtfe_gpu_write_binary_dev.argtypes = [H, C.c_char_p, vp, C.c_int64]
         lib.dtfe_gpu_download_vertex_density.argtypes = [H, vp]
         lib.dtfe_gpu_locate_points.argtypes = [H, C.c_int64, vp, C.c_int32, vp]
         lib.dtfe_gpu_stream.argtypes = [H]

@@ -1336,6 +1336,8 @@ struct dtfe_gpu_s {
   int64_t* pts_idx = nullptr;
   int64_t* pts_blocks = nullptr;
   float* pts_out = nullptr;
+  char* io_stage[2] = {nullptr, nullptr};  // pinned staging of dtfe_gpu_write_binary_dev
+  cudaEvent_t io_ev[2] = {nullptr, nullptr};
   double* m1_table = nullptr;     // method-1 Sobol points (100 NN x 3)
   int m1_table_nn = 0;
   void* m1_scratch = nullptr;     // method-1 counts, offsets, scan scratch
@@ -1587,6 +1589,10 @@ int dtfe_gpu_destroy(dtfe_handle h) {
                   h->m1_scratch, h->m1_lists})
     if (p) cudaFree(p);
   if (h->dep_out) cudaFree(h->dep_out);
+  for (int i = 0; i < 2; ++i) {
+    if (h->io_stage[i]) cudaFreeHost(h->io_stage[i]);
+    if (h->io_ev[i]) cudaEventDestroy(h->io_ev[i]);
+  }
   cudaEventDestroy(h->ev_h2d);
   cudaStreamDestroy(h->stream);
   delete h;
@@ -2503,6 +2509,47 @@ int dtfe_gpu_interpolate_cone_dev(dtfe_handle h, const float cone[6], const floa
   InterpParams P;
   if ((rc = cone_enqueue(h, cone, origin, dims, o, out_dev, P))) return rc;
   return read_status(h, nullptr);
+}
+
+// File chunk of dtfe_gpu_write_binary_dev: two pinned buffers of this size.
+static const int64_t kIoChunk = int64_t(1) << 25;
+
+int dtfe_gpu_write_binary_dev(dtfe_handle h, const char* path, const float* data_dev, int64_t n_floats) {
+  if (!h || !path || n_floats < 0 || (n_floats > 0 && !data_dev)) return set_error(DTFE_ERR_ARG, "null argument");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  for (int i = 0; i < 2; ++i) {
+    if (!h->io_stage[i]) DTFE_CUDA_TRY(cudaHostAlloc((void**)&h->io_stage[i], (size_t)kIoChunk, cudaHostAllocDefault));
+    if (!h->io_ev[i]) DTFE_CUDA_TRY(cudaEventCreateWithFlags(&h->io_ev[i], cudaEventDisableTiming));
+  }
+  std::FILE* f = std::fopen(path, "wb");
+  if (!f) return set_error(DTFE_ERR_IO, std::string("cannot open ") + path + " for writing");
+  const int64_t bytes = n_floats * (int64_t)sizeof(float);
+  const int64_t n_chunks = (bytes + kIoChunk - 1) / kIoChunk;
+  const char* src = reinterpret_cast<const char*>(data_dev);
+  auto chunk_size = [&](int64_t c) { return (size_t)std::min(kIoChunk, bytes - c * kIoChunk); };
+  auto enqueue = [&](int64_t c) -> cudaError_t {
+    cudaError_t e = cudaMemcpyAsync(h->io_stage[c & 1], src + c * kIoChunk, chunk_size(c), cudaMemcpyDeviceToHost,
+                                    h->stream);
+    return e == cudaSuccess ? cudaEventRecord(h->io_ev[c & 1], h->stream) : e;
+  };
+  // the copy of chunk c + 1 runs while chunk c is written to the file; a
+  // buffer is refilled only after its previous chunk has been written
+  int rc = DTFE_OK;
+  cudaError_t e = n_chunks > 0 ? enqueue(0) : cudaSuccess;
+  for (int64_t c = 0; c < n_chunks && e == cudaSuccess && rc == DTFE_OK; ++c) {
+    if (c + 1 < n_chunks) e = enqueue(c + 1);
+    if (e == cudaSuccess) e = cudaEventSynchronize(h->io_ev[c & 1]);
+    if (e == cudaSuccess && std::fwrite(h->io_stage[c & 1], 1, chunk_size(c), f) != chunk_size(c))
+      rc = set_error(DTFE_ERR_IO, std::string("short write to ") + path);
+  }
+  if (e != cudaSuccess) {
+    cudaStreamSynchronize(h->stream);  // no copy into a staging buffer outlives the call
+    std::fclose(f);
+    return set_error(DTFE_ERR_CUDA, std::string("writing ") + path + ": " + cudaGetErrorString(e));
+  }
+  if (rc != DTFE_OK) cudaStreamSynchronize(h->stream);
+  if (std::fclose(f) != 0 && rc == DTFE_OK) rc = set_error(DTFE_ERR_IO, std::string("cannot close ") + path);
+  return rc;
 }
 
 int dtfe_gpu_interpolate_dev_async(dtfe_handle h, const dtfe_interp_opts* opts,

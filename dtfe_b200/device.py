@@ -199,6 +199,13 @@ class DeviceDTFE:
         N.check(self.lib.dtfe_gpu_interpolate_cone_dev(self.h, c.ctypes.data, org.ctypes.data, d.ctypes.data,
                                                        C.byref(o), optr))
 
+    def write_binary_dev(self, path: str, tensor) -> None:
+        """Streams a contiguous float32 CUDA tensor to `path` in the
+        reference's binary output format (dtfe_gpu_write_binary_dev)."""
+        if not tensor.is_contiguous() or str(tensor.dtype) != "torch.float32":
+            raise ValueError("write_binary_dev takes a contiguous float32 tensor")
+        N.check(self.lib.dtfe_gpu_write_binary_dev(self.h, path.encode(), tensor.data_ptr(), tensor.numel()))
+
     def interpolate_dev_async(self, fields, outs_dev: dict, method: int = 0, n_samples: int = 1, seed: int = 0,
                               fix: bool = False) -> None:
         """Queues the interpolation into device outputs without waiting

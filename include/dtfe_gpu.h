@@ -47,7 +47,8 @@ enum {
   DTFE_ERR_WALK = 5,         /* a point-location walk hit its step limit */
   DTFE_ERR_DEGENERATE = 6,   /* fewer than 4 vertices: no tetrahedra */
   DTFE_ERR_NO_DEVICE = 7,    /* no usable CUDA device / extension */
-  DTFE_ERR_TOO_LARGE = 8     /* request exceeds a documented maximum */
+  DTFE_ERR_TOO_LARGE = 8,    /* request exceeds a documented maximum */
+  DTFE_ERR_IO = 9            /* an output file could not be opened or written */
 };
 
 /* ---- output field slots (bit i of a field mask = slot i) --------------- */
@@ -232,6 +233,16 @@ int dtfe_gpu_interpolate_cone(dtfe_handle h, const float cone[6], const float or
 /* Same, writing into device buffers (dims[0] dims[1] dims[2] rows each). */
 int dtfe_gpu_interpolate_cone_dev(dtfe_handle h, const float cone[6], const float origin[3], const int32_t dims[3],
                                   const dtfe_interp_opts* opts, float* const out_dev[DTFE_NUM_FIELDS]);
+/* Writes n_floats floats of device memory (a field in the Quantities layout)
+ * to `path` in the reference's binary output format: the raw floats, no
+ * header, the file writeBinaryFile (src/io/binary_io.cc:185-216) writes for
+ * the same field; name it with dtfe_field_suffix (include/dtfe_host.h) as
+ * writeOutputData does.  The copy is ordered after earlier work on the
+ * handle's stream and streamed through two pinned buffers (the copy of one
+ * chunk overlaps the file write of the previous), so a device-resident field
+ * needs no host copy of its own.  DTFE_ERR_IO when the file cannot be opened
+ * or fully written. */
+int dtfe_gpu_write_binary_dev(dtfe_handle h, const char* path, const float* data_dev, int64_t n_floats);
 /* Same as dtfe_gpu_interpolate_dev, but only queues the work on the handle's
  * stream and returns without waiting: consecutive steps (vertex densities,
  * interpolation, ...) then run back to back on the device; the walk counters

@@ -14,6 +14,8 @@
  *   dtfe_tessellate(_batch)  delaunayTriangulation         src/CGAL_triangulation/triangulation.cpp:162-195
  *   dtfe_plan_build          DTFE() + DTFE_parallel() up to the interpolation
  *                            src/DTFE.cpp:76-251, 287-385
+ *   dtfe_write_binary        writeBinaryFile               src/io/binary_io.cc:185-216
+ *   dtfe_field_suffix        writeOutputData's file names  src/input_output.cc:216-275
  */
 #ifndef DTFE_HOST_H
 #define DTFE_HOST_H
@@ -107,6 +109,19 @@ int dtfe_plan_build(int kind, const float* pos, const float* w, const float* vel
                     float padding_particles, double average_density, dtfe_plan* out);
 int dtfe_plan_get(dtfe_plan p, dtfe_plan_view* view);
 void dtfe_plan_release(dtfe_plan p);
+
+/* Output files in the reference's binary format (outputFileType 101).
+ * dtfe_write_binary writes `bytes` raw bytes of `data` (a field's cells x
+ * components floats) to `path`, created or truncated, without a header: the
+ * file writeBinaryFile (src/io/binary_io.cc:185-216) makes from the
+ * corresponding Quantities vector.  DTFE_ERR_IO when the file cannot be
+ * opened or fully written.  dtfe_field_suffix gives writeOutputData's file
+ * suffix (src/input_output.cc:216-275) of field `slot` for uQuantities
+ * (averaged = 0: ".den", ".vel", ".velGrad", ...) or aQuantities
+ * (".a_den", ...); NULL for a slot without a file (the unaveraged velocity
+ * standard deviation) or out of range. */
+int dtfe_write_binary(const char* path, const void* data, int64_t bytes);
+const char* dtfe_field_suffix(int32_t slot, int32_t averaged);
 
 #ifdef __cplusplus
 }

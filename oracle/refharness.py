@@ -184,3 +184,43 @@ def time_boxes(plan, threads: int, which: int = 0, n_points: int = 1):
     for k, t in enumerate(per_box):
         loads[k % len(loads)] += t
     return max(loads), per_box
+
+
+def write_binary(path: str, data, ncomp: int) -> None:
+    """The reference's writeBinaryFile of rows x ncomp floats (a std::vector
+    of Real for 1, of Pvector<Real, ncomp> for 3, 5, 9) into `path`."""
+    a = np.ascontiguousarray(data, np.float32)
+    L = lib()
+    L.ref_write_binary.argtypes = [C.c_char_p, C.c_void_p, C.c_int64, C.c_int]
+    rc = L.ref_write_binary(path.encode(), a.ctypes.data, a.size // ncomp, ncomp)
+    if rc:
+        raise RuntimeError(f"ref_write_binary failed ({rc})")
+
+
+_SLOTS = ["density", "velocity", "velocity_gradient", "velocity_divergence", "velocity_shear",
+          "velocity_vorticity", "velocity_std", "scalar", "scalar_gradient"]
+
+
+def write_output(base: str, n: int, u: dict, a: dict) -> None:
+    """The reference's writeOutputData (binary output) of n rows per field:
+    u / a map field names to float arrays (uQuantities / aQuantities)."""
+    keep = []
+
+    def table(d):
+        ptrs = (C.c_void_p * 9)()
+        mask = 0
+        for s, f in enumerate(_SLOTS):
+            if f in d:
+                arr = np.ascontiguousarray(d[f], np.float32)
+                keep.append(arr)
+                ptrs[s] = arr.ctypes.data
+                mask |= 1 << s
+        return ptrs, mask
+
+    up, um = table(u)
+    ap, am = table(a)
+    L = lib()
+    L.ref_write_output.argtypes = [C.c_char_p, C.c_int64, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]
+    rc = L.ref_write_output(base.encode(), n, um, am, C.cast(up, C.c_void_p), C.cast(ap, C.c_void_p))
+    if rc:
+        raise RuntimeError(f"ref_write_output failed ({rc})")

@@ -172,6 +172,8 @@ def gpu() -> C.CDLL:
         lib.dtfe_gpu_interpolate_points.argtypes = [H, C.c_int64, vp, vp, C.POINTER(InterpOpts), C.POINTER(vp),
                                                     C.POINTER(C.c_int64)]
         lib.dtfe_gpu_interpolate_cone.argtypes = [H, vp, vp, vp, C.POINTER(InterpOpts), C.POINTER(vp)]
+        lib.dtfe_gpu_average_points.argtypes = [H, C.c_int64, vp, vp, vp, C.POINTER(InterpOpts), C.POINTER(vp),
+                                                C.POINTER(C.c_int64)]
         lib.dtfe_gpu_interpolate_cone_dev.argtypes = [H, vp, vp, vp, C.POINTER(InterpOpts), C.POINTER(vp)]
         lib.dtfe_gpu_write_binary_dev.argtypes = [H, C.c_char_p, vp, C.c_int64]
         lib.dtfe_gpu_download_vertex_density.argtypes = [H, vp]

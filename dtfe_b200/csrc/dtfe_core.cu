@@ -994,6 +994,78 @@ struct ConeGrid {
   }
 };
 
+// Walk seed of a point in the handle's single sub-box: the bin of the tile
+// cell nearest the point (when the seeds are built), so points beyond the
+// tile (padding zone, outside the hull) start at the tile's edge; else the
+// sub-box's first tetrahedron.  -1 for a sub-box without tetrahedra.  The
+// located tetrahedron does not depend on the start.
+__device__ __forceinline__ int point_seed(const InterpParams& P, const float pf[3], int use_bins) {
+  const dtfe_subbox& B = P.boxes[0];
+  int t0 = B.n_tets > 0 ? (int)B.tet_offset : -1;
+  if (use_bins && t0 >= 0 && B.tile_dims[0] > 0 && B.tile_dims[1] > 0 && B.tile_dims[2] > 0) {
+    SampleCell c;
+    int ijk[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float f = floorf((pf[a] - B.lo[a]) / B.dx[a]);
+      ijk[a] = (int)fminf(fmaxf(f, 0.f), (float)(B.tile_dims[a] - 1));
+    }
+    c.b = 0;
+    c.i = ijk[0];
+    c.j = ijk[1];
+    c.k = ijk[2];
+    c.local = ((int64_t)ijk[0] * B.tile_dims[1] + ijk[1]) * B.tile_dims[2] + ijk[2];
+    t0 = seed_of(P, c);
+  }
+  return t0;
+}
+
+template <int S>
+__device__ __forceinline__ void zero_out(CellOut& e) {
+  e.dens = 0.f;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) e.vel[c] = 0.f;
+#pragma unroll
+  for (int c = 0; c < 9; ++c) e.grad[c] = 0.f;
+#pragma unroll
+  for (int q = 0; q < S; ++q) {
+    e.sc[q] = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) e.scg[3 * q + c] = 0.f;
+  }
+}
+
+// One output row of every requested field (derived fields from the gradient).
+template <int S>
+__device__ __forceinline__ void store_row(const InterpParams& P, int64_t o, const CellOut& e) {
+  const uint32_t F = P.fields;
+  if (has_field(F, DTFE_DENSITY)) P.out[DTFE_DENSITY][o] = e.dens;
+  if (has_field(F, DTFE_VELOCITY))
+#pragma unroll
+    for (int c = 0; c < 3; ++c) P.out[DTFE_VELOCITY][3 * o + c] = e.vel[c];
+  if (has_field(F, DTFE_VELOCITY_GRADIENT))
+#pragma unroll
+    for (int c = 0; c < 9; ++c) P.out[DTFE_VELOCITY_GRADIENT][9 * o + c] = e.grad[c];
+  if (has_field(F, DTFE_VELOCITY_DIVERGENCE) || has_field(F, DTFE_VELOCITY_SHEAR) ||
+      has_field(F, DTFE_VELOCITY_VORTICITY)) {
+    float dv, sh[5], vo[3];
+    derived_fields(e.grad, dv, sh, vo);
+    if (has_field(F, DTFE_VELOCITY_DIVERGENCE)) P.out[DTFE_VELOCITY_DIVERGENCE][o] = dv;
+    if (has_field(F, DTFE_VELOCITY_SHEAR))
+#pragma unroll
+      for (int c = 0; c < 5; ++c) P.out[DTFE_VELOCITY_SHEAR][5 * o + c] = sh[c];
+    if (has_field(F, DTFE_VELOCITY_VORTICITY))
+#pragma unroll
+      for (int c = 0; c < 3; ++c) P.out[DTFE_VELOCITY_VORTICITY][3 * o + c] = vo[c];
+  }
+  if (S > 0 && has_field(F, DTFE_SCALAR))
+#pragma unroll
+    for (int q = 0; q < S; ++q) P.out[DTFE_SCALAR][(int64_t)S * o + q] = e.sc[q];
+  if (S > 0 && has_field(F, DTFE_SCALAR_GRADIENT))
+#pragma unroll
+    for (int q = 0; q < 3 * S; ++q) P.out[DTFE_SCALAR_GRADIENT][(int64_t)3 * S * o + q] = e.scg[q];
+}
+
 // tet_out (may be null): the located tetrahedron of each row, kOutside when
 // outside the hull.  Four blocks per SM (64 registers), as the fused
 // cell-centre kernel's default: the walks are latency-bound.
@@ -1008,27 +1080,7 @@ __global__ void __launch_bounds__(256, 4) k_points_eval(InterpParams P, int64_t 
   unsigned n_loc = 0, n_out = 0, n_fail = 0;
   if (active) {
     const double p[3] = {(double)pf[0], (double)pf[1], (double)pf[2]};
-    const dtfe_subbox& B = P.boxes[0];
-    int t0 = B.n_tets > 0 ? (int)B.tet_offset : -1;
-    if (use_bins && t0 >= 0 && B.tile_dims[0] > 0 && B.tile_dims[1] > 0 && B.tile_dims[2] > 0) {
-      // the bin of the tile cell nearest the point: points beyond the tile
-      // (padding zone, outside the hull) start at the tile's edge rather than
-      // at the first tetrahedron (the located tetrahedron does not depend on
-      // the start)
-      SampleCell c;
-      int ijk[3];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const float f = floorf((pf[a] - B.lo[a]) / B.dx[a]);
-        ijk[a] = (int)fminf(fmaxf(f, 0.f), (float)(B.tile_dims[a] - 1));
-      }
-      c.b = 0;
-      c.i = ijk[0];
-      c.j = ijk[1];
-      c.k = ijk[2];
-      c.local = ((int64_t)ijk[0] * B.tile_dims[1] + ijk[1]) * B.tile_dims[2] + ijk[2];
-      t0 = seed_of(P, c);
-    }
+    const int t0 = point_seed(P, pf, use_bins);
     int v[4];
     float X[4][3];
     int t = t0 < 0 ? kOutside : walk_locate<true>(P.tet_v, P.tet_n, P.posd, p, t0, P.max_steps, v, X, st);
@@ -1039,17 +1091,7 @@ __global__ void __launch_bounds__(256, 4) k_points_eval(InterpParams P, int64_t 
     }
     n_out += t < 0;
     CellOut e;
-    e.dens = 0.f;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) e.vel[c] = 0.f;
-#pragma unroll
-    for (int c = 0; c < 9; ++c) e.grad[c] = 0.f;
-#pragma unroll
-    for (int q = 0; q < S; ++q) {
-      e.sc[q] = 0.f;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) e.scg[3 * q + c] = 0.f;
-    }
+    zero_out<S>(e);
     const uint32_t F = P.fields;
     const bool want_grad = has_field(F, DTFE_VELOCITY_GRADIENT) || has_field(F, DTFE_VELOCITY_DIVERGENCE) ||
                            has_field(F, DTFE_VELOCITY_SHEAR) || has_field(F, DTFE_VELOCITY_VORTICITY);
@@ -1057,31 +1099,128 @@ __global__ void __launch_bounds__(256, 4) k_points_eval(InterpParams P, int64_t 
     const bool want_sc = S > 0 && (has_field(F, DTFE_SCALAR) || has_field(F, DTFE_SCALAR_GRADIENT));
     if (t >= 0) cell_eval<S>(v, X, p, P.posd, P.vel4, P.scal, has_field(F, DTFE_DENSITY), want_vel, want_sc, P.fix != 0, e);
     if (tet_out) tet_out[o] = t;
-    if (has_field(F, DTFE_DENSITY)) P.out[DTFE_DENSITY][o] = e.dens;
-    if (has_field(F, DTFE_VELOCITY))
+    store_row<S>(P, o, e);
+  }
+  fold_counters(P, n_loc, n_out, n_fail, st);
+}
+
+// Volume averages at point samples (averaged_interpolation_2.cc:245-662):
+// NN points per sample, offsets u in (-0.5, 0.5) from Philox keyed by
+// (seed, sample index, w) instead of the reference's mt19937 stream (the
+// comparison with the reference is statistical); each point walked from the
+// tetrahedron of the sample's centre (the reference's `previous` hint), the
+// fields summed in float in sample order, points outside the hull skipped
+// but counted, divided by NN (:154-155, 195).
+// Sources: user points (interpolateUserSampling_averaged_2, :470-647): point
+// = float(position + u delta) per axis; redshift-cone bins
+// (interpolateRedshiftCone_averaged_2, :245-466): r, theta, psi each
+// float(centre + u d), then o + (r sin theta) cos psi ... in float, with
+// sin/cos evaluated in double and rounded to float.
+struct PointAvgList {
+  PointList pl;
+  const float* delta;
+  __device__ __forceinline__ bool get(int64_t i, float pf[3], int64_t& row) const { return pl.get(i, pf, row); }
+  __device__ __forceinline__ void sample(int64_t i, const double u[3], float pf[3]) const {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) P.out[DTFE_VELOCITY][3 * o + c] = e.vel[c];
-    if (has_field(F, DTFE_VELOCITY_GRADIENT))
-#pragma unroll
-      for (int c = 0; c < 9; ++c) P.out[DTFE_VELOCITY_GRADIENT][9 * o + c] = e.grad[c];
-    if (has_field(F, DTFE_VELOCITY_DIVERGENCE) || has_field(F, DTFE_VELOCITY_SHEAR) ||
-        has_field(F, DTFE_VELOCITY_VORTICITY)) {
-      float dv, sh[5], vo[3];
-      derived_fields(e.grad, dv, sh, vo);
-      if (has_field(F, DTFE_VELOCITY_DIVERGENCE)) P.out[DTFE_VELOCITY_DIVERGENCE][o] = dv;
-      if (has_field(F, DTFE_VELOCITY_SHEAR))
-#pragma unroll
-        for (int c = 0; c < 5; ++c) P.out[DTFE_VELOCITY_SHEAR][5 * o + c] = sh[c];
-      if (has_field(F, DTFE_VELOCITY_VORTICITY))
-#pragma unroll
-        for (int c = 0; c < 3; ++c) P.out[DTFE_VELOCITY_VORTICITY][3 * o + c] = vo[c];
+    for (int c = 0; c < 3; ++c)
+      pf[c] = (float)__dadd_rn((double)pl.pts[3 * i + c], __dmul_rn(u[c], (double)delta[3 * i + c]));
+  }
+};
+struct ConeAvgGrid {
+  ConeGrid g;
+  const float* th;  // theta bin centres [n1]
+  const float* ps;  // psi bin centres [n2]
+  float d[3];       // bin sizes in r, theta, psi (radians)
+  __device__ __forceinline__ bool get(int64_t s, float pf[3], int64_t& row) const { return g.get(s, pf, row); }
+  __device__ __forceinline__ void sample(int64_t s, const double u[3], float pf[3]) const {
+    const uint64_t ij = (uint64_t)s / g.n2;
+    const uint32_t k = (uint32_t)((uint64_t)s - ij * g.n2);
+    const uint32_t i = (uint32_t)(ij / g.n1), j = (uint32_t)(ij - (uint64_t)i * g.n1);
+    const float R = (float)__dadd_rn((double)__ldg(&g.r[i]), __dmul_rn(u[0], (double)d[0]));
+    const float T = (float)__dadd_rn((double)__ldg(&th[j]), __dmul_rn(u[1], (double)d[1]));
+    const float Q = (float)__dadd_rn((double)__ldg(&ps[k]), __dmul_rn(u[2], (double)d[2]));
+    const float st = (float)sin((double)T), ct = (float)cos((double)T);
+    const float cq = (float)cos((double)Q), sq = (float)sin((double)Q);
+    const float rs = __fmul_rn(R, st);
+    pf[0] = __fadd_rn(g.o[0], __fmul_rn(rs, cq));
+    pf[1] = __fadd_rn(g.o[1], __fmul_rn(rs, sq));
+    pf[2] = __fadd_rn(g.o[2], __fmul_rn(R, ct));
+  }
+};
+
+template <int S, class Src>
+__global__ void __launch_bounds__(256, 4) k_points_average(InterpParams P, int64_t n, Src src, int use_bins,
+                                                        uint64_t key) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  float pc[3];
+  int64_t o = 0;
+  const bool active = i < n && src.get(i, pc, o);
+  WalkStats st{0, 0, 0};
+  unsigned n_loc = 0, n_out = 0, n_fail = 0;
+  if (active) {
+    const uint32_t F = P.fields;
+    const bool want_grad = has_field(F, DTFE_VELOCITY_GRADIENT) || has_field(F, DTFE_VELOCITY_DIVERGENCE) ||
+                           has_field(F, DTFE_VELOCITY_SHEAR) || has_field(F, DTFE_VELOCITY_VORTICITY);
+    const bool want_vel = has_field(F, DTFE_VELOCITY) || want_grad;
+    const bool want_dens = has_field(F, DTFE_DENSITY);
+    const bool want_sc = S > 0 && (has_field(F, DTFE_SCALAR) || has_field(F, DTFE_SCALAR_GRADIENT));
+    int t0 = point_seed(P, pc, use_bins);
+    if (t0 >= 0) {
+      // the centre's tetrahedron seeds the sample walks
+      const double p[3] = {(double)pc[0], (double)pc[1], (double)pc[2]};
+      int v[4];
+      float X[4][3];
+      const int tc = walk_locate<true>(P.tet_v, P.tet_n, P.posd, p, t0, P.max_steps, v, X, st);
+      ++n_loc;
+      if (tc == kWalkFail) ++n_fail;
+      if (tc >= 0) t0 = tc;
     }
-    if (S > 0 && has_field(F, DTFE_SCALAR))
+    CellOut acc;
+    zero_out<S>(acc);
+    const int NN = P.NN;
+    for (int w = 0; w < NN && t0 >= 0; ++w) {
+      double u[3];
+      mc_offsets(key, (uint64_t)i, (uint32_t)w, u);
+      float pf[3];
+      src.sample(i, u, pf);
+      const double p[3] = {(double)pf[0], (double)pf[1], (double)pf[2]};
+      int v[4];
+      float X[4][3];
+      int t = walk_locate<true>(P.tet_v, P.tet_n, P.posd, p, t0, P.max_steps, v, X, st);
+      ++n_loc;
+      if (t == kWalkFail) {
+        ++n_fail;
+        t = kOutside;
+      }
+      n_out += t < 0;
+      if (t < 0) continue;
+      CellOut e;
+      cell_eval<S>(v, X, p, P.posd, P.vel4, P.scal, want_dens, want_vel, want_sc, P.fix != 0, e);
+      acc.dens += e.dens;
 #pragma unroll
-      for (int q = 0; q < S; ++q) P.out[DTFE_SCALAR][(int64_t)S * o + q] = e.sc[q];
-    if (S > 0 && has_field(F, DTFE_SCALAR_GRADIENT))
+      for (int q = 0; q < 3; ++q) acc.vel[q] += e.vel[q];
 #pragma unroll
-      for (int q = 0; q < 3 * S; ++q) P.out[DTFE_SCALAR_GRADIENT][(int64_t)3 * S * o + q] = e.scg[q];
+      for (int q = 0; q < 9; ++q) acc.grad[q] += e.grad[q];
+#pragma unroll
+      for (int q = 0; q < S; ++q) {
+        acc.sc[q] += e.sc[q];
+#pragma unroll
+        for (int r = 0; r < 3; ++r) acc.scg[3 * q + r] += e.scg[3 * q + r];
+      }
+    }
+    const float fn = (float)NN;
+    acc.dens = acc.dens / fn;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) acc.vel[q] = acc.vel[q] / fn;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) acc.grad[q] = acc.grad[q] / fn;
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+      acc.sc[q] = acc.sc[q] / fn;
+#pragma unroll
+      for (int r = 0; r < 3; ++r) acc.scg[3 * q + r] = acc.scg[3 * q + r] / fn;
+    }
+    store_row<S>(P, o, acc);
   }
   fold_counters(P, n_loc, n_out, n_fail, st);
 }
@@ -2265,8 +2404,14 @@ namespace {
 // Argument checks shared by the point-sample entry points (user points,
 // redshift cones): one sub-box with its vertex densities, the centre method,
 // known fields with their output buffers.
-int check_point_call(dtfe_handle h, const dtfe_interp_opts* o, float* const out[DTFE_NUM_FIELDS], const char* what) {
-  if (o->method != DTFE_METHOD_CENTRE) return set_error(DTFE_ERR_ARG, std::string(what) + " take the centre method");
+int check_point_call(dtfe_handle h, const dtfe_interp_opts* o, float* const out[DTFE_NUM_FIELDS], const char* what,
+                     bool centre_ok = true, bool average_ok = false) {
+  const bool centre = o->method == DTFE_METHOD_CENTRE, average = o->method == DTFE_METHOD_MONTE_CARLO;
+  if (!((centre && centre_ok) || (average && average_ok)))
+    return set_error(DTFE_ERR_ARG, std::string(what) + (average_ok ? (centre_ok ? " take the centre or the Monte-Carlo method"
+                                                                                : " take the Monte-Carlo method")
+                                                                   : " take the centre method"));
+  if (average && o->n_samples < 1) return set_error(DTFE_ERR_ARG, "Monte-Carlo averages need n_samples >= 1");
   if (h->K != 1)
     return set_error(DTFE_ERR_STATE,
                      std::string(what) + " need one sub-box (the reference runs them without the split)");
@@ -2337,11 +2482,30 @@ void launch_points_eval(dtfe_handle h, const InterpParams& P, int64_t n, const S
   }
 }
 
+template <class Src>
+void launch_points_average(dtfe_handle h, const InterpParams& P, int64_t n, const Src& src, int use_bins,
+                           uint64_t key) {
+  const unsigned g = blocks_for(n, 256);
+  cudaStream_t st = h->stream;
+  switch (h->S) {
+    case 0: k_points_average<0, Src><<<g, 256, 0, st>>>(P, n, src, use_bins, key); break;
+    case 1: k_points_average<1, Src><<<g, 256, 0, st>>>(P, n, src, use_bins, key); break;
+    case 2: k_points_average<2, Src><<<g, 256, 0, st>>>(P, n, src, use_bins, key); break;
+    case 3: k_points_average<3, Src><<<g, 256, 0, st>>>(P, n, src, use_bins, key); break;
+    case 4: k_points_average<4, Src><<<g, 256, 0, st>>>(P, n, src, use_bins, key); break;
+    case 5: k_points_average<5, Src><<<g, 256, 0, st>>>(P, n, src, use_bins, key); break;
+    case 6: k_points_average<6, Src><<<g, 256, 0, st>>>(P, n, src, use_bins, key); break;
+    case 7: k_points_average<7, Src><<<g, 256, 0, st>>>(P, n, src, use_bins, key); break;
+    default: k_points_average<8, Src><<<g, 256, 0, st>>>(P, n, src, use_bins, key); break;
+  }
+}
+
 // Per-axis tables of a redshift-cone grid in the reference's float arithmetic
 // (checkAngles, triangulation_miscellaneous.cc:162-197; the bin loops of
 // interpolateRedshiftCone, unaveraged_interpolation.cc:387-447; the checks of
-// src/user_options.cc:1000-1009).  tab: r[n0], st[n1], ct[n1], cp[n2], sp[n2].
-int cone_tables(const float cone[6], const int32_t dims[3], std::vector<float>& tab) {
+// src/user_options.cc:1000-1009).  tab: r[n0], st[n1], ct[n1], cp[n2], sp[n2],
+// theta[n1], psi[n2]; d: the bin sizes (r, theta and psi in radians).
+int cone_tables(const float cone[6], const int32_t dims[3], std::vector<float>& tab, float d[3]) {
   float b[6];
   for (int i = 0; i < 6; ++i) b[i] = cone[i];
   for (int a = 0; a < 3; ++a)
@@ -2356,24 +2520,29 @@ int cone_tables(const float cone[6], const int32_t dims[3], std::vector<float>& 
   float dx[3];
   for (int a = 0; a < 3; ++a) dx[a] = (b[2 * a + 1] - b[2 * a]) / (float)dims[a];
   const size_t n0 = (size_t)dims[0], n1 = (size_t)dims[1], n2 = (size_t)dims[2];
-  tab.assign(n0 + 2 * n1 + 2 * n2, 0.f);
+  tab.assign(n0 + 3 * n1 + 3 * n2, 0.f);
   float* r = tab.data();
   float* st = r + n0;
   float* ct = st + n1;
   float* cp = ct + n1;
   float* sp = cp + n2;
+  float* th = sp + n2;
+  float* ps = th + n1;
   float x = (float)((double)b[0] + (double)dx[0] / 2.);
   for (size_t i = 0; i < n0; ++i, x += dx[0]) r[i] = x;
   x = (float)((double)b[2] + (double)dx[1] / 2.);
   for (size_t j = 0; j < n1; ++j, x += dx[1]) {
+    th[j] = x;
     st[j] = std::sin(x);
     ct[j] = std::cos(x);
   }
   x = (float)((double)b[4] + (double)dx[2] / 2.);
   for (size_t k = 0; k < n2; ++k, x += dx[2]) {
+    ps[k] = x;
     cp[k] = std::cos(x);
     sp[k] = std::sin(x);
   }
+  for (int a = 0; a < 3; ++a) d[a] = dx[a];
   return DTFE_OK;
 }
 
@@ -2430,6 +2599,50 @@ int dtfe_gpu_interpolate_points(dtfe_handle h, int64_t n, const float* xyz, cons
   return read_status(h, nullptr);
 }
 
+int dtfe_gpu_average_points(dtfe_handle h, int64_t n, const float* xyz, const float* delta, const float region[6],
+                            const dtfe_interp_opts* o, float* const out[DTFE_NUM_FIELDS], int64_t* n_out) {
+  if (!h || !o || !region || !out || !n_out || (n > 0 && (!xyz || !delta)) || n < 0)
+    return set_error(DTFE_ERR_ARG, "null argument");
+  int rc = check_point_call(h, o, out, "volume averages at user sampling points", false, true);
+  if (rc) return rc;
+  *n_out = 0;
+  if (n == 0) return DTFE_OK;
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  if ((rc = prepare_centres(h))) return rc;
+  cudaStream_t st = h->stream;
+  const uint32_t F = o->fields;
+  const size_t comps = point_components(h, F);
+  const int64_t nb = (n + kScanBlock - 1) / kScanBlock;
+  // pts_buf: positions, then the cell sizes
+  if ((rc = dev_alloc(h, &h->pts_buf, (size_t)6 * n)) || (rc = dev_alloc(h, &h->pts_keep, (size_t)n)) ||
+      (rc = dev_alloc(h, &h->pts_idx, (size_t)n + 1)) || (rc = dev_alloc(h, &h->pts_blocks, (size_t)nb + 1)) ||
+      (rc = dev_alloc(h, &h->pts_out, std::max<size_t>(comps, 1) * (size_t)n)))
+    return rc;
+  DTFE_CUDA_TRY(cudaMemcpyAsync(h->pts_buf, xyz, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, st));
+  DTFE_CUDA_TRY(cudaMemcpyAsync(h->pts_buf + 3 * n, delta, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, st));
+  Region6 R;
+  for (int c = 0; c < 6; ++c) R.r[c] = region[c];
+  k_points_keep<<<blocks_for(n, 256), 256, 0, st>>>(n, h->pts_buf, R, h->pts_keep);
+  k_scan_blocks<<<(unsigned)nb, kScanBlock, 0, st>>>(n, h->pts_keep, h->pts_idx, h->pts_blocks);
+  k_scan_totals<<<1, kScanBlock, 0, st>>>(nb, h->pts_blocks, h->pts_idx + n);
+  k_scan_add<<<(unsigned)nb, kScanBlock, 0, st>>>(n, h->pts_idx, h->pts_blocks);
+  DTFE_CUDA_TRY(cudaMemsetAsync(h->counters, 0, sizeof(unsigned long long) * CNT_N, st));
+  InterpParams P = point_params(h, o, n);
+  P.NN = o->n_samples;
+  const int use_bins = h->prep_ready && !h->prep_raster ? 1 : 0;
+  PointAvgList src{PointList{h->pts_buf, h->pts_keep, h->pts_idx}, h->pts_buf + 3 * n};
+  // interpolateUserSampling_averaged_2: no partition, so the seed itself
+  launch_points_average(h, P, n, src, use_bins, mc_key(o->seed, -1));
+  DTFE_CUDA_TRY(cudaGetLastError());
+  int64_t m = 0;
+  DTFE_CUDA_TRY(cudaMemcpyAsync(&m, h->pts_idx + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  DTFE_CUDA_TRY(cudaStreamSynchronize(st));
+  if ((rc = copy_point_rows(h, P, F, m, out))) return rc;
+  *n_out = m;
+  h->tet_c_valid = false;
+  return read_status(h, nullptr);
+}
+
 }  // extern "C"
 
 namespace {
@@ -2439,7 +2652,8 @@ namespace {
 int cone_enqueue(dtfe_handle h, const float cone[6], const float origin[3], const int32_t dims[3],
                  const dtfe_interp_opts* o, float* const outp[DTFE_NUM_FIELDS], InterpParams& P) {
   std::vector<float> tab;
-  int rc = cone_tables(cone, dims, tab);
+  float d[3];
+  int rc = cone_tables(cone, dims, tab, d);
   if (rc) return rc;
   const int64_t n = (int64_t)dims[0] * dims[1] * dims[2];
   if ((rc = prepare_centres(h))) return rc;
@@ -2460,6 +2674,19 @@ int cone_enqueue(dtfe_handle h, const float cone[6], const float origin[3], cons
   src.n1 = (uint32_t)dims[1];
   src.n2 = (uint32_t)dims[2];
   const int use_bins = h->prep_ready && !h->prep_raster ? 1 : 0;
+  if (o->method == DTFE_METHOD_MONTE_CARLO) {
+    // interpolateRedshiftCone_averaged_2: no partition, so the seed itself
+    P.NN = o->n_samples;
+    ConeAvgGrid avg;
+    avg.g = src;
+    avg.th = src.sp + dims[2];
+    avg.ps = avg.th + dims[1];
+    for (int a = 0; a < 3; ++a) avg.d[a] = d[a];
+    launch_points_average(h, P, n, avg, use_bins, mc_key(o->seed, -1));
+    DTFE_CUDA_TRY(cudaGetLastError());
+    h->tet_c_valid = false;
+    return DTFE_OK;
+  }
   launch_points_eval(h, P, n, src, use_bins, h->pts_keep);
   DTFE_CUDA_TRY(cudaGetLastError());
   if (!(o->flags & DTFE_FLAG_FIX_OUTSIDE_RASTER)) {
@@ -2479,7 +2706,7 @@ extern "C" {
 int dtfe_gpu_interpolate_cone(dtfe_handle h, const float cone[6], const float origin[3], const int32_t dims[3],
                               const dtfe_interp_opts* o, float* const out[DTFE_NUM_FIELDS]) {
   if (!h || !o || !cone || !origin || !dims || !out) return set_error(DTFE_ERR_ARG, "null argument");
-  int rc = check_point_call(h, o, out, "redshift-cone grids");
+  int rc = check_point_call(h, o, out, "redshift-cone grids", true, true);
   if (rc) return rc;
   for (int a = 0; a < 3; ++a)
     if (dims[a] <= 0) return set_error(DTFE_ERR_ARG, "redshift-cone bins must be positive");
@@ -2503,7 +2730,7 @@ int dtfe_gpu_interpolate_cone(dtfe_handle h, const float cone[6], const float or
 int dtfe_gpu_interpolate_cone_dev(dtfe_handle h, const float cone[6], const float origin[3], const int32_t dims[3],
                                   const dtfe_interp_opts* o, float* const out_dev[DTFE_NUM_FIELDS]) {
   if (!h || !o || !cone || !origin || !dims || !out_dev) return set_error(DTFE_ERR_ARG, "null argument");
-  int rc = check_point_call(h, o, out_dev, "redshift-cone grids");
+  int rc = check_point_call(h, o, out_dev, "redshift-cone grids", true, true);
   if (rc) return rc;
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
   InterpParams P;

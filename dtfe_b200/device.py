@@ -162,10 +162,37 @@ class DeviceDTFE:
                                                      C.byref(m)))
         return {f: a[:m.value] for f, a in res.items()}
 
-    def interpolate_cone(self, fields, cone, origin, dims, fix: bool = False, fix_outside: bool = False) -> dict:
+    def average_points(self, fields, pts: np.ndarray, delta: np.ndarray, region, n_samples: int, seed: int = 0,
+                       fix: bool = False) -> dict:
+        """Monte-Carlo volume averages at user sampling points
+        (dtfe_gpu_average_points): dict field -> float32 array of the points
+        inside `region`, in order."""
+        pts = np.ascontiguousarray(pts, np.float32).reshape(-1, 3)
+        delta = np.ascontiguousarray(delta, np.float32).reshape(-1, 3)
+        if delta.shape != pts.shape:
+            raise ValueError("one delta (3 floats) per point")
+        n = len(pts)
+        reg = np.ascontiguousarray(region, np.float32)
+        outs = [None] * N.NUM_FIELDS
+        res = {}
+        for f in fields:
+            s = N.FIELD_SLOTS[f]
+            nc = N.field_components(s, self.n_scalars)
+            a = np.zeros((n, nc) if nc > 1 else n, np.float32)
+            res[f] = a
+            outs[s] = N.ptr(a)
+        optr = (C.c_void_p * N.NUM_FIELDS)(*outs)
+        o = self._opts(fields, N.METHOD_MONTE_CARLO, n_samples, seed, fix)
+        m = C.c_int64(0)
+        N.check(self.lib.dtfe_gpu_average_points(self.h, n, pts.ctypes.data, delta.ctypes.data, reg.ctypes.data,
+                                                 C.byref(o), optr, C.byref(m)))
+        return {f: a[:m.value] for f, a in res.items()}
+
+    def interpolate_cone(self, fields, cone, origin, dims, fix: bool = False, fix_outside: bool = False,
+                         n_samples: int = 0, seed: int = 0) -> dict:
         """Fields on a redshift-cone grid (dtfe_gpu_interpolate_cone): dict
         field -> float32 array of dims[0] * dims[1] * dims[2] rows, r slowest
-        and psi fastest."""
+        and psi fastest; n_samples > 0 gives the Monte-Carlo bin averages."""
         d = np.ascontiguousarray(dims, np.int32)
         c = np.ascontiguousarray(cone, np.float32)
         org = np.ascontiguousarray(origin, np.float32)
@@ -179,7 +206,10 @@ class DeviceDTFE:
             res[f] = a
             outs[s] = N.ptr(a)
         optr = (C.c_void_p * N.NUM_FIELDS)(*outs)
-        o = self._opts(fields, N.METHOD_CENTRE, 1, 0, fix, fix_outside)
+        if n_samples > 0:
+            o = self._opts(fields, N.METHOD_MONTE_CARLO, n_samples, seed, fix)
+        else:
+            o = self._opts(fields, N.METHOD_CENTRE, 1, 0, fix, fix_outside)
         N.check(self.lib.dtfe_gpu_interpolate_cone(self.h, c.ctypes.data, org.ctypes.data, d.ctypes.data, C.byref(o),
                                                    optr))
         return res

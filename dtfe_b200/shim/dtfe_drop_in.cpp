@@ -23,11 +23,13 @@
 // User sampling points (the samples vector) give uQuantities at the samples
 // inside the box, in order (interpolateUserSampling); a redshift cone
 // (redshiftConeOn) gives them on its gridSize bins (interpolateRedshiftCone).
+// Volume averages there are Monte-Carlo averages, as the reference forces
+// (method 2, 20 points unless noPointsOn; Philox offsets instead of mt19937).
 // Unlike the reference, failures throw std::runtime_error instead of calling
-// exit(), and options this path does not cover throw as well: volume
-// averages at user sampling points or on redshift cones, --region,
+// exit(), and options this path does not cover throw as well: --region,
 // --partition, random subsamples, Poisson particles, explicit padding
-// lengths, scalar fields with NGP/CIC/TSC.  The GPU is device 0 unless DTFE_GPU_DEVICE names another.
+// lengths, scalar fields with NGP/CIC/TSC, NGP/CIC/TSC/SPH at user points or
+// on cones.  The GPU is device 0 unless DTFE_GPU_DEVICE names another.
 
 #include <omp.h>
 
@@ -98,6 +100,19 @@ void outputs(const Field& f, Quantities* q, size_t G, float* out[DTFE_NUM_FIELDS
   set(f.scalar_gradient, DTFE_SCALAR_GRADIENT, f.scalar_gradient ? sized(q->scalar_gradient, G) : nullptr);
 }
 
+// Keeps the first n rows of every selected field (the user samples inside
+// the region).
+void resize_all(const Field& f, Quantities* q, size_t n) {
+  if (f.density) q->density.resize(n);
+  if (f.velocity) q->velocity.resize(n);
+  if (f.velocity_gradient) q->velocity_gradient.resize(n);
+  if (f.velocity_divergence) q->velocity_divergence.resize(n);
+  if (f.velocity_shear) q->velocity_shear.resize(n);
+  if (f.velocity_vorticity) q->velocity_vorticity.resize(n);
+  if (f.scalar) q->scalar.resize(n);
+  if (f.scalar_gradient) q->scalar_gradient.resize(n);
+}
+
 bool any(const Field& f) {
   return f.density || f.velocity || f.velocity_gradient || f.velocity_divergence || f.velocity_shear ||
          f.velocity_vorticity || f.velocity_std || f.scalar || f.scalar_gradient;
@@ -110,8 +125,14 @@ void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& s
   User_options& o = userOptions;
   const bool user_points = !samples.empty() || o.userDefinedSampling;
   const bool cone = o.redshiftConeOn && !user_points;  // user samples switch the cone off (user_options.cc:962-964)
-  unsupported(cone && (o.NGP || o.CIC || o.TSC || o.SPH || any(o.aField)),
-              "volume averages or NGP/CIC/TSC/SPH on redshift-cone grids");
+  unsupported((user_points || cone) && (o.NGP || o.CIC || o.TSC || o.SPH),
+              "NGP/CIC/TSC/SPH at user-defined sampling points or on redshift-cone grids");
+  // volume averages there are Monte-Carlo averages (User_options::updateEntries,
+  // src/user_options.cc:962-983; DTFE() writes the choice back)
+  if ((user_points || cone) && any(o.aField) && o.method != 2) {
+    o.method = 2;
+    if (!o.noPointsOn) o.noPoints = 20;
+  }
   unsupported(cone && (o.redshiftCone.coords.size() != 6 || o.originPosition.size() != 3),
               "redshift cones without 6 limits and a 3-D origin");
   unsupported(o.regionOn, "--region");
@@ -122,8 +143,6 @@ void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& s
               "explicit padding lengths");
   unsupported(o.gridSize.size() != 3, "grids other than 3-D regular grids");
   const bool dtfe = !(o.NGP || o.CIC || o.TSC || o.SPH);
-  unsupported(user_points && (!dtfe || any(o.aField)),
-              "volume averages or NGP/CIC/TSC/SPH at user-defined sampling points");
   unsupported(dtfe && any(o.aField) && (o.method < 1 || o.method > 3), "averaging methods other than 1, 2, 3");
   unsupported(!dtfe && !o.SPH && (o.aField.scalar || o.aField.scalar_gradient), "scalar fields with NGP/CIC/TSC");
 
@@ -215,16 +234,7 @@ void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& s
     int64_t kept = 0;
     check(dtfe_gpu_interpolate_points(gpu.h, (int64_t)m, pts.data(), box, &io, out, &kept),
           "interpolation at user sampling points");
-    Quantities* q = uQuantities;
-    const Field& f = o.uField;
-    if (f.density) q->density.resize(kept);
-    if (f.velocity) q->velocity.resize(kept);
-    if (f.velocity_gradient) q->velocity_gradient.resize(kept);
-    if (f.velocity_divergence) q->velocity_divergence.resize(kept);
-    if (f.velocity_shear) q->velocity_shear.resize(kept);
-    if (f.velocity_vorticity) q->velocity_vorticity.resize(kept);
-    if (f.scalar) q->scalar.resize(kept);
-    if (f.scalar_gradient) q->scalar_gradient.resize(kept);
+    resize_all(o.uField, uQuantities, (size_t)kept);
   } else if (any(o.uField) && cone) {
     // interpolateRedshiftCone: gridSize bins in (r, theta, psi)
     float* out[DTFE_NUM_FIELDS];
@@ -240,7 +250,34 @@ void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& s
     outputs(o.uField, uQuantities, G, out, &io.fields);
     check(dtfe_gpu_interpolate(gpu.h, &io, out, &st), "cell-centre interpolation");
   }
-  if (any(o.aField)) {
+  if (any(o.aField) && (user_points || cone)) {
+    // interpolateUserSampling_averaged_2 / interpolateRedshiftCone_averaged_2
+    // (no velocity standard deviation there)
+    Field f = o.aField;
+    f.velocity_std = false;
+    dtfe_interp_opts io = {DTFE_METHOD_MONTE_CARLO, (int32_t)o.noPoints, (uint64_t)o.randomSeed, 0, 0};
+    float* out[DTFE_NUM_FIELDS];
+    if (user_points) {
+      const size_t m = samples.size();
+      std::vector<float> pts(3 * m), dl(3 * m);
+      for (size_t i = 0; i < m; ++i)
+        for (int c = 0; c < 3; ++c) {
+          pts[3 * i + c] = samples[i].position(c);
+          dl[3 * i + c] = samples[i].delta(c);
+        }
+      outputs(f, aQuantities, m, out, &io.fields);
+      int64_t kept = 0;
+      check(dtfe_gpu_average_points(gpu.h, (int64_t)m, pts.data(), dl.data(), box, &io, out, &kept),
+            "volume averages at user sampling points");
+      resize_all(f, aQuantities, (size_t)kept);
+    } else {
+      outputs(f, aQuantities, G, out, &io.fields);
+      float lim[6], org[3];
+      for (int i = 0; i < 6; ++i) lim[i] = o.redshiftCone.coords[i];
+      for (int i = 0; i < 3; ++i) org[i] = o.originPosition[i];
+      check(dtfe_gpu_interpolate_cone(gpu.h, lim, org, grid, &io, out), "redshift-cone volume averages");
+    }
+  } else if (any(o.aField)) {
     float* out[DTFE_NUM_FIELDS];
     const int method = o.method == 1 ? DTFE_METHOD_TETRAHEDRA
                                      : (o.method == 2 ? DTFE_METHOD_MONTE_CARLO : DTFE_METHOD_EQUIDISTANT);

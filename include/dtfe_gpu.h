@@ -212,6 +212,19 @@ int dtfe_gpu_interpolate_async(dtfe_handle h, const dtfe_interp_opts* opts, floa
  * components (size them for n). */
 int dtfe_gpu_interpolate_points(dtfe_handle h, int64_t n, const float* xyz, const float region[6],
                                 const dtfe_interp_opts* opts, float* const out[DTFE_NUM_FIELDS], int64_t* n_out);
+/* Volume averages at user sampling points (interpolateUserSampling_averaged_2,
+ * averaged_interpolation_2.cc:470-647; the reference switches any averaged
+ * field at user points to this method, src/user_options.cc:962-972): for
+ * every point inside region[6], opts->n_samples points
+ * float(position + u delta) per axis, u in (-0.5, 0.5) (delta: 3 floats per
+ * point, Sample_point::delta), each located and evaluated as a cell centre;
+ * the mean over the samples, those outside the hull counted as zeros.
+ * opts->method must be DTFE_METHOD_MONTE_CARLO; u comes from Philox4x32-10
+ * keyed by opts->seed and counted by (point index, sample), so it is
+ * reproducible but not the reference's mt19937 stream.  No velocity
+ * standard deviation (the reference computes none here). */
+int dtfe_gpu_average_points(dtfe_handle h, int64_t n, const float* xyz, const float* delta, const float region[6],
+                            const dtfe_interp_opts* opts, float* const out[DTFE_NUM_FIELDS], int64_t* n_out);
 /* Fields on a redshift-cone grid (interpolateRedshiftCone,
  * unaveraged_interpolation.cc:381-547; DTFE() runs cones without the sub-box
  * split, src/DTFE.cpp:301).  cone = (r_min, r_max, theta_min, theta_max,
@@ -227,7 +240,13 @@ int dtfe_gpu_interpolate_points(dtfe_handle h, int64_t n, const float* xyz, cons
  * DTFE_FLAG_FIX_OUTSIDE_RASTER advances psi regardless.  Theta limits outside
  * [0, 180] or a psi range of 360 degrees or more are refused (DTFE_ERR_ARG,
  * src/user_options.cc:1000-1009).  The handle must hold one sub-box and its
- * vertex densities; opts->method must be DTFE_METHOD_CENTRE. */
+ * vertex densities.  opts->method DTFE_METHOD_CENTRE gives the bin centres;
+ * DTFE_METHOD_MONTE_CARLO the bin averages of interpolateRedshiftCone_averaged_2
+ * (averaged_interpolation_2.cc:245-466): opts->n_samples points per bin with
+ * r, theta, psi each float(centre + u size), u in (-0.5, 0.5) from Philox
+ * keyed by opts->seed and counted by (bin, sample), sin and cos of the random
+ * angles in double rounded to float; outside points count as zeros; no stuck
+ * psi there (the reference's averaged loop has none). */
 int dtfe_gpu_interpolate_cone(dtfe_handle h, const float cone[6], const float origin[3], const int32_t dims[3],
                               const dtfe_interp_opts* opts, float* const out[DTFE_NUM_FIELDS]);
 /* Same, writing into device buffers (dims[0] dims[1] dims[2] rows each). */

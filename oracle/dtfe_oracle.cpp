@@ -741,6 +741,203 @@ int oracle_interpolate_cone(int64_t T, const int32_t* tv, const int32_t* tn, int
   return DTFE_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Monte-Carlo average of one point sample (averaged_interpolation_2.cc:
+// 343-418, 540-637): the centre located from `hint` (its tetrahedron, when
+// inside, seeds the sample walks as the reference's `previous`), NN points
+// from sample(w, u, q) with u the Philox offsets of (key, index, w), each
+// located and evaluated, summed in float (mode 0) or double (mode 1) in
+// sample order, outside points skipped but counted; the mean and its derived
+// fields written to row m.  Returns -2 on a walk failure.
+template <class Sample>
+int average_row(const Tess& g, const float* dens32, const double* dens64, const float centre[3], Sample sample,
+                uint64_t key, uint64_t index, int NN, int mode, bool fix, bool want_vel, bool want_sc,
+                int64_t& hint, int64_t lo, int64_t hi, uint32_t fields, double* const out[DTFE_NUM_FIELDS],
+                int64_t m) {
+  const int S = g.S;
+  auto has = [&](int s) { return (fields & DTFE_FIELD_BIT(s)) != 0 && out[s] != nullptr; };
+  float fD = 0.f, fV[3] = {0, 0, 0}, fG[9] = {0}, fS[DTFE_MAX_SCALARS] = {0}, fSG[3 * DTFE_MAX_SCALARS] = {0};
+  double dD = 0, dV[3] = {0, 0, 0}, dG[9] = {0}, dS[DTFE_MAX_SCALARS] = {0}, dSG[3 * DTFE_MAX_SCALARS] = {0};
+  if (hi > lo) {
+    const double pc[3] = {(double)centre[0], (double)centre[1], (double)centre[2]};
+    const int64_t tc = locate(g, pc, hint, lo, hi);
+    if (tc == -2) return -2;
+    if (tc >= 0) hint = tc;
+    for (int w = 0; w < NN; ++w) {
+      double u[3];
+      dtfe::mc_offsets(key, index, (uint32_t)w, u);
+      float q[3];
+      sample(u, q);
+      const double p[3] = {(double)q[0], (double)q[1], (double)q[2]};
+      const int64_t t = locate(g, p, hint, lo, hi);
+      if (t == -2) return -2;
+      if (t < 0) continue;
+      CellEval e{};
+      eval_cell(g, dens32, dens64, t, p, mode, fix, want_vel, want_sc, e);
+      if (mode == 0) {
+        fD += (float)e.dens;
+        for (int c = 0; c < 3; ++c) fV[c] += (float)e.vel[c];
+        for (int c = 0; c < 9; ++c) fG[c] += (float)e.grad[c];
+        for (int k = 0; k < S; ++k) {
+          fS[k] += (float)e.sc[k];
+          for (int c = 0; c < 3; ++c) fSG[3 * k + c] += (float)e.scg[3 * k + c];
+        }
+      } else {
+        dD += e.dens;
+        for (int c = 0; c < 3; ++c) dV[c] += e.vel[c];
+        for (int c = 0; c < 9; ++c) dG[c] += e.grad[c];
+        for (int k = 0; k < S; ++k) {
+          dS[k] += e.sc[k];
+          for (int c = 0; c < 3; ++c) dSG[3 * k + c] += e.scg[3 * k + c];
+        }
+      }
+    }
+  }
+  double D, Vv[3], Gg[9], Ss[DTFE_MAX_SCALARS], SGg[3 * DTFE_MAX_SCALARS];
+  if (mode == 0) {
+    const float fn = (float)NN;
+    D = (double)(fD / fn);
+    for (int c = 0; c < 3; ++c) Vv[c] = (double)(fV[c] / fn);
+    for (int c = 0; c < 9; ++c) Gg[c] = (double)(fG[c] / fn);
+    for (int k = 0; k < S; ++k) {
+      Ss[k] = (double)(fS[k] / fn);
+      for (int c = 0; c < 3; ++c) SGg[3 * k + c] = (double)(fSG[3 * k + c] / fn);
+    }
+  } else {
+    D = dD / NN;
+    for (int c = 0; c < 3; ++c) Vv[c] = dV[c] / NN;
+    for (int c = 0; c < 9; ++c) Gg[c] = dG[c] / NN;
+    for (int k = 0; k < S; ++k) {
+      Ss[k] = dS[k] / NN;
+      for (int c = 0; c < 3; ++c) SGg[3 * k + c] = dSG[3 * k + c] / NN;
+    }
+  }
+  if (has(DTFE_DENSITY)) out[DTFE_DENSITY][m] = D;
+  if (has(DTFE_VELOCITY))
+    for (int c = 0; c < 3; ++c) out[DTFE_VELOCITY][3 * m + c] = Vv[c];
+  if (has(DTFE_VELOCITY_GRADIENT))
+    for (int c = 0; c < 9; ++c) out[DTFE_VELOCITY_GRADIENT][9 * m + c] = Gg[c];
+  if (has(DTFE_VELOCITY_DIVERGENCE) || has(DTFE_VELOCITY_SHEAR) || has(DTFE_VELOCITY_VORTICITY)) {
+    double dv, sh[5], vo[3];
+    derived(Gg, mode, &dv, sh, vo);
+    if (has(DTFE_VELOCITY_DIVERGENCE)) out[DTFE_VELOCITY_DIVERGENCE][m] = dv;
+    if (has(DTFE_VELOCITY_SHEAR))
+      for (int c = 0; c < 5; ++c) out[DTFE_VELOCITY_SHEAR][5 * m + c] = sh[c];
+    if (has(DTFE_VELOCITY_VORTICITY))
+      for (int c = 0; c < 3; ++c) out[DTFE_VELOCITY_VORTICITY][3 * m + c] = vo[c];
+  }
+  if (has(DTFE_SCALAR))
+    for (int c = 0; c < S; ++c) out[DTFE_SCALAR][(int64_t)S * m + c] = Ss[c];
+  if (has(DTFE_SCALAR_GRADIENT))
+    for (int c = 0; c < 3 * S; ++c) out[DTFE_SCALAR_GRADIENT][(int64_t)3 * S * m + c] = SGg[c];
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Volume averages at user sampling points: interpolateUserSampling_averaged_2
+// (averaged_interpolation_2.cc:470-647).  Points outside `region` (closed)
+// dropped; for each kept point i, NN points float(position + u delta) per
+// axis (:545-553), u the Philox offsets of (seed, i, w) in place of the
+// reference's mt19937 stream (seed + 1000 partNo with partNo = -1 here).
+int oracle_average_points(int64_t T, const int32_t* tv, const int32_t* tn, int64_t V, const float* xyz,
+                          const float* vel, const float* scal, int S, const float* dens32, const double* dens64,
+                          int64_t lo, int64_t hi, int64_t n, const float* pts, const float* delta,
+                          const float region[6], uint32_t fields, int NN, uint64_t seed, int mode, int fix,
+                          double* const out[DTFE_NUM_FIELDS], int64_t* n_out) {
+  Tess g{T, V, tv, tn, xyz, vel, scal, S};
+  if ((fields & DTFE_FIELD_BIT(DTFE_VELOCITY_STD)) || NN < 1) return DTFE_ERR_ARG;
+  const bool want_vel = (fields & (DTFE_FIELD_BIT(DTFE_VELOCITY) | DTFE_FIELD_BIT(DTFE_VELOCITY_GRADIENT) |
+                                   DTFE_FIELD_BIT(DTFE_VELOCITY_DIVERGENCE) | DTFE_FIELD_BIT(DTFE_VELOCITY_SHEAR) |
+                                   DTFE_FIELD_BIT(DTFE_VELOCITY_VORTICITY))) != 0;
+  const bool want_sc = (fields & (DTFE_FIELD_BIT(DTFE_SCALAR) | DTFE_FIELD_BIT(DTFE_SCALAR_GRADIENT))) != 0;
+  const uint64_t key = dtfe::mc_key(seed, -1);
+  int64_t m = 0, hint = lo;
+  for (int64_t i = 0; i < n; ++i) {
+    const float* q = pts + 3 * i;
+    bool in = true;
+    for (int c = 0; c < 3; ++c) in = in && q[c] >= region[2 * c] && q[c] <= region[2 * c + 1];
+    if (!in) continue;
+    const float* dl = delta + 3 * i;
+    auto sample = [&](const double u[3], float r[3]) {
+      for (int c = 0; c < 3; ++c) r[c] = (float)((double)q[c] + u[c] * (double)dl[c]);
+    };
+    if (average_row(g, dens32, dens64, q, sample, key, (uint64_t)i, NN, mode, fix != 0, want_vel, want_sc, hint,
+                    lo, hi, fields, out, m))
+      return DTFE_ERR_WALK;
+    ++m;
+  }
+  *n_out = m;
+  return DTFE_OK;
+}
+
+// Volume averages on a redshift-cone grid: interpolateRedshiftCone_averaged_2
+// (averaged_interpolation_2.cc:245-466).  Bin (i, j, k) centred at the
+// oracle_cone_tables values; NN points with r, theta, psi each
+// float(centre + u size) (:360-362), sin and cos of the angles evaluated in
+// double and rounded to float, then o + (r st) cp ... in float; u the Philox
+// offsets of (seed, bin, w).  No stuck psi (the averaged loop has no
+// `continue` before its psi += dx).
+int oracle_average_cone(int64_t T, const int32_t* tv, const int32_t* tn, int64_t V, const float* xyz,
+                        const float* vel, const float* scal, int S, const float* dens32, const double* dens64,
+                        int64_t lo, int64_t hi, const float cone[6], const float origin[3], const int32_t dims[3],
+                        uint32_t fields, int NN, uint64_t seed, int mode, int fix,
+                        double* const out[DTFE_NUM_FIELDS]) {
+  Tess g{T, V, tv, tn, xyz, vel, scal, S};
+  if ((fields & DTFE_FIELD_BIT(DTFE_VELOCITY_STD)) || NN < 1) return DTFE_ERR_ARG;
+  std::vector<float> r(dims[0] > 0 ? dims[0] : 1), st(dims[1] > 0 ? dims[1] : 1), ct(st.size()),
+      cp(dims[2] > 0 ? dims[2] : 1), sp(cp.size());
+  int rc = oracle_cone_tables(cone, dims, r.data(), st.data(), ct.data(), cp.data(), sp.data());
+  if (rc) return rc;
+  // the bin centres and sizes of the angles, as oracle_cone_tables computes them
+  float b[6];
+  for (int i = 0; i < 6; ++i) b[i] = cone[i];
+  b[4] -= std::floor(b[4] / 360.f) * 360.f;
+  b[5] -= std::floor(b[5] / 360.f) * 360.f;
+  if (b[4] > b[5]) b[5] += 360.f;
+  const float rad = (float)(3.14159265 / 180.);
+  for (int i = 2; i < 6; ++i) b[i] *= rad;
+  float dx[3];
+  for (int a = 0; a < 3; ++a) dx[a] = (b[2 * a + 1] - b[2 * a]) / (float)dims[a];
+  std::vector<float> th(dims[1]), ps(dims[2]);
+  float x = (float)((double)b[2] + (double)dx[1] / 2.);
+  for (int j = 0; j < dims[1]; ++j, x += dx[1]) th[j] = x;
+  x = (float)((double)b[4] + (double)dx[2] / 2.);
+  for (int k = 0; k < dims[2]; ++k, x += dx[2]) ps[k] = x;
+  const bool want_vel = (fields & (DTFE_FIELD_BIT(DTFE_VELOCITY) | DTFE_FIELD_BIT(DTFE_VELOCITY_GRADIENT) |
+                                   DTFE_FIELD_BIT(DTFE_VELOCITY_DIVERGENCE) | DTFE_FIELD_BIT(DTFE_VELOCITY_SHEAR) |
+                                   DTFE_FIELD_BIT(DTFE_VELOCITY_VORTICITY))) != 0;
+  const bool want_sc = (fields & (DTFE_FIELD_BIT(DTFE_SCALAR) | DTFE_FIELD_BIT(DTFE_SCALAR_GRADIENT))) != 0;
+  const uint64_t key = dtfe::mc_key(seed, -1);
+  int64_t m = 0, hint = lo;
+  for (int i = 0; i < dims[0]; ++i)
+    for (int j = 0; j < dims[1]; ++j)
+      for (int k = 0; k < dims[2]; ++k, ++m) {
+        const float rs = r[i] * st[j];
+        const float centre[3] = {origin[0] + rs * cp[k], origin[1] + rs * sp[k], origin[2] + r[i] * ct[j]};
+        auto sample = [&](const double u[3], float q[3]) {
+          const float R = (float)((double)r[i] + u[0] * (double)dx[0]);
+          const float Th = (float)((double)th[j] + u[1] * (double)dx[1]);
+          const float Ps = (float)((double)ps[k] + u[2] * (double)dx[2]);
+          const float s1 = (float)std::sin((double)Th), c1 = (float)std::cos((double)Th);
+          const float c2 = (float)std::cos((double)Ps), s2 = (float)std::sin((double)Ps);
+          const float rr = R * s1;
+          q[0] = origin[0] + rr * c2;
+          q[1] = origin[1] + rr * s2;
+          q[2] = origin[2] + R * c1;
+        };
+        if (average_row(g, dens32, dens64, centre, sample, key, (uint64_t)m, NN, mode, fix != 0, want_vel, want_sc,
+                        hint, lo, hi, fields, out, m))
+          return DTFE_ERR_WALK;
+      }
+  return DTFE_OK;
+}
+
 // Averaging method 1: interpolateGrid_averaged_1
 // (src/CGAL_triangulation/averaged_interpolation_1.cc:197-421), per sub-box
 // over its tetrahedra in order.

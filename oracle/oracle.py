@@ -57,6 +57,12 @@ def lib() -> C.CDLL:
         L.oracle_interpolate_cone.argtypes = [C.c_int64, vp, vp, C.c_int64, vp, vp, vp, C.c_int, vp, vp,
                                               C.c_int64, C.c_int64, vp, vp, vp, C.c_uint32, C.c_int, C.c_int,
                                               C.c_int, C.POINTER(C.c_void_p)]
+        L.oracle_average_points.argtypes = [C.c_int64, vp, vp, C.c_int64, vp, vp, vp, C.c_int, vp, vp, C.c_int64,
+                                            C.c_int64, C.c_int64, vp, vp, vp, C.c_uint32, C.c_int, C.c_uint64,
+                                            C.c_int, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]
+        L.oracle_average_cone.argtypes = [C.c_int64, vp, vp, C.c_int64, vp, vp, vp, C.c_int, vp, vp, C.c_int64,
+                                          C.c_int64, vp, vp, vp, C.c_uint32, C.c_int, C.c_uint64, C.c_int, C.c_int,
+                                          C.POINTER(C.c_void_p)]
         L.oracle_sobol_simplex.argtypes = [C.c_int64, vp]
         L.oracle_sobol_simplex.restype = None
         _lib = L
@@ -316,6 +322,66 @@ def interpolate_cone(plan, dens32, dens64, fields, cone, origin, dims, mode: int
                                        d.ctypes.data, mask, mode, 1 if fix else 0, 1 if fix_outside else 0, optr)
     if rc:
         raise RuntimeError(f"oracle_interpolate_cone failed with status {rc}")
+    return arrs
+
+
+def _outputs(fields, n, S):
+    mask = 0
+    outs = [None] * N.NUM_FIELDS
+    arrs = {}
+    for f in fields:
+        s = N.FIELD_SLOTS[f]
+        mask |= 1 << s
+        nc = N.field_components(s, S)
+        a = np.zeros((n, nc) if nc > 1 else n, np.float64)
+        arrs[f] = a
+        outs[s] = a.ctypes.data
+    return mask, (C.c_void_p * N.NUM_FIELDS)(*[o if o else None for o in outs]), arrs
+
+
+def average_points(plan, dens32, dens64, fields, pts, delta, region, n_samples: int, seed: int = 0,
+                   mode: int = MODE_REF, fix: bool = False, box: int = 0):
+    """Monte-Carlo volume averages at user sampling points
+    (interpolateUserSampling_averaged_2) with the Philox offsets: dict field
+    -> float64 array of the points inside `region`, in order."""
+    pts = np.ascontiguousarray(pts, np.float32)
+    delta = np.ascontiguousarray(delta, np.float32)
+    n = len(pts)
+    mask, optr, arrs = _outputs(fields, n, plan.n_scalars)
+    vel = plan.velocity.ctypes.data if plan.velocity is not None else None
+    sc = plan.scalar.ctypes.data if plan.scalar is not None else None
+    b = plan.boxes[box]
+    reg = np.ascontiguousarray(region, np.float32)
+    n_out = C.c_int64(0)
+    rc = lib().oracle_average_points(plan.n_tets, plan.tet_v.ctypes.data, plan.tet_n.ctypes.data, plan.n_verts,
+                                     plan.xyz.ctypes.data, vel, sc, plan.n_scalars, dens32.ctypes.data,
+                                     dens64.ctypes.data, b.tet_offset, b.tet_offset + b.n_tets, n, pts.ctypes.data,
+                                     delta.ctypes.data, reg.ctypes.data, mask, n_samples, seed, mode,
+                                     1 if fix else 0, optr, C.byref(n_out))
+    if rc:
+        raise RuntimeError(f"oracle_average_points failed with status {rc}")
+    return {f: a[:n_out.value] for f, a in arrs.items()}
+
+
+def average_cone(plan, dens32, dens64, fields, cone, origin, dims, n_samples: int, seed: int = 0,
+                 mode: int = MODE_REF, fix: bool = False, box: int = 0):
+    """Monte-Carlo bin averages on a redshift-cone grid
+    (interpolateRedshiftCone_averaged_2) with the Philox offsets: dict field
+    -> float64 array of dims[0] * dims[1] * dims[2] rows."""
+    n = int(np.prod(dims))
+    mask, optr, arrs = _outputs(fields, n, plan.n_scalars)
+    vel = plan.velocity.ctypes.data if plan.velocity is not None else None
+    sc = plan.scalar.ctypes.data if plan.scalar is not None else None
+    b = plan.boxes[box]
+    c = np.ascontiguousarray(cone, np.float32)
+    o = np.ascontiguousarray(origin, np.float32)
+    d = np.ascontiguousarray(dims, np.int32)
+    rc = lib().oracle_average_cone(plan.n_tets, plan.tet_v.ctypes.data, plan.tet_n.ctypes.data, plan.n_verts,
+                                   plan.xyz.ctypes.data, vel, sc, plan.n_scalars, dens32.ctypes.data,
+                                   dens64.ctypes.data, b.tet_offset, b.tet_offset + b.n_tets, c.ctypes.data,
+                                   o.ctypes.data, d.ctypes.data, mask, n_samples, seed, mode, 1 if fix else 0, optr)
+    if rc:
+        raise RuntimeError(f"oracle_average_cone failed with status {rc}")
     return arrs
 
 

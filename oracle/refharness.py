@@ -135,6 +135,46 @@ def run_cone(plan, cone, origin, dims, dens, box: int = 0, timing: bool = False)
     return (out, secs.value) if timing else out
 
 
+def run_average(plan, dens, n_samples: int, seed: int, pts=None, delta=None, region=None, cone=None, origin=None,
+                dims=None, box: int = 0):
+    """The reference's Monte-Carlo averages (its own mt19937 stream): at user
+    points (interpolateUserSampling_averaged_2; pts, delta, region) or on a
+    redshift cone (interpolateRedshiftCone_averaged_2; cone, origin, dims).
+    Dict of density, velocity, gradient, scalar, scalar gradient rows."""
+    xyz, w, vel, tv, tn, _, _ = _box_args(plan, box)
+    b = plan.boxes[box]
+    v0, nv = b.vert_offset, b.n_verts
+    sc = None if plan.scalar is None else np.ascontiguousarray(plan.scalar[v0:v0 + nv, 0])
+    d = np.ascontiguousarray(dens[v0:v0 + nv], np.float32)
+    which = 0 if pts is not None else 1
+    n = len(pts) if which == 0 else int(np.prod(dims))
+    out = {"density": np.zeros(n, np.float32), "velocity": np.zeros((n, 3), np.float32),
+           "velocity_gradient": np.zeros((n, 9), np.float32), "scalar": np.zeros(n, np.float32),
+           "scalar_gradient": np.zeros((n, 3), np.float32)}
+    f32 = lambda a, k: np.ascontiguousarray(a if a is not None else np.zeros(k), np.float32)
+    P = f32(pts, 3)
+    D = f32(delta, 3)
+    R = f32(region, 6)
+    Cn = f32(cone, 6)
+    O = f32(origin, 3)
+    Dm = np.ascontiguousarray(dims if dims is not None else (1, 1, 1), np.int32)
+    L = lib()
+    vp = C.c_void_p
+    L.ref_average_samples.argtypes = [C.c_int, C.c_int64, vp, vp, vp, vp, C.c_int64, vp, vp, vp, C.c_int64, vp, vp,
+                                      vp, vp, vp, C.c_int, C.c_uint64, vp, vp, vp, vp, vp, vp,
+                                      C.POINTER(C.c_int64)]
+    p = lambda a: None if a is None else a.ctypes.data
+    m = C.c_int64(0)
+    rc = L.ref_average_samples(which, len(xyz), p(xyz), p(w), p(vel), p(sc), len(tv), p(tv), p(tn), p(R),
+                               n if which == 0 else 0, p(P), p(D), p(Cn), p(O), p(Dm), n_samples, seed, p(d),
+                               p(out["density"]), p(out["velocity"]), p(out["velocity_gradient"]),
+                               p(out["scalar"]) if sc is not None else None,
+                               p(out["scalar_gradient"]) if sc is not None else None, C.byref(m))
+    if rc:
+        raise RuntimeError(f"ref_average_samples failed ({rc})")
+    return {k: a[:m.value] for k, a in out.items()}
+
+
 def _box_args(plan, box):
     b = plan.boxes[box]
     v0, nv, t0, nt = b.vert_offset, b.n_verts, b.tet_offset, b.n_tets

@@ -107,12 +107,15 @@ int dropin_run(int estimator, const float* pos, const float* w, const float* vel
   return 0;
 }
 
-// DTFE() with user sampling points (n_samples, xyz 3 each) for the fields
-// u_fields: *n_kept rows (the samples inside the box) land in u_out.
+// DTFE() with user sampling points (n_samples, xyz 3 each, cell sizes sdelta
+// 3 each or NULL) for the fields u_fields / a_fields: *n_kept rows (the
+// samples inside the box) land in u_out / a_out.  n_points >= 0 sets
+// noPoints (noPointsOn), seed randomSeed.
 int dropin_run_points(const float* pos, const float* w, const float* vel, const float* scal, int64_t n,
                       const float box[6], int periodic, const int32_t grid[3], double average_density,
                       uint32_t u_fields, int64_t n_samples, const float* sxyz, int n_threads, float* const* u_out,
-                      int64_t* n_kept) {
+                      int64_t* n_kept, uint32_t a_fields, const float* sdelta, int n_points, uint64_t seed,
+                      float* const* a_out) {
   std::vector<Particle_data> p(n);
   for (int64_t i = 0; i < n; ++i) {
     for (int c = 0; c < 3; ++c) p[i].pos[c] = pos[3 * i + c];
@@ -127,11 +130,21 @@ int dropin_run_points(const float* pos, const float* w, const float* vel, const 
   o.averageDensity = (Real)average_density;
   o.userDefinedSampling = true;
   set_fields(o.uField, u_fields);
+  set_fields(o.aField, a_fields);
+  if (n_points >= 0) {
+    o.noPoints = n_points;
+    o.noPointsOn = true;
+  }
+  o.randomSeed = (size_t)seed;
   if (n_threads > 0) omp_set_num_threads(n_threads);
   std::vector<Sample_point> samples((size_t)n_samples);
   for (int64_t i = 0; i < n_samples; ++i) {
     float q[3] = {sxyz[3 * i], sxyz[3 * i + 1], sxyz[3 * i + 2]};
     samples[i].setPosition(q);
+    if (sdelta) {
+      float d[3] = {sdelta[3 * i], sdelta[3 * i + 1], sdelta[3 * i + 2]};
+      samples[i].setDelta(d);
+    }
   }
   Quantities uq, aq;
   try {
@@ -140,19 +153,21 @@ int dropin_run_points(const float* pos, const float* w, const float* vel, const 
     g_error = e.what();
     return 1;
   }
-  const size_t m = uq.density.size() ? uq.density.size() : uq.velocity.size();
+  size_t m = uq.density.size() ? uq.density.size() : uq.velocity.size();
+  if (!u_fields) m = aq.density.size() ? aq.density.size() : aq.velocity.size();
   *n_kept = (int64_t)m;
   copy_all(uq, u_out, m);
+  copy_all(aq, a_out, m);
   return 0;
 }
 
 // DTFE() on a redshift-cone grid: cone = (r_min, r_max, theta_min,
 // theta_max, psi_min, psi_max), origin = the apex, grid = bins in r, theta,
-// psi; u_out receive grid[0] grid[1] grid[2] rows.
+// psi; u_out / a_out receive grid[0] grid[1] grid[2] rows.
 int dropin_run_cone(const float* pos, const float* w, const float* vel, const float* scal, int64_t n,
                     const float box[6], int periodic, const int32_t grid[3], double average_density,
                     uint32_t u_fields, const float cone[6], const float origin[3], int n_threads,
-                    float* const* u_out) {
+                    float* const* u_out, uint32_t a_fields, int n_points, uint64_t seed, float* const* a_out) {
   std::vector<Particle_data> p(n);
   for (int64_t i = 0; i < n; ++i) {
     for (int c = 0; c < 3; ++c) p[i].pos[c] = pos[3 * i + c];
@@ -169,6 +184,12 @@ int dropin_run_cone(const float* pos, const float* w, const float* vel, const fl
   o.redshiftCone.coords.assign(cone, cone + 6);
   o.originPosition.assign(origin, origin + 3);
   set_fields(o.uField, u_fields);
+  set_fields(o.aField, a_fields);
+  if (n_points >= 0) {
+    o.noPoints = n_points;
+    o.noPointsOn = true;
+  }
+  o.randomSeed = (size_t)seed;
   if (n_threads > 0) omp_set_num_threads(n_threads);
   std::vector<Sample_point> samples;
   Quantities uq, aq;
@@ -179,6 +200,7 @@ int dropin_run_cone(const float* pos, const float* w, const float* vel, const fl
     return 1;
   }
   copy_all(uq, u_out, (size_t)grid[0] * grid[1] * grid[2]);
+  copy_all(aq, a_out, (size_t)grid[0] * grid[1] * grid[2]);
   return 0;
 }
 

@@ -12,6 +12,8 @@
 //   interpolateGrid_averaged_3  averaged_interpolation_2.cc:664-866
 //   interpolateUserSampling     unaveraged_interpolation.cc:560-691
 //   interpolateRedshiftCone     unaveraged_interpolation.cc:381-547
+//   interpolateUserSampling_averaged_2, interpolateRedshiftCone_averaged_2
+//                               averaged_interpolation_2.cc:245-647
 //   interpolateGrid_averaged_1  averaged_interpolation_1.cc:197-421 (Sobol points
 //                               from dtfe_b200/csrc/sobol.h behind the GSL API)
 //
@@ -44,6 +46,9 @@ void interpolateGrid_averaged_1(DT& dt, User_options& userOptions, Quantities* q
 void interpolateUserSampling(DT& dt, std::vector<Sample_point>& samples, User_options& userOptions,
                              Quantities* quantities);
 void interpolateRedshiftCone(DT& dt, User_options& userOptions, Quantities* quantities);
+void interpolateUserSampling_averaged_2(DT& dt, std::vector<Sample_point>& samples, User_options& userOptions,
+                                        Quantities* quantities);
+void interpolateRedshiftCone_averaged_2(DT& dt, User_options& userOptions, Quantities* quantities);
 
 User_options::User_options() {
   periodic = false;
@@ -268,6 +273,67 @@ int ref_interpolate_cone(int64_t nv, const float* xyz, const float* w, const flo
   interpolateRedshiftCone(dt, opt, &q);
   if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   const size_t m = (size_t)dims[0] * dims[1] * dims[2];
+  if (out_density && q.density.size() == m) std::memcpy(out_density, q.density.data(), m * sizeof(float));
+  if (out_velocity && q.velocity.size() == m) std::memcpy(out_velocity, q.velocity.data(), 3 * m * sizeof(float));
+  if (out_gradient && q.velocity_gradient.size() == m)
+    std::memcpy(out_gradient, q.velocity_gradient.data(), 9 * m * sizeof(float));
+  if (out_scalar && q.scalar.size() == m) std::memcpy(out_scalar, q.scalar.data(), m * sizeof(float));
+  if (out_scalar_gradient && q.scalar_gradient.size() == m)
+    std::memcpy(out_scalar_gradient, q.scalar_gradient.data(), 3 * m * sizeof(float));
+  return 0;
+}
+
+// The reference's Monte-Carlo averages at user points (which 0: samples xyz
+// with cell sizes delta, n of them; region = the kept box) or on a redshift
+// cone (which 1: cone, origin, dims), noPoints = NN, randomSeed = seed, on one
+// tessellation with LOCAL indices and the given vertex densities.  Outputs
+// as ref_interpolate_points / ref_interpolate_cone; *n_out = rows written.
+int ref_average_samples(int which, int64_t nv, const float* xyz, const float* w, const float* vel,
+                        const float* scal, int64_t nt, const int32_t* tv, const int32_t* tn, const float region[6],
+                        int64_t n, const float* pts, const float* delta, const float cone[6], const float origin[3],
+                        const int32_t dims[3], int NN, uint64_t seed, const float* dens, float* out_density,
+                        float* out_velocity, float* out_gradient, float* out_scalar, float* out_scalar_gradient,
+                        int64_t* n_out) {
+  DT dt;
+  const std::vector<DT::Vertex*>& verts = dt.load_flat(nv, xyz, nt, tv, tn);
+  for (int64_t i = 0; i < nv; ++i) {
+    vertexData& d = verts[i]->info();
+    d.weight() = w[i];
+    for (int c = 0; c < 3; ++c) d.velocity(c) = vel ? vel[3 * i + c] : 0.f;
+    d.scalar(0) = scal ? scal[i] : 0.f;
+    d.setDensity(dens[i]);
+  }
+  User_options opt;
+  opt.noPoints = NN;
+  opt.randomSeed = (size_t)seed;
+  Field f;
+  f.density = out_density != nullptr;
+  f.velocity = out_velocity != nullptr;
+  f.velocity_gradient = out_gradient != nullptr;
+  f.scalar = out_scalar != nullptr;
+  f.scalar_gradient = out_scalar_gradient != nullptr;
+  opt.aField = f;
+  Quantities q;
+  if (which == 0) {
+    opt.region.coords.assign(region, region + 6);
+    opt.userDefinedSampling = true;
+    std::vector<Sample_point> samples((size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
+      float p[3] = {pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
+      float dl[3] = {delta[3 * i], delta[3 * i + 1], delta[3 * i + 2]};
+      samples[i].setPosition(p);
+      samples[i].setDelta(dl);
+    }
+    interpolateUserSampling_averaged_2(dt, samples, opt, &q);
+  } else {
+    opt.redshiftConeOn = true;
+    opt.redshiftCone.coords.assign(cone, cone + 6);
+    opt.originPosition.assign(origin, origin + 3);
+    opt.gridSize.assign({(size_t)dims[0], (size_t)dims[1], (size_t)dims[2]});
+    interpolateRedshiftCone_averaged_2(dt, opt, &q);
+  }
+  const size_t m = f.density ? q.density.size() : (f.velocity ? q.velocity.size() : q.velocity_gradient.size());
+  *n_out = (int64_t)m;
   if (out_density && q.density.size() == m) std::memcpy(out_density, q.density.data(), m * sizeof(float));
   if (out_velocity && q.velocity.size() == m) std::memcpy(out_velocity, q.velocity.data(), 3 * m * sizeof(float));
   if (out_gradient && q.velocity_gradient.size() == m)

@@ -28,9 +28,10 @@ def lib():
                                  C.c_uint32, C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_int, vp, vp,
                                  C.POINTER(C.c_double), C.POINTER(C.c_int64)]
         L.dropin_run_points.argtypes = [vp, vp, vp, vp, C.c_int64, vp, C.c_int, vp, C.c_double, C.c_uint32,
-                                        C.c_int64, vp, C.c_int, vp, C.POINTER(C.c_int64)]
+                                        C.c_int64, vp, C.c_int, vp, C.POINTER(C.c_int64), C.c_uint32, vp, C.c_int,
+                                        C.c_uint64, vp]
         L.dropin_run_cone.argtypes = [vp, vp, vp, vp, C.c_int64, vp, C.c_int, vp, C.c_double, C.c_uint32, vp, vp,
-                                      C.c_int, vp]
+                                      C.c_int, vp, C.c_uint32, C.c_int, C.c_uint64, vp]
         L.dropin_error.restype = C.c_char_p
         _lib = L
     return _lib
@@ -68,36 +69,48 @@ def run(estimator, pos, w, vel, scal, grid, box=(0, 100, 0, 100, 0, 100), period
 
 
 def run_points(pos, w, vel, scal, grid, samples, box=(0, 100, 0, 100, 0, 100), periodic=True,
-               average_density=-1.0, u_fields=("density",), n_threads=4):
+               average_density=-1.0, u_fields=("density",), n_threads=4, a_fields=(), delta=None, n_points=-1,
+               seed=0):
     """DTFE() with user sampling points: dict field -> rows of the samples
-    inside the box, in order."""
+    inside the box, in order (with a_fields: (u dict, a dict))."""
     pos = np.ascontiguousarray(pos, np.float32)
     samples = np.ascontiguousarray(samples, np.float32)
     m = len(samples)
     d = {f: np.full((m, NCOMP[SLOTS[f]]), np.nan, np.float32) for f in u_fields}
+    da = {f: np.full((m, NCOMP[SLOTS[f]]), np.nan, np.float32) for f in a_fields}
     ptrs = (C.c_void_p * 9)(*[d[f].ctypes.data if f in d else None for f in SLOTS])
+    aptrs = (C.c_void_p * 9)(*[da[f].ctypes.data if f in da else None for f in SLOTS])
     mask = sum(1 << SLOTS[f] for f in u_fields)
+    amask = sum(1 << SLOTS[f] for f in a_fields)
     g = np.ascontiguousarray(grid, np.int32)
     bx = np.ascontiguousarray(box, np.float32)
+    dl = np.ascontiguousarray(delta, np.float32) if delta is not None else None
     keep = [np.ascontiguousarray(a, np.float32) if a is not None else None for a in (w, vel, scal)]
     kept = C.c_int64()
     rc = lib().dropin_run_points(pos.ctypes.data, *[a.ctypes.data if a is not None else None for a in keep],
                                  len(pos), bx.ctypes.data, int(periodic), g.ctypes.data, float(average_density),
-                                 mask, m, samples.ctypes.data, n_threads, ptrs, C.byref(kept))
+                                 mask, m, samples.ctypes.data, n_threads, ptrs, C.byref(kept), amask,
+                                 dl.ctypes.data if dl is not None else None, n_points, seed, aptrs)
     if rc:
         raise RuntimeError(lib().dropin_error().decode())
-    return {f: a[:kept.value] for f, a in d.items()}
+    u = {f: a[:kept.value] for f, a in d.items()}
+    if a_fields:
+        return u, {f: a[:kept.value] for f, a in da.items()}
+    return u
 
 
 def run_cone(pos, w, vel, scal, grid, cone, origin, box=(0, 100, 0, 100, 0, 100), periodic=True,
-             average_density=-1.0, u_fields=("density",), n_threads=4):
+             average_density=-1.0, u_fields=("density",), n_threads=4, a_fields=(), n_points=-1, seed=0):
     """DTFE() on a redshift-cone grid: dict field -> grid[0] grid[1] grid[2]
-    rows, r slowest and psi fastest."""
+    rows, r slowest and psi fastest (with a_fields: (u dict, a dict))."""
     pos = np.ascontiguousarray(pos, np.float32)
     G = int(np.prod(grid))
     d = {f: np.full((G, NCOMP[SLOTS[f]]), np.nan, np.float32) for f in u_fields}
+    da = {f: np.full((G, NCOMP[SLOTS[f]]), np.nan, np.float32) for f in a_fields}
     ptrs = (C.c_void_p * 9)(*[d[f].ctypes.data if f in d else None for f in SLOTS])
+    aptrs = (C.c_void_p * 9)(*[da[f].ctypes.data if f in da else None for f in SLOTS])
     mask = sum(1 << SLOTS[f] for f in u_fields)
+    amask = sum(1 << SLOTS[f] for f in a_fields)
     g = np.ascontiguousarray(grid, np.int32)
     bx = np.ascontiguousarray(box, np.float32)
     c = np.ascontiguousarray(cone, np.float32)
@@ -105,7 +118,9 @@ def run_cone(pos, w, vel, scal, grid, cone, origin, box=(0, 100, 0, 100, 0, 100)
     keep = [np.ascontiguousarray(a, np.float32) if a is not None else None for a in (w, vel, scal)]
     rc = lib().dropin_run_cone(pos.ctypes.data, *[a.ctypes.data if a is not None else None for a in keep],
                                len(pos), bx.ctypes.data, int(periodic), g.ctypes.data, float(average_density),
-                               mask, c.ctypes.data, o.ctypes.data, n_threads, ptrs)
+                               mask, c.ctypes.data, o.ctypes.data, n_threads, ptrs, amask, n_points, seed, aptrs)
     if rc:
         raise RuntimeError(lib().dropin_error().decode())
+    if a_fields:
+        return d, da
     return d

@@ -93,3 +93,21 @@ def test_cone_errors(gpu_built):
         d.vertex_density(split.rho_bar)
         with pytest.raises(N.DTFEError, match="one sub-box"):
             d.interpolate_cone(["density"], (1, 10, 0, 90, 0, 90), (50, 50, 50), (2, 2, 2))
+
+
+def test_cone_average_vs_oracle(gpu_built):
+    """Monte-Carlo bin averages on a redshift cone (dtfe_gpu_interpolate_cone
+    with DTFE_METHOD_MONTE_CARLO): bit-identical to the oracle's float mode
+    with the same Philox offsets."""
+    from dtfe_b200.device import DeviceDTFE
+    plan = _plan(59)
+    d32, d64, _ = O.vertex_density(plan)
+    with DeviceDTFE(0, 1) as d:
+        d.load(plan)
+        d.vertex_density(plan.rho_bar)
+        for cone, origin, dims in CONES[:2]:
+            for nn, seed in ((1, 0), (12, 5)):
+                want = O.average_cone(plan, d32, d64, FIELDS, cone, origin, dims, nn, seed=seed, mode=O.MODE_REF)
+                got = d.interpolate_cone(FIELDS, cone, origin, dims, n_samples=nn, seed=seed)
+                for f in FIELDS:
+                    assert np.array_equal(got[f], want[f].astype(np.float32)), (cone, nn, f)

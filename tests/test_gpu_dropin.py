@@ -143,3 +143,30 @@ def test_dropin_redshift_cone(particles):
     for f in fields:
         assert np.array_equal(u[f].reshape(ref[f].shape), ref[f].astype(np.float32)), f
     assert (ref["density"] == 0).any() and (ref["density"] != 0).any()
+
+
+def test_dropin_averages_at_samples_and_cones(particles):
+    """DTFE() with aField at user sampling points and on a redshift cone: the
+    reference's forced Monte-Carlo averages (method 2, 20 points unless
+    noPointsOn), equal to the device API's dtfe_gpu_average_points /
+    Monte-Carlo cone on the single-box plan with the same seed."""
+    from dtfe_b200.device import DeviceDTFE
+    pos, w, vel, sc = particles
+    rng = np.random.default_rng(12)
+    samples = rng.uniform(-10, 110, (1500, 3)).astype(np.float32)
+    delta = rng.uniform(1, 9, (1500, 3)).astype(np.float32)
+    fields = ["density", "velocity", "velocity_gradient", "scalar"]
+    cone, origin = (2.0, 80.0, 5.0, 175.0, 0.0, 300.0), (50.0, 40.0, 60.0)
+    u, a = D.run_points(pos, w, vel, sc, GRID, samples, u_fields=["density"], a_fields=fields, delta=delta, seed=9)
+    _, ac = D.run_cone(pos, w, vel, sc, GRID, cone, origin, u_fields=["density"], a_fields=fields, n_points=6,
+                       seed=4)
+    plan = P.make_plan(pos, w, vel, sc[:, None], grid=GRID, n_threads=1)
+    with DeviceDTFE(0, 1) as dev:
+        dev.load(plan)
+        dev.vertex_density(plan.rho_bar)
+        ref = dev.average_points(fields, samples, delta, [0, 100, 0, 100, 0, 100], 20, seed=9)
+        refc = dev.interpolate_cone(fields, cone, origin, GRID, n_samples=6, seed=4)
+    for f in fields:
+        assert len(a[f]) == len(ref[f]) == len(u["density"]) < len(samples)
+        assert np.array_equal(a[f].reshape(ref[f].shape), ref[f]), f
+        assert np.array_equal(ac[f].reshape(refc[f].shape), refc[f]), f

@@ -52,3 +52,33 @@ def test_points_errors(gpu_built):
         d.vertex_density(plan.rho_bar)
         with pytest.raises(N.DTFEError, match="one sub-box"):
             d.interpolate_points(["density"], np.zeros((4, 3), np.float32), [0, 100, 0, 100, 0, 100])
+
+
+def test_average_points_vs_oracle(gpu_built):
+    """Monte-Carlo volume averages at user points (dtfe_gpu_average_points):
+    bit-identical to the oracle's float mode with the same Philox offsets
+    (the oracle's estimator matches the reference's statistically,
+    tests/test_reference_live.py)."""
+    from dtfe_b200.device import DeviceDTFE
+    pos, psi = S.zeldovich_lattice(12, 100.0, 0.9, seed=71)
+    rng = np.random.default_rng(72)
+    w = rng.uniform(0.5, 1.5, len(pos)).astype(np.float32)
+    vel = (60 * psi).astype(np.float32)
+    sc = rng.standard_normal((len(pos), 1)).astype(np.float32)
+    plan = P.make_plan(pos, w, vel, sc, grid=(12, 12, 12), n_threads=1, average_density_value=float(w.sum()) / 1e6)
+    pts = np.concatenate([rng.uniform(-60, 160, (1000, 3)), rng.uniform(0, 100, (2000, 3))]).astype(np.float32)
+    delta = rng.uniform(0.5, 12, pts.shape).astype(np.float32)
+    region = np.array([-50, 150, -40, 140, -50, 150], np.float32)
+    d32, d64, _ = O.vertex_density(plan)
+    for nn, seed in ((1, 0), (20, 7)):
+        want = O.average_points(plan, d32, d64, FIELDS, pts, delta, region, nn, seed=seed, mode=O.MODE_REF)
+        with DeviceDTFE(0, 1) as d:
+            d.load(plan)
+            for loc in (11, 0):
+                d.set_variants(loc, 2)
+                d.vertex_density(plan.rho_bar)
+                got = d.average_points(FIELDS, pts, delta, region, nn, seed=seed)
+                for f in FIELDS:
+                    assert got[f].shape[0] == want[f].shape[0]
+                    assert np.array_equal(got[f], want[f].astype(np.float32)), (nn, loc, f)
+    assert (want["density"] == 0).any() and (want["density"] != 0).any()

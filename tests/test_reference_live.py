@@ -202,3 +202,41 @@ def test_live_redshift_cone(built):
     fixed = O.interpolate_cone(plan, d32, d64, ["density"], cone, origin, dims, mode=O.MODE_REF, fix_outside=True)
     assert (ora["density"] == 0).any() and (ora["density"] != 0).any()
     assert ((ora["density"] == 0) & (fixed["density"] != 0)).any()
+
+
+def test_live_averaged_samples_statistical(built):
+    """Monte-Carlo volume averages at user points and on a redshift cone: the
+    oracle (Philox offsets) against the reference's own
+    interpolateUserSampling_averaged_2 / interpolateRedshiftCone_averaged_2
+    (its mt19937 offsets).  The random points differ, so the check is
+    statistical: the median absolute difference oracle - reference matches
+    the one between two oracle seeds (the same estimator spread) within 25%
+    (medians, since a rare sample in a sliver tetrahedron carries a huge
+    gradient), and the mean difference lies within 4 standard errors of
+    zero."""
+    pos, psi = S.zeldovich_lattice(12, 100.0, 0.9, seed=61)
+    rng = np.random.default_rng(62)
+    w = rng.uniform(0.5, 1.5, len(pos)).astype(np.float32)
+    vel = (60 * psi).astype(np.float32)
+    plan = P.make_plan(pos, w, vel, None, grid=(12, 12, 12), n_threads=1, average_density_value=float(w.sum()) / 1e6)
+    d32, d64, _ = O.vertex_density(plan)
+    fields = ["density", "velocity", "velocity_gradient"]
+    pts = rng.uniform(5, 95, (2000, 3)).astype(np.float32)
+    delta = rng.uniform(2, 8, (2000, 3)).astype(np.float32)
+    region = np.array([0, 100, 0, 100, 0, 100], np.float32)
+    cone, origin, dims = (1.0, 45.0, 5.0, 175.0, 0.0, 350.0), (50.0, 50.0, 50.0), (8, 10, 25)
+    NN = 16
+    cases = [(O.average_points(plan, d32, d64, fields, pts, delta, region, NN, seed=1),
+              O.average_points(plan, d32, d64, fields, pts, delta, region, NN, seed=2),
+              R.run_average(plan, d32, NN, 3, pts=pts, delta=delta, region=region)),
+             (O.average_cone(plan, d32, d64, fields, cone, origin, dims, NN, seed=1),
+              O.average_cone(plan, d32, d64, fields, cone, origin, dims, NN, seed=2),
+              R.run_average(plan, d32, NN, 3, cone=cone, origin=origin, dims=dims))]
+    for a, b, ref in cases:
+        for f in fields:
+            assert len(ref[f]) == len(a[f])
+            d_ref = (a[f].astype(np.float32) - ref[f]).astype(np.float64).ravel()
+            d_self = (a[f] - b[f]).ravel()
+            ratio = np.median(np.abs(d_ref)) / np.median(np.abs(d_self))
+            assert 0.8 < ratio < 1.25, (f, ratio)
+            assert abs(d_ref.mean()) < 4 * d_ref.std() / np.sqrt(d_ref.size), f

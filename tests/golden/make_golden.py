@@ -18,6 +18,10 @@ fixture does not depend on it), then:
   * interpolateGrid_averaged_1 with 100 points per cell (the reference's
     default method and count; its GSL Sobol generator stood in by
     dtfe_b200/csrc/sobol.h);
+  * interpolateUserSampling at 600 points (some outside the region, some
+    beyond the hull, ten on vertices) and interpolateRedshiftCone on a
+    7 x 6 x 9 cone whose psi range wraps and whose outer shells leave the
+    hull, both with the reference's own vertex densities;
   * NGP / CIC / TSC density and velocity of the same particles in a region;
   * SPH_interpolation (32 neighbours) density, velocity and intensive scalar
     of the padded particle set on the 10^3 grid of the box;
@@ -80,6 +84,22 @@ def main():
     m1 = R.run(plan, 0, which=1, n_points=100)
     for f in ("density", "velocity", "velocity_gradient", "scalar", "scalar_gradient"):
         out["ref_method1_100_" + f] = m1[f]
+
+    rho_ref = centre["vertex_density"]
+    pts = np.random.default_rng(14).uniform(-40, 140, (600, 3)).astype(np.float32)
+    pts[:10] = plan.xyz[:10]
+    pregion = np.array([-30, 130, -25, 125, -30, 130], np.float32)
+    up = R.run_points(plan, pts, pregion, rho_ref)
+    out["points_xyz"], out["points_region"] = pts, pregion
+    for f in ("density", "velocity", "velocity_gradient", "scalar", "scalar_gradient"):
+        out["ref_points_" + f] = up[f]
+    cone = np.array([1.0, 95.0, 5.0, 175.0, 300.0, 60.0], np.float32)
+    origin = np.array([50.0, 45.0, 55.0], np.float32)
+    cdims = np.array([7, 6, 9], np.int32)
+    uc = R.run_cone(plan, cone, origin, cdims, rho_ref)
+    out["cone_limits"], out["cone_origin"], out["cone_dims"] = cone, origin, cdims
+    for f in ("density", "velocity", "velocity_gradient", "scalar", "scalar_gradient"):
+        out["ref_cone_" + f] = uc[f]
 
     region = np.array([10, 90, 5, 95, 0, 100], np.float32)
     dgrid = np.array([8, 9, 10], np.int32)

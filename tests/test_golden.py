@@ -99,3 +99,19 @@ def test_sph_bit_exact_vs_reference(g):
     assert np.array_equal(sc[:, 0].astype(np.float32), g["ref_sph32_scalar"])
     d64, v64, _ = O.sph(plan, k=32, velocity=True, mode=O.MODE_FP64)
     assert rel_err(d64, g["ref_sph32_density"]) < 1e-6
+
+
+def test_user_points_and_cone_bit_exact_vs_reference(g):
+    """interpolateUserSampling and interpolateRedshiftCone with the
+    reference's own vertex densities: the oracle's float mode reproduces the
+    reference's rows bit for bit (points dropped by the region, zeros beyond
+    the hull, the cone's stuck psi)."""
+    plan = golden_plan(g)
+    _, d64, _ = O.vertex_density(plan)
+    ref_dens = np.ascontiguousarray(g["ref_vertex_density"])
+    pts = O.interpolate_points(plan, ref_dens, d64, FIELDS, g["points_xyz"], g["points_region"], mode=O.MODE_REF)
+    cone = O.interpolate_cone(plan, ref_dens, d64, FIELDS, g["cone_limits"], g["cone_origin"], g["cone_dims"],
+                              mode=O.MODE_REF)
+    for f in FIELDS:
+        assert np.array_equal(pts[f].astype(np.float32), g[f"ref_points_{f}"].reshape(pts[f].shape)), f
+        assert np.array_equal(cone[f].astype(np.float32), g[f"ref_cone_{f}"].reshape(cone[f].shape)), f

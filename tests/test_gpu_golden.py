@@ -32,6 +32,25 @@ def test_gpu_vs_reference_fields(g):
                 assert rel_err(out[f], g[f"ref_{tag}_{f}"].reshape(out[f].shape)) <= 1e-6, (tag, f)
 
 
+def test_gpu_points_and_cone_vs_reference(g):
+    """User sampling points and the redshift cone through the C ABI against
+    the reference's interpolateUserSampling / interpolateRedshiftCone rows
+    (same rows kept, same zeros, values within the vertex-density bar)."""
+    from dtfe_b200.device import DeviceDTFE
+    plan = golden_plan(g)
+    with DeviceDTFE(0, 1) as d:
+        d.load(plan)
+        d.vertex_density(plan.rho_bar)
+        pts = d.interpolate_points(FIELDS, g["points_xyz"], g["points_region"])
+        cone = d.interpolate_cone(FIELDS, g["cone_limits"], g["cone_origin"], g["cone_dims"])
+    for f in FIELDS:
+        for got, tag in ((pts[f], "points"), (cone[f], "cone")):
+            want = g[f"ref_{tag}_{f}"].reshape(got.shape)
+            if f == "density":  # zero exactly where the reference found no tetrahedron
+                assert np.array_equal(got == 0, want == 0), tag
+            assert rel_err(got, want) <= 1e-6, (tag, f)
+
+
 @pytest.mark.parametrize("kind,name", [(0, "ngp"), (1, "cic"), (2, "tsc")])
 def test_gpu_deposit_vs_reference(g, kind, name):
     from dtfe_b200.device import DeviceDTFE

@@ -588,6 +588,29 @@ def sampling_leg(args, local: int, threads: int, cpu: bool) -> dict:
         dev.vertex_density(plan.rho_bar)
         stream = torch.cuda.ExternalStream(dev.stream, device=cuda)
 
+        # padded-box selection with the 27 periodic images (findParticlesInBox)
+        # of the n^3 particles: device vs the host restatement on all threads
+        pad = 5.0 * S.BOX / n
+        full = [0.0, S.BOX, 0.0, S.BOX, 0.0, S.BOX]
+        padded = [-pad, S.BOX + pad, -pad, S.BOX + pad, -pad, S.BOX + pad]
+        pos_dev = torch.from_numpy(pos).to(cuda)
+        for _ in range(2):
+            dev.select_in_box(pos_dev, full, padded)
+        torch.cuda.synchronize()
+        t0 = time.time()
+        sel_i, sel_p = dev.select_in_box(pos_dev, full, padded)
+        torch.cuda.synchronize()
+        t_sel = time.time() - t0
+        t0 = time.time()
+        h_i, h_p = P.select_in_box(pos, full, padded, True)
+        t_host = time.time() - t0
+        res["selection"] = {"particles": G, "selected": int(sel_i.numel()), "gpu_ms": 1e3 * t_sel,
+                            "host_ms": 1e3 * t_host,
+                            "bit_exact_vs_host": bool(np.array_equal(sel_i.cpu().numpy(), h_i) and
+                                                      np.array_equal(sel_p.cpu().numpy(), h_p)),
+                            "timing": "wall clock around the call (count, scan, one host sync, write)"}
+        del pos_dev, sel_i, sel_p
+
         def timed(fn, k=5):
             for _ in range(2):
                 fn()

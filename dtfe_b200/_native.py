@@ -176,6 +176,8 @@ def gpu() -> C.CDLL:
                                                 C.POINTER(C.c_int64)]
         lib.dtfe_gpu_interpolate_cone_dev.argtypes = [H, vp, vp, vp, C.POINTER(InterpOpts), C.POINTER(vp)]
         lib.dtfe_gpu_write_binary_dev.argtypes = [H, C.c_char_p, vp, C.c_int64]
+        lib.dtfe_gpu_select_in_box_dev.argtypes = [H, vp, C.c_int64, vp, vp, C.c_int, vp, vp, C.c_int64,
+                                                   C.POINTER(C.c_int64)]
         lib.dtfe_gpu_download_vertex_density.argtypes = [H, vp]
         lib.dtfe_gpu_locate_points.argtypes = [H, C.c_int64, vp, C.c_int32, vp]
         lib.dtfe_gpu_stream.argtypes = [H]

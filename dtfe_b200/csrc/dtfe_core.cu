@@ -932,6 +932,66 @@ __global__ void __launch_bounds__(256) k_cone_rows(InterpParams P, int* __restri
     zero_after_outside(P, tet_c, q * nz, q * nz, nz, lane);
 }
 
+// Particles of the padded box (findParticlesInBox / insertParticlesInBox,
+// src/subpartition.h:79-154): for each of up to 27 box translations (order
+// i1, i2, i3 over {-1, 0, 1}, offset (i - 1) * box length in float) the
+// translated padded box selects particles (closed, isParticleInBox), which
+// are emitted shifted back by the offset (float subtraction), translation
+// after translation, particles in input order within one.  Block b covers
+// chunk b % nchunks of translation b / nchunks, so the exclusive prefix of
+// the per-block counts is every block's first output row.
+constexpr int kSelChunk = 1024;
+struct SelBoxes {
+  float box[27][6];
+  float off[27][3];
+};
+__device__ __forceinline__ bool sel_in(const float* __restrict__ pos, int64_t i, const float* b) {
+  const float x = __ldg(&pos[3 * i]), y = __ldg(&pos[3 * i + 1]), z = __ldg(&pos[3 * i + 2]);
+  return x >= b[0] && x <= b[1] && y >= b[2] && y <= b[3] && z >= b[4] && z <= b[5];
+}
+__global__ void __launch_bounds__(kSelChunk) k_select_count(const float* __restrict__ pos, int64_t n,
+                                                            int64_t nchunks, SelBoxes S, int* __restrict__ counts) {
+  const int64_t b = blockIdx.x;
+  const int o = (int)(b / nchunks);
+  const int64_t i = (b - (int64_t)o * nchunks) * kSelChunk + threadIdx.x;
+  const int c = __syncthreads_count(i < n && sel_in(pos, i, S.box[o]));
+  if (threadIdx.x == 0) counts[b] = c;
+}
+__global__ void __launch_bounds__(kSelChunk) k_select_write(const float* __restrict__ pos, int64_t n,
+                                                            int64_t nchunks, SelBoxes S,
+                                                            const int64_t* __restrict__ first,
+                                                            int32_t* __restrict__ idx_out,
+                                                            float* __restrict__ pos_out) {
+  __shared__ int warp_first[kSelChunk / 32];
+  const int64_t b = blockIdx.x;
+  const int o = (int)(b / nchunks);
+  const int64_t i = (b - (int64_t)o * nchunks) * kSelChunk + threadIdx.x;
+  const bool in = i < n && sel_in(pos, i, S.box[o]);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned m = __ballot_sync(0xffffffffu, in);
+  if (lane == 0) warp_first[warp] = __popc(m);
+  __syncthreads();
+  if (warp == 0) {
+    const int v = warp_first[lane];  // kSelChunk / 32 == 32 warps
+    int incl = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d) incl += y;
+    }
+    warp_first[lane] = incl - v;
+  }
+  __syncthreads();
+  if (in) {
+    const int64_t at = __ldg(&first[b]) + warp_first[warp] + __popc(m & ((1u << lane) - 1u));
+    if (idx_out) idx_out[at] = (int32_t)i;
+    if (pos_out) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) pos_out[3 * at + k] = __fsub_rn(__ldg(&pos[3 * i + k]), S.off[o][k]);
+    }
+  }
+}
+
 // Fields at user sampling points (interpolateUserSampling,
 // unaveraged_interpolation.cc:560-691), one thread per point of a single
 // sub-box's tessellation.  keep[i]: the point lies in the region (closed);
@@ -1475,6 +1535,9 @@ struct dtfe_gpu_s {
   int64_t* pts_idx = nullptr;
   int64_t* pts_blocks = nullptr;
   float* pts_out = nullptr;
+  int* sel_counts = nullptr;      // dtfe_gpu_select_in_box_dev: per-block counts and first rows
+  int64_t* sel_first = nullptr;
+  int64_t* sel_blocks = nullptr;
   char* io_stage[2] = {nullptr, nullptr};  // pinned staging of dtfe_gpu_write_binary_dev
   cudaEvent_t io_ev[2] = {nullptr, nullptr};
   double* m1_table = nullptr;     // method-1 Sobol points (100 NN x 3)
@@ -1725,7 +1788,7 @@ int dtfe_gpu_destroy(dtfe_handle h) {
   if (h->dep_scratch) cudaFree(h->dep_scratch);
   for (void* p : {(void*)h->g_rho, (void*)h->g_x, (void*)h->g_v, (void*)h->g_S, (void*)h->g_m, (void*)h->vbar,
                   (void*)h->adj_a, h->sph_scratch, (void*)h->sph_out, (void*)h->upload_buf, (void*)h->m1_table,
-                  h->m1_scratch, h->m1_lists})
+                  h->m1_scratch, h->m1_lists, (void*)h->sel_counts, (void*)h->sel_first, (void*)h->sel_blocks})
     if (p) cudaFree(p);
   if (h->dep_out) cudaFree(h->dep_out);
   for (int i = 0; i < 2; ++i) {
@@ -2736,6 +2799,62 @@ int dtfe_gpu_interpolate_cone_dev(dtfe_handle h, const float cone[6], const floa
   InterpParams P;
   if ((rc = cone_enqueue(h, cone, origin, dims, o, out_dev, P))) return rc;
   return read_status(h, nullptr);
+}
+
+int dtfe_gpu_select_in_box_dev(dtfe_handle h, const float* pos_dev, int64_t n, const float full_box[6],
+                               const float padded[6], int periodic, int32_t* idx_dev, float* pos_out_dev,
+                               int64_t capacity, int64_t* count) {
+  if (!h || !full_box || !padded || !count || n < 0 || (n > 0 && !pos_dev) || capacity < 0)
+    return set_error(DTFE_ERR_ARG, "null argument");
+  if (n >= (int64_t(1) << 31)) return set_error(DTFE_ERR_TOO_LARGE, "particle indices are 32-bit");
+  *count = 0;
+  if (n == 0) return DTFE_OK;
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  SelBoxes S;
+  int n_off = 1;
+  if (!periodic) {
+    for (int k = 0; k < 6; ++k) S.box[0][k] = padded[k];
+    for (int k = 0; k < 3; ++k) S.off[0][k] = 0.f;
+  } else {
+    float len[3];
+    for (int k = 0; k < 3; ++k) len[k] = full_box[2 * k + 1] - full_box[2 * k];
+    n_off = 27;
+    for (int i1 = 0; i1 < 3; ++i1)
+      for (int i2 = 0; i2 < 3; ++i2)
+        for (int i3 = 0; i3 < 3; ++i3) {
+          const int o = i1 * 9 + i2 * 3 + i3;
+          const int ii[3] = {i1, i2, i3};
+          for (int k = 0; k < 3; ++k) {
+            S.off[o][k] = (float)(ii[k] - 1) * len[k];
+            S.box[o][2 * k] = padded[2 * k] + S.off[o][k];
+            S.box[o][2 * k + 1] = padded[2 * k + 1] + S.off[o][k];
+          }
+        }
+  }
+  const int64_t nchunks = (n + kSelChunk - 1) / kSelChunk;
+  const int64_t nblk = nchunks * n_off;
+  const int64_t nb = (nblk + kScanBlock - 1) / kScanBlock;
+  int rc;
+  if ((rc = dev_alloc(h, &h->sel_counts, (size_t)nblk)) || (rc = dev_alloc(h, &h->sel_first, (size_t)nblk + 1)) ||
+      (rc = dev_alloc(h, &h->sel_blocks, (size_t)nb + 1)))
+    return rc;
+  cudaStream_t st = h->stream;
+  k_select_count<<<(unsigned)nblk, kSelChunk, 0, st>>>(pos_dev, n, nchunks, S, h->sel_counts);
+  k_scan_blocks<<<(unsigned)nb, kScanBlock, 0, st>>>(nblk, h->sel_counts, h->sel_first, h->sel_blocks);
+  k_scan_totals<<<1, kScanBlock, 0, st>>>(nb, h->sel_blocks, h->sel_first + nblk);
+  k_scan_add<<<(unsigned)nb, kScanBlock, 0, st>>>(nblk, h->sel_first, h->sel_blocks);
+  DTFE_CUDA_TRY(cudaGetLastError());
+  int64_t total = 0;
+  DTFE_CUDA_TRY(cudaMemcpyAsync(&total, h->sel_first + nblk, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  DTFE_CUDA_TRY(cudaStreamSynchronize(st));
+  *count = total;
+  if (!idx_dev && !pos_out_dev) return DTFE_OK;
+  if (total > capacity)
+    return set_error(DTFE_ERR_TOO_LARGE, "selection larger than the output capacity (count returned)");
+  k_select_write<<<(unsigned)nblk, kSelChunk, 0, st>>>(pos_dev, n, nchunks, S, h->sel_first, idx_dev, pos_out_dev);
+  DTFE_CUDA_TRY(cudaGetLastError());
+  DTFE_CUDA_TRY(cudaStreamSynchronize(st));
+  return DTFE_OK;
 }
 
 // File chunk of dtfe_gpu_write_binary_dev: two pinned buffers of this size.

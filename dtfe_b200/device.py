@@ -229,6 +229,26 @@ class DeviceDTFE:
         N.check(self.lib.dtfe_gpu_interpolate_cone_dev(self.h, c.ctypes.data, org.ctypes.data, d.ctypes.data,
                                                        C.byref(o), optr))
 
+    def select_in_box(self, pos, full_box, padded, periodic: bool = True):
+        """Particles of the padded box on the device (dtfe_gpu_select_in_box_dev):
+        pos a (n, 3) float32 CUDA tensor; returns (int32 source indices,
+        (m, 3) shifted positions) as CUDA tensors."""
+        import torch
+        if not pos.is_cuda or not pos.is_contiguous() or pos.dtype != torch.float32:
+            raise ValueError("select_in_box takes a contiguous float32 CUDA tensor")
+        fb = np.ascontiguousarray(full_box, np.float32)
+        pb = np.ascontiguousarray(padded, np.float32)
+        n = pos.shape[0]
+        cnt = C.c_int64(0)
+        N.check(self.lib.dtfe_gpu_select_in_box_dev(self.h, pos.data_ptr(), n, fb.ctypes.data, pb.ctypes.data,
+                                                    1 if periodic else 0, None, None, 0, C.byref(cnt)))
+        idx = torch.empty(cnt.value, dtype=torch.int32, device=pos.device)
+        out = torch.empty((cnt.value, 3), dtype=torch.float32, device=pos.device)
+        N.check(self.lib.dtfe_gpu_select_in_box_dev(self.h, pos.data_ptr(), n, fb.ctypes.data, pb.ctypes.data,
+                                                    1 if periodic else 0, idx.data_ptr(), out.data_ptr(),
+                                                    cnt.value, C.byref(cnt)))
+        return idx, out
+
     def write_binary_dev(self, path: str, tensor) -> None:
         """Streams a contiguous float32 CUDA tensor to `path` in the
         reference's binary output format (dtfe_gpu_write_binary_dev)."""

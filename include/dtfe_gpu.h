@@ -252,6 +252,22 @@ int dtfe_gpu_interpolate_cone(dtfe_handle h, const float cone[6], const float or
 /* Same, writing into device buffers (dims[0] dims[1] dims[2] rows each). */
 int dtfe_gpu_interpolate_cone_dev(dtfe_handle h, const float cone[6], const float origin[3], const int32_t dims[3],
                                   const dtfe_interp_opts* opts, float* const out_dev[DTFE_NUM_FIELDS]);
+/* Particles of a padded box on the device (findParticlesInBox /
+ * insertParticlesInBox, src/subpartition.h:79-154; the same selection as
+ * dtfe_select_in_box in include/dtfe_host.h, bit for bit): pos_dev holds n
+ * positions (3 floats each).  Non-periodic: particles with
+ * padded[lo] <= pos <= padded[hi].  Periodic: for each of the 27 translations
+ * (i1, i2, i3 over {-1, 0, 1}, offset (i - 1) x box length of full_box) the
+ * translated padded box selects particles, emitted shifted back by the
+ * offset, translation after translation, in input order within one.
+ * *count = the number selected; idx_dev (int32 source indices) and
+ * pos_out_dev (shifted positions), when not NULL, receive them if count <=
+ * capacity (else DTFE_ERR_TOO_LARGE with *count set, nothing written).
+ * n must be below 2^31. */
+int dtfe_gpu_select_in_box_dev(dtfe_handle h, const float* pos_dev, int64_t n, const float full_box[6],
+                               const float padded[6], int periodic, int32_t* idx_dev, float* pos_out_dev,
+                               int64_t capacity, int64_t* count);
+
 /* Writes n_floats floats of device memory (a field in the Quantities layout)
  * to `path` in the reference's binary output format: the raw floats, no
  * header, the file writeBinaryFile (src/io/binary_io.cc:185-216) writes for

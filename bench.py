@@ -73,6 +73,12 @@ def parse():
                     help="particles per side of the redshift-cone / user-point workload (one box)")
     ap.add_argument("--no-sampling", action="store_true")
     ap.add_argument("--no-output", action="store_true", help="skip the binary output-file leg")
+    ap.add_argument("--scalars", type=int, default=0,
+                    help="extra N(0,1) scalar fields per particle, interpolated with their gradients")
+    ap.add_argument("--fp64-cells", type=int, default=50000,
+                    help="cells checked against the FP64 oracle in the CPU-baseline leg (0 = none)")
+    ap.add_argument("--cpu-kind", default="auto", choices=["auto", "port"],
+                    help="CPU baseline: the reference's code when built (auto) or the oracle port")
     return ap.parse_args()
 
 
@@ -85,7 +91,7 @@ def host_threads(req: int) -> int:
         return os.cpu_count() or 1
 
 
-def build_workload(n: int, rank: int, threads: int):
+def build_workload(n: int, rank: int, threads: int, scalars: int = 0):
     from dtfe_b200 import plan as P
     from dtfe_b200 import synthetic as S
     t0 = time.time()
@@ -94,9 +100,11 @@ def build_workload(n: int, rank: int, threads: int):
     vel = (100.0 * psi / (S.BOX / n) + rng.normal(0.0, 50.0, psi.shape)).astype(np.float32)
     del psi
     w = np.ones(len(pos), np.float32)
+    sc = (np.random.default_rng(8 + 1000 * rank).standard_normal((len(pos), scalars)).astype(np.float32)
+          if scalars else None)
     t_ics = time.time() - t0
     t0 = time.time()
-    plan = P.make_plan(pos, w, vel, None, grid=(n, n, n), n_threads=threads,
+    plan = P.make_plan(pos, w, vel, sc, grid=(n, n, n), n_threads=threads,
                        average_density_value=float(len(pos)) / S.BOX ** 3)
     plan.timings["ics_s"] = t_ics
     plan.timings["plan_total_s"] = time.time() - t0
@@ -203,24 +211,68 @@ def reference_method1(plan, threads: int, n_points: int):
                                    f"sub-boxes {min(per_box):.2f}-{max(per_box):.2f} s"}
 
 
-def cpu_baseline(plan, threads: int, target_s: float) -> dict:
+def fp64_check(plan, outs: dict, fields, cells: int, d32, d64) -> dict:
+    """Error of the device's fields against the FP64 oracle on a sample:
+    `cells` grid cells drawn uniformly from every sub-box's tile, evaluated
+    by the oracle (FP64 mode, the sub-box's own tessellation) at the same
+    float cell centres.  Per field: max |gpu - fp64| / max(|fp64|, rms(fp64))
+    over the sample (the relative error with the field's RMS as the floor of
+    the denominator)."""
+    import torch
+    import oracle as O
+    rng = np.random.default_rng(123)
+    G1, G2 = plan.grid[1], plan.grid[2]
+    per_box = max(1, cells // plan.n_boxes)
+    got = {f: [] for f in fields}
+    want = {f: [] for f in fields}
+    big = [-1e30, 1e30, -1e30, 1e30, -1e30, 1e30]
+    for b in range(plan.n_boxes):
+        B = plan.boxes[b]
+        dims = [int(B.tile_dims[a]) for a in range(3)]
+        if min(dims) <= 0:
+            continue
+        ijk = np.stack([rng.integers(0, dims[a], per_box) for a in range(3)], 1)
+        pts = np.stack([plan.xs[B.coord_offset[0] + ijk[:, 0]], plan.ys[B.coord_offset[1] + ijk[:, 1]],
+                        plan.zs[B.coord_offset[2] + ijk[:, 2]]], 1).astype(np.float32)
+        cell = ((B.tile_origin[0] + ijk[:, 0]) * G1 + (B.tile_origin[1] + ijk[:, 1])) * G2 + (B.tile_origin[2]
+                                                                                          + ijk[:, 2])
+        ref = O.interpolate_points(plan, d32, d64, fields, pts, big, mode=O.MODE_FP64, box=b)
+        sel = torch.from_numpy(cell.astype(np.int64)).to(next(iter(outs.values())).device)
+        for f in fields:
+            got[f].append(outs[f].index_select(0, sel).cpu().numpy().reshape(len(cell), -1))
+            want[f].append(ref[f].reshape(len(cell), -1))
+    err = {}
+    for f in fields:
+        a = np.concatenate(got[f]).astype(np.float64)
+        w = np.concatenate(want[f])
+        floor = max(np.sqrt(np.mean(w ** 2)), 1e-300)
+        err[f] = float(np.max(np.abs(a - w) / np.maximum(np.abs(w), floor)))
+    return {"cells": int(sum(len(x) for x in got[fields[0]])), "max_rel_err_rms_floor": err,
+            "max_over_fields": max(err.values()), "bar": 1e-5}
+
+
+def cpu_baseline(plan, threads: int, target_s: float, kind: str = "auto", check=None) -> dict:
     """The reference's own code on the host cores (reference_code_step) on
     the whole workload; without the harness, the CPU oracle in the
     reference's arithmetic on a sample (vertex densities over the whole
     tessellation plus cell-centre interpolation of the first x-slabs of
     sub-box 0, scaled to the full grid)."""
     G = int(np.prod(plan.grid))
-    ref = reference_code_step(plan, threads)
+    import oracle as O
+    ref = reference_code_step(plan, threads) if kind == "auto" else None
     if ref is not None:
         t, per_box = ref
-        return {"value": G / t, "unit": "grid samples/s", "cores": min(threads, plan.n_boxes), "kind": "reference",
-                "sample": f"the whole workload: the reference's vertexDensity + interpolateGrid (density, velocity, "
-                          f"velocity gradient) on all {plan.n_boxes} sub-boxes, one host thread each (its "
-                          f"DTFE_parallel split); slowest thread {t:.2f} s, sub-boxes {min(per_box):.2f}-"
-                          f"{max(per_box):.2f} s",
-                "step_s": t}
+        res = {"value": G / t, "unit": "grid samples/s", "cores": min(threads, plan.n_boxes), "kind": "reference",
+               "sample": f"the whole workload: the reference's vertexDensity + interpolateGrid (density, velocity, "
+                         f"velocity gradient) on all {plan.n_boxes} sub-boxes, one host thread each (its "
+                         f"DTFE_parallel split); slowest thread {t:.2f} s, sub-boxes {min(per_box):.2f}-"
+                         f"{max(per_box):.2f} s",
+               "step_s": t}
+        if check is not None:
+            d32, d64, _ = O.vertex_density(plan)
+            res["fp64_check"] = fp64_check(plan, *check, d32, d64)
+        return res
     import copy
-    import oracle as O
     from dtfe_b200 import _native as N
     t0 = time.time()
     d32, d64, _ = O.vertex_density(plan)
@@ -245,11 +297,14 @@ def cpu_baseline(plan, threads: int, target_s: float) -> dict:
     cells = slabs * per_slab
     G = int(np.prod(plan.grid))
     t_step = t_vd + elapsed * G / cells
-    return {"value": G / t_step, "unit": "grid samples/s", "cores": threads, "kind": "port",
-            "sample": f"vertex densities of all {plan.n_verts} vertices ({t_vd:.2f} s) + cell-centre "
-                      f"interpolation of {cells} of {G} cells ({elapsed:.2f} s, x-slabs of sub-box 0), "
-                      f"scaled to the full grid",
-            "vertex_density_s": t_vd, "interp_cells_per_s": cells / elapsed}
+    res = {"value": G / t_step, "unit": "grid samples/s", "cores": threads, "kind": "port",
+           "sample": f"vertex densities of all {plan.n_verts} vertices ({t_vd:.2f} s) + cell-centre "
+                     f"interpolation of {cells} of {G} cells ({elapsed:.2f} s, x-slabs of sub-box 0), "
+                     f"scaled to the full grid",
+           "vertex_density_s": t_vd, "interp_cells_per_s": cells / elapsed}
+    if check is not None:
+        res["fp64_check"] = fp64_check(plan, *check, d32, d64)
+    return res
 
 
 def _events(stream, fn, steps):
@@ -780,13 +835,15 @@ def run_ours(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     threads = max(1, host_threads(args.threads) // max(1, world if world > 1 else 1))
-    plan = build_workload(args.n, rank, threads)
+    plan = build_workload(args.n, rank, threads, args.scalars)
     G = int(np.prod(plan.grid))
+    from dtfe_b200 import _native as NN_
+    FIELDS = list(globals()["FIELDS"]) + (["scalar", "scalar_gradient"] if args.scalars else [])
+    ncomp = {f: NN_.field_components(NN_.FIELD_SLOTS[f], args.scalars) for f in FIELDS}
 
-    dev = DeviceDTFE(local, 0)
+    dev = DeviceDTFE(local, args.scalars)
     dev.load(plan)
-    outs = {f: torch.empty((G, [1, 3, 9, 1, 5, 3][i]), dtype=torch.float32, device=f"cuda:{local}")
-            for i, f in enumerate(FIELDS)}
+    outs = {f: torch.empty((G, ncomp[f]), dtype=torch.float32, device=f"cuda:{local}") for f in FIELDS}
     stream = torch.cuda.ExternalStream(dev.stream, device=f"cuda:{local}")
 
     def step():
@@ -900,7 +957,7 @@ def run_ours(args):
         hp.weight, hp.velocity = pin(plan.weight), pin(plan.velocity)
         # the tessellation as the planner caches it for the transfer: packed
         packed = pin(PL.pack_tets(plan.tet_v, plan.tet_n))
-        host_out = {f: pin(np.empty((G, [1, 3, 9, 1, 5, 3][i]), np.float32)) for i, f in enumerate(FIELDS)}
+        host_out = {f: pin(np.empty((G, ncomp[f]), np.float32)) for f in FIELDS}
         h_vert = hp.xyz.nbytes + hp.weight.nbytes + hp.velocity.nbytes + 4 * (len(hp.xs) + len(hp.ys) + len(hp.zs))
         d2h = sum(a.nbytes for a in host_out.values())
 
@@ -939,7 +996,7 @@ def run_ours(args):
         nbuf = max(2, args.e2e_buffers)
         ring = [dev]
         for _ in range(nbuf - 1):
-            d = DeviceDTFE(local, 0)
+            d = DeviceDTFE(local, args.scalars)
             d.set_variants(*variants)
             ring.append(d)
         outs2 = [host_out] + [{f: pin(np.empty_like(a)) for f, a in host_out.items()} for _ in range(nbuf - 1)]
@@ -988,7 +1045,7 @@ def run_ours(args):
                                         "h2d_bytes_per_step": int(hp.tet_v.nbytes + hp.tet_n.nbytes + h_vert)}}
 
     peak, peak_kind = measured_peak()
-    b_alg = 16 * plan.n_tets + plan.n_verts * (12 + 4 + 12) + 4 * C_OUT * G
+    b_alg = 16 * plan.n_tets + plan.n_verts * (12 + 4 + 12 + 4 * args.scalars) + 4 * sum(ncomp.values()) * G
     achieved = b_alg / t_interp / 1e9
     # the interpolation kernel(s) of the chosen locate variant: 9..11 walk and
     # evaluate in one kernel, 3..8 walk then evaluate
@@ -997,7 +1054,9 @@ def run_ours(args):
     kname = ("k_locate_eval (walk + evaluation in one kernel)" if fused
              else "k_locate_cells + k_eval_centre (cell-centre interpolation)")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic.get("dram_bytes_per_launch_scaled") if traffic else None,
+                # the ncu capture's DRAM bytes scaled by this launch's algorithmic bytes
+                "traffic": (int(traffic["dram_bytes_measured"] * b_alg / traffic["algorithmic_bytes_measured_case"])
+                            if traffic else None),
                 "kernel": kname, "kernel_ms": 1e3 * t_interp,
                 "algorithmic_bytes": int(b_alg), "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})"}
 
@@ -1024,7 +1083,8 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(plan, host_threads(args.threads), args.cpu_seconds)
+        check = (outs, FIELDS, args.fp64_cells) if args.fp64_cells > 0 else None
+        cpu = cpu_baseline(plan, host_threads(args.threads), args.cpu_seconds, args.cpu_kind, check)
 
     line = {
         "metric": METRIC, "value": value, "unit": "grid samples/s", "n_gpus": world, "steps": args.steps,
@@ -1032,7 +1092,9 @@ def run_ours(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"zeldovich{args.n}: {args.n}^3 Zel'dovich particles (rms 1.0 spacing, "
                                f"periodic 100 Mpc/h, padding 5) -> {args.n}^3 grid, cell-centre "
-                               "density+velocity+gradient+div/shear/vort per step, vertex densities included",
+                               "density+velocity+gradient+div/shear/vort"
+                               + (f" + {args.scalars} N(0,1) scalars and their gradients" if args.scalars else "")
+                               + " per step, vertex densities included",
                    "grid": list(plan.grid), "particles": args.n ** 3, "vertices": plan.n_verts,
                    "tetrahedra": plan.n_tets, "subboxes": plan.n_boxes,
                    "l2": "inputs larger than L2 (tessellation arrays > 126 MB)",

@@ -837,25 +837,27 @@ def run_ours(args):
     threads = max(1, host_threads(args.threads) // max(1, world if world > 1 else 1))
     plan = build_workload(args.n, rank, threads, args.scalars)
     G = int(np.prod(plan.grid))
-    from dtfe_b200 import _native as NN_
-    FIELDS = list(globals()["FIELDS"]) + (["scalar", "scalar_gradient"] if args.scalars else [])
-    ncomp = {f: NN_.field_components(NN_.FIELD_SLOTS[f], args.scalars) for f in FIELDS}
+    from dtfe_b200 import _native as NF
+    # the step's fields: the six velocity-derived ones, plus the scalars and
+    # their gradients when the workload carries scalars
+    fields = FIELDS + (["scalar", "scalar_gradient"] if args.scalars else [])
+    ncomp = {f: NF.field_components(NF.FIELD_SLOTS[f], args.scalars) for f in fields}
 
     dev = DeviceDTFE(local, args.scalars)
     dev.load(plan)
-    outs = {f: torch.empty((G, ncomp[f]), dtype=torch.float32, device=f"cuda:{local}") for f in FIELDS}
+    outs = {f: torch.empty((G, ncomp[f]), dtype=torch.float32, device=f"cuda:{local}") for f in fields}
     stream = torch.cuda.ExternalStream(dev.stream, device=f"cuda:{local}")
 
     def step():
         dev.vertex_density(plan.rho_bar)
-        return dev.interpolate_dev(FIELDS, outs, method=0)
+        return dev.interpolate_dev(fields, outs, method=0)
 
     dev.vertex_density(plan.rho_bar)
     if args.variants:
         variants = tuple(int(x) for x in args.variants.split(","))
         dev.set_variants(*variants)
     else:
-        variants = dev.autotune(FIELDS)
+        variants = dev.autotune(fields)
 
     for _ in range(args.warmup):
         step()
@@ -878,7 +880,7 @@ def run_ours(args):
     for i in range(args.steps):
         dev.vertex_density(plan.rho_bar)
         ki0[i].record(stream)
-        dev.interpolate_dev_async(FIELDS, outs, method=0)
+        dev.interpolate_dev_async(fields, outs, method=0)
         ki1[i].record(stream)
     ev1.record(stream)
     ev1.synchronize()
@@ -903,14 +905,14 @@ def run_ours(args):
     if side and not args.no_mc:
         for _ in range(2):
             dev.vertex_density(plan.rho_bar)
-            dev.interpolate_dev(FIELDS, outs, method=2, n_samples=8, seed=3)
+            dev.interpolate_dev(fields, outs, method=2, n_samples=8, seed=3)
         dev.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(3):
             dev.vertex_density(plan.rho_bar)
-            dev.interpolate_dev(FIELDS, outs, method=2, n_samples=8, seed=3)
+            dev.interpolate_dev(fields, outs, method=2, n_samples=8, seed=3)
         e1.record(stream)
         e1.synchronize()
         tm = e0.elapsed_time(e1) / 3e3
@@ -924,14 +926,14 @@ def run_ours(args):
         from dtfe_b200 import _native as N1
         for _ in range(2):
             dev.vertex_density(plan.rho_bar)
-            dev.interpolate_dev(FIELDS, outs, method=N1.METHOD_TETRAHEDRA, n_samples=args.m1_points)
+            dev.interpolate_dev(fields, outs, method=N1.METHOD_TETRAHEDRA, n_samples=args.m1_points)
         dev.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(3):
             dev.vertex_density(plan.rho_bar)
-            dev.interpolate_dev(FIELDS, outs, method=N1.METHOD_TETRAHEDRA, n_samples=args.m1_points)
+            dev.interpolate_dev(fields, outs, method=N1.METHOD_TETRAHEDRA, n_samples=args.m1_points)
         e1.record(stream)
         e1.synchronize()
         tm = e0.elapsed_time(e1) / 3e3
@@ -957,7 +959,7 @@ def run_ours(args):
         hp.weight, hp.velocity = pin(plan.weight), pin(plan.velocity)
         # the tessellation as the planner caches it for the transfer: packed
         packed = pin(PL.pack_tets(plan.tet_v, plan.tet_n))
-        host_out = {f: pin(np.empty((G, ncomp[f]), np.float32)) for f in FIELDS}
+        host_out = {f: pin(np.empty((G, ncomp[f]), np.float32)) for f in fields}
         h_vert = hp.xyz.nbytes + hp.weight.nbytes + hp.velocity.nbytes + 4 * (len(hp.xs) + len(hp.ys) + len(hp.zs))
         d2h = sum(a.nbytes for a in host_out.values())
 
@@ -965,12 +967,12 @@ def run_ours(args):
             dev.upload_packed(hp, packed)
             dev.set_subboxes(hp)
             dev.vertex_density(hp.rho_bar)
-            dev.interpolate(FIELDS, method=0, out=host_out)
+            dev.interpolate(fields, method=0, out=host_out)
 
         def e2e_plain():
             dev.load(hp)
             dev.vertex_density(hp.rho_bar)
-            dev.interpolate(FIELDS, method=0, out=host_out)
+            dev.interpolate(fields, method=0, out=host_out)
 
         def time_e2e(fn):
             fn()
@@ -1012,7 +1014,7 @@ def run_ours(args):
             d.synchronize()
             d.upload_packed(hp, packed)
             d.vertex_density(hp.rho_bar)
-            d.interpolate_async(FIELDS, outs2[k % nbuf], method=0)
+            d.interpolate_async(fields, outs2[k % nbuf], method=0)
         for k in range(nbuf):
             e2e_pipelined(k)
         for d in ring:
@@ -1083,7 +1085,7 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        check = (outs, FIELDS, args.fp64_cells) if args.fp64_cells > 0 else None
+        check = (outs, fields, args.fp64_cells) if args.fp64_cells > 0 else None
         cpu = cpu_baseline(plan, host_threads(args.threads), args.cpu_seconds, args.cpu_kind, check)
 
     line = {

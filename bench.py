@@ -1101,7 +1101,9 @@ def run_ours(args):
                    "tetrahedra": plan.n_tets, "subboxes": plan.n_boxes,
                    "l2": "inputs larger than L2 (tessellation arrays > 126 MB)",
                    "parallelism": f"dp{world} (independent boxes per GPU)"},
-        "gpu_launches": (3 if variants[0] >= 9 else 4) * args.steps,
+        # per step: volumes + seeds, vertex densities, the walk and evaluation
+        # (one fused kernel or two), the outside-pencil pass
+        "gpu_launches": (4 if variants[0] >= 9 else 5) * args.steps,
         "launch_variants": {"locate": variants[0], "eval": variants[1]},
         "clocks": clk,
         "e2e": e2e,

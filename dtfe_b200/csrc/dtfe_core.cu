@@ -1255,6 +1255,7 @@ __global__ void __launch_bounds__(256, 4) k_points_average(InterpParams P, int64
       n_out += t < 0;
       if (t < 0) continue;
       CellOut e;
+      zero_out<S>(e);  // fields not requested stay 0 in the sums
       cell_eval<S>(v, X, p, P.posd, P.vel4, P.scal, want_dens, want_vel, want_sc, P.fix != 0, e);
       acc.dens += e.dens;
 #pragma unroll

@@ -29,3 +29,16 @@ def test_write_binary_dev(gpu_built, tmp_path):
         assert [p.rsplit(".", 1)[1] for p in paths] == ["a_den", "a_velGrad"]
         for p, f in zip(paths, ["density", "velocity_gradient"]):
             assert np.array_equal(np.fromfile(p, np.float32), fields[f].cpu().numpy().ravel())
+
+
+def test_write_binary_dev_unwritable(gpu_built, tmp_path):
+    import torch
+    from dtfe_b200 import _native as N
+    from dtfe_b200.device import DeviceDTFE
+    with DeviceDTFE(0) as d:
+        with pytest.raises(N.DTFEError) as e:
+            d.write_binary_dev(str(tmp_path / "missing_dir" / "x.den"), torch.zeros(100, device="cuda"))
+        assert e.value.code == N.ERR_IO
+        # the handle stays usable
+        d.write_binary_dev(str(tmp_path / "ok.den"), torch.ones(100, device="cuda"))
+        assert np.array_equal(np.fromfile(str(tmp_path / "ok.den"), np.float32), np.ones(100, np.float32))

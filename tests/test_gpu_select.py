@@ -39,3 +39,25 @@ def test_select_vs_host_and_reference(gpu_built):
                 assert np.array_equal(got_i, want_i) and np.array_equal(got_p, want_p), (len(pos), periodic)
         empty_i, empty_p = _gpu(d, np.zeros((0, 3), np.float32), full, [0, 1, 0, 1, 0, 1], True)
         assert len(empty_i) == 0 and empty_p.shape == (0, 3)
+
+
+def test_select_capacity_and_arguments(gpu_built):
+    """A capacity below the selection is refused with the count returned and
+    nothing written; 2^31 particles and more are refused."""
+    import ctypes as C
+    import torch
+    from dtfe_b200 import _native as N
+    from dtfe_b200.device import DeviceDTFE
+    pos = torch.rand(5000, 3, device="cuda") * 100
+    full = np.array([0, 100, 0, 100, 0, 100], np.float32)
+    padded = np.array([-5, 105, -5, 105, -5, 105], np.float32)
+    idx = torch.full((10,), -7, dtype=torch.int32, device="cuda")
+    with DeviceDTFE(0) as d:
+        cnt = C.c_int64(0)
+        rc = d.lib.dtfe_gpu_select_in_box_dev(d.h, pos.data_ptr(), 5000, full.ctypes.data, padded.ctypes.data, 1,
+                                              idx.data_ptr(), None, 10, C.byref(cnt))
+        assert rc == N.ERR_TOO_LARGE and cnt.value > 5000
+        assert (idx.cpu().numpy() == -7).all()
+        rc = d.lib.dtfe_gpu_select_in_box_dev(d.h, pos.data_ptr(), 1 << 31, full.ctypes.data, padded.ctypes.data, 1,
+                                              None, None, 0, C.byref(cnt))
+        assert rc == N.ERR_TOO_LARGE

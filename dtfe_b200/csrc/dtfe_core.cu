@@ -908,6 +908,9 @@ __device__ __forceinline__ void zero_after_outside(const InterpParams& P, int* _
 // the z pencil re-locates that outside point and gets zeros.  One warp per
 // pencil of the sub-box tiles.
 __global__ void __launch_bounds__(256) k_outside_pencils(InterpParams P, int* __restrict__ tet_c, int64_t n_pencils) {
+  // the locate kernels of this call have counted the outside samples: none,
+  // nothing to zero (every thread reads the same count, so all return)
+  if (*(volatile const unsigned long long*)&P.counters[CNT_OUTSIDE] == 0ull) return;
   const int lane = threadIdx.x & 31;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t q = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; q < n_pencils; q += nw) {
@@ -926,6 +929,7 @@ __global__ void __launch_bounds__(256) k_outside_pencils(InterpParams P, int* __
 // (unaveraged_interpolation.cc:466 jumps over :527), so the rest of its psi
 // row repeats it.  Rows of nz samples, sample index = output row.
 __global__ void __launch_bounds__(256) k_cone_rows(InterpParams P, int* __restrict__ tet_c, int64_t n_rows, int nz) {
+  if (*(volatile const unsigned long long*)&P.counters[CNT_OUTSIDE] == 0ull) return;  // no bin outside
   const int lane = threadIdx.x & 31;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t q = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; q < n_rows; q += nw)

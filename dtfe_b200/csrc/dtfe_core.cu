@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(kSortBlock) k_sort_incidence_staged(int64_t V,
 }
 
 // ---- per step ------------------------------------------------------------
-constexpr int kVolBlock = 256;
+constexpr int kVolBlock = 64;  // 64: 5.67 ms per 256^3 step; 128: 5.70; 256: 5.77; 512: 6.21
 
 // Signed volume of every tetrahedron (FP64, streamed out once) and, when
 // DO_BINS, the walk seeds: per grid cell, among the tetrahedra whose
@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(kRasterBlock, MINB) k_tet_volume_raster(
 // handles 32 consecutive vertices, whose incidence lists are contiguous: it
 // stages the lists' volumes in shared memory with coalesced loads (in chunks),
 // then every lane sums its own list sequentially.
-constexpr int kDensBlock = 256;
+constexpr int kDensBlock = 64;  // 64: 5.59 ms per 256^3 step (volumes at 64); 128: 5.63; 256: 5.67
 constexpr int kDensChunk = 512;  // incidences staged per warp and pass
 __global__ void __launch_bounds__(kDensBlock) k_vertex_density(
     int64_t V, const float* __restrict__ w, const double* __restrict__ vol, const int64_t* __restrict__ off,

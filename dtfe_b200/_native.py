@@ -50,7 +50,18 @@ class PlanView(C.Structure):
                 ("n_xs", C.c_int64), ("n_ys", C.c_int64), ("n_zs", C.c_int64),
                 ("n_particles", C.c_int64), ("dep_pos", C.c_void_p), ("dep_weight", C.c_void_p),
                 ("dep_velocity", C.c_void_p), ("dep_src", C.c_void_p), ("n_dep_boxes", C.c_int32),
-                ("dep_boxes", C.c_void_p)]
+                ("dep_boxes", C.c_void_p), ("region", C.c_float * 6)]
+
+
+class PlanOptions(C.Structure):
+    """dtfe_plan_options (include/dtfe_host.h)."""
+    _fields_ = [("n_parts", C.c_int32), ("padding_mode", C.c_int32), ("padding_particles", C.c_float),
+                ("padding", C.c_float * 6), ("region_on", C.c_int32), ("region", C.c_float * 6),
+                ("partition_on", C.c_int32), ("partition", C.c_int32 * 3), ("part_no", C.c_int32),
+                ("average_density", C.c_double)]
+
+
+PAD_PARTICLES, PAD_RELATIVE, PAD_ABSOLUTE = 0, 1, 2
 
 
 class InterpOpts(C.Structure):
@@ -143,6 +154,8 @@ def host() -> C.CDLL:
         lib.dtfe_tets_unpack.argtypes = [vp, C.c_int64, vp, vp]
         lib.dtfe_plan_build.argtypes = [C.c_int, vp, vp, vp, vp, C.c_int32, C.c_int64, vp, C.c_int, vp, C.c_int32,
                                         C.c_float, C.c_double, C.POINTER(C.c_void_p)]
+        lib.dtfe_plan_build_ex.argtypes = [C.c_int, vp, vp, vp, vp, C.c_int32, C.c_int64, vp, C.c_int, vp,
+                                           C.POINTER(PlanOptions), C.POINTER(C.c_void_p)]
         lib.dtfe_plan_get.argtypes = [C.c_void_p, C.POINTER(PlanView)]
         lib.dtfe_plan_release.argtypes = [C.c_void_p]
         _host = lib
@@ -180,6 +193,8 @@ def gpu() -> C.CDLL:
                                                    C.POINTER(C.c_int64)]
         lib.dtfe_gpu_download_vertex_density.argtypes = [H, vp]
         lib.dtfe_gpu_locate_points.argtypes = [H, C.c_int64, vp, C.c_int32, vp]
+        lib.dtfe_gpu_download_located.argtypes = [H, vp]
+        lib.dtfe_gpu_set_max_walk_steps.argtypes = [H, C.c_int32]
         lib.dtfe_gpu_stream.argtypes = [H]
         lib.dtfe_gpu_stream.restype = C.c_void_p
         lib.dtfe_gpu_synchronize.argtypes = [H]

@@ -80,7 +80,9 @@ def build_oracle(force: bool = False) -> str:
     return out
 
 
-REFERENCE_TREE = "/root/reference"
+# the reference source tree (read only; the harness and the drop-in compile
+# against it where it exists): DTFE_REFERENCE_TREE, else the default checkout
+REFERENCE_TREE = os.environ.get("DTFE_REFERENCE_TREE", "/root/reference")
 
 
 def build_ref() -> str | None:

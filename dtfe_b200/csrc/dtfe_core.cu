@@ -71,6 +71,23 @@ __global__ void k_pack_xyz(int64_t n, const float* __restrict__ xyz, float4* __r
   if (i < n) out[i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], wval);
 }
 
+// Range check of a plain upload before any kernel indexes with it: vertex
+// ids in [0, V), neighbour ids in [-1, T).  Reads only the uploaded arrays;
+// every tetrahedron out of range counts into *bad.
+__global__ void k_check_tets(int64_t T, int64_t V, const int4* __restrict__ tet_v, const int4* __restrict__ tet_n,
+                             unsigned long long* __restrict__ bad) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  bool ok = true;
+  if (t < T) {
+    const int4 v = __ldg(&tet_v[t]);
+    const int4 n = __ldg(&tet_n[t]);
+    ok = v.x >= 0 && v.x < V && v.y >= 0 && v.y < V && v.z >= 0 && v.z < V && v.w >= 0 && v.w < V &&
+         n.x >= -1 && n.x < T && n.y >= -1 && n.y < T && n.z >= -1 && n.z < T && n.w >= -1 && n.w < T;
+  }
+  const unsigned nbad = __popc(__ballot_sync(0xffffffffu, !ok));
+  if ((threadIdx.x & 31) == 0 && nbad) atomicAdd(bad, (unsigned long long)nbad);
+}
+
 __global__ void k_hull_marks(int64_t T, const int4* __restrict__ tet_v, const int4* __restrict__ tet_n,
                              int* __restrict__ hull) {
   int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -1866,7 +1883,13 @@ static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const fl
   // then the kernels: decode the tetrahedra, pack positions and velocities
   // into 16-byte records
   DTFE_CUDA_TRY(cudaMemsetAsync(h->counters + CNT_DECODE, 0, sizeof(unsigned long long), st));
-  if (n_tets && (rc = tets_finish(h, stage))) return rc;
+  if (n_tets && (rc = tets_finish(h, stage))) {
+    // nothing usable was uploaded: later calls see an empty handle
+    h->T = h->V = 0;
+    h->density_ready = h->prep_ready = h->tet_c_valid = false;
+    drop_graph(h);
+    return rc;
+  }
   if (n_verts) {
     k_pack_xyz<<<blocks_for(n_verts, 256), 256, 0, st>>>(n_verts, sx, h->posd, 0.f);
     if (vel) k_pack_xyz<<<blocks_for(n_verts, 256), 256, 0, st>>>(n_verts, sv, h->vel4, 0.f);
@@ -1913,7 +1936,24 @@ int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n, i
         DTFE_CUDA_TRY(cudaMemcpyAsync(hh->tet_n, tet_n, 16 * n_tets, cudaMemcpyHostToDevice, hh->stream));
         return DTFE_OK;
       },
-      [&](dtfe_handle, char*) -> int { return DTFE_OK; });
+      [&](dtfe_handle hh, char*) -> int {
+        // every id in range before the hull, incidence and walk kernels use
+        // them: the check waits for its count (the packed path's decoder
+        // sanitises instead and reports at the next status read)
+        unsigned long long bad = 0;
+        k_check_tets<<<blocks_for(n_tets, 256), 256, 0, hh->stream>>>(n_tets, n_verts, hh->tet_v, hh->tet_n,
+                                                                       hh->counters + CNT_DECODE);
+        DTFE_CUDA_TRY(cudaGetLastError());
+        DTFE_CUDA_TRY(cudaMemcpyAsync(&bad, hh->counters + CNT_DECODE, sizeof(bad), cudaMemcpyDeviceToHost,
+                                      hh->stream));
+        DTFE_CUDA_TRY(cudaStreamSynchronize(hh->stream));
+        if (bad) {
+          DTFE_CUDA_TRY(cudaMemsetAsync(hh->counters + CNT_DECODE, 0, sizeof(unsigned long long), hh->stream));
+          return set_error(DTFE_ERR_ARG, std::to_string(bad) + " tetrahedra with a vertex id outside [0, n_verts)"
+                                         " or a neighbour id outside [-1, n_tets)");
+        }
+        return DTFE_OK;
+      });
 }
 
 int dtfe_gpu_upload_packed(dtfe_handle h, const void* packed, int64_t packed_bytes, const float* xyz,
@@ -3028,6 +3068,39 @@ int dtfe_gpu_locate_points(dtfe_handle h, int64_t np, const double* pts, int32_t
   DTFE_CUDA_TRY(cudaFreeAsync(dp, st));
   DTFE_CUDA_TRY(cudaFreeAsync(dout, st));
   DTFE_CUDA_TRY(cudaStreamSynchronize(st));
+  return DTFE_OK;
+}
+
+int dtfe_gpu_set_max_walk_steps(dtfe_handle h, int32_t max_walk_steps) {
+  if (!h) return set_error(DTFE_ERR_ARG, "null handle");
+  if (max_walk_steps < 0) return set_error(DTFE_ERR_ARG, "max_walk_steps must be >= 0");
+  h->max_steps = max_walk_steps > 0 ? max_walk_steps : 65536;
+  drop_graph(h);  // a captured step holds the old limit
+  return DTFE_OK;
+}
+
+// Per grid cell the tetrahedron its centre was located in by the last
+// cell-centre interpolation (tet_c is kept per sample, in tile order: each
+// sample goes back to its main-grid cell); -1 outside the hull and for cells
+// outside every tile.
+int dtfe_gpu_download_located(dtfe_handle h, int32_t* loc) {
+  if (!h || !loc) return set_error(DTFE_ERR_ARG, "null argument");
+  if (!h->tet_c_valid) return set_error(DTFE_ERR_STATE, "no cell-centre interpolation to report");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  std::vector<int32_t> per_sample((size_t)h->n_cells);
+  DTFE_CUDA_TRY(cudaMemcpyAsync(per_sample.data(), h->tet_c, sizeof(int32_t) * h->n_cells, cudaMemcpyDeviceToHost,
+                                h->stream));
+  DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  const int64_t G = (int64_t)h->grid[0] * h->grid[1] * h->grid[2];
+  std::fill(loc, loc + G, -1);
+  int64_t s = 0;
+  for (const dtfe_subbox& B : h->boxes_h)
+    for (int i = 0; i < B.tile_dims[0]; ++i)
+      for (int j = 0; j < B.tile_dims[1]; ++j) {
+        const int64_t row = ((int64_t)(B.tile_origin[0] + i) * h->grid[1] + (B.tile_origin[1] + j)) * h->grid[2] +
+                            B.tile_origin[2];
+        for (int k = 0; k < B.tile_dims[2]; ++k, ++s) loc[row + k] = per_sample[s] < 0 ? -1 : per_sample[s];
+      }
   return DTFE_OK;
 }
 

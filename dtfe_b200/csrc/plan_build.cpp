@@ -3,8 +3,9 @@
 // (src/DTFE.cpp:76-251, 287-385), for callers without Python — the DTFE()
 // drop-in in particular.  Same arithmetic and ordering as dtfe_b200/plan.py
 // (make_plan, make_deposit_plan), so both produce identical plans:
-//   padding (updatePadding), average density, periodic images of the padded
-//   box (findParticlesInBox), parallelGrid + optimalPartitionSplit into
+//   padding (updatePadding, given lengths included), average density,
+//   --region and --partition / --partNo chunks, periodic images of the
+//   padded box (findParticlesInBox), parallelGrid + optimalPartitionSplit into
 //   sub-boxes, each sub-box's particles of its padded region, vertices in
 //   Morton order, tessellation of every sub-box in parallel, concatenation
 //   with global ids, per-sub-box coordinate tables (the x += dx raster).
@@ -18,6 +19,7 @@
 #include <vector>
 
 #include "../../include/dtfe_host.h"
+#include "morton.h"
 
 struct dtfe_plan_s {
   dtfe_plan_view view{};
@@ -43,49 +45,6 @@ struct Tile {
   int part_no;
 };
 
-uint64_t spread21(uint64_t x) {
-  x &= 0x1FFFFFull;
-  x = (x | (x << 32)) & 0x1F00000000FFFFull;
-  x = (x | (x << 16)) & 0x1F0000FF0000FFull;
-  x = (x | (x << 8)) & 0x100F00F00F00F00Full;
-  x = (x | (x << 4)) & 0x10C30C30C30C30C3ull;
-  x = (x | (x << 2)) & 0x1249249249249249ull;
-  return x;
-}
-
-// Stable Z-order permutation (quantisation to 21 bits per axis over the
-// set's bounding box in double), as plan.morton_order.
-std::vector<int64_t> morton_order(const std::vector<float>& pos) {
-  const int64_t n = (int64_t)pos.size() / 3;
-  std::vector<int64_t> order(n);
-  std::iota(order.begin(), order.end(), 0);
-  if (n == 0) return order;
-  float mn[3] = {pos[0], pos[1], pos[2]}, mx[3] = {pos[0], pos[1], pos[2]};
-  for (int64_t i = 0; i < n; ++i)
-    for (int c = 0; c < 3; ++c) {
-      mn[c] = std::min(mn[c], pos[3 * i + c]);
-      mx[c] = std::max(mx[c], pos[3 * i + c]);
-    }
-  double lo[3], ext[3];
-  for (int c = 0; c < 3; ++c) {
-    lo[c] = (double)mn[c];
-    ext[c] = std::max((double)mx[c] - lo[c], 1e-30);
-  }
-  const double top = (double)((1 << 21) - 1);
-  std::vector<uint64_t> key(n);
-  for (int64_t i = 0; i < n; ++i) {
-    uint64_t q[3];
-    for (int c = 0; c < 3; ++c) {
-      double v = ((double)pos[3 * i + c] - lo[c]) / ext[c] * top;
-      v = v < 0.0 ? 0.0 : (v > top ? top : v);
-      q[c] = (uint64_t)v;
-    }
-    key[i] = spread21(q[0]) | (spread21(q[1]) << 1) | (spread21(q[2]) << 2);
-  }
-  std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return key[a] < key[b]; });
-  return order;
-}
-
 PointSet select(const float* pos, int64_t n, const float box[6], const float padded[6], int periodic) {
   PointSet s;
   const int64_t m = dtfe_select_in_box(pos, n, box, padded, periodic, nullptr, nullptr);
@@ -95,30 +54,26 @@ PointSet select(const float* pos, int64_t n, const float box[6], const float pad
   return s;
 }
 
-// decompose() of plan.py: the padded, imaged particle set and its split.
-int decompose(const float* pos, int64_t n, const int64_t grid[3], const float box[6], int periodic,
-              int32_t n_parts, const float pad[6], std::vector<PointSet>& sets, std::vector<Tile>& tiles) {
-  const float padded[6] = {box[0] - pad[0], box[1] + pad[1], box[2] - pad[2],
-                           box[3] + pad[3], box[4] - pad[4], box[5] + pad[5]};
-  PointSet all;
-  if (periodic) {
-    all = select(pos, n, box, padded, 1);
-  } else {
-    all.src.resize(n);
-    std::iota(all.src.begin(), all.src.end(), 0);
-    all.pos.assign(pos, pos + 3 * n);
-  }
+// DTFE_parallel (src/DTFE.cpp:287-385) on one region's particles `all`:
+// parallelGrid(n_parts) sub-boxes of the region's grid, balanced by
+// optimalPartitionSplit, each with the particles of its padded sub-box
+// (non-periodic, findParticlesInBox); the tiles are placed at `origin` in the
+// output grid.  A single part interpolates the region directly with every
+// particle (the one-thread branch, :300-305), under `single_part_no`.
+int parallel_split(PointSet all, const int64_t grid[3], const float region[6], const int64_t origin[3],
+                   int32_t n_parts, const float pad[6], int single_part_no, std::vector<PointSet>& sets,
+                   std::vector<Tile>& tiles) {
   int64_t pg[3];
   dtfe_parallel_grid(n_parts, grid, pg);
   const int64_t np = pg[0] * pg[1] * pg[2];
   if (np == 1) {
     Tile t;
     for (int a = 0; a < 3; ++a) {
-      t.origin[a] = 0;
+      t.origin[a] = origin[a];
       t.dims[a] = grid[a];
     }
-    std::memcpy(t.region, box, sizeof(t.region));
-    t.part_no = -1;
+    std::memcpy(t.region, region, sizeof(t.region));
+    t.part_no = single_part_no;
     sets.push_back(std::move(all));
     tiles.push_back(t);
     return 0;
@@ -126,7 +81,7 @@ int decompose(const float* pos, int64_t n, const int64_t grid[3], const float bo
   std::vector<int64_t> sub(6 * np);
   std::vector<float> coords(6 * np);
   const int64_t nall = (int64_t)all.src.size();
-  if (dtfe_optimal_partition(all.pos.data(), nall, grid, box, pg, sub.data(), coords.data())) return 1;
+  if (dtfe_optimal_partition(all.pos.data(), nall, grid, region, pg, sub.data(), coords.data())) return 1;
   for (int64_t k = 0; k < np; ++k) {
     const float* r = &coords[6 * k];
     const float pb[6] = {r[0] - pad[0], r[1] + pad[1], r[2] - pad[2], r[3] + pad[3], r[4] - pad[4], r[5] + pad[5]};
@@ -134,15 +89,98 @@ int decompose(const float* pos, int64_t n, const int64_t grid[3], const float bo
     for (auto& i : part.src) i = all.src[i];
     Tile t;
     for (int a = 0; a < 3; ++a) {
-      t.origin[a] = sub[6 * k + 2 * a];
+      t.origin[a] = origin[a] + sub[6 * k + 2 * a];
       t.dims[a] = sub[6 * k + 2 * a + 1] - sub[6 * k + 2 * a];
     }
     std::memcpy(t.region, r, sizeof(t.region));
-    t.part_no = (int)k;
+    t.part_no = (int)k;  // DTFE_parallel's tempOptions.partNo = thread number
     sets.push_back(std::move(part));
     tiles.push_back(t);
   }
   return 0;
+}
+
+// findParticlesInBox of a subset: the particles of `from` in `padded`, with
+// their input ids.
+PointSet select_from(const PointSet& from, const float full_box[6], const float padded[6], int periodic) {
+  PointSet s = select(from.pos.data(), (int64_t)from.src.size(), full_box, padded, periodic);
+  for (auto& i : s.src) i = from.src[i];
+  return s;
+}
+
+// The steps of DTFE() from its option checks to its DTFE_parallel calls
+// (src/DTFE.cpp:76-251): --region selects the particles of the padded region
+// (periodic images on the full box) and makes the region the full box,
+// non-periodic; --partition splits the region with optimalPartitionSplit
+// into chunks, each selecting the particles of its padded chunk, and runs
+// DTFE_parallel on every chunk into its place in the main grid, or, with
+// --partNo, on that one chunk into a grid of the chunk's size; otherwise the
+// padded box (with periodic images) feeds one DTFE_parallel over the region.
+// grid_out / region_out: the grid and region the results cover.
+int flow(const float* pos, int64_t n, const float box[6], int periodic, const int32_t grid[3],
+         const dtfe_plan_options& o, const float pad[6], std::vector<PointSet>& sets, std::vector<Tile>& tiles,
+         int32_t grid_out[3], float region_out[6]) {
+  const int64_t g64[3] = {grid[0], grid[1], grid[2]};
+  const int64_t zero[3] = {0, 0, 0};
+  float full[6];
+  std::memcpy(full, box, sizeof(full));
+  int per = periodic;
+  PointSet cur;
+  cur.src.resize(n);
+  std::iota(cur.src.begin(), cur.src.end(), 0);
+  cur.pos.assign(pos, pos + 3 * n);
+  float region[6];
+  std::memcpy(region, box, sizeof(region));
+  if (o.region_on) {
+    std::memcpy(region, o.region, sizeof(region));
+    // Box::validSubBox (src/box.h:115-138)
+    for (int a = 0; a < 3; ++a) {
+      const float lo = box[2 * a], hi = box[2 * a + 1];
+      const bool bad = per ? (region[2 * a] < 2 * lo - hi || region[2 * a + 1] > 2 * hi - lo)
+                           : (region[2 * a] < lo || region[2 * a + 1] > hi);
+      if (bad) return 4;
+    }
+    const float padded[6] = {region[0] - pad[0], region[1] + pad[1], region[2] - pad[2],
+                             region[3] + pad[3], region[4] - pad[4], region[5] + pad[5]};
+    cur = select_from(cur, full, padded, per);
+    per = 0;
+    std::memcpy(full, region, sizeof(full));
+  }
+  for (int a = 0; a < 3; ++a) grid_out[a] = grid[a];
+  std::memcpy(region_out, region, sizeof(region));
+  if (o.partition_on) {
+    const int64_t parts[3] = {o.partition[0], o.partition[1], o.partition[2]};
+    const int64_t np = parts[0] * parts[1] * parts[2];
+    if (parts[0] < 1 || parts[1] < 1 || parts[2] < 1 || o.part_no >= np) return 1;
+    std::vector<int64_t> sub(6 * np);
+    std::vector<float> coords(6 * np);
+    if (dtfe_optimal_partition(cur.pos.data(), (int64_t)cur.src.size(), g64, region, parts, sub.data(),
+                               coords.data()))
+      return 1;
+    const int64_t first = o.part_no >= 0 ? o.part_no : 0, last = o.part_no >= 0 ? o.part_no + 1 : np;
+    for (int64_t k = first; k < last; ++k) {
+      const float* r = &coords[6 * k];
+      const float padded[6] = {r[0] - pad[0], r[1] + pad[1], r[2] - pad[2], r[3] + pad[3], r[4] - pad[4],
+                               r[5] + pad[5]};
+      const int64_t dims[3] = {sub[6 * k + 1] - sub[6 * k], sub[6 * k + 3] - sub[6 * k + 2],
+                               sub[6 * k + 5] - sub[6 * k + 4]};
+      const int64_t at[3] = {sub[6 * k], sub[6 * k + 2], sub[6 * k + 4]};
+      if (parallel_split(select_from(cur, full, padded, per), dims, r, o.part_no >= 0 ? zero : at, o.n_parts, pad,
+                         (int)k, sets, tiles))
+        return 1;
+      if (o.part_no >= 0) {
+        for (int a = 0; a < 3; ++a) grid_out[a] = (int32_t)dims[a];
+        std::memcpy(region_out, r, sizeof(float) * 6);
+      }
+    }
+    return 0;
+  }
+  if (!o.region_on && per) {
+    const float padded[6] = {box[0] - pad[0], box[1] + pad[1], box[2] - pad[2],
+                             box[3] + pad[3], box[4] - pad[4], box[5] + pad[5]};
+    cur = select_from(cur, box, padded, 1);
+  }
+  return parallel_split(std::move(cur), g64, region, zero, o.n_parts, pad, -1, sets, tiles);
 }
 
 template <class T>
@@ -156,7 +194,7 @@ int assemble(dtfe_plan_s& P, std::vector<PointSet>& sets, const std::vector<Tile
              const float* vel, const float* scal, int32_t S) {
   const int k = (int)sets.size();
   for (auto& s : sets) {
-    const std::vector<int64_t> o = morton_order(s.pos);
+    const std::vector<int64_t> o = dtfe::morton_order(s.pos.data(), (int64_t)s.pos.size() / 3);
     PointSet t;
     t.src.resize(o.size());
     t.pos.resize(3 * o.size());
@@ -241,7 +279,7 @@ void deposit_assemble(dtfe_plan_s& P, std::vector<PointSet>& sets, const std::ve
   int64_t off = 0;
   P.dep_boxes.resize(sets.size());
   for (size_t k = 0; k < sets.size(); ++k) {
-    const std::vector<int64_t> o = morton_order(sets[k].pos);
+    const std::vector<int64_t> o = dtfe::morton_order(sets[k].pos.data(), (int64_t)sets[k].pos.size() / 3);
     for (int64_t i : o) {
       for (int c = 0; c < 3; ++c) P.dep_pos.push_back(sets[k].pos[3 * i + c]);
       P.dep_src.push_back(sets[k].src[i]);
@@ -270,30 +308,46 @@ void deposit_assemble(dtfe_plan_s& P, std::vector<PointSet>& sets, const std::ve
 
 extern "C" {
 
-int dtfe_plan_build(int kind, const float* pos, const float* w, const float* vel, const float* scal, int32_t S,
-                    int64_t n, const float box[6], int periodic, const int32_t grid[3], int32_t n_parts,
-                    float padding_particles, double average_density, dtfe_plan* out) {
-  if (!out || !box || !grid || (n > 0 && !pos) || n_parts < 1 || kind < 0 || kind > 3) return 1;
+int dtfe_plan_build_ex(int kind, const float* pos, const float* w, const float* vel, const float* scal, int32_t S,
+                       int64_t n, const float box[6], int periodic, const int32_t grid[3],
+                       const dtfe_plan_options* opts, dtfe_plan* out) {
+  if (!out || !box || !grid || !opts || (n > 0 && !pos) || opts->n_parts < 1 || kind < 0 || kind > 3) return 1;
   *out = nullptr;
+  const dtfe_plan_options& o = *opts;
+  if (o.padding_mode < DTFE_PAD_PARTICLES || o.padding_mode > DTFE_PAD_ABSOLUTE) return 1;
   std::unique_ptr<dtfe_plan_s> P(new (std::nothrow) dtfe_plan_s());
   if (!P) return 3;
   const int64_t g64[3] = {grid[0], grid[1], grid[2]};
   const float blen[3] = {box[1] - box[0], box[3] - box[2], box[5] - box[4]};
-  // updatePadding kinds: DTFE/SPH 0, TSC/NGP 1, CIC 2
-  const int pad_kind = kind == DTFE_PLAN_DTFE ? 0 : (kind == DTFE_PLAN_CIC ? 2 : 1);
+  // User_options::updatePadding (src/user_options.cc:1062-1089): six given
+  // lengths unless all are zero (isNullBox), in box lengths or absolute;
+  // else the particle count's padding for the estimator (DTFE/SPH 0,
+  // TSC/NGP 1, CIC 2)
   float pad[6];
-  dtfe_padding_length(pad_kind, padding_particles, n, blen, g64, pad);
-  const double rho_bar = average_density > 0.0 ? (double)(float)average_density : (double)dtfe_average_density(w, n);
+  bool given = false;
+  for (int i = 0; i < 6; ++i) given = given || (o.padding_mode != DTFE_PAD_PARTICLES && o.padding[i] != 0.f);
+  if (given) {
+    for (int i = 0; i < 6; ++i)
+      pad[i] = o.padding_mode == DTFE_PAD_RELATIVE ? o.padding[i] * blen[i % 2] : o.padding[i];
+  } else {
+    const int pad_kind = kind == DTFE_PLAN_DTFE ? 0 : (kind == DTFE_PLAN_CIC ? 2 : 1);
+    dtfe_padding_length(pad_kind, o.padding_particles, n, blen, g64, pad);
+  }
+  const double rho_bar =
+      o.average_density > 0.0 ? (double)(float)o.average_density : (double)dtfe_average_density(w, n);
   std::vector<PointSet> sets;
   std::vector<Tile> tiles;
-  if (decompose(pos, n, g64, box, periodic, n_parts, pad, sets, tiles)) return 1;
+  int32_t grid_out[3];
+  float region_out[6];
+  if (int frc = flow(pos, n, box, periodic, grid, o, pad, sets, tiles, grid_out, region_out)) return frc;
   int rc = 0;
   if (kind == DTFE_PLAN_DTFE) rc = assemble(*P, sets, tiles, w, vel, scal, S);
   else deposit_assemble(*P, sets, tiles, w, vel);
   if (rc) return rc;
   dtfe_plan_view& v = P->view;
   v.kind = kind;
-  for (int a = 0; a < 3; ++a) v.grid[a] = grid[a];
+  for (int a = 0; a < 3; ++a) v.grid[a] = grid_out[a];
+  std::memcpy(v.region, region_out, sizeof(region_out));
   v.rho_bar = rho_bar;
   std::memcpy(v.padding, pad, sizeof(pad));
   v.n_verts = (int64_t)P->src.size();
@@ -324,6 +378,19 @@ int dtfe_plan_build(int kind, const float* pos, const float* w, const float* vel
   v.dep_boxes = P->dep_boxes.data();
   *out = P.release();
   return 0;
+}
+
+int dtfe_plan_build(int kind, const float* pos, const float* w, const float* vel, const float* scal, int32_t S,
+                    int64_t n, const float box[6], int periodic, const int32_t grid[3], int32_t n_parts,
+                    float padding_particles, double average_density, dtfe_plan* out) {
+  dtfe_plan_options o;
+  std::memset(&o, 0, sizeof(o));
+  o.n_parts = n_parts;
+  o.padding_mode = DTFE_PAD_PARTICLES;
+  o.padding_particles = padding_particles;
+  o.part_no = -1;
+  o.average_density = average_density;
+  return dtfe_plan_build_ex(kind, pos, w, vel, scal, S, n, box, periodic, grid, &o, out);
 }
 
 int dtfe_plan_get(dtfe_plan p, dtfe_plan_view* view) {

@@ -112,8 +112,9 @@ class DeviceDTFE:
         optr = (C.c_void_p * N.NUM_FIELDS)(*outs)
         st = N.Status()
         o = self._opts(fields, method, n_samples, seed, fix, fix_outside)
-        N.check(self.lib.dtfe_gpu_interpolate(self.h, C.byref(o), optr, C.byref(st)))
-        self.last_status = st.as_dict()
+        rc = self.lib.dtfe_gpu_interpolate(self.h, C.byref(o), optr, C.byref(st))
+        self.last_status = st.as_dict()  # also when the call reports a walk failure
+        N.check(rc)
         return res
 
     def interpolate_async(self, fields, out: dict, method: int = 0, n_samples: int = 1, seed: int = 0,
@@ -354,6 +355,17 @@ class DeviceDTFE:
 
     def set_variants(self, locate: int, evaluate: int) -> None:
         N.check(self.lib.dtfe_gpu_set_variants(self.h, locate, evaluate))
+
+    def download_located(self) -> np.ndarray:
+        """Per grid cell the tetrahedron of the last cell-centre interpolation
+        (dtfe_gpu_download_located): int32 (G,), -1 outside the hull."""
+        out = np.empty(int(np.prod(self.grid)), np.int32)
+        N.check(self.lib.dtfe_gpu_download_located(self.h, out.ctypes.data))
+        return out
+
+    def set_max_walk_steps(self, n: int) -> None:
+        """Step limit of the point-location walks (0 = default)."""
+        N.check(self.lib.dtfe_gpu_set_max_walk_steps(self.h, int(n)))
 
     def locate_points(self, pts: np.ndarray, start: int = 0) -> np.ndarray:
         pts = np.ascontiguousarray(pts, np.float64)

@@ -47,6 +47,7 @@ class Plan:
     padding: np.ndarray        # (6,) float32
     timings: dict = field(default_factory=dict)
     regions: np.ndarray | None = None  # (K, 6) float32 tile regions (xmin, xmax, ymin, ymax, zmin, zmax)
+    covered_region: np.ndarray | None = None  # (6,) float32 the region the grid covers
 
     @property
     def n_tets(self) -> int:
@@ -431,10 +432,16 @@ def _view_array(ptr, dtype, shape):
 
 def native_plan(kind: str, pos, weight, velocity=None, scalar=None, grid=(64, 64, 64),
                 box=(0, 100, 0, 100, 0, 100), periodic: bool = True, n_threads: int = 1,
-                padding_particles: float = 5.0, average_density_value: float | None = None):
-    """The same plan built by the C++ planner (dtfe_plan_build,
+                padding_particles: float = 5.0, average_density_value: float | None = None,
+                region=None, partition=None, part_no: int = -1, padding=None, padding_absolute: bool = False):
+    """The same plan built by the C++ planner (dtfe_plan_build_ex,
     include/dtfe_host.h): a Plan for "DTFE", a DepositPlan for "NGP", "CIC",
-    "TSC"."""
+    "TSC".  DTFE()'s options: region (6 absolute coordinates, --region),
+    partition (3 chunk counts, --partition) with part_no (--partNo, -1 all
+    chunks), padding (6 lengths, in box lengths or absolute with
+    padding_absolute: --padding l1..l6 / --paddingMpc).  The plan's grid
+    and .covered_region are what the results cover (one chunk's with
+    part_no >= 0)."""
     kinds = {"DTFE": 0, "NGP": 1, "CIC": 2, "TSC": 3}
     k = kinds[kind]
     pos = _f32(pos)
@@ -446,14 +453,26 @@ def native_plan(kind: str, pos, weight, velocity=None, scalar=None, grid=(64, 64
     g = np.ascontiguousarray(grid, np.int32)
     lib = N.host()
     h = C.c_void_p()
-    rc = lib.dtfe_plan_build(k, pos.ctypes.data, None if w is None else w.ctypes.data,
-                             None if vel is None else vel.ctypes.data, None if sc is None else sc.ctypes.data, S,
-                             len(pos), bx.ctypes.data, int(periodic), g.ctypes.data, int(n_threads),
-                             float(padding_particles),
-                             float(np.float32(average_density_value)) if average_density_value is not None else 0.0,
-                             C.byref(h))
+    o = N.PlanOptions()
+    o.n_parts = int(n_threads)
+    o.padding_particles = float(padding_particles)
+    o.padding_mode = N.PAD_PARTICLES
+    if padding is not None:
+        o.padding_mode = N.PAD_ABSOLUTE if padding_absolute else N.PAD_RELATIVE
+        o.padding[:] = [float(x) for x in np.asarray(padding, np.float32)]
+    if region is not None:
+        o.region_on = 1
+        o.region[:] = [float(x) for x in np.asarray(region, np.float32)]
+    if partition is not None:
+        o.partition_on = 1
+        o.partition[:] = [int(x) for x in partition]
+    o.part_no = int(part_no)
+    o.average_density = float(np.float32(average_density_value)) if average_density_value is not None else 0.0
+    rc = lib.dtfe_plan_build_ex(k, pos.ctypes.data, None if w is None else w.ctypes.data,
+                                None if vel is None else vel.ctypes.data, None if sc is None else sc.ctypes.data, S,
+                                len(pos), bx.ctypes.data, int(periodic), g.ctypes.data, C.byref(o), C.byref(h))
     if rc:
-        raise RuntimeError(f"dtfe_plan_build failed with status {rc}")
+        raise RuntimeError(f"dtfe_plan_build_ex failed with status {rc}")
     try:
         v = N.PlanView()
         lib.dtfe_plan_get(h, C.byref(v))
@@ -470,7 +489,8 @@ def native_plan(kind: str, pos, weight, velocity=None, scalar=None, grid=(64, 64
                         ys=_view_array(v.ys, np.float32, (v.n_ys,)), zs=_view_array(v.zs, np.float32, (v.n_zs,)),
                         grid=tuple(int(x) for x in v.grid), rho_bar=float(v.rho_bar),
                         padding=np.array(list(v.padding), np.float32),
-                        regions=_view_array(v.regions, np.float32, (K, 6)) if v.regions else None)
+                        regions=_view_array(v.regions, np.float32, (K, 6)) if v.regions else None,
+                        covered_region=np.array(list(v.region), np.float32))
         n, K = v.n_particles, v.n_dep_boxes
         boxes = (N.DepositBox * K)()
         C.memmove(C.addressof(boxes), v.dep_boxes, C.sizeof(N.DepositBox) * K)

@@ -25,15 +25,20 @@
 // (redshiftConeOn) gives them on its gridSize bins (interpolateRedshiftCone).
 // Volume averages there are Monte-Carlo averages, as the reference forces
 // (method 2, 20 points unless noPointsOn; Philox offsets instead of mt19937).
+// --region, --partition / --partNo and given padding lengths (--padding
+// l1..l6, --paddingMpc) plan as the reference's DTFE() does; the chunks of
+// --partition run in one batched GPU step instead of one after another, and
+// --partNo returns the chunk's grid only, as the reference.
 // Unlike the reference, failures throw std::runtime_error instead of calling
-// exit(), and options this path does not cover throw as well: --region,
-// --partition, random subsamples, Poisson particles, explicit padding
-// lengths, scalar fields with NGP/CIC/TSC, NGP/CIC/TSC/SPH at user points or
-// on cones.  The GPU is device 0 unless DTFE_GPU_DEVICE names another.
+// exit(), and options this path does not cover throw as well: random
+// subsamples, Poisson particles, scalar fields with NGP/CIC/TSC,
+// NGP/CIC/TSC/SPH at user points or on cones.  The GPU is device 0 unless
+// DTFE_GPU_DEVICE names another.
 
 #include <omp.h>
 
 #include <cstdlib>
+#include <cstring>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -135,13 +140,21 @@ void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& s
   }
   unsupported(cone && (o.redshiftCone.coords.size() != 6 || o.originPosition.size() != 3),
               "redshift cones without 6 limits and a 3-D origin");
-  unsupported(o.regionOn, "--region");
-  unsupported(o.partitionOn, "--partition");
   unsupported(o.randomSample >= Real(0.), "random subsamples");
   unsupported(o.poisson != 0, "Poisson particles");
-  unsupported(o.paddingOn && !o.paddingLength.coords.empty() && o.paddingLength.coords[0] != Real(0.),
-              "explicit padding lengths");
   unsupported(o.gridSize.size() != 3, "grids other than 3-D regular grids");
+  unsupported(o.boxCoordinates.coords.size() != 6, "a box without 6 coordinates");
+  unsupported(o.regionOn && o.region.coords.size() != 6, "--region without 6 coordinates");
+  unsupported(o.partitionOn && o.partition.size() != 3, "--partition without 3 chunk counts");
+  unsupported(!o.paddingLength.coords.empty() && o.paddingLength.coords.size() != 6,
+              "padding lengths other than 6 values");
+  // --partition is not available at user points or on cones
+  // (User_options::updateEntries, src/user_options.cc:986-995)
+  if (o.partitionOn && (user_points || cone)) {
+    o.partitionOn = false;
+    for (size_t i = 0; i < o.partition.size(); ++i) o.partition[i] = 1;
+    o.partNo = -1;
+  }
   const bool dtfe = !(o.NGP || o.CIC || o.TSC || o.SPH);
   unsupported(dtfe && any(o.aField) && (o.method < 1 || o.method > 3), "averaging methods other than 1, 2, 3");
   unsupported(!dtfe && !o.SPH && (o.aField.scalar || o.aField.scalar_gradient), "scalar fields with NGP/CIC/TSC");
@@ -175,18 +188,55 @@ void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& s
 
   float box[6];
   for (int i = 0; i < 6; ++i) box[i] = o.boxCoordinates.coords[i];
-  const int32_t grid[3] = {(int32_t)o.gridSize[0], (int32_t)o.gridSize[1], (int32_t)o.gridSize[2]};
-  const size_t G = (size_t)grid[0] * grid[1] * grid[2];
+  const int32_t main_grid[3] = {(int32_t)o.gridSize[0], (int32_t)o.gridSize[1], (int32_t)o.gridSize[2]};
   if (o.averageDensity < Real(0.)) o.averageDensity = dtfe_average_density(w.data(), n);
   const int kind = dtfe || o.SPH ? DTFE_PLAN_DTFE : (o.NGP ? DTFE_PLAN_NGP : (o.CIC ? DTFE_PLAN_CIC : DTFE_PLAN_TSC));
 
+  // the planning options, as User_options::updateEntries / updatePadding
+  // read them (src/user_options.cc:926-1089), box fractions converted with
+  // the reference's own [i % 2] indexing of the box offset and length
+  dtfe_plan_options po;
+  std::memset(&po, 0, sizeof(po));
+  po.n_parts = user_points || cone ? 1 : omp_get_max_threads();  // no split (src/DTFE.cpp:301)
+  po.padding_particles = (float)o.paddingParticles;
+  po.padding_mode = DTFE_PAD_PARTICLES;
+  if (o.paddingLength.coords.size() == 6) {
+    po.padding_mode = o.paddingOn && !o.paddingMpcOn ? DTFE_PAD_RELATIVE : DTFE_PAD_ABSOLUTE;
+    for (int i = 0; i < 6; ++i) po.padding[i] = o.paddingLength.coords[i];
+  }
+  const float off[3] = {box[0], box[2], box[4]}, len[3] = {box[1] - box[0], box[3] - box[2], box[5] - box[4]};
+  if (o.regionOn) {
+    po.region_on = 1;
+    for (int i = 0; i < 6; ++i)
+      po.region[i] = o.regionMpcOn ? (float)o.region.coords[i] : off[i % 2] + (float)o.region.coords[i] * len[i % 2];
+  }
+  if (o.partitionOn) {
+    po.partition_on = 1;
+    for (int a = 0; a < 3; ++a) po.partition[a] = (int32_t)o.partition[a];
+    po.part_no = o.partNo;
+  } else {
+    po.part_no = -1;
+  }
+  po.average_density = (double)o.averageDensity;
+
   PlanGuard plan;
-  check(dtfe_plan_build(kind, pos.data(), w.data(), velp, scp, S, n, box, o.periodic ? 1 : 0, grid,
-                        user_points || cone ? 1 : omp_get_max_threads(),  // no split (src/DTFE.cpp:301)
-                        (float)o.paddingParticles, (double)o.averageDensity, &plan.p),
-        "planning");
+  const int prc = dtfe_plan_build_ex(kind, pos.data(), w.data(), velp, scp, S, n, box, o.periodic ? 1 : 0, main_grid,
+                                     &po, &plan.p);
+  if (prc == 4)
+    throw std::runtime_error("DTFE (GPU): the region is not a valid sub-box of the data box (Box::validSubBox)");
+  if (prc) throw std::runtime_error("DTFE (GPU): planning failed (status " + std::to_string(prc) + ")");
   dtfe_plan_view v;
   check(dtfe_plan_get(plan.p, &v), "plan view");
+  // what updateEntries and DTFE() leave in userOptions: the padding as
+  // absolute lengths, the region in absolute coordinates (the box without
+  // --region; the chunk with --partNo, src/DTFE.cpp:151)
+  o.paddingLength.coords.assign(v.padding, v.padding + 6);
+  o.paddingOn = o.paddingMpcOn = true;
+  o.region.coords.assign(v.region, v.region + 6);
+  if (o.regionOn) o.regionMpcOn = true;
+  // the grid the results cover: the chunk's own with --partNo
+  const int32_t grid[3] = {v.grid[0], v.grid[1], v.grid[2]};
+  const size_t G = (size_t)grid[0] * grid[1] * grid[2];
 
   dtfe_config cfg = {0, dtfe || o.SPH ? S : 0, 0, 0};
   if (const char* d = std::getenv("DTFE_GPU_DEVICE")) cfg.device = std::atoi(d);
@@ -232,7 +282,7 @@ void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& s
     dtfe_interp_opts io = {DTFE_METHOD_CENTRE, 1, 0, 0, 0};
     outputs(o.uField, uQuantities, m, out, &io.fields);
     int64_t kept = 0;
-    check(dtfe_gpu_interpolate_points(gpu.h, (int64_t)m, pts.data(), box, &io, out, &kept),
+    check(dtfe_gpu_interpolate_points(gpu.h, (int64_t)m, pts.data(), v.region, &io, out, &kept),
           "interpolation at user sampling points");
     resize_all(o.uField, uQuantities, (size_t)kept);
   } else if (any(o.uField) && cone) {
@@ -267,7 +317,7 @@ void DTFE(std::vector<Particle_data>* allParticles, std::vector<Sample_point>& s
         }
       outputs(f, aQuantities, m, out, &io.fields);
       int64_t kept = 0;
-      check(dtfe_gpu_average_points(gpu.h, (int64_t)m, pts.data(), dl.data(), box, &io, out, &kept),
+      check(dtfe_gpu_average_points(gpu.h, (int64_t)m, pts.data(), dl.data(), v.region, &io, out, &kept),
             "volume averages at user sampling points");
       resize_all(f, aQuantities, (size_t)kept);
     } else {

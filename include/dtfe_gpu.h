@@ -146,6 +146,10 @@ const char* dtfe_last_error(void);
 /* Upload a (multi-)tessellation and its vertex data (host arrays).
  * xyz: 3V floats (vertex positions, Particle_data::pos), w: V weights,
  * vel: 3V velocities or NULL, scal: V*S scalars or NULL.
+ * Every tet_v entry must lie in [0, n_verts) and every tet_n entry in
+ * [-1, n_tets): a device kernel checks them before anything indexes with
+ * them and the call returns DTFE_ERR_ARG (the handle then holds nothing)
+ * otherwise.
  * Replaces the CGAL vertex storage filled by vertexData::setData
  * (src/CGAL_triangulation/vertexData.h:45-56). */
 int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n,
@@ -392,6 +396,20 @@ int dtfe_gpu_download_vertex_density(dtfe_handle h, float* dens);
  * hull, -2 walk failure.  (dt.locate, unaveraged_interpolation.cc:289.) */
 int dtfe_gpu_locate_points(dtfe_handle h, int64_t np, const double* pts, int32_t start,
                            int32_t* out);
+/* The tetrahedron each cell centre was located in by the handle's last
+ * cell-centre interpolation: loc (host, grid cells) receives per main-grid
+ * cell the canonical tetrahedron id (the Cell_handle that dt.locate returns
+ * at unaveraged_interpolation.cc:289, as an index into tet_v), -1 for a
+ * centre outside the hull (the reference's infinite cell) and for cells
+ * outside every tile.  DTFE_ERR_STATE before a cell-centre interpolation. */
+int dtfe_gpu_download_located(dtfe_handle h, int32_t* loc);
+/* Step limit of every point-location walk (dtfe_config::max_walk_steps;
+ * 0 = the default 65536).  A walk that reaches it counts as a failure: its
+ * sample gets zeros and the call reports DTFE_ERR_WALK with
+ * dtfe_status::n_walk_failures > 0; the handle stays usable.  The reference
+ * has no such limit (CGAL's walk has none; its errors exit the process,
+ * src/message.h:57-64). */
+int dtfe_gpu_set_max_walk_steps(dtfe_handle h, int32_t max_walk_steps);
 
 /* Vertex densities without any device allocation, for callers that cannot
  * let a library allocate: host applications that hand out all device memory

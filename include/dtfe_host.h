@@ -12,7 +12,7 @@
  *   dtfe_optimal_partition   optimalPartitionSplit         src/subpartition.h:163-372
  *   dtfe_axis_coords         the x += dx sample raster     src/unaveraged_interpolation.cc:252-358
  *   dtfe_tessellate(_batch)  delaunayTriangulation         src/CGAL_triangulation/triangulation.cpp:162-195
- *   dtfe_plan_build          DTFE() + DTFE_parallel() up to the interpolation
+ *   dtfe_plan_build(_ex)     DTFE() + DTFE_parallel() up to the interpolation
  *                            src/DTFE.cpp:76-251, 287-385
  *   dtfe_write_binary        writeBinaryFile               src/io/binary_io.cc:185-216
  *   dtfe_field_suffix        writeOutputData's file names  src/input_output.cc:216-275
@@ -95,7 +95,32 @@ typedef struct {
   const int64_t* dep_src;     /* n */
   int32_t n_dep_boxes;
   const dtfe_deposit_box* dep_boxes;
+  /* the region the grid covers: the box, the --region, or with --partNo the
+   * chunk (the reference sets userOptions.region to it, src/DTFE.cpp:151) */
+  float region[6];
 } dtfe_plan_view;
+
+/* Options of DTFE() that change the planning (User_options members,
+ * src/user_options.h:100-190). */
+enum {
+  DTFE_PAD_PARTICLES = 0, /* --padding n: n particle spacings (paddingParticles) */
+  DTFE_PAD_RELATIVE = 1,  /* --padding l1..l6: lengths in box lengths */
+  DTFE_PAD_ABSOLUTE = 2   /* --paddingMpc l1..l6: lengths in the particles' units */
+};
+typedef struct {
+  int32_t n_parts;          /* parallelGrid split (the OpenMP thread count) */
+  int32_t padding_mode;     /* DTFE_PAD_*; six zero lengths fall back to the particle count, as
+                               User_options::updatePadding (isNullBox) */
+  float padding_particles;  /* paddingParticles (5 by default) */
+  float padding[6];         /* paddingLength: left/right per axis, x first */
+  int32_t region_on;        /* --region: interpolate only region[6] */
+  float region[6];          /* absolute coordinates (User_options::updateEntries converts box
+                               fractions, src/user_options.cc:952-958) */
+  int32_t partition_on;     /* --partition: split into partition[0..2] chunks */
+  int32_t partition[3];
+  int32_t part_no;          /* --partNo: only that chunk (its own grid); -1 all chunks */
+  double average_density;   /* <= 0: the reference's automatic value */
+} dtfe_plan_options;
 
 /* Plans one box of n particles (pos 3n, w n or NULL = unit, vel 3n or
  * NULL, scal S*n or NULL) in [box] on a grid of grid[0..2] cells, split
@@ -107,6 +132,18 @@ typedef struct {
 int dtfe_plan_build(int kind, const float* pos, const float* w, const float* vel, const float* scal, int32_t S,
                     int64_t n, const float box[6], int periodic, const int32_t grid[3], int32_t n_parts,
                     float padding_particles, double average_density, dtfe_plan* out);
+/* Same with DTFE()'s region, partition and padding options
+ * (src/DTFE.cpp:76-251): --region selects the particles of the padded region
+ * and interpolates only there; --partition plans every chunk of
+ * optimalPartitionSplit with its own padded particles, each split further
+ * into n_parts sub-boxes, all placed in the main grid (the GPU runs them in
+ * one batched step instead of one chunk after another); --partNo plans one
+ * chunk onto a grid of its own size (view.grid, view.region).  Returns 0, 1
+ * for bad arguments, 4 for a region that is not a valid sub-box of the box
+ * (Box::validSubBox, src/box.h:115-138). */
+int dtfe_plan_build_ex(int kind, const float* pos, const float* w, const float* vel, const float* scal, int32_t S,
+                       int64_t n, const float box[6], int periodic, const int32_t grid[3],
+                       const dtfe_plan_options* opts, dtfe_plan* out);
 int dtfe_plan_get(dtfe_plan p, dtfe_plan_view* view);
 void dtfe_plan_release(dtfe_plan p);
 

@@ -363,6 +363,40 @@ int oracle_vertex_density(int64_t T, const int32_t* tv, const int32_t* tn, int64
   return 0;
 }
 
+// The reference's own vertexDensity arithmetic (triangulation.cpp:200-279):
+// per vertex the float sum `Real vol += volume(cell)` of its incident finite
+// cells in ascending cell id (the harness's incident_cells order), each
+// volume the double determinant / 6 rounded to float (volume(),
+// triangulation_miscellaneous.cc:205-213); 0 when an incident cell is
+// infinite; density = (weight * factor) / vol in float, factor =
+// (NO_DIM+1.) / averageDensity as a float.
+int oracle_vertex_density_ref(int64_t T, const int32_t* tv, const int32_t* tn, int64_t V, const float* xyz,
+                              const float* w, double rho_bar, float* dens, int K, const dtfe_subbox* boxes,
+                              int nthreads) {
+  std::vector<float> vol(V, 0.f);
+  std::vector<char> hull(V, 0);
+  const int nb = (K > 0 && boxes) ? K : 1;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads > 0 ? nthreads : 1)
+  for (int b = 0; b < nb; ++b) {
+    int64_t lo = (K > 0 && boxes) ? boxes[b].tet_offset : 0;
+    int64_t hi = (K > 0 && boxes) ? boxes[b].tet_offset + boxes[b].n_tets : T;
+    for (int64_t t = lo; t < hi; ++t) {  // ascending: every vertex adds its cells in ascending id
+      double X[4][3];
+      for (int a = 0; a < 4; ++a)
+        for (int k = 0; k < 3; ++k) X[a][k] = (double)xyz[3 * (int64_t)tv[4 * t + a] + k];
+      const float vt = (float)(dtfe::orient_det(X[0], X[1], X[2], X[3]) / 6.0);
+      for (int a = 0; a < 4; ++a) vol[tv[4 * t + a]] += vt;
+      for (int i = 0; i < 4; ++i)
+        if (tn[4 * t + i] < 0)
+          for (int a = 0; a < 4; ++a)
+            if (a != i) hull[tv[4 * t + a]] = 1;
+    }
+  }
+  const float factor = (float)(4.0 / (double)(float)rho_bar);
+  for (int64_t v = 0; v < V; ++v) dens[v] = hull[v] ? 0.f : (w[v] * factor) / vol[v];
+  return 0;
+}
+
 // Canonical location of np points (double xyz) in tetrahedra [lo, hi).
 int oracle_locate(int64_t T, const int32_t* tv, const int32_t* tn, const float* xyz,
                   int64_t lo, int64_t hi, int64_t np, const double* pts, int64_t* out) {

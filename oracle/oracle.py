@@ -32,6 +32,8 @@ def lib() -> C.CDLL:
         vp = C.c_void_p
         L.oracle_vertex_density.argtypes = [C.c_int64, vp, vp, C.c_int64, vp, vp, C.c_double, vp, vp, vp,
                                             C.c_int, vp, C.c_int]
+        L.oracle_vertex_density_ref.argtypes = [C.c_int64, vp, vp, C.c_int64, vp, vp, C.c_double, vp, C.c_int, vp,
+                                                C.c_int]
         L.oracle_locate.argtypes = [C.c_int64, vp, vp, vp, C.c_int64, C.c_int64, C.c_int64, vp, vp]
         L.oracle_interpolate.argtypes = [C.c_int64, vp, vp, C.c_int64, vp, vp, vp, C.c_int, vp, vp, C.c_int,
                                          vp, vp, vp, vp, vp, C.POINTER(N.InterpOpts), C.c_int,
@@ -167,6 +169,17 @@ def vertex_density(plan, rho_bar: float | None = None, nthreads: int = 0):
                                 d32.ctypes.data, d64.ctypes.data, vs.ctypes.data,
                                 plan.n_boxes, C.addressof(plan.boxes), nthreads or (os.cpu_count() or 1))
     return d32, d64, vs
+
+
+def vertex_density_ref(plan, rho_bar: float | None = None, nthreads: int = 0) -> np.ndarray:
+    """The reference's own vertexDensity arithmetic (float sums of the
+    incident cells' float volumes in ascending cell id): float32 (V,)."""
+    rb = plan.rho_bar if rho_bar is None else rho_bar
+    out = np.empty(plan.n_verts, np.float32)
+    lib().oracle_vertex_density_ref(plan.n_tets, plan.tet_v.ctypes.data, plan.tet_n.ctypes.data, plan.n_verts,
+                                    plan.xyz.ctypes.data, plan.weight.ctypes.data, rb, out.ctypes.data,
+                                    plan.n_boxes, C.addressof(plan.boxes), nthreads or (os.cpu_count() or 1))
+    return out
 
 
 def locate(plan, pts: np.ndarray, box: int = 0) -> np.ndarray:

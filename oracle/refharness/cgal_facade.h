@@ -30,6 +30,7 @@
 #include <utility>
 #include <vector>
 
+#include "../../dtfe_b200/csrc/morton.h"
 #include "../../dtfe_b200/csrc/predicates.h"
 
 extern "C" int dtfe_tessellate(const double* xyz, int64_t n, uint64_t seed, int sort_tets, void** handle);
@@ -265,10 +266,15 @@ class Delaunay_triangulation_3 {
     }
     Cell* h = hint;
     Cell* t = (h && !h->infinite) ? h : (h && h->infinite ? h->n[0] : finite_cells_[0]);
+    int zmask = 0;  // faces of the final cell through p
     for (size_t step = 0; step < 4 * finite_cells_.size() + 64; ++step) {
       int exit = -1;
-      for (int i = 0; i < 4 && exit < 0; ++i)
-        if (face_sign(t, i, p) < 0) exit = i;
+      zmask = 0;
+      for (int i = 0; i < 4 && exit < 0; ++i) {
+        const int s = face_sign(t, i, p);
+        if (s < 0) exit = i;
+        else if (s == 0) zmask |= 1 << i;
+      }
       if (exit < 0) break;
       Cell* nb = t->n[exit];
       if (nb->infinite) {
@@ -277,25 +283,33 @@ class Delaunay_triangulation_3 {
       }
       t = nb;
     }
-    // canonical tie rule: lowest id among the finite cells whose closure holds p
+    lt = CELL;
+    // p strictly inside: no other cell's closure holds it
+    if (zmask == 0) return t;
+    // canonical tie rule: lowest id among the finite cells whose closure
+    // holds p (they share the face, edge or vertex through p), searched
+    // across the faces through p
     Cell* best = t;
-    std::vector<Cell*> seen{t}, queue{t};
-    while (!queue.empty()) {
-      Cell* u = queue.back();
-      queue.pop_back();
+    constexpr int kSeen = 256;
+    Cell* seen[kSeen];
+    Cell* queue[kSeen];
+    int n_seen = 1, n_queue = 1;
+    seen[0] = queue[0] = t;
+    while (n_queue > 0) {
+      Cell* u = queue[--n_queue];
       for (int i = 0; i < 4; ++i) {
         if (face_sign(u, i, p) != 0) continue;
         Cell* nb = u->n[i];
-        if (nb->infinite || std::find(seen.begin(), seen.end(), nb) != seen.end()) continue;
-        seen.push_back(nb);
+        if (nb->infinite || std::find(seen, seen + n_seen, nb) != seen + n_seen) continue;
+        if (n_seen == kSeen) return best;  // more cells around p than any vertex star holds here
+        seen[n_seen++] = nb;
         bool inside = true;
         for (int k = 0; k < 4 && inside; ++k) inside = face_sign(nb, k, p) >= 0;
         if (!inside) continue;
-        queue.push_back(nb);
+        queue[n_queue++] = nb;
         if (nb->id < best->id) best = nb;
       }
     }
-    lt = CELL;
     return best;
   }
   Cell_handle locate(const Point& p, Locate_type& lt, int& li, Cell_handle hint = Cell_handle()) {
@@ -320,10 +334,17 @@ class Delaunay_triangulation_3 {
 
   void ensure() {
     if (built_) return;
-    // tessellate the inserted points with the project's exact tessellator
-    std::vector<double> xyz(3 * verts_.size());
+    // tessellate the inserted points with the project's exact tessellator,
+    // numbered in the planner's Z-order (CGAL's own cell vertex order is
+    // internal to it): the cells, their vertex order and ids are then those
+    // of the planner's sub-box for the same points
+    std::vector<double> pts(3 * verts_.size());
     for (size_t i = 0; i < verts_.size(); ++i)
-      for (int k = 0; k < 3; ++k) xyz[3 * i + k] = verts_[i]->p.c[k];
+      for (int k = 0; k < 3; ++k) pts[3 * i + k] = verts_[i]->p.c[k];
+    const std::vector<int64_t> order = dtfe::morton_order(pts.data(), (int64_t)verts_.size());
+    std::vector<double> xyz(3 * verts_.size());
+    for (size_t r = 0; r < order.size(); ++r)
+      for (int k = 0; k < 3; ++k) xyz[3 * r + k] = pts[3 * order[r] + k];
     void* h = nullptr;
     dtfe_tessellate(xyz.data(), (int64_t)verts_.size(), 12345, 1, &h);
     int64_t nt = 0, np = 0, nd = 0;
@@ -331,6 +352,7 @@ class Delaunay_triangulation_3 {
     std::vector<int32_t> tv(4 * nt), tn(4 * nt), vm(np);
     dtfe_tess_export(h, tv.data(), tn.data(), vm.data());
     dtfe_tess_release(h);
+    for (auto& q : tv) q = (int32_t)order[q];  // rank -> inserted vertex
     link(nt, tv.data(), tn.data());
   }
 

@@ -88,27 +88,8 @@ User_options::User_options() {
 
 extern "C" {
 
-// GSL stand-ins: gsl_qrng_sobol as the Bratley-Fox construction of
-// dtfe_b200/csrc/sobol.h (the only generator averaging method 1 uses).
-struct gsl_qrng_type_s {
-  int id;
-};
-struct gsl_qrng_s {
-  mutable dtfe::Sobol3 seq;
-};
-static const gsl_qrng_type kSobolType{1};
-static const gsl_qrng_type kNiederreiterType{2};
-const gsl_qrng_type* gsl_qrng_sobol = &kSobolType;
-const gsl_qrng_type* gsl_qrng_niederreiter_2 = &kNiederreiterType;
-gsl_qrng* gsl_qrng_alloc(const gsl_qrng_type* T, unsigned int d) {
-  if (T != gsl_qrng_sobol || d != 3) {
-    std::fprintf(stderr, "reference harness: only the 3-dimensional Sobol generator is available\n");
-    std::abort();
-  }
-  return new gsl_qrng;
-}
-int gsl_qrng_get(const gsl_qrng* q, double* x) { return q->seq.next(x) ? 0 : 1; }
-void gsl_qrng_free(gsl_qrng* q) { delete q; }
+// GSL stand-ins: gsl_standin.cpp (linked into the same library).
+
 
 // Runs the reference on one (sub-box) tessellation with LOCAL indices.
 //   which: 0 cell-centre (interpolateGrid), 1 / 2 / 3 averaging methods.

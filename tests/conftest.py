@@ -45,6 +45,21 @@ def rel_err(a, b):
     return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), rms))) if b.size else 0.0
 
 
+def rel_err_plain(a, b, floor_frac=0.01):
+    """max_i |a_i - b_i| / |b_i| over the entries with |b_i| above floor_frac
+    times the field's RMS (the plain relative error; entries nearer zero are
+    cancellation residues whose relative error says nothing)."""
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    if not b.size:
+        return 0.0
+    rms = np.sqrt(np.mean(b * b))
+    keep = np.abs(b) > floor_frac * rms
+    if not keep.any():
+        return 0.0
+    return float(np.max(np.abs(a[keep] - b[keep]) / np.abs(b[keep])))
+
+
 GOLDEN = os.path.join(ROOT, "tests", "golden", "ref_zeldovich10.npz")
 
 

@@ -152,6 +152,9 @@ def host() -> C.CDLL:
         lib.dtfe_tets_pack.argtypes = [vp, vp, C.c_int64, vp]
         lib.dtfe_tets_pack.restype = C.c_int64
         lib.dtfe_tets_unpack.argtypes = [vp, C.c_int64, vp, vp]
+        lib.dtfe_tets_pack_vertices.argtypes = [vp, C.c_int64, vp]
+        lib.dtfe_tets_pack_vertices.restype = C.c_int64
+        lib.dtfe_tets_unpack_vertices.argtypes = [vp, C.c_int64, vp]
         lib.dtfe_plan_build.argtypes = [C.c_int, vp, vp, vp, vp, C.c_int32, C.c_int64, vp, C.c_int, vp, C.c_int32,
                                         C.c_float, C.c_double, C.POINTER(C.c_void_p)]
         lib.dtfe_plan_build_ex.argtypes = [C.c_int, vp, vp, vp, vp, C.c_int32, C.c_int64, vp, C.c_int, vp,
@@ -194,6 +197,7 @@ def gpu() -> C.CDLL:
         lib.dtfe_gpu_download_vertex_density.argtypes = [H, vp]
         lib.dtfe_gpu_locate_points.argtypes = [H, C.c_int64, vp, C.c_int32, vp]
         lib.dtfe_gpu_download_located.argtypes = [H, vp]
+        lib.dtfe_gpu_download_tets.argtypes = [H, vp, vp]
         lib.dtfe_gpu_set_max_walk_steps.argtypes = [H, C.c_int32]
         lib.dtfe_gpu_stream.argtypes = [H]
         lib.dtfe_gpu_stream.restype = C.c_void_p

@@ -90,7 +90,7 @@ def build_ref() -> str | None:
     exists; elsewhere the prebuilt library, if any, is used as is."""
     if not os.path.isdir(os.path.join(REFERENCE_TREE, "src")):
         return None
-    _run(["make", "-s", "-C", ORACLE, "ref", "REF=" + REFERENCE_TREE])
+    _run(["make", "-s", "-C", ORACLE, "ref", "refmain", "REF=" + REFERENCE_TREE])
     return os.path.join(ORACLE, "_ref", "libdtfe_ref.so")
 
 

@@ -72,7 +72,8 @@ __global__ void k_pack_xyz(int64_t n, const float* __restrict__ xyz, float4* __r
 }
 
 // Range check of a plain upload before any kernel indexes with it: vertex
-// ids in [0, V), neighbour ids in [-1, T).  Reads only the uploaded arrays;
+// ids in [0, V), neighbour ids (when given) in [-1, T).  Reads only the
+// uploaded arrays;
 // every tetrahedron out of range counts into *bad.
 __global__ void k_check_tets(int64_t T, int64_t V, const int4* __restrict__ tet_v, const int4* __restrict__ tet_n,
                              unsigned long long* __restrict__ bad) {
@@ -80,7 +81,7 @@ __global__ void k_check_tets(int64_t T, int64_t V, const int4* __restrict__ tet_
   bool ok = true;
   if (t < T) {
     const int4 v = __ldg(&tet_v[t]);
-    const int4 n = __ldg(&tet_n[t]);
+    const int4 n = tet_n ? __ldg(&tet_n[t]) : make_int4(-1, -1, -1, -1);
     ok = v.x >= 0 && v.x < V && v.y >= 0 && v.y < V && v.z >= 0 && v.z < V && v.w >= 0 && v.w < V &&
          n.x >= -1 && n.x < T && n.y >= -1 && n.y < T && n.z >= -1 && n.z < T && n.w >= -1 && n.w < T;
   }
@@ -214,6 +215,123 @@ __global__ void __launch_bounds__(kPackBlock)
   }
   tet_v[t] = make_int4(v[0], v[1], v[2], v[3]);
   tet_n[t] = make_int4(n[0], n[1], n[2], n[3]);
+}
+
+// Decoder of the vertex-only packed tessellation (dtfe_tets_pack_vertices,
+// host_plan.cpp), laid out as k_unpack_tets: one thread per tetrahedron, one
+// block per packing block of 256, the block's bytes staged in shared memory.
+// Block scans place each thread's fields (4 bytes + one per bit of its width
+// nibble) and its first escape, and a third scan adds up the first-vertex
+// differences from the block's base.  Every read is checked against the
+// buffer and every vertex against [0, V) and the canonical order (first
+// vertex smallest, second smallest of the rest); a violation counts into
+// *err and stores vertex 0 four times, so later kernels stay in range.
+__global__ void __launch_bounds__(kPackBlock)
+    k_unpack_tet_vertices(int64_t T, int64_t V, const int32_t* __restrict__ base, const int32_t* __restrict__ esc_off,
+                          const int64_t* __restrict__ boff, const uint8_t* __restrict__ flags,
+                          const uint8_t* __restrict__ orient, const uint32_t* __restrict__ data, int64_t data_bytes,
+                          const int32_t* __restrict__ esc, int64_t n_esc, int4* __restrict__ tet_v,
+                          unsigned long long* err) {
+  __shared__ uint32_t s_data[kPackMaxBlockBytes / 4 + 2];
+  __shared__ int s_scan[3][kPackBlock / 32];
+  const int64_t b = blockIdx.x;
+  const int64_t t = b * kPackBlock + threadIdx.x;
+  const bool valid = t < T;
+  const int flag = valid ? ((int)__ldg(&flags[t >> 1]) >> ((t & 1) * 4)) & 15 : 0;
+  const int size = valid ? 4 + __popc(flag) : 0;
+  int block_bytes;
+  const int off = pack_block_scan(size, s_scan[0], &block_bytes);
+  const int64_t b0 = __ldg(&boff[b]), b1 = __ldg(&boff[b + 1]);
+  const bool block_ok = b0 >= 0 && b1 - b0 == block_bytes && b1 <= data_bytes;
+  const int64_t w0 = block_ok ? b0 >> 2 : 0;
+  const int nw = block_ok ? (int)(((b1 + 3) >> 2) - w0) : 0;
+  for (int i = threadIdx.x; i < nw; i += kPackBlock) s_data[i] = __ldg(&data[w0 + i]);
+  __syncthreads();
+  const uint8_t* sb = (const uint8_t*)s_data + (block_ok ? (b0 & 3) : 0);
+  uint32_t raw[4];
+  int p = off, ne = 0;
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    const bool wide = (flag >> f) & 1;
+    raw[f] = sb[p++];
+    if (wide) raw[f] |= (uint32_t)sb[p++] << 8;
+    if (f == 0) ne += (wide ? (int)(int16_t)raw[0] : (int)(int8_t)raw[0]) == (wide ? 32767 : 127);
+    else ne += raw[f] == (wide ? 0xFFFFu : 0xFFu);
+  }
+  if (!valid) ne = 0;
+  const int e_in = pack_block_scan(ne, s_scan[1], nullptr);
+  const int64_t e0 = (int64_t)__ldg(&esc_off[b]) + e_in;
+  bool ok = block_ok && e0 >= 0 && e0 + ne <= n_esc;
+  const int32_t* e = esc + (ok ? e0 : 0);
+  int d[4] = {0, 0, 0, 0};
+  if (valid && ok) {
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      const bool wide = (flag >> f) & 1;
+      if (f == 0) {
+        const int sv = wide ? (int)(int16_t)raw[0] : (int)(int8_t)raw[0];
+        d[0] = sv == (wide ? 32767 : 127) ? __ldg(e++) : sv;
+      } else {
+        d[f] = raw[f] == (wide ? 0xFFFFu : 0xFFu) ? __ldg(e++) : (int)raw[f];
+      }
+    }
+  }
+  // first vertex: the block's base plus the differences up to this tetrahedron
+  const int before = pack_block_scan(d[0], s_scan[2], nullptr);
+  if (!valid) return;
+  const int64_t v0 = (int64_t)__ldg(&base[b]) + before + d[0];
+  const int64_t v1 = v0 + d[1], lo = v1 + d[2], hi = lo + d[3];
+  ok = ok && v0 >= 0 && d[1] > 0 && d[2] > 0 && d[3] > 0 && hi < V;
+  if (!ok) {
+    atomicAdd(err, 1ull);
+    tet_v[t] = make_int4(0, 0, 0, 0);
+    return;
+  }
+  const bool third_larger = (__ldg(&orient[t >> 3]) >> (t & 7)) & 1;
+  tet_v[t] = make_int4((int)v0, (int)v1, (int)(third_larger ? hi : lo), (int)(third_larger ? lo : hi));
+}
+
+// Neighbour array from the vertex array and the incidence lists (ascending):
+// the tetrahedra around edge (v0, v1) of t are the common entries of the
+// lists of v0 and v1; among them (t aside) the one holding v2 lies across
+// the face opposite v3 and the one holding v3 across the face opposite v2.
+// Edge (v2, v3) gives the faces opposite v0 and v1 the same way.  A face no
+// other tetrahedron holds is on the convex hull (-1, CGAL's infinite cell).
+__device__ __forceinline__ bool holds(const int4& u, int v) { return u.x == v || u.y == v || u.z == v || u.w == v; }
+
+__device__ __forceinline__ void edge_faces(int t, int a, int b, int c, int d, const int64_t* __restrict__ off,
+                                           const int* __restrict__ inc, const int4* __restrict__ tet_v, int& nc,
+                                           int& nd) {
+  // nc: the tetrahedron holding (a, b, c), nd: the one holding (a, b, d)
+  int64_t i = __ldg(&off[a]), ie = __ldg(&off[a + 1]);
+  int64_t j = __ldg(&off[b]), je = __ldg(&off[b + 1]);
+  while (i < ie && j < je) {
+    const int x = __ldg(&inc[i]), y = __ldg(&inc[j]);
+    if (x < y) {
+      ++i;
+    } else if (y < x) {
+      ++j;
+    } else {
+      if (x != t) {
+        const int4 u = __ldg(&tet_v[x]);
+        if (holds(u, c)) nc = x;
+        else if (holds(u, d)) nd = x;
+      }
+      ++i;
+      ++j;
+    }
+  }
+}
+
+__global__ void k_derive_neighbours(int64_t T, const int4* __restrict__ tet_v, const int64_t* __restrict__ off,
+                                    const int* __restrict__ inc, int4* __restrict__ tet_n) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= T) return;
+  const int4 q = __ldg(&tet_v[t]);
+  int n0 = -1, n1 = -1, n2 = -1, n3 = -1;
+  edge_faces((int)t, q.x, q.y, q.z, q.w, off, inc, tet_v, n3, n2);  // faces (v0 v1 v2), (v0 v1 v3)
+  edge_faces((int)t, q.z, q.w, q.y, q.x, off, inc, tet_v, n0, n1);  // faces (v2 v3 v1), (v2 v3 v0)
+  tet_n[t] = make_int4(n0, n1, n2, n3);
 }
 
 __global__ void k_degree(int64_t T, const int4* __restrict__ tet_v, int* __restrict__ deg) {
@@ -1843,7 +1961,7 @@ extern "C++" {
 template <class TetH2D, class TetFinish>
 static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const float* w, const float* vel,
                        const float* scal, int64_t n_verts, size_t tets_bytes, TetH2D tets_h2d,
-                       TetFinish tets_finish) {
+                       TetFinish tets_finish, bool derive_neighbours = false) {
   if (!h || !xyz || !w) return set_error(DTFE_ERR_ARG, "null argument");
   if (n_tets < 0 || n_verts < 0 || n_tets > 0x7FFFFFFF || n_verts >= 0x7F7F7F7F)
     return set_error(DTFE_ERR_TOO_LARGE, "tetrahedron or vertex count beyond int32 indexing");
@@ -1896,9 +2014,6 @@ static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const fl
     else DTFE_CUDA_TRY(cudaMemsetAsync(h->vel4, 0, sizeof(float4) * n_verts, st));
     if (h->S > 0 && !scal) DTFE_CUDA_TRY(cudaMemsetAsync(h->scal, 0, sizeof(float) * h->S * n_verts, st));
   }
-  // hull vertices (a property of the tessellation's topology)
-  if (n_verts) DTFE_CUDA_TRY(cudaMemsetAsync(h->hull, 0, sizeof(int) * n_verts, st));
-  if (n_tets) k_hull_marks<<<blocks_for(n_tets, 256), 256, 0, st>>>(n_tets, h->tet_v, h->tet_n, h->hull);
   // vertex -> tetrahedron incidence lists (ascending tetrahedron ids)
   if (n_verts) {
     DTFE_CUDA_TRY(cudaMemsetAsync(h->scratch_i, 0, sizeof(int) * n_verts, st));
@@ -1914,6 +2029,12 @@ static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const fl
                                                                                        h->inc);
     }
   }
+  // neighbours from the vertices, when they did not cross
+  if (n_tets && derive_neighbours)
+    k_derive_neighbours<<<blocks_for(n_tets, 256), 256, 0, st>>>(n_tets, h->tet_v, h->inc_off, h->inc, h->tet_n);
+  // hull vertices (a property of the tessellation's topology)
+  if (n_verts) DTFE_CUDA_TRY(cudaMemsetAsync(h->hull, 0, sizeof(int) * n_verts, st));
+  if (n_tets) k_hull_marks<<<blocks_for(n_tets, 256), 256, 0, st>>>(n_tets, h->tet_v, h->tet_n, h->hull);
   DTFE_CUDA_TRY(cudaGetLastError());
   h->has_vel = vel != nullptr;
   h->has_scal = scal != nullptr;
@@ -1928,12 +2049,13 @@ static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const fl
 int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n, int64_t n_tets,
                     const float* xyz, const float* w, const float* vel, const float* scal,
                     int64_t n_verts) {
-  if (!tet_v || !tet_n) return set_error(DTFE_ERR_ARG, "null argument");
+  if (n_tets > 0 && !tet_v) return set_error(DTFE_ERR_ARG, "null argument");
   return upload_impl(
       h, n_tets, xyz, w, vel, scal, n_verts, 0,
       [&](dtfe_handle hh, char*) -> int {
         DTFE_CUDA_TRY(cudaMemcpyAsync(hh->tet_v, tet_v, 16 * n_tets, cudaMemcpyHostToDevice, hh->stream));
-        DTFE_CUDA_TRY(cudaMemcpyAsync(hh->tet_n, tet_n, 16 * n_tets, cudaMemcpyHostToDevice, hh->stream));
+        if (tet_n)
+          DTFE_CUDA_TRY(cudaMemcpyAsync(hh->tet_n, tet_n, 16 * n_tets, cudaMemcpyHostToDevice, hh->stream));
         return DTFE_OK;
       },
       [&](dtfe_handle hh, char*) -> int {
@@ -1941,7 +2063,8 @@ int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n, i
         // them: the check waits for its count (the packed path's decoder
         // sanitises instead and reports at the next status read)
         unsigned long long bad = 0;
-        k_check_tets<<<blocks_for(n_tets, 256), 256, 0, hh->stream>>>(n_tets, n_verts, hh->tet_v, hh->tet_n,
+        k_check_tets<<<blocks_for(n_tets, 256), 256, 0, hh->stream>>>(n_tets, n_verts, hh->tet_v,
+                                                                       tet_n ? hh->tet_n : nullptr,
                                                                        hh->counters + CNT_DECODE);
         DTFE_CUDA_TRY(cudaGetLastError());
         DTFE_CUDA_TRY(cudaMemcpyAsync(&bad, hh->counters + CNT_DECODE, sizeof(bad), cudaMemcpyDeviceToHost,
@@ -1953,7 +2076,47 @@ int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n, i
                                          " or a neighbour id outside [-1, n_tets)");
         }
         return DTFE_OK;
-      });
+      },
+      tet_n == nullptr);
+}
+
+// The vertex-only packed form ("DTP3", dtfe_tets_pack_vertices): header
+// magic, T, n_blocks, n_escapes, then the byte offsets of block bases, escape
+// prefix, block byte offsets, width flags, orientation bits and data; the
+// escapes follow the data's 16-byte aligned end.  The neighbours are derived
+// on the device from the vertices.
+static int upload_packed_vertices(dtfe_handle h, const int64_t hd[10], const void* packed, int64_t packed_bytes,
+                                  const float* xyz, const float* w, const float* vel, const float* scal,
+                                  int64_t n_verts) {
+  const int64_t T = hd[1], nb = hd[2], n_esc = hd[3];
+  bool ok = T >= 0 && nb == (T + kPackBlock - 1) / kPackBlock && n_esc >= 0 && hd[4] >= 80 &&
+            hd[5] >= hd[4] + 4 * nb && hd[6] >= hd[5] + 4 * (nb + 1) && hd[7] >= hd[6] + 8 * (nb + 1) &&
+            hd[8] >= hd[7] + (T + 1) / 2 && hd[9] >= hd[8] + (T + 7) / 8 && hd[9] <= packed_bytes;
+  for (int k = 4; k < 10; ++k) ok = ok && hd[k] % 16 == 0;
+  int64_t data_end = 0;
+  if (ok) {
+    int64_t last = 0;  // byte size of the data: the last block offset
+    std::memcpy(&last, (const char*)packed + hd[6] + 8 * nb, sizeof(last));
+    ok = last >= 0 && last <= packed_bytes;
+    data_end = hd[9] + ((last + 16 + 15) & ~(int64_t)15);
+    ok = ok && data_end + 4 * n_esc <= packed_bytes;
+  }
+  if (!ok) return set_error(DTFE_ERR_ARG, "not a packed tessellation (dtfe_tets_pack_vertices)");
+  return upload_impl(
+      h, T, xyz, w, vel, scal, n_verts, (size_t)packed_bytes,
+      [&](dtfe_handle hh, char* dev) -> int {
+        DTFE_CUDA_TRY(cudaMemcpyAsync(dev, packed, (size_t)packed_bytes, cudaMemcpyHostToDevice, hh->stream));
+        return DTFE_OK;
+      },
+      [&](dtfe_handle hh, char* dev) -> int {
+        k_unpack_tet_vertices<<<(unsigned)nb, kPackBlock, 0, hh->stream>>>(
+            T, n_verts, (const int32_t*)(dev + hd[4]), (const int32_t*)(dev + hd[5]), (const int64_t*)(dev + hd[6]),
+            (const uint8_t*)(dev + hd[7]), (const uint8_t*)(dev + hd[8]), (const uint32_t*)(dev + hd[9]),
+            data_end - hd[9], (const int32_t*)(dev + data_end), n_esc, hh->tet_v, hh->counters + CNT_DECODE);
+        DTFE_CUDA_TRY(cudaGetLastError());
+        return DTFE_OK;
+      },
+      true);
 }
 
 int dtfe_gpu_upload_packed(dtfe_handle h, const void* packed, int64_t packed_bytes, const float* xyz,
@@ -1963,6 +2126,7 @@ int dtfe_gpu_upload_packed(dtfe_handle h, const void* packed, int64_t packed_byt
   int64_t hd[10];
   if (!packed || packed_bytes < (int64_t)sizeof(hd)) return set_error(DTFE_ERR_ARG, "null or short packed buffer");
   std::memcpy(hd, packed, sizeof(hd));
+  if (hd[0] == 0x33505444) return upload_packed_vertices(h, hd, packed, packed_bytes, xyz, w, vel, scal, n_verts);
   const int64_t T = hd[1], nb = hd[2], n_esc = hd[3];
   bool ok = hd[0] == 0x32505444 && T >= 0 && nb == (T + kPackBlock - 1) / kPackBlock && n_esc >= 0 &&
             hd[4] >= (int64_t)sizeof(hd) && hd[5] >= hd[4] + 4 * nb && hd[6] >= hd[5] + 4 * (nb + 1) &&
@@ -3068,6 +3232,18 @@ int dtfe_gpu_locate_points(dtfe_handle h, int64_t np, const double* pts, int32_t
   DTFE_CUDA_TRY(cudaFreeAsync(dp, st));
   DTFE_CUDA_TRY(cudaFreeAsync(dout, st));
   DTFE_CUDA_TRY(cudaStreamSynchronize(st));
+  return DTFE_OK;
+}
+
+int dtfe_gpu_download_tets(dtfe_handle h, int32_t* tet_v, int32_t* tet_n) {
+  if (!h) return set_error(DTFE_ERR_ARG, "null handle");
+  if (h->T > 0 && (!tet_v && !tet_n)) return set_error(DTFE_ERR_ARG, "null argument");
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  if (tet_v && h->T)
+    DTFE_CUDA_TRY(cudaMemcpyAsync(tet_v, h->tet_v, 16 * h->T, cudaMemcpyDeviceToHost, h->stream));
+  if (tet_n && h->T)
+    DTFE_CUDA_TRY(cudaMemcpyAsync(tet_n, h->tet_n, 16 * h->T, cudaMemcpyDeviceToHost, h->stream));
+  DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return DTFE_OK;
 }
 

@@ -496,3 +496,192 @@ int dtfe_tets_unpack(const void* packed, int64_t bytes, int32_t* tet_v, int32_t*
 }
 
 }  // extern "C"
+
+// ---- vertex-only packed tessellation (dtfe_tets_pack_vertices) ------------
+// The neighbour array follows from the vertex array (two tetrahedra are
+// neighbours across the face whose three vertices both hold), so it need
+// not cross PCIe at all: the device derives it (dtfe_gpu_upload_packed).
+// The vertices are coded as differences: the first vertex against the
+// previous tetrahedron's first vertex (signed), the second against the first,
+// the smaller of the last two against the second and the larger against the
+// smaller (all positive: the first vertex is the smallest and the second the
+// smallest of the rest in the canonical order), with one bit saying whether
+// the third vertex is the larger.  Every field takes 1 or 2 bytes, a 4-bit
+// width flag per tetrahedron says which, and values that fit neither are
+// escaped to a 32-bit list (as the difference itself).  About 5 bytes per
+// tetrahedron instead of 32.
+// Layout:
+//   header       10 x int64: magic "DTP3", T, n_blocks, n_escapes, and the byte
+//                offsets of block_base, block_esc, block_off, flags, orient, data
+//                (the escapes follow the data at its 16-byte aligned end)
+//   block_base   int32 per block: the first vertex of the block's first
+//                tetrahedron (its own first field is 0)
+//   block_esc    int32 per block + 1: escapes before the block
+//   block_off    int64 per block + 1: byte offset of the block in data
+//   flags        4 bits per tetrahedron (even t: low nibble): bit f set = field f takes 2 bytes
+//   orient       1 bit per tetrahedron (bit t % 8 of byte t / 8): the third vertex is the larger
+//   data         the fields, tetrahedron after tetrahedron, little endian:
+//                field 0 signed (maximum: escaped), fields 1-3 unsigned (all ones: escaped)
+//   escapes      int32 values of the escaped fields, in (tetrahedron, field) order
+namespace {
+constexpr int64_t kPack3Magic = 0x33505444;  // "DTP3"
+
+struct Tet3Code {
+  uint8_t flag;
+  bool orient;
+  int nbytes, nesc;
+  uint16_t val[4];
+  int32_t esc[4];
+};
+
+inline bool encode_tet3(const int32_t* v, int32_t prev0, Tet3Code& c) {
+  c.flag = 0;
+  c.nbytes = 0;
+  c.nesc = 0;
+  const int32_t lo = std::min(v[2], v[3]), hi = std::max(v[2], v[3]);
+  c.orient = v[2] > v[3];
+  if (!(v[1] > v[0] && lo > v[1] && hi > lo)) return false;  // not in canonical order
+  const int64_t d0 = (int64_t)v[0] - prev0;
+  if (d0 >= -127 && d0 <= 126) { c.val[0] = (uint16_t)(uint8_t)(int8_t)d0; c.nbytes += 1; }
+  else if (d0 >= -32767 && d0 <= 32766) { c.val[0] = (uint16_t)(int16_t)d0; c.flag |= 1; c.nbytes += 2; }
+  else { c.val[0] = 127; c.nbytes += 1; c.esc[c.nesc++] = (int32_t)d0; }
+  const int64_t d[3] = {(int64_t)v[1] - v[0], (int64_t)lo - v[1], (int64_t)hi - lo};
+  for (int f = 1; f < 4; ++f) {
+    const int64_t o = d[f - 1];
+    if (o < 0xFF) { c.val[f] = (uint16_t)o; c.nbytes += 1; }
+    else if (o < 0xFFFF) { c.val[f] = (uint16_t)o; c.flag |= (uint8_t)(1u << f); c.nbytes += 2; }
+    else { c.val[f] = 0xFF; c.nbytes += 1; c.esc[c.nesc++] = (int32_t)o; }
+  }
+  return true;
+}
+}  // namespace
+
+extern "C" {
+
+// Packs T tetrahedra given by their vertices alone (tet_v: 4 int32 each, in
+// the canonical order of the planner's tessellations: the smallest vertex
+// first, the second the smallest of the rest).  out == NULL: returns the size
+// in bytes; otherwise writes it and returns the same size.  Negative on bad
+// arguments or a tetrahedron not in canonical order.
+int64_t dtfe_tets_pack_vertices(const int32_t* tet_v, int64_t T, void* out) {
+  if (T < 0 || (T > 0 && !tet_v)) return -1;
+  const int64_t nb = (T + kPackBlock - 1) / kPackBlock;
+  std::vector<int32_t> base(nb), cnt(nb + 1, 0);
+  std::vector<int64_t> boff(nb + 1, 0);
+  int bad = 0;
+#pragma omp parallel for schedule(static) reduction(+ : bad)
+  for (int64_t b = 0; b < nb; ++b) {
+    const int64_t t0 = b * kPackBlock, t1 = std::min(T, t0 + kPackBlock);
+    base[b] = tet_v[4 * t0];
+    int ne = 0;
+    int64_t bytes = 0;
+    Tet3Code c;
+    for (int64_t t = t0; t < t1; ++t) {
+      if (!encode_tet3(tet_v + 4 * t, t == t0 ? base[b] : tet_v[4 * (t - 1)], c)) ++bad;
+      ne += c.nesc;
+      bytes += c.nbytes;
+    }
+    cnt[b + 1] = ne;
+    boff[b + 1] = bytes;
+  }
+  if (bad) return -2;
+  for (int64_t b = 0; b < nb; ++b) {
+    cnt[b + 1] += cnt[b];
+    boff[b + 1] += boff[b];
+  }
+  PackHeader hd;
+  hd.magic = kPack3Magic;
+  hd.T = T;
+  hd.n_blocks = nb;
+  hd.n_esc = cnt[nb];
+  hd.off_base = (int64_t)align16(sizeof(PackHeader));
+  hd.off_esc = hd.off_base + (int64_t)align16(sizeof(int32_t) * nb);
+  hd.off_boff = hd.off_esc + (int64_t)align16(sizeof(int32_t) * (nb + 1));
+  hd.off_flags = hd.off_boff + (int64_t)align16(sizeof(int64_t) * (nb + 1));
+  // off_data holds the orientation bits' offset; the data follows them
+  hd.off_data = hd.off_flags + (int64_t)align16((size_t)(T + 1) / 2);
+  hd.off_escapes = hd.off_data + (int64_t)align16((size_t)(T + 7) / 8);
+  const int64_t data_end = hd.off_escapes + (int64_t)align16((size_t)boff[nb] + 16);
+  const int64_t total = data_end + (int64_t)align16(sizeof(int32_t) * hd.n_esc);
+  if (!out) return total;
+  char* o = (char*)out;
+  std::memset(o, 0, (size_t)total);
+  std::memcpy(o, &hd, sizeof(hd));
+  std::memcpy(o + hd.off_base, base.data(), sizeof(int32_t) * nb);
+  std::memcpy(o + hd.off_esc, cnt.data(), sizeof(int32_t) * (nb + 1));
+  std::memcpy(o + hd.off_boff, boff.data(), sizeof(int64_t) * (nb + 1));
+  uint8_t* flags = (uint8_t*)(o + hd.off_flags);
+  uint8_t* orient = (uint8_t*)(o + hd.off_data);
+  uint8_t* data = (uint8_t*)(o + hd.off_escapes);
+  int32_t* esc = (int32_t*)(o + data_end);
+  // blocks of 256 tetrahedra start on whole flag and orientation bytes
+#pragma omp parallel for schedule(static)
+  for (int64_t b = 0; b < nb; ++b) {
+    const int64_t t0 = b * kPackBlock, t1 = std::min(T, t0 + kPackBlock);
+    uint8_t* d = data + boff[b];
+    int32_t* e = esc + cnt[b];
+    Tet3Code c;
+    for (int64_t t = t0; t < t1; ++t) {
+      encode_tet3(tet_v + 4 * t, t == t0 ? base[b] : tet_v[4 * (t - 1)], c);
+      flags[t >> 1] |= (uint8_t)(c.flag << ((t & 1) * 4));
+      if (c.orient) orient[t >> 3] |= (uint8_t)(1u << (t & 7));
+      for (int f = 0; f < 4; ++f) {
+        *d++ = (uint8_t)(c.val[f] & 0xFF);
+        if (c.flag >> f & 1) *d++ = (uint8_t)(c.val[f] >> 8);
+      }
+      for (int q = 0; q < c.nesc; ++q) *e++ = c.esc[q];
+    }
+  }
+  return total;
+}
+
+// Host decoder of dtfe_tets_pack_vertices' format: restores tet_v.  Returns
+// 0, or 1 for a malformed buffer.
+int dtfe_tets_unpack_vertices(const void* packed, int64_t bytes, int32_t* tet_v) {
+  if (!packed || bytes < (int64_t)sizeof(PackHeader)) return 1;
+  PackHeader hd;
+  std::memcpy(&hd, packed, sizeof(hd));
+  if (hd.magic != kPack3Magic || hd.T < 0 || hd.n_blocks != (hd.T + kPackBlock - 1) / kPackBlock) return 1;
+  const char* p = (const char*)packed;
+  const int64_t* boff = (const int64_t*)(p + hd.off_boff);
+  const int64_t data_end = hd.off_escapes + (int64_t)align16((size_t)boff[hd.n_blocks] + 16);
+  if (data_end + 4 * hd.n_esc > bytes) return 1;
+  const int32_t* base = (const int32_t*)(p + hd.off_base);
+  const int32_t* cnt = (const int32_t*)(p + hd.off_esc);
+  const uint8_t* flags = (const uint8_t*)(p + hd.off_flags);
+  const uint8_t* orient = (const uint8_t*)(p + hd.off_data);
+  const uint8_t* data = (const uint8_t*)(p + hd.off_escapes);
+  const int32_t* esc = (const int32_t*)(p + data_end);
+  for (int64_t b = 0; b < hd.n_blocks; ++b) {
+    const uint8_t* d = data + boff[b];
+    const int32_t* e = esc + cnt[b];
+    int32_t prev = base[b];
+    for (int64_t t = b * kPackBlock; t < std::min(hd.T, (b + 1) * kPackBlock); ++t) {
+      const int flag = (flags[t >> 1] >> ((t & 1) * 4)) & 15;
+      uint32_t raw[4];
+      for (int f = 0; f < 4; ++f) {
+        raw[f] = *d++;
+        if (flag >> f & 1) raw[f] |= (uint32_t)(*d++) << 8;
+      }
+      const bool w0 = flag & 1;
+      const int32_t s0 = w0 ? (int32_t)(int16_t)raw[0] : (int32_t)(int8_t)raw[0];
+      const int32_t d0 = s0 == (w0 ? 32767 : 127) ? *e++ : s0;
+      int32_t dd[3];
+      for (int f = 1; f < 4; ++f) {
+        const bool wide = flag >> f & 1;
+        dd[f - 1] = raw[f] == (wide ? 0xFFFFu : 0xFFu) ? *e++ : (int32_t)raw[f];
+      }
+      int32_t* v = tet_v + 4 * t;
+      v[0] = prev + d0;
+      v[1] = v[0] + dd[0];
+      const int32_t lo = v[1] + dd[1], hi = lo + dd[2];
+      const bool third_larger = orient[t >> 3] >> (t & 7) & 1;
+      v[2] = third_larger ? hi : lo;
+      v[3] = third_larger ? lo : hi;
+      prev = v[0];
+    }
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -51,9 +51,11 @@ class DeviceDTFE:
     def synchronize(self) -> None:
         N.check(self.lib.dtfe_gpu_synchronize(self.h))
 
-    def upload(self, plan) -> None:
+    def upload(self, plan, neighbours: bool = True) -> None:
+        """Plain upload; neighbours=False sends tet_v alone and the device
+        derives the neighbours."""
         N.check(self.lib.dtfe_gpu_upload(
-            self.h, N.ptr(plan.tet_v), N.ptr(plan.tet_n), plan.n_tets, N.ptr(plan.xyz),
+            self.h, N.ptr(plan.tet_v), N.ptr(plan.tet_n) if neighbours else None, plan.n_tets, N.ptr(plan.xyz),
             N.ptr(plan.weight), N.ptr(plan.velocity), N.ptr(plan.scalar), plan.n_verts))
 
     def upload_packed(self, plan, packed: np.ndarray) -> None:
@@ -362,6 +364,13 @@ class DeviceDTFE:
         out = np.empty(int(np.prod(self.grid)), np.int32)
         N.check(self.lib.dtfe_gpu_download_located(self.h, out.ctypes.data))
         return out
+
+    def download_tets(self, n_tets: int):
+        """The device's (tet_v, tet_n) arrays, (T, 4) int32 each."""
+        tv = np.empty((n_tets, 4), np.int32)
+        tn = np.empty((n_tets, 4), np.int32)
+        N.check(self.lib.dtfe_gpu_download_tets(self.h, tv.ctypes.data, tn.ctypes.data))
+        return tv, tn
 
     def set_max_walk_steps(self, n: int) -> None:
         """Step limit of the point-location walks (0 = default)."""

@@ -518,6 +518,28 @@ def pack_tets(tet_v: np.ndarray, tet_n: np.ndarray, out: np.ndarray | None = Non
     return buf
 
 
+def pack_tet_vertices(tet_v: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
+    """The vertex-only packed form of a tessellation
+    (dtfe_tets_pack_vertices, about 5 bytes per tetrahedron): the device
+    derives the neighbours.  ``out`` (e.g. pinned memory) is used when it is
+    large enough."""
+    tv = np.ascontiguousarray(tet_v, np.int32)
+    lib = N.host()
+    n = int(lib.dtfe_tets_pack_vertices(tv.ctypes.data, len(tv), None))
+    if n < 0:
+        raise ValueError("cannot pack these arrays (tetrahedra not in canonical vertex order)")
+    buf = out[:n] if out is not None and out.nbytes >= n else np.empty(n, np.uint8)
+    lib.dtfe_tets_pack_vertices(tv.ctypes.data, len(tv), buf.ctypes.data)
+    return buf
+
+
+def unpack_tet_vertices(packed: np.ndarray, n_tets: int) -> np.ndarray:
+    tv = np.empty((n_tets, 4), np.int32)
+    if N.host().dtfe_tets_unpack_vertices(packed.ctypes.data, packed.nbytes, tv.ctypes.data):
+        raise ValueError("malformed packed tessellation")
+    return tv
+
+
 def unpack_tets(packed: np.ndarray, n_tets: int):
     tv = np.empty((n_tets, 4), np.int32)
     tn = np.empty((n_tets, 4), np.int32)

@@ -145,7 +145,10 @@ const char* dtfe_last_error(void);
 
 /* Upload a (multi-)tessellation and its vertex data (host arrays).
  * xyz: 3V floats (vertex positions, Particle_data::pos), w: V weights,
- * vel: 3V velocities or NULL, scal: V*S scalars or NULL.
+ * vel: 3V velocities or NULL, scal: V*S scalars or NULL.  tet_n may be NULL:
+ * the device then derives the neighbours from tet_v (the other tetrahedron
+ * holding a face's three vertices, -1 on the hull), so only half the arrays
+ * cross PCIe.
  * Every tet_v entry must lie in [0, n_verts) and every tet_n entry in
  * [-1, n_tets): a device kernel checks them before anything indexes with
  * them and the call returns DTFE_ERR_ARG (the handle then holds nothing)
@@ -155,9 +158,14 @@ const char* dtfe_last_error(void);
 int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n,
                     int64_t n_tets, const float* xyz, const float* w,
                     const float* vel, const float* scal, int64_t n_verts);
-/* Same, with the tetrahedra in the packed form of dtfe_tets_pack
- * (include/dtfe_host.h): about 16 bytes per tetrahedron instead of 32 cross
- * to the device, where a kernel restores tet_v/tet_n.  No counterpart in the
+/* Same, with the tetrahedra in a packed form (include/dtfe_host.h):
+ * dtfe_tets_pack (about 11.5 bytes per tetrahedron instead of 32; a kernel
+ * restores tet_v and tet_n) or dtfe_tets_pack_vertices (about 5 bytes; a
+ * kernel restores tet_v and the neighbours are derived on the device from
+ * the vertices: across each face the other tetrahedron holding its three
+ * vertices, -1 on the hull).  A malformed buffer is refused when its header
+ * is wrong, else reported by the next status read (DTFE_ERR_ARG) with every
+ * bad tetrahedron stored as vertex 0 four times.  No counterpart in the
  * reference (its tessellation never leaves the host). */
 int dtfe_gpu_upload_packed(dtfe_handle h, const void* packed, int64_t packed_bytes, const float* xyz,
                            const float* w, const float* vel, const float* scal, int64_t n_verts);
@@ -403,6 +411,10 @@ int dtfe_gpu_locate_points(dtfe_handle h, int64_t np, const double* pts, int32_t
  * centre outside the hull (the reference's infinite cell) and for cells
  * outside every tile.  DTFE_ERR_STATE before a cell-centre interpolation. */
 int dtfe_gpu_download_located(dtfe_handle h, int32_t* loc);
+/* Copies the device's tessellation arrays (4 T int32 each, either may be
+ * NULL) to the host: after a packed or neighbour-less upload, the restored
+ * tet_v and the derived tet_n. */
+int dtfe_gpu_download_tets(dtfe_handle h, int32_t* tet_v, int32_t* tet_n);
 /* Step limit of every point-location walk (dtfe_config::max_walk_steps;
  * 0 = the default 65536).  A walk that reaches it counts as a failure: its
  * sample gets zeros and the call reports DTFE_ERR_WALK with

@@ -55,6 +55,18 @@ void dtfe_tess_release(void* handle);
  * the arrays (0 on success, 1 for a malformed buffer). */
 int64_t dtfe_tets_pack(const int32_t* tet_v, const int32_t* tet_n, int64_t T, void* out);
 int dtfe_tets_unpack(const void* packed, int64_t bytes, int32_t* tet_v, int32_t* tet_n);
+/* Vertex-only packed form (format "DTP3"), about 5 bytes per tetrahedron:
+ * the neighbours are not sent, the device derives them.  Per tetrahedron
+ * four 1- or 2-byte differences (first vertex against the previous
+ * tetrahedron's, second against the first, the smaller of the last two
+ * against the second, the larger against the smaller), a 4-bit width flag
+ * and a bit saying whether the third vertex is the larger; escapes to 32
+ * bits.  The tetrahedra must be in the planner's canonical vertex order
+ * (the first vertex the smallest, the second the smallest of the rest;
+ * returns -2 otherwise).  Sizes and return values as dtfe_tets_pack;
+ * dtfe_tets_unpack_vertices restores tet_v. */
+int64_t dtfe_tets_pack_vertices(const int32_t* tet_v, int64_t T, void* out);
+int dtfe_tets_unpack_vertices(const void* packed, int64_t bytes, int32_t* tet_v);
 
 /* ---- whole-run planning --------------------------------------------------- */
 enum {

@@ -189,16 +189,54 @@ def _box_args(plan, box):
     return xyz, w, vel, tv, tn, dims, region
 
 
-def time_boxes(plan, threads: int, which: int = 0, n_points: int = 1):
+MAIN_LIB = os.path.join(_HERE, "_ref", "libdtfe_refmain.so")
+_main = None
+
+
+def main_lib() -> C.CDLL:
+    """The reference's own src/DTFE.cpp in the harness (libdtfe_refmain.so)."""
+    global _main
+    if _main is None:
+        L = C.CDLL(MAIN_LIB)
+        vp = C.c_void_p
+        L.ref_derived_timed.argtypes = [C.c_int64, vp, vp, vp, vp, C.POINTER(C.c_double)]
+        L.ref_derived_timed.restype = C.c_int
+        _main = L
+    return _main
+
+
+def derived(grad: np.ndarray):
+    """The reference's computeDivergenceShearVorticity (src/DTFE.cpp:436-475)
+    on a gradient grid (G, 9): (divergence, shear, vorticity, seconds of the
+    call alone)."""
+    g = np.ascontiguousarray(grad, np.float32).reshape(-1, 9)
+    G = len(g)
+    div = np.empty(G, np.float32)
+    sh = np.empty((G, 5), np.float32)
+    vo = np.empty((G, 3), np.float32)
+    sec = C.c_double(0.0)
+    if main_lib().ref_derived_timed(G, g.ctypes.data, div.ctypes.data, sh.ctypes.data, vo.ctypes.data,
+                                    C.byref(sec)):
+        raise RuntimeError("ref_derived_timed failed")
+    return div, sh, vo, sec.value
+
+
+def time_boxes(plan, threads: int, which: int = 0, n_points: int = 1, with_derived: bool = False):
     """Times the reference's own per-thread work of DTFE_parallel
     (src/DTFE.cpp:331-356): vertexDensity + the interpolation ``which``
     (0 interpolateGrid, 1/2/3 the averaging methods with ``n_points``) of
     density, velocity and velocity gradient on every sub-box, the sub-boxes
     spread over ``threads`` host threads as the reference's OpenMP team would.
-    Returns (seconds of the slowest thread, per-box seconds); only the
-    reference's calls are timed, not loading the tessellation."""
+    with_derived adds, after the threads, DTFE()'s one serial
+    computeDivergenceShearVorticity on the main grid's gradient
+    (src/DTFE.cpp:248-249, the reference's own code from
+    libdtfe_refmain.so).  Returns (seconds: the slowest thread plus the
+    derived pass, per-box seconds); only the reference's calls are timed, not
+    loading the tessellation."""
     from concurrent.futures import ThreadPoolExecutor
     L = lib()
+    G1, G2 = plan.grid[1], plan.grid[2]
+    main_grad = np.zeros((int(np.prod(plan.grid)), 9), np.float32) if with_derived else None
 
     def one(box):
         xyz, w, vel, tv, tn, dims, region = _box_args(plan, box)
@@ -214,6 +252,13 @@ def time_boxes(plan, threads: int, which: int = 0, n_points: int = 1):
                                      None, None, None, 7, C.byref(sec))
         if rc:
             raise RuntimeError(f"ref_interpolate_timed failed ({rc})")
+        if main_grad is not None:
+            # copySubgridResultsToMain (src/subpartition.h:399-432), untimed
+            b = plan.boxes[box]
+            o = [b.tile_origin[a] for a in range(3)]
+            d = [int(x) for x in dims]
+            view = main_grad.reshape(plan.grid[0], G1, G2, 9)
+            view[o[0]:o[0] + d[0], o[1]:o[1] + d[1], o[2]:o[2] + d[2]] = grad.reshape(d[0], d[1], d[2], 9)
         return sec.value
     K = plan.n_boxes
     with ThreadPoolExecutor(max_workers=max(1, min(threads, K))) as ex:
@@ -223,7 +268,8 @@ def time_boxes(plan, threads: int, which: int = 0, n_points: int = 1):
     loads = [0.0] * max(1, min(threads, K))
     for k, t in enumerate(per_box):
         loads[k % len(loads)] += t
-    return max(loads), per_box
+    t_derived = derived(main_grad)[3] if main_grad is not None else 0.0
+    return max(loads) + t_derived, per_box
 
 
 def write_binary(path: str, data, ncomp: int) -> None:

@@ -170,3 +170,60 @@ def test_dropin_averages_at_samples_and_cones(particles):
         assert len(a[f]) == len(ref[f]) == len(u["density"]) < len(samples)
         assert np.array_equal(a[f].reshape(ref[f].shape), ref[f]), f
         assert np.array_equal(ac[f].reshape(refc[f].shape), refc[f]), f
+
+
+PLANNING = {
+    "region_fractions": dict(region=(0.2, 0.7, 0.1, 0.6, 0.3, 0.9)),
+    "region_absolute": dict(region=(10.0, 60.0, 20.0, 75.0, 5.0, 55.0), region_mpc=True),
+    "partition_all": dict(partition=(2, 1, 2)),
+    "partition_one": dict(partition=(2, 2, 1), part_no=3),
+    "padding_relative": dict(padding=(0.05, 0.06, 0.07, 0.05, 0.04, 0.08), padding_mode=1),
+    "padding_absolute": dict(padding=(6.0, 5.0, 7.0, 6.0, 5.0, 8.0), padding_mode=2),
+    "region_partition_one": dict(region=(0.1, 0.8, 0.2, 0.9, 0.0, 0.7), partition=(2, 2, 2), part_no=5),
+}
+
+
+@pytest.mark.parametrize("case", list(PLANNING))
+def test_dropin_planning_options(particles, case):
+    """--region, --partition (every chunk in one batched step, or one
+    --partNo chunk on its own grid) and given padding lengths through
+    DTFE(): the device API on the planner's plan for the same options, bit for
+    bit, and the reference's own DTFE() (its src/DTFE.cpp in the harness) on
+    the same call: the same grid and region, fields within 2e-6 (RMS floor)
+    — its vertex densities are float sums of float volumes, the GPU's exact
+    sums of FP64 volumes, a few 1e-7 apart on this input."""
+    from conftest import rel_err
+    from dtfe_b200.device import DeviceDTFE
+    if not D.available("reference"):
+        pytest.skip("the reference's DTFE() is not built")
+    pos, w, vel, _ = particles
+    opts = PLANNING[case]
+    avg = float(w.sum()) / 1e6
+    fields = ["density", "velocity", "velocity_gradient", "velocity_divergence"]
+    kw = dict(average_density=avg, u_fields=fields, a_fields=["density"], method=3, n_points=8, n_threads=4, **opts)
+    u, a, reg = D.run_ex("DTFE", pos, w, vel, None, GRID, which="dropin", **kw)
+    ur, ar, regr = D.run_ex("DTFE", pos, w, vel, None, GRID, which="reference", **kw)
+    assert np.array_equal(reg, regr)
+    pk = {}
+    if "region" in opts:
+        r = np.asarray(opts["region"], np.float32)
+        pk["region"] = r if opts.get("region_mpc") else np.float32(100.0) * r
+    if "partition" in opts:
+        pk["partition"] = opts["partition"]
+        pk["part_no"] = opts.get("part_no", -1)
+    if "padding" in opts:
+        pk["padding"] = opts["padding"]
+        pk["padding_absolute"] = opts.get("padding_mode", 1) == 2
+    plan = P.native_plan("DTFE", pos, w, vel, None, grid=GRID, n_threads=4, average_density_value=avg, **pk)
+    assert np.array_equal(plan.covered_region, reg)
+    with DeviceDTFE(0) as dev:
+        dev.load(plan)
+        dev.vertex_density(plan.rho_bar)
+        ref_u = dev.interpolate(fields, method=0)
+        ref_a = dev.interpolate(["density"], method=3, n_samples=8)
+    assert len(u["density"]) == len(ur["density"]) == int(np.prod(plan.grid))
+    for f in fields:
+        assert np.array_equal(u[f].reshape(ref_u[f].shape), ref_u[f]), f
+        assert rel_err(u[f], ur[f]) <= 2e-6, (f, rel_err(u[f], ur[f]))
+    assert np.array_equal(a["density"].reshape(ref_a["density"].shape), ref_a["density"])
+    assert rel_err(a["density"], ar["density"]) <= 2e-6

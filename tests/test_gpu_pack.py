@@ -101,3 +101,82 @@ def test_packed_malformed_is_reported(gpu_built):
         dev.upload_packed(plan, packed)
         dev.vertex_density(plan.rho_bar)
         dev.interpolate(["density"], method=0)
+
+
+def _plans():
+    """A periodic multi-sub-box plan and a sparse non-periodic one (many hull
+    faces, sub-boxes with few or no tetrahedra)."""
+    pos, psi = S.zeldovich_lattice(18, 100.0, 1.0, seed=15)
+    vel = (40 * psi).astype(np.float32)
+    a = P.make_plan(pos, np.ones(len(pos), np.float32), vel, None, grid=(18, 16, 20), n_threads=8)
+    rng = np.random.default_rng(16)
+    p2 = (rng.random((300, 3)) * 100).astype(np.float32)
+    b = P.make_plan(p2, rng.uniform(0.5, 1.5, 300).astype(np.float32), rng.standard_normal((300, 3)).astype(
+        np.float32), None, grid=(12, 12, 12), n_threads=6, periodic=False, padding=np.full(6, 4.0, np.float32),
+        average_density_value=3e-4)
+    return [a, b]
+
+
+@pytest.mark.parametrize("which", [0, 1])
+@pytest.mark.parametrize("form", ["plain_without_neighbours", "packed_vertices"])
+def test_neighbours_derived_on_device(gpu_built, which, form):
+    """Only the vertices cross (tet_n = NULL, or the vertex-only packed form
+    of dtfe_tets_pack_vertices): the device's tet_v and its derived tet_n
+    equal the host arrays exactly (-1 on the hull), and the fields equal
+    those of the full upload bit for bit."""
+    from dtfe_b200.device import DeviceDTFE
+    plan = _plans()[which]
+    with DeviceDTFE(0) as ref_dev:
+        ref_dev.load(plan)
+        ref_dev.vertex_density(plan.rho_bar)
+        ref = ref_dev.interpolate(FIELDS, method=0)
+        ref_d = ref_dev.download_vertex_density(plan.n_verts)
+    with DeviceDTFE(0) as dev:
+        if form == "plain_without_neighbours":
+            dev.upload(plan, neighbours=False)
+        else:
+            dev.upload_packed(plan, P.pack_tet_vertices(plan.tet_v))
+        tv, tn = dev.download_tets(plan.n_tets)
+        assert np.array_equal(tv, plan.tet_v)
+        assert np.array_equal(tn, plan.tet_n)
+        dev.set_subboxes(plan)
+        dev.vertex_density(plan.rho_bar)
+        got = dev.interpolate(FIELDS, method=0)
+        assert np.array_equal(dev.download_vertex_density(plan.n_verts), ref_d)
+    for f in FIELDS:
+        assert np.array_equal(got[f], ref[f]), f
+
+
+def test_packed_vertices_malformed_is_reported(gpu_built):
+    """A vertex-only packed buffer with a wrong header is refused at upload;
+    one whose block sizes no longer add up, or whose vertices leave the
+    canonical order, is counted by the decoder's checks and reported by the
+    next status read; a good upload clears it."""
+    from dtfe_b200 import _native as N
+    from dtfe_b200.device import DeviceDTFE
+    pos, _ = S.zeldovich_lattice(12, 100.0, 1.0, seed=17)
+    plan = P.make_plan(pos, np.ones(len(pos), np.float32), None, None, grid=(12, 12, 12), n_threads=2)
+    packed = P.pack_tet_vertices(plan.tet_v)
+    hd = packed[:80].view(np.int64)
+    assert hd[0] == 0x33505444
+    with DeviceDTFE(0) as dev:
+        bad = packed.copy()
+        bad[:80].view(np.int64)[9] = packed.nbytes + 16     # data beyond the buffer
+        with pytest.raises(N.DTFEError):
+            dev.upload_packed(plan, bad)
+        for corrupt in ("flag", "data"):
+            bad = packed.copy()
+            if corrupt == "flag":
+                bad[int(hd[7]) + 1] ^= 0x01      # a width nibble of block 0: its bytes no longer add up
+            else:
+                data = int(hd[9])
+                bad[data + 1] = 0                # tetrahedron 0's second-vertex offset: 0, not above the first
+            dev.upload_packed(plan, bad)
+            dev.set_subboxes(plan)
+            dev.vertex_density(plan.rho_bar)
+            with pytest.raises(N.DTFEError, match="did not decode"):
+                dev.interpolate(["density"], method=0)
+        dev.upload_packed(plan, packed)
+        dev.set_subboxes(plan)
+        dev.vertex_density(plan.rho_bar)
+        dev.interpolate(["density"], method=0)

@@ -47,3 +47,39 @@ def test_pack_layout_header(built):
     sizes = 8 + np.unpackbits(flags[:, None], axis=1).sum(1)
     per_block = np.add.reduceat(sizes, np.arange(0, T, 256))
     assert np.array_equal(np.diff(boff), per_block)
+
+
+def test_pack_vertices_roundtrip(built):
+    """The vertex-only form (dtfe_tets_pack_vertices): tet_v restored bit for
+    bit, well under a fifth of the 32 bytes per tetrahedron of the plain
+    arrays."""
+    pos, _ = S.zeldovich_lattice(16, 100.0, 1.0, seed=2)
+    plan = P.make_plan(pos, np.ones(len(pos), np.float32), None, None, grid=(16, 16, 16), n_threads=4)
+    packed = P.pack_tet_vertices(plan.tet_v)
+    assert packed.nbytes < 0.2 * (plan.tet_v.nbytes + plan.tet_n.nbytes)
+    assert np.array_equal(P.unpack_tet_vertices(packed, plan.n_tets), plan.tet_v)
+
+
+def test_pack_vertices_escapes_and_order(built):
+    """Far jumps between consecutive tetrahedra and large offsets escape to
+    32 bits; tetrahedra not in the canonical vertex order are refused."""
+    rng = np.random.default_rng(1)
+    T = 3000
+    tv = np.empty((T, 4), np.int64)
+    tv[:, 0] = rng.integers(0, 1_000_000_000, T)
+    tv[:, 1] = tv[:, 0] + rng.integers(1, 100_000, T)
+    lo = tv[:, 1] + rng.integers(1, 300, T)
+    hi = lo + rng.integers(1, 70_000, T)
+    swap = rng.random(T) < 0.5
+    tv[:, 2] = np.where(swap, hi, lo)
+    tv[:, 3] = np.where(swap, lo, hi)
+    tv = tv.astype(np.int32)
+    packed = P.pack_tet_vertices(tv)
+    assert np.array_equal(P.unpack_tet_vertices(packed, T), tv)
+    e = P.pack_tet_vertices(np.zeros((0, 4), np.int32))
+    assert P.unpack_tet_vertices(e, 0).shape == (0, 4)
+    bad = tv.copy()
+    bad[7] = bad[7, ::-1]
+    import pytest
+    with pytest.raises(ValueError):
+        P.pack_tet_vertices(bad)

@@ -240,3 +240,23 @@ def test_live_averaged_samples_statistical(built):
             ratio = np.median(np.abs(d_ref)) / np.median(np.abs(d_self))
             assert 0.8 < ratio < 1.25, (f, ratio)
             assert abs(d_ref.mean()) < 4 * d_ref.std() / np.sqrt(d_ref.size), f
+
+
+@pytest.mark.skipif(not __import__("os").path.exists(R.MAIN_LIB), reason="reference DTFE.cpp harness not built")
+def test_live_divergence_shear_vorticity(built):
+    """Divergence, shear and vorticity of the oracle in the reference's
+    arithmetic (the GPU's fused epilogue is bit-identical to it) against the
+    reference's own computeDivergenceShearVorticity (src/DTFE.cpp:436-475,
+    compiled in the harness) applied to the same float gradient: bit for
+    bit."""
+    pos, psi = S.zeldovich_lattice(12, 100.0, 0.9, seed=31)
+    vel = (80 * psi + np.random.default_rng(32).normal(0, 20, psi.shape)).astype(np.float32)
+    plan = P.make_plan(pos, np.ones(len(pos), np.float32), vel, None, grid=(14, 12, 10), n_threads=3,
+                       average_density_value=len(pos) / 1e6)
+    d32, d64, _ = O.vertex_density(plan)
+    fields = ["velocity_gradient", "velocity_divergence", "velocity_shear", "velocity_vorticity"]
+    ora, _ = O.interpolate(plan, d32, d64, fields, mode=O.MODE_REF)
+    div, sh, vo, _ = R.derived(ora["velocity_gradient"].astype(np.float32))
+    assert np.array_equal(div, ora["velocity_divergence"].astype(np.float32))
+    assert np.array_equal(sh, ora["velocity_shear"].astype(np.float32))
+    assert np.array_equal(vo, ora["velocity_vorticity"].astype(np.float32))

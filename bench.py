@@ -77,6 +77,9 @@ def parse():
                     help="extra N(0,1) scalar fields per particle, interpolated with their gradients")
     ap.add_argument("--fp64-cells", type=int, default=50000,
                     help="cells checked against the FP64 oracle in the CPU-baseline leg (0 = none)")
+    ap.add_argument("--split", action="store_true",
+                    help="split one box over the ranks (the reference's sub-boxes dealt to ranks, tiles "
+                         "gathered to rank 0 every step: strong scaling) instead of one box per rank")
     ap.add_argument("--cpu-kind", default="auto", choices=["auto", "port"],
                     help="CPU baseline: the reference's code when built (auto) or the oracle port")
     return ap.parse_args()
@@ -829,6 +832,103 @@ def run_reference(args):
     return 0
 
 
+def run_split(args):
+    """One n^3 box split over the ranks: the reference's decomposition into
+    ranks x parts sub-boxes (DTFE_parallel's split, src/DTFE.cpp:287-385),
+    the sub-boxes dealt to ranks by particle count (dtfe_b200/shard.py), each
+    rank tessellating and interpolating only its own; every step ends with
+    the tiles gathered to rank 0 through device memory (packed by a kernel,
+    NCCL gather, unpacked by a kernel: copySubgridResultsToMain,
+    src/subpartition.h:399-432).  Total work is fixed: strong scaling."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from dtfe_b200 import _native as NF
+    from dtfe_b200 import shard as SH
+    from dtfe_b200 import synthetic as S
+    from dtfe_b200.device import DeviceDTFE
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    n = args.n
+    threads = max(1, host_threads(args.threads) // world)
+    parts = max(1, 16 // world)
+    t0 = time.time()
+    pos, psi = S.zeldovich_lattice(n, S.BOX, 1.0, seed=1)
+    vel = (100.0 * psi / (S.BOX / n) + np.random.default_rng(2).normal(0.0, 50.0, psi.shape)).astype(np.float32)
+    del psi
+    w = np.ones(len(pos), np.float32)
+    plan, mine = SH.make_rank_plan(pos, w, vel, None, grid=(n, n, n), world=world, rank=rank, parts_per_rank=parts,
+                                   average_density_value=float(len(pos)) / S.BOX ** 3)
+    t_plan = time.time() - t0
+    del pos, vel
+    G = n ** 3
+    fields = FIELDS
+    ncomp = {f: NF.field_components(NF.FIELD_SLOTS[f], 0) for f in fields}
+    dev = DeviceDTFE(local, 0)
+    dev.load(plan)
+    outs = {f: torch.zeros((G, ncomp[f]), dtype=torch.float32, device=f"cuda:{local}") for f in fields}
+    stream = torch.cuda.ExternalStream(dev.stream, device=f"cuda:{local}")
+    tables = SH._exchange_tables(plan, None, f"cuda:{local}") if world > 1 else None
+
+    def step():
+        dev.vertex_density(plan.rho_bar)
+        dev.interpolate_dev_async(fields, outs, method=0)
+        if world > 1:
+            dev.synchronize()
+            SH.gather_fields_dev(dev, plan, outs, root=0, tables=tables)
+
+    for _ in range(args.warmup):
+        step()
+    dev.synchronize()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    st = dev.read_status()
+    t_total = ev0.elapsed_time(ev1) / 1e3
+    if world > 1:
+        t = torch.tensor([t_total], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_total = float(t.item())
+    line = {
+        "metric": METRIC, "value": G * args.steps / t_total, "unit": "grid samples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"zeldovich{n} split over {world} ranks: {n}^3 Zel'dovich particles (rms 1.0 spacing, "
+                               f"periodic 100 Mpc/h, padding 5) -> {n}^3 grid, cell-centre "
+                               "density+velocity+gradient+div/shear/vort, vertex densities included, tiles gathered "
+                               "to rank 0 every step",
+                   "subboxes": world * parts, "subboxes_this_rank": len(mine), "vertices_this_rank": plan.n_verts,
+                   "l2": "inputs larger than L2 (tessellation arrays > 126 MB)",
+                   "parallelism": f"split{world} (sub-boxes dealt to ranks, NCCL tile gather)"},
+        "gpu_launches": None, "clocks": clk, "e2e": None, "roofline": None, "cpu_baseline": None,
+        "walk": {k: st[k] for k in ("n_samples_located", "n_walk_steps", "n_outside")},
+        "host_prep_s": {"plan_s": t_plan},
+    }
+    dev.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -1157,6 +1257,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.split:
+        return run_split(args)
     return run_ours(args)
 
 

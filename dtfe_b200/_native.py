@@ -198,6 +198,8 @@ def gpu() -> C.CDLL:
         lib.dtfe_gpu_locate_points.argtypes = [H, C.c_int64, vp, C.c_int32, vp]
         lib.dtfe_gpu_download_located.argtypes = [H, vp]
         lib.dtfe_gpu_download_tets.argtypes = [H, vp, vp]
+        lib.dtfe_gpu_tiles_gather_dev.argtypes = [H, C.c_int32, vp, vp, C.c_int32, vp, vp]
+        lib.dtfe_gpu_tiles_scatter_dev.argtypes = [H, C.c_int32, vp, vp, C.c_int32, vp, vp]
         lib.dtfe_gpu_set_max_walk_steps.argtypes = [H, C.c_int32]
         lib.dtfe_gpu_stream.argtypes = [H]
         lib.dtfe_gpu_stream.restype = C.c_void_p

@@ -20,8 +20,9 @@
 // and each tetrahedron passes Vbar_t = sum_{v in t} dL/dS_v on to its
 // vertices through dV_t/dx_j.
 //
-// Per-cell terms are evaluated in FP64 and scattered with FP64 atomics; the
-// volume term is gathered per vertex over the incidence lists (no atomics).
+// Per-cell terms are evaluated in FP64 and scattered with FP64 atomics; S_v
+// is the forward pass's exact volume sum (fixed_volume.cuh) and the volume
+// term is gathered per vertex over the incidence lists (no atomics).
 // Tetrahedra whose edge matrix the forward pass treats as singular
 // (|det| / sum|M| <= 1e-6, triangulation_miscellaneous.cc:86-94) have zero
 // gradient fields, so only the rho_0 term remains.
@@ -31,6 +32,7 @@
 #include <cstdint>
 
 #include "../../include/dtfe_gpu.h"
+#include "fixed_volume.cuh"
 #include "tile_index.cuh"
 #include "predicates.h"
 
@@ -219,13 +221,18 @@ __global__ void k_adjoint_cells(AdjCellParams P) {
 // dL/dm_v and dL/dS_v from dL/drho_v (hull vertices have a constant density).
 __global__ void k_adjoint_vertices(int64_t V, const float4* __restrict__ posd, const float* __restrict__ w,
                                    const int* __restrict__ hull, const double* __restrict__ g_rho,
-                                   const double* __restrict__ vol, const int64_t* __restrict__ off,
-                                   const int* __restrict__ inc, float factor, double* __restrict__ g_S,
-                                   double* __restrict__ g_m) {
+                                   const long long* __restrict__ vacc, const dtfe::VolScale* __restrict__ vscale,
+                                   const int64_t* __restrict__ vprefix, int nsb, float factor,
+                                   double* __restrict__ g_S, double* __restrict__ g_m) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= V) return;
-  double S = 0.0;
-  for (int64_t q = off[i], e = off[i + 1]; q < e; ++q) S += vol[inc[q]];
+  int b = 0;  // the vertex's sub-box: its unit
+  for (int lo = 0, hi = nsb; hi - lo > 1;) {
+    const int mid = (lo + hi) >> 1;
+    if (vprefix[mid] <= i) lo = b = mid;
+    else hi = mid;
+  }
+  const double S = (double)vacc[i] * vscale[b].unit;
   if (hull[i] || S == 0.0) {
     g_S[i] = 0.0;
     g_m[i] = 0.0;
@@ -300,9 +307,10 @@ __global__ void k_adjoint_gather(int64_t V, const int4* __restrict__ tet_v, cons
 // Launch sequence used by dtfe_gpu_adjoint (dtfe_core.cu owns the buffers).
 extern "C" int dtfe_internal_adjoint(void* stream, const void* cell_params, int64_t n_cells, int64_t V, int64_t T,
                                      const int4* tet_v, const float4* posd, const float* w, const int* hull,
-                                     const double* vol, const int64_t* off, const int* inc, float factor,
-                                     double* g_rho, double* g_x, double* g_v, double* g_S, double* g_m,
-                                     double* vbar, float* out_x, float* out_v, float* out_w) {
+                                     const long long* vacc, const dtfe::VolScale* vscale, const int64_t* vprefix,
+                                     int nsb, const int64_t* off, const int* inc, float factor, double* g_rho,
+                                     double* g_x, double* g_v, double* g_S, double* g_m, double* vbar, float* out_x,
+                                     float* out_v, float* out_w) {
   cudaStream_t st = (cudaStream_t)stream;
   cudaMemsetAsync(g_rho, 0, sizeof(double) * V, st);
   cudaMemsetAsync(g_x, 0, sizeof(double) * 3 * V, st);
@@ -313,8 +321,8 @@ extern "C" int dtfe_internal_adjoint(void* stream, const void* cell_params, int6
   P.g_v = g_v;
   if (n_cells > 0) k_adjoint_cells<<<(unsigned)((n_cells + 255) / 256), 256, 0, st>>>(P);
   if (V > 0)
-    k_adjoint_vertices<<<(unsigned)((V + 255) / 256), 256, 0, st>>>(V, posd, w, hull, g_rho, vol, off, inc, factor,
-                                                                    g_S, g_m);
+    k_adjoint_vertices<<<(unsigned)((V + 255) / 256), 256, 0, st>>>(V, posd, w, hull, g_rho, vacc, vscale, vprefix,
+                                                                    nsb, factor, g_S, g_m);
   if (T > 0) k_adjoint_vbar<<<(unsigned)((T + 255) / 256), 256, 0, st>>>(T, tet_v, g_S, vbar);
   if (V > 0)
     k_adjoint_gather<<<(unsigned)((V + 255) / 256), 256, 0, st>>>(V, tet_v, posd, vbar, off, inc, g_x, g_v, g_m,

@@ -2,29 +2,32 @@
 // include/dtfe_gpu.h.
 //
 // Pipeline (all on the handle's stream):
-//   upload              tessellation (plain or packed) and vertex data;
+//   upload              tessellation (plain, packed, or its vertices alone)
+//                       and vertex data; k_unpack_tets / k_unpack_tet_vertices
+//                       decode packed forms; without neighbours the device
+//                       derives them (incidence lists, k_neighbours_star);
 //                       k_hull_marks flags the vertices of hull faces (the
-//                       reference's infinite cells); incidence lists per
-//                       vertex (k_degree, scan, k_fill_incidence, sorted by
-//                       k_sort_incidence_staged)
+//                       reference's infinite cells)
 //   k_tet_volume_bins   per step, one thread per tetrahedron: signed FP64
-//                       volume, and per grid cell the walk seed: the
-//                       tetrahedron whose centroid is nearest the cell's
+//                       volume added into its vertices' exact sums
+//                       (fixed_volume.cuh), and per grid cell the walk seed:
+//                       the tetrahedron whose centroid is nearest the cell's
 //                       sample point among those whose centroid lies in it
 //   k_vertex_density    rho_v = w (D+1)/(rho_bar sum V), 0 on the hull
-//                       (vertexDensity, triangulation.cpp:200-279), summed
-//                       over the incidence list in ascending tetrahedron order
-//   k_locate_cells      one thread per cell: walk from the seed to the cell
-//                       centre (canonical tetrahedron, bit-exact location)
-//   k_eval_centre       the reference's per-sample arithmetic and the
+//                       (vertexDensity, triangulation.cpp:200-279)
+//   k_locate_eval       one thread per cell: walk from the seed to the cell
+//                       centre (canonical tetrahedron, bit-exact location),
+//                       then the reference's per-sample arithmetic and the
 //                       divergence/shear/vorticity epilogue, every requested
-//                       field written once
+//                       field written once (k_locate_cells + k_eval_centre:
+//                       the same in two kernels)
 //   k_average           methods 2/3: n points per cell, each walked from the
 //                       centre's tetrahedron (averaged_interpolation_2.cc:123,145)
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <map>
@@ -34,6 +37,7 @@
 
 #include "../../include/dtfe_gpu.h"
 #include "dtfe_device.cuh"
+#include "fixed_volume.cuh"
 #include "philox.h"
 #include "tile_index.cuh"
 
@@ -87,6 +91,16 @@ __global__ void k_check_tets(int64_t T, int64_t V, const int4* __restrict__ tet_
   }
   const unsigned nbad = __popc(__ballot_sync(0xffffffffu, !ok));
   if ((threadIdx.x & 31) == 0 && nbad) atomicAdd(bad, (unsigned long long)nbad);
+}
+
+// Interleaved tetrahedron records for the record walk: rec[2t] = vertices,
+// rec[2t+1] = neighbours.
+__global__ void k_build_records(int64_t T, const int4* __restrict__ tet_v, const int4* __restrict__ tet_n,
+                                int4* __restrict__ rec) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= T) return;
+  rec[2 * t] = __ldg(&tet_v[t]);
+  rec[2 * t + 1] = __ldg(&tet_n[t]);
 }
 
 __global__ void k_hull_marks(int64_t T, const int4* __restrict__ tet_v, const int4* __restrict__ tet_n,
@@ -291,47 +305,124 @@ __global__ void __launch_bounds__(kPackBlock)
   tet_v[t] = make_int4((int)v0, (int)v1, (int)(third_larger ? hi : lo), (int)(third_larger ? lo : hi));
 }
 
-// Neighbour array from the vertex array and the incidence lists (ascending):
-// the tetrahedra around edge (v0, v1) of t are the common entries of the
-// lists of v0 and v1; among them (t aside) the one holding v2 lies across
-// the face opposite v3 and the one holding v3 across the face opposite v2.
-// Edge (v2, v3) gives the faces opposite v0 and v1 the same way.  A face no
-// other tetrahedron holds is on the convex hull (-1, CGAL's infinite cell).
 __device__ __forceinline__ bool holds(const int4& u, int v) { return u.x == v || u.y == v || u.z == v || u.w == v; }
 
-__device__ __forceinline__ void edge_faces(int t, int a, int b, int c, int d, const int64_t* __restrict__ off,
-                                           const int* __restrict__ inc, const int4* __restrict__ tet_v, int& nc,
-                                           int& nd) {
-  // nc: the tetrahedron holding (a, b, c), nd: the one holding (a, b, d)
-  int64_t i = __ldg(&off[a]), ie = __ldg(&off[a + 1]);
-  int64_t j = __ldg(&off[b]), je = __ldg(&off[b + 1]);
-  while (i < ie && j < je) {
-    const int x = __ldg(&inc[i]), y = __ldg(&inc[j]);
-    if (x < y) {
-      ++i;
-    } else if (y < x) {
-      ++j;
-    } else {
-      if (x != t) {
-        const int4 u = __ldg(&tet_v[x]);
-        if (holds(u, c)) nc = x;
-        else if (holds(u, d)) nd = x;
-      }
-      ++i;
-      ++j;
-    }
+// Fallback for the faces k_neighbours_star left unset (kUnsetNeighbour):
+// across face (a, b, c) of t lies the other tetrahedron of a's incidence
+// list that holds b and c (-1 if none: the convex hull, CGAL's infinite
+// cell).  Any list order will do.
+constexpr int kUnsetNeighbour = (int)0x80808080;  // the byte pattern 0x80 of a memset
+__device__ __forceinline__ int face_neighbour(int t, int a, int b, int c, const int64_t* __restrict__ off,
+                                              const int* __restrict__ inc, const int4* __restrict__ tet_v) {
+  for (int64_t i = __ldg(&off[a]), e = __ldg(&off[a + 1]); i < e; ++i) {
+    const int u = __ldg(&inc[i]);
+    if (u == t) continue;
+    const int4 q = __ldg(&tet_v[u]);
+    if (holds(q, b) && holds(q, c)) return u;
   }
+  return -1;
 }
 
 __global__ void k_derive_neighbours(int64_t T, const int4* __restrict__ tet_v, const int64_t* __restrict__ off,
                                     const int* __restrict__ inc, int4* __restrict__ tet_n) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= T) return;
+  int4 cur = tet_n[t];
+  if (cur.x != kUnsetNeighbour && cur.y != kUnsetNeighbour && cur.z != kUnsetNeighbour &&
+      cur.w != kUnsetNeighbour)
+    return;
   const int4 q = __ldg(&tet_v[t]);
-  int n0 = -1, n1 = -1, n2 = -1, n3 = -1;
-  edge_faces((int)t, q.x, q.y, q.z, q.w, off, inc, tet_v, n3, n2);  // faces (v0 v1 v2), (v0 v1 v3)
-  edge_faces((int)t, q.z, q.w, q.y, q.x, off, inc, tet_v, n0, n1);  // faces (v2 v3 v1), (v2 v3 v0)
-  tet_n[t] = make_int4(n0, n1, n2, n3);
+  if (cur.x == kUnsetNeighbour) cur.x = face_neighbour((int)t, q.y, q.z, q.w, off, inc, tet_v);
+  if (cur.y == kUnsetNeighbour) cur.y = face_neighbour((int)t, q.x, q.z, q.w, off, inc, tet_v);
+  if (cur.z == kUnsetNeighbour) cur.z = face_neighbour((int)t, q.x, q.y, q.w, off, inc, tet_v);
+  if (cur.w == kUnsetNeighbour) cur.w = face_neighbour((int)t, q.x, q.y, q.z, off, inc, tet_v);
+  tet_n[t] = cur;
+}
+
+// Neighbours from the stars of the vertices: every face is settled at its
+// smallest vertex v, by the one warp that reads v's incidence list.  Each
+// tetrahedron around v contributes its faces through v whose other two
+// vertices are larger than v, keyed by those two vertices; the two entries
+// with the same key are the tetrahedra on either side (one entry alone: a
+// hull face, -1).  The entries of one vertex sit in the warp's shared table;
+// a vertex with more than kStarCap entries leaves its faces unset for
+// k_derive_neighbours.  Each incidence list is read once and each
+// tetrahedron's vertices four times, instead of two list merges per
+// tetrahedron.
+constexpr int kStarWarps = 8;
+constexpr int kStarCap = 256;
+__global__ void __launch_bounds__(32 * kStarWarps) k_neighbours_star(int64_t V, const int4* __restrict__ tet_v,
+                                                                    const int64_t* __restrict__ off,
+                                                                    const int* __restrict__ inc,
+                                                                    int* __restrict__ tet_n) {
+  __shared__ unsigned long long s_key[kStarWarps][kStarCap];
+  __shared__ int s_tet[kStarWarps][kStarCap];
+  __shared__ unsigned char s_face[kStarWarps][kStarCap];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned long long* key = s_key[w];
+  int* tet = s_tet[w];
+  unsigned char* face = s_face[w];
+  for (int64_t v = (int64_t)blockIdx.x * kStarWarps + w; v < V; v += (int64_t)gridDim.x * kStarWarps) {
+    const int64_t a = __ldg(&off[v]), e = __ldg(&off[v + 1]);
+    int n = 0;  // entries so far (warp-uniform)
+    for (int64_t base = a; base < e; base += 32) {
+      const int64_t q = base + lane;
+      int cnt = 0, u = -1;
+      unsigned long long k3[3];
+      int f3[3];
+      if (q < e) {
+        u = __ldg(&inc[q]);
+        const int4 tv = __ldg(&tet_v[u]);
+        const int vv[4] = {tv.x, tv.y, tv.z, tv.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          if (vv[k] == (int)v) continue;  // the face opposite v does not hold v
+          int x = -1, y = -1;
+#pragma unroll
+          for (int m = 0; m < 4; ++m)
+            if (m != k && vv[m] != (int)v) {
+              if (x < 0) x = vv[m];
+              else y = vv[m];
+            }
+          if (x > (int)v && y > (int)v) {
+            const unsigned lo = (unsigned)min(x, y), hi = (unsigned)max(x, y);
+            k3[cnt] = ((unsigned long long)lo << 32) | hi;
+            f3[cnt] = k;
+            ++cnt;
+          }
+        }
+      }
+      int incl = cnt;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += y;
+      }
+      const int pos = n + incl - cnt;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        if (c < cnt && pos + c < kStarCap) {
+          key[pos + c] = k3[c];
+          tet[pos + c] = u;
+          face[pos + c] = (unsigned char)f3[c];
+        }
+      n += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    __syncwarp();
+    if (n <= kStarCap) {
+      for (int j = lane; j < n; j += 32) {
+        const unsigned long long kj = key[j];
+        int partner = -1;
+        for (int i = 0; i < n; ++i)
+          if (i != j && key[i] == kj) {
+            partner = tet[i];
+            break;
+          }
+        tet_n[4 * (int64_t)tet[j] + face[j]] = partner;
+      }
+    }
+    __syncwarp();
+  }
 }
 
 __global__ void k_degree(int64_t T, const int4* __restrict__ tet_v, int* __restrict__ deg) {
@@ -406,58 +497,6 @@ __global__ void k_fill_incidence(int64_t T, const int4* __restrict__ tet_v, cons
   }
 }
 
-// Ascending order inside every vertex's list: the FP64 volume sum then runs
-// in a fixed order (ascending tetrahedron id), independent of the atomics
-// that filled the lists.  A warp loads the incidence lists of its 32
-// vertices (contiguous) into shared memory with coalesced loads, every lane
-// insertion-sorts its own list there, and the warp writes them back; warps
-// whose lists exceed the staging area sort in global memory, lane by lane.
-constexpr int kSortBlock = 256;
-constexpr int kSortChunk = 1536;  // incidences staged per warp (6 KB)
-__global__ void __launch_bounds__(kSortBlock) k_sort_incidence_staged(int64_t V, const int64_t* __restrict__ off,
-                                                                      int* __restrict__ inc) {
-  __shared__ int s_inc[kSortBlock / 32][kSortChunk];
-  const int lane = threadIdx.x & 31;
-  int* sv = s_inc[threadIdx.x >> 5];
-  const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int64_t v0 = v - lane;
-  if (v0 >= V) return;
-  const int64_t vl = (v0 + 32 <= V) ? v0 + 32 : V;
-  const int64_t beg = off[v0], end = off[vl];
-  const bool mine = v < V;
-  if (end - beg > kSortChunk) {
-    if (!mine) return;
-    const int64_t a = off[v], b = off[v + 1];
-    for (int64_t i = a + 1; i < b; ++i) {
-      const int x = inc[i];
-      int64_t j = i - 1;
-      while (j >= a && inc[j] > x) {
-        inc[j + 1] = inc[j];
-        --j;
-      }
-      inc[j + 1] = x;
-    }
-    return;
-  }
-  const int n = (int)(end - beg);
-  for (int q = lane; q < n; q += 32) sv[q] = inc[beg + q];
-  __syncwarp();
-  if (mine) {
-    const int a = (int)(off[v] - beg), b = (int)(off[v + 1] - beg);
-    for (int i = a + 1; i < b; ++i) {
-      const int x = sv[i];
-      int j = i - 1;
-      while (j >= a && sv[j] > x) {
-        sv[j + 1] = sv[j];
-        --j;
-      }
-      sv[j + 1] = x;
-    }
-  }
-  __syncwarp();
-  for (int q = lane; q < n; q += 32) inc[beg + q] = sv[q];
-}
-
 // ---- per step ------------------------------------------------------------
 constexpr int kVolBlock = 64;  // 64: 5.67 ms per 256^3 step; 128: 5.70; 256: 5.77; 512: 6.21
 
@@ -471,10 +510,26 @@ constexpr int kVolBlock = 64;  // 64: 5.67 ms per 256^3 step; 128: 5.70; 256: 5.
 // atomic per run.  The seed only starts the walk (the located tetrahedron
 // does not depend on it), so the centroid's cell uses a fast approximate
 // division (the range checks keep the index in the tile).
+// Per-vertex volume sums in exact integer units (fixed_volume.cuh): the
+// scale of each tetrahedron's sub-box (tprefix: nsb + 1 tetrahedron range
+// starts), one reduction per vertex.
+struct VolSums {
+  long long* acc;
+  const VolScale* scale;
+  const int64_t* tprefix;
+  int nsb;
+};
+__device__ __forceinline__ void add_volume(const VolSums& S, int64_t t, const int v[4], double vol) {
+  const int b = S.nsb > 1 ? find_box(S.tprefix, S.nsb, t) : 0;
+  const unsigned long long q = (unsigned long long)__double2ll_rn(vol * S.scale[b].inv_q);
+#pragma unroll
+  for (int a = 0; a < 4; ++a) atomicAdd((unsigned long long*)&S.acc[v[a]], q);
+}
+
 constexpr unsigned long long kEmptySeed = ~0ull;
 template <bool DO_BINS>
 __global__ void __launch_bounds__(kVolBlock) k_tet_volume_bins(
-    int64_t T, const int4* __restrict__ tet_v, const float4* __restrict__ posd, double* __restrict__ vol,
+    int64_t T, const int4* __restrict__ tet_v, const float4* __restrict__ posd, VolSums VS,
     const dtfe_subbox* __restrict__ boxes, const int64_t* __restrict__ tprefix,
     const int64_t* __restrict__ bin_offset, int K, const float* __restrict__ xs, const float* __restrict__ ys,
     const float* __restrict__ zs, unsigned long long* __restrict__ bins) {
@@ -492,7 +547,7 @@ __global__ void __launch_bounds__(kVolBlock) k_tet_volume_bins(
     for (int a = 0; a < 4; ++a)
 #pragma unroll
       for (int c = 0; c < 3; ++c) D[a][c] = (double)X[a][c];
-    vol[t] = orient_det(D[0], D[1], D[2], D[3]) / 6.0;
+    add_volume(VS, t, v, orient_det(D[0], D[1], D[2], D[3]) / 6.0);
     if (DO_BINS) {
       const int b = find_box(tprefix, K, t);
       const dtfe_subbox& B = boxes[b];
@@ -549,7 +604,7 @@ struct RasterAxis {
 };
 template <int MINB>
 __global__ void __launch_bounds__(kRasterBlock, MINB) k_tet_volume_raster(
-    int64_t T, const int4* __restrict__ tet_v, const float4* __restrict__ posd, double* __restrict__ vol,
+    int64_t T, const int4* __restrict__ tet_v, const float4* __restrict__ posd, VolSums VS,
     const dtfe_subbox* __restrict__ boxes, const int64_t* __restrict__ tprefix,
     const int64_t* __restrict__ tile_prefix, const RasterAxis* __restrict__ axes, int K,
     const float* __restrict__ xs, const float* __restrict__ ys, const float* __restrict__ zs,
@@ -572,7 +627,7 @@ __global__ void __launch_bounds__(kRasterBlock, MINB) k_tet_volume_raster(
     for (int a = 0; a < 4; ++a)
 #pragma unroll
       for (int c = 0; c < 3; ++c) D[a][c] = (double)X[a][c];
-    vol[t] = orient_det(D[0], D[1], D[2], D[3]) / 6.0;
+    add_volume(VS, t, v, orient_det(D[0], D[1], D[2], D[3]) / 6.0);
     if (t >= __ldg(&tprefix[0]) && t < __ldg(&tprefix[K])) {
       const int b = find_box(tprefix, K, t);
       int r0[3], nr[3];
@@ -655,39 +710,66 @@ __global__ void __launch_bounds__(kRasterBlock, MINB) k_tet_volume_raster(
   if (lane == 0 && rt) atomicAdd(&counters[1], (unsigned long long)rt);
 }
 
-// rho_v = (w * factor) / sum of incident volumes, summed in ascending
-// tetrahedron order; 0 on the hull or without incident tetrahedra.  A warp
-// handles 32 consecutive vertices, whose incidence lists are contiguous: it
-// stages the lists' volumes in shared memory with coalesced loads (in chunks),
-// then every lane sums its own list sequentially.
-constexpr int kDensBlock = 64;  // 64: 5.59 ms per 256^3 step (volumes at 64); 128: 5.63; 256: 5.67
-constexpr int kDensChunk = 512;  // incidences staged per warp and pass
+// rho_v = (w * factor) / (its exact volume sum * its sub-box's unit), 0 on
+// the hull or without incident tetrahedra (vertexDensity,
+// triangulation.cpp:200-279).  vprefix: nsb + 1 vertex range starts.
+constexpr int kDensBlock = 256;
 __global__ void __launch_bounds__(kDensBlock) k_vertex_density(
-    int64_t V, const float* __restrict__ w, const double* __restrict__ vol, const int64_t* __restrict__ off,
-    const int* __restrict__ inc, const int* __restrict__ hull, float factor, float4* __restrict__ posd) {
-  __shared__ double s_vol[kDensBlock / 32][kDensChunk];
-  const int lane = threadIdx.x & 31;
-  double* sv = s_vol[threadIdx.x >> 5];
+    int64_t V, const float* __restrict__ w, const long long* __restrict__ acc, const int* __restrict__ hull,
+    const VolScale* __restrict__ scale, const int64_t* __restrict__ vprefix, int nsb, float factor,
+    float4* __restrict__ posd) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int64_t v0 = i - lane;
-  if (v0 >= V) return;
-  const int64_t vl = (v0 + 32 <= V) ? v0 + 32 : V;  // warp's vertex range [v0, vl)
-  const int64_t beg = __ldg(&off[v0]), end = __ldg(&off[vl]);
-  const bool mine = i < V;
-  const int64_t a = mine ? __ldg(&off[i]) : end, e = mine ? __ldg(&off[i + 1]) : end;
-  double sum = 0.0;
-  int64_t cur = a;  // next incidence of this lane to add
-  for (int64_t base = beg; base < end; base += kDensChunk) {
-    const int64_t lim = (end - base < kDensChunk) ? end : base + kDensChunk;
-    __syncwarp();
-    for (int64_t q = base + lane; q < lim; q += 32) sv[q - base] = __ldg(&vol[__ldg(&inc[q])]);
-    __syncwarp();
-    for (; cur < e && cur < lim; ++cur) sum += sv[cur - base];
+  if (i >= V) return;
+  const int b = nsb > 1 ? find_box(vprefix, nsb, i) : 0;
+  posd[i].w = density_from_fixed(__ldg(&acc[i]), __ldg(&scale[b].unit), __ldg(&w[i]), factor, __ldg(&hull[i]) != 0);
+}
+
+// Bounding box of every sub-box's vertices (float order keys): a warp whose
+// 32 vertices share a sub-box reduces before its atomics.
+__global__ void __launch_bounds__(256) k_box_bbox(int64_t V, const float4* __restrict__ posd,
+                                                  const int64_t* __restrict__ vprefix, int nsb,
+                                                  int* __restrict__ bbox) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const bool valid = i < V;
+  const int b = valid ? (nsb > 1 ? find_box(vprefix, nsb, i) : 0) : -1;
+  int k[3] = {INT_MAX, INT_MAX, INT_MAX};
+  if (valid) {
+    const float4 r = __ldg(&posd[i]);
+    k[0] = float_order_key(r.x);
+    k[1] = float_order_key(r.y);
+    k[2] = float_order_key(r.z);
   }
-  if (mine) {
-    float d = (hull[i] || sum == 0.0) ? 0.f : (float)((double)(w[i] * factor) / sum);
-    posd[i].w = d;
+  const int b0 = __shfl_sync(0xffffffffu, b, 0);
+  if (__all_sync(0xffffffffu, b == b0)) {
+    if (b0 < 0) return;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int lo = __reduce_min_sync(0xffffffffu, k[c]);
+      const int hi = __reduce_max_sync(0xffffffffu, valid ? k[c] : INT_MIN);
+      if ((threadIdx.x & 31) == 0) {
+        atomicMin(&bbox[6 * b0 + 2 * c], lo);
+        atomicMax(&bbox[6 * b0 + 2 * c + 1], hi);
+      }
+    }
+  } else if (valid) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      atomicMin(&bbox[6 * b + 2 * c], k[c]);
+      atomicMax(&bbox[6 * b + 2 * c + 1], k[c]);
+    }
   }
+}
+
+__global__ void k_box_bbox_init(int nsb, int* __restrict__ bbox) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < 6 * nsb) bbox[i] = (i & 1) ? INT_MIN : INT_MAX;
+}
+
+__global__ void k_box_scales(int nsb, const int* __restrict__ bbox, const int64_t* __restrict__ vprefix,
+                             VolScale* __restrict__ scale) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nsb) return;
+  scale[b] = vprefix[b + 1] > vprefix[b] ? vol_scale(bbox_volume(bbox + 6 * b)) : VolScale{0.0, 0.0};
 }
 
 // Offsets of the 26 neighbouring cells, nearest first (faces, edges, corners).
@@ -701,6 +783,7 @@ __constant__ signed char c_nbr[26][3] = {
 struct InterpParams {
   const int4* tet_v;
   const int4* tet_n;
+  const int4* tet_rec = nullptr;  // interleaved records (vertices, neighbours) per tetrahedron
   const float4* posd;
   const float4* vel4;
   const float* scal;
@@ -931,7 +1014,7 @@ __global__ void __launch_bounds__(kInterpBlock, MINB) k_eval_centre(InterpParams
 // the tetrahedron the walk ends in, whose vertices and positions are still
 // in registers; the warp is converged again after the walk, so the
 // evaluation and the staged stores run as in k_eval_centre.
-template <int S, int MINB>
+template <int S, int MINB, bool REC = false>
 __global__ void __launch_bounds__(kInterpBlock, MINB) k_locate_eval(InterpParams P, int* __restrict__ tet_c) {
   constexpr int CMAX = (3 * S > 9) ? 3 * S : 9;
   __shared__ __align__(16) float s_stage[kInterpBlock / 32][32 * CMAX];
@@ -971,9 +1054,12 @@ __global__ void __launch_bounds__(kInterpBlock, MINB) k_locate_eval(InterpParams
       // in registers: the evaluation uses them directly
       const double pc[3] = {(double)c.x, (double)c.y, (double)c.z};
       int v[4];
-      float X[4][3];
+      float X[4][3], D[4];
       const int t0 = seed_of(P, c);
-      int t = t0 < 0 ? kOutside : walk_locate<true>(P.tet_v, P.tet_n, P.posd, pc, t0, P.max_steps, v, X, wst);
+      int t = t0 < 0 ? kOutside
+                     : (REC ? walk_locate_rec<true>(P.tet_rec, P.tet_v, P.tet_n, P.posd, pc, t0, P.max_steps, v, X,
+                                                    D, wst)
+                            : walk_locate<true>(P.tet_v, P.tet_n, P.posd, pc, t0, P.max_steps, v, X, wst));
       ++n_loc;
       if (t == kWalkFail) {
         ++n_fail;
@@ -981,7 +1067,8 @@ __global__ void __launch_bounds__(kInterpBlock, MINB) k_locate_eval(InterpParams
       }
       n_out += t < 0;
       tet_c[s] = t;
-      if (t >= 0) cell_eval<S>(v, X, pc, P.posd, P.vel4, P.scal, want_dens, want_vel, want_sc, fix, e);
+      if (t >= 0)
+        cell_eval<S>(v, X, pc, P.posd, P.vel4, P.scal, want_dens, want_vel, want_sc, fix, e, REC ? D : nullptr);
     }
     const int64_t c0 = __shfl_sync(0xffffffffu, cell, 0);
     const bool contig = __all_sync(0xffffffffu, valid && cell == c0 + lane) && (c0 % 4 == 0);
@@ -1602,6 +1689,39 @@ __global__ void k_locate_points(int64_t np, const double* __restrict__ pts, cons
 
 }  // namespace
 
+// Tiles of a main grid <-> their values packed tile after tile (x, y, z
+// order inside a tile), the layout the tile exchange between ranks sends
+// (copySubgridResultsToMain, src/subpartition.h:399-432).  One thread per
+// packed float: its tile by binary search over the tiles' packed offsets;
+// consecutive threads walk z, so both sides are read and written in runs.
+struct TileRec {
+  int32_t o[3], d[3];
+};
+__global__ void k_tiles_copy(int n_tiles, const TileRec* __restrict__ tiles, const int64_t* __restrict__ start,
+                             int64_t G1, int64_t G2, int ncomp, int to_packed, const float* __restrict__ src,
+                             float* __restrict__ dst) {
+  const int64_t total = __ldg(&start[n_tiles]) * ncomp;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = e / ncomp;
+    const int c = (int)(e - s * ncomp);
+    int lo = 0, hi = n_tiles;  // start[lo] <= s < start[hi]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(&start[mid]) <= s) lo = mid;
+      else hi = mid;
+    }
+    const TileRec T = tiles[lo];
+    const int64_t local = s - __ldg(&start[lo]);
+    const int64_t plane = (int64_t)T.d[1] * T.d[2];
+    const int64_t i = local / plane, r = local - i * plane;
+    const int64_t j = r / T.d[2], k = r - j * T.d[2];
+    const int64_t cell = ((T.o[0] + i) * G1 + (T.o[1] + j)) * G2 + (T.o[2] + k);
+    if (to_packed) dst[e] = src[cell * ncomp + c];
+    else dst[cell * ncomp + c] = src[e];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Handle
 struct dtfe_gpu_s {
@@ -1616,9 +1736,16 @@ struct dtfe_gpu_s {
   float4* vel4 = nullptr;
   float* scal = nullptr;
   float* w = nullptr;
-  double* vol = nullptr;          // per-tetrahedron volume
+  long long* vacc = nullptr;      // per-vertex volume sums in exact units (fixed_volume.cuh)
+  VolScale* vscale = nullptr;     // per sub-box: its units (from its vertices' bounding box)
+  int* vbbox = nullptr;           // per sub-box bounding box (float order keys)
+  int64_t* sb_vprefix = nullptr;  // nsb + 1 vertex range starts of the scale boxes
+  int64_t* sb_tprefix = nullptr;  // nsb + 1 tetrahedron range starts
+  int nsb = 0;                    // scale boxes: the sub-boxes, or the whole upload before set_subboxes
+  bool scale_ready = false;
   int64_t* inc_off = nullptr;     // V+1 offsets into inc
-  int* inc = nullptr;             // incident tetrahedra per vertex, ascending
+  int* inc = nullptr;             // incident tetrahedra per vertex (built when needed)
+  bool inc_ready = false;
   int* scratch_i = nullptr;       // V ints (degrees / fill cursors)
   int64_t* scan_blocks = nullptr; // block totals of the offset scan
   int* hull = nullptr;
@@ -1687,6 +1814,10 @@ struct dtfe_gpu_s {
   void* m1_lists = nullptr;       // method-1 tetrahedra of every cell
   size_t m1_lists_bytes = 0;
   float* sph_out = nullptr;       // host-output SPH staging
+  int4* tet_rec = nullptr;        // interleaved (vertices, neighbours) per tetrahedron, built on first use
+  bool rec_ready = false;
+  TileRec* tile_recs = nullptr;   // dtfe_gpu_tiles_*: the tiles of one call
+  int64_t* tile_start = nullptr;  // ... and their packed offsets
 };
 
 namespace {
@@ -1743,26 +1874,98 @@ void drop_graph(dtfe_handle h) {
 // the cell centres with the raster fused into the volume kernel (3, 2 or 4
 // blocks per SM); variants 3..8 walk from seeds (blocks per SM, samples per
 // thread); variants 9..11 walk and evaluate in one kernel (3, 2 or 4 blocks
-// per SM; for the averaging methods they walk as variant 3).  Evaluation
-// variants: register budget of the evaluation kernel.
+// per SM; for the averaging methods they walk as variant 3); variants 12..13
+// do the same over the interleaved 32-byte tetrahedron records (4 or 3
+// blocks per SM).  Evaluation variants: register budget of the evaluation
+// kernel.
 constexpr int kNumRasterVariants = 3;
 struct LocVariant { int block, minb, r; };
 constexpr LocVariant kWalkVariants[] = {{256, 3, 1}, {256, 2, 1}, {256, 4, 1}, {256, 3, 2}, {256, 4, 2}, {256, 3, 4}};
 constexpr int kNumWalkVariants = sizeof(kWalkVariants) / sizeof(kWalkVariants[0]);
-constexpr int kFusedMinBlocks[] = {3, 2, 4};
+struct FusedVariant { int minb; bool rec; };
+constexpr FusedVariant kFused[] = {{3, false}, {2, false}, {4, false}, {4, true}, {3, true}};
 constexpr int kFirstFused = kNumRasterVariants + kNumWalkVariants;
-constexpr int kNumLocVariants = kFirstFused + sizeof(kFusedMinBlocks) / sizeof(kFusedMinBlocks[0]);
+constexpr int kNumLocVariants = kFirstFused + sizeof(kFused) / sizeof(kFused[0]);
+inline bool uses_records(int loc_variant) {
+  return loc_variant >= kFirstFused && kFused[loc_variant - kFirstFused].rec;
+}
 inline bool is_raster(int loc_variant) { return loc_variant < kNumRasterVariants; }
 inline bool is_fused(int loc_variant) { return loc_variant >= kFirstFused; }
 constexpr int kNumEvalVariants = 3;
 
-// Per step, before the interpolation: tetrahedron volumes and either the
-// cell centres' tetrahedra (raster) or the walk seeds.  Without sub-boxes,
-// volumes only.
+// Vertex -> tetrahedron incidence lists (in no particular order within a
+// vertex): degrees, their scan into offsets, the fill.  Built with a
+// neighbour-less upload (to derive the neighbours) or for the adjoint.
+int build_incidence(dtfe_handle h) {
+  const int64_t V = h->V, T = h->T;
+  int rc;
+  if ((rc = dev_alloc(h, &h->inc_off, V + 1)) || (rc = dev_alloc(h, &h->inc, 4 * T)) ||
+      (rc = dev_alloc(h, &h->scratch_i, V)) ||
+      (rc = dev_alloc(h, &h->scan_blocks, (V + kScanBlock - 1) / kScanBlock + 1)))
+    return rc;
+  cudaStream_t st = h->stream;
+  if (V) {
+    DTFE_CUDA_TRY(cudaMemsetAsync(h->scratch_i, 0, sizeof(int) * V, st));
+    if (T) k_degree<<<blocks_for(T, 256), 256, 0, st>>>(T, h->tet_v, h->scratch_i);
+    const int64_t nb = (V + kScanBlock - 1) / kScanBlock;
+    k_scan_blocks<<<(unsigned)nb, kScanBlock, 0, st>>>(V, h->scratch_i, h->inc_off, h->scan_blocks);
+    k_scan_totals<<<1, kScanBlock, 0, st>>>(nb, h->scan_blocks, h->inc_off + V);
+    k_scan_add<<<(unsigned)nb, kScanBlock, 0, st>>>(V, h->inc_off, h->scan_blocks);
+    DTFE_CUDA_TRY(cudaMemsetAsync(h->scratch_i, 0, sizeof(int) * V, st));
+    if (T) k_fill_incidence<<<blocks_for(T, 256), 256, 0, st>>>(T, h->tet_v, h->inc_off, h->scratch_i, h->inc);
+  }
+  DTFE_CUDA_TRY(cudaGetLastError());
+  h->inc_ready = true;
+  return DTFE_OK;
+}
+
+// The units of the exact volume sums (fixed_volume.cuh), one per sub-box
+// (the whole upload before dtfe_gpu_set_subboxes): the bounding box of its
+// vertices, then its scale.  Once per upload and sub-box layout.
+int ensure_scales(dtfe_handle h) {
+  if (h->scale_ready) return DTFE_OK;
+  const int nsb = h->K > 0 ? h->K : 1;
+  std::vector<int64_t> vp(nsb + 1), tp(nsb + 1);
+  if (h->K > 0) {
+    for (int b = 0; b < nsb; ++b) {
+      vp[b] = h->boxes_h[b].vert_offset;
+      tp[b] = h->boxes_h[b].tet_offset;
+    }
+    vp[nsb] = h->boxes_h[nsb - 1].vert_offset + h->boxes_h[nsb - 1].n_verts;
+    tp[nsb] = h->boxes_h[nsb - 1].tet_offset + h->boxes_h[nsb - 1].n_tets;
+  } else {
+    vp[0] = tp[0] = 0;
+    vp[1] = h->V;
+    tp[1] = h->T;
+  }
+  int rc;
+  if ((rc = dev_alloc(h, &h->sb_vprefix, nsb + 1)) || (rc = dev_alloc(h, &h->sb_tprefix, nsb + 1)) ||
+      (rc = dev_alloc(h, &h->vbbox, 6 * (size_t)nsb)) || (rc = dev_alloc(h, &h->vscale, (size_t)nsb)))
+    return rc;
+  cudaStream_t st = h->stream;
+  DTFE_CUDA_TRY(cudaMemcpyAsync(h->sb_vprefix, vp.data(), sizeof(int64_t) * (nsb + 1), cudaMemcpyHostToDevice, st));
+  DTFE_CUDA_TRY(cudaMemcpyAsync(h->sb_tprefix, tp.data(), sizeof(int64_t) * (nsb + 1), cudaMemcpyHostToDevice, st));
+  k_box_bbox_init<<<blocks_for(6 * nsb, 256), 256, 0, st>>>(nsb, h->vbbox);
+  if (h->V) k_box_bbox<<<blocks_for(h->V, 256), 256, 0, st>>>(h->V, h->posd, h->sb_vprefix, nsb, h->vbbox);
+  k_box_scales<<<blocks_for(nsb, 64), 64, 0, st>>>(nsb, h->vbbox, h->sb_vprefix, h->vscale);
+  DTFE_CUDA_TRY(cudaGetLastError());
+  DTFE_CUDA_TRY(cudaStreamSynchronize(st));  // the host prefix tables go out of scope
+  h->nsb = nsb;
+  h->scale_ready = true;
+  return DTFE_OK;
+}
+
+// Per step, before the interpolation: the tetrahedron volumes, added into
+// their vertices' exact sums, and either the cell centres' tetrahedra
+// (raster) or the walk seeds.  Without sub-boxes, volumes only.
 int launch_prep(dtfe_handle h) {
   cudaStream_t st = h->stream;
   const bool raster = is_raster(h->loc_variant);
+  int src = ensure_scales(h);
+  if (src) return src;
   DTFE_CUDA_TRY(cudaMemsetAsync(h->counters + CNT_RASTER_EXACT, 0, 2 * sizeof(unsigned long long), st));
+  if (h->V) DTFE_CUDA_TRY(cudaMemsetAsync(h->vacc, 0, sizeof(long long) * h->V, st));
+  const VolSums VS{h->vacc, h->vscale, h->sb_tprefix, h->nsb};
   if (h->K > 0 && raster) {
     int rc = dev_alloc(h, &h->tet_c, h->n_cells);
     if (rc) return rc;
@@ -1771,7 +1974,7 @@ int launch_prep(dtfe_handle h) {
       const unsigned nb = blocks_for(h->T, kRasterBlock);
       auto* k = h->loc_variant == 1 ? k_tet_volume_raster<2>
                                     : (h->loc_variant == 2 ? k_tet_volume_raster<4> : k_tet_volume_raster<3>);
-      k<<<nb, kRasterBlock, 0, st>>>(h->T, h->tet_v, h->posd, h->vol, h->boxes, h->tet_prefix, h->tile_prefix,
+      k<<<nb, kRasterBlock, 0, st>>>(h->T, h->tet_v, h->posd, VS, h->boxes, h->tet_prefix, h->tile_prefix,
                                      h->raster_axes, h->K, h->xs, h->ys, h->zs, (unsigned*)h->tet_c,
                                      h->counters + CNT_RASTER_EXACT);
     }
@@ -1779,11 +1982,11 @@ int launch_prep(dtfe_handle h) {
     DTFE_CUDA_TRY(cudaMemsetAsync(h->bins, 0xFF, sizeof(unsigned long long) * h->n_cells, st));
     if (h->T > 0)
       k_tet_volume_bins<true><<<blocks_for(h->T, kVolBlock), kVolBlock, 0, st>>>(
-          h->T, h->tet_v, h->posd, h->vol, h->boxes, h->tet_prefix, h->bin_offset, h->K, h->xs, h->ys, h->zs,
+          h->T, h->tet_v, h->posd, VS, h->boxes, h->tet_prefix, h->bin_offset, h->K, h->xs, h->ys, h->zs,
           h->bins);
   } else if (h->T > 0) {
     k_tet_volume_bins<false><<<blocks_for(h->T, kVolBlock), kVolBlock, 0, st>>>(
-        h->T, h->tet_v, h->posd, h->vol, h->boxes, h->tet_prefix, h->bin_offset, h->K, h->xs, h->ys, h->zs,
+        h->T, h->tet_v, h->posd, VS, h->boxes, h->tet_prefix, h->bin_offset, h->K, h->xs, h->ys, h->zs,
         h->bins);
   }
   DTFE_CUDA_TRY(cudaGetLastError());
@@ -1831,9 +2034,19 @@ void launch_eval(int method, int evariant, const InterpParams& P, const int* tet
 
 template <int S>
 void launch_fused(int fv, const InterpParams& P, int* tet_c, cudaStream_t st, unsigned grid, unsigned block) {
-  if (kFusedMinBlocks[fv] == 2) k_locate_eval<S, 2><<<grid, block, 0, st>>>(P, tet_c);
-  else if (kFusedMinBlocks[fv] == 4) k_locate_eval<S, 4><<<grid, block, 0, st>>>(P, tet_c);
-  else k_locate_eval<S, 3><<<grid, block, 0, st>>>(P, tet_c);
+  const FusedVariant& F = kFused[fv];
+  // record walks are built for the scalar counts a handle accepts (0-4, 8)
+  constexpr bool kRecOk = S <= 4 || S == 8;
+  if (F.rec && kRecOk) {
+    if (F.minb == 4) k_locate_eval<S, 4, kRecOk><<<grid, block, 0, st>>>(P, tet_c);
+    else k_locate_eval<S, 3, kRecOk><<<grid, block, 0, st>>>(P, tet_c);
+  } else if (F.minb == 2) {
+    k_locate_eval<S, 2><<<grid, block, 0, st>>>(P, tet_c);
+  } else if (F.minb == 4) {
+    k_locate_eval<S, 4><<<grid, block, 0, st>>>(P, tet_c);
+  } else {
+    k_locate_eval<S, 3><<<grid, block, 0, st>>>(P, tet_c);
+  }
 }
 
 void launch_fused_s(int S, int fv, const InterpParams& P, int* tet_c, cudaStream_t st, unsigned grid,
@@ -1916,7 +2129,8 @@ int dtfe_gpu_destroy(dtfe_handle h) {
   cudaSetDevice(h->device);
   cudaStreamSynchronize(h->stream);
   if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
-  void* ptrs[] = {h->tet_v, h->tet_n, h->posd, h->vel4, h->scal, h->w, h->vol, h->inc_off, h->inc,
+  void* ptrs[] = {h->tet_v, h->tet_n, h->posd, h->vel4, h->scal, h->w, h->vacc, h->vscale, h->vbbox,
+                  h->sb_vprefix, h->sb_tprefix, h->inc_off, h->inc,
                   h->scratch_i, h->scan_blocks, h->hull, h->pts_buf, h->pts_keep, h->pts_idx, h->pts_blocks,
                   h->pts_out,
                   h->boxes, h->tile_prefix, h->pencil_prefix, h->tet_prefix, h->bin_offset, h->bins,
@@ -1928,7 +2142,8 @@ int dtfe_gpu_destroy(dtfe_handle h) {
   if (h->dep_scratch) cudaFree(h->dep_scratch);
   for (void* p : {(void*)h->g_rho, (void*)h->g_x, (void*)h->g_v, (void*)h->g_S, (void*)h->g_m, (void*)h->vbar,
                   (void*)h->adj_a, h->sph_scratch, (void*)h->sph_out, (void*)h->upload_buf, (void*)h->m1_table,
-                  h->m1_scratch, h->m1_lists, (void*)h->sel_counts, (void*)h->sel_first, (void*)h->sel_blocks})
+                  h->m1_scratch, h->m1_lists, (void*)h->sel_counts, (void*)h->sel_first, (void*)h->sel_blocks,
+                  (void*)h->tile_recs, (void*)h->tile_start, (void*)h->tet_rec})
     if (p) cudaFree(p);
   if (h->dep_out) cudaFree(h->dep_out);
   for (int i = 0; i < 2; ++i) {
@@ -1973,10 +2188,7 @@ static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const fl
   const size_t vert_stage = sizeof(float) * 3 * (size_t)n_verts;
   if ((rc = dev_alloc(h, &h->tet_v, n_tets)) || (rc = dev_alloc(h, &h->tet_n, n_tets)) ||
       (rc = dev_alloc(h, &h->posd, n_verts)) || (rc = dev_alloc(h, &h->vel4, n_verts)) ||
-      (rc = dev_alloc(h, &h->w, n_verts)) || (rc = dev_alloc(h, &h->vol, n_tets)) ||
-      (rc = dev_alloc(h, &h->inc_off, n_verts + 1)) || (rc = dev_alloc(h, &h->inc, 4 * n_tets)) ||
-      (rc = dev_alloc(h, &h->scratch_i, n_verts)) ||
-      (rc = dev_alloc(h, &h->scan_blocks, (n_verts + kScanBlock - 1) / kScanBlock + 1)) ||
+      (rc = dev_alloc(h, &h->w, n_verts)) || (rc = dev_alloc(h, &h->vacc, n_verts)) ||
       (rc = dev_alloc(h, &h->hull, n_verts)) ||
       (rc = dev_alloc(h, &h->scal, (size_t)n_verts * h->S)) ||
       // staging kept in the handle (an allocation per upload would map and
@@ -2014,30 +2226,26 @@ static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const fl
     else DTFE_CUDA_TRY(cudaMemsetAsync(h->vel4, 0, sizeof(float4) * n_verts, st));
     if (h->S > 0 && !scal) DTFE_CUDA_TRY(cudaMemsetAsync(h->scal, 0, sizeof(float) * h->S * n_verts, st));
   }
-  // vertex -> tetrahedron incidence lists (ascending tetrahedron ids)
-  if (n_verts) {
-    DTFE_CUDA_TRY(cudaMemsetAsync(h->scratch_i, 0, sizeof(int) * n_verts, st));
-    if (n_tets) k_degree<<<blocks_for(n_tets, 256), 256, 0, st>>>(n_tets, h->tet_v, h->scratch_i);
-    int64_t nb = (n_verts + kScanBlock - 1) / kScanBlock;
-    k_scan_blocks<<<(unsigned)nb, kScanBlock, 0, st>>>(n_verts, h->scratch_i, h->inc_off, h->scan_blocks);
-    k_scan_totals<<<1, kScanBlock, 0, st>>>(nb, h->scan_blocks, h->inc_off + n_verts);
-    k_scan_add<<<(unsigned)nb, kScanBlock, 0, st>>>(n_verts, h->inc_off, h->scan_blocks);
-    DTFE_CUDA_TRY(cudaMemsetAsync(h->scratch_i, 0, sizeof(int) * n_verts, st));
-    if (n_tets) {
-      k_fill_incidence<<<blocks_for(n_tets, 256), 256, 0, st>>>(n_tets, h->tet_v, h->inc_off, h->scratch_i, h->inc);
-      k_sort_incidence_staged<<<blocks_for(n_verts, kSortBlock), kSortBlock, 0, st>>>(n_verts, h->inc_off,
-                                                                                       h->inc);
-    }
-  }
-  // neighbours from the vertices, when they did not cross
-  if (n_tets && derive_neighbours)
+  // vertex -> tetrahedron incidence lists, for deriving the neighbours
+  h->inc_ready = false;
+  if (derive_neighbours && (rc = build_incidence(h))) return rc;
+  // neighbours from the vertices, when they did not cross: every face at its
+  // smallest vertex's star, then the few faces of very large stars
+  if (n_tets && derive_neighbours) {
+    DTFE_CUDA_TRY(cudaMemsetAsync(h->tet_n, 0x80, sizeof(int4) * n_tets, st));
+    const int64_t want = (n_verts + kStarWarps - 1) / kStarWarps;
+    k_neighbours_star<<<(unsigned)std::min<int64_t>(want, 148 * 32), 32 * kStarWarps, 0, st>>>(
+        n_verts, h->tet_v, h->inc_off, h->inc, (int*)h->tet_n);
     k_derive_neighbours<<<blocks_for(n_tets, 256), 256, 0, st>>>(n_tets, h->tet_v, h->inc_off, h->inc, h->tet_n);
+  }
   // hull vertices (a property of the tessellation's topology)
   if (n_verts) DTFE_CUDA_TRY(cudaMemsetAsync(h->hull, 0, sizeof(int) * n_verts, st));
   if (n_tets) k_hull_marks<<<blocks_for(n_tets, 256), 256, 0, st>>>(n_tets, h->tet_v, h->tet_n, h->hull);
   DTFE_CUDA_TRY(cudaGetLastError());
   h->has_vel = vel != nullptr;
   h->has_scal = scal != nullptr;
+  h->rec_ready = false;
+  h->scale_ready = false;
   h->density_ready = false;
   h->prep_ready = false;
   h->tet_c_valid = false;
@@ -2238,6 +2446,7 @@ int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* box
     }
   h->n_cells = cells;
   h->n_pencils = ppre[n_boxes];
+  h->scale_ready = false;  // the exact sums' units are per sub-box
   h->grid[0] = grid[0]; h->grid[1] = grid[1]; h->grid[2] = grid[2];
   h->prep_ready = false;
   h->eq_nn = 0;
@@ -2270,8 +2479,8 @@ int dtfe_gpu_vertex_density(dtfe_handle h, double rho_bar) {
   float rb = (float)rho_bar;
   float factor = (float)(4.0 / (double)rb);
   h->factor = factor;
-  k_vertex_density<<<blocks_for(h->V, kDensBlock), kDensBlock, 0, st>>>(h->V, h->w, h->vol, h->inc_off, h->inc,
-                                                                       h->hull, factor, h->posd);
+  k_vertex_density<<<blocks_for(h->V, kDensBlock), kDensBlock, 0, st>>>(h->V, h->w, h->vacc, h->hull, h->vscale,
+                                                                       h->sb_vprefix, h->nsb, factor, h->posd);
   DTFE_CUDA_TRY(cudaGetLastError());
   h->density_ready = true;
   return DTFE_OK;
@@ -2359,8 +2568,15 @@ static int interp_enqueue(dtfe_handle h, const dtfe_interp_opts* o, float* const
   }
   DTFE_CUDA_TRY(cudaMemsetAsync(h->counters, 0, sizeof(unsigned long long) * CNT_N, st));
   InterpParams P;
+  if (uses_records(h->loc_variant) && method == DTFE_METHOD_CENTRE && !h->rec_ready) {
+    if ((rc = dev_alloc(h, &h->tet_rec, 2 * (size_t)h->T))) return rc;
+    k_build_records<<<blocks_for(h->T, 256), 256, 0, st>>>(h->T, h->tet_v, h->tet_n, h->tet_rec);
+    DTFE_CUDA_TRY(cudaGetLastError());
+    h->rec_ready = true;
+  }
   P.tet_v = h->tet_v;
   P.tet_n = h->tet_n;
+  P.tet_rec = h->tet_rec;
   P.posd = h->posd;
   P.vel4 = h->vel4;
   P.scal = h->scal;
@@ -2534,7 +2750,8 @@ int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xyz, const fl
                           size_t* scratch_bytes, void* saved);
 int dtfe_gpu_deposit_adjoint_impl(void* stream, const void* saved, const float* a_dev, float* gx_dev, float* gw_dev);
 int dtfe_internal_adjoint(void* stream, const void* cell_params, int64_t n_cells, int64_t V, int64_t T,
-                          const int4* tet_v, const float4* posd, const float* w, const int* hull, const double* vol,
+                          const int4* tet_v, const float4* posd, const float* w, const int* hull,
+                          const long long* vacc, const VolScale* vscale, const int64_t* vprefix, int nsb,
                           const int64_t* off, const int* inc, float factor, double* g_rho, double* g_x, double* g_v,
                           double* g_S, double* g_m, double* vbar, float* out_x, float* out_v, float* out_w);
 size_t dtfe_internal_adjoint_params_size();
@@ -2600,9 +2817,11 @@ int dtfe_gpu_adjoint_dev(dtfe_handle h, const float* grad_density_dev, const flo
   dtfe_internal_adjoint_fill_params(params, h->tet_v, h->posd, h->vel4, h->tet_c, h->boxes, h->tile_prefix, h->xs,
                                     h->ys, h->zs, h->K, h->grid[1], h->grid[2], h->n_cells, grad_density_dev,
                                     grad_divergence_dev, grad_velocity_dev, h->tet_c_fix ? 1 : 0);
-  rc = dtfe_internal_adjoint(h->stream, params, h->n_cells, h->V, h->T, h->tet_v, h->posd, h->w, h->hull, h->vol,
-                             h->inc_off, h->inc, h->factor, h->g_rho, h->g_x, h->g_v, h->g_S, h->g_m, h->vbar,
-                             grad_xyz_dev, grad_vel_dev, grad_w_dev);
+  // the volume-gradient gather runs over the incidence lists (built once per upload)
+  if (!h->inc_ready && (rc = build_incidence(h))) return rc;
+  rc = dtfe_internal_adjoint(h->stream, params, h->n_cells, h->V, h->T, h->tet_v, h->posd, h->w, h->hull, h->vacc,
+                             h->vscale, h->sb_vprefix, h->nsb, h->inc_off, h->inc, h->factor, h->g_rho, h->g_x,
+                             h->g_v, h->g_S, h->g_m, h->vbar, grad_xyz_dev, grad_vel_dev, grad_w_dev);
   if (rc) return set_error(rc, "adjoint kernels failed");
   DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return DTFE_OK;
@@ -3245,6 +3464,52 @@ int dtfe_gpu_download_tets(dtfe_handle h, int32_t* tet_v, int32_t* tet_n) {
     DTFE_CUDA_TRY(cudaMemcpyAsync(tet_n, h->tet_n, 16 * h->T, cudaMemcpyDeviceToHost, h->stream));
   DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return DTFE_OK;
+}
+
+// dtfe_gpu_tiles_gather_dev / dtfe_gpu_tiles_scatter_dev
+static int tiles_copy(dtfe_handle h, int32_t n_tiles, const int32_t* tiles, const int32_t grid[3], int32_t ncomp,
+                      const float* src_dev, float* dst_dev, int to_packed) {
+  if (!h || n_tiles < 0 || (n_tiles > 0 && (!tiles || !src_dev || !dst_dev)) || !grid || ncomp < 1)
+    return set_error(DTFE_ERR_ARG, "null argument or bad size");
+  if (n_tiles == 0) return DTFE_OK;
+  std::vector<TileRec> recs((size_t)n_tiles);
+  std::vector<int64_t> start((size_t)n_tiles + 1, 0);
+  for (int t = 0; t < n_tiles; ++t) {
+    for (int a = 0; a < 3; ++a) {
+      recs[t].o[a] = tiles[6 * t + a];
+      recs[t].d[a] = tiles[6 * t + 3 + a];
+      if (recs[t].o[a] < 0 || recs[t].d[a] < 0 || (int64_t)recs[t].o[a] + recs[t].d[a] > grid[a])
+        return set_error(DTFE_ERR_ARG, "tile outside the grid");
+    }
+    start[t + 1] = start[t] + (int64_t)recs[t].d[0] * recs[t].d[1] * recs[t].d[2];
+  }
+  DTFE_CUDA_TRY(cudaSetDevice(h->device));
+  int rc;
+  if ((rc = dev_alloc(h, &h->tile_recs, (size_t)n_tiles)) || (rc = dev_alloc(h, &h->tile_start, (size_t)n_tiles + 1)))
+    return rc;
+  cudaStream_t st = h->stream;
+  DTFE_CUDA_TRY(cudaMemcpyAsync(h->tile_recs, recs.data(), sizeof(TileRec) * n_tiles, cudaMemcpyHostToDevice, st));
+  DTFE_CUDA_TRY(cudaMemcpyAsync(h->tile_start, start.data(), sizeof(int64_t) * (n_tiles + 1),
+                                cudaMemcpyHostToDevice, st));
+  const int64_t total = start[n_tiles] * ncomp;
+  if (total > 0) {
+    const unsigned nb = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 64);
+    k_tiles_copy<<<nb, 256, 0, st>>>(n_tiles, h->tile_recs, h->tile_start, grid[1], grid[2], ncomp, to_packed,
+                                     src_dev, dst_dev);
+    DTFE_CUDA_TRY(cudaGetLastError());
+  }
+  DTFE_CUDA_TRY(cudaStreamSynchronize(st));  // the host tables go out of scope
+  return DTFE_OK;
+}
+
+int dtfe_gpu_tiles_gather_dev(dtfe_handle h, int32_t n_tiles, const int32_t* tiles, const int32_t grid[3],
+                              int32_t ncomp, const float* field_dev, float* packed_dev) {
+  return tiles_copy(h, n_tiles, tiles, grid, ncomp, field_dev, packed_dev, 1);
+}
+
+int dtfe_gpu_tiles_scatter_dev(dtfe_handle h, int32_t n_tiles, const int32_t* tiles, const int32_t grid[3],
+                               int32_t ncomp, const float* packed_dev, float* field_dev) {
+  return tiles_copy(h, n_tiles, tiles, grid, ncomp, packed_dev, field_dev, 0);
 }
 
 int dtfe_gpu_set_max_walk_steps(dtfe_handle h, int32_t max_walk_steps) {

@@ -346,6 +346,89 @@ __device__ __forceinline__ int walk_locate(const int4* __restrict__ tet_v, const
   return kWalkFail;
 }
 
+// The same walk over interleaved 32-byte tetrahedron records (rec[2t] = the
+// vertices, rec[2t+1] = the neighbours of t): a step reads one sector for the
+// next tetrahedron's vertices and neighbours together, then the one new
+// vertex.  The vertices' densities (posd .w) ride along in D for the
+// evaluation.  Same tests in the same order as walk_locate, so the same
+// tetrahedron is located (ties resolved by canonical_tie on the plain arrays).
+template <bool FLOAT_POINT = false>
+__device__ __forceinline__ int walk_locate_rec(const int4* __restrict__ rec, const int4* __restrict__ tet_v,
+                                               const int4* __restrict__ tet_n, const float4* __restrict__ posd,
+                                               const double p[3], int t, int max_steps, int v[4], float X[4][3],
+                                               float D[4], WalkStats& st) {
+  const float pf[3] = {(float)p[0], (float)p[1], (float)p[2]};
+  int4 q = __ldg(&rec[2 * (int64_t)t]);
+  int4 n = __ldg(&rec[2 * (int64_t)t + 1]);
+  v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const float4 r = __ldg(&posd[v[a]]);
+    X[a][0] = r.x; X[a][1] = r.y; X[a][2] = r.z; D[a] = r.w;
+  }
+  int came = -1;
+  for (int step = 0; step < max_steps; ++step) {
+    ++st.steps;
+    int need = 15 & ~(came >= 0 ? (1 << came) : 0);
+    int zmask;
+    int exit_face = FLOAT_POINT ? first_exit_face_f32(X, pf, need, zmask, st.exact)
+                                : first_exit_face(X, p, need, zmask, st.exact);
+    if (exit_face < 0) {
+      if (zmask) {
+        ++st.tie;
+        int b = canonical_tie(tet_v, tet_n, posd, t, zmask, p[0], p[1], p[2]);
+        if (b != t) {
+          t = b;
+          const int4 qq = __ldg(&rec[2 * (int64_t)t]);
+          v[0] = qq.x; v[1] = qq.y; v[2] = qq.z; v[3] = qq.w;
+#pragma unroll
+          for (int a = 0; a < 4; ++a) {
+            const float4 r = __ldg(&posd[v[a]]);
+            X[a][0] = r.x; X[a][1] = r.y; X[a][2] = r.z; D[a] = r.w;
+          }
+        }
+      }
+      return t;
+    }
+    const int nb = nb_of(n, exit_face);
+    if (nb < 0) return kOutside;
+    q = __ldg(&rec[2 * (int64_t)nb]);
+    n = __ldg(&rec[2 * (int64_t)nb + 1]);
+    int nv[4] = {q.x, q.y, q.z, q.w};
+    float NX[4][3], ND[4];
+    came = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      bool found = false;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) NX[j][c] = 0.f;
+      ND[j] = 0.f;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const bool m = (k != exit_face) && (v[k] == nv[j]);
+        found = found || m;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) NX[j][c] = m ? X[k][c] : NX[j][c];
+        ND[j] = m ? D[k] : ND[j];
+      }
+      if (!found) {
+        const float4 r = __ldg(&posd[nv[j]]);
+        NX[j][0] = r.x; NX[j][1] = r.y; NX[j][2] = r.z; ND[j] = r.w;
+        came = j;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      v[j] = nv[j];
+      D[j] = ND[j];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) X[j][c] = NX[j][c];
+    }
+    t = nb;
+  }
+  return kWalkFail;
+}
+
 // ---- per-sample arithmetic (reference precision pattern) -----------------
 
 // minorDeterminant + matrixInverse (triangulation_miscellaneous.cc:42-96).
@@ -378,7 +461,8 @@ __device__ __forceinline__ void cell_eval(const int v[4], const float X[4][3], c
                                           const float4* __restrict__ posd,
                                           const float4* __restrict__ vel4,
                                           const float* __restrict__ scal, bool want_dens,
-                                          bool want_vel, bool want_sc, bool fix, CellOut& e) {
+                                          bool want_vel, bool want_sc, bool fix, CellOut& e,
+                                          const float* Dv = nullptr) {
   double A[3][3];
 #pragma unroll
   for (int r = 0; r < 3; ++r)
@@ -390,10 +474,11 @@ __device__ __forceinline__ void cell_eval(const int v[4], const float X[4][3], c
 #pragma unroll
   for (int c = 0; c < 3; ++c) rel[c] = (float)(p[c] - (double)X[0][c]);
   if (want_dens) {
-    float d0 = __ldg(&posd[v[0]]).w;
+    // vertex densities: carried from the walk (Dv), else read
+    float d0 = Dv ? Dv[0] : __ldg(&posd[v[0]]).w;
     float dd[3];
 #pragma unroll
-    for (int i = 0; i < 3; ++i) dd[i] = __ldg(&posd[v[i + 1]]).w - d0;
+    for (int i = 0; i < 3; ++i) dd[i] = (Dv ? Dv[i + 1] : __ldg(&posd[v[i + 1]]).w) - d0;
     float gr[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {

@@ -372,6 +372,25 @@ class DeviceDTFE:
         N.check(self.lib.dtfe_gpu_download_tets(self.h, tv.ctypes.data, tn.ctypes.data))
         return tv, tn
 
+    def tiles_gather_dev(self, tiles: np.ndarray, grid, field, packed) -> None:
+        """Copies the tiles (K, 6 int: origin, dims) of a main-grid field
+        (CUDA tensor, cells x components) into ``packed`` (CUDA tensor), tile
+        after tile (dtfe_gpu_tiles_gather_dev)."""
+        t = np.ascontiguousarray(tiles, np.int32).reshape(-1, 6)
+        g = np.ascontiguousarray(grid, np.int32)
+        nc = int(field.numel() // int(np.prod(g))) if field.numel() else 1
+        N.check(self.lib.dtfe_gpu_tiles_gather_dev(self.h, len(t), t.ctypes.data, g.ctypes.data, nc,
+                                                   N.ptr(field), N.ptr(packed)))
+
+    def tiles_scatter_dev(self, tiles: np.ndarray, grid, packed, field) -> None:
+        """Writes a packed buffer back into the tiles of a main-grid field
+        (dtfe_gpu_tiles_scatter_dev)."""
+        t = np.ascontiguousarray(tiles, np.int32).reshape(-1, 6)
+        g = np.ascontiguousarray(grid, np.int32)
+        nc = int(field.numel() // int(np.prod(g))) if field.numel() else 1
+        N.check(self.lib.dtfe_gpu_tiles_scatter_dev(self.h, len(t), t.ctypes.data, g.ctypes.data, nc,
+                                                    N.ptr(packed), N.ptr(field)))
+
     def set_max_walk_steps(self, n: int) -> None:
         """Step limit of the point-location walks (0 = default)."""
         N.check(self.lib.dtfe_gpu_set_max_walk_steps(self.h, int(n)))

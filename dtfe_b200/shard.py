@@ -7,10 +7,19 @@ grid (copySubgridResultsToMain, src/subpartition.h:399-432).  Here the same
 split is made for ``world * parts_per_rank`` parts; each rank tessellates and
 interpolates only the parts assigned to it (greedy by particle count, so the
 heaviest part goes to the least loaded rank) and the disjoint grid tiles are
-exchanged once with an all-gather of packed tiles.  No collective runs
-inside the interpolation itself.
+exchanged once with an all-gather (or a gather to one rank) of packed
+tiles.  No collective runs inside the interpolation itself.
 
-Every rank must call ``gather_fields`` (a collective) in the same order.
+``gather_fields_dev`` exchanges device fields: the tiles are packed and
+unpacked by kernels (dtfe_gpu_tiles_gather_dev / _scatter_dev) and, with
+NCCL, never leave the GPUs; ``gather_fields`` is the host form for numpy
+fields.  Every rank must call them (collectives) in the same order.
+
+Grid deposition (NGP / CIC / TSC) needs no halo exchange here: the reference
+deposits every region's own padded particles into the region's own tile
+with stencils clipped at its edges (src/CIC_interpolation.cc:119-264), so
+ranks holding different regions write disjoint tiles and the same tile
+exchange assembles the grid.
 """
 from __future__ import annotations
 
@@ -83,17 +92,7 @@ def gather_fields(plan, fields: dict, group=None, device=None) -> dict:
     import torch
     import torch.distributed as dist
     world = dist.get_world_size(group)
-    table = tile_table(plan)
-    counts = torch.tensor([table.shape[0]], dtype=torch.int64, device=device)
-    all_counts = [torch.zeros_like(counts) for _ in range(world)]
-    dist.all_gather(all_counts, counts, group=group)
-    kmax = int(max(int(c.item()) for c in all_counts))
-    tpad = torch.full((max(kmax, 1), 6), -1, dtype=torch.int64, device=device)
-    if table.shape[0]:
-        tpad[:table.shape[0]] = torch.from_numpy(table).to(tpad.device)
-    tables = [torch.zeros_like(tpad) for _ in range(world)]
-    dist.all_gather(tables, tpad, group=group)
-    tables = [t[:int(c.item())].cpu().numpy() for t, c in zip(tables, all_counts)]
+    tables = _exchange_tables(plan, group, device)
     sizes = [int(np.prod(t[:, 3:6], axis=1).sum()) if len(t) else 0 for t in tables]
     smax = max(max(sizes), 1)
     g = plan.grid
@@ -115,4 +114,76 @@ def gather_fields(plan, fields: dict, group=None, device=None) -> dict:
                 full[o0:o0 + d0, o1:o1 + d1, o2:o2 + d2] = vals[pos:pos + m].reshape((d0, d1, d2) + comp)
                 pos += m
         out[name] = full.reshape((-1,) + comp)
+    return out
+
+
+def _exchange_tables(plan, group, device):
+    """Every rank's tile table: list of (K_r, 6) int64 arrays, rank order."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    table = tile_table(plan)
+    counts = torch.tensor([table.shape[0]], dtype=torch.int64, device=device)
+    all_counts = [torch.zeros_like(counts) for _ in range(world)]
+    dist.all_gather(all_counts, counts, group=group)
+    kmax = int(max(int(c.item()) for c in all_counts))
+    tpad = torch.full((max(kmax, 1), 6), -1, dtype=torch.int64, device=device)
+    if table.shape[0]:
+        tpad[:table.shape[0]] = torch.from_numpy(table).to(tpad.device)
+    tables = [torch.zeros_like(tpad) for _ in range(world)]
+    dist.all_gather(tables, tpad, group=group)
+    return [t[:int(c.item())].cpu().numpy() for t, c in zip(tables, all_counts)]
+
+
+def gather_fields_dev(dev, plan, fields: dict, group=None, root: int | None = None, tables=None) -> dict:
+    """The tile exchange on device fields: ``fields`` maps names to CUDA
+    tensors in the main-grid layout (cells x components; only this rank's
+    tiles meaningful).  This rank's tiles are packed on the device, one
+    all-gather per field (or one gather to ``root``) moves the packed
+    buffers, and each rank's buffer is scattered into a full-grid tensor on
+    the device.  With NCCL the buffers stay in device memory; with gloo (CPU
+    collectives) they are staged through host memory.  Returns name -> full
+    grid (CUDA tensor) on every rank, or on ``root`` only (None elsewhere).
+    ``tables`` (every rank's tile table) may be passed to skip their
+    exchange on repeated calls."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    on_gpu = dist.get_backend(group) == "nccl"
+    any_field = next(iter(fields.values()))
+    cdev = any_field.device
+    tables = tables if tables is not None else _exchange_tables(plan, group, cdev if on_gpu else None)
+    sizes = [int(np.prod(t[:, 3:6], axis=1).sum()) if len(t) else 0 for t in tables]
+    smax = max(max(sizes), 1)
+    grid = tuple(int(x) for x in plan.grid)
+    G = int(np.prod(grid))
+    mine = tile_table(plan)
+    out = {}
+    for name, arr in fields.items():
+        nc = int(arr.numel() // G)
+        buf = torch.zeros(smax * nc, dtype=torch.float32, device=cdev)
+        # buffers are filled on torch's stream, packed and unpacked on the
+        # handle's (each of those calls returns when its copy is done)
+        torch.cuda.current_stream(cdev).synchronize()
+        if sizes[rank]:
+            dev.tiles_gather_dev(mine, grid, arr, buf)
+        send = buf if on_gpu else buf.cpu()
+        if root is None:
+            bufs = [torch.empty_like(send) for _ in range(world)]
+            dist.all_gather(bufs, send, group=group)
+        else:
+            bufs = [torch.empty_like(send) for _ in range(world)] if rank == root else None
+            dist.gather(send, bufs, dst=root, group=group)
+        if root is not None and rank != root:
+            out[name] = None
+            continue
+        if not on_gpu:
+            bufs = [b.to(cdev) for b in bufs]
+        full = torch.zeros(arr.shape, dtype=torch.float32, device=cdev)
+        torch.cuda.current_stream(cdev).synchronize()  # the collective, copies and fill, before the unpacking
+        for t, b, n in zip(tables, bufs, sizes):
+            if n:
+                dev.tiles_scatter_dev(t, grid, b, full)
+        out[name] = full
     return out

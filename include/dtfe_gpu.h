@@ -195,7 +195,10 @@ int dtfe_gpu_set_subboxes(dtfe_handle h, int32_t n_boxes, const dtfe_subbox* box
 int dtfe_gpu_set_regions(dtfe_handle h, int32_t n_boxes, const float* regions);
 
 /* Vertex densities rho_v = w_v (D+1) / (rho_bar * sum of incident volumes),
- * 0 on the hull (vertexDensity, triangulation.cpp:200-279). */
+ * 0 on the hull (vertexDensity, triangulation.cpp:200-279).  Each FP64
+ * volume is added as an exact integer in units of 2^-62 of its sub-box's
+ * vertex bounding-box volume, so the sums do not depend on the order the
+ * GPU adds in (the reference adds floats in its incident-cell order). */
 int dtfe_gpu_vertex_density(dtfe_handle h, double rho_bar);
 
 /* Interpolate to the grid.  out[slot] receives field `slot` when its bit is
@@ -411,6 +414,18 @@ int dtfe_gpu_locate_points(dtfe_handle h, int64_t np, const double* pts, int32_t
  * centre outside the hull (the reference's infinite cell) and for cells
  * outside every tile.  DTFE_ERR_STATE before a cell-centre interpolation. */
 int dtfe_gpu_download_located(dtfe_handle h, int32_t* loc);
+/* Tile exchange between ranks that split one box (the multi-GPU form of
+ * copySubgridResultsToMain, src/subpartition.h:399-432): tiles holds
+ * n_tiles records of 6 int32 (origin x, y, z, dims x, y, z) of a grid of
+ * grid[0..2] cells; a field has ncomp floats per cell in the Quantities
+ * layout.  gather copies the tiles' values out of field_dev into packed_dev,
+ * tile after tile (x, y, z order inside a tile); scatter writes a packed
+ * buffer back into the tiles of field_dev.  Device pointers, ordered on the
+ * handle's stream; the call returns once the copy is done. */
+int dtfe_gpu_tiles_gather_dev(dtfe_handle h, int32_t n_tiles, const int32_t* tiles, const int32_t grid[3],
+                              int32_t ncomp, const float* field_dev, float* packed_dev);
+int dtfe_gpu_tiles_scatter_dev(dtfe_handle h, int32_t n_tiles, const int32_t* tiles, const int32_t grid[3],
+                               int32_t ncomp, const float* packed_dev, float* field_dev);
 /* Copies the device's tessellation arrays (4 T int32 each, either may be
  * NULL) to the host: after a packed or neighbour-less upload, the restored
  * tet_v and the derived tet_n. */
@@ -430,14 +445,20 @@ int dtfe_gpu_set_max_walk_steps(dtfe_handle h, int32_t max_walk_steps);
  * counterpart in the reference (it has no GPU path).
  * Inputs and output are DEVICE pointers on the current device: tet_v/tet_n
  * (4 int32 per tetrahedron, 16-byte aligned), xyz (3 floats per vertex), w
- * (V floats); dens receives V floats, the same values as
- * dtfe_gpu_vertex_density.  Scratch is a static device array for at most
- * DTFE_NOALLOC_MAX_VERTS vertices (12 MiB, resident on every device that
- * loads the library until exit); larger inputs return DTFE_ERR_TOO_LARGE.
- * All calls share that scratch: calls that overlap on the GPU race.  The
- * first call on a device looks up the scratch address; make it before any
- * stream capture.  stream: a cudaStream_t (NULL = default stream); the call
- * returns after the stream has finished it. */
+ * (V floats); dens receives V floats: rho_v = w (D+1) / (rho_bar * sum of
+ * incident volumes), 0 on the hull (vertexDensity,
+ * triangulation.cpp:200-279), with the volumes summed exactly as integers
+ * in units of 2^-62 of the vertices' bounding-box volume, so every call
+ * gives the same bits, those of dtfe_gpu_vertex_density for the same
+ * vertices uploaded as one sub-box.  Scratch
+ * is a static device array for at most DTFE_NOALLOC_MAX_VERTS vertices
+ * (12 MiB, resident on every device that loads the library until exit);
+ * larger inputs return DTFE_ERR_TOO_LARGE.  All calls share that scratch:
+ * calls that overlap on the GPU race.  The first call on a device looks up
+ * the scratch address; make it before any stream capture.  stream: a
+ * cudaStream_t (NULL = default stream); every call returns only after that
+ * stream has finished the work (it reads back its range check).  A tet_v
+ * entry outside [0, n_verts) returns DTFE_ERR_ARG and leaves dens as it was. */
 #define DTFE_NOALLOC_MAX_VERTS (1 << 20)
 int dtfe_vertex_density_noalloc(const int32_t* tet_v_dev, const int32_t* tet_n_dev, int64_t n_tets,
                                 const float* xyz_dev, const float* w_dev, int64_t n_verts,

@@ -33,6 +33,7 @@
 // agreement with an independent tessellator (scipy Qhull).
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -40,6 +41,7 @@
 
 #include "../include/dtfe_gpu.h"
 #include "../dtfe_b200/csrc/philox.h"
+#include "../dtfe_b200/csrc/fixed_volume.cuh"
 #include "../dtfe_b200/csrc/predicates.h"
 #include "../dtfe_b200/csrc/sobol.h"
 
@@ -325,11 +327,17 @@ extern "C" {
 // double in ascending tetrahedron order within each sub-box.  dens32: mode-0 result, float
 // factor (D+1)/rho_bar (:220) times the weight, divided by the double sum;
 // dens64: all-double result.  Either output may be NULL.
+// dens32: the device's arithmetic — per sub-box, each FP64 volume rounded
+// to integer units of 2^-62 of the sub-box vertices' bounding-box volume and
+// summed exactly (fixed_volume.cuh), then (w * factor) / volume rounded to
+// float; dens64 and volsum_out: plain FP64 sums (the FP64 oracle).
 int oracle_vertex_density(int64_t T, const int32_t* tv, const int32_t* tn, int64_t V,
                           const float* xyz, const float* w, double rho_bar, float* dens32,
                           double* dens64, double* volsum_out, int K, const dtfe_subbox* boxes,
                           int nthreads) {
   std::vector<double> vol(V, 0.0);
+  std::vector<long long> fixed(V, 0);
+  std::vector<double> unit(V, 0.0);
   std::vector<char> hull(V, 0);
   // Sub-boxes own disjoint vertex and tetrahedron ranges, so they run in
   // parallel (one host thread each, as the reference's OpenMP threads do).
@@ -338,13 +346,28 @@ int oracle_vertex_density(int64_t T, const int32_t* tv, const int32_t* tn, int64
   for (int b = 0; b < nb; ++b) {
     int64_t lo = (K > 0 && boxes) ? boxes[b].tet_offset : 0;
     int64_t hi = (K > 0 && boxes) ? boxes[b].tet_offset + boxes[b].n_tets : T;
+    const int64_t v0 = (K > 0 && boxes) ? boxes[b].vert_offset : 0;
+    const int64_t v1 = (K > 0 && boxes) ? boxes[b].vert_offset + boxes[b].n_verts : V;
+    int bb[6] = {INT32_MAX, INT32_MIN, INT32_MAX, INT32_MIN, INT32_MAX, INT32_MIN};
+    for (int64_t v = v0; v < v1; ++v)
+      for (int c = 0; c < 3; ++c) {
+        const int k = dtfe::float_order_key(xyz[3 * v + c]);
+        bb[2 * c] = std::min(bb[2 * c], k);
+        bb[2 * c + 1] = std::max(bb[2 * c + 1], k);
+      }
+    const dtfe::VolScale sc = v1 > v0 ? dtfe::vol_scale(dtfe::bbox_volume(bb)) : dtfe::VolScale{0.0, 0.0};
+    for (int64_t v = v0; v < v1; ++v) unit[v] = sc.unit;
     for (int64_t t = lo; t < hi; ++t) {
       double X[4][3];
       for (int a = 0; a < 4; ++a)
         for (int k = 0; k < 3; ++k) X[a][k] = (double)xyz[3 * (int64_t)tv[4 * t + a] + k];
       double v6 = dtfe::orient_det(X[0], X[1], X[2], X[3]);
       double vt = v6 / 6.0;
-      for (int a = 0; a < 4; ++a) vol[tv[4 * t + a]] += vt;
+      const long long q = std::llrint(vt * sc.inv_q);
+      for (int a = 0; a < 4; ++a) {
+        vol[tv[4 * t + a]] += vt;
+        fixed[tv[4 * t + a]] += q;
+      }
       for (int i = 0; i < 4; ++i)
         if (tn[4 * t + i] < 0)
           for (int a = 0; a < 4; ++a)
@@ -356,7 +379,7 @@ int oracle_vertex_density(int64_t T, const int32_t* tv, const int32_t* tn, int64
 #pragma omp parallel for schedule(static) num_threads(nthreads > 0 ? nthreads : 1)
   for (int64_t v = 0; v < V; ++v) {
     bool zero = hull[v] || vol[v] == 0.0;
-    if (dens32) dens32[v] = zero ? 0.f : (float)((double)(w[v] * factor) / vol[v]);
+    if (dens32) dens32[v] = dtfe::density_from_fixed(fixed[v], unit[v], w[v], factor, hull[v] != 0);
     if (dens64) dens64[v] = zero ? 0.0 : (double)w[v] * 4.0 / ((double)rb * vol[v]);
     if (volsum_out) volsum_out[v] = vol[v];
   }

@@ -3,7 +3,8 @@
 Bars:
   * point location: bit-exact tetrahedron ids (canonical tie rule);
   * vertex densities: bit-identical to the oracle's mode-"ref" values (both
-    sum the FP64 volumes of a vertex in ascending tetrahedron order);
+    add a vertex's FP64 volumes as exact integers in units of its sub-box,
+    fixed_volume.cuh);
   * interpolated fields vs the oracle in the reference's arithmetic (mode ref):
     relative error <= 1e-6;
   * interpolated fields vs the FP64 oracle: relative error <= 1e-5 (the

@@ -185,6 +185,19 @@ def profile_traffic():
         return None
 
 
+def workload_config(args, plan, world: int) -> dict:
+    """The workload block of the JSON line, the same for both arms."""
+    return {"workload": f"zeldovich{args.n}: {args.n}^3 Zel'dovich particles (rms 1.0 spacing, "
+                        f"periodic 100 Mpc/h, padding 5) -> {args.n}^3 grid, cell-centre "
+                        "density+velocity+gradient+div/shear/vort"
+                        + (f" + {args.scalars} N(0,1) scalars and their gradients" if args.scalars else "")
+                        + " per step, vertex densities included",
+            "grid": list(plan.grid), "particles": args.n ** 3, "vertices": plan.n_verts,
+            "tetrahedra": plan.n_tets, "subboxes": plan.n_boxes,
+            "l2": "inputs larger than L2 (tessellation arrays > 126 MB)",
+            "parallelism": f"dp{world} (independent boxes per GPU)"}
+
+
 def reference_code_step(plan, threads: int):
     """The reference's own code on the host cores, when the harness built
     from its sources is present (oracle/_ref): per sub-box, one host thread
@@ -821,9 +834,7 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": f"zeldovich{args.n}: {args.n}^3 particles -> {args.n}^3 grid, cell-centre "
-                               "density+velocity+gradient+div/shear/vort", "grid": [args.n] * 3,
-                   "particles": args.n ** 3},
+        "config": workload_config(args, plan, 1),
         "cpu_baseline": {"value": value, "unit": "grid samples/s", "cores": cores, "kind": kind,
                          "sample": sample},
         "e2e": {"value": value, "unit": "grid samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -1209,15 +1220,7 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": "grid samples/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"zeldovich{args.n}: {args.n}^3 Zel'dovich particles (rms 1.0 spacing, "
-                               f"periodic 100 Mpc/h, padding 5) -> {args.n}^3 grid, cell-centre "
-                               "density+velocity+gradient+div/shear/vort"
-                               + (f" + {args.scalars} N(0,1) scalars and their gradients" if args.scalars else "")
-                               + " per step, vertex densities included",
-                   "grid": list(plan.grid), "particles": args.n ** 3, "vertices": plan.n_verts,
-                   "tetrahedra": plan.n_tets, "subboxes": plan.n_boxes,
-                   "l2": "inputs larger than L2 (tessellation arrays > 126 MB)",
-                   "parallelism": f"dp{world} (independent boxes per GPU)"},
+        "config": workload_config(args, plan, world),
         # per step: volumes + seeds, vertex densities, the walk and evaluation
         # (one fused kernel or two), the outside-pencil pass
         "gpu_launches": (4 if variants[0] >= 9 else 5) * args.steps,

@@ -483,11 +483,18 @@ def backward_leg(args, local: int, threads: int) -> dict:
             "vertices": V, "tetrahedra": plan.n_tets, "host_plan_s": t_plan}
 
 
-def compare_leg(args, plan, local: int, threads: int) -> dict:
+def compare_leg(args, plan, local: int, threads: int, cpu: bool = False) -> dict:
     """The comparison estimators on the main workload, device-timed: SPH with
     32 neighbours on the same padded sub-box particle sets and grid tiles,
     CIC and TSC deposition (their own paddings, the reference's sub-box
-    split) of density and velocity."""
+    split) of density and velocity.  With cpu (and the reference harness
+    built), each also times the reference's own implementation on a sample
+    of the same sub-boxes, one per host thread."""
+    ref = None
+    if cpu:
+        import refharness as R
+        ref = R if R.available() else None
+    hthreads = host_threads(args.threads)
     import torch
     from dtfe_b200 import plan as P
     from dtfe_b200 import synthetic as S
@@ -507,6 +514,11 @@ def compare_leg(args, plan, local: int, threads: int) -> dict:
     t = _events(stream, sph, 2)
     res["SPH32"] = {"ms": 1e3 * t, "grid_samples_per_s": G / t}
     dev.close()
+    if ref is not None:
+        rate, m = ref.time_sph_boxes(plan, hthreads, 32)
+        res["SPH32"]["reference_cpu"] = {"grid_samples_per_s": rate, "boxes_sampled": m, "cores": min(m, hthreads),
+                                         "kind": "reference", "sample": f"{m} of {plan.n_boxes} padded sub-boxes, "
+                                                                         "one per host thread, density + velocity"}
     n = args.n
     pos, psi = S.zeldovich_lattice(n, S.BOX, 1.0, seed=1)
     rng = np.random.default_rng(2)
@@ -529,10 +541,29 @@ def compare_leg(args, plan, local: int, threads: int) -> dict:
             dd.deposit_dev(dp, d, v)
         dep()
         t = _events(ds, dep, 3)
-        res[kind] = {"ms": 1e3 * t, "grid_samples_per_s": G / t, "particle_copies": dp.n,
-                     "h2d_bytes": int(dp.pos.nbytes + dp.weight.nbytes + dp.velocity.nbytes),
-                     "note": "includes the host->device copy of the particles from pinned memory (host-input API)"}
+        # the same deposit with the particles already resident on the device
+        pd, wd, vd = (torch.from_numpy(a).to(cuda) for a in (dp.pos, dp.weight, dp.velocity))
+        torch.cuda.synchronize()
+
+        def dep_resident():
+            dd.deposit_resident(dp, pd, wd, vd, d, v)
+        dep_resident()
+        tr = _events(ds, dep_resident, 3)
+        res[kind] = {"ms": 1e3 * tr, "grid_samples_per_s": G / tr, "particle_copies": dp.n,
+                     "particles_per_s": dp.n / tr,
+                     "note": "particles resident on the device (dtfe_gpu_deposit_resident)",
+                     "host_input": {"ms": 1e3 * t, "grid_samples_per_s": G / t,
+                                    "h2d_bytes": int(dp.pos.nbytes + dp.weight.nbytes + dp.velocity.nbytes),
+                                    "note": "dtfe_gpu_deposit_dev: includes the host->device copy of the "
+                                            "particles from pinned memory"}}
+        del pd, wd, vd
         dd.close()
+        if ref is not None:
+            rate, m, npart = ref.time_deposit_boxes(dp, hthreads)
+            res[kind]["reference_cpu"] = {"grid_samples_per_s": rate, "boxes_sampled": m, "cores": min(m, hthreads),
+                                          "kind": "reference",
+                                          "sample": f"{m} of {len(dp.boxes)} sub-box regions ({npart} particles), "
+                                                    "one per host thread, density + velocity"}
     return res
 
 
@@ -1192,7 +1223,7 @@ def run_ours(args):
 
     compare = None
     if side and not args.no_compare:
-        compare = compare_leg(args, plan, local, threads)
+        compare = compare_leg(args, plan, local, threads, rank == 0 and world == 1 and not args.no_cpu)
 
     batch = None
     if side and not args.no_batch:

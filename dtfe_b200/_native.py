@@ -207,6 +207,8 @@ def gpu() -> C.CDLL:
         lib.dtfe_gpu_deposit.argtypes = [H, C.c_int32, vp, vp, vp, C.c_int64, C.c_int32, vp, vp, C.c_double, vp, vp]
         lib.dtfe_gpu_deposit_dev.argtypes = [H, C.c_int32, vp, vp, vp, C.c_int64, C.c_int32, vp, vp, C.c_double,
                                              vp, vp]
+        lib.dtfe_gpu_deposit_resident.argtypes = [H, C.c_int32, vp, vp, vp, C.c_int64, C.c_int32, vp, vp,
+                                                  C.c_double, vp, vp]
         lib.dtfe_gpu_graph_build.argtypes = [H, C.c_double, C.POINTER(InterpOpts), C.POINTER(vp)]
         lib.dtfe_gpu_graph_launch.argtypes = [H]
         lib.dtfe_gpu_read_status.argtypes = [H, C.POINTER(Status)]

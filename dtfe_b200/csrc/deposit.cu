@@ -10,10 +10,12 @@
 // The contributions are accumulated in 64-bit fixed point: every sum is exact,
 // so the grid is deterministic and independent of the order in which threads
 // add.  The fixed-point scales are powers of two chosen from the total |mass|
-// and |momentum| so that no cell can overflow.  A block of 256 particles
-// (Morton-ordered within its sub-box) whose stencils fit an 8x8x8 cell tile
-// accumulates in shared memory first and flushes each touched cell with one
-// global atomic per component; other blocks add to global memory directly.
+// and |momentum| so that no cell can overflow.  A block of 512 particles
+// (Morton-ordered within its sub-box) whose stencils fit a tile of at most
+// 2048 cells accumulates in shared memory first and flushes each touched cell
+// with one global atomic per component; other blocks add to global memory
+// directly.  The global sums of one cell (mass and the three momenta) share
+// one 32-byte sector.
 
 #include <cuda_runtime.h>
 
@@ -29,8 +31,9 @@ extern "C" int dtfe_internal_set_error(int code, const char* msg);
 namespace {
 
 constexpr int kDepBlock = 256;
-constexpr int kTile = 8;  // shared tile edge in cells
-constexpr int kTileCells = kTile * kTile * kTile;
+constexpr int kDepPPT = 2;                          // particles per thread
+constexpr int kDepChunk = kDepBlock * kDepPPT;      // consecutive particles per block
+constexpr int kTileCap = 2048;                      // cells of a block's shared tile
 
 struct DepBox {
   int64_t off, n;         // particle range
@@ -61,8 +64,7 @@ struct DepParams {
   int64_t n;
   int64_t G1, G2;
   const double* scales;   // device: fixed-point scales of mass and momentum, then their inverses
-  unsigned long long* acc_m;  // per cell
-  unsigned long long* acc_p;  // 3 per cell (null: no velocity)
+  unsigned long long* acc;    // per grid cell: mass, then (with velocity) px, py, pz
 };
 
 __device__ __forceinline__ int find_dep_box(const int64_t* __restrict__ prefix, int K, int64_t s) {
@@ -133,127 +135,197 @@ __device__ __forceinline__ unsigned long long to_fixed(float v, double scale) {
   return (unsigned long long)llrint((double)v * scale);
 }
 
-// KIND: 0 NGP, 1 CIC, 2 TSC.
-template <int KIND>
-__global__ void __launch_bounds__(kDepBlock) k_deposit(DepParams P) {
-  __shared__ unsigned long long s_m[kTileCells];
-  __shared__ unsigned long long s_p[3][kTileCells];
-  __shared__ int s_box, s_lo[3], s_hi[3], s_ok;
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const bool valid = i < P.n;
-  const bool with_vel = P.acc_p != nullptr;
-  const double scale_m = __ldg(&P.scales[0]), scale_p = __ldg(&P.scales[1]);
-
-  int b = 0;
+// One particle's stencil: per axis up to three region-local cells and their
+// weights.  CIC's interior stencil spans three cells of which one always has
+// weight 0 (the reference loops over all three); that cell is dropped, which
+// changes no sum and keeps the block's tile tight.
+struct Stencil {
   int cell[3][3];
   float w[3][3];
-  int count[3] = {0, 0, 0};
-  float wt = 0.f, v[3] = {0.f, 0.f, 0.f};
-  if (valid) {
-    b = find_dep_box(P.prefix, P.K, i);
-    const DepBox& B = P.boxes[b];
-    float4 q = __ldg(&P.pw[i]);
-    const float p[3] = {q.x, q.y, q.z};
-    wt = q.w;
-    if (with_vel && P.vel) {
-      float4 u = __ldg(&P.vel[i]);
-      v[0] = u.x; v[1] = u.y; v[2] = u.z;
+  int count[3];
+};
+
+template <class T>
+__device__ __forceinline__ T pick3(const T (&a)[3], int i) {
+  return i == 0 ? a[0] : (i == 1 ? a[1] : a[2]);
+}
+
+template <int KIND>
+__device__ __forceinline__ bool particle_stencil(const DepBox& B, const float p[3], Stencil& S) {
+  S.count[0] = S.count[1] = S.count[2] = 0;
+  if (KIND == 0) {
+    bool ok = true;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      S.cell[j][0] = (int)floorf((p[j] - B.lo[j]) / B.dx[j]);
+      S.w[j][0] = 1.f;
+      ok = ok && S.cell[j][0] >= 0 && S.cell[j][0] < B.dims[j];
     }
-    if (KIND == 0) {
-      bool ok = true;
+    if (ok) S.count[0] = S.count[1] = S.count[2] = 1;
+  } else {
+    const bool inner = in_box(p, B.inner);
+    if (inner || in_box(p, B.outer)) {
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
-        cell[j][0] = (int)floorf((p[j] - B.lo[j]) / B.dx[j]);
-        w[j][0] = 1.f;
-        ok = ok && cell[j][0] >= 0 && cell[j][0] < B.dims[j];
-      }
-      if (ok) count[0] = count[1] = count[2] = 1;
-    } else {
-      const bool inner = in_box(p, B.inner);
-      if (inner || in_box(p, B.outer)) {
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          float temp = (p[j] - B.lo[j]) / B.dx[j];
-          axis_stencil<KIND>(inner, temp, B.dims[j], cell[j], w[j], count[j]);
+        float temp = (p[j] - B.lo[j]) / B.dx[j];
+        axis_stencil<KIND>(inner, temp, B.dims[j], S.cell[j], S.w[j], S.count[j]);
+        if (KIND == 1 && S.count[j] == 3) {
+          if (S.w[j][2] == 0.f) S.count[j] = 2;
+          else if (S.w[j][0] == 0.f) {
+            S.cell[j][0] = S.cell[j][1]; S.w[j][0] = S.w[j][1];
+            S.cell[j][1] = S.cell[j][2]; S.w[j][1] = S.w[j][2];
+            S.count[j] = 2;
+          }
         }
       }
     }
   }
-  const bool any = count[0] > 0 && count[1] > 0 && count[2] > 0;
+  return S.count[0] > 0 && S.count[1] > 0 && S.count[2] > 0;
+}
 
-  // Does the whole block fit one shared tile of one sub-box?
+// KIND: 0 NGP, 1 CIC, 2 TSC; VEL: momentum accumulated beside the mass.
+// A block takes kDepChunk consecutive particles (Morton-ordered within their
+// sub-box).  When they all belong to one sub-box and their stencils fit a
+// tile of at most kTileCap cells, the block adds into that tile in shared
+// memory and flushes each touched cell with one global atomic per component;
+// otherwise every contribution goes to global memory directly.  Contributions
+// that round to 0 in fixed point are not added at all.
+template <int KIND, bool VEL>
+__global__ void __launch_bounds__(kDepBlock, 3) k_deposit(DepParams P) {
+  extern __shared__ unsigned long long s_acc[];  // [component][kTileCap]
+  __shared__ int s_box, s_ok, s_lo[3], s_hi[3];
+  constexpr int C = VEL ? 4 : 1;
+  // stencil points per axis (CIC: two, once its zero-weight cell is dropped)
+  constexpr int M = KIND == 0 ? 1 : (KIND == 1 ? 2 : 3);
+  constexpr int M3 = M * M * M;
+  const int rot = (threadIdx.x & 31) % M3;
+  const int64_t base = (int64_t)blockIdx.x * kDepChunk;
+  const int64_t end = min(base + (int64_t)kDepChunk, P.n);
+  const double scale_m = __ldg(&P.scales[0]), scale_p = __ldg(&P.scales[1]);
   if (threadIdx.x == 0) {
-    s_box = valid ? b : -1;
-    s_ok = 1;
+    const int b = find_dep_box(P.prefix, P.K, base);
+    s_box = b;
+    s_ok = __ldg(&P.prefix[b + 1]) >= end;
     for (int c = 0; c < 3; ++c) { s_lo[c] = 0x7FFFFFFF; s_hi[c] = -0x7FFFFFFF; }
   }
+  float4 q[kDepPPT], u[kDepPPT];
+#pragma unroll
+  for (int r = 0; r < kDepPPT; ++r) {
+    const int64_t i = base + r * kDepBlock + threadIdx.x;
+    q[r] = i < end ? __ldg(&P.pw[i]) : make_float4(0.f, 0.f, 0.f, 0.f);
+    u[r] = (VEL && P.vel && i < end) ? __ldg(&P.vel[i]) : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
   __syncthreads();
-  if (valid && b != s_box) s_ok = 0;
-  if (any) {
+  const bool one_box = s_ok;
+
+  // the block's cell bounds (single-box blocks only)
+  if (one_box) {
+    const DepBox& B = P.boxes[s_box];
+    int lo[3] = {0x7FFFFFFF, 0x7FFFFFFF, 0x7FFFFFFF}, hi[3] = {-0x7FFFFFFF, -0x7FFFFFFF, -0x7FFFFFFF};
+#pragma unroll
+    for (int r = 0; r < kDepPPT; ++r) {
+      const int64_t i = base + r * kDepBlock + threadIdx.x;
+      Stencil S;
+      const float p[3] = {q[r].x, q[r].y, q[r].z};
+      if (i < end && particle_stencil<KIND>(B, p, S)) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          lo[c] = min(lo[c], S.cell[c][0]);
+          hi[c] = max(hi[c], S.count[c] == 1 ? S.cell[c][0] : S.count[c] == 2 ? S.cell[c][1] : S.cell[c][2]);
+        }
+      }
+    }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      atomicMin(&s_lo[c], cell[c][0]);
-      atomicMax(&s_hi[c], cell[c][count[c] - 1]);
+      lo[c] = __reduce_min_sync(0xffffffffu, lo[c]);
+      hi[c] = __reduce_max_sync(0xffffffffu, hi[c]);
+    }
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        atomicMin(&s_lo[c], lo[c]);
+        atomicMax(&s_hi[c], hi[c]);
+      }
     }
   }
   __syncthreads();
-  bool staged = s_ok && s_box >= 0;
-  int tlo[3] = {s_lo[0], s_lo[1], s_lo[2]};
-#pragma unroll
-  for (int c = 0; c < 3; ++c) staged = staged && s_hi[c] >= s_lo[c] && s_hi[c] - s_lo[c] < kTile;
+  const int tlo[3] = {s_lo[0], s_lo[1], s_lo[2]};
+  bool staged = one_box && s_hi[0] >= tlo[0] && s_hi[1] >= tlo[1] && s_hi[2] >= tlo[2];
+  int sy = 1, sz = 1;
+  int64_t cells = 0;
   if (staged) {
-    for (int k = threadIdx.x; k < kTileCells; k += blockDim.x) {
-      s_m[k] = 0ull;
-      s_p[0][k] = s_p[1][k] = s_p[2][k] = 0ull;
-    }
+    sy = s_hi[1] - tlo[1] + 1;
+    sz = s_hi[2] - tlo[2] + 1;
+    cells = (int64_t)(s_hi[0] - tlo[0] + 1) * sy * sz;
+    staged = cells <= kTileCap;
+  }
+  if (staged) {
+    for (int k = threadIdx.x; k < C * kTileCap; k += kDepBlock) s_acc[k] = 0ull;
     __syncthreads();
   }
 
-  if (any) {
+#pragma unroll
+  for (int r = 0; r < kDepPPT; ++r) {
+    const int64_t i = base + r * kDepBlock + threadIdx.x;
+    if (i >= end) continue;
+    const int b = one_box ? s_box : find_dep_box(P.prefix, P.K, i);
     const DepBox& B = P.boxes[b];
-    for (int a = 0; a < count[0]; ++a)
-      for (int bb = 0; bb < count[1]; ++bb)
-        for (int c = 0; c < count[2]; ++c) {
-          const float result = wt * w[0][a] * w[1][bb] * w[2][c];
-          const unsigned long long fm = to_fixed(result, scale_m);
-          unsigned long long fp[3];
-          if (with_vel) {
+    const float p[3] = {q[r].x, q[r].y, q[r].z};
+    const float wt = q[r].w, v[3] = {u[r].x, u[r].y, u[r].z};
+    Stencil S;
+    if (!particle_stencil<KIND>(B, p, S)) continue;
+    // The stencil's M^3 corners in an order rotated by the lane: neighbouring
+    // particles of a warp share cells, and at one step of the loop the lanes
+    // then mostly add to different cells instead of queueing on the same
+    // shared word.  Fixed trip counts with guards and selects (not indexed
+    // arrays) keep the stencil in registers.
 #pragma unroll
-            for (int q = 0; q < 3; ++q) fp[q] = to_fixed(v[q] * result, scale_p);
-          }
-          if (staged) {
-            const int k = ((cell[0][a] - tlo[0]) * kTile + (cell[1][bb] - tlo[1])) * kTile + (cell[2][c] - tlo[2]);
-            atomicAdd(&s_m[k], fm);
-            if (with_vel) {
+    for (int s = 0; s < M3; ++s) {
+      int qc = rot + s;
+      if (qc >= M3) qc -= M3;
+      const int a = qc / (M * M), bb = (qc / M) % M, c = qc % M;
+      if (a >= S.count[0] || bb >= S.count[1] || c >= S.count[2]) continue;
+      const float result = wt * pick3(S.w[0], a) * pick3(S.w[1], bb) * pick3(S.w[2], c);
+      unsigned long long f[C];
+      f[0] = to_fixed(result, scale_m);
+      unsigned long long nz = f[0];
+      if (VEL) {
 #pragma unroll
-              for (int q = 0; q < 3; ++q) atomicAdd(&s_p[q][k], fp[q]);
-            }
-          } else {
-            const int64_t idx = ((int64_t)(B.origin[0] + cell[0][a]) * P.G1 + (B.origin[1] + cell[1][bb])) * P.G2 +
-                                (B.origin[2] + cell[2][c]);
-            atomicAdd(&P.acc_m[idx], fm);
-            if (with_vel) {
-#pragma unroll
-              for (int q = 0; q < 3; ++q) atomicAdd(&P.acc_p[3 * idx + q], fp[q]);
-            }
-          }
+        for (int k = 1; k < C; ++k) {
+          f[k] = to_fixed(v[k - 1] * result, scale_p);
+          nz |= f[k];
         }
+      }
+      if (nz == 0ull) continue;
+      const int c0 = pick3(S.cell[0], a), c1 = pick3(S.cell[1], bb), c2 = pick3(S.cell[2], c);
+      if (staged) {
+        const int k = ((c0 - tlo[0]) * sy + (c1 - tlo[1])) * sz + (c2 - tlo[2]);
+#pragma unroll
+        for (int m = 0; m < C; ++m) atomicAdd(&s_acc[m * kTileCap + k], f[m]);
+      } else {
+        const int64_t idx = ((int64_t)(B.origin[0] + c0) * P.G1 + (B.origin[1] + c1)) * P.G2 + (B.origin[2] + c2);
+#pragma unroll
+        for (int m = 0; m < C; ++m) atomicAdd(&P.acc[C * idx + m], f[m]);
+      }
+    }
   }
   if (staged) {
     __syncthreads();
     const DepBox& B = P.boxes[s_box];
-    for (int k = threadIdx.x; k < kTileCells; k += blockDim.x) {
-      const int ci = k / (kTile * kTile), cj = (k / kTile) % kTile, ck = k % kTile;
-      const int gi = tlo[0] + ci, gj = tlo[1] + cj, gk = tlo[2] + ck;
-      if (gi >= B.dims[0] || gj >= B.dims[1] || gk >= B.dims[2]) continue;
-      const bool touched = s_m[k] != 0ull || (with_vel && (s_p[0][k] | s_p[1][k] | s_p[2][k]) != 0ull);
-      if (!touched) continue;
-      const int64_t idx = ((int64_t)(B.origin[0] + gi) * P.G1 + (B.origin[1] + gj)) * P.G2 + (B.origin[2] + gk);
-      atomicAdd(&P.acc_m[idx], s_m[k]);
-      if (with_vel) {
+    const int syz = sy * sz;
+    for (int k = threadIdx.x; k < (int)cells; k += kDepBlock) {
+      const int ci = k / syz, cj = (k - ci * syz) / sz, ck = k - ci * syz - cj * sz;
+      unsigned long long f[C], nz = 0ull;
 #pragma unroll
-        for (int q = 0; q < 3; ++q) atomicAdd(&P.acc_p[3 * idx + q], s_p[q][k]);
+      for (int m = 0; m < C; ++m) {
+        f[m] = s_acc[m * kTileCap + k];
+        nz |= f[m];
       }
+      if (nz == 0ull) continue;
+      const int64_t idx = ((int64_t)(B.origin[0] + tlo[0] + ci) * P.G1 + (B.origin[1] + tlo[1] + cj)) * P.G2 +
+                          (B.origin[2] + tlo[2] + ck);
+#pragma unroll
+      for (int m = 0; m < C; ++m) atomicAdd(&P.acc[C * idx + m], f[m]);
     }
   }
 }
@@ -263,9 +335,9 @@ __global__ void __launch_bounds__(kDepBlock) k_deposit(DepParams P) {
 // Box::volume() / rho_bar), Box::volume() being the hard-coded 35000^3.
 __global__ void k_deposit_finalize(int64_t n_tile_cells, const DepBox* __restrict__ boxes,
                                    const int64_t* __restrict__ tile_prefix, int K, int64_t G1, int64_t G2,
-                                   const unsigned long long* __restrict__ acc_m,
-                                   const unsigned long long* __restrict__ acc_p, const double* __restrict__ scales,
-                                   float* __restrict__ density, float* __restrict__ velocity) {
+                                   const unsigned long long* __restrict__ acc, int stride,
+                                   const double* __restrict__ scales, float* __restrict__ density,
+                                   float* __restrict__ velocity) {
   int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (s >= n_tile_cells) return;
   const int b = find_dep_box(tile_prefix, K, s);
@@ -276,11 +348,11 @@ __global__ void k_deposit_finalize(int64_t n_tile_cells, const DepBox* __restric
   const int i = (int)(local / ((int64_t)B.dims[2] * B.dims[1]));
   const int64_t idx = ((int64_t)(B.origin[0] + i) * G1 + (B.origin[1] + j)) * G2 + (B.origin[2] + k);
   const double inv_m = __ldg(&scales[2]), inv_p = __ldg(&scales[3]);
-  const float m = (float)((double)(long long)acc_m[idx] * inv_m);
+  const float m = (float)((double)(long long)acc[stride * idx] * inv_m);
   if (velocity) {
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
-      const float p = (float)((double)(long long)acc_p[3 * idx + q] * inv_p);
+      const float p = (float)((double)(long long)acc[stride * idx + 1 + q] * inv_p);
       velocity[3 * idx + q] = m != 0.f ? p / m : 0.f;
     }
   }
@@ -423,14 +495,28 @@ __global__ void k_pack4(int64_t n, const float* __restrict__ a3, const float* __
   if (i < n) out[i] = make_float4(a3[3 * i], a3[3 * i + 1], a3[3 * i + 2], b1 ? b1[i] : 1.f);
 }
 
-}  // namespace
-
 extern "C" size_t dtfe_internal_deposit_saved_size() { return sizeof(DepSaved); }
 
+template <int KIND>
+void launch_deposit(bool with_vel, unsigned nb, cudaStream_t st, const DepParams& P) {
+  if (with_vel) {
+    const int smem = 4 * kTileCap * (int)sizeof(unsigned long long);
+    cudaFuncSetAttribute(k_deposit<KIND, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k_deposit<KIND, true><<<nb, kDepBlock, smem, st>>>(P);
+  } else {
+    k_deposit<KIND, false><<<nb, kDepBlock, kTileCap * sizeof(unsigned long long), st>>>(P);
+  }
+}
+
+}  // namespace
+
+// inputs_dev: xyz, w and vel are device pointers (else host pointers, copied
+// on the stream).
 extern "C" int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xyz, const float* w, const float* vel,
                                      int64_t n, int32_t n_boxes, const dtfe_deposit_box* boxes,
                                      const int32_t grid[3], double average_density, float* density_dev,
-                                     float* velocity_dev, void** scratch, size_t* scratch_bytes, void* saved) {
+                                     float* velocity_dev, void** scratch, size_t* scratch_bytes, void* saved,
+                                     int inputs_dev) {
   if (kind < 0 || kind > 2) return dtfe_internal_set_error(DTFE_ERR_ARG, "deposit kind must be 0 (NGP), 1 (CIC), 2 (TSC)");
   if (n < 0 || n_boxes <= 0 || !boxes || !grid) return dtfe_internal_set_error(DTFE_ERR_ARG, "bad deposit arguments");
   if (!(average_density > 0.0)) return dtfe_internal_set_error(DTFE_ERR_ARG, "averageDensity must be positive");
@@ -473,11 +559,12 @@ extern "C" int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xy
     tprefix[b + 1] = tprefix[b] + cells;
     B.factor = (float)cells / vol / (float)average_density;
   }
-  // scratch: particles (2 float4), boxes, prefix, accumulators (4 per cell)
+  // scratch: particles (2 float4), boxes, prefix, accumulators (1 or 4 per cell)
+  const int comps = velocity_dev ? 4 : 1;
   const size_t bytes_part = sizeof(float4) * 2 * (size_t)n;
   const size_t bytes_box = sizeof(DepBox) * n_boxes + 2 * sizeof(int64_t) * (n_boxes + 1);
   const size_t bytes_acc = sizeof(unsigned long long) * 4 * (size_t)G;
-  const size_t bytes_tmp = sizeof(float) * 4 * (size_t)n;  // 3-float records as they arrive
+  const size_t bytes_tmp = sizeof(float) * 4 * (size_t)n;  // host inputs: 3-float records as they arrive
   const size_t need = bytes_part + bytes_box + bytes_acc + bytes_tmp + 4096;
   if (*scratch_bytes < need) {
     if (*scratch) cudaFree(*scratch);
@@ -491,8 +578,7 @@ extern "C" int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xy
   float4* d_pw = (float4*)base;
   float4* d_vel = d_pw + n;
   size_t o = align(bytes_part);
-  unsigned long long* acc_m = (unsigned long long*)(base + o);
-  unsigned long long* acc_p = acc_m + G;
+  unsigned long long* acc = (unsigned long long*)(base + o);
   o = align(o + bytes_acc);
   DepBox* d_boxes = (DepBox*)(base + o);
   int64_t* d_prefix = (int64_t*)(base + o + sizeof(DepBox) * n_boxes);
@@ -501,7 +587,10 @@ extern "C" int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xy
   double* d_scales = (double*)(base + align(align(o + bytes_box) + bytes_tmp));
   unsigned* d_maxbits = (unsigned*)(d_scales + 4);
   cudaError_t e;
-  if (n > 0) {
+  if (n > 0 && inputs_dev) {
+    k_pack4<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, xyz, w, d_pw);
+    if (vel) k_pack4<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, vel, nullptr, d_vel);
+  } else if (n > 0) {
     float* t3 = tmp;
     float* t1 = tmp + 3 * n;
     cudaMemcpyAsync(t3, xyz, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, st);
@@ -515,7 +604,7 @@ extern "C" int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xy
   cudaMemcpyAsync(d_boxes, hb.data(), sizeof(DepBox) * n_boxes, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(d_prefix, prefix.data(), sizeof(int64_t) * (n_boxes + 1), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(d_tprefix, tprefix.data(), sizeof(int64_t) * (n_boxes + 1), cudaMemcpyHostToDevice, st);
-  cudaMemsetAsync(acc_m, 0, bytes_acc, st);
+  cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * comps * (size_t)G, st);
   DepParams P;
   P.pw = d_pw;
   P.vel = vel ? d_vel : nullptr;
@@ -532,18 +621,17 @@ extern "C" int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xy
                                                                                           d_maxbits);
   k_deposit_scales<<<1, 32, 0, st>>>(n, d_maxbits, d_scales);
   P.scales = d_scales;
-  P.acc_m = acc_m;
-  P.acc_p = velocity_dev ? acc_p : nullptr;
+  P.acc = acc;
   if (n > 0) {
-    const unsigned nb = (unsigned)((n + kDepBlock - 1) / kDepBlock);
-    if (kind == 0) k_deposit<0><<<nb, kDepBlock, 0, st>>>(P);
-    else if (kind == 1) k_deposit<1><<<nb, kDepBlock, 0, st>>>(P);
-    else k_deposit<2><<<nb, kDepBlock, 0, st>>>(P);
+    const unsigned nb = (unsigned)((n + kDepChunk - 1) / kDepChunk);
+    if (kind == 0) launch_deposit<0>(velocity_dev != nullptr, nb, st, P);
+    else if (kind == 1) launch_deposit<1>(velocity_dev != nullptr, nb, st, P);
+    else launch_deposit<2>(velocity_dev != nullptr, nb, st, P);
   }
   const int64_t nt = tprefix[n_boxes];
   if (nt > 0)
     k_deposit_finalize<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(nt, d_boxes, d_tprefix, n_boxes, grid[1], grid[2],
-                                                                     acc_m, acc_p, d_scales,
+                                                                     acc, comps, d_scales,
                                                                      density_dev, velocity_dev);
   if ((e = cudaGetLastError()) != cudaSuccess) return dtfe_internal_set_error(DTFE_ERR_CUDA, cudaGetErrorString(e));
   // state for dtfe_gpu_deposit_adjoint (the scratch keeps particles and boxes)

@@ -308,17 +308,20 @@ __global__ void __launch_bounds__(kPackBlock)
 __device__ __forceinline__ bool holds(const int4& u, int v) { return u.x == v || u.y == v || u.z == v || u.w == v; }
 
 // Fallback for the faces k_neighbours_star left unset (kUnsetNeighbour):
-// across face (a, b, c) of t lies the other tetrahedron of a's incidence
-// list that holds b and c (-1 if none: the convex hull, CGAL's infinite
-// cell).  Any list order will do.
+// across face (a, b, c) of t lies the other tetrahedron of the list of the
+// face's smallest vertex that holds all three (-1 if none: the convex hull,
+// CGAL's infinite cell).  Any list order will do.  A tetrahedron holding the
+// face has its smallest vertex as its own smallest or second smallest, so
+// the star lists (k_fill_star) hold it.
 constexpr int kUnsetNeighbour = (int)0x80808080;  // the byte pattern 0x80 of a memset
 __device__ __forceinline__ int face_neighbour(int t, int a, int b, int c, const int64_t* __restrict__ off,
                                               const int* __restrict__ inc, const int4* __restrict__ tet_v) {
-  for (int64_t i = __ldg(&off[a]), e = __ldg(&off[a + 1]); i < e; ++i) {
+  const int m = min(a, min(b, c));
+  for (int64_t i = __ldg(&off[m]), e = __ldg(&off[m + 1]); i < e; ++i) {
     const int u = __ldg(&inc[i]);
     if (u == t) continue;
     const int4 q = __ldg(&tet_v[u]);
-    if (holds(q, b) && holds(q, c)) return u;
+    if (holds(q, a) && holds(q, b) && holds(q, c)) return u;
   }
   return -1;
 }
@@ -340,33 +343,45 @@ __global__ void k_derive_neighbours(int64_t T, const int4* __restrict__ tet_v, c
 }
 
 // Neighbours from the stars of the vertices: every face is settled at its
-// smallest vertex v, by the one warp that reads v's incidence list.  Each
-// tetrahedron around v contributes its faces through v whose other two
-// vertices are larger than v, keyed by those two vertices; the two entries
-// with the same key are the tetrahedra on either side (one entry alone: a
-// hull face, -1).  The entries of one vertex sit in the warp's shared table;
-// a vertex with more than kStarCap entries leaves its faces unset for
-// k_derive_neighbours.  Each incidence list is read once and each
-// tetrahedron's vertices four times, instead of two list merges per
-// tetrahedron.
-constexpr int kStarWarps = 8;
-constexpr int kStarCap = 256;
-__global__ void __launch_bounds__(32 * kStarWarps) k_neighbours_star(int64_t V, const int4* __restrict__ tet_v,
-                                                                    const int64_t* __restrict__ off,
-                                                                    const int* __restrict__ inc,
-                                                                    int* __restrict__ tet_n) {
-  __shared__ unsigned long long s_key[kStarWarps][kStarCap];
-  __shared__ int s_tet[kStarWarps][kStarCap];
-  __shared__ unsigned char s_face[kStarWarps][kStarCap];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  unsigned long long* key = s_key[w];
-  int* tet = s_tet[w];
-  unsigned char* face = s_face[w];
-  for (int64_t v = (int64_t)blockIdx.x * kStarWarps + w; v < V; v += (int64_t)gridDim.x * kStarWarps) {
+// smallest vertex v, by the one warp that reads v's star list (the
+// tetrahedra whose smallest or second smallest vertex is v, k_fill_star:
+// only these have a face whose smallest vertex is v).  Each listed
+// tetrahedron contributes its faces through v whose other two vertices are
+// larger than v, keyed by those two vertices; the two entries with the same
+// key are the tetrahedra on either side (one entry alone: a hull face, -1).
+// The entries of one vertex sit in its group's shared table.  A first pass
+// gives each vertex a group of 8 lanes (four vertices' dependent loads --
+// list offsets, list, tetrahedra -- in flight per warp) and a table of 96
+// entries; the few vertices with more (about 0.1% of a Zel'dovich
+// tessellation) are listed and settled by a second pass with a warp and 768
+// entries each; faces of larger stars stay unset for k_derive_neighbours.
+// Each tetrahedron's vertices are read twice.
+//   FROM_LIST = false: every vertex v < V; stars above CAP are appended to
+//                      list (count in *n_list, at most list_cap kept).
+//   FROM_LIST = true:  the listed vertices.
+template <int THREADS, int LANES, int CAP, bool FROM_LIST>
+__global__ void __launch_bounds__(THREADS) k_neighbours_star(int64_t V, const int4* __restrict__ tet_v,
+                                                            const int64_t* __restrict__ off,
+                                                            const int* __restrict__ inc, int* __restrict__ tet_n,
+                                                            int* __restrict__ list, unsigned* __restrict__ n_list,
+                                                            unsigned list_cap) {
+  constexpr int kGroups = THREADS / LANES;
+  __shared__ unsigned long long s_key[kGroups][CAP];
+  __shared__ int s_tet[kGroups][CAP];
+  __shared__ unsigned char s_face[kGroups][CAP];
+  const int g = threadIdx.x / LANES, gl = threadIdx.x % LANES;
+  const unsigned gmask = LANES == 32 ? 0xffffffffu
+                                     : ((1u << (LANES & 31)) - 1u) << ((threadIdx.x & 31) & ~(LANES - 1));
+  unsigned long long* key = s_key[g];
+  int* tet = s_tet[g];
+  unsigned char* face = s_face[g];
+  const int64_t n_items = FROM_LIST ? (int64_t)min(*n_list, list_cap) : V;
+  for (int64_t it = (int64_t)blockIdx.x * kGroups + g; it < n_items; it += (int64_t)gridDim.x * kGroups) {
+    const int64_t v = FROM_LIST ? (int64_t)__ldg(&list[it]) : it;
     const int64_t a = __ldg(&off[v]), e = __ldg(&off[v + 1]);
-    int n = 0;  // entries so far (warp-uniform)
-    for (int64_t base = a; base < e; base += 32) {
-      const int64_t q = base + lane;
+    int n = 0;  // entries so far (uniform in the group)
+    for (int64_t base = a; base < e; base += LANES) {
+      const int64_t q = base + gl;
       int cnt = 0, u = -1;
       unsigned long long k3[3];
       int f3[3];
@@ -386,31 +401,39 @@ __global__ void __launch_bounds__(32 * kStarWarps) k_neighbours_star(int64_t V, 
             }
           if (x > (int)v && y > (int)v) {
             const unsigned lo = (unsigned)min(x, y), hi = (unsigned)max(x, y);
-            k3[cnt] = ((unsigned long long)lo << 32) | hi;
-            f3[cnt] = k;
+            const unsigned long long kk = ((unsigned long long)lo << 32) | hi;
+            // constant indices keep k3 / f3 in registers
+            if (cnt == 0) { k3[0] = kk; f3[0] = k; }
+            else if (cnt == 1) { k3[1] = kk; f3[1] = k; }
+            else { k3[2] = kk; f3[2] = k; }
             ++cnt;
           }
         }
       }
       int incl = cnt;
 #pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, incl, d);
-        if (lane >= d) incl += y;
+      for (int d = 1; d < LANES; d <<= 1) {
+        const int y = __shfl_up_sync(gmask, incl, d, LANES);
+        if (gl >= d) incl += y;
       }
       const int pos = n + incl - cnt;
 #pragma unroll
       for (int c = 0; c < 3; ++c)
-        if (c < cnt && pos + c < kStarCap) {
+        if (c < cnt && pos + c < CAP) {
           key[pos + c] = k3[c];
           tet[pos + c] = u;
           face[pos + c] = (unsigned char)f3[c];
         }
-      n += __shfl_sync(0xffffffffu, incl, 31);
+      n += __shfl_sync(gmask, incl, LANES - 1, LANES);
     }
-    __syncwarp();
-    if (n <= kStarCap) {
-      for (int j = lane; j < n; j += 32) {
+    __syncwarp(gmask);
+    if (n > CAP) {
+      if (!FROM_LIST && gl == 0) {
+        const unsigned slot = atomicAdd(n_list, 1u);
+        if (slot < list_cap) list[slot] = (int)v;
+      }
+    } else {
+      for (int j = gl; j < n; j += LANES) {
         const unsigned long long kj = key[j];
         int partner = -1;
         for (int i = 0; i < n; ++i)
@@ -421,8 +444,35 @@ __global__ void __launch_bounds__(32 * kStarWarps) k_neighbours_star(int64_t V, 
         tet_n[4 * (int64_t)tet[j] + face[j]] = partner;
       }
     }
-    __syncwarp();
+    __syncwarp(gmask);
   }
+}
+
+// The two smallest of a tetrahedron's four vertex ids (a < b).
+__device__ __forceinline__ void two_smallest(const int4& q, int& a, int& b) {
+  const int lo1 = min(q.x, q.y), hi1 = max(q.x, q.y), lo2 = min(q.z, q.w), hi2 = max(q.z, q.w);
+  a = min(lo1, lo2);
+  b = min(max(lo1, lo2), min(hi1, hi2));
+}
+
+// Star lists: each tetrahedron at its smallest and second smallest vertex.
+__global__ void k_degree_star(int64_t T, const int4* __restrict__ tet_v, int* __restrict__ deg) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= T) return;
+  int a, b;
+  two_smallest(__ldg(&tet_v[t]), a, b);
+  atomicAdd(&deg[a], 1);
+  atomicAdd(&deg[b], 1);
+}
+
+__global__ void k_fill_star(int64_t T, const int4* __restrict__ tet_v, const int64_t* __restrict__ off,
+                            int* __restrict__ cursor, int* __restrict__ inc) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= T) return;
+  int a, b;
+  two_smallest(__ldg(&tet_v[t]), a, b);
+  inc[__ldg(&off[a]) + atomicAdd(&cursor[a], 1)] = (int)t;
+  inc[__ldg(&off[b]) + atomicAdd(&cursor[b], 1)] = (int)t;
 }
 
 __global__ void k_degree(int64_t T, const int4* __restrict__ tet_v, int* __restrict__ deg) {
@@ -724,40 +774,75 @@ __global__ void __launch_bounds__(kDensBlock) k_vertex_density(
   posd[i].w = density_from_fixed(__ldg(&acc[i]), __ldg(&scale[b].unit), __ldg(&w[i]), factor, __ldg(&hull[i]) != 0);
 }
 
-// Bounding box of every sub-box's vertices (float order keys): a warp whose
-// 32 vertices share a sub-box reduces before its atomics.
+// Bounding box of every sub-box's vertices (float order keys).  Grid-stride
+// over 32-vertex chunks: a warp keeps running per-lane extremes while its
+// chunks stay in one sub-box and reduces them into that box's six atomics
+// when the box changes and at its end (chunks that straddle two sub-boxes
+// add per vertex), so the six words of a box see a few atomics per warp
+// instead of one per 32 vertices.
+__device__ __forceinline__ void bbox_flush(int b, const int lo[3], const int hi[3], int* __restrict__ bbox) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const int l = __reduce_min_sync(0xffffffffu, lo[c]);
+    const int u = __reduce_max_sync(0xffffffffu, hi[c]);
+    if ((threadIdx.x & 31) == 0 && l <= u) {
+      atomicMin(&bbox[6 * b + 2 * c], l);
+      atomicMax(&bbox[6 * b + 2 * c + 1], u);
+    }
+  }
+}
+
 __global__ void __launch_bounds__(256) k_box_bbox(int64_t V, const float4* __restrict__ posd,
                                                   const int64_t* __restrict__ vprefix, int nsb,
                                                   int* __restrict__ bbox) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const bool valid = i < V;
-  const int b = valid ? (nsb > 1 ? find_box(vprefix, nsb, i) : 0) : -1;
-  int k[3] = {INT_MAX, INT_MAX, INT_MAX};
-  if (valid) {
-    const float4 r = __ldg(&posd[i]);
-    k[0] = float_order_key(r.x);
-    k[1] = float_order_key(r.y);
-    k[2] = float_order_key(r.z);
-  }
-  const int b0 = __shfl_sync(0xffffffffu, b, 0);
-  if (__all_sync(0xffffffffu, b == b0)) {
-    if (b0 < 0) return;
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  int cur = -1;  // the warp's current sub-box (warp-uniform)
+  int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+  for (int64_t base = warp * 32; base < V; base += n_warps * 32) {
+    const int64_t i = base + lane;
+    const bool valid = i < V;
+    const int b = valid ? (nsb > 1 ? find_box(vprefix, nsb, i) : 0) : -1;
+    int k[3] = {INT_MAX, INT_MAX, INT_MAX};
+    if (valid) {
+      const float4 r = __ldg(&posd[i]);
+      k[0] = float_order_key(r.x);
+      k[1] = float_order_key(r.y);
+      k[2] = float_order_key(r.z);
+    }
+    const int b0 = __shfl_sync(0xffffffffu, b, 0);
+    const bool uniform = __all_sync(0xffffffffu, b == b0 || b < 0);
+    if (uniform && b0 == cur) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const int lo = __reduce_min_sync(0xffffffffu, k[c]);
-      const int hi = __reduce_max_sync(0xffffffffu, valid ? k[c] : INT_MIN);
-      if ((threadIdx.x & 31) == 0) {
-        atomicMin(&bbox[6 * b0 + 2 * c], lo);
-        atomicMax(&bbox[6 * b0 + 2 * c + 1], hi);
+      for (int c = 0; c < 3; ++c) {
+        lo[c] = min(lo[c], k[c]);
+        if (valid) hi[c] = max(hi[c], k[c]);
+      }
+      continue;
+    }
+    if (cur >= 0) bbox_flush(cur, lo, hi, bbox);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) { lo[c] = INT_MAX; hi[c] = INT_MIN; }
+    if (uniform) {
+      cur = b0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        lo[c] = k[c];
+        if (valid) hi[c] = k[c];
+      }
+    } else {
+      cur = -1;
+      if (valid) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          atomicMin(&bbox[6 * b + 2 * c], k[c]);
+          atomicMax(&bbox[6 * b + 2 * c + 1], k[c]);
+        }
       }
     }
-  } else if (valid) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      atomicMin(&bbox[6 * b + 2 * c], k[c]);
-      atomicMax(&bbox[6 * b + 2 * c + 1], k[c]);
-    }
   }
+  if (cur >= 0) bbox_flush(cur, lo, hi, bbox);
 }
 
 __global__ void k_box_bbox_init(int nsb, int* __restrict__ bbox) {
@@ -1743,6 +1828,7 @@ struct dtfe_gpu_s {
   int64_t* sb_tprefix = nullptr;  // nsb + 1 tetrahedron range starts
   int nsb = 0;                    // scale boxes: the sub-boxes, or the whole upload before set_subboxes
   bool scale_ready = false;
+  std::vector<int64_t> sb_vprefix_h, sb_tprefix_h;  // host copies of sb_vprefix / sb_tprefix
   int64_t* inc_off = nullptr;     // V+1 offsets into inc
   int* inc = nullptr;             // incident tetrahedra per vertex (built when needed)
   bool inc_ready = false;
@@ -1894,28 +1980,33 @@ inline bool is_fused(int loc_variant) { return loc_variant >= kFirstFused; }
 constexpr int kNumEvalVariants = 3;
 
 // Vertex -> tetrahedron incidence lists (in no particular order within a
-// vertex): degrees, their scan into offsets, the fill.  Built with a
-// neighbour-less upload (to derive the neighbours) or for the adjoint.
-int build_incidence(dtfe_handle h) {
+// vertex): degrees, their scan into offsets, the fill.  star: each
+// tetrahedron listed at its two smallest vertices only (deriving the
+// neighbours of a neighbour-less upload); else at all four (the adjoint).
+int build_incidence(dtfe_handle h, bool star = false) {
   const int64_t V = h->V, T = h->T;
   int rc;
   if ((rc = dev_alloc(h, &h->inc_off, V + 1)) || (rc = dev_alloc(h, &h->inc, 4 * T)) ||
-      (rc = dev_alloc(h, &h->scratch_i, V)) ||
+      (rc = dev_alloc(h, &h->scratch_i, V + 1)) ||
       (rc = dev_alloc(h, &h->scan_blocks, (V + kScanBlock - 1) / kScanBlock + 1)))
     return rc;
   cudaStream_t st = h->stream;
   if (V) {
     DTFE_CUDA_TRY(cudaMemsetAsync(h->scratch_i, 0, sizeof(int) * V, st));
-    if (T) k_degree<<<blocks_for(T, 256), 256, 0, st>>>(T, h->tet_v, h->scratch_i);
+    if (T && star) k_degree_star<<<blocks_for(T, 256), 256, 0, st>>>(T, h->tet_v, h->scratch_i);
+    else if (T) k_degree<<<blocks_for(T, 256), 256, 0, st>>>(T, h->tet_v, h->scratch_i);
     const int64_t nb = (V + kScanBlock - 1) / kScanBlock;
     k_scan_blocks<<<(unsigned)nb, kScanBlock, 0, st>>>(V, h->scratch_i, h->inc_off, h->scan_blocks);
     k_scan_totals<<<1, kScanBlock, 0, st>>>(nb, h->scan_blocks, h->inc_off + V);
     k_scan_add<<<(unsigned)nb, kScanBlock, 0, st>>>(V, h->inc_off, h->scan_blocks);
     DTFE_CUDA_TRY(cudaMemsetAsync(h->scratch_i, 0, sizeof(int) * V, st));
-    if (T) k_fill_incidence<<<blocks_for(T, 256), 256, 0, st>>>(T, h->tet_v, h->inc_off, h->scratch_i, h->inc);
+    if (T && star)
+      k_fill_star<<<blocks_for(T, 256), 256, 0, st>>>(T, h->tet_v, h->inc_off, h->scratch_i, h->inc);
+    else if (T)
+      k_fill_incidence<<<blocks_for(T, 256), 256, 0, st>>>(T, h->tet_v, h->inc_off, h->scratch_i, h->inc);
   }
   DTFE_CUDA_TRY(cudaGetLastError());
-  h->inc_ready = true;
+  h->inc_ready = !star;
   return DTFE_OK;
 }
 
@@ -1943,13 +2034,24 @@ int ensure_scales(dtfe_handle h) {
       (rc = dev_alloc(h, &h->vbbox, 6 * (size_t)nsb)) || (rc = dev_alloc(h, &h->vscale, (size_t)nsb)))
     return rc;
   cudaStream_t st = h->stream;
-  DTFE_CUDA_TRY(cudaMemcpyAsync(h->sb_vprefix, vp.data(), sizeof(int64_t) * (nsb + 1), cudaMemcpyHostToDevice, st));
-  DTFE_CUDA_TRY(cudaMemcpyAsync(h->sb_tprefix, tp.data(), sizeof(int64_t) * (nsb + 1), cudaMemcpyHostToDevice, st));
+  // the prefix tables cross only when they change (a new sub-box layout or
+  // counts), from handle-owned copies: a step whose upload keeps the layout
+  // queues kernels only, so its host thread never waits for the device here
+  if (vp != h->sb_vprefix_h || tp != h->sb_tprefix_h) {
+    h->sb_vprefix_h = std::move(vp);
+    h->sb_tprefix_h = std::move(tp);
+    DTFE_CUDA_TRY(cudaMemcpyAsync(h->sb_vprefix, h->sb_vprefix_h.data(), sizeof(int64_t) * (nsb + 1),
+                                  cudaMemcpyHostToDevice, st));
+    DTFE_CUDA_TRY(cudaMemcpyAsync(h->sb_tprefix, h->sb_tprefix_h.data(), sizeof(int64_t) * (nsb + 1),
+                                  cudaMemcpyHostToDevice, st));
+  }
   k_box_bbox_init<<<blocks_for(6 * nsb, 256), 256, 0, st>>>(nsb, h->vbbox);
-  if (h->V) k_box_bbox<<<blocks_for(h->V, 256), 256, 0, st>>>(h->V, h->posd, h->sb_vprefix, nsb, h->vbbox);
+  if (h->V)
+    k_box_bbox<<<(unsigned)std::min<int64_t>(blocks_for(h->V, 256), 148 * 4), 256, 0, st>>>(h->V, h->posd,
+                                                                                           h->sb_vprefix, nsb,
+                                                                                           h->vbbox);
   k_box_scales<<<blocks_for(nsb, 64), 64, 0, st>>>(nsb, h->vbbox, h->sb_vprefix, h->vscale);
   DTFE_CUDA_TRY(cudaGetLastError());
-  DTFE_CUDA_TRY(cudaStreamSynchronize(st));  // the host prefix tables go out of scope
   h->nsb = nsb;
   h->scale_ready = true;
   return DTFE_OK;
@@ -2226,16 +2328,23 @@ static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const fl
     else DTFE_CUDA_TRY(cudaMemsetAsync(h->vel4, 0, sizeof(float4) * n_verts, st));
     if (h->S > 0 && !scal) DTFE_CUDA_TRY(cudaMemsetAsync(h->scal, 0, sizeof(float) * h->S * n_verts, st));
   }
-  // vertex -> tetrahedron incidence lists, for deriving the neighbours
+  // star lists, for deriving the neighbours
   h->inc_ready = false;
-  if (derive_neighbours && (rc = build_incidence(h))) return rc;
+  if (derive_neighbours && (rc = build_incidence(h, true))) return rc;
   // neighbours from the vertices, when they did not cross: every face at its
   // smallest vertex's star, then the few faces of very large stars
   if (n_tets && derive_neighbours) {
     DTFE_CUDA_TRY(cudaMemsetAsync(h->tet_n, 0x80, sizeof(int4) * n_tets, st));
-    const int64_t want = (n_verts + kStarWarps - 1) / kStarWarps;
-    k_neighbours_star<<<(unsigned)std::min<int64_t>(want, 148 * 32), 32 * kStarWarps, 0, st>>>(
-        n_verts, h->tet_v, h->inc_off, h->inc, (int*)h->tet_n);
+    // after the star fill, scratch_i holds the list of large stars and
+    // scratch_i[V] its count
+    int* big = h->scratch_i;
+    unsigned* n_big = (unsigned*)(h->scratch_i + n_verts);
+    DTFE_CUDA_TRY(cudaMemsetAsync(n_big, 0, sizeof(unsigned), st));
+    const int64_t want = (n_verts + 31) / 32;
+    k_neighbours_star<256, 8, 96, false><<<(unsigned)std::min<int64_t>(want, 148 * 32), 256, 0, st>>>(
+        n_verts, h->tet_v, h->inc_off, h->inc, (int*)h->tet_n, big, n_big, (unsigned)n_verts);
+    k_neighbours_star<128, 32, 768, true><<<148 * 4, 128, 0, st>>>(
+        n_verts, h->tet_v, h->inc_off, h->inc, (int*)h->tet_n, big, n_big, (unsigned)n_verts);
     k_derive_neighbours<<<blocks_for(n_tets, 256), 256, 0, st>>>(n_tets, h->tet_v, h->inc_off, h->inc, h->tet_n);
   }
   // hull vertices (a property of the tessellation's topology)
@@ -2747,7 +2856,7 @@ int dtfe_gpu_set_variants(dtfe_handle h, int32_t locate_variant, int32_t eval_va
 int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xyz, const float* w, const float* vel, int64_t n,
                           int32_t n_boxes, const dtfe_deposit_box* boxes, const int32_t grid[3],
                           double average_density, float* density_dev, float* velocity_dev, void** scratch,
-                          size_t* scratch_bytes, void* saved);
+                          size_t* scratch_bytes, void* saved, int inputs_dev);
 int dtfe_gpu_deposit_adjoint_impl(void* stream, const void* saved, const float* a_dev, float* gx_dev, float* gw_dev);
 int dtfe_internal_adjoint(void* stream, const void* cell_params, int64_t n_cells, int64_t V, int64_t T,
                           const int4* tet_v, const float4* posd, const float* w, const int* hull,
@@ -2767,19 +2876,35 @@ void dtfe_internal_adjoint_fill_params(void* out, const int4* tet_v, const float
                                        int64_t G2, int64_t n_total, const float* a, const float* b,
                                        const float* c, int full_value);
 
-int dtfe_gpu_deposit_dev(dtfe_handle h, int32_t kind, const float* xyz, const float* w, const float* vel, int64_t n,
-                         int32_t n_boxes, const dtfe_deposit_box* boxes, const int32_t grid[3],
-                         double average_density, float* density_dev, float* velocity_dev) {
+static int deposit_common(dtfe_handle h, int32_t kind, const float* xyz, const float* w, const float* vel,
+                          int64_t n, int32_t n_boxes, const dtfe_deposit_box* boxes, const int32_t grid[3],
+                          double average_density, float* density_dev, float* velocity_dev, int inputs_dev) {
   if (!h || !grid || (n > 0 && !xyz)) return set_error(DTFE_ERR_ARG, "null argument");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
   int64_t G = (int64_t)grid[0] * grid[1] * grid[2];
   if (density_dev) DTFE_CUDA_TRY(cudaMemsetAsync(density_dev, 0, sizeof(float) * G, h->stream));
   if (velocity_dev) DTFE_CUDA_TRY(cudaMemsetAsync(velocity_dev, 0, sizeof(float) * 3 * G, h->stream));
   int rc = dtfe_gpu_deposit_impl(h->stream, kind, xyz, w, vel, n, n_boxes, boxes, grid, average_density,
-                                 density_dev, velocity_dev, &h->dep_scratch, &h->dep_bytes, h->dep_saved);
+                                 density_dev, velocity_dev, &h->dep_scratch, &h->dep_bytes, h->dep_saved,
+                                 inputs_dev);
   if (rc) return rc;
   DTFE_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return DTFE_OK;
+}
+
+int dtfe_gpu_deposit_dev(dtfe_handle h, int32_t kind, const float* xyz, const float* w, const float* vel, int64_t n,
+                         int32_t n_boxes, const dtfe_deposit_box* boxes, const int32_t grid[3],
+                         double average_density, float* density_dev, float* velocity_dev) {
+  return deposit_common(h, kind, xyz, w, vel, n, n_boxes, boxes, grid, average_density, density_dev, velocity_dev,
+                        0);
+}
+
+int dtfe_gpu_deposit_resident(dtfe_handle h, int32_t kind, const float* xyz_dev, const float* w_dev,
+                              const float* vel_dev, int64_t n, int32_t n_boxes, const dtfe_deposit_box* boxes,
+                              const int32_t grid[3], double average_density, float* density_dev,
+                              float* velocity_dev) {
+  return deposit_common(h, kind, xyz_dev, w_dev, vel_dev, n, n_boxes, boxes, grid, average_density, density_dev,
+                        velocity_dev, 1);
 }
 
 int dtfe_gpu_deposit(dtfe_handle h, int32_t kind, const float* xyz, const float* w, const float* vel, int64_t n,

@@ -311,6 +311,16 @@ class DeviceDTFE:
                                               grid.ctypes.data, dplan.rho_bar, N.ptr(density_dev),
                                               N.ptr(velocity_dev)))
 
+    def deposit_resident(self, dplan, pos_dev, weight_dev, velocity_in_dev, density_dev, velocity_dev=None) -> None:
+        """Deposit with the particles already on the device (dtfe_gpu_deposit_resident):
+        pos_dev (n, 3), weight_dev (n,) or None, velocity_in_dev (n, 3) or None."""
+        grid = np.asarray(dplan.grid, np.int32)
+        N.check(self.lib.dtfe_gpu_deposit_resident(self.h, dplan.kind, N.ptr(pos_dev), N.ptr(weight_dev),
+                                                   N.ptr(velocity_in_dev) if velocity_dev is not None else None,
+                                                   dplan.n, len(dplan.boxes), C.addressof(dplan.boxes),
+                                                   grid.ctypes.data, dplan.rho_bar, N.ptr(density_dev),
+                                                   N.ptr(velocity_dev)))
+
     def sph(self, rho_bar: float, n_neighbors: int = 32, velocity: bool = True, scalars: bool = False,
             extensive: bool = False) -> dict:
         """SPH density (and velocity, scalars) on the host."""

@@ -330,6 +330,14 @@ int dtfe_gpu_deposit(dtfe_handle h, int32_t kind, const float* xyz, const float*
 int dtfe_gpu_deposit_dev(dtfe_handle h, int32_t kind, const float* xyz, const float* w, const float* vel,
                          int64_t n, int32_t n_boxes, const dtfe_deposit_box* boxes, const int32_t grid[3],
                          double average_density, float* density_dev, float* velocity_dev);
+/* Same with the particles already on the device as well (xyz_dev 3n floats,
+ * w_dev n or NULL, vel_dev 3n or NULL): no host copy at all.  Not in the
+ * reference, whose particles live in host memory; for callers that keep
+ * their particles resident between steps. */
+int dtfe_gpu_deposit_resident(dtfe_handle h, int32_t kind, const float* xyz_dev, const float* w_dev,
+                              const float* vel_dev, int64_t n, int32_t n_boxes, const dtfe_deposit_box* boxes,
+                              const int32_t grid[3], double average_density, float* density_dev,
+                              float* velocity_dev);
 
 /* ---- batched step as one CUDA graph --------------------------------------
  * The reference loops over its sub-boxes (DTFE_parallel, src/DTFE.cpp:

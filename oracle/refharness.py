@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import time
 
 import numpy as np
 
@@ -270,6 +271,79 @@ def time_boxes(plan, threads: int, which: int = 0, n_points: int = 1, with_deriv
         loads[k % len(loads)] += t
     t_derived = derived(main_grad)[3] if main_grad is not None else 0.0
     return max(loads) + t_derived, per_box
+
+
+def _time_sample(fn, n_items: int, threads: int):
+    """Runs fn(k) for the first min(threads, n_items) items concurrently, one
+    host thread each (the reference's OpenMP team gives each thread one
+    sub-box); returns (wall seconds, items run)."""
+    from concurrent.futures import ThreadPoolExecutor
+    m = max(1, min(threads, n_items))
+    with ThreadPoolExecutor(max_workers=m) as ex:
+        t0 = time.perf_counter()
+        list(ex.map(fn, range(m)))
+        return time.perf_counter() - t0, m
+
+
+def time_deposit_boxes(dplan, threads: int, velocity: bool = True):
+    """Times the reference's own NGP/CIC/TSC_interpolation_regular_grid
+    (src/CIC_interpolation.cc:67-273, src/TSC_interpolation.cc:67-254) on a
+    sample of the deposit plan's sub-boxes, one per host thread, each with its
+    region's particles and grid tile.  Returns (grid cells of the sampled
+    tiles per second of wall time, sampled boxes, particles in them); the
+    wall time includes the harness copying the arrays into the reference's
+    Particle_data records."""
+    L = lib()
+    vp = C.c_void_p
+    L.ref_deposit.argtypes = [C.c_int, vp, vp, vp, C.c_int64, vp, vp, C.c_double, vp, vp]
+    boxes = list(dplan.boxes)
+    cells = [int(b.tile_dims[0]) * int(b.tile_dims[1]) * int(b.tile_dims[2]) for b in boxes]
+
+    def one(k):
+        b = boxes[k]
+        o, n = int(b.particle_offset), int(b.n_particles)
+        pos = np.ascontiguousarray(dplan.pos[o:o + n])
+        w = np.ascontiguousarray(dplan.weight[o:o + n])
+        vel = np.ascontiguousarray(dplan.velocity[o:o + n]) if velocity and dplan.velocity is not None else None
+        region = np.array([b.region[a] for a in range(6)], np.float32)
+        dims = np.array([b.tile_dims[a] for a in range(3)], np.int32)
+        dens = np.zeros(cells[k], np.float32)
+        velo = np.zeros((cells[k], 3), np.float32) if vel is not None else None
+        rc = L.ref_deposit(int(dplan.kind), pos.ctypes.data, w.ctypes.data, None if vel is None else vel.ctypes.data,
+                           n, region.ctypes.data, dims.ctypes.data, float(dplan.rho_bar), dens.ctypes.data,
+                           None if velo is None else velo.ctypes.data)
+        if rc:
+            raise RuntimeError(f"ref_deposit failed ({rc})")
+    wall, m = _time_sample(one, len(boxes), threads)
+    return sum(cells[:m]) / wall, m, int(sum(int(b.n_particles) for b in boxes[:m]))
+
+
+def time_sph_boxes(plan, threads: int, n_neighbors: int = 32):
+    """Times the reference's own SPH_interpolation (src/SPH_interpolation.cc:
+    47-146 and 252-474, with its kd-tree) of density and velocity on a sample
+    of the plan's padded sub-boxes, one per host thread, each on its grid
+    tile.  Returns (grid cells of the sampled tiles per second of wall time,
+    sampled boxes)."""
+    L = lib()
+    vp = C.c_void_p
+    L.ref_sph.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int64, vp, vp, C.c_double, C.c_int, vp, vp, vp]
+    K = plan.n_boxes
+    cells = []
+    for k in range(K):
+        b = plan.boxes[k]
+        cells.append(int(b.tile_dims[0]) * int(b.tile_dims[1]) * int(b.tile_dims[2]))
+
+    def one(k):
+        xyz, w, vel, _tv, _tn, dims, region = _box_args(plan, k)
+        dens = np.zeros(cells[k], np.float32)
+        velo = np.zeros((cells[k], 3), np.float32)
+        rc = L.ref_sph(xyz.ctypes.data, w.ctypes.data, None if vel is None else vel.ctypes.data, None, 0, len(xyz),
+                       region.ctypes.data, dims.ctypes.data, float(plan.rho_bar), n_neighbors, dens.ctypes.data,
+                       None if vel is None else velo.ctypes.data, None)
+        if rc:
+            raise RuntimeError(f"ref_sph failed ({rc})")
+    wall, m = _time_sample(one, K, threads)
+    return sum(cells[:m]) / wall, m
 
 
 def write_binary(path: str, data, ncomp: int) -> None:

@@ -104,8 +104,11 @@ def test_packed_malformed_is_reported(gpu_built):
 
 
 def _plans():
-    """A periodic multi-sub-box plan and a sparse non-periodic one (many hull
-    faces, sub-boxes with few or no tetrahedra)."""
+    """A periodic multi-sub-box plan, a sparse non-periodic one (many hull
+    faces, sub-boxes with few or no tetrahedra) and a single box around one
+    vertex of very high degree (400 points on a jittered shell around it:
+    its star holds far more faces than a per-vertex table, so the fallback
+    search settles them)."""
     pos, psi = S.zeldovich_lattice(18, 100.0, 1.0, seed=15)
     vel = (40 * psi).astype(np.float32)
     a = P.make_plan(pos, np.ones(len(pos), np.float32), vel, None, grid=(18, 16, 20), n_threads=8)
@@ -114,10 +117,18 @@ def _plans():
     b = P.make_plan(p2, rng.uniform(0.5, 1.5, 300).astype(np.float32), rng.standard_normal((300, 3)).astype(
         np.float32), None, grid=(12, 12, 12), n_threads=6, periodic=False, padding=np.full(6, 4.0, np.float32),
         average_density_value=3e-4)
-    return [a, b]
+    rng = np.random.default_rng(17)
+    d = rng.standard_normal((400, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    shell = 50.0 + d * (20.0 * (1.0 + 0.05 * rng.random((400, 1))))
+    p3 = np.vstack([[[50.0, 50.0, 50.0]], shell, rng.random((200, 3)) * 100.0]).astype(np.float32)
+    c = P.make_plan(p3, np.ones(len(p3), np.float32), rng.standard_normal((len(p3), 3)).astype(np.float32), None,
+                    grid=(10, 10, 10), n_threads=1, periodic=False, padding=np.full(6, 2.0, np.float32),
+                    average_density_value=1e-3)
+    return [a, b, c]
 
 
-@pytest.mark.parametrize("which", [0, 1])
+@pytest.mark.parametrize("which", [0, 1, 2])
 @pytest.mark.parametrize("form", ["plain_without_neighbours", "packed_vertices"])
 def test_neighbours_derived_on_device(gpu_built, which, form):
     """Only the vertices cross (tet_n = NULL, or the vertex-only packed form

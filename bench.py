@@ -111,6 +111,8 @@ def build_workload(n: int, rank: int, threads: int, scalars: int = 0):
                        average_density_value=float(len(pos)) / S.BOX ** 3)
     plan.timings["ics_s"] = t_ics
     plan.timings["plan_total_s"] = time.time() - t0
+    # the input particles, for the upload that ships them once
+    plan.particles = {"pos": pos, "weight": w, "velocity": vel, "scalar": sc}
     return plan
 
 
@@ -1116,12 +1118,20 @@ def run_ours(args):
         # vertices packed (dtfe_tets_pack_vertices); the device derives the
         # neighbours
         packed = pin(PL.pack_tet_vertices(plan.tet_v))
+        # the input particles cross once; each padded vertex is a 4-byte code
+        # (source particle, periodic image) that a kernel expands
+        codes, box_len = PL.vertex_codes(plan, plan.particles["pos"])
+        parts = {"pos": pin(plan.particles["pos"]), "weight": pin(plan.particles["weight"]),
+                 "velocity": pin(plan.particles["velocity"]), "scalar": pin(plan.particles["scalar"]),
+                 "codes": pin(codes.view(np.int32)).view(np.uint32), "box_length": box_len}
         host_out = {f: pin(np.empty((G, ncomp[f]), np.float32)) for f in fields}
-        h_vert = hp.xyz.nbytes + hp.weight.nbytes + hp.velocity.nbytes + 4 * (len(hp.xs) + len(hp.ys) + len(hp.zs))
+        h_tables = 4 * (len(hp.xs) + len(hp.ys) + len(hp.zs))
+        h_vert = hp.xyz.nbytes + hp.weight.nbytes + hp.velocity.nbytes + h_tables
+        h_parts = sum(a.nbytes for k, a in parts.items() if k != "box_length" and a is not None) + h_tables
         d2h = sum(a.nbytes for a in host_out.values())
 
         def e2e_packed():
-            dev.upload_packed(hp, packed)
+            dev.upload_packed_particles(hp, packed, parts)
             dev.set_subboxes(hp)
             dev.vertex_density(hp.rho_bar)
             dev.interpolate(fields, method=0, out=host_out)
@@ -1160,7 +1170,7 @@ def run_ours(args):
             ring.append(d)
         outs2 = [host_out] + [{f: pin(np.empty_like(a)) for f, a in host_out.items()} for _ in range(nbuf - 1)]
         for d in ring:
-            d.upload_packed(hp, packed)
+            d.upload_packed_particles(hp, packed, parts)
             d.set_subboxes(hp)
         # the handles' inputs cross PCIe one after the other, in step order
         for i, d in enumerate(ring):
@@ -1169,7 +1179,7 @@ def run_ours(args):
         def e2e_pipelined(k):
             d = ring[k % nbuf]
             d.synchronize()
-            d.upload_packed(hp, packed)
+            d.upload_packed_particles(hp, packed, parts)
             d.vertex_density(hp.rho_bar)
             d.interpolate_async(fields, outs2[k % nbuf], method=0)
         for k in range(nbuf):
@@ -1193,13 +1203,15 @@ def run_ours(args):
             d.chain_uploads(None)
         for d in ring[1:]:
             d.close()
-        e2e = {"value": world * G / te, "unit": "grid samples/s", "h2d_bytes_per_step": int(packed.nbytes + h_vert),
+        e2e = {"value": world * G / te, "unit": "grid samples/s", "h2d_bytes_per_step": int(packed.nbytes + h_parts),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * te,
-               "path": "per step: dtfe_gpu_upload_packed (vertex-only packed tetrahedra, neighbours derived on "
-                       "the device) + vertex_density + interpolate_async into pinned host "
+               "path": "per step: dtfe_gpu_upload_packed_particles (vertex-only packed tetrahedra, neighbours "
+                       "derived on the device; the input particles once plus a 4-byte source/image code per "
+                       "padded vertex) + vertex_density + interpolate_async into pinned host "
                        f"buffers, {nbuf} handles in turn (uploads chained in step order); sub-box geometry set "
                        "once per handle", "buffers": nbuf,
                "packed_bytes_per_tet": packed.nbytes / plan.n_tets,
+               "particles": len(parts["pos"]), "padded_vertices": plan.n_verts,
                "samples_located_last_step": st2["n_samples_located"],
                "single_step_latency_ms": 1e3 * te_lat,
                "unpacked_single_step": {"value": world * G / te_plain, "ms_per_step": 1e3 * te_plain,

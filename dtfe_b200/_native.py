@@ -177,6 +177,8 @@ def gpu() -> C.CDLL:
         lib.dtfe_gpu_upload.argtypes = [H, vp, vp, C.c_int64, vp, vp, vp, vp, C.c_int64]
         lib.dtfe_gpu_chain_uploads.argtypes = [H, H]
         lib.dtfe_gpu_upload_packed.argtypes = [H, vp, C.c_int64, vp, vp, vp, vp, C.c_int64]
+        lib.dtfe_gpu_upload_packed_particles.argtypes = [H, vp, C.c_int64, vp, vp, vp, vp, C.c_int64, vp,
+                                                         C.c_int64, vp]
         lib.dtfe_gpu_set_subboxes.argtypes = [H, C.c_int32, vp, vp, C.c_int64, vp, C.c_int64,
                                               vp, C.c_int64, vp]
         lib.dtfe_gpu_set_regions.argtypes = [H, C.c_int32, vp]

@@ -75,6 +75,37 @@ __global__ void k_pack_xyz(int64_t n, const float* __restrict__ xyz, float4* __r
   if (i < n) out[i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], wval);
 }
 
+// Vertices from the input particles: code = source particle (bits 0-26) |
+// periodic image (bits 27-31, i1 * 9 + i2 * 3 + i3 with i in {0, 1, 2}); the
+// vertex sits at the particle's position minus (i - 1) * box length per
+// axis, the float arithmetic of the padded-box selection
+// (findParticlesInBox, src/subpartition.h:79-154).  A code outside
+// [0, n_src) x [0, 27) counts into *bad and yields particle 0 unshifted.
+constexpr uint32_t kSrcBits = 27;
+__global__ void k_gather_particles(int64_t V, int S, const uint32_t* __restrict__ codes,
+                                   const float* __restrict__ pxyz, const float* __restrict__ pvel,
+                                   const float* __restrict__ pw, const float* __restrict__ pscal, int64_t n_src,
+                                   float L0, float L1, float L2, float4* __restrict__ posd,
+                                   float4* __restrict__ vel4, float* __restrict__ w, float* __restrict__ scal,
+                                   unsigned long long* __restrict__ bad) {
+  const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (v >= V) return;
+  const uint32_t c = __ldg(&codes[v]);
+  int64_t s = c & ((1u << kSrcBits) - 1u);
+  int img = (int)(c >> kSrcBits);
+  if (s >= n_src || img > 26) {
+    atomicAdd(bad, 1ull);
+    s = 0;
+    img = 13;
+  }
+  const float o0 = (float)(img / 9 - 1) * L0, o1 = (float)((img / 3) % 3 - 1) * L1, o2 = (float)(img % 3 - 1) * L2;
+  posd[v] = make_float4(__ldg(&pxyz[3 * s]) - o0, __ldg(&pxyz[3 * s + 1]) - o1, __ldg(&pxyz[3 * s + 2]) - o2, 0.f);
+  vel4[v] = pvel ? make_float4(__ldg(&pvel[3 * s]), __ldg(&pvel[3 * s + 1]), __ldg(&pvel[3 * s + 2]), 0.f)
+                 : make_float4(0.f, 0.f, 0.f, 0.f);
+  w[v] = __ldg(&pw[s]);
+  for (int k = 0; k < S; ++k) scal[v * S + k] = pscal ? __ldg(&pscal[s * S + k]) : 0.f;
+}
+
 // Range check of a plain upload before any kernel indexes with it: vertex
 // ids in [0, V), neighbour ids (when given) in [-1, T).  Reads only the
 // uploaded arrays;
@@ -2275,19 +2306,38 @@ extern "C++" {
 // of an upload are queued before any of its kernels, so that a chained
 // handle's upload (dtfe_gpu_chain_uploads) can start on the copy engine as
 // soon as these have crossed.
+// Vertices given as codes into the input particle arrays (k_gather_particles)
+// instead of one record each.
+struct ParticleSource {
+  const uint32_t* codes;  // n_verts host codes
+  int64_t n;              // particles
+  float len[3];           // box lengths of the periodic images
+};
+
 template <class TetH2D, class TetFinish>
 static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const float* w, const float* vel,
                        const float* scal, int64_t n_verts, size_t tets_bytes, TetH2D tets_h2d,
-                       TetFinish tets_finish, bool derive_neighbours = false) {
-  if (!h || !xyz || !w) return set_error(DTFE_ERR_ARG, "null argument");
+                       TetFinish tets_finish, bool derive_neighbours = false,
+                       const ParticleSource* ps = nullptr) {
+  if (!h || !xyz || !w || (ps && n_verts > 0 && !ps->codes)) return set_error(DTFE_ERR_ARG, "null argument");
   if (n_tets < 0 || n_verts < 0 || n_tets > 0x7FFFFFFF || n_verts >= 0x7F7F7F7F)
     return set_error(DTFE_ERR_TOO_LARGE, "tetrahedron or vertex count beyond int32 indexing");
+  if (ps && (ps->n < 0 || ps->n > ((int64_t)1 << kSrcBits)))
+    return set_error(DTFE_ERR_TOO_LARGE, "more than 2^27 particles for vertex codes");
+  if (ps && n_verts > 0 && ps->n == 0) return set_error(DTFE_ERR_ARG, "vertex codes without particles");
   DTFE_CUDA_TRY(cudaSetDevice(h->device));
   int rc;
   h->T = n_tets;
   h->V = n_verts;
-  const size_t tets_stage = (tets_bytes + 255) & ~(size_t)255;
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t tets_stage = al(tets_bytes);
   const size_t vert_stage = sizeof(float) * 3 * (size_t)n_verts;
+  // particle mode: xyz, vel (3n each), w (n), scalars (S n), codes (V)
+  const int64_t np = ps ? ps->n : 0;
+  const size_t p3 = al(sizeof(float) * 3 * (size_t)np), p1 = al(sizeof(float) * (size_t)np);
+  const size_t ps_stage = ps ? 2 * p3 + p1 + al(sizeof(float) * h->S * (size_t)np) +
+                                   al(sizeof(uint32_t) * (size_t)n_verts)
+                             : 0;
   if ((rc = dev_alloc(h, &h->tet_v, n_tets)) || (rc = dev_alloc(h, &h->tet_n, n_tets)) ||
       (rc = dev_alloc(h, &h->posd, n_verts)) || (rc = dev_alloc(h, &h->vel4, n_verts)) ||
       (rc = dev_alloc(h, &h->w, n_verts)) || (rc = dev_alloc(h, &h->vacc, n_verts)) ||
@@ -2295,7 +2345,7 @@ static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const fl
       (rc = dev_alloc(h, &h->scal, (size_t)n_verts * h->S)) ||
       // staging kept in the handle (an allocation per upload would map and
       // unmap device memory every time): tetrahedra, positions, velocities
-      (rc = dev_alloc(h, &h->upload_buf, tets_stage + 2 * vert_stage)))
+      (rc = dev_alloc(h, &h->upload_buf, tets_stage + (ps ? ps_stage : 2 * vert_stage))))
     return rc;
   cudaStream_t st = h->stream;
   char* stage = h->upload_buf;
@@ -2304,7 +2354,23 @@ static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const fl
   // copies first: wait for the chained handle's transfers, queue ours, mark them
   if (h->upload_after) DTFE_CUDA_TRY(cudaStreamWaitEvent(st, h->upload_after->ev_h2d, 0));
   if (n_tets && (rc = tets_h2d(h, stage))) return rc;
-  if (n_verts) {
+  if (ps) {
+    char* q = stage + tets_stage;
+    float* pxyz = (float*)q;
+    float* pvel = (float*)(q + p3);
+    float* pw = (float*)(q + 2 * p3);
+    float* pscal = (float*)(q + 2 * p3 + p1);
+    uint32_t* pcode = (uint32_t*)(q + 2 * p3 + p1 + al(sizeof(float) * h->S * (size_t)np));
+    if (np) {
+      DTFE_CUDA_TRY(cudaMemcpyAsync(pxyz, xyz, sizeof(float) * 3 * np, cudaMemcpyHostToDevice, st));
+      if (vel) DTFE_CUDA_TRY(cudaMemcpyAsync(pvel, vel, sizeof(float) * 3 * np, cudaMemcpyHostToDevice, st));
+      DTFE_CUDA_TRY(cudaMemcpyAsync(pw, w, sizeof(float) * np, cudaMemcpyHostToDevice, st));
+      if (h->S > 0 && scal)
+        DTFE_CUDA_TRY(cudaMemcpyAsync(pscal, scal, sizeof(float) * h->S * np, cudaMemcpyHostToDevice, st));
+    }
+    if (n_verts)
+      DTFE_CUDA_TRY(cudaMemcpyAsync(pcode, ps->codes, sizeof(uint32_t) * n_verts, cudaMemcpyHostToDevice, st));
+  } else if (n_verts) {
     DTFE_CUDA_TRY(cudaMemcpyAsync(sx, xyz, vert_stage, cudaMemcpyHostToDevice, st));
     if (vel) DTFE_CUDA_TRY(cudaMemcpyAsync(sv, vel, vert_stage, cudaMemcpyHostToDevice, st));
     DTFE_CUDA_TRY(cudaMemcpyAsync(h->w, w, sizeof(float) * n_verts, cudaMemcpyHostToDevice, st));
@@ -2322,7 +2388,14 @@ static int upload_impl(dtfe_handle h, int64_t n_tets, const float* xyz, const fl
     drop_graph(h);
     return rc;
   }
-  if (n_verts) {
+  if (ps && n_verts) {
+    const char* q = stage + tets_stage;
+    k_gather_particles<<<blocks_for(n_verts, 256), 256, 0, st>>>(
+        n_verts, h->S, (const uint32_t*)(q + 2 * p3 + p1 + al(sizeof(float) * h->S * (size_t)np)),
+        (const float*)q, vel ? (const float*)(q + p3) : nullptr, (const float*)(q + 2 * p3),
+        (h->S > 0 && scal) ? (const float*)(q + 2 * p3 + p1) : nullptr, np, ps->len[0], ps->len[1], ps->len[2],
+        h->posd, h->vel4, h->w, h->scal, h->counters + CNT_DECODE);
+  } else if (n_verts) {
     k_pack_xyz<<<blocks_for(n_verts, 256), 256, 0, st>>>(n_verts, sx, h->posd, 0.f);
     if (vel) k_pack_xyz<<<blocks_for(n_verts, 256), 256, 0, st>>>(n_verts, sv, h->vel4, 0.f);
     else DTFE_CUDA_TRY(cudaMemsetAsync(h->vel4, 0, sizeof(float4) * n_verts, st));
@@ -2404,7 +2477,7 @@ int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n, i
 // on the device from the vertices.
 static int upload_packed_vertices(dtfe_handle h, const int64_t hd[10], const void* packed, int64_t packed_bytes,
                                   const float* xyz, const float* w, const float* vel, const float* scal,
-                                  int64_t n_verts) {
+                                  int64_t n_verts, const ParticleSource* ps) {
   const int64_t T = hd[1], nb = hd[2], n_esc = hd[3];
   bool ok = T >= 0 && nb == (T + kPackBlock - 1) / kPackBlock && n_esc >= 0 && hd[4] >= 80 &&
             hd[5] >= hd[4] + 4 * nb && hd[6] >= hd[5] + 4 * (nb + 1) && hd[7] >= hd[6] + 8 * (nb + 1) &&
@@ -2433,17 +2506,19 @@ static int upload_packed_vertices(dtfe_handle h, const int64_t hd[10], const voi
         DTFE_CUDA_TRY(cudaGetLastError());
         return DTFE_OK;
       },
-      true);
+      true, ps);
 }
 
-int dtfe_gpu_upload_packed(dtfe_handle h, const void* packed, int64_t packed_bytes, const float* xyz,
-                           const float* w, const float* vel, const float* scal, int64_t n_verts) {
+static int upload_packed_any(dtfe_handle h, const void* packed, int64_t packed_bytes, const float* xyz,
+                             const float* w, const float* vel, const float* scal, int64_t n_verts,
+                             const ParticleSource* ps) {
   // header: magic "DTP2", T, n_blocks, n_escapes, then the byte offsets of
   // block bases, escape prefix, block byte offsets, flags, data, escapes
   int64_t hd[10];
   if (!packed || packed_bytes < (int64_t)sizeof(hd)) return set_error(DTFE_ERR_ARG, "null or short packed buffer");
   std::memcpy(hd, packed, sizeof(hd));
-  if (hd[0] == 0x33505444) return upload_packed_vertices(h, hd, packed, packed_bytes, xyz, w, vel, scal, n_verts);
+  if (hd[0] == 0x33505444)
+    return upload_packed_vertices(h, hd, packed, packed_bytes, xyz, w, vel, scal, n_verts, ps);
   const int64_t T = hd[1], nb = hd[2], n_esc = hd[3];
   bool ok = hd[0] == 0x32505444 && T >= 0 && nb == (T + kPackBlock - 1) / kPackBlock && n_esc >= 0 &&
             hd[4] >= (int64_t)sizeof(hd) && hd[5] >= hd[4] + 4 * nb && hd[6] >= hd[5] + 4 * (nb + 1) &&
@@ -2464,7 +2539,21 @@ int dtfe_gpu_upload_packed(dtfe_handle h, const void* packed, int64_t packed_byt
             hd[9] - hd[8], (const int32_t*)(dev + hd[9]), n_esc, hh->tet_v, hh->tet_n, hh->counters + CNT_DECODE);
         DTFE_CUDA_TRY(cudaGetLastError());
         return DTFE_OK;
-      });
+      },
+      false, ps);
+}
+
+int dtfe_gpu_upload_packed(dtfe_handle h, const void* packed, int64_t packed_bytes, const float* xyz,
+                           const float* w, const float* vel, const float* scal, int64_t n_verts) {
+  return upload_packed_any(h, packed, packed_bytes, xyz, w, vel, scal, n_verts, nullptr);
+}
+
+int dtfe_gpu_upload_packed_particles(dtfe_handle h, const void* packed, int64_t packed_bytes, const float* xyz,
+                                     const float* w, const float* vel, const float* scal, int64_t n_particles,
+                                     const uint32_t* vertex_codes, int64_t n_verts, const float box_length[3]) {
+  if (!box_length) return set_error(DTFE_ERR_ARG, "null argument");
+  ParticleSource ps{vertex_codes, n_particles, {box_length[0], box_length[1], box_length[2]}};
+  return upload_packed_any(h, packed, packed_bytes, xyz, w, vel, scal, n_verts, &ps);
 }
 
 int dtfe_gpu_chain_uploads(dtfe_handle h, dtfe_handle after) {

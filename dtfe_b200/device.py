@@ -64,6 +64,18 @@ class DeviceDTFE:
             self.h, packed.ctypes.data, packed.nbytes, N.ptr(plan.xyz), N.ptr(plan.weight), N.ptr(plan.velocity),
             N.ptr(plan.scalar), plan.n_verts))
 
+    def upload_packed_particles(self, plan, packed: np.ndarray, particles: dict) -> None:
+        """Packed tetrahedra plus the input particles once
+        (dtfe_gpu_upload_packed_particles): ``particles`` holds ``pos``,
+        ``weight``, ``velocity`` (or None), ``scalar`` (or None) of the n input
+        particles, ``codes`` (plan.vertex_codes) and ``box_length`` (3 floats)."""
+        L = np.ascontiguousarray(particles["box_length"], np.float32)
+        codes = particles["codes"]
+        N.check(self.lib.dtfe_gpu_upload_packed_particles(
+            self.h, packed.ctypes.data, packed.nbytes, N.ptr(particles["pos"]), N.ptr(particles["weight"]),
+            N.ptr(particles.get("velocity")), N.ptr(particles.get("scalar")), len(particles["pos"]),
+            N.ptr(codes), len(codes), L.ctypes.data))
+
     def chain_uploads(self, after: "DeviceDTFE | None") -> None:
         """Uploads on this handle wait for ``after``'s latest transfers
         (dtfe_gpu_chain_uploads); None removes the link."""

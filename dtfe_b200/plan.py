@@ -518,6 +518,35 @@ def pack_tets(tet_v: np.ndarray, tet_n: np.ndarray, out: np.ndarray | None = Non
     return buf
 
 
+def vertex_codes(plan, pos: np.ndarray, box=(0.0, 100.0, 0.0, 100.0, 0.0, 100.0)):
+    """Per vertex its source particle and periodic image as one uint32
+    (dtfe_gpu_upload_packed_particles): bits 0-26 plan.src, bits 27-31
+    i1 * 9 + i2 * 3 + i3 where vertex = pos[src] - (i - 1) * box length per
+    axis in float32, the padded-box selection's arithmetic.  Returns
+    (codes, box_length float32[3]); raises if a vertex is not such an image
+    of its particle."""
+    pos = np.asarray(pos, np.float32)
+    if len(pos) > (1 << 27):
+        raise ValueError("more than 2^27 particles")
+    b = np.asarray(box, np.float32)
+    L = np.array([b[1] - b[0], b[3] - b[2], b[5] - b[4]], np.float32)
+    p = pos[plan.src]
+    img = np.zeros(plan.n_verts, np.uint32)
+    for k in range(3):
+        found = np.zeros(plan.n_verts, bool)
+        ik = np.full(plan.n_verts, 1, np.uint32)
+        for i in (1, 0, 2):
+            shifted = (p[:, k] - np.float32(i - 1) * L[k]).astype(np.float32)
+            hit = ~found & (shifted == plan.xyz[:, k])
+            ik[hit] = i
+            found |= hit
+        if not found.all():
+            raise ValueError("vertices that are not periodic images of their particles")
+        img = img * 3 + ik
+    codes = (plan.src.astype(np.uint32) | (img << np.uint32(27))).astype(np.uint32)
+    return codes, L
+
+
 def pack_tet_vertices(tet_v: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
     """The vertex-only packed form of a tessellation
     (dtfe_tets_pack_vertices, about 5 bytes per tetrahedron): the device

@@ -169,6 +169,21 @@ int dtfe_gpu_upload(dtfe_handle h, const int32_t* tet_v, const int32_t* tet_n,
  * reference (its tessellation never leaves the host). */
 int dtfe_gpu_upload_packed(dtfe_handle h, const void* packed, int64_t packed_bytes, const float* xyz,
                            const float* w, const float* vel, const float* scal, int64_t n_verts);
+/* Same, with the input particles crossing once instead of one record per
+ * padded vertex (a periodic box's padding repeats about a third of its
+ * particles): xyz (3 n), w (n), vel (3 n or NULL), scal (S n or NULL) are
+ * the n_particles input particles, and vertex_codes holds per vertex its
+ * source particle in bits 0-26 and its periodic image in bits 27-31
+ * (i1 * 9 + i2 * 3 + i3, i in {0, 1, 2}; 13 = unshifted).  A kernel places
+ * vertex v at its particle's position minus (i - 1) * box_length per axis in
+ * float, the arithmetic of the padded-box selection (findParticlesInBox,
+ * src/subpartition.h:79-154), so the vertices equal the padded set the host
+ * tessellated.  At most 2^27 particles (DTFE_ERR_TOO_LARGE); a code out of
+ * range is reported by the next status read (DTFE_ERR_ARG).  No counterpart
+ * in the reference. */
+int dtfe_gpu_upload_packed_particles(dtfe_handle h, const void* packed, int64_t packed_bytes, const float* xyz,
+                                     const float* w, const float* vel, const float* scal, int64_t n_particles,
+                                     const uint32_t* vertex_codes, int64_t n_verts, const float box_length[3]);
 /* Orders uploads between two handles used alternately (double buffering
  * across snapshots): every later upload on h waits until the host->device
  * copies of after's most recent upload have crossed, so the two handles'

@@ -191,3 +191,49 @@ def test_packed_vertices_malformed_is_reported(gpu_built):
         dev.set_subboxes(plan)
         dev.vertex_density(plan.rho_bar)
         dev.interpolate(["density"], method=0)
+
+
+@pytest.mark.parametrize("form", ["packed", "packed_vertices"])
+def test_packed_particles_upload(gpu_built, form):
+    """The input particles cross once with a code per vertex
+    (dtfe_gpu_upload_packed_particles): the device rebuilds the padded,
+    periodic vertex set exactly (positions, weights, velocities, scalars),
+    so vertex densities and fields equal those of the per-vertex upload bit
+    for bit; a code outside the particles is reported by the next status
+    read and a good upload clears it."""
+    from dtfe_b200 import _native as N
+    from dtfe_b200.device import DeviceDTFE
+    pos, psi = S.zeldovich_lattice(16, 100.0, 1.0, seed=18)
+    rng = np.random.default_rng(19)
+    w = rng.uniform(0.5, 1.5, len(pos)).astype(np.float32)
+    vel = (40 * psi).astype(np.float32)
+    sc = rng.standard_normal((len(pos), 2)).astype(np.float32)
+    plan = P.make_plan(pos, w, vel, sc, grid=(16, 14, 18), n_threads=8)
+    codes, L = P.vertex_codes(plan, pos)
+    assert (codes >> 27).max() > 13 and (codes >> 27).min() < 13  # images on both sides
+    parts = {"pos": pos, "weight": w, "velocity": vel, "scalar": sc, "codes": codes, "box_length": L}
+    packed = P.pack_tets(plan.tet_v, plan.tet_n) if form == "packed" else P.pack_tet_vertices(plan.tet_v)
+    fields = FIELDS + ["scalar", "scalar_gradient"]
+    with DeviceDTFE(0, 2) as ref_dev:
+        ref_dev.load(plan)
+        ref_dev.vertex_density(plan.rho_bar)
+        ref = ref_dev.interpolate(fields, method=0)
+        ref_d = ref_dev.download_vertex_density(plan.n_verts)
+    with DeviceDTFE(0, 2) as dev:
+        dev.upload_packed_particles(plan, packed, parts)
+        dev.set_subboxes(plan)
+        dev.vertex_density(plan.rho_bar)
+        got = dev.interpolate(fields, method=0)
+        assert np.array_equal(dev.download_vertex_density(plan.n_verts).view(np.int32), ref_d.view(np.int32))
+        for f in fields:
+            assert np.array_equal(got[f], ref[f]), f
+        bad = dict(parts, codes=codes.copy())
+        bad["codes"][7] = np.uint32(len(pos))              # a particle that does not exist
+        dev.upload_packed_particles(plan, packed, bad)
+        dev.vertex_density(plan.rho_bar)
+        with pytest.raises(N.DTFEError, match="did not decode"):
+            dev.interpolate(["density"], method=0)
+        dev.upload_packed_particles(plan, packed, parts)
+        dev.vertex_density(plan.rho_bar)
+        again = dev.interpolate(["density"], method=0)
+        assert np.array_equal(again["density"], ref["density"])

@@ -1,5 +1,6 @@
 """Packed tessellation (dtfe_tets_pack / dtfe_tets_unpack) round trips."""
 import numpy as np
+import pytest
 
 from dtfe_b200 import plan as P
 from dtfe_b200 import synthetic as S
@@ -83,3 +84,30 @@ def test_pack_vertices_escapes_and_order(built):
     import pytest
     with pytest.raises(ValueError):
         P.pack_tet_vertices(bad)
+
+
+def test_vertex_codes_rebuild_the_padded_vertices():
+    """plan.vertex_codes: each vertex is its source particle shifted by the
+    coded periodic image in float32, exactly the position the planner
+    selected; images on both sides of the box occur, and an unrelated
+    position is refused."""
+    import numpy as np
+    from dtfe_b200 import plan as P
+    from dtfe_b200 import synthetic as S
+    pos, psi = S.zeldovich_lattice(14, 100.0, 1.0, seed=40)
+    plan = P.make_plan(pos, np.ones(len(pos), np.float32), None, None, grid=(14, 14, 14), n_threads=4)
+    codes, L = P.vertex_codes(plan, pos)
+    src = codes & np.uint32((1 << 27) - 1)
+    img = codes >> np.uint32(27)
+    assert np.array_equal(src, plan.src.astype(np.uint32))
+    i = np.stack([img // 9, (img // 3) % 3, img % 3], axis=1).astype(np.float32) - np.float32(1)
+    rebuilt = (pos[src] - i * L).astype(np.float32)
+    assert np.array_equal(rebuilt, plan.xyz)
+    assert img.min() < 13 < img.max()
+    bad = plan.xyz.copy()
+    plan.xyz[5, 0] += np.float32(0.5)
+    try:
+        with pytest.raises(ValueError):
+            P.vertex_codes(plan, pos)
+    finally:
+        plan.xyz[...] = bad

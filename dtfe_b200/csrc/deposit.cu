@@ -13,10 +13,9 @@
 // and |momentum| so that no cell can overflow.  A block of 512 particles
 // (Morton-ordered within its sub-box) whose stencils fit a tile of at most
 // 2048 cells accumulates in shared memory first and flushes each touched cell
-// with one global atomic per component; in a block whose particles span more,
-// each warp stages its own 64 particles in a tile of up to 256 cells; only
-// particles of neither kind add to global memory directly.  The global sums
-// of one cell (mass and the three momenta) share one 32-byte sector.
+// with one global atomic per component; other blocks add to global memory
+// directly.  The global sums of one cell (mass and the three momenta) share
+// one 32-byte sector.
 
 #include <cuda_runtime.h>
 
@@ -35,7 +34,6 @@ constexpr int kDepBlock = 256;
 constexpr int kDepPPT = 2;                          // particles per thread
 constexpr int kDepChunk = kDepBlock * kDepPPT;      // consecutive particles per block
 constexpr int kTileCap = 2048;                      // cells of a block's shared tile
-constexpr int kWarpCap = kTileCap / (kDepBlock / 32);  // cells of a warp's tile
 
 struct DepBox {
   int64_t off, n;         // particle range
@@ -190,10 +188,8 @@ __device__ __forceinline__ bool particle_stencil(const DepBox& B, const float p[
 // sub-box).  When they all belong to one sub-box and their stencils fit a
 // tile of at most kTileCap cells, the block adds into that tile in shared
 // memory and flushes each touched cell with one global atomic per component;
-// otherwise each warp tries the same with its own 64 particles and a tile of
-// kWarpCap cells, and a warp whose particles span more adds every
-// contribution to global memory directly.  Contributions that round to 0 in
-// fixed point are not added at all.
+// otherwise every contribution goes to global memory directly.  Contributions
+// that round to 0 in fixed point are not added at all.
 template <int KIND, bool VEL>
 __global__ void __launch_bounds__(kDepBlock, 3) k_deposit(DepParams P) {
   extern __shared__ unsigned long long s_acc[];  // [component][kTileCap]
@@ -205,10 +201,6 @@ __global__ void __launch_bounds__(kDepBlock, 3) k_deposit(DepParams P) {
   const int rot = (threadIdx.x & 31) % M3;
   const int64_t base = (int64_t)blockIdx.x * kDepChunk;
   const int64_t end = min(base + (int64_t)kDepChunk, P.n);
-  // a warp takes 32 * kDepPPT consecutive particles, 32 per round
-  auto pslot = [](int r) -> int64_t {
-    return (int64_t)((threadIdx.x >> 5) * (32 * kDepPPT) + r * 32 + (threadIdx.x & 31));
-  };
   const double scale_m = __ldg(&P.scales[0]), scale_p = __ldg(&P.scales[1]);
   if (threadIdx.x == 0) {
     const int b = find_dep_box(P.prefix, P.K, base);
@@ -219,20 +211,20 @@ __global__ void __launch_bounds__(kDepBlock, 3) k_deposit(DepParams P) {
   float4 q[kDepPPT], u[kDepPPT];
 #pragma unroll
   for (int r = 0; r < kDepPPT; ++r) {
-    const int64_t i = base + pslot(r);
+    const int64_t i = base + r * kDepBlock + threadIdx.x;
     q[r] = i < end ? __ldg(&P.pw[i]) : make_float4(0.f, 0.f, 0.f, 0.f);
     u[r] = (VEL && P.vel && i < end) ? __ldg(&P.vel[i]) : make_float4(0.f, 0.f, 0.f, 0.f);
   }
   __syncthreads();
   const bool one_box = s_ok;
 
-  // the warp's and the block's cell bounds (single-box blocks only)
-  int lo[3] = {0x7FFFFFFF, 0x7FFFFFFF, 0x7FFFFFFF}, hi[3] = {-0x7FFFFFFF, -0x7FFFFFFF, -0x7FFFFFFF};
+  // the block's cell bounds (single-box blocks only)
   if (one_box) {
     const DepBox& B = P.boxes[s_box];
+    int lo[3] = {0x7FFFFFFF, 0x7FFFFFFF, 0x7FFFFFFF}, hi[3] = {-0x7FFFFFFF, -0x7FFFFFFF, -0x7FFFFFFF};
 #pragma unroll
     for (int r = 0; r < kDepPPT; ++r) {
-      const int64_t i = base + pslot(r);
+      const int64_t i = base + r * kDepBlock + threadIdx.x;
       Stencil S;
       const float p[3] = {q[r].x, q[r].y, q[r].z};
       if (i < end && particle_stencil<KIND>(B, p, S)) {
@@ -271,30 +263,10 @@ __global__ void __launch_bounds__(kDepBlock, 3) k_deposit(DepParams P) {
     for (int k = threadIdx.x; k < C * kTileCap; k += kDepBlock) s_acc[k] = 0ull;
     __syncthreads();
   }
-  // A block whose particles span too many cells (its Morton range crosses a
-  // large Morton boundary) gives each warp a tile of its own 64 particles
-  // instead, in the warp's slice of the same shared memory.
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  bool wstaged = !staged && one_box && hi[0] >= lo[0] && hi[1] >= lo[1] && hi[2] >= lo[2];
-  int wsy = 1, wsz = 1, wcells = 0;
-  if (wstaged) {
-    wsy = hi[1] - lo[1] + 1;
-    wsz = hi[2] - lo[2] + 1;
-    const int64_t wc = (int64_t)(hi[0] - lo[0] + 1) * wsy * wsz;
-    wstaged = wc <= kWarpCap;
-    wcells = (int)wc;
-  }
-  unsigned long long* wacc = s_acc + warp * kWarpCap;
-  if (wstaged) {
-#pragma unroll
-    for (int m = 0; m < C; ++m)
-      for (int k = lane; k < kWarpCap; k += 32) wacc[m * kTileCap + k] = 0ull;
-    __syncwarp();
-  }
 
 #pragma unroll
   for (int r = 0; r < kDepPPT; ++r) {
-    const int64_t i = base + pslot(r);
+    const int64_t i = base + r * kDepBlock + threadIdx.x;
     if (i >= end) continue;
     const int b = one_box ? s_box : find_dep_box(P.prefix, P.K, i);
     const DepBox& B = P.boxes[b];
@@ -330,34 +302,11 @@ __global__ void __launch_bounds__(kDepBlock, 3) k_deposit(DepParams P) {
         const int k = ((c0 - tlo[0]) * sy + (c1 - tlo[1])) * sz + (c2 - tlo[2]);
 #pragma unroll
         for (int m = 0; m < C; ++m) atomicAdd(&s_acc[m * kTileCap + k], f[m]);
-      } else if (wstaged) {
-        const int k = ((c0 - lo[0]) * wsy + (c1 - lo[1])) * wsz + (c2 - lo[2]);
-#pragma unroll
-        for (int m = 0; m < C; ++m) atomicAdd(&wacc[m * kTileCap + k], f[m]);
       } else {
         const int64_t idx = ((int64_t)(B.origin[0] + c0) * P.G1 + (B.origin[1] + c1)) * P.G2 + (B.origin[2] + c2);
 #pragma unroll
         for (int m = 0; m < C; ++m) atomicAdd(&P.acc[C * idx + m], f[m]);
       }
-    }
-  }
-  if (wstaged) {
-    __syncwarp();
-    const DepBox& B = P.boxes[s_box];
-    const int syz = wsy * wsz;
-    for (int k = lane; k < wcells; k += 32) {
-      const int ci = k / syz, cj = (k - ci * syz) / wsz, ck = k - ci * syz - cj * wsz;
-      unsigned long long f[C], nz = 0ull;
-#pragma unroll
-      for (int m = 0; m < C; ++m) {
-        f[m] = wacc[m * kTileCap + k];
-        nz |= f[m];
-      }
-      if (nz == 0ull) continue;
-      const int64_t idx = ((int64_t)(B.origin[0] + lo[0] + ci) * P.G1 + (B.origin[1] + lo[1] + cj)) * P.G2 +
-                          (B.origin[2] + lo[2] + ck);
-#pragma unroll
-      for (int m = 0; m < C; ++m) atomicAdd(&P.acc[C * idx + m], f[m]);
     }
   }
   if (staged) {

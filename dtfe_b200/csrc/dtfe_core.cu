@@ -1260,160 +1260,6 @@ __global__ void __launch_bounds__(kInterpBlock, MINB) k_locate_eval(InterpParams
   fold_counters(P, n_loc, n_out, n_fail, wst);
 }
 
-// The fused walk + evaluation with the walks compacted (locate variants
-// 14..15).  Most cell centres lie in their seed tetrahedron; the rest walk a
-// few steps, and in k_locate_eval a warp waits for its longest walk with the
-// finished lanes idle.  Here a block takes 256 consecutive samples: every
-// lane tests its seed; the samples that leave it are listed in shared memory
-// with the neighbour they step into and walked by the block's first threads,
-// one per sample, so the walking warps are full; then every lane evaluates
-// its own sample (those that walked reload their tetrahedron) and the stores
-// are the warp-staged ones of k_locate_eval.  The walk from the neighbour
-// tests the face just crossed again (p is strictly beyond it, so it is never
-// the exit) and otherwise takes the same steps, so the located tetrahedra
-// are those of walk_locate.
-template <int S, int MINB>
-__global__ void __launch_bounds__(kInterpBlock, MINB) k_locate_eval_compact(InterpParams P, int* __restrict__ tet_c) {
-  constexpr int CMAX = (3 * S > 9) ? 3 * S : 9;
-  constexpr int kWarps = kInterpBlock / 32;
-  __shared__ __align__(16) float s_stage[kWarps][32 * CMAX];
-  __shared__ int s_start[kInterpBlock];   // listed sample: the tetrahedron its walk starts in
-  __shared__ short s_slot[kInterpBlock];  // listed sample: its thread in the block
-  __shared__ int s_final[kInterpBlock];   // per thread: the tetrahedron its sample's walk ended in
-  __shared__ int s_wcount[kWarps];
-  float* stage = s_stage[threadIdx.x >> 5];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t F = P.fields;
-  const bool want_grad = has_field(F, DTFE_VELOCITY_GRADIENT) || has_field(F, DTFE_VELOCITY_DIVERGENCE) ||
-                         has_field(F, DTFE_VELOCITY_SHEAR) || has_field(F, DTFE_VELOCITY_VORTICITY);
-  const bool want_vel = has_field(F, DTFE_VELOCITY) || want_grad;
-  const bool want_dens = has_field(F, DTFE_DENSITY);
-  const bool want_sc = S > 0 && (has_field(F, DTFE_SCALAR) || has_field(F, DTFE_SCALAR_GRADIENT));
-  const bool fix = P.fix != 0;
-  WalkStats wst{0, 0, 0};
-  unsigned n_loc = 0, n_out = 0, n_fail = 0;
-  for (int64_t chunk = blockIdx.x * (int64_t)kInterpBlock; chunk < P.n_total;
-       chunk += (int64_t)gridDim.x * kInterpBlock) {
-    const int64_t s = chunk + threadIdx.x;
-    const bool valid = s < P.n_total;
-    int64_t cell = -1;
-    double pc[3] = {0.0, 0.0, 0.0};
-    int v[4] = {0, 0, 0, 0};
-    float X[4][3];
-    int t = kOutside, start = -1;
-    bool listed = false;
-    if (valid) {
-      const SampleCell c = sample_cell(P, s);
-      cell = c.cell;
-      pc[0] = (double)c.x;
-      pc[1] = (double)c.y;
-      pc[2] = (double)c.z;
-      ++n_loc;
-      const int t0 = seed_of(P, c);
-      if (t0 >= 0) {
-        const float pf[3] = {c.x, c.y, c.z};
-        load_tet(P.tet_v, P.posd, t0, v, X);
-        ++wst.steps;
-        int zmask;
-        const int ef = first_exit_face_f32(X, pf, 15, zmask, wst.exact);
-        if (ef < 0) {
-          t = t0;
-          if (zmask) {
-            ++wst.tie;
-            const int b = canonical_tie(P.tet_v, P.tet_n, P.posd, t0, zmask, pc[0], pc[1], pc[2]);
-            if (b != t0) {
-              t = b;
-              load_tet(P.tet_v, P.posd, t, v, X);
-            }
-          }
-        } else {
-          const int nb = nb_of(__ldg(&P.tet_n[t0]), ef);
-          if (nb >= 0) {
-            listed = true;
-            start = nb;
-          }
-        }
-      }
-    }
-    // list the samples that walk on
-    const unsigned lm = __ballot_sync(0xffffffffu, listed);
-    if (lane == 0) s_wcount[warp] = __popc(lm);
-    __syncthreads();
-    int off = 0, total = 0;
-#pragma unroll
-    for (int w = 0; w < kWarps; ++w) {
-      const int cw = s_wcount[w];
-      off += w < warp ? cw : 0;
-      total += cw;
-    }
-    if (listed) {
-      const int k = off + __popc(lm & ((1u << lane) - 1u));
-      s_start[k] = start;
-      s_slot[k] = (short)threadIdx.x;
-    }
-    __syncthreads();
-    if (threadIdx.x < total) {
-      const int j = s_slot[threadIdx.x];
-      const SampleCell cj = sample_cell(P, chunk + j);
-      const double pj[3] = {(double)cj.x, (double)cj.y, (double)cj.z};
-      int vj[4];
-      float Xj[4][3];
-      s_final[j] = walk_locate<true>(P.tet_v, P.tet_n, P.posd, pj, s_start[threadIdx.x], P.max_steps - 1, vj, Xj,
-                                     wst);
-    }
-    __syncthreads();
-    if (listed) {
-      t = s_final[threadIdx.x];
-      if (t >= 0) load_tet(P.tet_v, P.posd, t, v, X);
-    }
-    CellOut e;
-    e.dens = 0.f;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) e.vel[c] = 0.f;
-#pragma unroll
-    for (int c = 0; c < 9; ++c) e.grad[c] = 0.f;
-#pragma unroll
-    for (int q = 0; q < S; ++q) {
-      e.sc[q] = 0.f;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) e.scg[3 * q + c] = 0.f;
-    }
-    if (valid) {
-      if (t == kWalkFail) {
-        ++n_fail;
-        t = kOutside;
-      }
-      n_out += t < 0;
-      tet_c[s] = t;
-      if (t >= 0) cell_eval<S>(v, X, pc, P.posd, P.vel4, P.scal, want_dens, want_vel, want_sc, fix, e);
-    }
-    const int64_t c0 = __shfl_sync(0xffffffffu, cell, 0);
-    const bool contig = __all_sync(0xffffffffu, valid && cell == c0 + lane) && (c0 % 4 == 0);
-    if (has_field(F, DTFE_DENSITY)) store_field<1>(P.out[DTFE_DENSITY], cell, valid, &e.dens, contig, c0, stage);
-    if (has_field(F, DTFE_VELOCITY)) store_field<3>(P.out[DTFE_VELOCITY], cell, valid, e.vel, contig, c0, stage);
-    if (has_field(F, DTFE_VELOCITY_GRADIENT))
-      store_field<9>(P.out[DTFE_VELOCITY_GRADIENT], cell, valid, e.grad, contig, c0, stage);
-    if (has_field(F, DTFE_VELOCITY_DIVERGENCE) || has_field(F, DTFE_VELOCITY_SHEAR) ||
-        has_field(F, DTFE_VELOCITY_VORTICITY)) {
-      float dv, sh[5], vo[3];
-      derived_fields(e.grad, dv, sh, vo);
-      if (has_field(F, DTFE_VELOCITY_DIVERGENCE))
-        store_field<1>(P.out[DTFE_VELOCITY_DIVERGENCE], cell, valid, &dv, contig, c0, stage);
-      if (has_field(F, DTFE_VELOCITY_SHEAR))
-        store_field<5>(P.out[DTFE_VELOCITY_SHEAR], cell, valid, sh, contig, c0, stage);
-      if (has_field(F, DTFE_VELOCITY_VORTICITY))
-        store_field<3>(P.out[DTFE_VELOCITY_VORTICITY], cell, valid, vo, contig, c0, stage);
-    }
-    if (S > 0 && has_field(F, DTFE_SCALAR))
-      store_field<(S > 0 ? S : 1)>(P.out[DTFE_SCALAR], cell, valid, e.sc, contig, c0, stage);
-    if (S > 0 && has_field(F, DTFE_SCALAR_GRADIENT))
-      store_field<(S > 0 ? 3 * S : 1)>(P.out[DTFE_SCALAR_GRADIENT], cell, valid, e.scg, contig, c0, stage);
-    // s_start / s_slot / s_final are rewritten by the next chunk
-    __syncthreads();
-  }
-  fold_counters(P, n_loc, n_out, n_fail, wst);
-}
-
 // Zeroes every sample of a pencil of nz samples after its first outside one
 // (tet_c[s0 + k] < 0): the pencil's samples are tet_c[s0 .. s0 + nz), its
 // cells P.out rows c0 .. c0 + nz.  One warp reads the located tetrahedra 32 at
@@ -2196,17 +2042,14 @@ void drop_graph(dtfe_handle h) {
 // thread); variants 9..11 walk and evaluate in one kernel (3, 2 or 4 blocks
 // per SM; for the averaging methods they walk as variant 3); variants 12..13
 // do the same over the interleaved 32-byte tetrahedron records (4 or 3
-// blocks per SM); variants 14..15 compact the walks that leave their seed
-// (k_locate_eval_compact, 3 or 2 blocks per SM).  Evaluation variants:
-// register budget of the evaluation kernel.
+// blocks per SM).  Evaluation variants: register budget of the evaluation
+// kernel.
 constexpr int kNumRasterVariants = 3;
 struct LocVariant { int block, minb, r; };
 constexpr LocVariant kWalkVariants[] = {{256, 3, 1}, {256, 2, 1}, {256, 4, 1}, {256, 3, 2}, {256, 4, 2}, {256, 3, 4}};
 constexpr int kNumWalkVariants = sizeof(kWalkVariants) / sizeof(kWalkVariants[0]);
-struct FusedVariant { int minb; bool rec; bool compact; };
-constexpr FusedVariant kFused[] = {{3, false, false}, {2, false, false}, {4, false, false},
-                                   {4, true, false},  {3, true, false},  {3, false, true},
-                                   {2, false, true}};
+struct FusedVariant { int minb; bool rec; };
+constexpr FusedVariant kFused[] = {{3, false}, {2, false}, {4, false}, {4, true}, {3, true}};
 constexpr int kFirstFused = kNumRasterVariants + kNumWalkVariants;
 constexpr int kNumLocVariants = kFirstFused + sizeof(kFused) / sizeof(kFused[0]);
 inline bool uses_records(int loc_variant) {
@@ -2376,10 +2219,7 @@ void launch_fused(int fv, const InterpParams& P, int* tet_c, cudaStream_t st, un
   const FusedVariant& F = kFused[fv];
   // record walks are built for the scalar counts a handle accepts (0-4, 8)
   constexpr bool kRecOk = S <= 4 || S == 8;
-  if (F.compact) {
-    if (F.minb == 2) k_locate_eval_compact<S, 2><<<grid, block, 0, st>>>(P, tet_c);
-    else k_locate_eval_compact<S, 3><<<grid, block, 0, st>>>(P, tet_c);
-  } else if (F.rec && kRecOk) {
+  if (F.rec && kRecOk) {
     if (F.minb == 4) k_locate_eval<S, 4, kRecOk><<<grid, block, 0, st>>>(P, tet_c);
     else k_locate_eval<S, 3, kRecOk><<<grid, block, 0, st>>>(P, tet_c);
   } else if (F.minb == 2) {

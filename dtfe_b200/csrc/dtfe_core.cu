@@ -1179,9 +1179,7 @@ __global__ void __launch_bounds__(kInterpBlock, MINB) k_eval_centre(InterpParams
 // the tetrahedron the walk ends in, whose vertices and positions are still
 // in registers; the warp is converged again after the walk, so the
 // evaluation and the staged stores run as in k_eval_centre.
-// PRE (with REC): the seed's velocities are prefetched into L1 while the
-// walk tests the seed (walk_locate_rec).
-template <int S, int MINB, bool REC = false, bool PRE = false>
+template <int S, int MINB, bool REC = false>
 __global__ void __launch_bounds__(kInterpBlock, MINB) k_locate_eval(InterpParams P, int* __restrict__ tet_c) {
   constexpr int CMAX = (3 * S > 9) ? 3 * S : 9;
   __shared__ __align__(16) float s_stage[kInterpBlock / 32][32 * CMAX];
@@ -1225,7 +1223,7 @@ __global__ void __launch_bounds__(kInterpBlock, MINB) k_locate_eval(InterpParams
       const int t0 = seed_of(P, c);
       int t = t0 < 0 ? kOutside
                      : (REC ? walk_locate_rec<true>(P.tet_rec, P.tet_v, P.tet_n, P.posd, pc, t0, P.max_steps, v, X,
-                                                    D, wst, PRE && want_vel ? P.vel4 : nullptr)
+                                                    D, wst)
                             : walk_locate<true>(P.tet_v, P.tet_n, P.posd, pc, t0, P.max_steps, v, X, wst));
       ++n_loc;
       if (t == kWalkFail) {
@@ -2044,16 +2042,14 @@ void drop_graph(dtfe_handle h) {
 // thread); variants 9..11 walk and evaluate in one kernel (3, 2 or 4 blocks
 // per SM; for the averaging methods they walk as variant 3); variants 12..13
 // do the same over the interleaved 32-byte tetrahedron records (4 or 3
-// blocks per SM); variants 14..15 add the L1 prefetch of the seed's
-// velocities (4 or 3 blocks per SM).  Evaluation variants: register budget
-// of the evaluation kernel.
+// blocks per SM).  Evaluation variants: register budget of the evaluation
+// kernel.
 constexpr int kNumRasterVariants = 3;
 struct LocVariant { int block, minb, r; };
 constexpr LocVariant kWalkVariants[] = {{256, 3, 1}, {256, 2, 1}, {256, 4, 1}, {256, 3, 2}, {256, 4, 2}, {256, 3, 4}};
 constexpr int kNumWalkVariants = sizeof(kWalkVariants) / sizeof(kWalkVariants[0]);
-struct FusedVariant { int minb; bool rec; bool pre; };
-constexpr FusedVariant kFused[] = {{3, false, false}, {2, false, false}, {4, false, false}, {4, true, false},
-                                   {3, true, false},  {4, true, true},   {3, true, true}};
+struct FusedVariant { int minb; bool rec; };
+constexpr FusedVariant kFused[] = {{3, false}, {2, false}, {4, false}, {4, true}, {3, true}};
 constexpr int kFirstFused = kNumRasterVariants + kNumWalkVariants;
 constexpr int kNumLocVariants = kFirstFused + sizeof(kFused) / sizeof(kFused[0]);
 inline bool uses_records(int loc_variant) {
@@ -2223,10 +2219,7 @@ void launch_fused(int fv, const InterpParams& P, int* tet_c, cudaStream_t st, un
   const FusedVariant& F = kFused[fv];
   // record walks are built for the scalar counts a handle accepts (0-4, 8)
   constexpr bool kRecOk = S <= 4 || S == 8;
-  if (F.rec && kRecOk && F.pre) {
-    if (F.minb == 4) k_locate_eval<S, 4, kRecOk, kRecOk><<<grid, block, 0, st>>>(P, tet_c);
-    else k_locate_eval<S, 3, kRecOk, kRecOk><<<grid, block, 0, st>>>(P, tet_c);
-  } else if (F.rec && kRecOk) {
+  if (F.rec && kRecOk) {
     if (F.minb == 4) k_locate_eval<S, 4, kRecOk><<<grid, block, 0, st>>>(P, tet_c);
     else k_locate_eval<S, 3, kRecOk><<<grid, block, 0, st>>>(P, tet_c);
   } else if (F.minb == 2) {

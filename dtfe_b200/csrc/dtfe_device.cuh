@@ -352,25 +352,15 @@ __device__ __forceinline__ int walk_locate(const int4* __restrict__ tet_v, const
 // vertex.  The vertices' densities (posd .w) ride along in D for the
 // evaluation.  Same tests in the same order as walk_locate, so the same
 // tetrahedron is located (ties resolved by canonical_tie on the plain arrays).
-//
-// prefetch (may be null): a per-vertex array (the velocities) that the
-// caller reads for the located tetrahedron.  Most cell centres lie in their
-// seed, so the seed's four entries are prefetched into L1 as soon as its
-// vertices are known, and their latency overlaps the orientation tests
-// instead of following them.
 template <bool FLOAT_POINT = false>
 __device__ __forceinline__ int walk_locate_rec(const int4* __restrict__ rec, const int4* __restrict__ tet_v,
                                                const int4* __restrict__ tet_n, const float4* __restrict__ posd,
                                                const double p[3], int t, int max_steps, int v[4], float X[4][3],
-                                               float D[4], WalkStats& st, const float4* prefetch = nullptr) {
+                                               float D[4], WalkStats& st) {
   const float pf[3] = {(float)p[0], (float)p[1], (float)p[2]};
   int4 q = __ldg(&rec[2 * (int64_t)t]);
   int4 n = __ldg(&rec[2 * (int64_t)t + 1]);
   v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
-  if (prefetch) {
-#pragma unroll
-    for (int a = 0; a < 4; ++a) asm volatile("prefetch.global.L1 [%0];" ::"l"(prefetch + v[a]));
-  }
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     const float4 r = __ldg(&posd[v[a]]);

@@ -30,7 +30,9 @@ def _plan(n, grid, threads, seed, disp=0.8, scalars=1):
 
 @pytest.mark.parametrize("n,grid,threads,k,extensive", [(16, (16, 16, 16), 1, 32, False),
                                                         (20, (24, 20, 18), 8, 32, True),
-                                                        (18, (12, 12, 12), 4, 16, False)])
+                                                        (18, (12, 12, 12), 4, 16, False),
+                                                        (18, (12, 14, 10), 2, 64, False),
+                                                        (16, (10, 10, 10), 1, 100, True)])
 def test_sph_matches_oracle(gpu_built, n, grid, threads, k, extensive):
     from dtfe_b200.device import DeviceDTFE
     plan = _plan(n, grid, threads, seed=n + k)

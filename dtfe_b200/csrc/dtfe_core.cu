@@ -657,6 +657,7 @@ __device__ __forceinline__ void add_volume(const VolSums& S, int64_t t, const in
 }
 
 constexpr unsigned long long kEmptySeed = ~0ull;
+constexpr int kVolTPT = 2;  // tetrahedra per thread of the step's volume kernel (4: slower)
 template <bool DO_BINS>
 __global__ void __launch_bounds__(kVolBlock) k_tet_volume_bins(
     int64_t T, const int4* __restrict__ tet_v, const float4* __restrict__ posd, VolSums VS,
@@ -706,6 +707,78 @@ __global__ void __launch_bounds__(kVolBlock) k_tet_volume_bins(
   if (DO_BINS) {
     // segmented minimum over runs of equal keys; the run's first lane issues
     const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long ov = __shfl_down_sync(0xffffffffu, val, o);
+      const int ok = __shfl_down_sync(0xffffffffu, key, o);
+      if (lane + o < 32 && ok == key && ov < val) val = ov;
+    }
+    const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+    if (key >= 0 && (lane == 0 || prev != key)) atomicMin(&bins[key], val);
+  }
+}
+
+// k_tet_volume_bins<true> with TPT tetrahedra per thread: a warp takes
+// 32 TPT consecutive tetrahedra, lane l the l-th, (32 + l)-th, ..., and issues
+// all their records' loads, then all their position gathers, before any
+// arithmetic, so TPT times the gathers are in flight per thread.
+template <int TPT>
+__global__ void __launch_bounds__(kVolBlock) k_tet_volume_bins2(
+    int64_t T, const int4* __restrict__ tet_v, const float4* __restrict__ posd, VolSums VS,
+    const dtfe_subbox* __restrict__ boxes, const int64_t* __restrict__ tprefix,
+    const int64_t* __restrict__ bin_offset, int K, const float* __restrict__ xs, const float* __restrict__ ys,
+    const float* __restrict__ zs, unsigned long long* __restrict__ bins) {
+  const int lane = threadIdx.x & 31;
+  const int64_t base = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * (32 * TPT);
+  int4 q[TPT];
+#pragma unroll
+  for (int r = 0; r < TPT; ++r) {
+    const int64_t t = base + 32 * r + lane;
+    q[r] = t < T ? __ldg(&tet_v[t]) : make_int4(0, 0, 0, 0);
+  }
+  float X[TPT][4][3];
+#pragma unroll
+  for (int r = 0; r < TPT; ++r) {
+    const int v[4] = {q[r].x, q[r].y, q[r].z, q[r].w};
+#pragma unroll
+    for (int a = 0; a < 4; ++a) load_posf(posd, v[a], X[r][a]);
+  }
+#pragma unroll
+  for (int r = 0; r < TPT; ++r) {
+    const int64_t t = base + 32 * r + lane;
+    int key = -1;
+    unsigned long long val = kEmptySeed;
+    if (t < T) {
+      const int v[4] = {q[r].x, q[r].y, q[r].z, q[r].w};
+      double D[4][3];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) D[a][c] = (double)X[r][a][c];
+      add_volume(VS, t, v, orient_det(D[0], D[1], D[2], D[3]) / 6.0);
+      const int b = find_box(tprefix, K, t);
+      const dtfe_subbox& B = boxes[b];
+      int idx[3];
+      float cen[3];
+      bool inside = true;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        cen[c] = 0.25f * ((X[r][0][c] + X[r][1][c]) + (X[r][2][c] + X[r][3][c]));
+        const float f = floorf(__fdividef(cen[c] - __ldg(&B.lo[c]), __ldg(&B.dx[c])));
+        const int n = __ldg(&B.tile_dims[c]);
+        inside = inside && (f >= 0.f && f < (float)n);
+        idx[c] = inside ? (int)f : 0;
+      }
+      if (inside) {
+        key = (int)(__ldg(&bin_offset[b]) +
+                    ((int64_t)idx[0] * __ldg(&B.tile_dims[1]) + idx[1]) * __ldg(&B.tile_dims[2]) + idx[2]);
+        const float dxs = cen[0] - __ldg(&xs[B.coord_offset[0] + idx[0]]);
+        const float dys = cen[1] - __ldg(&ys[B.coord_offset[1] + idx[1]]);
+        const float dzs = cen[2] - __ldg(&zs[B.coord_offset[2] + idx[2]]);
+        const float d2 = dxs * dxs + dys * dys + dzs * dzs;
+        val = ((unsigned long long)__float_as_uint(d2) << 32) | (unsigned)t;
+      }
+    }
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const unsigned long long ov = __shfl_down_sync(0xffffffffu, val, o);
@@ -2163,7 +2236,7 @@ int launch_prep(dtfe_handle h) {
   } else if (h->K > 0) {
     DTFE_CUDA_TRY(cudaMemsetAsync(h->bins, 0xFF, sizeof(unsigned long long) * h->n_cells, st));
     if (h->T > 0)
-      k_tet_volume_bins<true><<<blocks_for(h->T, kVolBlock), kVolBlock, 0, st>>>(
+      k_tet_volume_bins2<kVolTPT><<<blocks_for((h->T + kVolTPT - 1) / kVolTPT, kVolBlock), kVolBlock, 0, st>>>(
           h->T, h->tet_v, h->posd, VS, h->boxes, h->tet_prefix, h->bin_offset, h->K, h->xs, h->ys, h->zs,
           h->bins);
   } else if (h->T > 0) {

@@ -111,3 +111,18 @@ def test_vertex_codes_rebuild_the_padded_vertices():
             P.vertex_codes(plan, pos)
     finally:
         plan.xyz[...] = bad
+
+
+def test_vertex_codes_non_periodic():
+    """Without periodic images every vertex is its particle unshifted
+    (image 13), and the codes index the particle arrays directly."""
+    import numpy as np
+    from dtfe_b200 import plan as P
+    rng = np.random.default_rng(41)
+    pos = (rng.random((2000, 3)) * 100.0).astype(np.float32)
+    plan = P.make_plan(pos, np.ones(len(pos), np.float32), None, None, grid=(10, 10, 10), n_threads=4,
+                       periodic=False, padding=np.full(6, 3.0, np.float32), average_density_value=2e-3)
+    codes, L = P.vertex_codes(plan, pos)
+    assert np.all((codes >> np.uint32(27)) == 13)
+    src = codes & np.uint32((1 << 27) - 1)
+    assert np.array_equal(pos[src], plan.xyz)

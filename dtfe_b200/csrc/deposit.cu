@@ -11,10 +11,10 @@
 // so the grid is deterministic and independent of the order in which threads
 // add.  The fixed-point scales are powers of two chosen from the total |mass|
 // and |momentum| so that no cell can overflow.  A block of 512 particles
-// (Morton-ordered within its sub-box) whose stencils fit a tile of at most
-// 2048 cells accumulates in shared memory first and flushes each touched cell
-// with one global atomic per component; other blocks add to global memory
-// directly.  The global sums of one cell (mass and the three momenta) share
+// (256 for TSC; Morton-ordered within its sub-box) whose stencils fit a tile
+// of at most 2048 cells accumulates in shared memory first and flushes each
+// touched cell with one global atomic per component; other blocks add to
+// global memory directly.  The global sums of one cell (mass and the three momenta) share
 // one 32-byte sector.
 
 #include <cuda_runtime.h>
@@ -31,8 +31,9 @@ extern "C" int dtfe_internal_set_error(int code, const char* msg);
 namespace {
 
 constexpr int kDepBlock = 256;
-constexpr int kDepPPT = 2;                          // particles per thread
-constexpr int kDepChunk = kDepBlock * kDepPPT;      // consecutive particles per block
+// particles per thread: TSC's 3^3 stencils widen a block's tile, so its
+// blocks take 256 particles, NGP's and CIC's 512
+__host__ __device__ constexpr int dep_ppt(int kind) { return kind == 2 ? 1 : 2; }
 constexpr int kTileCap = 2048;                      // cells of a block's shared tile
 
 struct DepBox {
@@ -184,10 +185,11 @@ __device__ __forceinline__ bool particle_stencil(const DepBox& B, const float p[
 }
 
 // KIND: 0 NGP, 1 CIC, 2 TSC; VEL: momentum accumulated beside the mass.
-// A block takes kDepChunk consecutive particles (Morton-ordered within their
-// sub-box).  When they all belong to one sub-box and their stencils fit a
-// tile of at most kTileCap cells, the block adds into that tile in shared
-// memory and flushes each touched cell with one global atomic per component;
+// A block takes 256 dep_ppt(KIND) consecutive particles (Morton-ordered
+// within their sub-box).  When they all belong to one sub-box and their
+// stencils fit a tile of at most kTileCap cells, the block adds into that
+// tile in shared memory and flushes each touched cell with one global atomic
+// per component;
 // otherwise every contribution goes to global memory directly.  Contributions
 // that round to 0 in fixed point are not added at all.
 template <int KIND, bool VEL>
@@ -199,6 +201,7 @@ __global__ void __launch_bounds__(kDepBlock, 3) k_deposit(DepParams P) {
   constexpr int M = KIND == 0 ? 1 : (KIND == 1 ? 2 : 3);
   constexpr int M3 = M * M * M;
   const int rot = (threadIdx.x & 31) % M3;
+  constexpr int kDepPPT = dep_ppt(KIND), kDepChunk = kDepBlock * kDepPPT;
   const int64_t base = (int64_t)blockIdx.x * kDepChunk;
   const int64_t end = min(base + (int64_t)kDepChunk, P.n);
   const double scale_m = __ldg(&P.scales[0]), scale_p = __ldg(&P.scales[1]);
@@ -623,7 +626,8 @@ extern "C" int dtfe_gpu_deposit_impl(void* stream, int32_t kind, const float* xy
   P.scales = d_scales;
   P.acc = acc;
   if (n > 0) {
-    const unsigned nb = (unsigned)((n + kDepChunk - 1) / kDepChunk);
+    const int64_t chunk = (int64_t)kDepBlock * dep_ppt(kind);
+    const unsigned nb = (unsigned)((n + chunk - 1) / chunk);
     if (kind == 0) launch_deposit<0>(velocity_dev != nullptr, nb, st, P);
     else if (kind == 1) launch_deposit<1>(velocity_dev != nullptr, nb, st, P);
     else launch_deposit<2>(velocity_dev != nullptr, nb, st, P);

@@ -223,6 +223,11 @@ def gpu() -> C.CDLL:
         lib.dtfe_gpu_variant_counts.argtypes = [vp]
         lib.dtfe_vertex_density_noalloc.argtypes = [vp, vp, C.c_int64, vp, vp, C.c_int64, C.c_double, vp, vp]
         lib.dtfe_vertex_density_noalloc.restype = C.c_int
+        lib.dtfe_gpu_tessellate.argtypes = [vp, C.c_int32, vp, vp, C.POINTER(vp)]
+        lib.dtfe_gpu_tess_sizes.argtypes = [vp, vp, vp]
+        lib.dtfe_gpu_tess_export.argtypes = [vp, vp, C.c_int32]
+        lib.dtfe_gpu_tess_stats.argtypes = [vp, vp, C.c_int32]
+        lib.dtfe_gpu_tess_release.argtypes = [vp]
         _gpu = lib
     return _gpu
 

@@ -26,7 +26,8 @@ NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 HOST_SOURCES = ["delaunay.cpp", "host_plan.cpp", "plan_build.cpp", "host_io.cpp"]
-GPU_SOURCES = ["dtfe_core.cu", "deposit.cu", "adjoint.cu", "sph.cu", "method1.cu", "noalloc.cu"]
+GPU_SOURCES = ["dtfe_core.cu", "deposit.cu", "adjoint.cu", "sph.cu", "method1.cu", "noalloc.cu",
+               "delaunay.cu"]
 
 
 def _run(cmd: list[str]) -> None:

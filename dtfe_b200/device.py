@@ -422,3 +422,60 @@ class DeviceDTFE:
         out = np.empty(len(pts), np.int32)
         N.check(self.lib.dtfe_gpu_locate_points(self.h, len(pts), pts.ctypes.data, int(start), out.ctypes.data))
         return out
+
+
+TESS_REASONS = ("duplicate", "candidates", "star", "no_start", "flat", "undecided", "tie", "not_delaunay",
+                "link", "open", "overflow", "run")
+
+
+def tessellate(point_sets: list, device: int = 0, return_ms: bool = False, return_stats: bool = False):
+    """Delaunay tessellations of float32 point sets on the GPU
+    (dtfe_gpu_tessellate), in the host tessellator's canonical order.
+
+    Returns [(tet_v (T,4) int32 with indices local to the set, status)];
+    status 0 means the set was certified on the device, any other value
+    (flag bits of dtfe_gpu_tess_sizes) that the set needs the host
+    tessellator (co-spherical or coplanar points, capacity limits) and its
+    tet_v is empty.  With return_ms, also the device time of the call in ms
+    (CUDA events around it on its stream); with return_stats, the number of
+    vertex stars that failed for each of TESS_REASONS."""
+    import torch
+
+    lib = N.gpu()
+    k = len(point_sets)
+    sizes = [len(p) for p in point_sets]
+    vpre = np.zeros(k + 1, np.int64)
+    vpre[1:] = np.cumsum(sizes)
+    xyz = np.ascontiguousarray(np.concatenate([np.asarray(p, np.float32).reshape(-1, 3) for p in point_sets]))
+    dev = torch.device("cuda", device)
+    with torch.cuda.device(dev):
+        xyz_d = torch.from_numpy(xyz).to(dev)
+        stream = torch.cuda.current_stream(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        handle = C.c_void_p()
+        e0.record(stream)
+        N.check(lib.dtfe_gpu_tessellate(C.c_void_p(stream.cuda_stream), k, vpre.ctypes.data,
+                                        C.c_void_p(xyz_d.data_ptr()), C.byref(handle)))
+        e1.record(stream)
+        try:
+            tpre = np.zeros(k + 1, np.int64)
+            status = np.zeros(k, np.int32)
+            N.check(lib.dtfe_gpu_tess_sizes(handle, tpre.ctypes.data, status.ctypes.data))
+            why = np.zeros(len(TESS_REASONS) + 2, np.int64)
+            N.check(lib.dtfe_gpu_tess_stats(handle, why.ctypes.data, len(why)))
+            tv = np.empty((int(tpre[-1]), 4), np.int32)
+            if len(tv):
+                N.check(lib.dtfe_gpu_tess_export(handle, tv.ctypes.data, 0))
+        finally:
+            lib.dtfe_gpu_tess_release(handle)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+    out = [(tv[tpre[s]:tpre[s + 1]] - np.int32(vpre[s]), int(status[s])) for s in range(k)]
+    res = [out]
+    if return_ms:
+        res.append(ms)
+    if return_stats:
+        d = dict(zip(TESS_REASONS, (int(x) for x in why)))
+        d["first_vertex"], d["first_reason"] = int(why[-2]), int(why[-1])
+        res.append(d)
+    return res[0] if len(res) == 1 else tuple(res)

@@ -461,6 +461,43 @@ int dtfe_gpu_download_tets(dtfe_handle h, int32_t* tet_v, int32_t* tet_n);
  * src/message.h:57-64). */
 int dtfe_gpu_set_max_walk_steps(dtfe_handle h, int32_t max_walk_steps);
 
+/* Delaunay tessellation on the device, the counterpart of
+ * delaunayTriangulation() (src/CGAL_triangulation/triangulation.cpp:162-195)
+ * and of the host tessellator dtfe_tessellate / dtfe_tess_sizes /
+ * dtfe_tess_export / dtfe_tess_release (include/dtfe_host.h), whose output
+ * it reproduces: n_sets independent float32 point sets, set s being the
+ * vertices vprefix[s] .. vprefix[s+1]-1 (host array, vprefix[0] = 0) of the
+ * DEVICE array xyz (3 floats per vertex).  Each set gives its finite
+ * Delaunay tetrahedra, positively oriented, each in its smallest even vertex
+ * rotation, sorted by the Morton key of the FP64 centroid and then by the
+ * vertex tuple; vertex ids are global (index into xyz).  stream: a
+ * cudaStream_t (NULL = the default stream); the call returns when the
+ * tessellation is complete.  Every tetrahedron is certified (empty
+ * circumsphere over the whole set, exact predicates).  A set whose certificate
+ * meets an exact tie (five co-spherical or four coplanar deciding points,
+ * duplicates), a non-finite coordinate or a capacity limit is not
+ * tessellated: its status is non-zero (flag bits: 1 tie, 2 capacity,
+ * 4 output overflow, 8 certificate repair failed, 16 exact arithmetic out of
+ * range, 32 non-finite or flat input) and it has no tetrahedra; the host
+ * tessellator, whose insertion order breaks such ties as CGAL's does, is then
+ * the one to use for it. */
+int dtfe_gpu_tessellate(void* stream, int32_t n_sets, const int64_t* vprefix, const float* xyz, void** tess);
+/* tprefix (n_sets+1, may be NULL): tetrahedron offsets of the sets in the
+ * exported array; status (n_sets, may be NULL): 0 or the flag bits above. */
+int dtfe_gpu_tess_sizes(void* tess, int64_t* tprefix, int32_t* status);
+/* Copies the tprefix[n_sets] tetrahedra (4 int32 each) to tet_v: a host
+ * pointer, or a device pointer when to_device is non-zero. */
+int dtfe_gpu_tess_export(void* tess, int32_t* tet_v, int32_t to_device);
+/* Why stars failed, summed over all sets: counts[i] (i < n, up to 12) is
+ * the number of vertex stars that met reason i: 0 duplicate point,
+ * 1 candidate capacity, 2 star capacity, 3 no start triangle, 4 all points
+ * on one plane, 5 exact arithmetic out of range, 6 exact tie, 7 face not
+ * Delaunay, 8 inconsistent link, 9 unclosed link, 10 output overflow,
+ * 11 more than 64 equal Morton keys; counts[12] is the first vertex whose
+ * star failed (global id, -1 if none) and counts[13] its reason. */
+int dtfe_gpu_tess_stats(void* tess, int64_t* counts, int32_t n);
+int dtfe_gpu_tess_release(void* tess);
+
 /* Vertex densities without any device allocation, for callers that cannot
  * let a library allocate: host applications that hand out all device memory
  * from their own fixed-budget pool, or latency-critical loops where an

@@ -73,6 +73,7 @@ def parse():
                     help="particles per side of the redshift-cone / user-point workload (one box)")
     ap.add_argument("--no-sampling", action="store_true")
     ap.add_argument("--no-output", action="store_true", help="skip the binary output-file leg")
+    ap.add_argument("--no-tess", action="store_true", help="skip the GPU tessellation leg")
     ap.add_argument("--scalars", type=int, default=0,
                     help="extra N(0,1) scalar fields per particle, interpolated with their gradients")
     ap.add_argument("--fp64-cells", type=int, default=50000,
@@ -92,6 +93,25 @@ def host_threads(req: int) -> int:
         return len(os.sched_getaffinity(0))
     except Exception:
         return os.cpu_count() or 1
+
+
+def tessellation_leg(plan) -> dict:
+    """The Delaunay tessellations of the step's padded sub-box point sets on
+    the GPU (dtfe_gpu_tessellate, CUDA events around the call) beside the host
+    tessellator's time for the same sets (host_prep_s.tessellation_s), and
+    whether every set's tetrahedra equal the host's array for array."""
+    from dtfe_b200 import device as D
+    sets = [plan.xyz[b.vert_offset:b.vert_offset + b.n_verts] for b in plan.boxes]
+    D.tessellate([sets[0][:64]])  # module load, small allocations
+    out, ms, why = D.tessellate(sets, return_ms=True, return_stats=True)
+    equal = []
+    for b, (tv, st) in zip(plan.boxes, out):
+        host = plan.tet_v[b.tet_offset:b.tet_offset + b.n_tets] - np.int32(b.vert_offset)
+        equal.append(bool(st == 0 and tv.shape == host.shape and np.array_equal(tv, host)))
+    return {"gpu_ms": ms, "host_s": plan.timings.get("tessellation_s"), "sets": len(sets),
+            "vertices": int(sum(len(x) for x in sets)), "tetrahedra": int(sum(len(tv) for tv, _ in out)),
+            "equal_to_host": all(equal), "sets_equal": int(sum(equal)),
+            "status": [st for _, st in out if st], "failed_stars": {k: v for k, v in why.items() if v > 0}}
 
 
 def build_workload(n: int, rank: int, threads: int, scalars: int = 0):
@@ -1254,6 +1274,10 @@ def run_ours(args):
     if side and not args.no_sampling:
         sampling = sampling_leg(args, local, threads, rank == 0 and not args.no_cpu)
 
+    tess = None
+    if side and not args.no_tess:
+        tess = tessellation_leg(plan)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         check = (outs, fields, args.fp64_cells) if args.fp64_cells > 0 else None
@@ -1289,6 +1313,7 @@ def run_ours(args):
                         "bar": 1e-5}
                        if cpu and cpu.get("fp64_check") else None),
         "host_prep_s": plan.timings,
+        "tessellation": tess,
     }
     dev.close()
     if world > 1:

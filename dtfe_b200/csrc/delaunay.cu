@@ -259,7 +259,7 @@ __device__ __forceinline__ double det3d(const double* u, const double* v, const 
 }
 
 // Filtered in-sphere test (the host's double evaluation and bound).
-__device__ __forceinline__ int insphere_f(float3 a, float3 b, float3 c, float3 d, float3 e) {
+__device__ __noinline__ int insphere_f(float3 a, float3 b, float3 c, float3 d, float3 e) {
   const float3 P[4] = {a, b, c, d};
   double r[4][3], lift[4];
 #pragma unroll
@@ -404,24 +404,73 @@ __device__ __forceinline__ float3 point(const Ctx& C, int id) {
   return make_float3(__ldg(q), __ldg(q + 1), __ldg(q + 2));
 }
 
-// Among the lanes' apex candidates for face (p, u, v) (best >= 0 on a lane,
-// sphere sb), the one whose sphere holds none of the others: the apices are
-// ordered by the position of their sphere centre along the face normal n
-// (smaller = better); overlapping error intervals are resolved with the exact
-// in-sphere sign.  Returns the id (coordinates in W), -1 when no lane has
-// one, -2 on an exact tie (flag set).
-__device__ int warp_select(Ctx& C, float3 U, float3 V, int best, float3 Bx, const Sphere& sb, bool tied, float3& W) {
-  const float3 P = C.P;
-  const double A[3] = {(double)U.x - P.x, (double)U.y - P.y, (double)U.z - P.z};
-  const double Bv[3] = {(double)V.x - P.x, (double)V.y - P.y, (double)V.z - P.z};
-  const double nv[3] = {A[1] * Bv[2] - A[2] * Bv[1], A[2] * Bv[0] - A[0] * Bv[2], A[0] * Bv[1] - A[1] * Bv[0]};
+// A face (p, u, v) with its normal n = (u - p) x (v - p) in double and the
+// magnitudes of n's two products per component: orient(p, u, v, x) is the
+// sign of (x - p).n, filtered with the host's orientation bound (the same
+// determinant expanded along x's row) and exact otherwise.
+struct Face {
+  float3 Pf, Uf, Vf;
+  double P[3], n[3], na[3];
+};
+
+__device__ __forceinline__ Face make_face(float3 P, float3 U, float3 V) {
+  Face F;
+  F.Pf = P;
+  F.Uf = U;
+  F.Vf = V;
+  F.P[0] = P.x; F.P[1] = P.y; F.P[2] = P.z;
+  const double b[3] = {(double)U.x - P.x, (double)U.y - P.y, (double)U.z - P.z};
+  const double c[3] = {(double)V.x - P.x, (double)V.y - P.y, (double)V.z - P.z};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int i = (k + 1) % 3, j = (k + 2) % 3;
+    const double m1 = b[i] * c[j], m2 = b[j] * c[i];
+    F.n[k] = m1 - m2;
+    F.na[k] = fabs(m1) + fabs(m2);
+  }
+  return F;
+}
+
+__device__ __forceinline__ int orient_face(const Face& F, float3 X) {
+  const double d0 = (double)X.x - F.P[0], d1 = (double)X.y - F.P[1], d2 = (double)X.z - F.P[2];
+  const double det = d0 * F.n[0] + d1 * F.n[1] + d2 * F.n[2];
+  const double perm = fabs(d0) * F.na[0] + fabs(d1) * F.na[1] + fabs(d2) * F.na[2];
+  const double bound = kOrientErr * perm;
+  if (det > bound) return 1;
+  if (-det > bound) return -1;
+  return orient_exact_f(F.Pf, F.Uf, F.Vf, X);
+}
+
+// In-sphere sign of x for the positively oriented (p, u, v, b) whose sphere
+// is S: decided by the distance to the bounded centre when x is clearly in
+// or out, else by the determinant.
+__device__ __forceinline__ int insphere_face(const Face& F, float3 B, const Sphere& S, float3 X) {
+  if (S.ok) {
+    const double dx = (double)X.x - S.c[0], dy = (double)X.y - S.c[1], dz = (double)X.z - S.c[2];
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    const double hi = S.r + 2.0 * S.err;
+    if (d2 > hi * hi * (1.0 + 1e-9)) return -1;
+    const double lo = S.r - 2.0 * S.err;
+    if (lo > 0.0 && d2 < lo * lo * (1.0 - 1e-9)) return 1;
+  }
+  return insphere_f(F.Pf, F.Uf, F.Vf, B, X);
+}
+
+// Among the lanes' apex candidates for face F (best >= 0 on a lane, sphere
+// sb), the one whose sphere holds none of the others: the apices are ordered
+// by the position of their sphere centre along the face normal (smaller =
+// better); overlapping error intervals are resolved with the exact in-sphere
+// sign (an exact tie keeps the current winner: the verification of the
+// winner's sphere reports it).  Returns the id (coordinates in W), -1 when no
+// lane has one, -2 on failure (flag set).
+__device__ __noinline__ int warp_select(Ctx& C, const Face& F, int best, float3 Bx, const Sphere& sb, float3& W) {
   double lo = kInf, hi = kInf;
   if (best >= 0) {
     if (sb.ok) {
-      const double d[3] = {sb.c[0] - P.x, sb.c[1] - P.y, sb.c[2] - P.z};
-      const double lam = nv[0] * d[0] + nv[1] * d[1] + nv[2] * d[2];
-      const double nn = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
-      const double e = (nn * sb.err + 4.0 * kEps * (fabs(nv[0] * d[0]) + fabs(nv[1] * d[1]) + fabs(nv[2] * d[2]))) *
+      const double d[3] = {sb.c[0] - F.P[0], sb.c[1] - F.P[1], sb.c[2] - F.P[2]};
+      const double lam = F.n[0] * d[0] + F.n[1] * d[1] + F.n[2] * d[2];
+      const double nn = sqrt(F.n[0] * F.n[0] + F.n[1] * F.n[1] + F.n[2] * F.n[2]);
+      const double e = (nn * sb.err + 4.0 * kEps * (fabs(F.n[0] * d[0]) + fabs(F.n[1] * d[1]) + fabs(F.n[2] * d[2]))) *
                        (1.0 + 1e-6);
       lo = lam - e;
       hi = lam + e;
@@ -442,38 +491,32 @@ __device__ int warp_select(Ctx& C, float3 U, float3 V, int best, float3 Bx, cons
   W.x = __shfl_sync(0xffffffffu, Bx.x, ml);
   W.y = __shfl_sync(0xffffffffu, Bx.y, ml);
   W.z = __shfl_sync(0xffffffffu, Bx.z, ml);
-  bool wtied = __shfl_sync(0xffffffffu, (int)tied, ml) != 0;
   for (unsigned amb = ballot(best >= 0 && C.lane != ml && lo <= mh); amb; amb &= amb - 1) {
     const int l = __ffs(amb) - 1;
     const int id = __shfl_sync(0xffffffffu, best, l);
-    const bool lt = __shfl_sync(0xffffffffu, (int)tied, l) != 0;
     float3 X;
     X.x = __shfl_sync(0xffffffffu, Bx.x, l);
     X.y = __shfl_sync(0xffffffffu, Bx.y, l);
     X.z = __shfl_sync(0xffffffffu, Bx.z, l);
-    const int s = insphere_f(P, U, V, W, X);
+    const int s = insphere_f(F.Pf, F.Uf, F.Vf, W, X);
     if (s == 2) {
       fail(C, kFlagUndecided, kWhyUndecided);
       return -2;
     }
-    if (s == 0) wtied = true;
-    else if (s > 0) { w = id; W = X; wtied = lt; }
-  }
-  // the winning sphere passes through another point beyond the face
-  if (wtied) {
-    fail(C, kFlagDegenerate, kWhyTie);
-    return -2;
+    if (s > 0) { w = id; W = X; }
   }
   return w;
 }
 
-// The best apex for face (p, u, v) among all points of the grid cells that
-// the sphere of the positively oriented (p, u, v, w) touches: the point
-// beyond the face, strictly inside that sphere, whose own sphere holds no
-// other.  Every point beyond the face with a smaller sphere lies in w's
-// sphere, so the result is the apex over the whole set.  Returns its id
-// (coordinates in Wb), -1 when w's sphere is empty, -2 on failure.
-__device__ int sphere_scan(Ctx& C, int u, float3 U, int v, float3 V, int w, float3 W, const Sphere& Sp, float3& Wb) {
+// Scan of the grid cells touched by the sphere Sp of the positively oriented
+// (p, u, v, w).  Returns the best point beyond the face strictly inside the
+// sphere (the apex over the whole set: every point beyond the face with a
+// smaller sphere lies in this one; coordinates in Wb), -1 when the sphere
+// holds no point (w is certified), -2 on failure: a point exactly on the
+// sphere of a certified w (a tie), a point inside it not beyond the face, or
+// an undecidable test (flag set).
+__device__ __noinline__ int sphere_scan(Ctx& C, const Face& F, int u, int v, int w, float3 W, const Sphere& Sp,
+                                        float3& Wb) {
   const TSet& S = *C.S;
   const double rad = Sp.r + 2.0 * Sp.err + S.slack;
   int c0[3], n[3];
@@ -484,7 +527,7 @@ __device__ int sphere_scan(Ctx& C, int u, float3 U, int v, float3 V, int w, floa
   }
   const long long total = (long long)n[0] * n[1] * n[2];
   int best = -1, flag = 0, why = 0;
-  bool tied = false, on_w = false;  // best ties another violator; a point on w's sphere
+  bool on_w = false;
   float3 Bx = C.P;
   Sphere sb;
   sb.ok = false;
@@ -508,26 +551,18 @@ __device__ int sphere_scan(Ctx& C, int u, float3 U, int v, float3 V, int w, floa
       const int id = __float_as_int(x4.w);
       if (id == C.p || id == u || id == v || id == w) continue;
       const float3 X = f3(x4);
-      if (sph_outside(Sp, X)) continue;
-      if (best >= 0 && sb.ok && sph_outside(sb, X)) continue;
-      const int s0 = insphere_f(C.P, U, V, W, X);
+      const int s0 = insphere_face(F, W, Sp, X);
       if (s0 == 2) { flag = kFlagUndecided; why = kWhyUndecided; break; }
       if (s0 == 0) { on_w = true; continue; }
       if (s0 < 0) continue;
-      const int o = orient_f(C.P, U, V, X);
+      if (best >= 0 && insphere_face(F, Bx, sb, X) <= 0) continue;  // not better than this lane's best
+      const int o = orient_face(F, X);
       if (o != 1) {
-        flag = o == 2 ? kFlagUndecided : (o == 0 ? kFlagDegenerate : kFlagRepair);
-        why = o == 2 ? kWhyUndecided : (o == 0 ? kWhyTie : kWhyNotDelaunay);
+        flag = o == 2 ? kFlagUndecided : kFlagRepair;
+        why = o == 2 ? kWhyUndecided : kWhyNotDelaunay;
         break;
       }
-      if (best < 0) {
-        best = id; Bx = X; sb = circum(C.P, U, V, X);
-        continue;
-      }
-      const int s1 = insphere_f(C.P, U, V, Bx, X);
-      if (s1 == 2) { flag = kFlagUndecided; why = kWhyUndecided; break; }
-      if (s1 == 0) tied = true;
-      else if (s1 > 0) { best = id; Bx = X; sb = circum(C.P, U, V, X); tied = false; }
+      best = id; Bx = X; sb = circum(C.P, F.Uf, F.Vf, X);
     }
     if (flag) break;
   }
@@ -537,7 +572,7 @@ __device__ int sphere_scan(Ctx& C, int u, float3 U, int v, float3 V, int w, floa
     fail(C, __shfl_sync(0xffffffffu, flag, l), __shfl_sync(0xffffffffu, why, l));
     return -2;
   }
-  const int r = warp_select(C, U, V, best, Bx, sb, tied, Wb);
+  const int r = warp_select(C, F, best, Bx, sb, Wb);
   if (r == -1 && ballot(on_w)) {  // w stays, and its sphere passes through another point
     fail(C, kFlagDegenerate, kWhyTie);
     return -2;
@@ -550,7 +585,7 @@ __device__ int sphere_scan(Ctx& C, int u, float3 U, int v, float3 V, int w, floa
 // point of the plane on or inside the face's circumcircle, or an undecidable
 // test (flag set).  (p, v, u, c) is the certified tetrahedron on the other
 // side of the face (c < 0: none yet; every point of the plane then fails).
-__device__ int halfspace_scan(Ctx& C, int u, float3 U, int v, float3 V, int c, float3 Cc) {
+__device__ __noinline__ int halfspace_scan(Ctx& C, int u, float3 U, int v, float3 V, int c, float3 Cc) {
   const TSet& S = *C.S;
   const double A[3] = {(double)U.x - C.P.x, (double)U.y - C.P.y, (double)U.z - C.P.z};
   const double B[3] = {(double)V.x - C.P.x, (double)V.y - C.P.y, (double)V.z - C.P.z};
@@ -614,40 +649,35 @@ __device__ int halfspace_scan(Ctx& C, int u, float3 U, int v, float3 V, int c, f
 // whose circumsphere with p, u, v holds no point of the set (face (p, u, v)
 // being a Delaunay face).  Returns w >= 0 (coordinates in W), -1 when no
 // point lies beyond the face (a hull face), -2 on failure (flag set).
+// (p, v, u, c) is the certified tetrahedron on the other side (c < 0: none).
 // full: certify against the grid even when the sphere fits the candidate ball.
-__device__ int wrap(Ctx& C, int u, float3 U, int v, float3 V, int c, float3 Cc, bool full, float3& W) {
-  const float3 P = C.P;
+__device__ __noinline__ int wrap(Ctx& C, int u, float3 U, int v, float3 V, int c, float3 Cc, bool full, float3& W) {
+  const Face F = make_face(C.P, U, V);
   int best = -1, flag = 0;
-  bool tied = false;
-  float3 Bx = P;
+  float3 Bx = C.P;
   Sphere sb;
   sb.ok = false;
+  // gift wrapping over the candidates: each lane keeps the best of its share
   for (int j = C.lane; j < C.ncand; j += 32) {
     const float4 c4 = C.cand[j];
     const int id = __float_as_int(c4.w);
     if (id == C.p || id == u || id == v) continue;
     const float3 X = f3(c4);
-    if (best >= 0 && sb.ok && sph_outside(sb, X)) continue;
-    const int o = orient_f(P, U, V, X);
-    if (o == 2) { flag |= kFlagUndecided; continue; }
-    if (o <= 0) continue;
-    if (best < 0) {
-      best = id; Bx = X; sb = circum(P, U, V, X);
-      continue;
+    if (best >= 0) {
+      const int si = insphere_face(F, Bx, sb, X);
+      if (si == 2) { flag = kFlagUndecided; continue; }
+      if (si <= 0) continue;
     }
-    const int s = insphere_f(P, U, V, Bx, X);
-    if (s == 2) flag |= kFlagUndecided;
-    else if (s == 0) tied = true;
-    else if (s > 0) { best = id; Bx = X; sb = circum(P, U, V, X); tied = false; }
+    const int o = orient_face(F, X);
+    if (o == 2) { flag = kFlagUndecided; continue; }
+    if (o <= 0) continue;
+    best = id; Bx = X; sb = circum(C.P, U, V, X);
   }
-  const unsigned fb = ballot(flag != 0);
-  if (fb) {
-    int f = 0;
-    for (unsigned m = fb; m; m &= m - 1) f |= __shfl_sync(0xffffffffu, flag, __ffs(m) - 1);
-    fail(C, f, (f & kFlagUndecided) ? kWhyUndecided : kWhyTie);
+  if (ballot(flag != 0)) {
+    fail(C, kFlagUndecided, kWhyUndecided);
     return -2;
   }
-  int w = warp_select(C, U, V, best, Bx, sb, tied, W);
+  int w = warp_select(C, F, best, Bx, sb, W);
   if (w == -2) return -2;
   bool from_cands = true;
   if (w < 0) {
@@ -656,22 +686,44 @@ __device__ int wrap(Ctx& C, int u, float3 U, int v, float3 V, int c, float3 Cc, 
     W = point(C, w);
     from_cands = false;
   }
-  // Certification: the sphere holds no point of the set, or the best point
-  // inside it (the true apex) replaces w.
-  const Sphere Sp = circum(P, U, V, W);
-  if (!Sp.ok) {
-    fail(C, kFlagUndecided, kWhyUndecided);
-    return -2;
-  }
-  if (!full && from_cands && 2.0 * (Sp.r + Sp.err) * (1.0 + 1e-9) < C.R) return w;
-  float3 Y;
-  const int y = sphere_scan(C, u, U, v, V, w, W, Sp, Y);
-  if (y == -2) return -2;
-  if (y >= 0) {
+  for (int it = 0; it < 4; ++it) {
+    const Sphere Sp = circum(C.P, U, V, W);
+    if (!Sp.ok) {
+      fail(C, kFlagUndecided, kWhyUndecided);
+      return -2;
+    }
+    if (!full && from_cands && 2.0 * (Sp.r + Sp.err) * (1.0 + 1e-9) < C.R) {
+      // the sphere lies in the candidate ball: verify it against every
+      // candidate (a point on it is a tie; one inside cannot occur)
+      int bad = 0;
+      for (int j = C.lane; j < C.ncand; j += 32) {
+        const float4 c4 = C.cand[j];
+        const int id = __float_as_int(c4.w);
+        if (id == C.p || id == u || id == v || id == w) continue;
+        const int si = insphere_face(F, W, Sp, f3(c4));
+        if (si == 2) bad |= 1;
+        else if (si == 0) bad |= 2;
+        else if (si > 0) bad |= 4;
+      }
+      const unsigned b1 = ballot(bad & 1), b2 = ballot(bad & 2), b4 = ballot(bad & 4);
+      if (b1 | b2 | b4) {
+        if (b1) fail(C, kFlagUndecided, kWhyUndecided);
+        else if (b4) fail(C, kFlagRepair, kWhyNotDelaunay);
+        else fail(C, kFlagDegenerate, kWhyTie);
+        return -2;
+      }
+      return w;
+    }
+    float3 Y;
+    const int y = sphere_scan(C, F, u, v, w, W, Sp, Y);
+    if (y == -2) return -2;
+    if (y < 0) return w;
     w = y;
     W = Y;
+    from_cands = false;
   }
-  return w;
+  fail(C, kFlagRepair, kWhyNotDelaunay);
+  return -2;
 }
 
 struct StarArgs {
@@ -745,7 +797,7 @@ __device__ int block_count_within(const TSet& S, const int32_t* cell_start, cons
 // One warp per vertex p: p's Delaunay star, certified; emits the tetrahedra
 // whose smallest vertex is p.  Work is fetched from a global counter so that
 // slow stars (near the convex hull) do not hold up a fixed share of vertices.
-__global__ void __launch_bounds__(kWarps * 32) k_tess_stars(StarArgs A) {
+__global__ void __launch_bounds__(kWarps * 32, 3) k_tess_stars(StarArgs A) {
   extern __shared__ float4 s_dyn[];
   __shared__ int s_fill[kWarps];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;

@@ -60,9 +60,11 @@ constexpr int kFlagUndecided = 16;   // exact path outside the 384-bit budget
 constexpr int kFlagInput = 32;       // non-finite coordinates or flat set
 
 constexpr int kWarps = 4;            // warps per block of the star kernel
-constexpr int kCandCap = 512;        // candidates per warp
+constexpr int kCandCap = 256;        // candidates per warp
 constexpr int kTriCap = 512;         // link triangles per warp
-constexpr size_t kStarSmem = (size_t)kWarps * (kCandCap + kTriCap) * 16;  // dynamic shared memory per block
+// dynamic shared memory per block: candidate offsets (3 doubles) and ids,
+// link triangles (int4)
+constexpr size_t kStarSmem = (size_t)kWarps * ((size_t)kCandCap * 28 + (size_t)kTriCap * 16);
 
 constexpr double kEps = 1.1102230246251565e-16;  // 2^-53
 constexpr double kOrientErr = 12.0 * kEps;        // same bounds as the host predicates
@@ -232,23 +234,6 @@ __device__ __noinline__ int insphere_exact_f(float3 a, float3 b, float3 c, float
   return -w_sign(det);
 }
 
-// Filtered orientation (the host's double evaluation and bound).
-__device__ __forceinline__ int orient_f(float3 a, float3 b, float3 c, float3 d) {
-  const double bax = (double)b.x - a.x, bay = (double)b.y - a.y, baz = (double)b.z - a.z;
-  const double cax = (double)c.x - a.x, cay = (double)c.y - a.y, caz = (double)c.z - a.z;
-  const double dax = (double)d.x - a.x, day = (double)d.y - a.y, daz = (double)d.z - a.z;
-  const double m0 = cay * daz, m1 = caz * day;
-  const double m2 = caz * dax, m3 = cax * daz;
-  const double m4 = cax * day, m5 = cay * dax;
-  const double det = bax * (m0 - m1) + bay * (m2 - m3) + baz * (m4 - m5);
-  const double perm = fabs(bax) * (fabs(m0) + fabs(m1)) + fabs(bay) * (fabs(m2) + fabs(m3)) +
-                      fabs(baz) * (fabs(m4) + fabs(m5));
-  const double bound = kOrientErr * perm;
-  if (det > bound) return 1;
-  if (-det > bound) return -1;
-  return orient_exact_f(a, b, c, d);
-}
-
 __device__ __forceinline__ double det3d(const double* u, const double* v, const double* w, double& perm) {
   const double m0 = v[1] * w[2], m1 = v[2] * w[1];
   const double m2 = v[2] * w[0], m3 = v[0] * w[2];
@@ -282,25 +267,24 @@ __device__ __noinline__ int insphere_f(float3 a, float3 b, float3 c, float3 d, f
   return insphere_exact_f(a, b, c, d, e);
 }
 
-// Circumsphere of (p, a, b, c) in double with a bound on the centre's error:
-// the centre is p + N / D with N = |A|^2 (B x C) + |B|^2 (C x A) + |C|^2 (A x B)
-// and D = 2 A.(B x C) (A = a - p, ...); both carry at most kCircErr times
-// the sums of their terms' magnitudes.  |centre - true centre| <= err and
-// |r - true radius| <= err.  ok is false when D is not resolved.
+// Circumsphere in the frame of the star's centre p: a, b, c are the offsets
+// (rounded once to double) of three points from p.  The centre is
+// N / D with N = |a|^2 (b x c) + |b|^2 (c x a) + |c|^2 (a x b) and
+// D = 2 a.(b x c); both carry at most kCircErr times the sums of their
+// terms' magnitudes (a first-order count of the roundings, the offsets'
+// included, gives under 16 eps).  |c - true centre| <= err and
+// |r - true radius| <= err; ok is false when D is not resolved.
 struct Sphere {
-  double c[3], r, err;
+  double c[3], r, err;  // c: offset of the centre from p
   bool ok;
 };
 
-__device__ Sphere circum(float3 p, float3 a, float3 b, float3 c) {
+__device__ Sphere circum_rel(const double* A, const double* B, const double* C) {
   Sphere S;
-  const double A[3] = {(double)a.x - p.x, (double)a.y - p.y, (double)a.z - p.z};
-  const double B[3] = {(double)b.x - p.x, (double)b.y - p.y, (double)b.z - p.z};
-  const double C[3] = {(double)c.x - p.x, (double)c.y - p.y, (double)c.z - p.z};
   const double la = A[0] * A[0] + A[1] * A[1] + A[2] * A[2];
   const double lb = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];
   const double lc = C[0] * C[0] + C[1] * C[1] + C[2] * C[2];
-  double N[3], Np[3], bc[3], bca[3];
+  double N[3], Np[3];
   double D = 0.0, Dp = 0.0;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -308,12 +292,11 @@ __device__ Sphere circum(float3 p, float3 a, float3 b, float3 c) {
     const double x1 = B[i] * C[j], x2 = B[j] * C[i];
     const double y1 = C[i] * A[j], y2 = C[j] * A[i];
     const double z1 = A[i] * B[j], z2 = A[j] * B[i];
-    bc[k] = x1 - x2;
-    bca[k] = fabs(x1) + fabs(x2);
-    N[k] = la * bc[k] + lb * (y1 - y2) + lc * (z1 - z2);
-    Np[k] = la * bca[k] + lb * (fabs(y1) + fabs(y2)) + lc * (fabs(z1) + fabs(z2));
-    D += A[k] * bc[k];
-    Dp += fabs(A[k]) * bca[k];
+    const double bc = x1 - x2, bca = fabs(x1) + fabs(x2);
+    N[k] = la * bc + lb * (y1 - y2) + lc * (z1 - z2);
+    Np[k] = la * bca + lb * (fabs(y1) + fabs(y2)) + lc * (fabs(z1) + fabs(z2));
+    D += A[k] * bc;
+    Dp += fabs(A[k]) * bca;
   }
   D *= 2.0;
   Dp *= 2.0;
@@ -321,27 +304,19 @@ __device__ Sphere circum(float3 p, float3 a, float3 b, float3 c) {
   const double dD = kCircErr * Dp;
   if (!(fabs(D) > 2.0 * dD)) {
     S.ok = false;
-    S.c[0] = p.x; S.c[1] = p.y; S.c[2] = p.z;
+    S.c[0] = S.c[1] = S.c[2] = 0.0;
     S.r = kInf;
     S.err = kInf;
     return S;
   }
-  const double o[3] = {N[0] / D, N[1] / D, N[2] / D};
-  S.r = sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
-  S.c[0] = p.x + o[0];
-  S.c[1] = p.y + o[1];
-  S.c[2] = p.z + o[2];
-  const double pm = fmax(fabs((double)p.x), fmax(fabs((double)p.y), fabs((double)p.z)));
-  S.err = (2.0 * dN + S.r * dD) / (fabs(D) - dD) * (1.0 + 1e-6) + 8.0 * kEps * (S.r + pm);
+  const double inv = 1.0 / D;
+  S.c[0] = N[0] * inv;
+  S.c[1] = N[1] * inv;
+  S.c[2] = N[2] * inv;
+  S.r = sqrt(S.c[0] * S.c[0] + S.c[1] * S.c[1] + S.c[2] * S.c[2]);
+  S.err = (2.0 * dN + S.r * dD) / (fabs(D) - dD) * (1.0 + 1e-6) + 8.0 * kEps * S.r;
   S.ok = true;
   return S;
-}
-
-// x strictly outside the true sphere (sufficient test).
-__device__ __forceinline__ bool sph_outside(const Sphere& S, float3 x) {
-  const double dx = (double)x.x - S.c[0], dy = (double)x.y - S.c[1], dz = (double)x.z - S.c[2];
-  const double rr = S.r + 2.0 * S.err;
-  return dx * dx + dy * dy + dz * dz > rr * rr * (1.0 + 1e-9);
 }
 
 // Bounded box of a grid cell: interior cells are [lo + i h, lo + (i+1) h];
@@ -362,14 +337,18 @@ __device__ __forceinline__ int cell_coord(const TSet& S, double x, int a) {
 
 __device__ __forceinline__ float3 f3(float4 v) { return make_float3(v.x, v.y, v.z); }
 
-// Per-warp context of one star.
+// Per-warp context of one star.  Candidates are the points within R of p,
+// stored as double offsets from p (structure of arrays in shared memory).
 struct Ctx {
   const TSet* S;
   const float* xyz;            // all vertices, 3 floats each
   double hi[3];
   const int32_t* cell_start;   // global
   const float4* sorted;
-  const float4* cand;          // this warp's candidates (shared)
+  const double* cx;            // candidate offsets from p
+  const double* cy;
+  const double* cz;
+  const int* cid;              // candidate vertex ids
   int ncand;
   int p;
   float3 P;
@@ -404,73 +383,79 @@ __device__ __forceinline__ float3 point(const Ctx& C, int id) {
   return make_float3(__ldg(q), __ldg(q + 1), __ldg(q + 2));
 }
 
-// A face (p, u, v) with its normal n = (u - p) x (v - p) in double and the
-// magnitudes of n's two products per component: orient(p, u, v, x) is the
-// sign of (x - p).n, filtered with the host's orientation bound (the same
-// determinant expanded along x's row) and exact otherwise.
+__device__ __forceinline__ void rel(const Ctx& C, float3 X, double* d) {
+  d[0] = (double)X.x - C.P.x;
+  d[1] = (double)X.y - C.P.y;
+  d[2] = (double)X.z - C.P.z;
+}
+
+// A face (p, u, v) in p's frame: the offsets a = u - p, b = v - p, the normal
+// n = a x b and the magnitudes of n's two products per component.
+// orient(p, u, v, x) is the sign of d.n (d = x - p), filtered with the host's
+// orientation bound (the same determinant expanded along x's row) and exact
+// otherwise (the float inputs fetched by id).
 struct Face {
-  float3 Pf, Uf, Vf;
-  double P[3], n[3], na[3];
+  int u, v;
+  double a[3], b[3], n[3], na[3];
 };
 
-__device__ __forceinline__ Face make_face(float3 P, float3 U, float3 V) {
+__device__ __forceinline__ Face make_face(const Ctx& C, int u, int v) {
   Face F;
-  F.Pf = P;
-  F.Uf = U;
-  F.Vf = V;
-  F.P[0] = P.x; F.P[1] = P.y; F.P[2] = P.z;
-  const double b[3] = {(double)U.x - P.x, (double)U.y - P.y, (double)U.z - P.z};
-  const double c[3] = {(double)V.x - P.x, (double)V.y - P.y, (double)V.z - P.z};
+  F.u = u;
+  F.v = v;
+  rel(C, point(C, u), F.a);
+  rel(C, point(C, v), F.b);
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     const int i = (k + 1) % 3, j = (k + 2) % 3;
-    const double m1 = b[i] * c[j], m2 = b[j] * c[i];
+    const double m1 = F.a[i] * F.b[j], m2 = F.a[j] * F.b[i];
     F.n[k] = m1 - m2;
     F.na[k] = fabs(m1) + fabs(m2);
   }
   return F;
 }
 
-__device__ __forceinline__ int orient_face(const Face& F, float3 X) {
-  const double d0 = (double)X.x - F.P[0], d1 = (double)X.y - F.P[1], d2 = (double)X.z - F.P[2];
-  const double det = d0 * F.n[0] + d1 * F.n[1] + d2 * F.n[2];
-  const double perm = fabs(d0) * F.na[0] + fabs(d1) * F.na[1] + fabs(d2) * F.na[2];
+__device__ __forceinline__ int orient_face(const Ctx& C, const Face& F, const double* d, int id) {
+  const double det = d[0] * F.n[0] + d[1] * F.n[1] + d[2] * F.n[2];
+  const double perm = fabs(d[0]) * F.na[0] + fabs(d[1]) * F.na[1] + fabs(d[2]) * F.na[2];
   const double bound = kOrientErr * perm;
   if (det > bound) return 1;
   if (-det > bound) return -1;
-  return orient_exact_f(F.Pf, F.Uf, F.Vf, X);
+  return orient_exact_f(C.P, point(C, F.u), point(C, F.v), point(C, id));
 }
 
-// In-sphere sign of x for the positively oriented (p, u, v, b) whose sphere
-// is S: decided by the distance to the bounded centre when x is clearly in
-// or out, else by the determinant.
-__device__ __forceinline__ int insphere_face(const Face& F, float3 B, const Sphere& S, float3 X) {
+// In-sphere sign of x (offset d, id) for the positively oriented (p, u, v, b)
+// whose sphere is S: decided by the distance to the bounded centre when x is
+// clearly in or out, else by the determinant over the float inputs.
+__device__ __forceinline__ int insphere_face(const Ctx& C, const Face& F, int b, const Sphere& S, const double* d,
+                                             int id) {
   if (S.ok) {
-    const double dx = (double)X.x - S.c[0], dy = (double)X.y - S.c[1], dz = (double)X.z - S.c[2];
+    const double dx = d[0] - S.c[0], dy = d[1] - S.c[1], dz = d[2] - S.c[2];
     const double d2 = dx * dx + dy * dy + dz * dz;
     const double hi = S.r + 2.0 * S.err;
     if (d2 > hi * hi * (1.0 + 1e-9)) return -1;
     const double lo = S.r - 2.0 * S.err;
     if (lo > 0.0 && d2 < lo * lo * (1.0 - 1e-9)) return 1;
   }
-  return insphere_f(F.Pf, F.Uf, F.Vf, B, X);
+  return insphere_f(C.P, point(C, F.u), point(C, F.v), point(C, b), point(C, id));
 }
 
-// Among the lanes' apex candidates for face F (best >= 0 on a lane, sphere
-// sb), the one whose sphere holds none of the others: the apices are ordered
-// by the position of their sphere centre along the face normal (smaller =
-// better); overlapping error intervals are resolved with the exact in-sphere
-// sign (an exact tie keeps the current winner: the verification of the
-// winner's sphere reports it).  Returns the id (coordinates in W), -1 when no
+// Among the lanes' apex candidates for face F (best >= 0 on a lane, offset
+// bd, sphere sb), the one whose sphere holds none of the others: the apices
+// are ordered by the position of their sphere centre along the face normal
+// (smaller = better); overlapping error intervals are resolved with the exact
+// in-sphere sign (an exact tie keeps the current winner: the verification of
+// the winner's sphere reports it).  Returns the id (offset in Wd), -1 when no
 // lane has one, -2 on failure (flag set).
-__device__ __noinline__ int warp_select(Ctx& C, const Face& F, int best, float3 Bx, const Sphere& sb, float3& W) {
+__device__ __noinline__ int warp_select(Ctx& C, const Face& F, int best, const double* bd, const Sphere& sb,
+                                        double* Wd) {
   double lo = kInf, hi = kInf;
   if (best >= 0) {
     if (sb.ok) {
-      const double d[3] = {sb.c[0] - F.P[0], sb.c[1] - F.P[1], sb.c[2] - F.P[2]};
-      const double lam = F.n[0] * d[0] + F.n[1] * d[1] + F.n[2] * d[2];
+      const double lam = F.n[0] * sb.c[0] + F.n[1] * sb.c[1] + F.n[2] * sb.c[2];
       const double nn = sqrt(F.n[0] * F.n[0] + F.n[1] * F.n[1] + F.n[2] * F.n[2]);
-      const double e = (nn * sb.err + 4.0 * kEps * (fabs(F.n[0] * d[0]) + fabs(F.n[1] * d[1]) + fabs(F.n[2] * d[2]))) *
+      const double e = (nn * sb.err +
+                        4.0 * kEps * (fabs(F.n[0] * sb.c[0]) + fabs(F.n[1] * sb.c[1]) + fabs(F.n[2] * sb.c[2]))) *
                        (1.0 + 1e-6);
       lo = lam - e;
       hi = lam + e;
@@ -488,22 +473,21 @@ __device__ __noinline__ int warp_select(Ctx& C, const Face& F, int best, float3 
     if (oh < mh || (oh == mh && ol < ml)) { mh = oh; ml = ol; }
   }
   int w = __shfl_sync(0xffffffffu, best, ml);
-  W.x = __shfl_sync(0xffffffffu, Bx.x, ml);
-  W.y = __shfl_sync(0xffffffffu, Bx.y, ml);
-  W.z = __shfl_sync(0xffffffffu, Bx.z, ml);
+  for (int k = 0; k < 3; ++k) Wd[k] = __shfl_sync(0xffffffffu, bd[k], ml);
   for (unsigned amb = ballot(best >= 0 && C.lane != ml && lo <= mh); amb; amb &= amb - 1) {
     const int l = __ffs(amb) - 1;
     const int id = __shfl_sync(0xffffffffu, best, l);
-    float3 X;
-    X.x = __shfl_sync(0xffffffffu, Bx.x, l);
-    X.y = __shfl_sync(0xffffffffu, Bx.y, l);
-    X.z = __shfl_sync(0xffffffffu, Bx.z, l);
-    const int s = insphere_f(F.Pf, F.Uf, F.Vf, W, X);
+    double X[3];
+    for (int k = 0; k < 3; ++k) X[k] = __shfl_sync(0xffffffffu, bd[k], l);
+    const int s = insphere_f(C.P, point(C, F.u), point(C, F.v), point(C, w), point(C, id));
     if (s == 2) {
       fail(C, kFlagUndecided, kWhyUndecided);
       return -2;
     }
-    if (s > 0) { w = id; W = X; }
+    if (s > 0) {
+      w = id;
+      for (int k = 0; k < 3; ++k) Wd[k] = X[k];
+    }
   }
   return w;
 }
@@ -511,60 +495,69 @@ __device__ __noinline__ int warp_select(Ctx& C, const Face& F, int best, float3 
 // Scan of the grid cells touched by the sphere Sp of the positively oriented
 // (p, u, v, w).  Returns the best point beyond the face strictly inside the
 // sphere (the apex over the whole set: every point beyond the face with a
-// smaller sphere lies in this one; coordinates in Wb), -1 when the sphere
-// holds no point (w is certified), -2 on failure: a point exactly on the
-// sphere of a certified w (a tie), a point inside it not beyond the face, or
-// an undecidable test (flag set).
-__device__ __noinline__ int sphere_scan(Ctx& C, const Face& F, int u, int v, int w, float3 W, const Sphere& Sp,
-                                        float3& Wb) {
+// smaller sphere lies in this one; offset in Yd), -1 when the sphere holds
+// no point (w is certified), -2 on failure: a point exactly on the sphere of
+// a certified w (a tie), a point inside it not beyond the face, or an
+// undecidable test (flag set).
+__device__ __noinline__ int sphere_scan(Ctx& C, const Face& F, int w, const Sphere& Sp, double* Yd) {
   const TSet& S = *C.S;
   const double rad = Sp.r + 2.0 * Sp.err + S.slack;
-  int c0[3], n[3];
-  for (int a = 0; a < 3; ++a) {
-    const int l = cell_coord(S, Sp.c[a] - rad, a), h = cell_coord(S, Sp.c[a] + rad, a);
-    c0[a] = l;
-    n[a] = h - l + 1;
-  }
-  const long long total = (long long)n[0] * n[1] * n[2];
+  const double cen[3] = {C.P.x + Sp.c[0], C.P.y + Sp.c[1], C.P.z + Sp.c[2]};
+  // columns of cells along a2, the axis of the centre's largest offset from p
+  // (a large sphere then meets the grid in a thin cap across the columns);
+  // in each column, the cells within the sphere's reach along a2
+  int a2 = 0;
+  for (int a = 1; a < 3; ++a)
+    if (fabs(Sp.c[a]) > fabs(Sp.c[a2])) a2 = a;
+  const int a0 = a2 == 0 ? 1 : 0, a1 = a2 == 2 ? 1 : 2;
+  const int i0 = cell_coord(S, cen[a0] - rad, a0), i1 = cell_coord(S, cen[a0] + rad, a0);
+  const int j0 = cell_coord(S, cen[a1] - rad, a1), j1 = cell_coord(S, cen[a1] + rad, a1);
+  const int nj = j1 - j0 + 1;
+  const int ncol = (i1 - i0 + 1) * nj;
   int best = -1, flag = 0, why = 0;
   bool on_w = false;
-  float3 Bx = C.P;
+  double bd[3] = {0.0, 0.0, 0.0};
   Sphere sb;
   sb.ok = false;
-  for (long long t = C.lane; t < total; t += 32) {
-    const int k = (int)(t % n[2]);
-    const int j = (int)((t / n[2]) % n[1]);
-    const int i = (int)(t / ((long long)n[1] * n[2]));
-    const int ci[3] = {c0[0] + i, c0[1] + j, c0[2] + k};
-    double d2 = 0.0;
-    for (int a = 0; a < 3; ++a) {
-      double b0, b1;
-      cell_box(S, C.hi, ci[a], a, b0, b1);
-      const double q = Sp.c[a] < b0 ? b0 - Sp.c[a] : (Sp.c[a] > b1 ? Sp.c[a] - b1 : 0.0);
-      d2 += q * q;
-    }
-    if (d2 > rad * rad * (1.0 + 1e-9)) continue;
-    const int64_t g = S.cell0 + ((int64_t)ci[0] * S.dims[1] + ci[1]) * S.dims[2] + ci[2];
-    const int e0 = __ldg(&C.cell_start[g]), e1 = __ldg(&C.cell_start[g + 1]);
-    for (int e = e0; e < e1 && !flag; ++e) {
-      const float4 x4 = __ldg(&C.sorted[e]);
-      const int id = __float_as_int(x4.w);
-      if (id == C.p || id == u || id == v || id == w) continue;
-      const float3 X = f3(x4);
-      const int s0 = insphere_face(F, W, Sp, X);
-      if (s0 == 2) { flag = kFlagUndecided; why = kWhyUndecided; break; }
-      if (s0 == 0) { on_w = true; continue; }
-      if (s0 < 0) continue;
-      if (best >= 0 && insphere_face(F, Bx, sb, X) <= 0) continue;  // not better than this lane's best
-      const int o = orient_face(F, X);
-      if (o != 1) {
-        flag = o == 2 ? kFlagUndecided : kFlagRepair;
-        why = o == 2 ? kWhyUndecided : kWhyNotDelaunay;
-        break;
+  for (int t = C.lane; t < ncol && !flag; t += 32) {
+    int ci[3];
+    ci[a0] = i0 + t / nj;
+    ci[a1] = j0 + t % nj;
+    double bx0, bx1, by0, by1;
+    cell_box(S, C.hi, ci[a0], a0, bx0, bx1);
+    cell_box(S, C.hi, ci[a1], a1, by0, by1);
+    const double qx = cen[a0] < bx0 ? bx0 - cen[a0] : (cen[a0] > bx1 ? cen[a0] - bx1 : 0.0);
+    const double qy = cen[a1] < by0 ? by0 - cen[a1] : (cen[a1] > by1 ? cen[a1] - by1 : 0.0);
+    const double rest = rad * rad * (1.0 + 1e-9) - (qx * qx + qy * qy);
+    if (rest < 0.0) continue;
+    const double half = sqrt(rest) * (1.0 + 1e-9) + S.slack;
+    const int k0 = cell_coord(S, cen[a2] - half, a2), k1 = cell_coord(S, cen[a2] + half, a2);
+    for (int k = k0; k <= k1 && !flag; ++k) {
+      ci[a2] = k;
+      const int64_t g = S.cell0 + ((int64_t)ci[0] * S.dims[1] + ci[1]) * S.dims[2] + ci[2];
+      const int e0 = __ldg(&C.cell_start[g]), e1 = __ldg(&C.cell_start[g + 1]);
+      for (int e = e0; e < e1; ++e) {
+        const float4 x4 = __ldg(&C.sorted[e]);
+        const int id = __float_as_int(x4.w);
+        if (id == C.p || id == F.u || id == F.v || id == w) continue;
+        double d[3];
+        rel(C, f3(x4), d);
+        const int s0 = insphere_face(C, F, w, Sp, d, id);
+        if (s0 == 2) { flag = kFlagUndecided; why = kWhyUndecided; break; }
+        if (s0 == 0) { on_w = true; continue; }
+        if (s0 < 0) continue;
+        if (best >= 0 && insphere_face(C, F, best, sb, d, id) <= 0) continue;  // not better than this lane's best
+        const int o = orient_face(C, F, d, id);
+        if (o != 1) {
+          flag = o == 2 ? kFlagUndecided : kFlagRepair;
+          why = o == 2 ? kWhyUndecided : kWhyNotDelaunay;
+          break;
+        }
+        best = id;
+        bd[0] = d[0]; bd[1] = d[1]; bd[2] = d[2];
+        sb = circum_rel(F.a, F.b, d);
       }
-      best = id; Bx = X; sb = circum(C.P, F.Uf, F.Vf, X);
     }
-    if (flag) break;
   }
   const unsigned fb = ballot(flag != 0);
   if (fb) {
@@ -572,7 +565,7 @@ __device__ __noinline__ int sphere_scan(Ctx& C, const Face& F, int u, int v, int
     fail(C, __shfl_sync(0xffffffffu, flag, l), __shfl_sync(0xffffffffu, why, l));
     return -2;
   }
-  const int r = warp_select(C, F, best, Bx, sb, Wb);
+  const int r = warp_select(C, F, best, bd, sb, Yd);
   if (r == -1 && ballot(on_w)) {  // w stays, and its sphere passes through another point
     fail(C, kFlagDegenerate, kWhyTie);
     return -2;
@@ -585,47 +578,61 @@ __device__ __noinline__ int sphere_scan(Ctx& C, const Face& F, int u, int v, int
 // point of the plane on or inside the face's circumcircle, or an undecidable
 // test (flag set).  (p, v, u, c) is the certified tetrahedron on the other
 // side of the face (c < 0: none yet; every point of the plane then fails).
-__device__ __noinline__ int halfspace_scan(Ctx& C, int u, float3 U, int v, float3 V, int c, float3 Cc) {
+__device__ __noinline__ int halfspace_scan(Ctx& C, const Face& F, int c) {
   const TSet& S = *C.S;
-  const double A[3] = {(double)U.x - C.P.x, (double)U.y - C.P.y, (double)U.z - C.P.z};
-  const double B[3] = {(double)V.x - C.P.x, (double)V.y - C.P.y, (double)V.z - C.P.z};
-  const double nv[3] = {A[1] * B[2] - A[2] * B[1], A[2] * B[0] - A[0] * B[2], A[0] * B[1] - A[1] * B[0]};
   const double Pd[3] = {C.P.x, C.P.y, C.P.z};
-  // slack on n.(x - p): rounding of n and of the products
-  const double nn = fabs(nv[0]) + fabs(nv[1]) + fabs(nv[2]);
-  const double ab = (fabs(A[0]) + fabs(A[1]) + fabs(A[2])) * (fabs(B[0]) + fabs(B[1]) + fabs(B[2]));
-  const long long total = (long long)S.dims[0] * S.dims[1] * S.dims[2];
+  // columns of cells along the normal's dominant axis a2; in each, the cells
+  // that reach beyond the plane (whose a2-coordinate over the column's
+  // rectangle lies between the plane's values at its corners)
+  int a2 = 0;
+  for (int a = 1; a < 3; ++a)
+    if (fabs(F.n[a]) > fabs(F.n[a2])) a2 = a;
+  const int a0 = a2 == 0 ? 1 : 0, a1 = a2 == 2 ? 1 : 2;
+  const long long ncol = (long long)S.dims[a0] * S.dims[a1];
   int found = -1, flag = 0;
-  for (long long t0 = 0; t0 < total; t0 += 32) {
+  for (long long t0 = 0; t0 < ncol; t0 += 32) {
     const long long t = t0 + C.lane;
-    if (t < total) {
-      const int k = (int)(t % S.dims[2]);
-      const int j = (int)((t / S.dims[2]) % S.dims[1]);
-      const int i = (int)(t / ((long long)S.dims[1] * S.dims[2]));
-      const int ci[3] = {i, j, k};
-      double m = 0.0, ext = 0.0;
-      for (int a = 0; a < 3; ++a) {
-        double b0, b1;
-        cell_box(S, C.hi, ci[a], a, b0, b1);
-        const double x = nv[a] > 0.0 ? b1 : b0;
-        m += nv[a] * (x - Pd[a]);
-        ext += fabs(x - Pd[a]);
+    if (t < ncol) {
+      int ci[3];
+      ci[a0] = (int)(t / S.dims[a1]);
+      ci[a1] = (int)(t % S.dims[a1]);
+      double x0, x1, y0, y1;
+      cell_box(S, C.hi, ci[a0], a0, x0, x1);
+      cell_box(S, C.hi, ci[a1], a1, y0, y1);
+      const double xs[2] = {x0 - Pd[a0], x1 - Pd[a0]}, ys[2] = {y0 - Pd[a1], y1 - Pd[a1]};
+      double tmin = kInf, tmax = -kInf;
+      for (int u = 0; u < 2; ++u)
+        for (int v = 0; v < 2; ++v) {
+          const double tz = Pd[a2] - (F.n[a0] * xs[u] + F.n[a1] * ys[v]) / F.n[a2];
+          tmin = fmin(tmin, tz);
+          tmax = fmax(tmax, tz);
+        }
+      const double margin = 1e-6 * (fabs(Pd[a2]) + fabs(tmin) + fabs(tmax) + S.h) + S.slack;
+      int k0, k1;
+      if (F.n[a2] > 0.0) {
+        k0 = cell_coord(S, tmin - margin, a2);
+        k1 = S.dims[a2] - 1;
+      } else {
+        k0 = 0;
+        k1 = cell_coord(S, tmax + margin, a2);
       }
-      if (m > -(1e-9 * (nn + ab) * ext + 1e-300)) {
-        const int64_t g = S.cell0 + ((int64_t)i * S.dims[1] + j) * S.dims[2] + k;
+      for (int k = k0; k <= k1 && found < 0 && !flag; ++k) {
+        ci[a2] = k;
+        const int64_t g = S.cell0 + ((int64_t)ci[0] * S.dims[1] + ci[1]) * S.dims[2] + ci[2];
         const int e0 = __ldg(&C.cell_start[g]), e1 = __ldg(&C.cell_start[g + 1]);
         for (int e = e0; e < e1 && found < 0 && !flag; ++e) {
           const float4 x4 = __ldg(&C.sorted[e]);
           const int id = __float_as_int(x4.w);
-          if (id == C.p || id == u || id == v) continue;
-          const float3 X = f3(x4);
-          const int o = orient_f(C.P, U, V, X);
+          if (id == C.p || id == F.u || id == F.v) continue;
+          double d[3];
+          rel(C, f3(x4), d);
+          const int o = orient_face(C, F, d, id);
           if (o == 2) flag = kFlagUndecided;
           else if (o > 0) found = id;
           else if (o == 0) {
             // on the face's plane: harmless outside the face's circumcircle,
             // which is where the certified sphere across the face meets it
-            const int s = c >= 0 ? insphere_f(C.P, V, U, Cc, X) : 0;
+            const int s = c >= 0 ? insphere_f(C.P, point(C, F.v), point(C, F.u), point(C, c), f3(x4)) : 0;
             if (s == 2) flag = kFlagUndecided;
             else if (s >= 0) flag = kFlagDegenerate;
           }
@@ -647,60 +654,61 @@ __device__ __noinline__ int halfspace_scan(Ctx& C, int u, float3 U, int v, float
 
 // Apex across the face (p, u, v): the point w with orient(p, u, v, w) > 0
 // whose circumsphere with p, u, v holds no point of the set (face (p, u, v)
-// being a Delaunay face).  Returns w >= 0 (coordinates in W), -1 when no
-// point lies beyond the face (a hull face), -2 on failure (flag set).
-// (p, v, u, c) is the certified tetrahedron on the other side (c < 0: none).
-// full: certify against the grid even when the sphere fits the candidate ball.
-__device__ __noinline__ int wrap(Ctx& C, int u, float3 U, int v, float3 V, int c, float3 Cc, bool full, float3& W) {
-  const Face F = make_face(C.P, U, V);
+// being a Delaunay face).  Returns w >= 0, -1 when no point lies beyond the
+// face (a hull face), -2 on failure (flag set).  (p, v, u, c) is the
+// certified tetrahedron on the other side (c < 0: none).
+__device__ __noinline__ int wrap(Ctx& C, int u, int v, int c) {
+  const Face F = make_face(C, u, v);
   int best = -1, flag = 0;
-  float3 Bx = C.P;
+  double bd[3] = {0.0, 0.0, 0.0};
   Sphere sb;
   sb.ok = false;
   // gift wrapping over the candidates: each lane keeps the best of its share
   for (int j = C.lane; j < C.ncand; j += 32) {
-    const float4 c4 = C.cand[j];
-    const int id = __float_as_int(c4.w);
-    if (id == C.p || id == u || id == v) continue;
-    const float3 X = f3(c4);
+    const int id = C.cid[j];
+    if (id == u || id == v) continue;
+    const double d[3] = {C.cx[j], C.cy[j], C.cz[j]};
     if (best >= 0) {
-      const int si = insphere_face(F, Bx, sb, X);
-      if (si == 2) { flag = kFlagUndecided; continue; }
+      const int si = insphere_face(C, F, best, sb, d, id);
+      if (si == 2) { flag = 1; continue; }
       if (si <= 0) continue;
     }
-    const int o = orient_face(F, X);
-    if (o == 2) { flag = kFlagUndecided; continue; }
+    const int o = orient_face(C, F, d, id);
+    if (o == 2) { flag = 1; continue; }
     if (o <= 0) continue;
-    best = id; Bx = X; sb = circum(C.P, U, V, X);
+    best = id;
+    bd[0] = d[0]; bd[1] = d[1]; bd[2] = d[2];
+    sb = circum_rel(F.a, F.b, d);
   }
   if (ballot(flag != 0)) {
     fail(C, kFlagUndecided, kWhyUndecided);
     return -2;
   }
-  int w = warp_select(C, F, best, Bx, sb, W);
+  double Wd[3];
+  int w = warp_select(C, F, best, bd, sb, Wd);
   if (w == -2) return -2;
   bool from_cands = true;
   if (w < 0) {
-    w = halfspace_scan(C, u, U, v, V, c, Cc);
+    w = halfspace_scan(C, F, c);
     if (w < 0) return w;  // -1: hull face; -2: failure
-    W = point(C, w);
+    rel(C, point(C, w), Wd);
     from_cands = false;
   }
   for (int it = 0; it < 4; ++it) {
-    const Sphere Sp = circum(C.P, U, V, W);
+    const Sphere Sp = circum_rel(F.a, F.b, Wd);
     if (!Sp.ok) {
       fail(C, kFlagUndecided, kWhyUndecided);
       return -2;
     }
-    if (!full && from_cands && 2.0 * (Sp.r + Sp.err) * (1.0 + 1e-9) < C.R) {
+    if (from_cands && 2.0 * (Sp.r + Sp.err) * (1.0 + 1e-9) < C.R) {
       // the sphere lies in the candidate ball: verify it against every
       // candidate (a point on it is a tie; one inside cannot occur)
       int bad = 0;
       for (int j = C.lane; j < C.ncand; j += 32) {
-        const float4 c4 = C.cand[j];
-        const int id = __float_as_int(c4.w);
-        if (id == C.p || id == u || id == v || id == w) continue;
-        const int si = insphere_face(F, W, Sp, f3(c4));
+        const int id = C.cid[j];
+        if (id == u || id == v || id == w) continue;
+        const double d[3] = {C.cx[j], C.cy[j], C.cz[j]};
+        const int si = insphere_face(C, F, w, Sp, d, id);
         if (si == 2) bad |= 1;
         else if (si == 0) bad |= 2;
         else if (si > 0) bad |= 4;
@@ -714,12 +722,12 @@ __device__ __noinline__ int wrap(Ctx& C, int u, float3 U, int v, float3 V, int c
       }
       return w;
     }
-    float3 Y;
-    const int y = sphere_scan(C, F, u, v, w, W, Sp, Y);
+    double Yd[3];
+    const int y = sphere_scan(C, F, w, Sp, Yd);
     if (y == -2) return -2;
     if (y < 0) return w;
     w = y;
-    W = Y;
+    Wd[0] = Yd[0]; Wd[1] = Yd[1]; Wd[2] = Yd[2];
     from_cands = false;
   }
   fail(C, kFlagRepair, kWhyNotDelaunay);
@@ -759,36 +767,22 @@ __device__ __forceinline__ void tri_edge(const int4& T, int k, int& x, int& y) {
   y = k == 0 ? T.y : (k == 1 ? T.z : T.x);
 }
 
-// Points in the (2 rr + 1)^3 cells around ci (clipped to the grid).
-__device__ int block_count(const TSet& S, const int32_t* cell_start, const int* ci, int rr, int lane, int* c0,
-                           int* nc) {
-  for (int a = 0; a < 3; ++a) {
-    c0[a] = max(0, ci[a] - rr);
-    nc[a] = min(S.dims[a] - 1, ci[a] + rr) - c0[a] + 1;
-  }
+// Points of the block c0 + [0, nc) (other than p) strictly closer to P than
+// sqrt(d2max).
+__device__ int block_count_within(const Ctx& C, const int* c0, const int* nc, double d2max) {
+  const TSet& S = *C.S;
   const int total = nc[0] * nc[1] * nc[2];
   int cnt = 0;
-  for (int t = lane; t < total; t += 32) {
+  for (int t = C.lane; t < total; t += 32) {
     const int k = t % nc[2], j = (t / nc[2]) % nc[1], i = t / (nc[1] * nc[2]);
     const int64_t g = S.cell0 + ((int64_t)(c0[0] + i) * S.dims[1] + (c0[1] + j)) * S.dims[2] + (c0[2] + k);
-    cnt += __ldg(&cell_start[g + 1]) - __ldg(&cell_start[g]);
-  }
-  return __reduce_add_sync(0xffffffffu, cnt);
-}
-
-// Points of the block c0 + [0, nc) strictly closer to P than sqrt(d2max).
-__device__ int block_count_within(const TSet& S, const int32_t* cell_start, const float4* sorted, const int* c0,
-                                  const int* nc, int lane, float3 P, double d2max) {
-  const int total = nc[0] * nc[1] * nc[2];
-  int cnt = 0;
-  for (int t = lane; t < total; t += 32) {
-    const int k = t % nc[2], j = (t / nc[2]) % nc[1], i = t / (nc[1] * nc[2]);
-    const int64_t g = S.cell0 + ((int64_t)(c0[0] + i) * S.dims[1] + (c0[1] + j)) * S.dims[2] + (c0[2] + k);
-    const int e1 = __ldg(&cell_start[g + 1]);
-    for (int e = __ldg(&cell_start[g]); e < e1; ++e) {
-      const float4 x4 = __ldg(&sorted[e]);
-      const double dx = (double)x4.x - P.x, dy = (double)x4.y - P.y, dz = (double)x4.z - P.z;
-      cnt += dx * dx + dy * dy + dz * dz < d2max;
+    const int e1 = __ldg(&C.cell_start[g + 1]);
+    for (int e = __ldg(&C.cell_start[g]); e < e1; ++e) {
+      const float4 x4 = __ldg(&C.sorted[e]);
+      if (__float_as_int(x4.w) == C.p) continue;
+      double d[3];
+      rel(C, f3(x4), d);
+      cnt += d[0] * d[0] + d[1] * d[1] + d[2] * d[2] < d2max;
     }
   }
   return __reduce_add_sync(0xffffffffu, cnt);
@@ -798,11 +792,15 @@ __device__ int block_count_within(const TSet& S, const int32_t* cell_start, cons
 // whose smallest vertex is p.  Work is fetched from a global counter so that
 // slow stars (near the convex hull) do not hold up a fixed share of vertices.
 __global__ void __launch_bounds__(kWarps * 32, 3) k_tess_stars(StarArgs A) {
-  extern __shared__ float4 s_dyn[];
+  extern __shared__ double s_dyn[];
   __shared__ int s_fill[kWarps];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float4* cand = s_dyn + (size_t)wid * kCandCap;
-  int4* tri = reinterpret_cast<int4*>(s_dyn + (size_t)kWarps * kCandCap) + (size_t)wid * kTriCap;
+  double* cx = s_dyn + (size_t)wid * 3 * kCandCap;
+  double* cy = cx + kCandCap;
+  double* cz = cy + kCandCap;
+  int* cid = reinterpret_cast<int*>(s_dyn + (size_t)kWarps * 3 * kCandCap) + (size_t)wid * kCandCap;
+  int4* tri = reinterpret_cast<int4*>(reinterpret_cast<int*>(s_dyn + (size_t)kWarps * 3 * kCandCap) +
+                                      (size_t)kWarps * kCandCap) + (size_t)wid * kTriCap;
   for (;;) {
     unsigned long long pi = 0;
     if (lane == 0) pi = atomicAdd(A.next, 1ull);
@@ -819,109 +817,91 @@ __global__ void __launch_bounds__(kWarps * 32, 3) k_tess_stars(StarArgs A) {
     C.xyz = A.xyz;
     C.cell_start = A.cell_start;
     C.sorted = A.sorted;
-    C.cand = cand;
+    C.cx = cx;
+    C.cy = cy;
+    C.cz = cz;
+    C.cid = cid;
     C.p = p;
     C.lane = lane;
     C.bad = 0;
     C.stats = A.stats;
     for (int a = 0; a < 3; ++a) C.hi[a] = A.hi[3 * s + a];
     C.P = point(C, p);
-    // ---- candidates: the 5^3 (else 3^3) cells around p's cell
+    // ---- candidates: the points of the 5^3 cells around p's cell that lie
+    // within R of p, R being the distance from p to the block's faces (or a
+    // smaller radius holding at most kCandCap points, in dense clusters)
     const int lid = __ldg(&A.pcell[p]);
     const int ci[3] = {lid / (S.dims[1] * S.dims[2]), (lid / S.dims[2]) % S.dims[1], lid % S.dims[2]};
-    int rr = 2, c0[3], nc[3];
-    int cnt = block_count(S, A.cell_start, ci, rr, lane, c0, nc);
-    double rho2 = -1.0;  // >= 0: candidates limited to squared distance < rho2
-    if (cnt > kCandCap) {
-      rr = 1;
-      cnt = block_count(S, A.cell_start, ci, rr, lane, c0, nc);
-      if (cnt > kCandCap) {
-        // dense cluster: the largest radius (bisection on its square) within
-        // which the 3^3 block holds at most kCandCap points
-        double lo2 = 0.0, hi2 = 0.0;
-        const double Pd[3] = {C.P.x, C.P.y, C.P.z};
-        for (int a = 0; a < 3; ++a) {
-          double b0, b1, e0, e1;
-          cell_box(S, C.hi, c0[a], a, b0, b1);
-          cell_box(S, C.hi, c0[a] + nc[a] - 1, a, e0, e1);
-          const double m = fmax(Pd[a] - b0, e1 - Pd[a]);
-          hi2 += m * m;
-        }
-        for (int it = 0; it < 32; ++it) {
-          const double mid = 0.5 * (lo2 + hi2);
-          if (block_count_within(S, A.cell_start, A.sorted, c0, nc, lane, C.P, mid) <= kCandCap) lo2 = mid;
-          else hi2 = mid;
-        }
-        rho2 = lo2;
+    const int rr = 2;
+    int c0[3], nc[3];
+    double R = kInf, corner2 = 0.0;
+    {
+      const double Pd[3] = {C.P.x, C.P.y, C.P.z};
+      for (int a = 0; a < 3; ++a) {
+        c0[a] = max(0, ci[a] - rr);
+        nc[a] = min(S.dims[a] - 1, ci[a] + rr) - c0[a] + 1;
+        if (ci[a] - rr > 0) R = fmin(R, Pd[a] - (S.lo[a] + (ci[a] - rr) * S.h));
+        if (ci[a] + rr < S.dims[a] - 1) R = fmin(R, S.lo[a] + (ci[a] + rr + 1) * S.h - Pd[a]);
+        double b0, b1, e0, e1;
+        cell_box(S, C.hi, c0[a], a, b0, b1);
+        cell_box(S, C.hi, c0[a] + nc[a] - 1, a, e0, e1);
+        const double m = fmax(Pd[a] - b0, e1 - Pd[a]);
+        corner2 += m * m;
       }
     }
-    if (rho2 < 0.0) {
-      const int total = nc[0] * nc[1] * nc[2];
-      int base = 0;
-      for (int t0 = 0; t0 < total; t0 += 32) {
-        const int t = t0 + lane;
-        int c = 0, e0 = 0;
-        if (t < total) {
-          const int k = t % nc[2], j = (t / nc[2]) % nc[1], i = t / (nc[1] * nc[2]);
-          const int64_t g = S.cell0 + ((int64_t)(c0[0] + i) * S.dims[1] + (c0[1] + j)) * S.dims[2] + (c0[2] + k);
-          e0 = __ldg(&A.cell_start[g]);
-          c = __ldg(&A.cell_start[g + 1]) - e0;
-        }
-        int incl = c;
-        for (int off = 1; off < 32; off <<= 1) {
-          const int y = __shfl_up_sync(0xffffffffu, incl, off);
-          if (lane >= off) incl += y;
-        }
-        for (int q = 0; q < c; ++q) cand[base + incl - c + q] = __ldg(&A.sorted[e0 + q]);
-        base += __shfl_sync(0xffffffffu, incl, 31);
+    double thr2 = R < kInf ? R * R : corner2 * (1.0 + 1e-6);
+    if (block_count_within(C, c0, nc, thr2) > kCandCap) {
+      double lo2 = 0.0, hi2 = thr2;
+      for (int it = 0; it < 32; ++it) {
+        const double mid = 0.5 * (lo2 + hi2);
+        if (block_count_within(C, c0, nc, mid) <= kCandCap) lo2 = mid;
+        else hi2 = mid;
       }
-      C.ncand = base;
-    } else {
-      if (lane == 0) s_fill[wid] = 0;
-      __syncwarp();
+      thr2 = lo2;
+      R = fmin(R, sqrt(thr2) * (1.0 - 1e-12));
+    }
+    C.R = R - S.slack;
+    if (lane == 0) s_fill[wid] = 0;
+    __syncwarp();
+    {
       const int total = nc[0] * nc[1] * nc[2];
+      bool dup = false;
       for (int t = lane; t < total; t += 32) {
         const int k = t % nc[2], j = (t / nc[2]) % nc[1], i = t / (nc[1] * nc[2]);
         const int64_t g = S.cell0 + ((int64_t)(c0[0] + i) * S.dims[1] + (c0[1] + j)) * S.dims[2] + (c0[2] + k);
         const int e1 = __ldg(&A.cell_start[g + 1]);
         for (int e = __ldg(&A.cell_start[g]); e < e1; ++e) {
           const float4 x4 = __ldg(&A.sorted[e]);
-          const double dx = (double)x4.x - C.P.x, dy = (double)x4.y - C.P.y, dz = (double)x4.z - C.P.z;
-          if (dx * dx + dy * dy + dz * dz < rho2) {
+          const int id = __float_as_int(x4.w);
+          if (id == p) continue;
+          double d[3];
+          rel(C, f3(x4), d);
+          const double d2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+          if (d2 == 0.0) dup = true;
+          if (d2 < thr2) {
             const int slot = atomicAdd(&s_fill[wid], 1);
-            if (slot < kCandCap) cand[slot] = x4;
+            if (slot < kCandCap) {
+              cx[slot] = d[0];
+              cy[slot] = d[1];
+              cz[slot] = d[2];
+              cid[slot] = id;
+            }
           }
         }
       }
       __syncwarp();
       C.ncand = min(s_fill[wid], kCandCap);
-      __syncwarp();
+      if (ballot(dup)) fail(C, kFlagDegenerate, kWhyDuplicate);  // duplicates of p stop the set
     }
     __syncwarp();
-    {
-      double R = kInf;
-      const double Pd[3] = {C.P.x, C.P.y, C.P.z};
-      for (int a = 0; a < 3; ++a) {
-        if (ci[a] - rr > 0) R = fmin(R, Pd[a] - (S.lo[a] + (ci[a] - rr) * S.h));
-        if (ci[a] + rr < S.dims[a] - 1) R = fmin(R, S.lo[a] + (ci[a] + rr + 1) * S.h - Pd[a]);
-      }
-      if (rho2 >= 0.0) R = fmin(R, sqrt(rho2) * (1.0 - 1e-12));
-      C.R = R - S.slack;
-    }
-    // ---- nearest neighbour q (a Delaunay edge); duplicates of p stop the set
+    // ---- nearest neighbour q (a Delaunay edge)
     int q = -1;
-    float3 Q = C.P;
-    {
+    if (!C.bad) {
       double bd = kInf;
       int bi = 0x7fffffff;
-      bool dup = false;
       for (int j = lane; j < C.ncand; j += 32) {
-        const float4 c4 = cand[j];
-        const int id = __float_as_int(c4.w);
-        if (id == p) continue;
-        if (c4.x == C.P.x && c4.y == C.P.y && c4.z == C.P.z) dup = true;
-        const double dx = (double)c4.x - C.P.x, dy = (double)c4.y - C.P.y, dz = (double)c4.z - C.P.z;
-        const double d2 = dx * dx + dy * dy + dz * dz;
+        const double d2 = cx[j] * cx[j] + cy[j] * cy[j] + cz[j] * cz[j];
+        const int id = cid[j];
         if (d2 < bd || (d2 == bd && id < bi)) { bd = d2; bi = id; }
       }
       for (int off = 16; off; off >>= 1) {
@@ -929,24 +909,22 @@ __global__ void __launch_bounds__(kWarps * 32, 3) k_tess_stars(StarArgs A) {
         const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
         if (od < bd || (od == bd && oi < bi)) { bd = od; bi = oi; }
       }
-      if (ballot(dup)) fail(C, kFlagDegenerate, kWhyDuplicate);
-      if (bi != 0x7fffffff) { q = bi; Q = point(C, q); }
+      if (bi != 0x7fffffff) q = bi;
     }
     // ---- r: smallest circumradius of (p, q, r)
     int r = -1;
-    float3 Rr = C.P;
-    if (q >= 0 && !C.bad) {
-      const double a[3] = {(double)Q.x - C.P.x, (double)Q.y - C.P.y, (double)Q.z - C.P.z};
+    if (q >= 0) {
+      double a[3];
+      rel(C, point(C, q), a);
       const double la = a[0] * a[0] + a[1] * a[1] + a[2] * a[2];
       double br = kInf;
       int bi = 0x7fffffff;
       for (int j = lane; j < C.ncand; j += 32) {
-        const float4 c4 = cand[j];
-        const int id = __float_as_int(c4.w);
-        if (id == p || id == q) continue;
-        const double b[3] = {(double)c4.x - C.P.x, (double)c4.y - C.P.y, (double)c4.z - C.P.z};
-        const double cx = a[1] * b[2] - a[2] * b[1], cy = a[2] * b[0] - a[0] * b[2], cz = a[0] * b[1] - a[1] * b[0];
-        const double cr = cx * cx + cy * cy + cz * cz;
+        const int id = cid[j];
+        if (id == q) continue;
+        const double b[3] = {cx[j], cy[j], cz[j]};
+        const double ux = a[1] * b[2] - a[2] * b[1], uy = a[2] * b[0] - a[0] * b[2], uz = a[0] * b[1] - a[1] * b[0];
+        const double cr = ux * ux + uy * uy + uz * uz;
         if (!(cr > 0.0)) continue;
         const double lb = b[0] * b[0] + b[1] * b[1] + b[2] * b[2];
         const double d[3] = {a[0] - b[0], a[1] - b[1], a[2] - b[2]};
@@ -958,19 +936,18 @@ __global__ void __launch_bounds__(kWarps * 32, 3) k_tess_stars(StarArgs A) {
         const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
         if (od < br || (od == br && oi < bi)) { br = od; bi = oi; }
       }
-      if (bi != 0x7fffffff) { r = bi; Rr = point(C, r); }
+      if (bi != 0x7fffffff) r = bi;
     }
     if (!C.bad && (q < 0 || r < 0)) fail(C, q < 0 ? kFlagCapacity : kFlagDegenerate, kWhyNoStart);
     // ---- first tetrahedron: (p, q, r) closed on either side
     int nt = 0;
     if (!C.bad) {
-      float3 W;
-      int w = wrap(C, q, Q, r, Rr, -1, C.P, true, W);
+      int w = wrap(C, q, r, -1);
       if (w >= 0) {
         if (lane == 0) tri[0] = make_int4(q, r, w, 7);
         nt = 1;
       } else if (w == -1) {
-        w = wrap(C, r, Rr, q, Q, -1, C.P, true, W);
+        w = wrap(C, r, q, -1);
         if (w >= 0) {
           if (lane == 0) tri[0] = make_int4(r, q, w, 7);
           nt = 1;
@@ -980,10 +957,12 @@ __global__ void __launch_bounds__(kWarps * 32, 3) k_tess_stars(StarArgs A) {
       }
     }
     __syncwarp();
-    // ---- grow the star across the open edges of its link
+    // ---- grow the star across the open edges of its link; a triangle whose
+    // edges are all closed stays closed, so the search starts at a cursor
+    int cursor = 0;
     for (int iter = 0; !C.bad && iter < 3 * kTriCap + 8; ++iter) {
       int ft = -1, fe = 0;
-      for (int t0 = 0; t0 < nt; t0 += 32) {
+      for (int t0 = cursor; t0 < nt; t0 += 32) {
         const int t = t0 + lane;
         const int m = t < nt ? (tri[t].w & 7) : 0;
         const unsigned b = ballot(m != 0);
@@ -995,13 +974,12 @@ __global__ void __launch_bounds__(kWarps * 32, 3) k_tess_stars(StarArgs A) {
         }
       }
       if (ft < 0) break;  // closed (or bounded by hull faces)
+      cursor = ft;
       const int4 T = tri[ft];
       int x, y;
       tri_edge(T, fe, x, y);
       const int c3 = fe == 0 ? T.z : (fe == 1 ? T.x : T.y);  // T's vertex off the crossed edge
-      const float3 X = point(C, x), Y = point(C, y), Z = point(C, c3);
-      float3 W;
-      const int w = wrap(C, y, Y, x, X, c3, Z, false, W);
+      const int w = wrap(C, y, x, c3);
       __syncwarp();
       if (w == -2) break;
       if (lane == 0) tri[ft].w &= ~(1 << fe);

@@ -279,7 +279,7 @@ struct Sphere {
   bool ok;
 };
 
-__device__ Sphere circum_rel(const double* A, const double* B, const double* C) {
+__device__ __forceinline__ Sphere circum_rel(const double* A, const double* B, const double* C) {
   Sphere S;
   const double la = A[0] * A[0] + A[1] * A[1] + A[2] * A[2];
   const double lb = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];
@@ -657,28 +657,55 @@ __device__ __noinline__ int halfspace_scan(Ctx& C, const Face& F, int c) {
 // being a Delaunay face).  Returns w >= 0, -1 when no point lies beyond the
 // face (a hull face), -2 on failure (flag set).  (p, v, u, c) is the
 // certified tetrahedron on the other side (c < 0: none).
+__device__ __noinline__ int orient_slow(const Ctx& C, const Face& F, int id) {
+  return orient_exact_f(C.P, point(C, F.u), point(C, F.v), point(C, id));
+}
+
+__device__ __noinline__ int insphere_slow(const Ctx& C, const Face& F, int b, int id) {
+  return insphere_f(C.P, point(C, F.u), point(C, F.v), point(C, b), point(C, id));
+}
+
 __device__ __noinline__ int wrap(Ctx& C, int u, int v, int c) {
   const Face F = make_face(C, u, v);
+  // the loops below run on register copies (F and C live in memory: their
+  // addresses go to the out-of-line scans)
+  const double n0 = F.n[0], n1 = F.n[1], n2 = F.n[2], m0 = F.na[0], m1 = F.na[1], m2 = F.na[2];
+  const double fa[3] = {F.a[0], F.a[1], F.a[2]}, fb[3] = {F.b[0], F.b[1], F.b[2]};
+  const double* __restrict__ cx = C.cx;
+  const double* __restrict__ cy = C.cy;
+  const double* __restrict__ cz = C.cz;
+  const int* __restrict__ cid = C.cid;
+  const int ncand = C.ncand, lane = C.lane;
   int best = -1, flag = 0;
   double bd[3] = {0.0, 0.0, 0.0};
   Sphere sb;
   sb.ok = false;
   // gift wrapping over the candidates: each lane keeps the best of its share
-  for (int j = C.lane; j < C.ncand; j += 32) {
-    const int id = C.cid[j];
+  for (int j = lane; j < ncand; j += 32) {
+    const int id = cid[j];
     if (id == u || id == v) continue;
-    const double d[3] = {C.cx[j], C.cy[j], C.cz[j]};
+    const double d[3] = {cx[j], cy[j], cz[j]};
     if (best >= 0) {
-      const int si = insphere_face(C, F, best, sb, d, id);
+      int si = 0;
+      if (sb.ok) {
+        const double ex = d[0] - sb.c[0], ey = d[1] - sb.c[1], ez = d[2] - sb.c[2];
+        const double e2 = ex * ex + ey * ey + ez * ez;
+        const double hi = sb.r + 2.0 * sb.err, lo = sb.r - 2.0 * sb.err;
+        if (e2 > hi * hi * (1.0 + 1e-9)) si = -1;
+        else if (lo > 0.0 && e2 < lo * lo * (1.0 - 1e-9)) si = 1;
+      }
+      if (si == 0) si = insphere_slow(C, F, best, id);
       if (si == 2) { flag = 1; continue; }
       if (si <= 0) continue;
     }
-    const int o = orient_face(C, F, d, id);
+    const double det = d[0] * n0 + d[1] * n1 + d[2] * n2;
+    const double bound = kOrientErr * (fabs(d[0]) * m0 + fabs(d[1]) * m1 + fabs(d[2]) * m2);
+    const int o = det > bound ? 1 : (-det > bound ? -1 : orient_slow(C, F, id));
     if (o == 2) { flag = 1; continue; }
     if (o <= 0) continue;
     best = id;
     bd[0] = d[0]; bd[1] = d[1]; bd[2] = d[2];
-    sb = circum_rel(F.a, F.b, d);
+    sb = circum_rel(fa, fb, d);
   }
   if (ballot(flag != 0)) {
     fail(C, kFlagUndecided, kWhyUndecided);
@@ -695,7 +722,7 @@ __device__ __noinline__ int wrap(Ctx& C, int u, int v, int c) {
     from_cands = false;
   }
   for (int it = 0; it < 4; ++it) {
-    const Sphere Sp = circum_rel(F.a, F.b, Wd);
+    const Sphere Sp = circum_rel(fa, fb, Wd);
     if (!Sp.ok) {
       fail(C, kFlagUndecided, kWhyUndecided);
       return -2;
@@ -703,12 +730,16 @@ __device__ __noinline__ int wrap(Ctx& C, int u, int v, int c) {
     if (from_cands && 2.0 * (Sp.r + Sp.err) * (1.0 + 1e-9) < C.R) {
       // the sphere lies in the candidate ball: verify it against every
       // candidate (a point on it is a tie; one inside cannot occur)
+      const double hi = Sp.r + 2.0 * Sp.err, lo = Sp.r - 2.0 * Sp.err;
+      const double hi2 = hi * hi * (1.0 + 1e-9), lo2 = lo > 0.0 ? lo * lo * (1.0 - 1e-9) : -1.0;
       int bad = 0;
-      for (int j = C.lane; j < C.ncand; j += 32) {
-        const int id = C.cid[j];
+      for (int j = lane; j < ncand; j += 32) {
+        const int id = cid[j];
         if (id == u || id == v || id == w) continue;
-        const double d[3] = {C.cx[j], C.cy[j], C.cz[j]};
-        const int si = insphere_face(C, F, w, Sp, d, id);
+        const double ex = cx[j] - Sp.c[0], ey = cy[j] - Sp.c[1], ez = cz[j] - Sp.c[2];
+        const double e2 = ex * ex + ey * ey + ez * ez;
+        if (e2 > hi2) continue;
+        const int si = e2 < lo2 ? 1 : insphere_slow(C, F, w, id);
         if (si == 2) bad |= 1;
         else if (si == 0) bad |= 2;
         else if (si > 0) bad |= 4;

@@ -510,8 +510,11 @@ __device__ __noinline__ int sphere_scan(Ctx& C, const Face& F, int w, const Sphe
   for (int a = 1; a < 3; ++a)
     if (fabs(Sp.c[a]) > fabs(Sp.c[a2])) a2 = a;
   const int a0 = a2 == 0 ? 1 : 0, a1 = a2 == 2 ? 1 : 2;
-  const int i0 = cell_coord(S, cen[a0] - rad, a0), i1 = cell_coord(S, cen[a0] + rad, a0);
-  const int j0 = cell_coord(S, cen[a1] - rad, a1), j1 = cell_coord(S, cen[a1] + rad, a1);
+  // a centre beyond the grid along a2 reaches it only within a disk
+  const double gz = cen[a2] < S.lo[a2] ? S.lo[a2] - cen[a2] : (cen[a2] > C.hi[a2] ? cen[a2] - C.hi[a2] : 0.0);
+  const double reach = sqrt(fmax(0.0, rad * rad * (1.0 + 1e-9) - gz * gz)) * (1.0 + 1e-9) + S.slack;
+  const int i0 = cell_coord(S, cen[a0] - reach, a0), i1 = cell_coord(S, cen[a0] + reach, a0);
+  const int j0 = cell_coord(S, cen[a1] - reach, a1), j1 = cell_coord(S, cen[a1] + reach, a1);
   const int nj = j1 - j0 + 1;
   const int ncol = (i1 - i0 + 1) * nj;
   int best = -1, flag = 0, why = 0;

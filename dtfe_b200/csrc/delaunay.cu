@@ -1386,8 +1386,8 @@ extern "C" {
 int dtfe_gpu_tessellate(void* stream, int32_t n_sets, const int64_t* vprefix, const float* xyz_dev, void** out) {
   if (!out) return dtfe_internal_set_error(DTFE_ERR_ARG, "dtfe_gpu_tessellate: out is NULL");
   *out = nullptr;
-  if (n_sets < 1 || n_sets > 65535 || !vprefix || !xyz_dev)
-    return dtfe_internal_set_error(DTFE_ERR_ARG, "dtfe_gpu_tessellate: need 1..65535 sets, vprefix and xyz");
+  if (n_sets < 1 || n_sets > 65535 || !vprefix)
+    return dtfe_internal_set_error(DTFE_ERR_ARG, "dtfe_gpu_tessellate: need 1..65535 sets and vprefix");
   const int K = n_sets;
   if (vprefix[0] != 0) return dtfe_internal_set_error(DTFE_ERR_ARG, "dtfe_gpu_tessellate: vprefix[0] must be 0");
   int64_t maxn = 0;
@@ -1397,6 +1397,7 @@ int dtfe_gpu_tessellate(void* stream, int32_t n_sets, const int64_t* vprefix, co
     maxn = std::max<int64_t>(maxn, vprefix[s + 1] - vprefix[s]);
   }
   const int64_t V = vprefix[K];
+  if (V > 0 && !xyz_dev) return dtfe_internal_set_error(DTFE_ERR_ARG, "dtfe_gpu_tessellate: xyz is NULL");
   std::vector<int64_t> cpre(K + 1, 0), opre(K + 1, 0);
   for (int s = 0; s < K; ++s) {
     const int64_t n = vprefix[s + 1] - vprefix[s];

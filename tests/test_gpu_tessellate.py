@@ -55,9 +55,9 @@ def test_clustered_set(built):
 
 
 def test_ties_and_bad_input_are_reported(built):
-    """A cubic lattice (co-spherical corners), a non-finite coordinate and a
-    three-point set give non-zero status and no tetrahedra; a good set in
-    the same call is still tessellated."""
+    """A cubic lattice (co-spherical corners), a non-finite coordinate, a
+    three-point set and an empty set give non-zero status and no tetrahedra;
+    a good set in the same call is still tessellated."""
     from dtfe_b200 import device as D
     g = np.arange(5, dtype=np.float32)
     lattice = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
@@ -66,9 +66,12 @@ def test_ties_and_bad_input_are_reported(built):
     nan = good.copy()
     nan[7, 1] = np.nan
     tiny = good[:3].copy()
-    out = D.tessellate([lattice, good, nan, tiny])
+    empty = np.zeros((0, 3), np.float32)
+    out = D.tessellate([lattice, good, nan, tiny, empty])
     assert out[0][1] & 1 and len(out[0][0]) == 0
     assert out[1][1] == 0
     assert np.array_equal(out[1][0], P.tessellate_many([good])[0][0])
     assert out[2][1] & 32 and len(out[2][0]) == 0
     assert out[3][1] & 32 and len(out[3][0]) == 0
+    assert out[4][1] & 32 and len(out[4][0]) == 0
+    assert D.tessellate([empty])[0][1] & 32

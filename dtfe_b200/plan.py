@@ -139,6 +139,42 @@ def axis_coords(lo: float, dx: float, n: int) -> np.ndarray:
     return out
 
 
+def tessellate_many_gpu(point_sets: list, device: int = 0):
+    """The same tessellations as tessellate_many, built on the GPU
+    (dtfe_gpu_tessellate, which reproduces the host tessellator's arrays):
+    a set the device reports (exact ties such as lattice inputs, capacity
+    limits) is tessellated on the host instead; the neighbours of all sets
+    are derived on the device (dtfe_gpu_upload without tet_n)."""
+    from . import device as D
+    out = D.tessellate(point_sets, device=device)
+    redo = [i for i, (_, st) in enumerate(out) if st != 0]
+    host = dict(zip(redo, tessellate_many([point_sets[i] for i in redo]))) if redo else {}
+    tvs = [host[i][0] if i in host else tv for i, (tv, _) in enumerate(out)]
+    voff = np.concatenate([[0], np.cumsum([len(p) for p in point_sets])]).astype(np.int64)
+    toff = np.concatenate([[0], np.cumsum([len(t) for t in tvs])]).astype(np.int64)
+    tv_all = np.ascontiguousarray(np.concatenate([t + np.int32(voff[i]) for i, t in enumerate(tvs)]).astype(np.int32))
+    xyz = np.ascontiguousarray(np.concatenate([np.asarray(p, np.float32).reshape(-1, 3) for p in point_sets]))
+    tn_all = np.empty_like(tv_all)
+    if len(tv_all):
+        class _Flat:  # the arrays dtfe_gpu_upload reads
+            pass
+        f = _Flat()
+        f.tet_v, f.tet_n, f.n_tets, f.xyz, f.n_verts = tv_all, None, len(tv_all), xyz, len(xyz)
+        f.weight, f.velocity, f.scalar = np.ones(len(xyz), np.float32), None, None
+        with D.DeviceDTFE(device) as dev:
+            dev.upload(f, neighbours=False)
+            _, tn_all = dev.download_tets(len(tv_all))
+    res = []
+    for i, tv in enumerate(tvs):
+        if i in host:
+            res.append(host[i])
+            continue
+        tn = tn_all[toff[i]:toff[i + 1]]
+        res.append((tv, np.where(tn >= 0, tn - np.int32(toff[i]), -1).astype(np.int32),
+                    np.arange(len(point_sets[i]), dtype=np.int32)))
+    return res
+
+
 def tessellate_many(point_sets: list, seed: int = 12345, sort_tets: bool = True):
     """Delaunay tessellations of several float32 point sets in parallel.
 
@@ -200,7 +236,8 @@ def _make_box(voff, nv, toff, nt, origin, dims, coff, dx, lo, part_no):
     return b
 
 
-def assemble(sets: list, tiles: list, weight, velocity, scalar, grid, rho_bar, padding, timings) -> Plan:
+def assemble(sets: list, tiles: list, weight, velocity, scalar, grid, rho_bar, padding, timings,
+             tessellator: str = "host") -> Plan:
     """Concatenates per-sub-box (positions, source ids) and their tessellations.
 
     sets:  [(src_idx int32, pos float32 (n,3))]
@@ -211,7 +248,12 @@ def assemble(sets: list, tiles: list, weight, velocity, scalar, grid, rho_bar, p
     sets = [(src[o], pos[o]) for src, pos in sets for o in [morton_order(pos)]]
     timings["vertex_sort_s"] = time.time() - t0
     t0 = time.time()
-    tess = tessellate_many([p for _, p in sets])
+    if tessellator == "gpu":
+        tess = tessellate_many_gpu([p for _, p in sets])
+    elif tessellator == "host":
+        tess = tessellate_many([p for _, p in sets])
+    else:
+        raise ValueError("tessellator must be 'host' or 'gpu'")
     timings["tessellation_s"] = time.time() - t0
     tv_all, tn_all, xyz_all, src_all = [], [], [], []
     xs, ys, zs, regions = [], [], [], []
@@ -287,11 +329,13 @@ def decompose(pos, weight, grid, box, periodic: bool, n_threads: int, pad):
 
 def make_plan(pos, weight, velocity=None, scalar=None, grid=(64, 64, 64), box=(0, 100, 0, 100, 0, 100),
               periodic: bool = True, n_threads: int = 1, padding_particles: float = 5.0,
-              padding=None, average_density_value: float | None = None) -> Plan:
+              padding=None, average_density_value: float | None = None, tessellator: str = "host") -> Plan:
     """Plans a single-box DTFE run split into parallelGrid(n_threads) sub-boxes.
 
     average_density_value=None reproduces the reference's automatic value
-    (sum of weights / 35000^3); pass sum(w)/L^3 for the physical normalisation."""
+    (sum of weights / 35000^3); pass sum(w)/L^3 for the physical normalisation.
+    tessellator="gpu" builds the sub-box tessellations on the GPU (the same
+    arrays as the host tessellator's; sets with exact ties go to the host)."""
     timings = {}
     t0 = time.time()
     pos = _f32(pos)
@@ -302,7 +346,7 @@ def make_plan(pos, weight, velocity=None, scalar=None, grid=(64, 64, 64), box=(0
     rho_bar = average_density(weight) if average_density_value is None else float(np.float32(average_density_value))
     sets, tiles = decompose(pos, weight, grid, box, periodic, n_threads, pad)
     timings["selection_s"] = time.time() - t0
-    return assemble(sets, tiles, weight, velocity, scalar, grid, rho_bar, pad, timings)
+    return assemble(sets, tiles, weight, velocity, scalar, grid, rho_bar, pad, timings, tessellator)
 
 
 @dataclass

@@ -75,3 +75,17 @@ def test_ties_and_bad_input_are_reported(built):
     assert out[3][1] & 32 and len(out[3][0]) == 0
     assert out[4][1] & 32 and len(out[4][0]) == 0
     assert D.tessellate([empty])[0][1] & 32
+
+
+def test_plan_with_gpu_tessellator(built):
+    """make_plan(tessellator="gpu"): the same tet_v and tet_n as the host
+    tessellator's plan, neighbours derived on the device; a perfect lattice
+    (every set tied) falls back to the host set by set."""
+    for rms in (1.0, 0.0):
+        pos, _ = S.zeldovich_lattice(20, 100.0, rms, seed=6)
+        w = np.ones(len(pos), np.float32)
+        a = P.make_plan(pos, w, None, None, grid=(20, 20, 20), n_threads=4)
+        b = P.make_plan(pos, w, None, None, grid=(20, 20, 20), n_threads=4, tessellator="gpu")
+        assert np.array_equal(a.tet_v, b.tet_v)
+        assert np.array_equal(a.tet_n, b.tet_n)
+        assert np.array_equal(a.xyz, b.xyz)

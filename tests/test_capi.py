@@ -67,3 +67,21 @@ def test_create_without_device_fails_cleanly(built):
     rc = lib.dtfe_gpu_create(ctypes.byref(cfg), ctypes.byref(h))
     assert rc == N.ERR_NO_DEVICE
     assert b"device" in lib.dtfe_last_error()
+
+
+def test_tessellate_argument_errors_without_device(built):
+    """dtfe_gpu_tessellate checks its arguments before any device call:
+    no sets, a decreasing or non-zero-based vertex prefix and missing
+    positions give DTFE_ERR_ARG and no handle."""
+    assert "dtfe_gpu_tessellate" in declared_functions("dtfe_gpu.h")
+    lib = ctypes.CDLL(build.build_gpu())
+    lib.dtfe_gpu_tessellate.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.POINTER(ctypes.c_void_p)]
+    out = ctypes.c_void_p(1)
+    assert lib.dtfe_gpu_tessellate(None, 0, None, None, ctypes.byref(out)) == 1
+    assert not out.value
+    for pre in ((0, 5, 3), (1, 5), (0, 5)):
+        arr = (ctypes.c_int64 * len(pre))(*pre)
+        out = ctypes.c_void_p(1)
+        assert lib.dtfe_gpu_tessellate(None, len(pre) - 1, arr, None, ctypes.byref(out)) == 1
+        assert not out.value

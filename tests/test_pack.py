@@ -126,3 +126,13 @@ def test_vertex_codes_non_periodic():
     assert np.all((codes >> np.uint32(27)) == 13)
     src = codes & np.uint32((1 << 27) - 1)
     assert np.array_equal(pos[src], plan.xyz)
+
+
+def test_plan_rejects_unknown_tessellator():
+    """make_plan's tessellator is "host" (default) or "gpu"."""
+    from dtfe_b200 import plan as P
+    from dtfe_b200 import synthetic as S
+    pos, _ = S.zeldovich_lattice(8, 100.0, 1.0, seed=3)
+    with pytest.raises(ValueError):
+        P.make_plan(pos, np.ones(len(pos), np.float32), None, None, grid=(8, 8, 8), n_threads=2,
+                    tessellator="qhull")

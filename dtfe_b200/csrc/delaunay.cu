@@ -9,9 +9,11 @@
 // tests that decide it) the arrays equal the host's bit for bit.
 //
 // Method: star construction.  Every vertex p is handled by one warp, which
-//   1. gathers the points of the 5^3 grid cells around p's cell (a uniform
-//      grid of about two points per cell) into shared memory: every point
-//      closer to p than the block's faces is a candidate;
+//   1. gathers, from the 5^3 grid cells around p's cell (a uniform grid of
+//      about two points per cell), the points closer to p than R, the
+//      distance from p to the block's faces (a smaller radius holding at most
+//      256 points in a dense cluster), into shared memory as double offsets
+//      from p: every point within R of p is a candidate;
 //   2. starts from p's nearest neighbour q, the candidate r whose triangle
 //      pqr has the smallest circumradius (the smallest sphere through p, q, r
 //      is then empty) and the apex s that closes pqr to a tetrahedron;
@@ -21,11 +23,13 @@
 //      such point (gift wrapping; the spheres through p, v, u form a pencil
 //      ordered by the position of their centre along the face normal);
 //   4. certifies every tetrahedron it adds: its circumsphere is empty of all
-//      points of the set.  Spheres inside the candidate ball are covered by
-//      step 3 itself; larger ones are checked against every point of the grid
-//      cells they touch, and a point found inside replaces the apex.  A link
-//      edge without any point beyond it (certified over the whole grid) lies
-//      on the convex hull;
+//      points of the set.  A sphere inside the candidate ball is checked
+//      against every candidate; a larger one against every point of the grid
+//      columns it reaches (along the axis towards its centre), and the best
+//      point found inside replaces the apex.  A link edge without any point
+//      beyond it (certified by a column scan of the half-space) lies on the
+//      convex hull; a point exactly on such a face's plane is harmless
+//      outside the face's circumcircle;
 //   5. emits the tetrahedra of its star whose smallest vertex is p.
 // Orientation and in-sphere signs are exact: a double-precision evaluation
 // with a forward error bound (the host predicates' constants), else the

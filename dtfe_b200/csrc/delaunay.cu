@@ -451,7 +451,7 @@ __device__ __forceinline__ int insphere_face(const Ctx& C, const Face& F, int b,
 // in-sphere sign (an exact tie keeps the current winner: the verification of
 // the winner's sphere reports it).  Returns the id (offset in Wd), -1 when no
 // lane has one, -2 on failure (flag set).
-__device__ __noinline__ int warp_select(Ctx& C, const Face& F, int best, const double* bd, const Sphere& sb,
+__device__ __forceinline__ int warp_select(Ctx& C, const Face& F, int best, const double* bd, const Sphere& sb,
                                         double* Wd) {
   double lo = kInf, hi = kInf;
   if (best >= 0) {

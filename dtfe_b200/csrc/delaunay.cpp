@@ -79,7 +79,7 @@ struct MortonFrame {
 struct Tessellator {
   const double* P;
   int64_t n;
-  std::vector<int32_t> tv, tn;
+  std::vector<int32_t> cells;  // per tetrahedron: 4 vertices, then 4 neighbours (one 32-byte record)
   std::vector<uint32_t> mark;
   std::vector<int32_t> freelist;
   std::vector<int32_t> vmap;
@@ -107,30 +107,29 @@ struct Tessellator {
       freelist.pop_back();
       return t;
     }
-    int32_t t = (int32_t)(tv.size() / 4);
-    tv.resize(tv.size() + 4);
-    tn.resize(tn.size() + 4);
+    int32_t t = (int32_t)(cells.size() / 8);
+    cells.resize(cells.size() + 8);
     mark.push_back(0);
     return t;
   }
 
   int inf_index(int32_t t) const {
     for (int k = 0; k < 4; ++k)
-      if (tv[4 * t + k] == INF) return k;
+      if (cells[8 * (int64_t)t + k] == INF) return k;
     return -1;
   }
 
   // orientation of tetrahedron t with vertex k replaced by point p
   int orient_with(int32_t t, int k, const double* p) const {
     const double* q[4];
-    for (int i = 0; i < 4; ++i) q[i] = (i == k) ? p : pt(tv[4 * t + i]);
+    for (int i = 0; i < 4; ++i) q[i] = (i == k) ? p : pt(cells[8 * (int64_t)t + i]);
     return dtfe::orient(q[0], q[1], q[2], q[3]);
   }
 
   bool conflict(int32_t t, const double* p) const {
     int k = inf_index(t);
     if (k < 0) {
-      const int32_t* v = &tv[4 * t];
+      const int32_t* v = &cells[8 * (int64_t)t];
       return dtfe::insphere(pt(v[0]), pt(v[1]), pt(v[2]), pt(v[3]), p) > 0;
     }
     int o = orient_with(t, k, p);
@@ -139,8 +138,8 @@ struct Tessellator {
     // p on the plane of the hull face: in conflict iff it lies inside the
     // face's circumcircle, i.e. inside the circumsphere of the finite
     // neighbour across that face.
-    int32_t f = tn[4 * t + k];
-    const int32_t* v = &tv[4 * f];
+    int32_t f = cells[8 * (int64_t)t + 4 + k];
+    const int32_t* v = &cells[8 * (int64_t)f];
     return dtfe::insphere(pt(v[0]), pt(v[1]), pt(v[2]), pt(v[3]), p) > 0;
   }
 
@@ -152,7 +151,7 @@ struct Tessellator {
     int k = inf_index(t);
     if (k >= 0) {
       if (orient_with(t, k, p) > 0) return t;
-      t = tn[4 * t + k];
+      t = cells[8 * (int64_t)t + 4 + k];
     }
     int32_t prev = -1;
     uint32_t rot = 0;
@@ -160,7 +159,7 @@ struct Tessellator {
       bool moved = false;
       for (int j = 0; j < 4; ++j) {
         int i = (int)((j + rot) & 3);
-        int32_t nb = tn[4 * t + i];
+        int32_t nb = cells[8 * (int64_t)t + 4 + i];
         if (nb == prev) continue;
         if (orient_with(t, i, p) < 0) {
           prev = t;
@@ -173,15 +172,15 @@ struct Tessellator {
       if (inf_index(t) >= 0) return t;  // crossed a hull face
       rot = rot * 1103515245u + 12345u;
       rot >>= 16;
-      if (step > 4 * (int64_t)(tv.size() / 4) + 1000) {
+      if (step > 4 * (int64_t)(cells.size() / 8) + 1000) {
         status = 2;
         return t;
       }
     }
     for (int i = 0; i < 4; ++i) {
-      const double* q = pt(tv[4 * t + i]);
+      const double* q = pt(cells[8 * (int64_t)t + i]);
       if (q[0] == p[0] && q[1] == p[1] && q[2] == p[2]) {
-        dup = tv[4 * t + i];
+        dup = cells[8 * (int64_t)t + i];
         return t;
       }
     }
@@ -218,8 +217,8 @@ struct Tessellator {
       if (hkey[h] == key) {
         int32_t ot = hval[h] >> 2;
         int om = hval[h] & 3;
-        tn[4 * nt + m] = ot;
-        tn[4 * ot + om] = nt;
+        cells[8 * (int64_t)nt + 4 + m] = ot;
+        cells[8 * (int64_t)ot + 4 + om] = nt;
         hkey[h] = ~0ULL;  // consumed: each interior face has one twin
         return;
       }
@@ -249,7 +248,7 @@ struct Tessellator {
       stack.pop_back();
       cavity.push_back(t);
       for (int k = 0; k < 4; ++k) {
-        int32_t u = tn[4 * t + k];
+        int32_t u = cells[8 * (int64_t)t + 4 + k];
         if (mark[u] == s_in) continue;
         if (mark[u] == s_out) {
           boundary.emplace_back(t, k);
@@ -269,15 +268,15 @@ struct Tessellator {
     for (auto& bf : boundary) {
       int32_t t = bf.first;
       int k = bf.second;
-      int32_t u = tn[4 * t + k];
+      int32_t u = cells[8 * (int64_t)t + 4 + k];
       int32_t nt = new_tet();
       mark[nt] = 0;
-      for (int i = 0; i < 4; ++i) tv[4 * nt + i] = tv[4 * t + i];
-      tv[4 * nt + k] = pi;
-      tn[4 * nt + k] = u;
+      for (int i = 0; i < 4; ++i) cells[8 * (int64_t)nt + i] = cells[8 * (int64_t)t + i];
+      cells[8 * (int64_t)nt + k] = pi;
+      cells[8 * (int64_t)nt + 4 + k] = u;
       for (int j = 0; j < 4; ++j)
-        if (tn[4 * u + j] == t) {
-          tn[4 * u + j] = nt;
+        if (cells[8 * (int64_t)u + 4 + j] == t) {
+          cells[8 * (int64_t)u + 4 + j] = nt;
           break;
         }
       created.push_back(nt);
@@ -290,12 +289,12 @@ struct Tessellator {
         int32_t e[2];
         int ne = 0;
         for (int i = 0; i < 4; ++i)
-          if (i != m && i != k) e[ne++] = tv[4 * nt + i];
+          if (i != m && i != k) e[ne++] = cells[8 * (int64_t)nt + i];
         hash_link(e[0], e[1], nt, m);
       }
     }
     for (int32_t t : cavity) {
-      tv[4 * t] = tv[4 * t + 1] = tv[4 * t + 2] = tv[4 * t + 3] = -2;
+      cells[8 * (int64_t)t] = cells[8 * (int64_t)t + 1] = cells[8 * (int64_t)t + 2] = cells[8 * (int64_t)t + 3] = -2;
       freelist.push_back(t);
     }
     hint = created.back();
@@ -339,14 +338,14 @@ struct Tessellator {
     if (dtfe::orient(pt(v[0]), pt(v[1]), pt(v[2]), pt(v[3])) < 0) std::swap(v[2], v[3]);
     int32_t T[5];
     for (int i = 0; i < 5; ++i) T[i] = new_tet();
-    for (int i = 0; i < 4; ++i) tv[4 * T[0] + i] = v[i];
+    for (int i = 0; i < 4; ++i) cells[8 * (int64_t)T[0] + i] = v[i];
     for (int k = 0; k < 4; ++k) {
       int32_t t = T[1 + k];
-      for (int i = 0; i < 4; ++i) tv[4 * t + i] = v[i];
-      tv[4 * t + k] = INF;
+      for (int i = 0; i < 4; ++i) cells[8 * (int64_t)t + i] = v[i];
+      cells[8 * (int64_t)t + k] = INF;
       // the infinite vertex lies on the far side of face k: flip orientation
       int a = (k + 1) & 3, b = (k + 2) & 3;
-      std::swap(tv[4 * t + a], tv[4 * t + b]);
+      std::swap(cells[8 * (int64_t)t + a], cells[8 * (int64_t)t + b]);
     }
     for (int x = 0; x < 5; ++x)
       for (int y = 0; y < 5; ++y) {
@@ -358,9 +357,9 @@ struct Tessellator {
           for (int a = 0; a < 4; ++a) {
             if (a == i) continue;
             for (int b = 0; b < 4; ++b)
-              if (tv[4 * ty + b] == tv[4 * tx + a]) { ++shared; break; }
+              if (cells[8 * (int64_t)ty + b] == cells[8 * (int64_t)tx + a]) { ++shared; break; }
           }
-          if (shared == 3) tn[4 * tx + i] = ty;
+          if (shared == 3) cells[8 * (int64_t)tx + 4 + i] = ty;
         }
       }
     hint = T[0];
@@ -398,8 +397,7 @@ struct Tessellator {
       }
     }
     size_t reserve = (size_t)(n * 7.2) + 64;
-    tv.reserve(4 * reserve);
-    tn.reserve(4 * reserve);
+    cells.reserve(8 * reserve);
     mark.reserve(reserve);
     int used[4];
     if (!init(order, used)) return 1;
@@ -419,12 +417,12 @@ struct Result {
 };
 
 void compact(Tessellator& T, bool sort_tets, Result& R) {
-  int64_t cap = (int64_t)T.tv.size() / 4;
+  int64_t cap = (int64_t)T.cells.size() / 8;
   std::vector<int32_t> newid(cap, -1);
   std::vector<int32_t> finite;
   finite.reserve(cap);
   for (int64_t t = 0; t < cap; ++t) {
-    const int32_t* v = &T.tv[4 * t];
+    const int32_t* v = &T.cells[8 * (int64_t)t];
     if (v[0] < 0 || v[1] < 0 || v[2] < 0 || v[3] < 0) continue;  // infinite or freed
     finite.push_back((int32_t)t);
   }
@@ -437,7 +435,7 @@ void compact(Tessellator& T, bool sort_tets, Result& R) {
                                    {3, 1, 0, 2}, {3, 2, 1, 0}};
   std::vector<int8_t> perm(cap, 0);
   for (int32_t t : finite) {
-    const int32_t* v = &T.tv[4 * (int64_t)t];
+    const int32_t* v = &T.cells[8 * (int64_t)((int64_t)t)];
     int best = 0;
     for (int q = 1; q < 12; ++q)
       for (int k = 0; k < 4; ++k) {
@@ -449,32 +447,53 @@ void compact(Tessellator& T, bool sort_tets, Result& R) {
       }
     perm[t] = (int8_t)best;
   }
-  auto vert = [&](int64_t t, int k) { return T.tv[4 * t + kEven[perm[t]][k]]; };
+  auto vert = [&](int64_t t, int k) { return T.cells[8 * (int64_t)t + kEven[perm[t]][k]]; };
   if (sort_tets && !finite.empty()) {
+    // order: Morton key of the centroid, then the vertex tuple (a total
+    // order: no two tetrahedra share their vertices).  An LSD radix sort of
+    // the keys (stable, 8 bits per pass) and a tuple sort inside each run of
+    // equal keys give exactly that order.
     MortonFrame frame(T.P, T.n);
-    struct Key {
-      uint64_t m;
-      int32_t v[4];
-      int32_t t;
-      bool operator<(const Key& o) const {
-        if (m != o.m) return m < o.m;
-        for (int k = 0; k < 4; ++k)
-          if (v[k] != o.v[k]) return v[k] < o.v[k];
-        return false;
-      }
-    };
-    std::vector<Key> keyed(finite.size());
-    for (size_t i = 0; i < finite.size(); ++i) {
+    const size_t nf = finite.size();
+    std::vector<uint64_t> key(nf), key2(nf);
+    std::vector<int32_t> ord(nf), ord2(nf);
+    for (size_t i = 0; i < nf; ++i) {
       const int64_t t = finite[i];
       double c[3] = {0, 0, 0};
       for (int a = 0; a < 4; ++a)
         for (int k = 0; k < 3; ++k) c[k] += 0.25 * T.pt(vert(t, a))[k];
-      keyed[i].m = frame.key(c);
-      for (int a = 0; a < 4; ++a) keyed[i].v[a] = vert(t, a);
-      keyed[i].t = (int32_t)t;
+      key[i] = frame.key(c);
+      ord[i] = (int32_t)i;
     }
-    std::sort(keyed.begin(), keyed.end());
-    for (size_t i = 0; i < finite.size(); ++i) finite[i] = keyed[i].t;
+    for (int shift = 0; shift < 64; shift += 8) {
+      size_t count[257] = {0};
+      for (size_t i = 0; i < nf; ++i) ++count[((key[i] >> shift) & 0xff) + 1];
+      if (count[1 + ((key[0] >> shift) & 0xff)] == nf) continue;  // one digit value: nothing to move
+      for (int d = 0; d < 256; ++d) count[d + 1] += count[d];
+      for (size_t i = 0; i < nf; ++i) {
+        const size_t dst = count[(key[i] >> shift) & 0xff]++;
+        key2[dst] = key[i];
+        ord2[dst] = ord[i];
+      }
+      key.swap(key2);
+      ord.swap(ord2);
+    }
+    auto tuple_less = [&](int32_t x, int32_t y) {
+      for (int a = 0; a < 4; ++a) {
+        const int32_t vx = vert(finite[x], a), vy = vert(finite[y], a);
+        if (vx != vy) return vx < vy;
+      }
+      return false;
+    };
+    for (size_t i = 0; i < nf;) {
+      size_t j = i + 1;
+      while (j < nf && key[j] == key[i]) ++j;
+      if (j - i > 1) std::sort(ord.begin() + i, ord.begin() + j, tuple_less);
+      i = j;
+    }
+    std::vector<int32_t> sorted(nf);
+    for (size_t i = 0; i < nf; ++i) sorted[i] = finite[ord[i]];
+    finite.swap(sorted);
   }
   for (size_t i = 0; i < finite.size(); ++i) newid[finite[i]] = (int32_t)i;
   R.tet_v.resize(4 * finite.size());
@@ -483,8 +502,8 @@ void compact(Tessellator& T, bool sort_tets, Result& R) {
     int64_t t = finite[i];
     for (int k = 0; k < 4; ++k) {
       const int src = kEven[perm[t]][k];
-      R.tet_v[4 * i + k] = T.tv[4 * t + src];
-      int32_t nb = T.tn[4 * t + src];
+      R.tet_v[4 * i + k] = T.cells[8 * (int64_t)t + src];
+      int32_t nb = T.cells[8 * (int64_t)t + 4 + src];
       R.tet_n[4 * i + k] = newid[nb];  // -1 for an infinite neighbour
     }
   }
